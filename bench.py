@@ -1,0 +1,456 @@
+#!/usr/bin/env python
+"""bench.py -- DSPSR baseband hot path on B200: unpack -> overlap-save coherent
+dedispersion -> detection -> fold, in complex Msamples/s.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                  [--config c1]
+
+One step = one block of the workload processed end to end (unpack -> fold),
+the InputBuffering overlap carried from block to block.  Inputs are seeded
+synthetic baseband (Gaussian noise plus a pulse train dispersed by an FP64
+inverse chirp); blocks cycle through four distinct buffers larger than L2.
+
+Multi-GPU: the path has no exchange step (each GPU folds its own stream of
+blocks; profiles would be summed once at the end), so N GPUs run N
+independent replicas (weak scaling); rank 0 reports the max-over-ranks time.
+
+--impl reference times the reference's CPU algorithm for the same workload
+(the C++ CPU restatement in oracle/, all host cores), one bounded sample of
+the block per step.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "dspsr-kanyixia_b200"))
+
+START_MJD = (60000, 3600, 0.25)
+EPOCH_MJD = (59999, 0, 0.0)
+
+CONFIGS = {
+    "c1": dict(
+        workload=("single-channel coherent dedispersion: 16 MHz complex baseband at 1400 MHz, "
+                  "2 pol int8, DM 67.99, FFT 2^17 (2^15 is below the reference's minimum), "
+                  "Intensity, 1024-bin fold, P=89.33 ms, 2^24 samples/pol per block"),
+        cf=1400.0, bw=16.0, dm=67.99, nchan=1, npol=2, nfft=1 << 17, nbin=1024,
+        period=0.08933, state=0, ndat=1 << 24, duty=0.03, snr=20.0, sigma=10.0),
+}
+
+NBLOCKS = 4
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "power_w_max": max(power) if power else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes per unit of work of a kernel from a committed ncu summary
+    (profiles/ncu_traffic.txt: 'kernel=<name> bytes_per_part=<B>')."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        parts = dict(kv.split("=", 1) for kv in line.split() if "=" in kv)
+        if parts.get("kernel") == kernel and "bytes_per_part" in parts:
+            return float(parts["bytes_per_part"])
+    return None
+
+
+# ---------------------------------------------------------------------------
+# synthetic blocks
+# ---------------------------------------------------------------------------
+
+def make_blocks(cfg, seed, device):
+    """NBLOCKS consecutive int8 TFPD blocks generated on the GPU (torch is the
+    synthesis tool here; the product path never uses it)."""
+    import torch
+    from dspsr_b200 import synth
+    ndat, npol = cfg["ndat"], cfg["npol"]
+    rate = abs(cfg["bw"]) * 1e6
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    chirp = None
+    blocks = []
+    for b in range(NBLOCKS):
+        ph = torch.from_numpy(synth._phase(ndat, rate, cfg["period"], START_MJD, EPOCH_MJD,
+                                           idat0=b * ndat)).to(device)
+        on = (torch.remainder(ph - 0.3, 1.0) < cfg["duty"]).to(torch.float64)
+        if chirp is None:
+            dphi = torch.from_numpy(synth.dispersion_phase(ndat, cfg["cf"], cfg["bw"],
+                                                           cfg["dm"])).to(device)
+            chirp = torch.polar(torch.ones_like(dphi), dphi)
+            del dphi
+        out = torch.empty((ndat, npol, 2), dtype=torch.int8, device=device)
+        amp = np.sqrt(cfg["snr"]) * cfg["sigma"] / np.sqrt(2)
+        for p in range(npol):
+            s = torch.complex(torch.randn(ndat, generator=gen, device=device, dtype=torch.float64),
+                              torch.randn(ndat, generator=gen, device=device, dtype=torch.float64))
+            s = torch.fft.ifft(torch.fft.fft(s * (amp * on)) * chirp)
+            n = torch.randn((ndat, 2), generator=gen, device=device, dtype=torch.float64)
+            n = n * (cfg["sigma"] / np.sqrt(2))
+            n[:, 0] += s.real
+            n[:, 1] += s.imag
+            out[:, p, :] = torch.clamp(torch.round(n), -128, 127).to(torch.int8)
+            del s, n
+        blocks.append(out.reshape(-1).view(torch.uint8))
+        del ph, on
+    del chirp
+    torch.cuda.synchronize()
+    return blocks
+
+
+# ---------------------------------------------------------------------------
+# CPU: reference arm and cpu_baseline (the oracle restatement of the
+# reference's CPU path; test infrastructure, timed here as the CPU baseline)
+# ---------------------------------------------------------------------------
+
+def cpu_prepare(cfg):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    orc.lib()
+    pos = orc.smearing_samples(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nchan"], 1)
+    neg = orc.smearing_samples(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nchan"], -1)
+    lut, _ = orc.bittable8(0.0308)
+    h = orc.dedispersion_response(cfg["cf"], cfg["bw"], cfg["dm"], 1, cfg["nfft"], mode=0)
+    return orc, pos, neg, lut, h
+
+
+def cpu_sample(cfg, orc, pos, neg, lut, h, nparts, seed=1):
+    """Bounded sample: nparts FFT parts of the block (int8 noise + pulse)."""
+    from dspsr_b200 import synth
+    nk = cfg["nfft"] - pos - neg
+    ndat = cfg["nfft"] + (nparts - 1) * nk
+    raw = synth.noise_block(ndat, 1, cfg["npol"], cfg["sigma"], seed)
+    return raw, ndat
+
+
+def cpu_run(cfg, orc, pos, neg, lut, h, raw, ndat, threads):
+    rate = abs(cfg["bw"]) * 1e6
+    phi = orc.fold_phi(START_MJD, EPOCH_MJD, pos, rate, cfg["period"])
+    t0 = time.perf_counter()
+    orc.pipeline_c1(raw, ndat, lut, h, cfg["nfft"], pos, neg, phi, (1 / rate) / cfg["period"],
+                    cfg["nbin"], threads)
+    return time.perf_counter() - t0
+
+
+def block_parts(cfg, pos, neg):
+    """FFT parts one block of the workload holds."""
+    nk = cfg["nfft"] - pos - neg
+    return (cfg["ndat"] - pos - neg) // nk
+
+
+def cpu_baseline(cfg, target_s=15.0):
+    """One block of the workload through the CPU restatement, repeated until
+    about target_s seconds of CPU work have been timed."""
+    orc, pos, neg, lut, h = cpu_prepare(cfg)
+    threads = os.cpu_count() or 1
+    nparts = block_parts(cfg, pos, neg)
+    raw, ndat = cpu_sample(cfg, orc, pos, neg, lut, h, nparts)
+    cpu_run(cfg, orc, pos, neg, lut, h, raw, ndat, threads)      # plans, page-in
+    total, reps = 0.0, 0
+    while total < target_s:
+        total += cpu_run(cfg, orc, pos, neg, lut, h, raw, ndat, threads)
+        reps += 1
+    msps = ndat * cfg["npol"] * reps / total / 1e6
+    return {"value": round(msps, 3), "unit": "complex Msamples/s", "cores": threads,
+            "kind": "port",
+            "sample": (f"one workload block ({nparts} FFT parts, {ndat} samples/pol, "
+                       f"{cfg['npol']} pol) x {reps} through the oracle CPU restatement "
+                       f"(self-written FP32 FFT, OpenMP over parts), {total:.1f} s")}
+
+
+def run_reference(args, cfg, world, rank):
+    if rank != 0:
+        return
+    orc, pos, neg, lut, h = cpu_prepare(cfg)
+    threads = os.cpu_count() or 1
+    raw, ndat = cpu_sample(cfg, orc, pos, neg, lut, h, threads)
+    t1 = cpu_run(cfg, orc, pos, neg, lut, h, raw, ndat, threads)
+    budget = 150.0 / max(1, args.steps + args.warmup)
+    nparts = max(threads, int(threads * budget / max(t1, 1e-3)))
+    nparts = min(nparts, block_parts(cfg, pos, neg))
+    raw, ndat = cpu_sample(cfg, orc, pos, neg, lut, h, nparts)
+    for _ in range(args.warmup):
+        cpu_run(cfg, orc, pos, neg, lut, h, raw, ndat, threads)
+    ts = [cpu_run(cfg, orc, pos, neg, lut, h, raw, ndat, threads) for _ in range(args.steps)]
+    total = sum(ts)
+    msps = ndat * cfg["npol"] * args.steps / total / 1e6
+    line = {
+        "impl": "reference", "metric": "complex Msamples/s unpack->fold", "value": round(msps, 3),
+        "unit": "complex Msamples/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1e3 * total / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Gaussian noise, int8)",
+        "config": {"workload": cfg["workload"], "sample_parts_per_step": nparts},
+        "cpu_baseline": {"value": round(msps, 3), "unit": "complex Msamples/s", "cores": threads,
+                         "kind": "port",
+                         "sample": (f"{nparts} FFT parts per step ({ndat} samples/pol); the "
+                                    "reference's own build (DSPSR+PSRCHIVE+FFTW) is not "
+                                    "buildable here, so its CPU algorithm runs as the oracle "
+                                    "restatement")},
+        "e2e": {"value": round(msps, 3), "unit": "complex Msamples/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+def run_b200(args, cfg, world, rank, local):
+    import torch
+    import dspsr_b200 as b2
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    ctx = b2.Context(local)
+    pos, neg, nfft = b2.dispersion_plan(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nchan"],
+                                        cfg["nfft"])
+    nk = nfft - pos - neg
+    lut, _ = b2.bittable8()
+    c = b2.make_config(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nchan"], cfg["npol"], nfft, pos,
+                       neg, cfg["nbin"], cfg["period"], state=cfg["state"], lut=lut,
+                       start_mjd=START_MJD, epoch_mjd=EPOCH_MJD)
+    blocks = make_blocks(cfg, 1234 + rank, device)
+    ndat = cfg["ndat"]
+    samples_per_step = ndat * cfg["npol"]   # complex samples consumed per step (all pols)
+    bytes_per_block = blocks[0].numel()
+
+    # ---- device-resident timed region --------------------------------------
+    pl = b2.Pipeline(ctx, c)
+    for i in range(args.warmup):
+        pl.run(blocks[i % NBLOCKS], ndat)
+    torch.cuda.synchronize()
+    pl.profile(True)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    launches0 = b2.kernel_launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    folded = 0
+    for i in range(args.steps):
+        folded += pl.run(blocks[(args.warmup + i) % NBLOCKS], ndat)
+    ev1.record()
+    torch.cuda.synchronize()
+    launches = b2.kernel_launches() - launches0
+    clk = clocks.stop()
+    barrier(world)
+    ms = ev0.elapsed_time(ev1)
+    ms_max = max_over_ranks(ms, world)
+    ktimes = pl.kernel_times()
+    pl.profile(False)
+    info = pl.info()
+    prof, hits = pl.get_profiles()
+    pl.close()
+    value = samples_per_step * args.steps * world / (ms_max / 1e3) / 1e6
+
+    # ---- end to end through the public API from pinned host memory ----------
+    host = [b.cpu().pin_memory() for b in blocks]
+    pl = b2.Pipeline(ctx, c)
+    for i in range(args.warmup):
+        pl.run_host(host[i % NBLOCKS], ndat)
+        pl.get_profiles()
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(args.steps):
+        pl.run_host(host[(args.warmup + i) % NBLOCKS], ndat)
+        p2, h2 = pl.get_profiles()          # the step's result back on the host
+    e1.record()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    e2e_ms = max_over_ranks(max(e0.elapsed_time(e1), 1e3 * wall), world)
+    pl.close()
+    e2e = samples_per_step * args.steps * world / (e2e_ms / 1e3) / 1e6
+    d2h = p2.nbytes + h2.nbytes
+
+    # ---- roofline of the dominant kernel -----------------------------------
+    hbm_peak, bf16_peak, peak_src = measured_peaks()
+    name, (kms, kn) = max(ktimes.items(), key=lambda kv: kv[1][0])
+    # parts processed in the timed region = output samples / nkeep
+    parts = folded // nk
+    parts_per_launch = parts / max(kn, 1)
+    # algorithmic bytes per part: the int8 input of the new samples it
+    # dedisperses (2 bytes per complex sample per pol)
+    alg_bytes = 2.0 * cfg["npol"] * nk * parts_per_launch
+    avg_s = kms / 1e3 / max(kn, 1)
+    achieved = alg_bytes / avg_s / 1e9
+    tb = ncu_traffic(name)
+    traffic = tb * parts_per_launch if tb else None
+    # FP32 view: flops per output sample of the FFT convolution (log2 N radix-2
+    # count, both transforms, overlap included) + detection + fold
+    import math
+    flop_per_sample = (nfft / nk) * (2 * 5 * math.log2(nfft) + 6) + 5
+    fp32_tflops = flop_per_sample * folded * cfg["npol"] / (ms / 1e3) / 1e12
+    fp32_peak = 148 * 128 * 2 * (clk["sm_mhz"] or 1965.0) * 1e6 / 1e12
+
+    line = {
+        "metric": "complex Msamples/s unpack->fold", "value": round(value, 3),
+        "unit": "complex Msamples/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Gaussian noise + FP64-dispersed pulse train, int8)",
+        "config": {"workload": cfg["workload"], "nfft": nfft, "nfilt_pos": pos,
+                   "nfilt_neg": neg, "nkeep": nk, "fft_split": [info["n1"], info["n2"]],
+                   "parts_per_batch": info["max_batch"],
+                   "l2": f"inputs larger than L2: {NBLOCKS} distinct {bytes_per_block >> 20} MiB "
+                         "blocks cycled",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "clocks": clk,
+        "gpu_launches": int(launches),
+        "kernel_ms": {k: round(v[0], 3) for k, v in ktimes.items() if v[1]},
+        "roofline": {"bound": "hbm", "kernel": name, "achieved": round(achieved, 2),
+                     "peak": hbm_peak, "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
+                     "traffic": traffic, "peak_source": peak_src,
+                     "note": "path is FP32-ALU bound (2 B/sample in); see roofline_fp32"},
+        "roofline_fp32": {"achieved": round(fp32_tflops, 3), "unit": "TFLOP/s",
+                          "peak": round(fp32_peak, 1), "frac": round(fp32_tflops / fp32_peak, 4),
+                          "flop_per_sample": round(flop_per_sample, 1),
+                          "peak_source": "148 SM x 128 FP32 lanes x 2 x median SM clock"},
+        "e2e": {"value": round(e2e, 3), "unit": "complex Msamples/s",
+                "h2d_bytes_per_step": int(bytes_per_block), "d2h_bytes_per_step": int(d2h)},
+        "check": {"samples_folded": int(folded), "hits_total": int(hits.sum()),
+                  "profile_peak_over_median": float(np.max(prof) / max(np.median(prof), 1e-30))},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(cfg)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="c1", choices=sorted(CONFIGS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
+    cfg = CONFIGS[args.config]
+    world, rank, local = dist_init()
+    try:
+        if args.impl == "reference":
+            run_reference(args, cfg, world, rank)
+        else:
+            run_b200(args, cfg, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

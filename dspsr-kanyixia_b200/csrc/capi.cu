@@ -1,0 +1,989 @@
+// capi.cu -- the C ABI of libdspsr_b200.so (declared in include/dspsr_b200.h):
+// contexts, the engine objects that stand in for DSPSR's CUDA engines, and
+// the fused unpack -> convolve -> detect -> fold pipeline.
+
+#include "dspsr_b200.h"
+#include "kernels.cuh"
+#include "host_rules.h"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+using namespace b200;
+
+struct dspsr_b200_context
+{
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string error;
+  float* d_lut = nullptr;     // scratch LUT for the standalone unpacker
+};
+
+namespace {
+
+int fail (dspsr_b200_context* ctx, int code, const char* fmt, ...)
+{
+  char buf[512];
+  va_list ap;
+  va_start (ap, fmt);
+  vsnprintf (buf, sizeof (buf), fmt, ap);
+  va_end (ap);
+  if (ctx) ctx->error = buf;
+  return code;
+}
+
+int cuda_fail (dspsr_b200_context* ctx, cudaError_t err, const char* where)
+{
+  return fail (ctx, DSPSR_B200_ECUDA, "%s: %s", where, cudaGetErrorString (err));
+}
+
+#define B200_CHECK(ctx, call, where)                                  \
+  do {                                                                \
+    cudaError_t _e = (call);                                          \
+    if (_e != cudaSuccess) return cuda_fail ((ctx), _e, (where));     \
+  } while (0)
+
+bool is_pow2 (uint64_t x) { return x && !(x & (x - 1)); }
+
+// Device buffer owned by an engine object.
+template <typename T>
+struct DevBuf
+{
+  T* ptr = nullptr;
+  size_t n = 0;
+  cudaError_t reserve (size_t count)
+  {
+    if (count <= n) return cudaSuccess;
+    release ();
+    cudaError_t e = cudaMalloc (&ptr, count * sizeof (T));
+    if (e == cudaSuccess) n = count; else ptr = nullptr;
+    return e;
+  }
+  void release ()
+  {
+    if (ptr) cudaFree (ptr);
+    ptr = nullptr;
+    n = 0;
+  }
+};
+
+// Twiddle tables rounded once from double precision.
+std::vector<float2> make_tw2 (unsigned n)
+{
+  std::vector<float2> t (n);
+  for (unsigned m = 0; m < n; m++)
+  {
+    const double a = -2.0 * M_PI * double (m) / double (n);
+    t[m] = make_float2 (float (std::cos (a)), float (std::sin (a)));
+  }
+  return t;
+}
+
+std::vector<float2> make_tw4 (unsigned n1, unsigned n2)
+{
+  const uint64_t N = uint64_t (n1) * n2;
+  std::vector<float2> t (N);
+  for (unsigned k1 = 0; k1 < n1; k1++)
+    for (unsigned i = 0; i < n2; i++)
+    {
+      const uint64_t m = (uint64_t (k1) * i) % N;
+      const double a = -2.0 * M_PI * double (m) / double (N);
+      t[uint64_t (k1) * n2 + i] = make_float2 (float (std::cos (a)), float (std::sin (a)));
+    }
+  return t;
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+// convolution engine
+// ---------------------------------------------------------------------------
+
+struct dspsr_b200_convolution
+{
+  dspsr_b200_context* ctx = nullptr;
+  ConvShape shape {};
+  DevBuf<float2> tw2, tw4, H, tmp, scratch;
+  DevBuf<double> chan_par;
+  DevBuf<float> lut;
+  bool have_response = false;
+  unsigned max_batch = 1;
+
+  int init (dspsr_b200_context* c, unsigned nchan, unsigned npol, unsigned nfft,
+            unsigned pos, unsigned neg, uint64_t scratch_bytes);
+  ConvTables tables () const
+  {
+    ConvTables t;
+    t.tw2 = tw2.ptr;
+    t.tw4 = tw4.ptr;
+    t.H = H.ptr;
+    t.lut = lut.ptr;
+    return t;
+  }
+};
+
+int dspsr_b200_convolution::init (dspsr_b200_context* c, unsigned nchan, unsigned npol,
+                                  unsigned nfft, unsigned pos, unsigned neg,
+                                  uint64_t scratch_bytes)
+{
+  ctx = c;
+  if (nchan == 0 || npol == 0 || npol > 2)
+    return fail (ctx, DSPSR_B200_EINVAL, "convolution: invalid nchan=%u npol=%u", nchan, npol);
+  if (!is_pow2 (nfft) || nfft < 4096 || nfft > 262144)
+    return fail (ctx, DSPSR_B200_EINVAL,
+                 "convolution: nfft=%u must be a power of two in [4096, 262144]", nfft);
+  // Convolution::prepare (Convolution.C:456-459): the FFT must exceed the overlap
+  if (uint64_t (pos) + neg >= nfft)
+    return fail (ctx, DSPSR_B200_EINVAL, "convolution: nfft=%u <= nfilt=%u", nfft, pos + neg);
+  shape.nchan = nchan;
+  shape.npol = npol;
+  shape.nfft = nfft;
+  shape.nfilt_pos = pos;
+  shape.nfilt_neg = neg;
+  shape.nkeep = nfft - pos - neg;
+  if (nfft <= 8192)
+  {
+    shape.n1 = 1;
+    shape.n2 = nfft;
+  }
+  else
+  {
+    shape.n2 = 8192;
+    shape.n1 = nfft / 8192;
+  }
+  B200_CHECK (ctx, tw2.reserve (shape.n2), "cudaMalloc tw2");
+  std::vector<float2> t2 = make_tw2 (shape.n2);
+  B200_CHECK (ctx, cudaMemcpy (tw2.ptr, t2.data (), t2.size () * sizeof (float2),
+                               cudaMemcpyHostToDevice), "copy tw2");
+  if (shape.n1 > 1)
+  {
+    B200_CHECK (ctx, tw4.reserve (nfft), "cudaMalloc tw4");
+    std::vector<float2> t4 = make_tw4 (shape.n1, shape.n2);
+    B200_CHECK (ctx, cudaMemcpy (tw4.ptr, t4.data (), t4.size () * sizeof (float2),
+                                 cudaMemcpyHostToDevice), "copy tw4");
+    // parts in flight: keep the scratch near the L2 size unless told otherwise
+    const uint64_t per_part = uint64_t (nchan) * npol * nfft * sizeof (float2);
+    const uint64_t budget = scratch_bytes ? scratch_bytes : (uint64_t (48) << 20);
+    max_batch = unsigned (std::max<uint64_t> (1, budget / per_part));
+    if (max_batch > 65535) max_batch = 65535;
+    B200_CHECK (ctx, scratch.reserve (uint64_t (max_batch) * nchan * npol * nfft),
+                "cudaMalloc scratch");
+  }
+  else
+    max_batch = 65535;
+  B200_CHECK (ctx, H.reserve (uint64_t (nchan) * nfft), "cudaMalloc response");
+  B200_CHECK (ctx, lut.reserve (256), "cudaMalloc lut");
+  return DSPSR_B200_OK;
+}
+
+// ---------------------------------------------------------------------------
+// fold engine
+// ---------------------------------------------------------------------------
+
+struct dspsr_b200_fold
+{
+  dspsr_b200_context* ctx = nullptr;
+  unsigned nbin = 0, nchan = 0, npol = 0;
+  DevBuf<float> profiles;
+  DevBuf<unsigned> hits;
+  // double-buffered plan upload
+  DevBuf<FoldSegment> d_segs[2];
+  FoldSegment* h_segs[2] = {nullptr, nullptr};
+  size_t h_cap[2] = {0, 0};
+  cudaEvent_t done[2] = {nullptr, nullptr};
+  int cur = 0;
+  int nseg = 0;
+  uint64_t ndat = 0;
+  std::vector<FoldSegment> plan;
+
+  int init (dspsr_b200_context* c, unsigned nb, unsigned nc, unsigned np)
+  {
+    ctx = c;
+    nbin = nb;
+    nchan = nc;
+    npol = np;
+    if (nbin == 0 || nchan == 0 || npol == 0)
+      return fail (ctx, DSPSR_B200_EINVAL, "fold: invalid nbin=%u nchan=%u npol=%u", nbin,
+                   nchan, npol);
+    B200_CHECK (ctx, profiles.reserve (uint64_t (nchan) * npol * nbin), "cudaMalloc profiles");
+    B200_CHECK (ctx, hits.reserve (nbin), "cudaMalloc hits");
+    for (int i = 0; i < 2; i++)
+      B200_CHECK (ctx, cudaEventCreateWithFlags (&done[i], cudaEventDisableTiming),
+                  "cudaEventCreate");
+    return reset ();
+  }
+  int reset ()
+  {
+    B200_CHECK (ctx, cudaMemsetAsync (profiles.ptr, 0,
+                                      uint64_t (nchan) * npol * nbin * sizeof (float),
+                                      ctx->stream), "memset profiles");
+    B200_CHECK (ctx, cudaMemsetAsync (hits.ptr, 0, nbin * sizeof (unsigned), ctx->stream),
+                "memset hits");
+    return DSPSR_B200_OK;
+  }
+  // builds the exact plan on the host and uploads it on the context's stream
+  int set_bins (double phi, double pps, uint64_t n)
+  {
+    build_fold_plan (phi, pps, n, &plan);
+    ndat = n;
+    nseg = int (plan.size ());
+    cur ^= 1;
+    // the buffer about to be overwritten was last read by work queued before `done[cur]`
+    B200_CHECK (ctx, cudaEventSynchronize (done[cur]), "cudaEventSynchronize");
+    if (h_cap[cur] < plan.size ())
+    {
+      if (h_segs[cur]) cudaFreeHost (h_segs[cur]);
+      h_segs[cur] = nullptr;
+      h_cap[cur] = 0;
+      const size_t cap = plan.size () * 2 + 64;
+      B200_CHECK (ctx, cudaMallocHost (&h_segs[cur], cap * sizeof (FoldSegment)),
+                  "cudaMallocHost plan");
+      h_cap[cur] = cap;
+    }
+    B200_CHECK (ctx, d_segs[cur].reserve (std::max<size_t> (plan.size (), 1)),
+                "cudaMalloc plan");
+    std::memcpy (h_segs[cur], plan.data (), plan.size () * sizeof (FoldSegment));
+    if (!plan.empty ())
+      B200_CHECK (ctx, cudaMemcpyAsync (d_segs[cur].ptr, h_segs[cur],
+                                        plan.size () * sizeof (FoldSegment),
+                                        cudaMemcpyHostToDevice, ctx->stream), "upload plan");
+    return DSPSR_B200_OK;
+  }
+  // marks the end of the work that reads the current plan buffer
+  int release_plan ()
+  {
+    B200_CHECK (ctx, cudaEventRecord (done[cur], ctx->stream), "cudaEventRecord");
+    return DSPSR_B200_OK;
+  }
+  FoldView view (int state, int nout, unsigned nchan_prof)
+  {
+    (void) nchan_prof;
+    FoldView v;
+    v.segs = d_segs[cur].ptr;
+    v.nseg = nseg;
+    v.profiles = profiles.ptr;
+    v.hits = hits.ptr;
+    v.nbin = nbin;
+    v.state = state;
+    v.nout = nout;
+    return v;
+  }
+  void release ()
+  {
+    profiles.release ();
+    hits.release ();
+    for (int i = 0; i < 2; i++)
+    {
+      d_segs[i].release ();
+      if (h_segs[i]) cudaFreeHost (h_segs[i]);
+      h_segs[i] = nullptr;
+      if (done[i]) cudaEventDestroy (done[i]);
+      done[i] = nullptr;
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// fused pipeline
+// ---------------------------------------------------------------------------
+
+// Per-kernel CUDA-event clock of the pipeline (KernelClock hook).
+struct PipeClock
+{
+  bool on = false;
+  std::vector<cudaEvent_t> pool;
+  size_t used = 0;
+  std::vector<int> kind;              // kind of each (start, stop) pair
+  cudaEvent_t take ()
+  {
+    if (used == pool.size ())
+    {
+      cudaEvent_t e = nullptr;
+      cudaEventCreate (&e);
+      pool.push_back (e);
+    }
+    return pool[used++];
+  }
+  static void mark (void* self, int k, int phase, cudaStream_t st)
+  {
+    PipeClock* c = static_cast<PipeClock*> (self);
+    cudaEventRecord (c->take (), st);
+    if (phase == 0) c->kind.push_back (k);
+  }
+  void clear ()
+  {
+    used = 0;
+    kind.clear ();
+  }
+  ~PipeClock ()
+  {
+    for (cudaEvent_t e : pool) cudaEventDestroy (e);
+  }
+};
+
+struct dspsr_b200_pipeline
+{
+  dspsr_b200_context* ctx = nullptr;
+  PipeClock clock;
+  dspsr_b200_pipeline_config cfg {};
+  dspsr_b200_convolution conv;
+  dspsr_b200_fold fold;
+  int nout = 1;
+  uint64_t bytes_per_sample = 0;   // TFPD bytes per time sample (all chans, pols)
+  DevBuf<uint8_t> carry[2];         // carried input (TFPD bytes or FPT floats)
+  uint64_t carry_span = 0;          // FPT: complex samples per (chan, pol) row
+  uint64_t ncarry = 0;
+  int cur_carry = 0;
+  uint64_t in0 = 0;                 // global input index of the first sample of the block
+  DevBuf<uint8_t> staging;          // host->device staging for run_host
+  double rate = 0;
+};
+
+namespace {
+
+int pipeline_block (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat_new,
+                    uint64_t in_span, uint64_t* ndat_folded)
+{
+  dspsr_b200_context* ctx = pl->ctx;
+  const ConvShape& sh = pl->conv.shape;
+  const auto& cfg = pl->cfg;
+  const uint64_t nfilt = uint64_t (sh.nfilt_pos) + sh.nfilt_neg;
+  const uint64_t ndat = pl->ncarry + ndat_new;
+  const bool fpt = cfg.input_kind == DSPSR_B200_FLOAT_FPT;
+  if (ndat_folded) *ndat_folded = 0;
+
+  InputView in;
+  in.kind = cfg.input_kind == DSPSR_B200_INT8_TFPD ? IN_INT8
+          : cfg.input_kind == DSPSR_B200_INT16_TFPD ? IN_INT16 : IN_FLOAT;
+  in.pre = pl->carry[pl->cur_carry].ptr;
+  in.main = d_in;
+  in.npre = pl->ncarry;
+  in.pre_span = pl->carry_span;
+  in.main_span = fpt ? in_span : 0;
+  in.nchan = cfg.nchan;
+  in.npol = cfg.npol;
+  in.offset_binary = cfg.offset_binary;
+
+  uint64_t npart = 0;
+  if (ndat >= sh.nfft) npart = (ndat - nfilt) / sh.nkeep;   // Convolution.C:486-487
+  const uint64_t nout = npart * sh.nkeep;
+
+  if (npart > 0)
+  {
+    // Fold::fold (Fold.C:685-693): phase of the first output sample's midpoint;
+    // the output starts nfilt_pos samples after the input (Convolution.C:599)
+    const double phi = fold_phi (cfg.start_day, cfg.start_sec, cfg.start_frac, cfg.epoch_day,
+                                 cfg.epoch_sec, cfg.epoch_frac, pl->in0 + sh.nfilt_pos,
+                                 pl->rate, cfg.period_s, cfg.reference_phase);
+    const double sampling_interval = 1.0 / pl->rate;
+    const double pps = sampling_interval / cfg.period_s;   // Fold.C:754-756
+    int rc = pl->fold.set_bins (phi, pps, nout);
+    if (rc) return rc;
+    FoldView fv = pl->fold.view (cfg.state, pl->nout, cfg.nchan);
+    VoltView vv {nullptr, 0};
+    const ConvTables tb = pl->conv.tables ();
+    KernelClock kc {&PipeClock::mark, &pl->clock};
+    const KernelClock* clk = pl->clock.on ? &kc : nullptr;
+    for (uint64_t p0 = 0; p0 < npart; p0 += pl->conv.max_batch)
+    {
+      const unsigned nb = unsigned (std::min<uint64_t> (pl->conv.max_batch, npart - p0));
+      B200_CHECK (ctx, launch_convolution (sh, tb, in, p0, nb, pl->conv.scratch.ptr, OUT_FOLD, fv,
+                                           vv, ctx->stream, clk), "convolution kernels");
+    }
+    rc = pl->fold.release_plan ();
+    if (rc) return rc;
+  }
+
+  // InputBuffering (InputBuffering.C:66-174): samples [nout, ndat) carry over
+  const uint64_t keep = ndat - nout;
+  const int next = pl->cur_carry ^ 1;
+  if (!fpt)
+  {
+    const uint64_t bps = pl->bytes_per_sample;
+    B200_CHECK (ctx, pl->carry[next].reserve (std::max<uint64_t> (keep * bps, 16)),
+                "cudaMalloc carry");
+    uint64_t done = 0;
+    if (nout < pl->ncarry)
+    {
+      const uint64_t n = pl->ncarry - nout;
+      B200_CHECK (ctx, cudaMemcpyAsync (pl->carry[next].ptr, pl->carry[pl->cur_carry].ptr + nout * bps,
+                                        n * bps, cudaMemcpyDeviceToDevice, ctx->stream),
+                  "carry copy");
+      done = n;
+    }
+    if (keep > done)
+    {
+      const uint64_t from = nout + done - pl->ncarry;
+      B200_CHECK (ctx, cudaMemcpyAsync (pl->carry[next].ptr + done * bps,
+                                        static_cast<const uint8_t*> (d_in) + from * bps,
+                                        (keep - done) * bps, cudaMemcpyDeviceToDevice,
+                                        ctx->stream), "carry copy");
+    }
+  }
+  else
+  {
+    const uint64_t rows = uint64_t (cfg.nchan) * cfg.npol;
+    const uint64_t span = std::max<uint64_t> (keep, 1);
+    B200_CHECK (ctx, pl->carry[next].reserve (rows * span * sizeof (float2)), "cudaMalloc carry");
+    uint64_t done = 0;
+    if (nout < pl->ncarry)
+    {
+      const uint64_t n = pl->ncarry - nout;
+      B200_CHECK (ctx, cudaMemcpy2DAsync (pl->carry[next].ptr, span * sizeof (float2),
+                                          pl->carry[pl->cur_carry].ptr + nout * sizeof (float2),
+                                          pl->carry_span * sizeof (float2), n * sizeof (float2),
+                                          rows, cudaMemcpyDeviceToDevice, ctx->stream),
+                  "carry copy");
+      done = n;
+    }
+    if (keep > done)
+    {
+      const uint64_t from = nout + done - pl->ncarry;
+      B200_CHECK (ctx, cudaMemcpy2DAsync (pl->carry[next].ptr + done * sizeof (float2),
+                                          span * sizeof (float2),
+                                          static_cast<const uint8_t*> (d_in) + from * sizeof (float2),
+                                          in_span * sizeof (float2), (keep - done) * sizeof (float2),
+                                          rows, cudaMemcpyDeviceToDevice, ctx->stream),
+                  "carry copy");
+    }
+    pl->carry_span = span;
+  }
+  pl->cur_carry = next;
+  pl->ncarry = keep;
+  pl->in0 += nout;
+  if (ndat_folded) *ndat_folded = nout;
+  return DSPSR_B200_OK;
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+// exported functions
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+int dspsr_b200_version (void) { return 100; }
+
+int dspsr_b200_context_create (int device, void* stream, dspsr_b200_context** out)
+{
+  if (!out) return DSPSR_B200_EINVAL;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount (&ndev) != cudaSuccess || ndev == 0)
+    return DSPSR_B200_ENODEV;
+  if (device < 0 || device >= ndev) return DSPSR_B200_EINVAL;
+  if (cudaSetDevice (device) != cudaSuccess) return DSPSR_B200_ECUDA;
+  dspsr_b200_context* ctx = new (std::nothrow) dspsr_b200_context;
+  if (!ctx) return DSPSR_B200_ENOMEM;
+  ctx->device = device;
+  ctx->stream = static_cast<cudaStream_t> (stream);
+  if (cudaMalloc (&ctx->d_lut, 256 * sizeof (float)) != cudaSuccess)
+  {
+    delete ctx;
+    return DSPSR_B200_ECUDA;
+  }
+  *out = ctx;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_context_destroy (dspsr_b200_context* ctx)
+{
+  if (!ctx) return DSPSR_B200_EINVAL;
+  if (ctx->d_lut) cudaFree (ctx->d_lut);
+  delete ctx;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_context_set_stream (dspsr_b200_context* ctx, void* stream)
+{
+  if (!ctx) return DSPSR_B200_EINVAL;
+  ctx->stream = static_cast<cudaStream_t> (stream);
+  return DSPSR_B200_OK;
+}
+
+const char* dspsr_b200_last_error (const dspsr_b200_context* ctx)
+{
+  return ctx ? ctx->error.c_str () : "null context";
+}
+
+int dspsr_b200_synchronize (dspsr_b200_context* ctx)
+{
+  if (!ctx) return DSPSR_B200_EINVAL;
+  B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "cudaStreamSynchronize");
+  return DSPSR_B200_OK;
+}
+
+unsigned dspsr_b200_smearing_samples (double cf, double bw, double dm, unsigned nchan, int half)
+{
+  if (nchan == 0 || !(half == 0 || half == 1 || half == -1)) return 0;
+  return smearing_samples (cf, bw, dm, nchan, half);
+}
+
+unsigned dspsr_b200_minimum_ndat (unsigned pos, unsigned neg) { return minimum_ndat (pos, neg); }
+
+int64_t dspsr_b200_optimal_fft_length (uint64_t nbad, uint64_t nmax, unsigned factor)
+{
+  return optimal_fft_length (nbad, nmax, factor);
+}
+
+int dspsr_b200_bittable8 (double spacing, int twos_complement, float* lut, double* scale)
+{
+  if (!lut || !(spacing > 0)) return DSPSR_B200_EINVAL;
+  bittable8 (spacing, twos_complement != 0, lut, scale);
+  return DSPSR_B200_OK;
+}
+
+double dspsr_b200_fold_phi (int64_t sd, int64_t ss, double sf, int64_t ed, int64_t es, double ef,
+                            uint64_t idat_start, double rate, double period, double ref_phase)
+{
+  return fold_phi (sd, ss, sf, ed, es, ef, idat_start, rate, period, ref_phase);
+}
+
+int64_t dspsr_b200_fold_plan_count (double phi, double pps, uint64_t ndat)
+{
+  return build_fold_plan (phi, pps, ndat, nullptr);
+}
+
+// ---- unpack ----------------------------------------------------------------
+
+int dspsr_b200_unpack8 (dspsr_b200_context* ctx, const void* d_in, uint64_t ndat,
+                        unsigned nchan, unsigned npol, unsigned ndim, const float* lut256,
+                        float* d_out, uint64_t out_span)
+{
+  if (!ctx) return DSPSR_B200_EINVAL;
+  if (!d_in || !d_out || !lut256 || nchan == 0 || npol == 0 || ndim == 0)
+    return fail (ctx, DSPSR_B200_EINVAL, "unpack8: invalid argument");
+  if (out_span < ndat * ndim)
+    return fail (ctx, DSPSR_B200_EINVAL, "unpack8: out_span=%llu < ndat*ndim",
+                 (unsigned long long) out_span);
+  B200_CHECK (ctx, cudaMemcpyAsync (ctx->d_lut, lut256, 256 * sizeof (float),
+                                    cudaMemcpyHostToDevice, ctx->stream), "upload lut");
+  B200_CHECK (ctx, launch_unpack8 (static_cast<const uint8_t*> (d_in), ndat, nchan, npol, ndim,
+                                   ctx->d_lut, d_out, out_span, ctx->stream), "unpack8");
+  // the LUT buffer is reused by the next call: keep this call's upload ordered
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_unpack16 (dspsr_b200_context* ctx, const void* d_in, uint64_t ndat,
+                         unsigned nchan, unsigned npol, unsigned ndim, int offset_binary,
+                         float* d_out, uint64_t out_span)
+{
+  if (!ctx) return DSPSR_B200_EINVAL;
+  if (!d_in || !d_out || nchan == 0 || npol == 0 || ndim == 0)
+    return fail (ctx, DSPSR_B200_EINVAL, "unpack16: invalid argument");
+  if (out_span < ndat * ndim)
+    return fail (ctx, DSPSR_B200_EINVAL, "unpack16: out_span too small");
+  B200_CHECK (ctx, launch_unpack16 (static_cast<const int16_t*> (d_in), ndat, nchan, npol, ndim,
+                                    offset_binary, d_out, out_span, ctx->stream), "unpack16");
+  return DSPSR_B200_OK;
+}
+
+// ---- convolution -----------------------------------------------------------
+
+int dspsr_b200_convolution_create (dspsr_b200_context* ctx, unsigned nchan, unsigned npol,
+                                   unsigned nfft, unsigned pos, unsigned neg,
+                                   dspsr_b200_convolution** out)
+{
+  if (!ctx || !out) return DSPSR_B200_EINVAL;
+  *out = nullptr;
+  dspsr_b200_convolution* c = new (std::nothrow) dspsr_b200_convolution;
+  if (!c) return fail (ctx, DSPSR_B200_ENOMEM, "convolution: out of host memory");
+  int rc = c->init (ctx, nchan, npol, nfft, pos, neg, 0);
+  if (rc)
+  {
+    dspsr_b200_convolution_destroy (c);
+    return rc;
+  }
+  *out = c;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_convolution_destroy (dspsr_b200_convolution* c)
+{
+  if (!c) return DSPSR_B200_EINVAL;
+  c->tw2.release ();
+  c->tw4.release ();
+  c->H.release ();
+  c->tmp.release ();
+  c->scratch.release ();
+  c->chan_par.release ();
+  c->lut.release ();
+  delete c;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_convolution_copy_response (dspsr_b200_convolution* c, const float* response)
+{
+  if (!c) return DSPSR_B200_EINVAL;
+  dspsr_b200_context* ctx = c->ctx;
+  if (!response) return fail (ctx, DSPSR_B200_EINVAL, "copy_response: null response");
+  const ConvShape& sh = c->shape;
+  const uint64_t n = uint64_t (sh.nchan) * sh.nfft;
+  B200_CHECK (ctx, c->tmp.reserve (n), "cudaMalloc response staging");
+  B200_CHECK (ctx, cudaMemcpyAsync (c->tmp.ptr, response, n * sizeof (float2),
+                                    cudaMemcpyHostToDevice, ctx->stream), "upload response");
+  B200_CHECK (ctx, launch_permute_response (c->H.ptr, c->tmp.ptr, sh.nchan, sh.n1, sh.n2,
+                                            ctx->stream), "permute response");
+  B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "copy_response sync");
+  c->have_response = true;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_convolution_set_dedispersion (dspsr_b200_convolution* c, double cf, double bw,
+                                             double dm, int input_nchan, int dual_sideband,
+                                             int dc_centred, int chirp_mode, unsigned norm_nfft)
+{
+  if (!c) return DSPSR_B200_EINVAL;
+  dspsr_b200_context* ctx = c->ctx;
+  const ConvShape& sh = c->shape;
+  if (bw == 0 || !(cf > 0))
+    return fail (ctx, DSPSR_B200_EINVAL, "set_dedispersion: invalid frequency/bandwidth");
+  if (dc_centred && input_nchan > 1)
+    return fail (ctx, DSPSR_B200_EINVAL, "set_dedispersion: DC-centred channels not supported");
+  const unsigned nchan = sh.nchan;
+  // Observation::get_centre_frequency(ichan) (Observation.C:521-534) and the
+  // per-channel coefficient of Dedispersion::build_compute (Dedispersion.C:168-173)
+  std::vector<double> par (2 * nchan);
+  const double sign = bw / std::fabs (bw);
+  const double dispersion_per_MHz = 1e6 * dm / 2.41e-4;
+  for (unsigned ic = 0; ic < nchan; ic++)
+  {
+    const double base = cf - 0.5 * bw + 0.5 * bw / double (nchan);
+    const double chan_freq = base + double (ic) * bw / double (nchan);
+    par[ic] = chan_freq;
+    par[nchan + ic] = -sign * 2 * M_PI * dispersion_per_MHz / (chan_freq * chan_freq);
+  }
+  const double chanwidth = bw / double (nchan);
+  const double binwidth = chanwidth / double (sh.nfft);
+  // Response::swap_as_needed (Response.C:325-400) for the supported states
+  const int swap = (input_nchan == 1 && nchan == 1 && dual_sideband > 0)
+                || (input_nchan > 1 && unsigned (input_nchan) == nchan && dual_sideband != 0);
+  const float scale = float (1.0 / std::sqrt (double (norm_nfft ? norm_nfft : sh.nfft)));
+  B200_CHECK (ctx, c->chan_par.reserve (2 * nchan), "cudaMalloc channel table");
+  B200_CHECK (ctx, cudaMemcpyAsync (c->chan_par.ptr, par.data (), par.size () * sizeof (double),
+                                    cudaMemcpyHostToDevice, ctx->stream), "upload channels");
+  B200_CHECK (ctx, launch_build_chirp (c->H.ptr, c->chan_par.ptr, c->chan_par.ptr + nchan, nchan,
+                                       sh.nfft, sh.n1, sh.n2, binwidth, 0.5 * chanwidth, swap,
+                                       chirp_mode, scale, ctx->stream), "build chirp");
+  B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "set_dedispersion sync");
+  c->have_response = true;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_convolution_get_response (dspsr_b200_convolution* c, float* response)
+{
+  if (!c) return DSPSR_B200_EINVAL;
+  dspsr_b200_context* ctx = c->ctx;
+  if (!response) return fail (ctx, DSPSR_B200_EINVAL, "get_response: null pointer");
+  const ConvShape& sh = c->shape;
+  const uint64_t n = uint64_t (sh.nchan) * sh.nfft;
+  B200_CHECK (ctx, c->tmp.reserve (n), "cudaMalloc response staging");
+  B200_CHECK (ctx, launch_unpermute_response (c->tmp.ptr, c->H.ptr, sh.nchan, sh.n1, sh.n2,
+                                              ctx->stream), "unpermute response");
+  B200_CHECK (ctx, cudaMemcpyAsync (response, c->tmp.ptr, n * sizeof (float2),
+                                    cudaMemcpyDeviceToHost, ctx->stream), "download response");
+  B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "get_response sync");
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_convolution_perform (dspsr_b200_convolution* c, const float* d_in,
+                                    uint64_t in_span, uint64_t ndat, float* d_out,
+                                    uint64_t out_span, uint64_t* npart_out)
+{
+  if (!c) return DSPSR_B200_EINVAL;
+  dspsr_b200_context* ctx = c->ctx;
+  const ConvShape& sh = c->shape;
+  if (npart_out) *npart_out = 0;
+  if (!c->have_response) return fail (ctx, DSPSR_B200_ESTATE, "perform: no response set");
+  if (!d_in || !d_out) return fail (ctx, DSPSR_B200_EINVAL, "perform: null pointer");
+  if (in_span < ndat) return fail (ctx, DSPSR_B200_EINVAL, "perform: in_span < ndat");
+  uint64_t npart = 0;
+  const uint64_t nfilt = uint64_t (sh.nfilt_pos) + sh.nfilt_neg;
+  if (ndat >= sh.nfft) npart = (ndat - nfilt) / sh.nkeep;
+  if (out_span < npart * sh.nkeep)
+    return fail (ctx, DSPSR_B200_EINVAL, "perform: out_span=%llu < npart*nkeep=%llu",
+                 (unsigned long long) out_span, (unsigned long long) (npart * sh.nkeep));
+  InputView in {};
+  in.kind = IN_FLOAT;
+  in.pre = nullptr;
+  in.main = d_in;
+  in.npre = 0;
+  in.main_span = in_span;
+  in.nchan = sh.nchan;
+  in.npol = sh.npol;
+  FoldView fv {};
+  VoltView vv {reinterpret_cast<float2*> (d_out), out_span};
+  const ConvTables tb = c->tables ();
+  for (uint64_t p0 = 0; p0 < npart; p0 += c->max_batch)
+  {
+    const unsigned nb = unsigned (std::min<uint64_t> (c->max_batch, npart - p0));
+    B200_CHECK (ctx, launch_convolution (sh, tb, in, p0, nb, c->scratch.ptr, OUT_VOLTAGE, fv, vv,
+                                         ctx->stream), "convolution kernels");
+  }
+  if (npart_out) *npart_out = npart;
+  return DSPSR_B200_OK;
+}
+
+// ---- detection -------------------------------------------------------------
+
+int dspsr_b200_detect (dspsr_b200_context* ctx, const float* d_in, uint64_t in_span,
+                       uint64_t ndat, unsigned nchan, int state, float* d_out, uint64_t out_span)
+{
+  if (!ctx) return DSPSR_B200_EINVAL;
+  if (!d_in || !d_out || nchan == 0) return fail (ctx, DSPSR_B200_EINVAL, "detect: invalid argument");
+  if (state < 0 || state > 3) return fail (ctx, DSPSR_B200_EINVAL, "detect: invalid state %d", state);
+  if (in_span < ndat || out_span < ndat)
+    return fail (ctx, DSPSR_B200_EINVAL, "detect: span smaller than ndat");
+  B200_CHECK (ctx, launch_detect (reinterpret_cast<const float2*> (d_in), in_span, ndat, nchan,
+                                  state, d_out, out_span, ctx->stream), "detect");
+  return DSPSR_B200_OK;
+}
+
+// ---- fold --------------------------------------------------------------------
+
+int dspsr_b200_fold_create (dspsr_b200_context* ctx, unsigned nbin, unsigned nchan,
+                            unsigned npol, dspsr_b200_fold** out)
+{
+  if (!ctx || !out) return DSPSR_B200_EINVAL;
+  *out = nullptr;
+  dspsr_b200_fold* f = new (std::nothrow) dspsr_b200_fold;
+  if (!f) return fail (ctx, DSPSR_B200_ENOMEM, "fold: out of host memory");
+  int rc = f->init (ctx, nbin, nchan, npol);
+  if (rc)
+  {
+    f->release ();
+    delete f;
+    return rc;
+  }
+  *out = f;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_fold_destroy (dspsr_b200_fold* f)
+{
+  if (!f) return DSPSR_B200_EINVAL;
+  if (f->ctx) cudaStreamSynchronize (f->ctx->stream);
+  f->release ();
+  delete f;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_fold_set_bins (dspsr_b200_fold* f, double phi, double pps, uint64_t ndat,
+                              uint64_t idat_start, uint64_t* ndat_folded)
+{
+  if (!f) return DSPSR_B200_EINVAL;
+  (void) idat_start;   // the plan is relative to the first folded sample
+  int rc = f->set_bins (phi, pps, ndat);
+  if (rc) return rc;
+  if (ndat_folded) *ndat_folded = ndat;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_fold_fold (dspsr_b200_fold* f, const float* d_in, uint64_t in_span)
+{
+  if (!f) return DSPSR_B200_EINVAL;
+  dspsr_b200_context* ctx = f->ctx;
+  if (!d_in) return fail (ctx, DSPSR_B200_EINVAL, "fold: null input");
+  if (in_span < f->ndat) return fail (ctx, DSPSR_B200_EINVAL, "fold: in_span < ndat");
+  FoldView fv = f->view (0, 1, f->nchan);
+  B200_CHECK (ctx, launch_fold (d_in, in_span, f->ndat, f->nchan, f->npol, fv, ctx->stream),
+              "fold");
+  return f->release_plan ();
+}
+
+int dspsr_b200_fold_binplan (dspsr_b200_fold* f, uint32_t* d_binplan)
+{
+  if (!f) return DSPSR_B200_EINVAL;
+  dspsr_b200_context* ctx = f->ctx;
+  if (!d_binplan) return fail (ctx, DSPSR_B200_EINVAL, "binplan: null output");
+  B200_CHECK (ctx, launch_binplan (f->d_segs[f->cur].ptr, f->nseg, f->ndat, f->nbin, d_binplan,
+                                   ctx->stream), "binplan");
+  return f->release_plan ();
+}
+
+int dspsr_b200_fold_get_profiles (dspsr_b200_fold* f, float* profiles, uint32_t* hits)
+{
+  if (!f) return DSPSR_B200_EINVAL;
+  dspsr_b200_context* ctx = f->ctx;
+  if (profiles)
+    B200_CHECK (ctx, cudaMemcpyAsync (profiles, f->profiles.ptr,
+                                      uint64_t (f->nchan) * f->npol * f->nbin * sizeof (float),
+                                      cudaMemcpyDeviceToHost, ctx->stream), "download profiles");
+  if (hits)
+    B200_CHECK (ctx, cudaMemcpyAsync (hits, f->hits.ptr, f->nbin * sizeof (unsigned),
+                                      cudaMemcpyDeviceToHost, ctx->stream), "download hits");
+  B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "get_profiles sync");
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_fold_reset (dspsr_b200_fold* f)
+{
+  if (!f) return DSPSR_B200_EINVAL;
+  return f->reset ();
+}
+
+// ---- pipeline ----------------------------------------------------------------
+
+int dspsr_b200_pipeline_create (dspsr_b200_context* ctx, const dspsr_b200_pipeline_config* cfg,
+                                dspsr_b200_pipeline** out)
+{
+  if (!ctx || !cfg || !out) return DSPSR_B200_EINVAL;
+  *out = nullptr;
+  if (cfg->input_kind < 0 || cfg->input_kind > 2)
+    return fail (ctx, DSPSR_B200_EINVAL, "pipeline: invalid input_kind %d", cfg->input_kind);
+  if (cfg->state < 0 || cfg->state > 3)
+    return fail (ctx, DSPSR_B200_EINVAL, "pipeline: invalid state %d", cfg->state);
+  if (cfg->npol == 1 && cfg->state != DSPSR_B200_INTENSITY)
+    return fail (ctx, DSPSR_B200_EINVAL, "pipeline: state %d needs two polarisations", cfg->state);
+  if (!(cfg->period_s > 0) || cfg->nbin == 0)
+    return fail (ctx, DSPSR_B200_EINVAL, "pipeline: folding period and nbin must be positive");
+  if (cfg->nchan == 0 || cfg->bandwidth_mhz == 0)
+    return fail (ctx, DSPSR_B200_EINVAL, "pipeline: invalid nchan/bandwidth");
+  dspsr_b200_pipeline* pl = new (std::nothrow) dspsr_b200_pipeline;
+  if (!pl) return fail (ctx, DSPSR_B200_ENOMEM, "pipeline: out of host memory");
+  pl->ctx = ctx;
+  pl->cfg = *cfg;
+  pl->nout = detect_nout (cfg->state);
+  const uint64_t bytes_per_value = cfg->input_kind == DSPSR_B200_INT16_TFPD ? 2 : 1;
+  pl->bytes_per_sample = uint64_t (cfg->nchan) * cfg->npol * 2 * bytes_per_value;
+  pl->rate = std::fabs (cfg->bandwidth_mhz) / double (cfg->nchan) * 1e6;
+  int rc = pl->conv.init (ctx, cfg->nchan, cfg->npol, cfg->nfft, cfg->nfilt_pos, cfg->nfilt_neg,
+                          cfg->scratch_bytes);
+  if (!rc)
+    rc = dspsr_b200_convolution_set_dedispersion (&pl->conv, cfg->centre_freq_mhz,
+                                                  cfg->bandwidth_mhz, cfg->dm, cfg->nchan,
+                                                  cfg->dual_sideband, cfg->dc_centred,
+                                                  cfg->chirp_mode, cfg->nfft);
+  if (!rc && cfg->input_kind == DSPSR_B200_INT8_TFPD)
+  {
+    cudaError_t e = cudaMemcpy (pl->conv.lut.ptr, cfg->lut, 256 * sizeof (float),
+                                cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) rc = cuda_fail (ctx, e, "upload lut");
+  }
+  if (!rc) rc = pl->fold.init (ctx, cfg->nbin, cfg->nchan, pl->nout);
+  if (rc)
+  {
+    dspsr_b200_pipeline_destroy (pl);
+    return rc;
+  }
+  *out = pl;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_pipeline_destroy (dspsr_b200_pipeline* pl)
+{
+  if (!pl) return DSPSR_B200_EINVAL;
+  if (pl->ctx) cudaStreamSynchronize (pl->ctx->stream);
+  pl->conv.tw2.release ();
+  pl->conv.tw4.release ();
+  pl->conv.H.release ();
+  pl->conv.tmp.release ();
+  pl->conv.scratch.release ();
+  pl->conv.chan_par.release ();
+  pl->conv.lut.release ();
+  pl->fold.release ();
+  pl->carry[0].release ();
+  pl->carry[1].release ();
+  pl->staging.release ();
+  delete pl;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_pipeline_run (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat,
+                             uint64_t in_span, uint64_t* ndat_folded)
+{
+  if (!pl) return DSPSR_B200_EINVAL;
+  if (!d_in && ndat) return fail (pl->ctx, DSPSR_B200_EINVAL, "pipeline_run: null input");
+  if (pl->cfg.input_kind == DSPSR_B200_FLOAT_FPT && in_span < ndat)
+    return fail (pl->ctx, DSPSR_B200_EINVAL, "pipeline_run: in_span < ndat");
+  return pipeline_block (pl, d_in, ndat, in_span, ndat_folded);
+}
+
+int dspsr_b200_pipeline_run_host (dspsr_b200_pipeline* pl, const void* h_in, uint64_t ndat,
+                                  uint64_t* ndat_folded)
+{
+  if (!pl) return DSPSR_B200_EINVAL;
+  dspsr_b200_context* ctx = pl->ctx;
+  if (pl->cfg.input_kind == DSPSR_B200_FLOAT_FPT)
+    return fail (ctx, DSPSR_B200_EINVAL, "pipeline_run_host: TFPD input only");
+  if (!h_in && ndat) return fail (ctx, DSPSR_B200_EINVAL, "pipeline_run_host: null input");
+  const uint64_t bytes = ndat * pl->bytes_per_sample;
+  B200_CHECK (ctx, pl->staging.reserve (std::max<uint64_t> (bytes, 16)), "cudaMalloc staging");
+  B200_CHECK (ctx, cudaMemcpyAsync (pl->staging.ptr, h_in, bytes, cudaMemcpyHostToDevice,
+                                    ctx->stream), "upload block");
+  return pipeline_block (pl, pl->staging.ptr, ndat, 0, ndat_folded);
+}
+
+int dspsr_b200_pipeline_get_profiles (dspsr_b200_pipeline* pl, float* profiles, uint32_t* hits)
+{
+  if (!pl) return DSPSR_B200_EINVAL;
+  return dspsr_b200_fold_get_profiles (&pl->fold, profiles, hits);
+}
+
+int dspsr_b200_pipeline_reset (dspsr_b200_pipeline* pl)
+{
+  if (!pl) return DSPSR_B200_EINVAL;
+  pl->ncarry = 0;
+  pl->in0 = 0;
+  return pl->fold.reset ();
+}
+
+int dspsr_b200_pipeline_profile (dspsr_b200_pipeline* pl, int enable)
+{
+  if (!pl) return DSPSR_B200_EINVAL;
+  B200_CHECK (pl->ctx, cudaStreamSynchronize (pl->ctx->stream), "pipeline_profile sync");
+  pl->clock.clear ();
+  pl->clock.on = enable != 0;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_pipeline_kernel_times (dspsr_b200_pipeline* pl, double* ms, uint64_t* launches)
+{
+  if (!pl || !ms || !launches) return DSPSR_B200_EINVAL;
+  dspsr_b200_context* ctx = pl->ctx;
+  B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "kernel_times sync");
+  for (int k = 0; k < KK_COUNT; k++)
+  {
+    ms[k] = 0.0;
+    launches[k] = 0;
+  }
+  for (size_t i = 0; i < pl->clock.kind.size (); i++)
+  {
+    float t = 0.f;
+    B200_CHECK (ctx, cudaEventElapsedTime (&t, pl->clock.pool[2 * i], pl->clock.pool[2 * i + 1]),
+                "cudaEventElapsedTime");
+    ms[pl->clock.kind[i]] += t;
+    launches[pl->clock.kind[i]]++;
+  }
+  pl->clock.clear ();
+  return DSPSR_B200_OK;
+}
+
+uint64_t dspsr_b200_kernel_launches (void) { return kernel_launches (); }
+
+int dspsr_b200_pipeline_info (dspsr_b200_pipeline* pl, uint64_t* info)
+{
+  if (!pl || !info) return DSPSR_B200_EINVAL;
+  const ConvShape& sh = pl->conv.shape;
+  info[0] = sh.nfft;
+  info[1] = sh.nkeep;
+  info[2] = sh.n1;
+  info[3] = sh.n2;
+  info[4] = pl->conv.max_batch;
+  info[5] = pl->ncarry;
+  info[6] = pl->in0;
+  info[7] = uint64_t (pl->fold.nseg);
+  return DSPSR_B200_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,220 @@
+// fft_core.cuh -- FFT building blocks for the B200 convolution kernels.
+//
+// Everything here is __host__ __device__ so that the index arithmetic of the
+// shared-memory Stockham passes can be exercised on the CPU (one "thread" at a
+// time, phase by phase) as well as on the GPU.
+//
+// Conventions follow the reference's FTransform (FFTW): forward transforms use
+// exp(-2 pi i nk/N) (D = -1), backward transforms exp(+2 pi i nk/N) (D = +1),
+// both unnormalised.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define B200_HD __host__ __device__ __forceinline__
+
+namespace b200 {
+
+B200_HD float2 cadd (float2 a, float2 b) { return make_float2 (a.x + b.x, a.y + b.y); }
+B200_HD float2 csub (float2 a, float2 b) { return make_float2 (a.x - b.x, a.y - b.y); }
+B200_HD float2 cmul (float2 a, float2 b)
+{
+  return make_float2 (a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+B200_HD float2 cmulc (float2 a, float2 b)
+{
+  return make_float2 (a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+B200_HD float2 cscale (float2 a, float s) { return make_float2 (a.x * s, a.y * s); }
+
+// cos(2 pi j / 64) for j = 0..16, correctly rounded decimal expansions.
+B200_HD constexpr float quarter_cos64 (int j)
+{
+  return j == 0 ? 1.0f
+       : j == 1 ? 0.99518472667219692873f
+       : j == 2 ? 0.98078528040323043058f
+       : j == 3 ? 0.95694033573220882438f
+       : j == 4 ? 0.92387953251128673848f
+       : j == 5 ? 0.88192126434835504956f
+       : j == 6 ? 0.83146961230254523567f
+       : j == 7 ? 0.77301045336273699338f
+       : j == 8 ? 0.70710678118654752440f
+       : j == 9 ? 0.63439328416364548779f
+       : j == 10 ? 0.55557023301960222474f
+       : j == 11 ? 0.47139673682599764856f
+       : j == 12 ? 0.38268343236508977173f
+       : j == 13 ? 0.29028467725446236764f
+       : j == 14 ? 0.19509032201612826785f
+       : j == 15 ? 0.09801714032956060199f
+       : 0.0f;
+}
+
+// cos and sin of 2 pi j / 64 for any integer j (reduced to the first quadrant)
+B200_HD constexpr float cos64 (int j)
+{
+  return (j & 63) <= 16 ? quarter_cos64 (j & 63)
+       : (j & 63) <= 32 ? -quarter_cos64 (32 - (j & 63))
+       : (j & 63) <= 48 ? -quarter_cos64 ((j & 63) - 32)
+       : quarter_cos64 (64 - (j & 63));
+}
+B200_HD constexpr float sin64 (int j) { return cos64 (j - 16); }
+
+// v * w_R^k with w_R = exp(D 2 pi i / R); k is a compile-time constant after
+// unrolling, so the special cases cost nothing.
+template <int R, int D>
+B200_HD float2 tw_mul (int k, float2 v)
+{
+  const int j = (k * 64 / R) & 63;     // angle in units of 2 pi / 64
+  if (j == 0) return v;
+  if (j == 16) return D < 0 ? make_float2 (v.y, -v.x) : make_float2 (-v.y, v.x);
+  if (j == 32) return make_float2 (-v.x, -v.y);
+  if (j == 48) return D < 0 ? make_float2 (-v.y, v.x) : make_float2 (v.y, -v.x);
+  const float c = cos64 (j);
+  const float s = D < 0 ? -sin64 (j) : sin64 (j);
+  if (j == 8 || j == 24 || j == 40 || j == 56)
+  {
+    // |c| == |s| == sqrt(1/2): (v.x c - v.y s, v.x s + v.y c)
+    const float h = quarter_cos64 (8);
+    const float a = (c > 0 ? v.x : -v.x);
+    const float b = (s > 0 ? v.y : -v.y);
+    const float e = (s > 0 ? v.x : -v.x);
+    const float f = (c > 0 ? v.y : -v.y);
+    return make_float2 ((a - b) * h, (e + f) * h);
+  }
+  return make_float2 (v.x * c - v.y * s, v.x * s + v.y * c);
+}
+
+// In-register DFT of size R (power of two, R <= 64), natural order in and out.
+// Recursive radix-2 decimation in time, fully unrolled.
+template <int R, int D>
+struct RegDFT
+{
+  B200_HD static void run (float2* v)
+  {
+    float2 e[R / 2], o[R / 2];
+#pragma unroll
+    for (int i = 0; i < R / 2; i++)
+    {
+      e[i] = v[2 * i];
+      o[i] = v[2 * i + 1];
+    }
+    RegDFT<R / 2, D>::run (e);
+    RegDFT<R / 2, D>::run (o);
+#pragma unroll
+    for (int k = 0; k < R / 2; k++)
+    {
+      const float2 t = tw_mul<R, D> (k, o[k]);
+      v[k] = cadd (e[k], t);
+      v[k + R / 2] = csub (e[k], t);
+    }
+  }
+};
+
+template <int D>
+struct RegDFT<2, D>
+{
+  B200_HD static void run (float2* v)
+  {
+    const float2 a = v[0], b = v[1];
+    v[0] = cadd (a, b);
+    v[1] = csub (a, b);
+  }
+};
+
+template <int D>
+struct RegDFT<1, D>
+{
+  B200_HD static void run (float2*) {}
+};
+
+// Shared-memory index padding: one float2 of padding per 16 entries keeps the
+// strided Stockham stores of the early passes off a single bank.
+B200_HD int spad (int i) { return i + (i >> 4); }
+B200_HD constexpr int spad_size (int n) { return n + (n >> 4); }
+
+// Stockham pass schedule for an N-point transform run by T = N/16 threads:
+// every pass leaves each thread exactly 16 complex values in registers.
+// Returns the radix of pass p (0 when there is no such pass).
+B200_HD constexpr int stockham_radix (int N, int p)
+{
+  return N == 16384 ? (p < 3 ? 16 : p == 3 ? 4 : 0)
+       : N == 8192 ? (p < 3 ? 16 : p == 3 ? 2 : 0)
+       : N == 4096 ? (p < 3 ? 16 : 0)
+       : N == 2048 ? (p < 2 ? 16 : p == 2 ? 8 : 0)
+       : N == 1024 ? (p < 2 ? 16 : p == 2 ? 4 : 0)
+       : N == 512 ? (p < 2 ? 16 : p == 2 ? 2 : 0)
+       : N == 256 ? (p < 2 ? 16 : 0)
+       : 0;
+}
+
+B200_HD constexpr int stockham_npass (int N)
+{
+  return stockham_radix (N, 0) == 0 ? 0
+       : stockham_radix (N, 1) == 0 ? 1
+       : stockham_radix (N, 2) == 0 ? 2
+       : stockham_radix (N, 3) == 0 ? 3 : 4;
+}
+
+// product of the radices of passes before p
+B200_HD constexpr int stockham_ns (int N, int p)
+{
+  return p == 0 ? 1 : stockham_ns (N, p - 1) * stockham_radix (N, p - 1);
+}
+
+// threads of an N-point transform
+B200_HD constexpr int stockham_threads (int N) { return N / 16; }
+
+// One radix-R Stockham pass (Govindaraju et al., SC08, "High performance
+// discrete Fourier transforms on graphics processors"): butterfly j reads
+// x[j + r N/R], applies w_{Ns R}^{(j mod Ns) r}, performs an R-point DFT and
+// writes x'[(j div Ns) Ns R + (j mod Ns) + r Ns].  Output is in natural order
+// after the last pass.  tw[m] = exp(-2 pi i m / N) (FP64-computed, rounded).
+template <int N, int R, int T, int D>
+struct StockhamPass
+{
+  static constexpr int NB = N / R;      // butterflies in this pass
+  static constexpr int BPT = NB / T;    // butterflies per thread
+  static_assert (BPT >= 1 && BPT * T == NB, "thread count does not tile the pass");
+
+  B200_HD static void load (int tid, const float2* s, float2* v)
+  {
+#pragma unroll
+    for (int b = 0; b < BPT; b++)
+    {
+      const int j = tid + b * T;
+#pragma unroll
+      for (int r = 0; r < R; r++)
+        v[b * R + r] = s[spad (j + r * NB)];
+    }
+  }
+
+  B200_HD static void compute_store (int tid, int Ns, float2* v, float2* s, const float2* tw)
+  {
+#pragma unroll
+    for (int b = 0; b < BPT; b++)
+    {
+      const int j = tid + b * T;
+      const int a = j & (Ns - 1);
+      float2* x = v + b * R;
+      if (Ns > 1)
+      {
+        const int step = N / (Ns * R);
+#pragma unroll
+        for (int r = 1; r < R; r++)
+        {
+          const float2 w = tw[a * r * step];
+          x[r] = D < 0 ? cmul (x[r], w) : cmulc (x[r], w);
+        }
+      }
+      RegDFT<R, D>::run (x);
+      const int idxD = (j - a) * R + a;
+#pragma unroll
+      for (int r = 0; r < R; r++)
+        s[spad (idxD + r * Ns)] = x[r];
+    }
+  }
+};
+
+} // namespace b200

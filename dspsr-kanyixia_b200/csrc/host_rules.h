@@ -1,0 +1,31 @@
+// host_rules.h -- host-side rules of the B200 engine (see host_rules.cpp)
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+namespace b200 {
+
+// One arithmetic segment of the exact fold-bin plan: sample start+j (j below
+// the next segment's start) has frac(phi) = (m0 + j*dm) * g exactly.
+struct FoldSegment
+{
+  uint64_t start;
+  int64_t m0;
+  int64_t dm;
+  double g;
+};
+
+unsigned smearing_samples (double centre_frequency, double bandwidth, double dm,
+                           unsigned nchan, int half);
+unsigned minimum_ndat (unsigned impulse_pos, unsigned impulse_neg);
+int64_t optimal_fft_length (uint64_t nbad, uint64_t nfft_max, unsigned factor);
+void bittable8 (double spacing, bool twos_complement, float* lut, double* scale);
+double fold_phi (int64_t start_day, int64_t start_sec, double start_frac,
+                 int64_t epoch_day, int64_t epoch_sec, double epoch_frac,
+                 uint64_t idat_start, double rate, double period, double reference_phase);
+// Returns the number of segments; fills *out when non-null.
+int64_t build_fold_plan (double phi, double phase_per_sample, uint64_t ndat,
+                         std::vector<FoldSegment>* out);
+
+} // namespace b200

@@ -1,0 +1,803 @@
+// kernels.cu -- sm_100a kernels of the B200 baseband hot path.
+//
+// Overlap-save coherent dedispersion (Signal/General/Convolution.C:724-803 is
+// the CPU algorithm; CUDA::ConvolutionEngine runs it as cuFFT + 3 kernels per
+// batch) is restructured here as a four-step FFT of length N = n1 * n2:
+//
+//   K1 (columns)  unpack the int8/int16/float input on load, n1-point DFTs in
+//                 registers across the n1 chunks of n2 samples, store rows k1.
+//   K2 (rows)     twiddle w_N^{k1 n2}, n2-point Stockham FFT in shared memory,
+//                 multiply by the response (stored in four-step order), inverse
+//                 n2-point FFT, conjugate twiddle -- one read and one write.
+//   K3 (columns)  inverse n1-point DFTs in registers, overlap discard, and then
+//                 either write the voltages (Engine::perform) or detect and
+//                 fold in the same pass (warp-segmented reduction by bin).
+//
+// For n1 == 1 a single kernel does load, FFT, multiply, inverse FFT and the
+// epilogue entirely in shared memory: one HBM round trip per part.
+//
+// FFT sign conventions are FFTW's (forward -1, backward +1, unnormalised); the
+// 1/sqrt(N) normaliser is folded into the response, as Convolution::prepare
+// does (Convolution.C:401-414).
+
+#include "kernels.cuh"
+#include "fft_core.cuh"
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+
+namespace b200 {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+std::atomic<uint64_t> g_launches {0};
+
+struct ClockScope
+{
+  const KernelClock* c;
+  int kind;
+  cudaStream_t st;
+  ClockScope (const KernelClock* c_, int k, cudaStream_t s) : c (c_), kind (k), st (s)
+  {
+    g_launches++;
+    if (c) c->mark (c->self, kind, 0, st);
+  }
+  ~ClockScope ()
+  {
+    if (c) c->mark (c->self, kind, 1, st);
+  }
+};
+
+// --------------------------------------------------------------------------
+// input fetch (unpack fused into the load)
+// --------------------------------------------------------------------------
+
+template <int KIND>
+__device__ __forceinline__ float2 fetch (const InputView& in, const float* s_lut,
+                                         unsigned c, unsigned p, uint64_t t)
+{
+  const void* base = in.main;
+  uint64_t span = in.main_span;
+  if (t < in.npre)
+    base = in.pre, span = in.pre_span;
+  else
+    t -= in.npre;
+  if constexpr (KIND == IN_INT8)
+  {
+    const uint8_t* b = static_cast<const uint8_t*> (base)
+                       + ((t * in.nchan + c) * in.npol + p) * 2;
+    const unsigned short w = __ldg (reinterpret_cast<const unsigned short*> (b));
+    return make_float2 (s_lut[w & 0xff], s_lut[w >> 8]);
+  }
+  else if constexpr (KIND == IN_INT16)
+  {
+    const int16_t* q = static_cast<const int16_t*> (base)
+                       + ((t * in.nchan + c) * in.npol + p) * 2;
+    const unsigned w = __ldg (reinterpret_cast<const unsigned*> (q));
+    short re = short (w & 0xffff), im = short (w >> 16);
+    if (in.offset_binary)
+    {
+      re = short (re ^ 0x8000);
+      im = short (im ^ 0x8000);
+    }
+    // SixteenBitUnpacker.C:69: float(x) + 0.5 (the double 0.5 rounds to float)
+    return make_float2 (__fadd_rn (float (re), 0.5f), __fadd_rn (float (im), 0.5f));
+  }
+  else
+  {
+    const float2* f = static_cast<const float2*> (base);
+    return __ldg (f + (uint64_t (c) * in.npol + p) * span + t);
+  }
+}
+
+__device__ __forceinline__ void load_lut (const InputView& in, const float* lut, float* s_lut)
+{
+  if (in.kind == IN_INT8)
+    for (int i = threadIdx.x; i < 256; i += blockDim.x)
+      s_lut[i] = lut[i];
+}
+
+// --------------------------------------------------------------------------
+// detection (Detection.C:253-301 Intensity/PPQQ order, cross_detect.ic:38-41,
+// stokes_detect.ic:40-43); explicit _rn arithmetic so that no product is
+// fused into an FMA and every value rounds as the reference's CPU code does.
+// --------------------------------------------------------------------------
+
+__device__ __forceinline__ void detect_values (int state, unsigned npol, float2 p, float2 q,
+                                               float* o)
+{
+  if (state == 0)
+  {
+    float v = __fmul_rn (p.x, p.x);
+    v = __fadd_rn (v, __fmul_rn (p.y, p.y));
+    if (npol == 2)
+    {
+      v = __fadd_rn (v, __fmul_rn (q.x, q.x));
+      v = __fadd_rn (v, __fmul_rn (q.y, q.y));
+    }
+    o[0] = v;
+    return;
+  }
+  const float pp = __fadd_rn (__fmul_rn (p.x, p.x), __fmul_rn (p.y, p.y));
+  const float qq = __fadd_rn (__fmul_rn (q.x, q.x), __fmul_rn (q.y, q.y));
+  if (state == 1)
+  {
+    o[0] = pp;
+    o[1] = qq;
+    return;
+  }
+  const float re = __fadd_rn (__fmul_rn (p.x, q.x), __fmul_rn (p.y, q.y));
+  const float im = __fsub_rn (__fmul_rn (p.x, q.y), __fmul_rn (p.y, q.x));
+  if (state == 2)
+  {
+    o[0] = pp;
+    o[1] = qq;
+    o[2] = re;
+    o[3] = im;
+    return;
+  }
+  o[0] = __fadd_rn (pp, qq);
+  o[1] = __fsub_rn (pp, qq);
+  o[2] = __fmul_rn (2.0f, re);
+  o[3] = __fmul_rn (2.0f, im);
+}
+
+// --------------------------------------------------------------------------
+// fold
+// --------------------------------------------------------------------------
+
+// Exact bin of plan sample t (see host_rules.cpp for the segment algebra).
+__device__ __forceinline__ unsigned fold_bin (const FoldSegment* __restrict__ segs, int nseg,
+                                              uint64_t t, unsigned nbin)
+{
+  int lo = 0, hi = nseg - 1;
+  while (lo < hi)
+  {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg (&segs[mid].start) <= t) lo = mid; else hi = mid - 1;
+  }
+  const uint64_t start = __ldg (&segs[lo].start);
+  const int64_t m0 = __ldg (&segs[lo].m0);
+  const int64_t dm = __ldg (&segs[lo].dm);
+  const double g = __ldg (&segs[lo].g);
+  const double y = __dmul_rn (double (m0 + int64_t (t - start) * dm), g);
+  return __double2uint_rz (__dmul_rn (y, double (nbin)));
+}
+
+// All 32 lanes call this together.  Lanes holding consecutive time samples
+// with equal bins form runs; each run is summed by a segmented shuffle
+// reduction and added to the profile by its first lane with one atomic.
+template <int NOUT>
+__device__ __forceinline__ void warp_fold (bool ok, unsigned bin, const float* v,
+                                           float* prof, unsigned nbin, unsigned* hits)
+{
+  const int lane = threadIdx.x & 31;
+  const unsigned key = ok ? bin : 0xffffffffu;
+  const unsigned prev = __shfl_up_sync (FULL, key, 1);
+  const bool head = (lane == 0) || (prev != key);
+  const unsigned hm = __ballot_sync (FULL, head);
+  const int rid = __popc (hm & (FULL >> (31 - lane)));
+  float acc[NOUT];
+#pragma unroll
+  for (int k = 0; k < NOUT; k++) acc[k] = ok ? v[k] : 0.0f;
+  int cnt = ok ? 1 : 0;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1)
+  {
+    const int orid = __shfl_down_sync (FULL, rid, off);
+    const bool take = (lane + off < 32) && (orid == rid);
+#pragma unroll
+    for (int k = 0; k < NOUT; k++)
+    {
+      const float o = __shfl_down_sync (FULL, acc[k], off);
+      if (take) acc[k] += o;
+    }
+    const int oc = __shfl_down_sync (FULL, cnt, off);
+    if (take) cnt += oc;
+  }
+  if (head && ok)
+  {
+#pragma unroll
+    for (int k = 0; k < NOUT; k++)
+      atomicAdd (prof + uint64_t (k) * nbin + bin, acc[k]);
+    if (hits) atomicAdd (hits + bin, unsigned (cnt));
+  }
+}
+
+template <int NOUT>
+__device__ __forceinline__ void emit_fold (const FoldView& fv, unsigned c, unsigned npol, bool ok,
+                                           uint64_t t, float2 p, float2 q)
+{
+  float v[4] = {0.f, 0.f, 0.f, 0.f};
+  unsigned bin = 0;
+  if (ok)
+  {
+    detect_values (fv.state, npol, p, q, v);
+    bin = fold_bin (fv.segs, fv.nseg, t, fv.nbin);
+    ok = bin < fv.nbin;
+  }
+  warp_fold<NOUT> (ok, bin, v, fv.profiles + uint64_t (c) * NOUT * fv.nbin, fv.nbin,
+                   c == 0 ? fv.hits : nullptr);
+}
+
+// --------------------------------------------------------------------------
+// shared-memory Stockham FFT
+// --------------------------------------------------------------------------
+
+template <int N, int T, int D, int P>
+__device__ __forceinline__ void smem_pass (float2* s, float2* v, const float2* tw)
+{
+  if constexpr (P < stockham_npass (N))
+  {
+    constexpr int R = stockham_radix (N, P);
+    constexpr int Ns = stockham_ns (N, P);
+    StockhamPass<N, R, T, D>::load (threadIdx.x, s, v);
+    __syncthreads ();
+    StockhamPass<N, R, T, D>::compute_store (threadIdx.x, Ns, v, s, tw);
+    __syncthreads ();
+    smem_pass<N, T, D, P + 1> (s, v, tw);
+  }
+}
+
+// N-point FFT of s[spad(0..N-1)] in place; the caller has synchronised after
+// writing s.  Returns synchronised.
+template <int N, int T, int D>
+__device__ __forceinline__ void smem_fft (float2* s, const float2* tw)
+{
+  float2 v[N / T];
+  smem_pass<N, T, D, 0> (s, v, tw);
+}
+
+// --------------------------------------------------------------------------
+// K1: forward column DFTs with the unpack fused into the load
+// --------------------------------------------------------------------------
+
+template <int N1, int KIND>
+__global__ void __launch_bounds__ (128, 4)
+k_fwd_cols (const InputView in, const float* __restrict__ lut, const uint64_t nkeep,
+            const uint64_t part0, const unsigned n2, float2* __restrict__ scratch)
+{
+  __shared__ float s_lut[256];
+  load_lut (in, lut, s_lut);
+  __syncthreads ();
+  const unsigned i2 = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned b = blockIdx.y;
+  const unsigned c = blockIdx.z;
+  const uint64_t N = uint64_t (N1) * n2;
+  const uint64_t t0 = (part0 + b) * nkeep + i2;
+  for (unsigned p = 0; p < in.npol; p++)
+  {
+    float2 v[N1];
+#pragma unroll
+    for (int k = 0; k < N1; k++)
+      v[k] = fetch<KIND> (in, s_lut, c, p, t0 + uint64_t (k) * n2);
+    RegDFT<N1, -1>::run (v);
+    float2* dst = scratch + ((uint64_t (b) * in.nchan + c) * in.npol + p) * N + i2;
+#pragma unroll
+    for (int k = 0; k < N1; k++)
+      dst[uint64_t (k) * n2] = v[k];
+  }
+}
+
+// --------------------------------------------------------------------------
+// K2: rows -- twiddle, FFT, response, inverse FFT, conjugate twiddle
+// --------------------------------------------------------------------------
+
+template <int N2, int T>
+__global__ void __launch_bounds__ (T, 512 / T)
+k_rows (float2* __restrict__ scratch, const float2* __restrict__ tw4,
+        const float2* __restrict__ tw2, const float2* __restrict__ H, const unsigned n1,
+        const unsigned nchan, const unsigned npol)
+{
+  extern __shared__ float2 s[];
+  const unsigned k1 = blockIdx.x;
+  const unsigned b = blockIdx.y;
+  const unsigned cp = blockIdx.z;
+  const unsigned c = cp / npol;
+  const uint64_t N = uint64_t (n1) * N2;
+  float2* row = scratch + (uint64_t (b) * nchan * npol + cp) * N + uint64_t (k1) * N2;
+  const float2* twr = tw4 + uint64_t (k1) * N2;
+  for (int i = threadIdx.x; i < N2; i += T)
+    s[spad (i)] = cmul (row[i], __ldg (twr + i));
+  __syncthreads ();
+  smem_fft<N2, T, -1> (s, tw2);
+  const float2* h = H + (uint64_t (c) * n1 + k1) * N2;
+  for (int i = threadIdx.x; i < N2; i += T)
+  {
+    // Response::operate (Response.C:662-726): (f_r d_r - f_i d_i, f_i d_r + f_r d_i)
+    const float2 d = s[spad (i)];
+    const float2 f = __ldg (h + i);
+    s[spad (i)] = make_float2 (d.x * f.x - d.y * f.y, d.x * f.y + d.y * f.x);
+  }
+  __syncthreads ();
+  smem_fft<N2, T, +1> (s, tw2);
+  for (int i = threadIdx.x; i < N2; i += T)
+    row[i] = cmulc (s[spad (i)], __ldg (twr + i));
+}
+
+// --------------------------------------------------------------------------
+// K3: inverse column DFTs, overlap discard, voltage out or detect + fold
+// --------------------------------------------------------------------------
+
+template <int N1, int NPOL, int MODE, int NOUT>
+__global__ void __launch_bounds__ (128, 4)
+k_inv_cols (const float2* __restrict__ scratch, const unsigned n2, const unsigned nchan,
+            const uint64_t nkeep, const unsigned nfilt_pos, const uint64_t part0,
+            const FoldView fv, const VoltView vv)
+{
+  const unsigned i2 = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned b = blockIdx.y;
+  const unsigned c = blockIdx.z;
+  const uint64_t N = uint64_t (N1) * n2;
+  float2 v[NPOL][N1];
+#pragma unroll
+  for (int p = 0; p < NPOL; p++)
+  {
+    const float2* src = scratch + ((uint64_t (b) * nchan + c) * NPOL + p) * N + i2;
+#pragma unroll
+    for (int k = 0; k < N1; k++)
+      v[p][k] = src[uint64_t (k) * n2];
+    RegDFT<N1, +1>::run (v[p]);
+  }
+  const uint64_t tbase = (part0 + b) * nkeep;
+#pragma unroll
+  for (int k = 0; k < N1; k++)
+  {
+    const uint64_t tl = uint64_t (k) * n2 + i2;
+    const bool ok = tl >= nfilt_pos && tl < nfilt_pos + nkeep;
+    const uint64_t t = tbase + (tl - nfilt_pos);
+    if constexpr (MODE == OUT_VOLTAGE)
+    {
+      if (ok)
+      {
+#pragma unroll
+        for (int p = 0; p < NPOL; p++)
+          vv.out[(uint64_t (c) * NPOL + p) * vv.span + t] = v[p][k];
+      }
+    }
+    else
+      emit_fold<NOUT> (fv, c, NPOL, ok, t, v[0][k], v[NPOL - 1][k]);
+  }
+}
+
+// --------------------------------------------------------------------------
+// single-kernel path (n1 == 1): everything in shared memory
+// --------------------------------------------------------------------------
+
+template <int N, int T, int KIND, int MODE, int NOUT>
+__global__ void __launch_bounds__ (T, 512 / T)
+k_fused (const InputView in, const float* __restrict__ lut, const float2* __restrict__ tw,
+         const float2* __restrict__ H, const uint64_t nkeep, const unsigned nfilt_pos,
+         const uint64_t part0, const FoldView fv, const VoltView vv)
+{
+  extern __shared__ float2 s[];
+  __shared__ float s_lut[256];
+  constexpr int SP = spad_size (N);
+  const unsigned b = blockIdx.x;
+  const unsigned c = blockIdx.y;
+  const uint64_t part = part0 + b;
+  const unsigned npol = in.npol;
+  load_lut (in, lut, s_lut);
+  __syncthreads ();
+  for (unsigned p = 0; p < npol; p++)
+    for (int i = threadIdx.x; i < N; i += T)
+      s[p * SP + spad (i)] = fetch<KIND> (in, s_lut, c, p, part * nkeep + i);
+  __syncthreads ();
+  const float2* h = H + uint64_t (c) * N;
+  for (unsigned p = 0; p < npol; p++)
+  {
+    float2* sp = s + p * SP;
+    smem_fft<N, T, -1> (sp, tw);
+    for (int i = threadIdx.x; i < N; i += T)
+    {
+      const float2 d = sp[spad (i)];
+      const float2 f = __ldg (h + i);
+      sp[spad (i)] = make_float2 (d.x * f.x - d.y * f.y, d.x * f.y + d.y * f.x);
+    }
+    __syncthreads ();
+    smem_fft<N, T, +1> (sp, tw);
+  }
+  const uint64_t tbase = part * nkeep;
+  const unsigned rounds = unsigned ((nkeep + T - 1) / T);
+  for (unsigned r = 0; r < rounds; r++)
+  {
+    const uint64_t j = uint64_t (r) * T + threadIdx.x;
+    const bool ok = j < nkeep;
+    const int tl = ok ? int (nfilt_pos + j) : 0;
+    const float2 pv = s[spad (tl)];
+    const float2 qv = npol > 1 ? s[SP + spad (tl)] : make_float2 (0.f, 0.f);
+    if (MODE == OUT_VOLTAGE)
+    {
+      if (ok)
+      {
+        vv.out[(uint64_t (c) * npol) * vv.span + tbase + j] = pv;
+        if (npol > 1) vv.out[(uint64_t (c) * npol + 1) * vv.span + tbase + j] = qv;
+      }
+    }
+    else
+      emit_fold<NOUT> (fv, c, npol, ok, tbase + j, pv, qv);
+  }
+}
+
+// --------------------------------------------------------------------------
+// response construction
+// --------------------------------------------------------------------------
+
+// Dedispersion::build_compute (Dedispersion.C:166-186) on the grid of the
+// restated PlasmaResponse::build: channel ichan centred at chan_freq, bin ipt
+// at freq = ipt*binwidth - chanwidth/2 (natural order).  FFT-order index k
+// maps to ipt = k + N/2 (mod N) when the halves are swapped
+// (Response::doswap, Response.C:998-1050).  Written in four-step order
+// H[c][k1][k2] for k = k1 + n1*k2.
+__global__ void k_build_chirp (float2* __restrict__ H, const double* __restrict__ chan_freq,
+                               const double* __restrict__ coeff, const unsigned nfft,
+                               const unsigned n1, const unsigned n2, const double binwidth,
+                               const double half_chanwidth, const int swap_halves,
+                               const int chirp_mode, const float scale)
+{
+  const uint64_t idx = uint64_t (blockIdx.x) * blockDim.x + threadIdx.x;
+  const unsigned c = blockIdx.y;
+  if (idx >= nfft) return;
+  const unsigned k1 = unsigned (idx / n2), k2 = unsigned (idx % n2);
+  const unsigned k = k1 + n1 * k2;
+  const unsigned ipt = swap_halves ? (k + nfft / 2) % nfft : k;
+  const double cf = chan_freq[c];
+  const double freq = __dsub_rn (__dmul_rn (double (ipt), binwidth), half_chanwidth);
+  const double num = __dmul_rn (coeff[c], __dmul_rn (freq, freq));
+  const double phase = __ddiv_rn (num, __dadd_rn (cf, freq));
+  float re, im;
+  if (chirp_mode == 0)
+  {
+    // Dedispersion.C:104-111: phases stored as float, then polar(1.0f, phase)
+    const float ph = __double2float_rn (phase);
+    sincosf (ph, &im, &re);
+  }
+  else
+  {
+    const double two_pi = 6.283185307179586476925286766559;
+    const double red = __dsub_rn (phase, __dmul_rn (two_pi, rint (__ddiv_rn (phase, two_pi))));
+    double s, co;
+    sincos (red, &s, &co);
+    re = __double2float_rn (co);
+    im = __double2float_rn (s);
+  }
+  H[uint64_t (c) * nfft + idx] = make_float2 (__fmul_rn (re, scale), __fmul_rn (im, scale));
+}
+
+__global__ void k_permute (float2* __restrict__ dst, const float2* __restrict__ src,
+                           const unsigned n1, const unsigned n2, const int inverse)
+{
+  const uint64_t N = uint64_t (n1) * n2;
+  const uint64_t idx = uint64_t (blockIdx.x) * blockDim.x + threadIdx.x;
+  const unsigned c = blockIdx.y;
+  if (idx >= N) return;
+  const unsigned k1 = unsigned (idx / n2), k2 = unsigned (idx % n2);
+  const uint64_t k = k1 + uint64_t (n1) * k2;
+  if (inverse)
+    dst[c * N + k] = src[c * N + idx];
+  else
+    dst[c * N + idx] = src[c * N + k];
+}
+
+// --------------------------------------------------------------------------
+// standalone engines
+// --------------------------------------------------------------------------
+
+__global__ void k_unpack8 (const uint8_t* __restrict__ in, const uint64_t ndat,
+                           const unsigned nchan, const unsigned npol, const unsigned ndim,
+                           const float* __restrict__ lut, float* __restrict__ out,
+                           const uint64_t span)
+{
+  __shared__ float s_lut[256];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) s_lut[i] = lut[i];
+  __syncthreads ();
+  const uint64_t t = uint64_t (blockIdx.x) * blockDim.x + threadIdx.x;
+  const unsigned c = blockIdx.y;
+  if (t >= ndat) return;
+  const uint8_t* src = in + (t * nchan + c) * npol * ndim;
+  for (unsigned p = 0; p < npol; p++)
+    for (unsigned d = 0; d < ndim; d++)
+      out[(uint64_t (c) * npol + p) * span + t * ndim + d] = s_lut[src[p * ndim + d]];
+}
+
+__global__ void k_unpack16 (const int16_t* __restrict__ in, const uint64_t ndat,
+                            const unsigned nchan, const unsigned npol, const unsigned ndim,
+                            const int offset_binary, float* __restrict__ out,
+                            const uint64_t span)
+{
+  const uint64_t t = uint64_t (blockIdx.x) * blockDim.x + threadIdx.x;
+  const unsigned c = blockIdx.y;
+  if (t >= ndat) return;
+  const int16_t* src = in + (t * nchan + c) * npol * ndim;
+  for (unsigned p = 0; p < npol; p++)
+    for (unsigned d = 0; d < ndim; d++)
+    {
+      short v = src[p * ndim + d];
+      if (offset_binary) v = short (v ^ 0x8000);
+      out[(uint64_t (c) * npol + p) * span + t * ndim + d] = __fadd_rn (float (v), 0.5f);
+    }
+}
+
+__global__ void k_detect (const float2* __restrict__ in, const uint64_t in_span,
+                          const uint64_t ndat, const int state, float* __restrict__ out,
+                          const uint64_t out_span)
+{
+  const uint64_t t = uint64_t (blockIdx.x) * blockDim.x + threadIdx.x;
+  const unsigned c = blockIdx.y;
+  if (t >= ndat) return;
+  const float2 p = in[(uint64_t (c) * 2) * in_span + t];
+  const float2 q = in[(uint64_t (c) * 2 + 1) * in_span + t];
+  float v[4];
+  detect_values (state, 2, p, q, v);
+  const int nout = detect_nout (state);
+  for (int k = 0; k < nout; k++)
+    out[(uint64_t (c) * nout + k) * out_span + t] = v[k];
+}
+
+// Fold::Engine::fold on detected FPT floats (ndim 1): one warp covers 32
+// consecutive samples of one (chan, pol).
+__global__ void k_fold (const float* __restrict__ in, const uint64_t in_span,
+                        const uint64_t ndat, const unsigned npol, const FoldView fv)
+{
+  const uint64_t t = uint64_t (blockIdx.x) * blockDim.x + threadIdx.x;
+  const unsigned c = blockIdx.y;
+  bool ok = t < ndat;
+  unsigned bin = 0;
+  if (ok)
+  {
+    bin = fold_bin (fv.segs, fv.nseg, t, fv.nbin);
+    ok = bin < fv.nbin;
+  }
+  for (unsigned p = 0; p < npol; p++)
+  {
+    float v = ok ? in[(uint64_t (c) * npol + p) * in_span + t] : 0.f;
+    warp_fold<1> (ok, bin, &v, fv.profiles + (uint64_t (c) * npol + p) * fv.nbin, fv.nbin,
+                  (c == 0 && p == 0) ? fv.hits : nullptr);
+  }
+}
+
+__global__ void k_binplan (const FoldSegment* __restrict__ segs, const int nseg,
+                           const uint64_t ndat, const unsigned nbin, uint32_t* __restrict__ out)
+{
+  const uint64_t t = uint64_t (blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= ndat) return;
+  out[t] = fold_bin (segs, nseg, t, nbin);
+}
+
+// --------------------------------------------------------------------------
+// launch helpers
+// --------------------------------------------------------------------------
+
+template <int N1, int NPOL, int MODE, int NOUT>
+void launch_inv (const ConvShape& sh, dim3 grid, float2* scratch, uint64_t part0,
+                 const FoldView& fv, const VoltView& vv, cudaStream_t st)
+{
+  k_inv_cols<N1, NPOL, MODE, NOUT><<<grid, 128, 0, st>>> (scratch, sh.n2, sh.nchan, sh.nkeep,
+                                                          sh.nfilt_pos, part0, fv, vv);
+}
+
+template <int N2>
+void launch_rows (dim3 grid, float2* scratch, const ConvTables& tb, unsigned n1,
+                  const ConvShape& sh, cudaStream_t st)
+{
+  constexpr int T = stockham_threads (N2);
+  const size_t smem = spad_size (N2) * sizeof (float2);
+  k_rows<N2, T><<<grid, T, smem, st>>> (scratch, tb.tw4, tb.tw2, tb.H, n1, sh.nchan, sh.npol);
+}
+
+template <int N1>
+cudaError_t run_fourstep_n1 (const ConvShape& sh, const ConvTables& tb, const InputView& in,
+                             uint64_t part0, unsigned nbatch, float2* scratch, int mode,
+                             const FoldView& fv, const VoltView& vv, cudaStream_t st,
+                             const KernelClock* clk)
+{
+  const dim3 gcol (sh.n2 / 128, nbatch, sh.nchan);
+  {
+  ClockScope cs (clk, KK_FWD_COLS, st);
+  if (in.kind == IN_INT8)
+    k_fwd_cols<N1, IN_INT8><<<gcol, 128, 0, st>>> (in, tb.lut, sh.nkeep, part0, sh.n2, scratch);
+  else if (in.kind == IN_INT16)
+    k_fwd_cols<N1, IN_INT16><<<gcol, 128, 0, st>>> (in, tb.lut, sh.nkeep, part0, sh.n2, scratch);
+  else
+    k_fwd_cols<N1, IN_FLOAT><<<gcol, 128, 0, st>>> (in, tb.lut, sh.nkeep, part0, sh.n2, scratch);
+  }
+  const dim3 grow (N1, nbatch, sh.nchan * sh.npol);
+  {
+  ClockScope cs (clk, KK_ROWS, st);
+  if (sh.n2 == 8192)
+    launch_rows<8192> (grow, scratch, tb, N1, sh, st);
+  else if (sh.n2 == 4096)
+    launch_rows<4096> (grow, scratch, tb, N1, sh, st);
+  else
+    return cudaErrorInvalidValue;
+  }
+  ClockScope cs (clk, KK_INV_COLS, st);
+  if (sh.npol == 2)
+  {
+    if (mode == OUT_VOLTAGE) launch_inv<N1, 2, OUT_VOLTAGE, 1> (sh, gcol, scratch, part0, fv, vv, st);
+    else if (fv.nout == 1) launch_inv<N1, 2, OUT_FOLD, 1> (sh, gcol, scratch, part0, fv, vv, st);
+    else if (fv.nout == 2) launch_inv<N1, 2, OUT_FOLD, 2> (sh, gcol, scratch, part0, fv, vv, st);
+    else launch_inv<N1, 2, OUT_FOLD, 4> (sh, gcol, scratch, part0, fv, vv, st);
+  }
+  else
+  {
+    if (mode == OUT_VOLTAGE) launch_inv<N1, 1, OUT_VOLTAGE, 1> (sh, gcol, scratch, part0, fv, vv, st);
+    else launch_inv<N1, 1, OUT_FOLD, 1> (sh, gcol, scratch, part0, fv, vv, st);
+  }
+  return cudaGetLastError ();
+}
+
+template <int N, int KIND, int MODE, int NOUT>
+cudaError_t run_fused_t (const ConvShape& sh, const ConvTables& tb, const InputView& in,
+                         uint64_t part0, unsigned nbatch, const FoldView& fv,
+                         const VoltView& vv, cudaStream_t st, const KernelClock* clk)
+{
+  constexpr int T = stockham_threads (N);
+  const size_t smem = size_t (in.npol) * spad_size (N) * sizeof (float2);
+  auto kern = k_fused<N, T, KIND, MODE, NOUT>;
+  cudaError_t err = cudaFuncSetAttribute (kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          int (smem));
+  if (err != cudaSuccess) return err;
+  ClockScope cs (clk, KK_FUSED, st);
+  kern<<<dim3 (nbatch, sh.nchan), T, smem, st>>> (in, tb.lut, tb.tw2, tb.H, sh.nkeep,
+                                                  sh.nfilt_pos, part0, fv, vv);
+  return cudaGetLastError ();
+}
+
+template <int N, int KIND>
+cudaError_t run_fused_k (const ConvShape& sh, const ConvTables& tb, const InputView& in,
+                         uint64_t part0, unsigned nbatch, int mode, const FoldView& fv,
+                         const VoltView& vv, cudaStream_t st, const KernelClock* clk)
+{
+  if (mode == OUT_VOLTAGE)
+    return run_fused_t<N, KIND, OUT_VOLTAGE, 1> (sh, tb, in, part0, nbatch, fv, vv, st, clk);
+  if (fv.nout == 1)
+    return run_fused_t<N, KIND, OUT_FOLD, 1> (sh, tb, in, part0, nbatch, fv, vv, st, clk);
+  if (fv.nout == 2)
+    return run_fused_t<N, KIND, OUT_FOLD, 2> (sh, tb, in, part0, nbatch, fv, vv, st, clk);
+  return run_fused_t<N, KIND, OUT_FOLD, 4> (sh, tb, in, part0, nbatch, fv, vv, st, clk);
+}
+
+template <int N>
+cudaError_t run_fused (const ConvShape& sh, const ConvTables& tb, const InputView& in,
+                       uint64_t part0, unsigned nbatch, int mode, const FoldView& fv,
+                       const VoltView& vv, cudaStream_t st, const KernelClock* clk)
+{
+  if (in.kind == IN_INT8)
+    return run_fused_k<N, IN_INT8> (sh, tb, in, part0, nbatch, mode, fv, vv, st, clk);
+  if (in.kind == IN_INT16)
+    return run_fused_k<N, IN_INT16> (sh, tb, in, part0, nbatch, mode, fv, vv, st, clk);
+  return run_fused_k<N, IN_FLOAT> (sh, tb, in, part0, nbatch, mode, fv, vv, st, clk);
+}
+
+template <int N2>
+cudaError_t set_rows_smem ()
+{
+  const int smem = spad_size (N2) * sizeof (float2);
+  return cudaFuncSetAttribute (k_rows<N2, stockham_threads (N2)>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
+
+} // namespace
+
+uint64_t kernel_launches () { return g_launches.load (); }
+
+cudaError_t launch_convolution (const ConvShape& sh, const ConvTables& tb, const InputView& in,
+                                uint64_t part0, unsigned nbatch, float2* scratch, int mode,
+                                const FoldView& fv, const VoltView& vv, cudaStream_t st,
+                                const KernelClock* clk)
+{
+  if (nbatch == 0) return cudaSuccess;
+  if (sh.n1 == 1)
+  {
+    switch (sh.nfft)
+    {
+      case 4096: return run_fused<4096> (sh, tb, in, part0, nbatch, mode, fv, vv, st, clk);
+      case 8192: return run_fused<8192> (sh, tb, in, part0, nbatch, mode, fv, vv, st, clk);
+      default: return cudaErrorInvalidValue;
+    }
+  }
+  static bool attr_done = false;
+  if (!attr_done)
+  {
+    cudaError_t e = set_rows_smem<8192> ();
+    if (e == cudaSuccess) e = set_rows_smem<4096> ();
+    if (e != cudaSuccess) return e;
+    attr_done = true;
+  }
+  switch (sh.n1)
+  {
+    case 2: return run_fourstep_n1<2> (sh, tb, in, part0, nbatch, scratch, mode, fv, vv, st, clk);
+    case 4: return run_fourstep_n1<4> (sh, tb, in, part0, nbatch, scratch, mode, fv, vv, st, clk);
+    case 8: return run_fourstep_n1<8> (sh, tb, in, part0, nbatch, scratch, mode, fv, vv, st, clk);
+    case 16: return run_fourstep_n1<16> (sh, tb, in, part0, nbatch, scratch, mode, fv, vv, st, clk);
+    case 32: return run_fourstep_n1<32> (sh, tb, in, part0, nbatch, scratch, mode, fv, vv, st, clk);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_build_chirp (float2* H, const double* d_chan_freq, const double* d_coeff,
+                                unsigned nchan, unsigned nfft, unsigned n1, unsigned n2,
+                                double binwidth, double half_chanwidth, int swap_halves,
+                                int chirp_mode, float scale, cudaStream_t st)
+{
+  const dim3 grid ((nfft + 255) / 256, nchan);
+  g_launches++;
+  k_build_chirp<<<grid, 256, 0, st>>> (H, d_chan_freq, d_coeff, nfft, n1, n2, binwidth,
+                                        half_chanwidth, swap_halves, chirp_mode, scale);
+  return cudaGetLastError ();
+}
+
+cudaError_t launch_permute_response (float2* H, const float2* src, unsigned nchan, unsigned n1,
+                                     unsigned n2, cudaStream_t st)
+{
+  const uint64_t N = uint64_t (n1) * n2;
+  g_launches++;
+  k_permute<<<dim3 (unsigned ((N + 255) / 256), nchan), 256, 0, st>>> (H, src, n1, n2, 0);
+  return cudaGetLastError ();
+}
+
+cudaError_t launch_unpermute_response (float2* dst, const float2* H, unsigned nchan, unsigned n1,
+                                       unsigned n2, cudaStream_t st)
+{
+  const uint64_t N = uint64_t (n1) * n2;
+  g_launches++;
+  k_permute<<<dim3 (unsigned ((N + 255) / 256), nchan), 256, 0, st>>> (dst, H, n1, n2, 1);
+  return cudaGetLastError ();
+}
+
+cudaError_t launch_unpack8 (const uint8_t* in, uint64_t ndat, unsigned nchan, unsigned npol,
+                            unsigned ndim, const float* d_lut, float* out, uint64_t span,
+                            cudaStream_t st)
+{
+  if (ndat == 0) return cudaSuccess;
+  g_launches++;
+  k_unpack8<<<dim3 (unsigned ((ndat + 255) / 256), nchan), 256, 0, st>>> (
+      in, ndat, nchan, npol, ndim, d_lut, out, span);
+  return cudaGetLastError ();
+}
+
+cudaError_t launch_unpack16 (const int16_t* in, uint64_t ndat, unsigned nchan, unsigned npol,
+                             unsigned ndim, int offset_binary, float* out, uint64_t span,
+                             cudaStream_t st)
+{
+  if (ndat == 0) return cudaSuccess;
+  g_launches++;
+  k_unpack16<<<dim3 (unsigned ((ndat + 255) / 256), nchan), 256, 0, st>>> (
+      in, ndat, nchan, npol, ndim, offset_binary, out, span);
+  return cudaGetLastError ();
+}
+
+cudaError_t launch_detect (const float2* in, uint64_t in_span, uint64_t ndat, unsigned nchan,
+                           int state, float* out, uint64_t out_span, cudaStream_t st)
+{
+  if (ndat == 0) return cudaSuccess;
+  g_launches++;
+  k_detect<<<dim3 (unsigned ((ndat + 255) / 256), nchan), 256, 0, st>>> (in, in_span, ndat,
+                                                                          state, out, out_span);
+  return cudaGetLastError ();
+}
+
+cudaError_t launch_fold (const float* in, uint64_t in_span, uint64_t ndat, unsigned nchan,
+                         unsigned npol, const FoldView& fv, cudaStream_t st)
+{
+  if (ndat == 0) return cudaSuccess;
+  g_launches++;
+  k_fold<<<dim3 (unsigned ((ndat + 255) / 256), nchan), 256, 0, st>>> (in, in_span, ndat, npol,
+                                                                        fv);
+  return cudaGetLastError ();
+}
+
+cudaError_t launch_binplan (const FoldSegment* segs, int nseg, uint64_t ndat, unsigned nbin,
+                            uint32_t* out, cudaStream_t st)
+{
+  if (ndat == 0) return cudaSuccess;
+  g_launches++;
+  k_binplan<<<unsigned ((ndat + 255) / 256), 256, 0, st>>> (segs, nseg, ndat, nbin, out);
+  return cudaGetLastError ();
+}
+
+} // namespace b200

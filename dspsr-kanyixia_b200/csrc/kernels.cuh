@@ -1,0 +1,116 @@
+// kernels.cuh -- launch interface of the B200 hot-path kernels
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "host_rules.h"
+
+namespace b200 {
+
+enum InputKind { IN_INT8 = 0, IN_INT16 = 1, IN_FLOAT = 2 };
+enum OutMode { OUT_VOLTAGE = 0, OUT_FOLD = 1 };
+
+// Where complex sample t of (chan, pol) lives: a carried prefix of npre
+// samples followed by the main block, both in the same layout.
+struct InputView
+{
+  int kind;
+  const void* pre;
+  const void* main;
+  uint64_t npre;
+  uint64_t pre_span;     // FPT span (complex samples) of the prefix
+  uint64_t main_span;    // FPT span of the main block
+  unsigned nchan, npol;
+  int offset_binary;     // int16 encoding
+};
+
+// Fold / detection epilogue
+struct FoldView
+{
+  const FoldSegment* segs;
+  int nseg;
+  float* profiles;       // [chan][nout][nbin]
+  unsigned* hits;        // [nbin]
+  unsigned nbin;
+  int state;
+  int nout;
+};
+
+// Voltage epilogue (Convolution::Engine::perform output)
+struct VoltView
+{
+  float2* out;
+  uint64_t span;
+};
+
+// Overlap-save plan of one FFT shape
+struct ConvShape
+{
+  unsigned nchan, npol;
+  unsigned nfft, n1, n2;     // nfft = n1 * n2; n1 == 1 -> single-kernel path
+  unsigned nfilt_pos, nfilt_neg;
+  uint64_t nkeep;            // nfft - nfilt_pos - nfilt_neg
+};
+
+struct ConvTables
+{
+  const float2* tw2;         // n2-point table exp(-2 pi i m / n2)
+  const float2* tw4;         // [n1][n2] exp(-2 pi i k1 n2 / nfft), null when n1 == 1
+  const float2* H;           // [nchan][n1][n2] response in four-step order
+  const float* lut;          // 8-bit lookup table (device), 256 floats
+};
+
+// Kernels of the convolution path, for per-kernel timing.
+enum KernelKind { KK_FWD_COLS = 0, KK_ROWS = 1, KK_INV_COLS = 2, KK_FUSED = 3, KK_COUNT = 4 };
+
+// Optional per-kernel clock: mark(self, kind, 0|1, stream) is called right
+// before (0) and after (1) each kernel launch of the convolution path.
+struct KernelClock
+{
+  void (*mark) (void* self, int kind, int phase, cudaStream_t stream);
+  void* self;
+};
+
+// Number of kernels this library has launched since it was loaded.
+uint64_t kernel_launches ();
+
+// Runs parts [part0, part0 + nbatch) of one block.  scratch holds
+// nbatch*nchan*npol*nfft complex values (unused when n1 == 1).
+cudaError_t launch_convolution (const ConvShape& shape, const ConvTables& tables,
+                                const InputView& in, uint64_t part0, unsigned nbatch,
+                                float2* scratch, int mode, const FoldView& fold,
+                                const VoltView& volt, cudaStream_t stream,
+                                const KernelClock* clock = nullptr);
+
+// Builds the dispersion response directly in four-step order on the device.
+// chan_freq/coeff per response channel computed on the host in double.
+cudaError_t launch_build_chirp (float2* H, const double* d_chan_freq,
+                                const double* d_coeff, unsigned nchan, unsigned nfft,
+                                unsigned n1, unsigned n2, double binwidth,
+                                double half_chanwidth, int swap_halves, int chirp_mode,
+                                float scale, cudaStream_t stream);
+// Reorders an FFT-order response [nchan][nfft] into four-step order.
+cudaError_t launch_permute_response (float2* H, const float2* src, unsigned nchan,
+                                     unsigned n1, unsigned n2, cudaStream_t stream);
+// Inverse of launch_permute_response.
+cudaError_t launch_unpermute_response (float2* dst, const float2* H, unsigned nchan,
+                                       unsigned n1, unsigned n2, cudaStream_t stream);
+
+cudaError_t launch_unpack8 (const uint8_t* in, uint64_t ndat, unsigned nchan, unsigned npol,
+                            unsigned ndim, const float* d_lut, float* out, uint64_t span,
+                            cudaStream_t stream);
+cudaError_t launch_unpack16 (const int16_t* in, uint64_t ndat, unsigned nchan, unsigned npol,
+                             unsigned ndim, int offset_binary, float* out, uint64_t span,
+                             cudaStream_t stream);
+cudaError_t launch_detect (const float2* in, uint64_t in_span, uint64_t ndat, unsigned nchan,
+                           int state, float* out, uint64_t out_span, cudaStream_t stream);
+cudaError_t launch_fold (const float* in, uint64_t in_span, uint64_t ndat, unsigned nchan,
+                         unsigned npol, const FoldView& fold, cudaStream_t stream);
+cudaError_t launch_binplan (const FoldSegment* segs, int nseg, uint64_t ndat, unsigned nbin,
+                            uint32_t* out, cudaStream_t stream);
+
+// number of detected output polarisations for a detection state
+__host__ __device__ inline int detect_nout (int state) { return state == 0 ? 1 : state == 1 ? 2 : 4; }
+
+} // namespace b200

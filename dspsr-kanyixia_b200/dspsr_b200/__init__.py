@@ -1,0 +1,359 @@
+"""Host-side interface to the B200 engine of DSPSR's baseband hot path.
+
+This module mirrors the reference's operation / engine interfaces over the
+C ABI of libdspsr_b200.so (include/dspsr_b200.h):
+
+  Unpacker           -> unpack8 / unpack16      (GenericEightBitUnpacker, SixteenBitUnpacker)
+  Convolution engine -> Convolution             (CUDA::ConvolutionEngine)
+  Detection engine   -> detect                  (CUDA::DetectionEngine)
+  Fold engine        -> Fold                    (CUDA::FoldEngine with use_set_bins)
+  SingleThread loop  -> Pipeline                (unpack -> convolve -> detect -> fold)
+
+Device buffers are torch CUDA tensors (torch is only the allocator and stream
+provider here); every computation runs in the library's sm_100a kernels.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _capi
+from ._capi import (B200Error, PipelineConfig, INTENSITY, PPQQ, COHERENCE, STOKES, INT8_TFPD,
+                    INT16_TFPD, FLOAT_FPT, CHIRP_REFERENCE, CHIRP_FP64)
+
+__all__ = ["Context", "Convolution", "Fold", "Pipeline", "PipelineConfig", "B200Error",
+           "smearing_samples", "minimum_ndat", "optimal_fft_length", "bittable8", "fold_phi",
+           "fold_plan_count", "INTENSITY", "PPQQ", "COHERENCE", "STOKES", "INT8_TFPD",
+           "INT16_TFPD", "FLOAT_FPT", "CHIRP_REFERENCE", "CHIRP_FP64", "NOUT"]
+
+NOUT = {INTENSITY: 1, PPQQ: 2, COHERENCE: 4, STOKES: 4}
+# Jenet & Anderson (1998) optimal uniform-quantiser input spacing for 8 bits
+JA98_SPACING_8BIT = 0.0308
+
+
+def _ptr(x):
+    """Device pointer of a torch tensor (or an int address)."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    return x.data_ptr()
+
+
+def _fptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+# ---- host rules ---------------------------------------------------------------
+
+def smearing_samples(centre_freq, bandwidth, dm, nchan, half):
+    return _capi.lib().dspsr_b200_smearing_samples(centre_freq, bandwidth, dm, nchan, half)
+
+
+def minimum_ndat(impulse_pos, impulse_neg):
+    return _capi.lib().dspsr_b200_minimum_ndat(impulse_pos, impulse_neg)
+
+
+def optimal_fft_length(nbad, nfft_max=0, factor=1):
+    return _capi.lib().dspsr_b200_optimal_fft_length(nbad, nfft_max, factor)
+
+
+def bittable8(spacing=JA98_SPACING_8BIT, twos_complement=True):
+    lut = np.empty(256, np.float32)
+    scale = ctypes.c_double()
+    rc = _capi.lib().dspsr_b200_bittable8(spacing, int(twos_complement), _fptr(lut),
+                                          ctypes.byref(scale))
+    if rc:
+        raise B200Error(rc, "bittable8: invalid spacing")
+    return lut, scale.value
+
+
+def fold_phi(start_mjd, epoch_mjd, idat_start, rate, period, reference_phase=0.0):
+    return _capi.lib().dspsr_b200_fold_phi(start_mjd[0], start_mjd[1], start_mjd[2],
+                                           epoch_mjd[0], epoch_mjd[1], epoch_mjd[2], idat_start,
+                                           rate, period, reference_phase)
+
+
+def kernel_launches():
+    """Kernels the library has launched since it was loaded."""
+    return _capi.lib().dspsr_b200_kernel_launches()
+
+
+def fold_plan_count(phi, phase_per_sample, ndat):
+    return _capi.lib().dspsr_b200_fold_plan_count(phi, phase_per_sample, ndat)
+
+
+# ---- context ----------------------------------------------------------------------
+
+class Context:
+    """A device and a stream (CUDA::DeviceMemory(stream) in the reference)."""
+
+    def __init__(self, device=0, stream=None):
+        self._lib = _capi.lib()
+        h = ctypes.c_void_p()
+        rc = self._lib.dspsr_b200_context_create(device, stream, ctypes.byref(h))
+        if rc:
+            raise B200Error(rc, f"context_create(device={device}) failed")
+        self.handle = h
+
+    def check(self, rc, what=""):
+        if rc:
+            msg = self._lib.dspsr_b200_last_error(self.handle)
+            raise B200Error(rc, f"{what}: {msg.decode() if msg else ''}")
+
+    def set_stream(self, stream):
+        self.check(self._lib.dspsr_b200_context_set_stream(self.handle, stream), "set_stream")
+
+    def synchronize(self):
+        self.check(self._lib.dspsr_b200_synchronize(self.handle), "synchronize")
+
+    def close(self):
+        if self.handle:
+            self._lib.dspsr_b200_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- Unpacker ---------------------------------------------------------------
+    def unpack8(self, d_in, ndat, nchan, npol, ndim, lut, d_out, out_span):
+        lut = np.ascontiguousarray(lut, np.float32)
+        self.check(self._lib.dspsr_b200_unpack8(self.handle, _ptr(d_in), ndat, nchan, npol, ndim,
+                                                _fptr(lut), _ptr(d_out), out_span), "unpack8")
+
+    def unpack16(self, d_in, ndat, nchan, npol, ndim, d_out, out_span, offset_binary=False):
+        self.check(self._lib.dspsr_b200_unpack16(self.handle, _ptr(d_in), ndat, nchan, npol, ndim,
+                                                 int(offset_binary), _ptr(d_out), out_span),
+                   "unpack16")
+
+    # ---- Detection engine ----------------------------------------------------------
+    def detect(self, d_in, in_span, ndat, nchan, state, d_out, out_span):
+        self.check(self._lib.dspsr_b200_detect(self.handle, _ptr(d_in), in_span, ndat, nchan,
+                                               state, _ptr(d_out), out_span), "detect")
+
+
+class Convolution:
+    """Convolution::Engine: overlap-save FFT convolution on complex FPT data."""
+
+    def __init__(self, ctx, nchan, npol, nfft, nfilt_pos, nfilt_neg):
+        self.ctx = ctx
+        self._lib = ctx._lib
+        h = ctypes.c_void_p()
+        ctx.check(self._lib.dspsr_b200_convolution_create(ctx.handle, nchan, npol, nfft,
+                                                          nfilt_pos, nfilt_neg, ctypes.byref(h)),
+                  "convolution_create")
+        self.handle = h
+        self.nchan, self.npol, self.nfft = nchan, npol, nfft
+        self.nfilt_pos, self.nfilt_neg = nfilt_pos, nfilt_neg
+        self.nkeep = nfft - nfilt_pos - nfilt_neg
+
+    def copy_response(self, response):
+        r = np.ascontiguousarray(response, np.complex64)
+        assert r.size == self.nchan * self.nfft
+        self.ctx.check(self._lib.dspsr_b200_convolution_copy_response(
+            self.handle, _fptr(r.view(np.float32))), "copy_response")
+
+    def set_dedispersion(self, centre_freq, bandwidth, dm, input_nchan=None, dual_sideband=1,
+                         dc_centred=0, chirp_mode=CHIRP_REFERENCE, norm_nfft=None):
+        self.ctx.check(self._lib.dspsr_b200_convolution_set_dedispersion(
+            self.handle, centre_freq, bandwidth, dm,
+            self.nchan if input_nchan is None else input_nchan, dual_sideband, dc_centred,
+            chirp_mode, norm_nfft or self.nfft), "set_dedispersion")
+
+    def get_response(self):
+        out = np.empty(self.nchan * self.nfft, np.complex64)
+        self.ctx.check(self._lib.dspsr_b200_convolution_get_response(
+            self.handle, _fptr(out.view(np.float32))), "get_response")
+        return out.reshape(self.nchan, self.nfft)
+
+    def npart(self, ndat):
+        if ndat < self.nfft:
+            return 0
+        return (ndat - self.nfilt_pos - self.nfilt_neg) // self.nkeep
+
+    def perform(self, d_in, in_span, ndat, d_out, out_span):
+        n = ctypes.c_uint64()
+        self.ctx.check(self._lib.dspsr_b200_convolution_perform(
+            self.handle, _ptr(d_in), in_span, ndat, _ptr(d_out), out_span, ctypes.byref(n)),
+            "convolution_perform")
+        return n.value
+
+    def close(self):
+        if self.handle:
+            self._lib.dspsr_b200_convolution_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Fold:
+    """Fold::Engine with use_set_bins: exact bin plan on the host, fold on the GPU."""
+
+    def __init__(self, ctx, nbin, nchan, npol):
+        self.ctx = ctx
+        self._lib = ctx._lib
+        h = ctypes.c_void_p()
+        ctx.check(self._lib.dspsr_b200_fold_create(ctx.handle, nbin, nchan, npol, ctypes.byref(h)),
+                  "fold_create")
+        self.handle = h
+        self.nbin, self.nchan, self.npol = nbin, nchan, npol
+
+    def set_bins(self, phi, phase_per_sample, ndat, idat_start=0):
+        n = ctypes.c_uint64()
+        self.ctx.check(self._lib.dspsr_b200_fold_set_bins(self.handle, phi, phase_per_sample, ndat,
+                                                          idat_start, ctypes.byref(n)), "set_bins")
+        return n.value
+
+    def fold(self, d_in, in_span):
+        self.ctx.check(self._lib.dspsr_b200_fold_fold(self.handle, _ptr(d_in), in_span), "fold")
+
+    def binplan(self, d_out):
+        self.ctx.check(self._lib.dspsr_b200_fold_binplan(self.handle, _ptr(d_out)), "binplan")
+
+    def get_profiles(self):
+        prof = np.empty((self.nchan, self.npol, self.nbin), np.float32)
+        hits = np.empty(self.nbin, np.uint32)
+        self.ctx.check(self._lib.dspsr_b200_fold_get_profiles(
+            self.handle, _fptr(prof), hits.ctypes.data_as(_capi.c_u32p)), "get_profiles")
+        return prof, hits
+
+    def reset(self):
+        self.ctx.check(self._lib.dspsr_b200_fold_reset(self.handle), "fold_reset")
+
+    def close(self):
+        if self.handle:
+            self._lib.dspsr_b200_fold_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Pipeline:
+    """The fused SingleThread hot loop: unpack -> convolve -> detect -> fold."""
+
+    def __init__(self, ctx, config):
+        self.ctx = ctx
+        self._lib = ctx._lib
+        self.config = config
+        h = ctypes.c_void_p()
+        ctx.check(self._lib.dspsr_b200_pipeline_create(ctx.handle, ctypes.byref(config),
+                                                       ctypes.byref(h)), "pipeline_create")
+        self.handle = h
+        self.nout = NOUT[config.state]
+
+    def run(self, d_in, ndat, in_span=0):
+        n = ctypes.c_uint64()
+        self.ctx.check(self._lib.dspsr_b200_pipeline_run(self.handle, _ptr(d_in), ndat, in_span,
+                                                         ctypes.byref(n)), "pipeline_run")
+        return n.value
+
+    def run_host(self, h_in, ndat):
+        """h_in: a numpy array (or pinned torch CPU tensor) holding the TFPD block."""
+        addr = h_in.ctypes.data if isinstance(h_in, np.ndarray) else h_in.data_ptr()
+        n = ctypes.c_uint64()
+        self.ctx.check(self._lib.dspsr_b200_pipeline_run_host(self.handle, addr, ndat,
+                                                              ctypes.byref(n)), "pipeline_run_host")
+        return n.value
+
+    def get_profiles(self):
+        c = self.config
+        prof = np.empty((c.nchan, self.nout, c.nbin), np.float32)
+        hits = np.empty(c.nbin, np.uint32)
+        self.ctx.check(self._lib.dspsr_b200_pipeline_get_profiles(
+            self.handle, _fptr(prof), hits.ctypes.data_as(_capi.c_u32p)), "get_profiles")
+        return prof, hits
+
+    def reset(self):
+        self.ctx.check(self._lib.dspsr_b200_pipeline_reset(self.handle), "pipeline_reset")
+
+    def profile(self, enable=True):
+        self.ctx.check(self._lib.dspsr_b200_pipeline_profile(self.handle, int(enable)),
+                       "pipeline_profile")
+
+    KERNELS = ("fwd_cols", "rows", "inv_cols_detect_fold", "fused")
+
+    def kernel_times(self):
+        """{kernel: (milliseconds, launches)} since the last call."""
+        ms = (ctypes.c_double * 4)()
+        n = (ctypes.c_uint64 * 4)()
+        self.ctx.check(self._lib.dspsr_b200_pipeline_kernel_times(self.handle, ms, n),
+                       "kernel_times")
+        return {k: (ms[i], n[i]) for i, k in enumerate(self.KERNELS)}
+
+    def info(self):
+        a = (ctypes.c_uint64 * 8)()
+        self.ctx.check(self._lib.dspsr_b200_pipeline_info(self.handle, a), "pipeline_info")
+        keys = ["nfft", "nkeep", "n1", "n2", "max_batch", "ncarry", "in0", "nseg"]
+        return dict(zip(keys, list(a)))
+
+    def close(self):
+        if self.handle:
+            self._lib.dspsr_b200_pipeline_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def make_config(centre_freq, bandwidth, dm, nchan, npol, nfft, nfilt_pos, nfilt_neg, nbin,
+                period, state=INTENSITY, input_kind=INT8_TFPD, lut=None, chirp_mode=CHIRP_REFERENCE,
+                start_mjd=(60000, 0, 0.0), epoch_mjd=(60000, 0, 0.0), reference_phase=0.0,
+                dual_sideband=1, offset_binary=0, scratch_bytes=0):
+    """Fill a PipelineConfig (the fields DedispersionPipe / LoadToFold set up)."""
+    cfg = PipelineConfig()
+    cfg.centre_freq_mhz = centre_freq
+    cfg.bandwidth_mhz = bandwidth
+    cfg.dm = dm
+    cfg.nchan = nchan
+    cfg.npol = npol
+    cfg.input_kind = input_kind
+    if lut is None:
+        lut, _ = bittable8()
+    for i in range(256):
+        cfg.lut[i] = float(lut[i])
+    cfg.offset_binary = offset_binary
+    cfg.dual_sideband = dual_sideband
+    cfg.dc_centred = 0
+    cfg.nfft = nfft
+    cfg.nfilt_pos = nfilt_pos
+    cfg.nfilt_neg = nfilt_neg
+    cfg.chirp_mode = chirp_mode
+    cfg.state = state
+    cfg.nbin = nbin
+    cfg.period_s = period
+    cfg.reference_phase = reference_phase
+    cfg.epoch_day, cfg.epoch_sec, cfg.epoch_frac = epoch_mjd
+    cfg.start_day, cfg.start_sec, cfg.start_frac = start_mjd
+    cfg.scratch_bytes = scratch_bytes
+    return cfg
+
+
+def dispersion_plan(centre_freq, bandwidth, dm, nchan, nfft=None):
+    """nfilt_pos, nfilt_neg and nfft as PlasmaResponse / Response choose them.
+
+    PlasmaResponse::prepare (PlasmaResponse.C:91-119): impulse_neg is the
+    smear of the lower half of the worst channel, impulse_pos of the upper half.
+    Without an explicit nfft the minimum legal length is used
+    (Response::get_minimum_ndat)."""
+    neg = smearing_samples(centre_freq, bandwidth, dm, nchan, -1)
+    pos = smearing_samples(centre_freq, bandwidth, dm, nchan, 1)
+    nmin = minimum_ndat(pos, neg)
+    if nfft is None:
+        nfft = nmin
+    if nfft < nmin:
+        # Response::check_ndat (Response.C:605-621)
+        raise B200Error(_capi.EINVAL, f"specified nfft={nfft} < required minimum ndat={nmin}")
+    return pos, neg, nfft

@@ -1,0 +1,133 @@
+"""ctypes declarations of libdspsr_b200.so (include/dspsr_b200.h).
+
+The library is built in-tree by dspsr-kanyixia_b200/Makefile into
+dspsr-kanyixia_b200/lib/.  Loading fails loudly when it is missing: there is
+no CPU fallback for any entry point.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+PKG_ROOT = os.path.dirname(_HERE)
+LIB_PATH = os.path.join(PKG_ROOT, "lib", "libdspsr_b200.so")
+HEADER_PATH = os.path.join(os.path.dirname(PKG_ROOT), "include", "dspsr_b200.h")
+
+OK, EINVAL, ESTATE, ECUDA, ENOMEM, ENODEV = 0, 1, 2, 3, 4, 5
+INTENSITY, PPQQ, COHERENCE, STOKES = 0, 1, 2, 3
+INT8_TFPD, INT16_TFPD, FLOAT_FPT = 0, 1, 2
+CHIRP_REFERENCE, CHIRP_FP64 = 0, 1
+
+c_vp = ctypes.c_void_p
+c_u64 = ctypes.c_uint64
+c_i64 = ctypes.c_int64
+c_uint = ctypes.c_uint
+c_int = ctypes.c_int
+c_dbl = ctypes.c_double
+c_fp = ctypes.POINTER(ctypes.c_float)
+c_u32p = ctypes.POINTER(ctypes.c_uint32)
+c_u64p = ctypes.POINTER(ctypes.c_uint64)
+
+
+class PipelineConfig(ctypes.Structure):
+    """dspsr_b200_pipeline_config"""
+    _fields_ = [
+        ("centre_freq_mhz", c_dbl),
+        ("bandwidth_mhz", c_dbl),
+        ("dm", c_dbl),
+        ("nchan", c_uint),
+        ("npol", c_uint),
+        ("input_kind", c_int),
+        ("lut", ctypes.c_float * 256),
+        ("offset_binary", c_int),
+        ("dual_sideband", c_int),
+        ("dc_centred", c_int),
+        ("nfft", c_uint),
+        ("nfilt_pos", c_uint),
+        ("nfilt_neg", c_uint),
+        ("chirp_mode", c_int),
+        ("state", c_int),
+        ("nbin", c_uint),
+        ("period_s", c_dbl),
+        ("reference_phase", c_dbl),
+        ("epoch_day", c_i64),
+        ("epoch_sec", c_i64),
+        ("epoch_frac", c_dbl),
+        ("start_day", c_i64),
+        ("start_sec", c_i64),
+        ("start_frac", c_dbl),
+        ("scratch_bytes", c_u64),
+    ]
+
+
+SIGNATURES = {
+    "dspsr_b200_version": (c_int, []),
+    "dspsr_b200_context_create": (c_int, [c_int, c_vp, ctypes.POINTER(c_vp)]),
+    "dspsr_b200_context_destroy": (c_int, [c_vp]),
+    "dspsr_b200_context_set_stream": (c_int, [c_vp, c_vp]),
+    "dspsr_b200_last_error": (ctypes.c_char_p, [c_vp]),
+    "dspsr_b200_synchronize": (c_int, [c_vp]),
+    "dspsr_b200_smearing_samples": (c_uint, [c_dbl, c_dbl, c_dbl, c_uint, c_int]),
+    "dspsr_b200_minimum_ndat": (c_uint, [c_uint, c_uint]),
+    "dspsr_b200_optimal_fft_length": (c_i64, [c_u64, c_u64, c_uint]),
+    "dspsr_b200_bittable8": (c_int, [c_dbl, c_int, c_fp, ctypes.POINTER(c_dbl)]),
+    "dspsr_b200_fold_phi": (c_dbl, [c_i64, c_i64, c_dbl, c_i64, c_i64, c_dbl, c_u64, c_dbl,
+                                    c_dbl, c_dbl]),
+    "dspsr_b200_fold_plan_count": (c_i64, [c_dbl, c_dbl, c_u64]),
+    "dspsr_b200_unpack8": (c_int, [c_vp, c_vp, c_u64, c_uint, c_uint, c_uint, c_fp, c_vp, c_u64]),
+    "dspsr_b200_unpack16": (c_int, [c_vp, c_vp, c_u64, c_uint, c_uint, c_uint, c_int, c_vp,
+                                    c_u64]),
+    "dspsr_b200_convolution_create": (c_int, [c_vp, c_uint, c_uint, c_uint, c_uint, c_uint,
+                                              ctypes.POINTER(c_vp)]),
+    "dspsr_b200_convolution_destroy": (c_int, [c_vp]),
+    "dspsr_b200_convolution_copy_response": (c_int, [c_vp, c_fp]),
+    "dspsr_b200_convolution_set_dedispersion": (c_int, [c_vp, c_dbl, c_dbl, c_dbl, c_int, c_int,
+                                                        c_int, c_int, c_uint]),
+    "dspsr_b200_convolution_get_response": (c_int, [c_vp, c_fp]),
+    "dspsr_b200_convolution_perform": (c_int, [c_vp, c_vp, c_u64, c_u64, c_vp, c_u64, c_u64p]),
+    "dspsr_b200_detect": (c_int, [c_vp, c_vp, c_u64, c_u64, c_uint, c_int, c_vp, c_u64]),
+    "dspsr_b200_fold_create": (c_int, [c_vp, c_uint, c_uint, c_uint, ctypes.POINTER(c_vp)]),
+    "dspsr_b200_fold_destroy": (c_int, [c_vp]),
+    "dspsr_b200_fold_set_bins": (c_int, [c_vp, c_dbl, c_dbl, c_u64, c_u64, c_u64p]),
+    "dspsr_b200_fold_fold": (c_int, [c_vp, c_vp, c_u64]),
+    "dspsr_b200_fold_binplan": (c_int, [c_vp, c_vp]),
+    "dspsr_b200_fold_get_profiles": (c_int, [c_vp, c_fp, c_u32p]),
+    "dspsr_b200_fold_reset": (c_int, [c_vp]),
+    "dspsr_b200_pipeline_create": (c_int, [c_vp, ctypes.POINTER(PipelineConfig),
+                                           ctypes.POINTER(c_vp)]),
+    "dspsr_b200_pipeline_destroy": (c_int, [c_vp]),
+    "dspsr_b200_pipeline_run": (c_int, [c_vp, c_vp, c_u64, c_u64, c_u64p]),
+    "dspsr_b200_pipeline_run_host": (c_int, [c_vp, c_vp, c_u64, c_u64p]),
+    "dspsr_b200_pipeline_get_profiles": (c_int, [c_vp, c_fp, c_u32p]),
+    "dspsr_b200_pipeline_reset": (c_int, [c_vp]),
+    "dspsr_b200_pipeline_info": (c_int, [c_vp, c_u64p]),
+    "dspsr_b200_pipeline_profile": (c_int, [c_vp, c_int]),
+    "dspsr_b200_pipeline_kernel_times": (c_int, [c_vp, ctypes.POINTER(c_dbl), c_u64p]),
+    "dspsr_b200_kernel_launches": (c_u64, []),
+}
+
+_lib = None
+
+
+class B200Error(RuntimeError):
+    """A non-zero status from the C ABI (the reference's Error)."""
+
+    def __init__(self, code, message):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+
+
+def lib():
+    """Load libdspsr_b200.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `make -C dspsr-kanyixia_b200` "
+                "(there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib

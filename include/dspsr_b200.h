@@ -1,0 +1,258 @@
+/*
+ * dspsr_b200.h -- C ABI of libdspsr_b200.so, the B200 (sm_100a) engine for
+ * DSPSR's baseband hot path: unpack -> overlap-save coherent dedispersion ->
+ * detection -> fold.
+ *
+ * Plain C types only: device pointers are untyped or float pointers, sizes
+ * are uint64_t, streams are passed as an untyped pointer (a cudaStream_t).  Every call returns an int
+ * status (DSPSR_B200_OK == 0); the message of the last failure on a context is
+ * returned by dspsr_b200_last_error().  No exception crosses this boundary.
+ *
+ * Each entry point names the reference interface it replaces (paths relative
+ * to the DSPSR source tree).  The reference's CUDA engines are
+ * CUDA::ConvolutionEngine, CUDA::DetectionEngine, CUDA::FoldEngine and the
+ * generic_8bit_unpack kernel; their host classes (dsp::Convolution,
+ * dsp::Detection, dsp::Fold, dsp::GenericEightBitUnpacker) keep all
+ * bookkeeping and hand the engine raw device pointers, strides and counts,
+ * which is exactly what these functions take.
+ */
+#ifndef DSPSR_B200_H
+#define DSPSR_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DSPSR_B200_OK        0
+#define DSPSR_B200_EINVAL    1   /* InvalidParam in the reference's Error codes */
+#define DSPSR_B200_ESTATE    2   /* InvalidState */
+#define DSPSR_B200_ECUDA     3   /* FailedCall (CUDA runtime) */
+#define DSPSR_B200_ENOMEM    4
+#define DSPSR_B200_ENODEV    5   /* no CUDA device: the library never falls back to the CPU */
+
+/* Signal::State values accepted by detection and the fused path
+   (Signal/General/Detection.C:225-630) */
+#define DSPSR_B200_INTENSITY 0   /* PP+QQ, one output polarisation */
+#define DSPSR_B200_PPQQ      1   /* PP, QQ */
+#define DSPSR_B200_COHERENCE 2   /* PP, QQ, Re[p*q], Im[p*q] (cross_detect.ic:38-41) */
+#define DSPSR_B200_STOKES    3   /* I, Q, U, V (stokes_detect.ic:40-43) */
+
+/* input sample encodings */
+#define DSPSR_B200_INT8_TFPD   0 /* 8-bit two's complement, BitTable lookup */
+#define DSPSR_B200_INT16_TFPD  1 /* 16-bit, float(x)+0.5 (SixteenBitUnpacker.C:54-79) */
+#define DSPSR_B200_FLOAT_FPT   2 /* complex float, one span per (chan, pol) */
+
+/* dispersion response evaluation */
+#define DSPSR_B200_CHIRP_REFERENCE 0 /* phase rounded to float before sin/cos,
+                                        as Dedispersion.C:104-111 does */
+#define DSPSR_B200_CHIRP_FP64      1 /* phase reduced mod 2pi in FP64, then
+                                        rounded once to float */
+
+typedef struct dspsr_b200_context dspsr_b200_context;
+typedef struct dspsr_b200_convolution dspsr_b200_convolution;
+typedef struct dspsr_b200_fold dspsr_b200_fold;
+typedef struct dspsr_b200_pipeline dspsr_b200_pipeline;
+
+/* ---------------------------------------------------------------------- */
+/* Library and context                                                     */
+/* ---------------------------------------------------------------------- */
+
+/* library version, major*10000 + minor*100 + patch */
+int dspsr_b200_version (void);
+
+/* Replaces the CUDA::DeviceMemory(stream) + engine construction done in
+   SingleThread::construct (Signal/General/SingleThread.C:294-344): binds a
+   device and a stream (NULL = legacy default stream). */
+int dspsr_b200_context_create (int device, void* stream, dspsr_b200_context** ctx);
+int dspsr_b200_context_destroy (dspsr_b200_context* ctx);
+int dspsr_b200_context_set_stream (dspsr_b200_context* ctx, void* stream);
+const char* dspsr_b200_last_error (const dspsr_b200_context* ctx);
+/* blocks until all work queued on the context's stream is done */
+int dspsr_b200_synchronize (dspsr_b200_context* ctx);
+
+/* ---------------------------------------------------------------------- */
+/* Host-side rules (no GPU needed)                                         */
+/* ---------------------------------------------------------------------- */
+
+/* PlasmaResponse::smearing_samples (Signal/General/PlasmaResponse.C:210-250);
+   half = -1, 0, +1 */
+unsigned dspsr_b200_smearing_samples (double centre_freq_mhz, double bandwidth_mhz,
+                                      double dm, unsigned nchan, int half);
+/* Response::get_minimum_ndat (Signal/General/Response.C:529-545) */
+unsigned dspsr_b200_minimum_ndat (unsigned impulse_pos, unsigned impulse_neg);
+/* optimal_fft_length (Signal/General/optimize_fft.c:64-135) */
+int64_t dspsr_b200_optimal_fft_length (uint64_t nbadperfft, uint64_t nfft_max,
+                                       unsigned factor);
+/* BitTable::generate for nbit = 8 (Kernel/Classes/BitTable.C:104-225);
+   spacing = the JenetAnderson98 optimal input spacing for 8 bits */
+int dspsr_b200_bittable8 (double spacing, int twos_complement, float* lut256,
+                          double* scale);
+/* Fold::get_phi for a constant folding period (Signal/Pulsar/Fold.C:685-693,
+   975-979); MJDs are (day, second, fraction of a second) */
+double dspsr_b200_fold_phi (int64_t start_day, int64_t start_sec, double start_frac,
+                            int64_t epoch_day, int64_t epoch_sec, double epoch_frac,
+                            uint64_t idat_start, double rate, double period,
+                            double reference_phase);
+/* Number of arithmetic segments the exact fold-bin plan needs for a block
+   (see dspsr_b200_fold_set_bins); lets a caller size buffers. */
+int64_t dspsr_b200_fold_plan_count (double phi, double phase_per_sample,
+                                    uint64_t ndat);
+
+/* ---------------------------------------------------------------------- */
+/* Unpacker (GenericEightBitUnpacker::unpack_on_gpu,                       */
+/* Kernel/Classes/GenericEightBitUnpacker.C:92-131, and generic_8bit_unpack,*/
+/* Kernel/Classes/GenericEightBitUnpackerCUDA.cu:47-100)                    */
+/* ---------------------------------------------------------------------- */
+
+/* TFPD bytes (ndim values per (t, chan, pol)) -> FPT floats:
+   out[(ichan*npol + ipol)*out_span + idat*ndim + idim] = lut256[byte] */
+int dspsr_b200_unpack8 (dspsr_b200_context* ctx, const void* d_in, uint64_t ndat,
+                        unsigned nchan, unsigned npol, unsigned ndim,
+                        const float* lut256, float* d_out, uint64_t out_span);
+/* SixteenBitUnpacker::unpack (Kernel/Classes/SixteenBitUnpacker.C:23-79) */
+int dspsr_b200_unpack16 (dspsr_b200_context* ctx, const void* d_in, uint64_t ndat,
+                         unsigned nchan, unsigned npol, unsigned ndim,
+                         int offset_binary, float* d_out, uint64_t out_span);
+
+/* ---------------------------------------------------------------------- */
+/* Convolution::Engine (CUDA::ConvolutionEngine,                            */
+/* Signal/General/ConvolutionCUDA.cu:174-774; callers Convolution.C:446-452,*/
+/* 656-667, 690-698)                                                        */
+/* ---------------------------------------------------------------------- */
+
+/* Engine::prepare(Convolution*): sizes from Convolution::prepare
+   (Convolution.C:316-465).  nfft must be a power of two in [4096, 262144]. */
+int dspsr_b200_convolution_create (dspsr_b200_context* ctx, unsigned nchan,
+                                   unsigned npol, unsigned nfft, unsigned nfilt_pos,
+                                   unsigned nfilt_neg, dspsr_b200_convolution** conv);
+int dspsr_b200_convolution_destroy (dspsr_b200_convolution* conv);
+/* Engine::copy_response(const Response*): nchan*nfft complex floats
+   (interleaved re,im) in FFT order, normaliser already applied; host memory. */
+int dspsr_b200_convolution_copy_response (dspsr_b200_convolution* conv,
+                                          const float* response);
+/* Builds the Dedispersion response on the GPU in FP64 (Dedispersion.C:84-186
+   with the PlasmaResponse::build grid, Response::swap_as_needed
+   Response.C:325-400 and the 1/sqrt(norm_nfft) normaliser of
+   Convolution::prepare_normalizer Convolution.C:300-313,401-414). */
+int dspsr_b200_convolution_set_dedispersion (dspsr_b200_convolution* conv,
+                                             double centre_freq_mhz, double bandwidth_mhz,
+                                             double dm, int input_nchan, int dual_sideband,
+                                             int dc_centred, int chirp_mode,
+                                             unsigned norm_nfft);
+/* copies the response (FFT order) back to host memory, nchan*nfft complex */
+int dspsr_b200_convolution_get_response (dspsr_b200_convolution* conv, float* response);
+/* Engine::perform(input, output, npart): complex FPT in (span in complex
+   samples per (chan, pol)), complex FPT out; returns npart
+   = (ndat - nfilt_pos - nfilt_neg)/(nfft - nfilt_pos - nfilt_neg). */
+int dspsr_b200_convolution_perform (dspsr_b200_convolution* conv, const float* d_in,
+                                    uint64_t in_span, uint64_t ndat, float* d_out,
+                                    uint64_t out_span, uint64_t* npart);
+
+/* ---------------------------------------------------------------------- */
+/* Detection::Engine (CUDA::DetectionEngine, Signal/General/DetectionCUDA.cu;*/
+/* callers Detection.C:237-242, 483-489)                                    */
+/* ---------------------------------------------------------------------- */
+
+/* square_law / polarimetry on dual-pol complex FPT input; output FPT floats,
+   (ichan*nout + k)*out_span, nout = 1, 2, 4, 4 for the four states. */
+int dspsr_b200_detect (dspsr_b200_context* ctx, const float* d_in, uint64_t in_span,
+                       uint64_t ndat, unsigned nchan, int state, float* d_out,
+                       uint64_t out_span);
+
+/* ---------------------------------------------------------------------- */
+/* Fold::Engine (CUDA::FoldEngine, Signal/Pulsar/FoldCUDA.cu:78-704;        */
+/* callers Fold.C:760-887, 1011-1035)                                       */
+/* ---------------------------------------------------------------------- */
+
+int dspsr_b200_fold_create (dspsr_b200_context* ctx, unsigned nbin, unsigned nchan,
+                            unsigned npol, dspsr_b200_fold** fold);
+int dspsr_b200_fold_destroy (dspsr_b200_fold* fold);
+/* Engine::set_bins(phi, phase_per_sample, ndat, idat_start) with
+   use_set_bins = true (Fold.C:763-778): builds the bin plan of the sequential
+   FP64 recurrence of Fold.C:815-818 exactly, as arithmetic segments, on the
+   host in O(segments), and uploads it.  Returns ndat_folded. */
+int dspsr_b200_fold_set_bins (dspsr_b200_fold* fold, double phi, double phase_per_sample,
+                              uint64_t ndat, uint64_t idat_start, uint64_t* ndat_folded);
+/* Engine::fold(): accumulate float FPT input (ndim 1) into the profiles */
+int dspsr_b200_fold_fold (dspsr_b200_fold* fold, const float* d_in, uint64_t in_span);
+/* writes the per-sample bin indices of the current plan (for parity checks) */
+int dspsr_b200_fold_binplan (dspsr_b200_fold* fold, uint32_t* d_binplan);
+/* Engine::synch(PhaseSeries*): profiles [chan][pol][bin] floats and hits[bin]
+   into host memory */
+int dspsr_b200_fold_get_profiles (dspsr_b200_fold* fold, float* profiles, uint32_t* hits);
+int dspsr_b200_fold_reset (dspsr_b200_fold* fold);
+
+/* ---------------------------------------------------------------------- */
+/* Fused path: the SingleThread::run hot loop (SingleThread.C:687-736) over  */
+/* Unpacker -> Convolution -> Detection -> Fold for one block, with the     */
+/* InputBuffering overlap carry (InputBuffering.C:66-174), in one pass      */
+/* through HBM per FFT.                                                      */
+/* ---------------------------------------------------------------------- */
+
+typedef struct
+{
+  /* observation */
+  double centre_freq_mhz;   /* centre frequency of the band */
+  double bandwidth_mhz;     /* signed bandwidth of the band */
+  double dm;                /* dispersion measure, pc/cm^3 */
+  unsigned nchan;           /* input channels (complex-sampled) */
+  unsigned npol;            /* 1 or 2 */
+  int input_kind;           /* DSPSR_B200_INT8_TFPD, _INT16_TFPD or _FLOAT_FPT */
+  float lut[256];           /* 8-bit lookup table (BitTable) when INT8 */
+  int offset_binary;        /* 16-bit encoding */
+  int dual_sideband;        /* Observation::get_dual_sideband */
+  int dc_centred;
+  /* convolution */
+  unsigned nfft;            /* FFT length per part (power of two) */
+  unsigned nfilt_pos, nfilt_neg;
+  int chirp_mode;           /* DSPSR_B200_CHIRP_REFERENCE or _FP64 */
+  /* detection */
+  int state;                /* DSPSR_B200_INTENSITY ... _STOKES */
+  /* fold */
+  unsigned nbin;
+  double period_s;          /* constant folding period */
+  double reference_phase;
+  int64_t epoch_day, epoch_sec; double epoch_frac;   /* reference epoch MJD */
+  int64_t start_day, start_sec; double start_frac;   /* MJD of input sample 0 */
+  /* tuning: maximum scratch bytes for in-flight FFT parts (0 = default) */
+  uint64_t scratch_bytes;
+} dspsr_b200_pipeline_config;
+
+int dspsr_b200_pipeline_create (dspsr_b200_context* ctx,
+                                const dspsr_b200_pipeline_config* config,
+                                dspsr_b200_pipeline** pipe);
+int dspsr_b200_pipeline_destroy (dspsr_b200_pipeline* pipe);
+/* Processes one block of ndat new input samples (device memory, layout given
+   by input_kind; for FLOAT_FPT in_span is the complex-sample span per
+   (chan, pol), otherwise ignored).  Samples that do not complete an FFT part
+   are carried into the next call.  Returns the output samples folded. */
+int dspsr_b200_pipeline_run (dspsr_b200_pipeline* pipe, const void* d_in, uint64_t ndat,
+                             uint64_t in_span, uint64_t* ndat_folded);
+/* Same, from host memory: the pipeline copies the block to the device on its
+   stream (pinned host memory gives an asynchronous copy). */
+int dspsr_b200_pipeline_run_host (dspsr_b200_pipeline* pipe, const void* h_in,
+                                  uint64_t ndat, uint64_t* ndat_folded);
+/* profiles [chan][nout][nbin] and hits[nbin] into host memory */
+int dspsr_b200_pipeline_get_profiles (dspsr_b200_pipeline* pipe, float* profiles,
+                                      uint32_t* hits);
+int dspsr_b200_pipeline_reset (dspsr_b200_pipeline* pipe);
+/* Per-kernel timing: when enabled, CUDA events are recorded on the context's
+   stream around every kernel of the convolution path (column pass, row pass,
+   inverse column pass with detect+fold, single-kernel path). */
+int dspsr_b200_pipeline_profile (dspsr_b200_pipeline* pipe, int enable);
+/* Milliseconds and launch counts per kernel kind since the last call
+   (ms[4], launches[4]: columns, rows, inverse columns, single-kernel). */
+int dspsr_b200_pipeline_kernel_times (dspsr_b200_pipeline* pipe, double* ms,
+                                      uint64_t* launches);
+/* Kernels launched by this library since it was loaded. */
+uint64_t dspsr_b200_kernel_launches (void);
+/* shape of the plan: nfft, nkeep, FFT split n1 x n2, parts per batch */
+int dspsr_b200_pipeline_info (dspsr_b200_pipeline* pipe, uint64_t* info8);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,126 @@
+/*
+ * oracle.h -- CPU restatement of the DSPSR baseband hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the product library links, loads or
+ * calls this code.  Only tests/, __graft_entry__.smoke() and the cpu_baseline /
+ * reference arm of bench.py use it, and only as the checker or as the timed
+ * CPU baseline.
+ *
+ * Every function restates the reference algorithm cited beside it (paths are
+ * relative to the DSPSR source tree).  The reference itself cannot be built
+ * here (its Signal/General/dsp headers, PSRCHIVE and FFTW are absent), so the
+ * oracle carries its own FFT with FFTW's conventions (unnormalised; forward
+ * sign -1, backward sign +1).
+ *
+ * Parity pins:
+ *   - the Tukey impulse-response known-answer test restated from
+ *     Signal/General/tests/ConvolutionTest.cpp:148-308 (RMS error < 5e-8);
+ *   - the zero-DM passthrough of test/Convolution/test_Convolution.cpp;
+ *   - the closed-form detection tests of test/Detection/test_Detection.cpp;
+ *   - the fold bin recurrence (Signal/Pulsar/Fold.C:815-818) is the reference
+ *     loop itself, run literally.
+ * Unpinned: the 8-bit BitTable scale (needs PSRCHIVE's JenetAnderson98), the
+ * missing PlasmaResponse::build template (restated from its call site and the
+ * channel-frequency rule), PSRCHIVE's MJD arithmetic.
+ */
+#ifndef DSPSR_ORACLE_H
+#define DSPSR_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- FFT (FTransform::fcc1d / bcc1d conventions) ---------------------- */
+/* sign = -1 forward, +1 backward; unnormalised; in/out interleaved complex */
+void orc_fft_f32 (int n, int sign, const float* in, float* out);
+void orc_fft_f64 (int n, int sign, const double* in, double* out);
+
+/* ---- unpack (Kernel/Classes/BitTable.C:172-225, EightBitUnpacker.C:25-49,
+        BitUnpacker.C:97-138, SixteenBitUnpacker.C:23-79) ------------------ */
+/* 8-bit lookup table; spacing = JenetAnderson98 optimal input spacing */
+void orc_bittable8 (double spacing, int twos_complement, float* lut256, double* scale);
+/* TFPD bytes -> FPT floats; out[(ichan*npol+ipol)*out_span + idat*ndim + idim] */
+void orc_unpack8 (const uint8_t* in, uint64_t ndat, int nchan, int npol, int ndim,
+                  const float* lut256, float* out, uint64_t out_span);
+void orc_unpack16 (const int16_t* in, uint64_t ndat, int nchan, int npol, int ndim,
+                   int offset_binary, float* out, uint64_t out_span);
+
+/* ---- dispersion response (Signal/General/Dedispersion.C:84-186,
+        PlasmaResponse.C:91-269, Response.C:325-420,529-621,998-1050,
+        Kernel/Classes/Observation.C:521-534, optimize_fft.c:64-135) ------ */
+unsigned orc_smearing_samples (double centre_freq, double bandwidth, double dm,
+                               unsigned nchan, int half);
+unsigned orc_minimum_ndat (unsigned impulse_pos, unsigned impulse_neg);
+int64_t  orc_optimal_fft_length (uint64_t nbadperfft, uint64_t nfft_max, unsigned factor);
+/* Response in FFT order, nchan*ndat complex values, normaliser 1/sqrt(norm_nfft)
+   applied (Convolution.C:401-414).  mode 0: phase cast to float before
+   polar() (Dedispersion.C:104-111); mode 1: FP64 phase range-reduced in FP64. */
+void orc_dedispersion_response (double centre_freq, double bandwidth, double dm,
+                                unsigned nchan, unsigned ndat, int input_nchan,
+                                int dual_sideband, int dc_centred, int mode,
+                                unsigned norm_nfft, float* out);
+/* exact double-precision response (the FP64 oracle) */
+void orc_dedispersion_response_f64 (double centre_freq, double bandwidth, double dm,
+                                    unsigned nchan, unsigned ndat, int input_nchan,
+                                    int dual_sideband, int dc_centred,
+                                    unsigned norm_nfft, double* out);
+/* Tukey-window test response (Signal/General/testutils/TestResponse.cpp:30-165,
+   Apodization.C:123-146); spectral: ndat complex (FFT order, scaled 1/sqrt(ndat));
+   temporal: impulse_neg+impulse_pos complex */
+void orc_tukey_response (unsigned impulse_neg, unsigned impulse_pos, unsigned ndat,
+                         float* spectral, float* temporal);
+
+/* ---- overlap-save convolution (Signal/General/Convolution.C:316-813) ----- */
+/* in/out FPT: (ichan*npol+ipol)*span complex values; response nchan*nfft complex
+   (one filter for all polns).  Returns npart.  out holds npart*(nfft-nfilt) values. */
+uint64_t orc_convolve_f32 (const float* in, uint64_t ndat, uint64_t in_span,
+                           int nchan, int npol, const float* response,
+                           unsigned nfft, unsigned nfilt_pos, unsigned nfilt_neg,
+                           float* out, uint64_t out_span, int nthreads);
+uint64_t orc_convolve_f64 (const double* in, uint64_t ndat, uint64_t in_span,
+                           int nchan, int npol, const double* response,
+                           unsigned nfft, unsigned nfilt_pos, unsigned nfilt_neg,
+                           double* out, uint64_t out_span, int nthreads);
+
+/* ---- detection (Signal/General/Detection.C:225-630, stokes_detect.ic,
+        cross_detect.ic) -------------------------------------------------- */
+/* state: 0 Intensity (1 out pol), 1 PPQQ (2), 2 Coherence (4: PP,QQ,Re p*q,Im p*q),
+   3 Stokes (4: I,Q,U,V).  in: 2 pols complex FPT; out: FPT floats. */
+int orc_detect (const float* in, uint64_t ndat, uint64_t in_span, int nchan,
+                int state, float* out, uint64_t out_span);
+int orc_detect_f64 (const double* in, uint64_t ndat, uint64_t in_span, int nchan,
+                    int state, double* out, uint64_t out_span);
+
+/* ---- fold (Signal/Pulsar/Fold.C:662-990) -------------------------------- */
+/* phase of the first sample midpoint, constant period (Fold.C:975-979) */
+double orc_fold_phi (int64_t start_day, int64_t start_sec, double start_frac,
+                     int64_t epoch_day, int64_t epoch_sec, double epoch_frac,
+                     uint64_t idat_start, double rate, double period,
+                     double reference_phase);
+/* the literal sequential recurrence, Fold.C:790-837 */
+void orc_fold_binplan (double phi, double phase_per_sample, uint64_t ndat,
+                       unsigned nbin, uint32_t* binplan);
+/* accumulate FPT data (nchan*npol spans, ndim per sample) into profiles
+   [ichan][ipol][ibin*ndim+idim]; hits[ibin] += 1 per sample (Fold.C:893-931) */
+void orc_fold_accumulate (const float* in, uint64_t ndat, uint64_t in_span,
+                          int nchan, int npol, int ndim, const uint32_t* binplan,
+                          unsigned nbin, float* profiles, uint32_t* hits);
+void orc_fold_accumulate_f64 (const double* in, uint64_t ndat, uint64_t in_span,
+                              int nchan, int npol, int ndim, const uint32_t* binplan,
+                              unsigned nbin, double* profiles, uint32_t* hits);
+
+/* ---- the whole single-channel path, for the timed CPU baseline ----------- */
+/* int8 TFPD (nchan=1, npol=2, ndim=2) -> unpack -> convolve -> Intensity ->
+   fold.  Returns the number of output samples folded per pol. */
+uint64_t orc_pipeline_c1 (const uint8_t* in, uint64_t ndat, const float* lut256,
+                          const float* response, unsigned nfft, unsigned nfilt_pos,
+                          unsigned nfilt_neg, double phi, double phase_per_sample,
+                          unsigned nbin, float* profile, uint32_t* hits, int nthreads);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,228 @@
+"""ctypes loader for the CPU oracle (oracle/_build/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py, as the checker or as the timed CPU baseline.  The
+product library never imports it.  The C++ sources it wraps restate the DSPSR
+reference path; each function there cites the reference file:line it follows.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+i16p = np.ctypeslib.ndpointer(dtype=np.int16, flags="C_CONTIGUOUS")
+u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+c_u64 = ctypes.c_uint64
+c_i64 = ctypes.c_int64
+c_int = ctypes.c_int
+c_uint = ctypes.c_uint
+c_dbl = ctypes.c_double
+
+_SIGS = {
+    "orc_fft_f32": (None, [c_int, c_int, f32p, f32p]),
+    "orc_fft_f64": (None, [c_int, c_int, f64p, f64p]),
+    "orc_bittable8": (None, [c_dbl, c_int, f32p, ctypes.POINTER(c_dbl)]),
+    "orc_unpack8": (None, [u8p, c_u64, c_int, c_int, c_int, f32p, f32p, c_u64]),
+    "orc_unpack16": (None, [i16p, c_u64, c_int, c_int, c_int, c_int, f32p, c_u64]),
+    "orc_smearing_samples": (c_uint, [c_dbl, c_dbl, c_dbl, c_uint, c_int]),
+    "orc_minimum_ndat": (c_uint, [c_uint, c_uint]),
+    "orc_optimal_fft_length": (c_i64, [c_u64, c_u64, c_uint]),
+    "orc_dedispersion_response": (None, [c_dbl, c_dbl, c_dbl, c_uint, c_uint, c_int, c_int,
+                                         c_int, c_int, c_uint, f32p]),
+    "orc_dedispersion_response_f64": (None, [c_dbl, c_dbl, c_dbl, c_uint, c_uint, c_int,
+                                             c_int, c_int, c_uint, f64p]),
+    "orc_tukey_response": (None, [c_uint, c_uint, c_uint, f32p, f32p]),
+    "orc_convolve_f32": (c_u64, [f32p, c_u64, c_u64, c_int, c_int, f32p, c_uint, c_uint,
+                                 c_uint, f32p, c_u64, c_int]),
+    "orc_convolve_f64": (c_u64, [f64p, c_u64, c_u64, c_int, c_int, f64p, c_uint, c_uint,
+                                 c_uint, f64p, c_u64, c_int]),
+    "orc_detect": (c_int, [f32p, c_u64, c_u64, c_int, c_int, f32p, c_u64]),
+    "orc_detect_f64": (c_int, [f64p, c_u64, c_u64, c_int, c_int, f64p, c_u64]),
+    "orc_fold_phi": (c_dbl, [c_i64, c_i64, c_dbl, c_i64, c_i64, c_dbl, c_u64, c_dbl, c_dbl,
+                             c_dbl]),
+    "orc_fold_binplan": (None, [c_dbl, c_dbl, c_u64, c_uint, u32p]),
+    "orc_fold_accumulate": (None, [f32p, c_u64, c_u64, c_int, c_int, c_int, u32p, c_uint,
+                                   f32p, u32p]),
+    "orc_fold_accumulate_f64": (None, [f64p, c_u64, c_u64, c_int, c_int, c_int, u32p, c_uint,
+                                       f64p, u32p]),
+    "orc_pipeline_c1": (c_u64, [u8p, c_u64, f32p, f32p, c_uint, c_uint, c_uint, c_dbl, c_dbl,
+                                c_uint, f32p, u32p, c_int]),
+}
+
+
+def build():
+    """Compile the oracle with its Makefile (g++ only)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(_LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(_lib, name)
+            fn.restype = res
+            fn.argtypes = args
+    return _lib
+
+
+# ---- thin numpy helpers --------------------------------------------------
+
+def fft(x, sign=-1):
+    """Unnormalised complex FFT of a complex64/complex128 vector (FFTW conventions)."""
+    x = np.ascontiguousarray(x)
+    n = x.shape[0]
+    if x.dtype == np.complex64:
+        out = np.empty(n, np.complex64)
+        lib().orc_fft_f32(n, sign, x.view(np.float32), out.view(np.float32))
+    else:
+        x = x.astype(np.complex128)
+        out = np.empty(n, np.complex128)
+        lib().orc_fft_f64(n, sign, x.view(np.float64), out.view(np.float64))
+    return out
+
+
+def bittable8(spacing, twos_complement=True):
+    lut = np.empty(256, np.float32)
+    scale = c_dbl()
+    lib().orc_bittable8(spacing, int(twos_complement), lut, ctypes.byref(scale))
+    return lut, scale.value
+
+
+def unpack8(raw, ndat, nchan, npol, ndim, lut):
+    """TFPD uint8 bytes -> FPT float32 array of shape (nchan, npol, ndat*ndim)."""
+    out = np.empty((nchan, npol, ndat * ndim), np.float32)
+    lib().orc_unpack8(np.ascontiguousarray(raw.view(np.uint8).ravel()), ndat, nchan, npol,
+                      ndim, lut, out.reshape(-1), ndat * ndim)
+    return out
+
+
+def unpack16(raw, ndat, nchan, npol, ndim, offset_binary=False):
+    out = np.empty((nchan, npol, ndat * ndim), np.float32)
+    lib().orc_unpack16(np.ascontiguousarray(raw.view(np.int16).ravel()), ndat, nchan, npol,
+                       ndim, int(offset_binary), out.reshape(-1), ndat * ndim)
+    return out
+
+
+def smearing_samples(cf, bw, dm, nchan, half):
+    return lib().orc_smearing_samples(cf, bw, dm, nchan, half)
+
+
+def minimum_ndat(pos, neg):
+    return lib().orc_minimum_ndat(pos, neg)
+
+
+def optimal_fft_length(nbad, nmax=0, factor=1):
+    return lib().orc_optimal_fft_length(nbad, nmax, factor)
+
+
+def dedispersion_response(cf, bw, dm, nchan, ndat, input_nchan=1, dual_sideband=1,
+                          dc_centred=0, mode=0, norm_nfft=None):
+    out = np.empty(nchan * ndat, np.complex64)
+    lib().orc_dedispersion_response(cf, bw, dm, nchan, ndat, input_nchan, dual_sideband,
+                                    dc_centred, mode, norm_nfft or ndat, out.view(np.float32))
+    return out.reshape(nchan, ndat)
+
+
+def dedispersion_response_f64(cf, bw, dm, nchan, ndat, input_nchan=1, dual_sideband=1,
+                              dc_centred=0, norm_nfft=None):
+    out = np.empty(nchan * ndat, np.complex128)
+    lib().orc_dedispersion_response_f64(cf, bw, dm, nchan, ndat, input_nchan, dual_sideband,
+                                        dc_centred, norm_nfft or ndat, out.view(np.float64))
+    return out.reshape(nchan, ndat)
+
+
+def tukey_response(neg, pos, ndat):
+    spec = np.empty(ndat, np.complex64)
+    temp = np.empty(neg + pos, np.complex64)
+    lib().orc_tukey_response(neg, pos, ndat, spec.view(np.float32), temp.view(np.float32))
+    return spec, temp
+
+
+def convolve(x, response, nfft, nfilt_pos, nfilt_neg, nthreads=8):
+    """x: complex (nchan, npol, ndat); response: complex (nchan, nfft).
+    Returns the (nchan, npol, npart*nkeep) overlap-save output."""
+    nchan, npol, ndat = x.shape
+    nkeep = nfft - nfilt_pos - nfilt_neg
+    npart = (ndat - nfilt_pos - nfilt_neg) // nkeep if ndat >= nfft else 0
+    if x.dtype == np.complex64:
+        out = np.zeros((nchan, npol, npart * nkeep), np.complex64)
+        r = np.ascontiguousarray(response, np.complex64)
+        lib().orc_convolve_f32(np.ascontiguousarray(x).view(np.float32).ravel(), ndat, ndat,
+                               nchan, npol, r.view(np.float32).ravel(), nfft, nfilt_pos,
+                               nfilt_neg, out.view(np.float32).ravel(), npart * nkeep, nthreads)
+    else:
+        out = np.zeros((nchan, npol, npart * nkeep), np.complex128)
+        r = np.ascontiguousarray(response, np.complex128)
+        lib().orc_convolve_f64(np.ascontiguousarray(x, np.complex128).view(np.float64).ravel(),
+                               ndat, ndat, nchan, npol, r.view(np.float64).ravel(), nfft,
+                               nfilt_pos, nfilt_neg, out.view(np.float64).ravel(),
+                               npart * nkeep, nthreads)
+    return out
+
+
+STATES = {"Intensity": 0, "PPQQ": 1, "Coherence": 2, "Stokes": 3}
+NOUT = {0: 1, 1: 2, 2: 4, 3: 4}
+
+
+def detect(x, state):
+    """x: complex (nchan, 2, ndat) -> float (nchan, nout, ndat)."""
+    state = STATES.get(state, state)
+    nchan, npol, ndat = x.shape
+    assert npol == 2
+    nout = NOUT[state]
+    if x.dtype == np.complex64:
+        out = np.empty((nchan, nout, ndat), np.float32)
+        lib().orc_detect(np.ascontiguousarray(x).view(np.float32).ravel(), ndat, ndat, nchan,
+                         state, out.ravel(), ndat)
+    else:
+        out = np.empty((nchan, nout, ndat), np.float64)
+        lib().orc_detect_f64(np.ascontiguousarray(x, np.complex128).view(np.float64).ravel(),
+                             ndat, ndat, nchan, state, out.ravel(), ndat)
+    return out
+
+
+def fold_phi(start_mjd, epoch_mjd, idat_start, rate, period, reference_phase=0.0):
+    return lib().orc_fold_phi(start_mjd[0], start_mjd[1], start_mjd[2], epoch_mjd[0],
+                              epoch_mjd[1], epoch_mjd[2], idat_start, rate, period,
+                              reference_phase)
+
+
+def fold_binplan(phi, phase_per_sample, ndat, nbin):
+    out = np.empty(ndat, np.uint32)
+    lib().orc_fold_binplan(phi, phase_per_sample, ndat, nbin, out)
+    return out
+
+
+def fold_accumulate(data, binplan, nbin, profiles=None, hits=None):
+    """data: float (nchan, npol, ndat) (ndim 1).  Returns profiles (nchan,npol,nbin), hits."""
+    nchan, npol, ndat = data.shape
+    f64 = data.dtype == np.float64
+    if profiles is None:
+        profiles = np.zeros((nchan, npol, nbin), np.float64 if f64 else np.float32)
+    if hits is None:
+        hits = np.zeros(nbin, np.uint32)
+    fn = lib().orc_fold_accumulate_f64 if f64 else lib().orc_fold_accumulate
+    fn(np.ascontiguousarray(data).ravel(), ndat, ndat, nchan, npol, 1,
+       np.ascontiguousarray(binplan, np.uint32), nbin, profiles.reshape(-1), hits)
+    return profiles, hits
+
+
+def pipeline_c1(raw, ndat, lut, response, nfft, nfilt_pos, nfilt_neg, phi, pps, nbin,
+                nthreads=8):
+    prof = np.zeros(nbin, np.float32)
+    hits = np.zeros(nbin, np.uint32)
+    n = lib().orc_pipeline_c1(np.ascontiguousarray(raw.view(np.uint8).ravel()), ndat, lut,
+                              np.ascontiguousarray(response, np.complex64).view(np.float32).ravel(),
+                              nfft, nfilt_pos, nfilt_neg, phi, pps, nbin, prof, hits, nthreads)
+    return prof, hits, n

@@ -1,0 +1,699 @@
+// oracle.cpp -- CPU restatement of the DSPSR baseband hot path.
+//
+// TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the
+// CPU-baseline leg of bench.py as the checker / timed CPU baseline.  The
+// product library never links or calls it.
+//
+// Each function names the reference source it restates (paths relative to the
+// DSPSR tree).  Built by oracle/Makefile with -ffp-contract=off so that every
+// float operation rounds exactly as written, as the reference's x86-64 build
+// (SSE2, no FMA contraction) does.
+
+#include "../oracle.h"
+
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <vector>
+#include <memory>
+#include <algorithm>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// FFT with FFTW's conventions (FTransform::fcc1d forward sign -1, bcc1d
+// backward sign +1, both unnormalised).  Radix-2 decimation in time; twiddles
+// are computed in double and rounded once to T.
+// ---------------------------------------------------------------------------
+
+template <typename T>
+struct Plan
+{
+  int n = 0, log2n = 0;
+  std::vector<uint32_t> rev;
+  std::vector<std::complex<T>> tw;   // tw[k] = exp(-2 pi i k / n), k < n/2
+};
+
+std::mutex plan_mutex;
+
+template <typename T>
+const Plan<T>& get_plan (int n)
+{
+  static std::map<int, std::unique_ptr<Plan<T>>> plans;
+  std::lock_guard<std::mutex> lock (plan_mutex);
+  auto it = plans.find (n);
+  if (it != plans.end ())
+    return *it->second;
+  auto p = std::make_unique<Plan<T>> ();
+  p->n = n;
+  int lg = 0;
+  while ((1 << lg) < n) lg++;
+  p->log2n = lg;
+  p->rev.resize (n);
+  for (int i = 0; i < n; i++)
+  {
+    uint32_t r = 0;
+    for (int b = 0; b < lg; b++)
+      if (i & (1 << b)) r |= 1u << (lg - 1 - b);
+    p->rev[i] = r;
+  }
+  p->tw.resize (std::max (1, n / 2));
+  for (int k = 0; k < n / 2; k++)
+  {
+    double a = -2.0 * M_PI * double (k) / double (n);
+    p->tw[k] = std::complex<T> (T (std::cos (a)), T (std::sin (a)));
+  }
+  auto& ref = *p;
+  plans[n] = std::move (p);
+  return ref;
+}
+
+template <typename T>
+void fft (int n, int sign, const std::complex<T>* in, std::complex<T>* out)
+{
+  const Plan<T>& p = get_plan<T> (n);
+  if (in == out)
+  {
+    std::vector<std::complex<T>> tmp (in, in + n);
+    for (int i = 0; i < n; i++) out[p.rev[i]] = tmp[i];
+  }
+  else
+    for (int i = 0; i < n; i++) out[p.rev[i]] = in[i];
+
+  for (int len = 2; len <= n; len <<= 1)
+  {
+    const int half = len >> 1;
+    const int tstep = n / len;
+    for (int i = 0; i < n; i += len)
+    {
+      for (int j = 0; j < half; j++)
+      {
+        std::complex<T> w = p.tw[j * tstep];
+        if (sign > 0) w = std::conj (w);
+        const std::complex<T> a = out[i + j];
+        const std::complex<T> b0 = out[i + j + half];
+        // explicit real arithmetic: no library complex-multiply NaN handling
+        const T br = w.real () * b0.real () - w.imag () * b0.imag ();
+        const T bi = w.real () * b0.imag () + w.imag () * b0.real ();
+        out[i + j] = std::complex<T> (a.real () + br, a.imag () + bi);
+        out[i + j + half] = std::complex<T> (a.real () - br, a.imag () - bi);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Observation / PlasmaResponse helpers
+// ---------------------------------------------------------------------------
+
+// Dedispersion.C:32 -- DM (pc/cm^3) = 2.41e-4 D (s MHz^2)
+const double dm_dispersion = 2.41e-4;
+
+template <typename T> inline T sqr (T x) { return x * x; }
+
+// Dedispersion.C:136-140
+double delay_time (double dm, double freq)
+{
+  double dispersion = dm / dm_dispersion;
+  return dispersion * 1.0 / sqr (freq);
+}
+
+// Observation.C:521-534 (no channel swapping): centre of channel ichan
+double channel_centre (double cf, double bw, unsigned nchan, unsigned ichan, bool dc_centred)
+{
+  double base = dc_centred ? cf - 0.5 * bw : cf - 0.5 * bw + 0.5 * bw / double (nchan);
+  return base + double (ichan) * bw / double (nchan);
+}
+
+// Response.C:998-1050 doswap on a single-pol complex buffer of nchan*ndat
+template <typename T>
+void doswap (std::complex<T>* buf, unsigned nchan, unsigned ndat, unsigned divisions)
+{
+  // half_npts counts complex values here (the reference counts floats)
+  const uint64_t half = uint64_t (ndat) * nchan / (2 * divisions);
+  for (unsigned d = 0; d < divisions; d++)
+  {
+    std::complex<T>* p1 = buf + uint64_t (d) * 2 * half;
+    std::complex<T>* p2 = p1 + half;
+    for (uint64_t i = 0; i < half; i++) std::swap (p1[i], p2[i]);
+  }
+}
+
+// Response.C:325-400 swap_as_needed, for the states this path meets
+template <typename T>
+void swap_as_needed (std::complex<T>* buf, unsigned nchan, unsigned ndat,
+                     int input_nchan, int dual_sideband, int dc_centred)
+{
+  if (input_nchan == 1)
+  {
+    if (dual_sideband > 0)
+      doswap (buf, nchan, ndat, 1);
+    unsigned subswap = std::abs (dual_sideband);
+    if (subswap > 1)
+      doswap (buf, nchan, ndat, subswap);
+  }
+  else
+  {
+    if (dc_centred)
+    {
+      // Response::rotate(-ndat/2) within each channel
+      for (unsigned c = 0; c < nchan; c++)
+        std::rotate (buf + uint64_t (c) * ndat, buf + uint64_t (c) * ndat + ndat / 2,
+                     buf + uint64_t (c + 1) * ndat);
+    }
+    if (dual_sideband && unsigned (input_nchan) == nchan)
+      doswap (buf, nchan, ndat, nchan);
+  }
+}
+
+// Restatement of the missing PlasmaResponse::build template (called at
+// Dedispersion.C:128) with Dedispersion::build_compute (Dedispersion.C:166-186)
+// and interchannel_fractional_sample_delay = 0 (no SampleDelay).
+// Channel centres follow Observation.C:521-534; within a channel the ndat
+// frequency bins run low to high from -chanwidth/2, spanning the channel.
+void dedispersion_phases (double cf, double bw, double dm, unsigned nchan,
+                          unsigned ndat, bool dc_centred, std::vector<double>& phase)
+{
+  const double chanwidth = bw / double (nchan);
+  const double binwidth = chanwidth / double (ndat);
+  const double sign = bw / std::fabs (bw);
+  const double dispersion_per_MHz = 1e6 * dm / dm_dispersion;
+  phase.resize (uint64_t (nchan) * ndat);
+  for (unsigned ichan = 0; ichan < nchan; ichan++)
+  {
+    const double chan_freq = channel_centre (cf, bw, nchan, ichan, dc_centred);
+    const double coeff = -sign * 2 * M_PI * dispersion_per_MHz / sqr (chan_freq);
+    for (unsigned ipt = 0; ipt < ndat; ipt++)
+    {
+      const double freq = double (ipt) * binwidth - 0.5 * chanwidth;
+      const double delay_phase = -2.0 * M_PI * freq * 0.0;
+      phase[uint64_t (ichan) * ndat + ipt] = coeff * sqr (freq) / (chan_freq + freq) + delay_phase;
+    }
+  }
+}
+
+template <typename T>
+uint64_t convolve (const T* in, uint64_t ndat, uint64_t in_span, int nchan, int npol,
+                   const T* response, unsigned nfft, unsigned nfilt_pos, unsigned nfilt_neg,
+                   T* out, uint64_t out_span, int nthreads)
+{
+  typedef std::complex<T> C;
+  const uint64_t nsamp_overlap = nfilt_pos + nfilt_neg;
+  const uint64_t nsamp_step = nfft - nsamp_overlap;
+  uint64_t npart = 0;
+  if (ndat >= nfft)
+    npart = (ndat - nsamp_overlap) / nsamp_step;   // Convolution.C:486-487
+  const int64_t ntask = int64_t (nchan) * npol * npart;
+  (void) nthreads;
+#pragma omp parallel num_threads(nthreads > 0 ? nthreads : 1)
+  {
+    std::vector<C> spectrum (nfft), complex_time (nfft);
+#pragma omp for schedule(static)
+    for (int64_t task = 0; task < ntask; task++)
+    {
+      const uint64_t ipart = uint64_t (task) % npart;
+      const int ipol = int ((uint64_t (task) / npart) % npol);
+      const int ichan = int (uint64_t (task) / npart / npol);
+      const C* ptr = reinterpret_cast<const C*> (in) + (uint64_t (ichan) * npol + ipol) * in_span
+                     + ipart * nsamp_step;
+      fft<T> (nfft, -1, ptr, spectrum.data ());
+      // Response::operate (Response.C:662-726)
+      const C* f = reinterpret_cast<const C*> (response) + uint64_t (ichan) * nfft;
+      for (unsigned k = 0; k < nfft; k++)
+      {
+        const T d_r = spectrum[k].real (), d_i = spectrum[k].imag ();
+        const T f_r = f[k].real (), f_i = f[k].imag ();
+        spectrum[k] = C (f_r * d_r - f_i * d_i, f_i * d_r + f_r * d_i);
+      }
+      fft<T> (nfft, +1, spectrum.data (), complex_time.data ());
+      C* o = reinterpret_cast<C*> (out) + (uint64_t (ichan) * npol + ipol) * out_span
+             + ipart * nsamp_step;
+      std::memcpy (o, complex_time.data () + nfilt_pos, nsamp_step * sizeof (C));
+    }
+  }
+  return npart;
+}
+
+template <typename T>
+int detect (const T* in, uint64_t ndat, uint64_t in_span, int nchan, int state,
+            T* out, uint64_t out_span)
+{
+  const int nout = state == 0 ? 1 : state == 1 ? 2 : 4;
+  for (int c = 0; c < nchan; c++)
+  {
+    const T* p = in + 2 * (uint64_t (c) * 2 + 0) * in_span;
+    const T* q = in + 2 * (uint64_t (c) * 2 + 1) * in_span;
+    T* o[4];
+    for (int k = 0; k < nout; k++) o[k] = out + (uint64_t (c) * nout + k) * out_span;
+    for (uint64_t j = 0; j < ndat; j++)
+    {
+      const T p_r = p[2 * j], p_i = p[2 * j + 1], q_r = q[2 * j], q_i = q[2 * j + 1];
+      if (state == 0)
+      {
+        // Detection.C:253-301 (FPT, Intensity): accumulation in this order
+        T v = p_r * p_r;
+        v += p_i * p_i;
+        v += q_r * q_r;
+        v += q_i * q_i;
+        o[0][j] = v;
+      }
+      else if (state == 1)
+      {
+        T v = p_r * p_r; v += p_i * p_i; o[0][j] = v;
+        T w = q_r * q_r; w += q_i * q_i; o[1][j] = w;
+      }
+      else if (state == 2)
+      {
+        // cross_detect.ic:38-41
+        o[0][j] = p_r * p_r + p_i * p_i;
+        o[1][j] = q_r * q_r + q_i * q_i;
+        o[2][j] = p_r * q_r + p_i * q_i;
+        o[3][j] = p_r * q_i - p_i * q_r;
+      }
+      else
+      {
+        // stokes_detect.ic:40-43
+        const T pp = p_r * p_r + p_i * p_i;
+        const T qq = q_r * q_r + q_i * q_i;
+        o[0][j] = pp + qq;
+        o[1][j] = pp - qq;
+        o[2][j] = T (2.0 * (p_r * q_r + p_i * q_i));
+        o[3][j] = T (2.0 * (p_r * q_i - p_i * q_r));
+      }
+    }
+  }
+  return nout;
+}
+
+template <typename T>
+void fold_accumulate (const T* in, uint64_t ndat, uint64_t in_span, int nchan, int npol,
+                      int ndim, const uint32_t* binplan, unsigned nbin, T* profiles,
+                      uint32_t* hits)
+{
+  // Fold.C:893-931 (FPT); hits counted once per sample (Fold.C:829-835)
+  for (uint64_t idat = 0; idat < ndat; idat++)
+    if (binplan[idat] < nbin) hits[binplan[idat]]++;
+  for (int c = 0; c < nchan; c++)
+    for (int p = 0; p < npol; p++)
+    {
+      const T* timep = in + (uint64_t (c) * npol + p) * in_span;
+      T* phasep = profiles + (uint64_t (c) * npol + p) * nbin * ndim;
+      for (uint64_t idat = 0; idat < ndat; idat++)
+      {
+        if (binplan[idat] != nbin)
+        {
+          T* ph = phasep + uint64_t (binplan[idat]) * ndim;
+          for (int d = 0; d < ndim; d++) ph[d] += timep[d];
+        }
+        timep += ndim;
+      }
+    }
+}
+
+} // namespace
+
+extern "C" {
+
+void orc_fft_f32 (int n, int sign, const float* in, float* out)
+{
+  fft<float> (n, sign, reinterpret_cast<const std::complex<float>*> (in),
+              reinterpret_cast<std::complex<float>*> (out));
+}
+
+void orc_fft_f64 (int n, int sign, const double* in, double* out)
+{
+  fft<double> (n, sign, reinterpret_cast<const std::complex<double>*> (in),
+               reinterpret_cast<std::complex<double>*> (out));
+}
+
+// BitTable.C:172-225 with nbit = 8, zero_is_a_threshold = true.
+// NormalDistribution::cumulative_distribution(x) = (1 + erf(x/sqrt 2)) / 2.
+void orc_bittable8 (double input_spacing, int twos_complement, float* lut, double* scale_out)
+{
+  const unsigned unique_values = 256;
+  float values[256];
+  const double output_spacing = 1.0 / double (unique_values);
+  const double output_middle = double (unique_values - 1) / 2.0;
+  const unsigned input_middle = unique_values / 2;
+  const unsigned input_offset = twos_complement ? unique_values / 2 : 0;
+  double cumulative_probability = 0.0, variance = 0.0;
+  for (unsigned i = 0; i < unique_values; i++)
+  {
+    double output = (double (i) - output_middle) * output_spacing;
+    values[(i + input_offset) % unique_values] = output;
+    if (i < input_middle)
+    {
+      double threshold = double (int (i + 1) - int (input_middle)) * input_spacing;
+      double cumulative = 0.5 * (1.0 + std::erf (threshold / std::sqrt (2.0)));
+      double interval = cumulative - cumulative_probability;
+      cumulative_probability = cumulative;
+      variance += output * output * interval;
+    }
+  }
+  variance *= 2.0;
+  double scale = 1.0 / std::sqrt (variance);
+  for (unsigned i = 0; i < unique_values; i++)
+    values[i] *= scale;
+  scale *= output_spacing;
+  // BitTable::generate with values_per_byte = 1, no bit reversal: table[b] = values[b]
+  for (unsigned b = 0; b < 256; b++) lut[b] = values[b];
+  if (scale_out) *scale_out = scale;
+}
+
+// BitUnpacker.C:97-138 with EightBitUnpacker::unpack_bits (EightBitUnpacker.C:25-49)
+void orc_unpack8 (const uint8_t* in, uint64_t ndat, int nchan, int npol, int ndim,
+                  const float* lut, float* out, uint64_t out_span)
+{
+  const unsigned nskip = npol * nchan * ndim;
+  unsigned offset = 0;
+  for (int c = 0; c < nchan; c++)
+    for (int p = 0; p < npol; p++)
+      for (int d = 0; d < ndim; d++)
+      {
+        const uint8_t* from = in + offset;
+        float* into = out + (uint64_t (c) * npol + p) * out_span + d;
+        for (uint64_t idat = 0; idat < ndat; idat++)
+        {
+          *into = lut[*from];
+          from += nskip;
+          into += ndim;
+        }
+        offset++;
+      }
+}
+
+// SixteenBitUnpacker.C:23-79
+void orc_unpack16 (const int16_t* in, uint64_t ndat, int nchan, int npol, int ndim,
+                   int offset_binary, float* out, uint64_t out_span)
+{
+  const unsigned nskip = npol * nchan * ndim;
+  unsigned offset = 0;
+  for (int c = 0; c < nchan; c++)
+    for (int p = 0; p < npol; p++)
+      for (int d = 0; d < ndim; d++)
+      {
+        const int16_t* from = in + offset;
+        float* into = out + (uint64_t (c) * npol + p) * out_span + d;
+        for (uint64_t idat = 0; idat < ndat; idat++)
+        {
+          int16_t v = *from;
+          if (offset_binary) v = int16_t (v ^ 0x8000);
+          *into = float (v) + 0.5;
+          from += nskip;
+          into += ndim;
+        }
+        offset++;
+      }
+}
+
+// PlasmaResponse.C:161-250 (smearing_time(half), smearing_samples) with the
+// default 10% smearing buffer and all channels supported.
+unsigned orc_smearing_samples (double centre_frequency, double bandwidth, double dm,
+                               unsigned nchan, int half)
+{
+  double abs_bw = std::fabs (bandwidth);
+  double ch_abs_bw = abs_bw / double (nchan);
+  double lower_ch_cfreq = centre_frequency - (abs_bw - ch_abs_bw) / 2.0;
+  if (half)
+  {
+    ch_abs_bw /= 2.0;
+    lower_ch_cfreq += double (half) * ch_abs_bw;
+  }
+  // smearing_time (cfreq, bw) = delay_time (cfreq - |bw/2|, cfreq + |bw/2|)
+  double f1 = lower_ch_cfreq - std::fabs (0.5 * ch_abs_bw);
+  double f2 = lower_ch_cfreq + std::fabs (0.5 * ch_abs_bw);
+  double tsmear = delay_time (dm, f1) - delay_time (dm, f2);
+  double sampling_rate = std::fabs (bandwidth) / double (nchan) * 1e6;
+  tsmear *= (1.0 + double (0.1f));   // smearing_buffer is a float (PlasmaResponse.C:20)
+  return unsigned (std::ceil (tsmear * sampling_rate));
+}
+
+// Response.C:529-545
+unsigned orc_minimum_ndat (unsigned impulse_pos, unsigned impulse_neg)
+{
+  double impulse_tot = impulse_pos + impulse_neg;
+  if (impulse_tot == 0) return 0;
+  unsigned min = unsigned (std::pow (2.0, std::ceil (std::log (impulse_tot) / std::log (2.0))));
+  while (min <= impulse_tot) min *= 2;
+  return min;
+}
+
+// optimize_fft.c:64-135
+int64_t orc_optimal_fft_length (uint64_t nbadperfft, uint64_t nfft_max, unsigned factor)
+{
+  if (!nbadperfft) return -1;
+  uint64_t nfft_min = factor;
+  while (nbadperfft > nfft_min) nfft_min *= 2;
+  if (nfft_max && nfft_max < nfft_min) return -1;
+  uint64_t nfft = nfft_min;
+  double order_fft = (double) nfft * std::log ((double) nfft);
+  double timescale = order_fft / (double) (nfft - nbadperfft);
+  while (nfft_max == 0 || nfft * 2 < nfft_max)
+  {
+    double prev_timescale = timescale;
+    nfft *= 2;
+    order_fft = (double) nfft * std::log ((double) nfft);
+    timescale = order_fft / (double) (nfft - nbadperfft);
+    if (timescale > prev_timescale) { nfft /= 2; break; }
+  }
+  return (int64_t) nfft;
+}
+
+void orc_dedispersion_response (double cf, double bw, double dm, unsigned nchan,
+                                unsigned ndat, int input_nchan, int dual_sideband,
+                                int dc_centred, int mode, unsigned norm_nfft, float* out)
+{
+  std::vector<double> phase;
+  dedispersion_phases (cf, bw, dm, nchan, ndat, dc_centred != 0 && input_nchan > 1, phase);
+  std::complex<float>* h = reinterpret_cast<std::complex<float>*> (out);
+  const uint64_t npt = uint64_t (nchan) * ndat;
+  for (uint64_t i = 0; i < npt; i++)
+  {
+    if (mode == 0)
+    {
+      // Dedispersion.C:104-111: vector<float> phases, polar(float(1.0), phase)
+      const float ph = float (phase[i]);
+      h[i] = std::complex<float> (std::cos (ph), std::sin (ph));
+    }
+    else
+    {
+      // double phase, reduced modulo 2 pi in double, one rounding to float
+      const double ph = phase[i] - 2.0 * M_PI * std::nearbyint (phase[i] / (2.0 * M_PI));
+      h[i] = std::complex<float> (float (std::cos (ph)), float (std::sin (ph)));
+    }
+  }
+  swap_as_needed (h, nchan, ndat, input_nchan, dual_sideband, dc_centred);
+  // ScalarFilter (ScalarFilter.C:29-40) appended by Convolution::prepare_normalizer
+  const float s = float (1.0 / std::sqrt (double (norm_nfft)));
+  for (uint64_t i = 0; i < npt; i++)
+    h[i] = std::complex<float> (h[i].real () * s, h[i].imag () * s);
+}
+
+void orc_dedispersion_response_f64 (double cf, double bw, double dm, unsigned nchan,
+                                    unsigned ndat, int input_nchan, int dual_sideband,
+                                    int dc_centred, unsigned norm_nfft, double* out)
+{
+  std::vector<double> phase;
+  dedispersion_phases (cf, bw, dm, nchan, ndat, dc_centred != 0 && input_nchan > 1, phase);
+  std::complex<double>* h = reinterpret_cast<std::complex<double>*> (out);
+  const uint64_t npt = uint64_t (nchan) * ndat;
+  const double s = 1.0 / std::sqrt (double (norm_nfft));
+  for (uint64_t i = 0; i < npt; i++)
+    h[i] = std::complex<double> (std::cos (phase[i]) * s, std::sin (phase[i]) * s);
+  swap_as_needed (h, nchan, ndat, input_nchan, dual_sideband, dc_centred);
+}
+
+// TestResponse.cpp:30-165 with Apodization::Tukey (Apodization.C:123-146)
+void orc_tukey_response (unsigned impulse_neg, unsigned impulse_pos, unsigned ndat,
+                         float* spectral_out, float* temporal_out)
+{
+  const unsigned size = impulse_neg + impulse_pos;
+  std::vector<float> amp (size);
+  {
+    float denom_start = 2 * impulse_neg;
+    float denom_end = 2 * impulse_pos;
+    for (unsigned idat = 0; idat < size; idat++)
+    {
+      if (idat < impulse_neg)
+        amp[idat] = 0.5 * (1 - std::cos (2.0 * M_PI * float (idat) / denom_start));
+      else if (idat + 1 > size - impulse_pos)
+        amp[idat] = 0.5 * (1 - std::cos (2.0 * M_PI * float (size - idat - 1) / denom_end));
+      else
+        amp[idat] = 1.0;
+    }
+  }
+  std::vector<std::complex<float>> temporal (size);
+  std::complex<double> sum_temporal = 0.0;
+  std::vector<float> correction (size);
+  double sum_correction = 0.0;
+  for (unsigned idat = 0; idat < size; idat++)
+  {
+    double phase = 2.0 * M_PI * double (idat) / double (size);
+    temporal[idat] = amp[idat] * std::complex<float> (std::cos (phase), std::sin (phase));
+    sum_temporal += std::complex<double> (temporal[idat]);
+    correction[idat] = std::sin (0.5 * phase);
+    sum_correction += correction[idat];
+  }
+  auto mean_offset = sum_temporal / sum_correction;
+  for (unsigned idat = 0; idat < size; idat++)
+  {
+    std::complex<double> t = std::complex<double> (temporal[idat]) - mean_offset * double (correction[idat]);
+    temporal[idat] = std::complex<float> (t);
+  }
+  std::vector<std::complex<float>> padded (ndat, 0.0f);
+  for (unsigned idat = 0; idat < impulse_pos; idat++)
+    padded[idat] = temporal[idat + impulse_neg];
+  const unsigned offset = ndat - impulse_neg;
+  for (unsigned idat = 0; idat < impulse_neg; idat++)
+    padded[idat + offset] = temporal[idat];
+  std::complex<float>* spectral = reinterpret_cast<std::complex<float>*> (spectral_out);
+  fft<float> (ndat, -1, padded.data (), spectral);
+  float scalefac = 1.0 / std::sqrt (ndat);
+  for (unsigned idat = 0; idat < ndat; idat++)
+    spectral[idat] *= scalefac;
+  std::memcpy (temporal_out, temporal.data (), size * sizeof (std::complex<float>));
+}
+
+uint64_t orc_convolve_f32 (const float* in, uint64_t ndat, uint64_t in_span, int nchan,
+                           int npol, const float* response, unsigned nfft, unsigned nfilt_pos,
+                           unsigned nfilt_neg, float* out, uint64_t out_span, int nthreads)
+{
+  return convolve<float> (in, ndat, in_span, nchan, npol, response, nfft, nfilt_pos,
+                          nfilt_neg, out, out_span, nthreads);
+}
+
+uint64_t orc_convolve_f64 (const double* in, uint64_t ndat, uint64_t in_span, int nchan,
+                           int npol, const double* response, unsigned nfft, unsigned nfilt_pos,
+                           unsigned nfilt_neg, double* out, uint64_t out_span, int nthreads)
+{
+  return convolve<double> (in, ndat, in_span, nchan, npol, response, nfft, nfilt_pos,
+                           nfilt_neg, out, out_span, nthreads);
+}
+
+int orc_detect (const float* in, uint64_t ndat, uint64_t in_span, int nchan, int state,
+                float* out, uint64_t out_span)
+{
+  return detect<float> (in, ndat, in_span, nchan, state, out, out_span);
+}
+
+int orc_detect_f64 (const double* in, uint64_t ndat, uint64_t in_span, int nchan, int state,
+                    double* out, uint64_t out_span)
+{
+  return detect<double> (in, ndat, in_span, nchan, state, out, out_span);
+}
+
+// Fold.C:685-693 and 975-979: phi = fmod((t - epoch).in_seconds(), P)/P - ref_phase,
+// t = start_time + (idat_start + 0.5)/rate.  The MJD is (day, second, fraction of a
+// second); the difference in seconds is formed from the integer parts first.
+double orc_fold_phi (int64_t start_day, int64_t start_sec, double start_frac,
+                     int64_t epoch_day, int64_t epoch_sec, double epoch_frac,
+                     uint64_t idat_start, double rate, double period, double reference_phase)
+{
+  double mid_idat_start = double (idat_start) + 0.5;
+  double add = mid_idat_start / rate;
+  // MJD + seconds: carry whole seconds into the integer part
+  double whole = std::floor (add);
+  double frac = start_frac + (add - whole);
+  int64_t sec = start_sec + int64_t (whole);
+  if (frac >= 1.0) { frac -= 1.0; sec += 1; }
+  int64_t day = start_day + sec / 86400;
+  sec = sec % 86400;
+  double seconds = double ((day - epoch_day) * 86400 + (sec - epoch_sec)) + (frac - epoch_frac);
+  return std::fmod (seconds, period) / period - reference_phase;
+}
+
+// Fold.C:790-837, the sequential FP64 recurrence
+void orc_fold_binplan (double phi, double phase_per_sample, uint64_t ndat, unsigned nbin,
+                       uint32_t* binplan)
+{
+  const double double_nbin = double (nbin);
+  for (uint64_t idat = 0; idat < ndat; idat++)
+  {
+    phi -= std::floor (phi);
+    double double_ibin = phi * double_nbin;
+    unsigned ibin = unsigned (double_ibin);
+    phi += phase_per_sample;
+    binplan[idat] = ibin;
+  }
+}
+
+void orc_fold_accumulate (const float* in, uint64_t ndat, uint64_t in_span, int nchan,
+                          int npol, int ndim, const uint32_t* binplan, unsigned nbin,
+                          float* profiles, uint32_t* hits)
+{
+  fold_accumulate<float> (in, ndat, in_span, nchan, npol, ndim, binplan, nbin, profiles, hits);
+}
+
+void orc_fold_accumulate_f64 (const double* in, uint64_t ndat, uint64_t in_span, int nchan,
+                              int npol, int ndim, const uint32_t* binplan, unsigned nbin,
+                              double* profiles, uint32_t* hits)
+{
+  fold_accumulate<double> (in, ndat, in_span, nchan, npol, ndim, binplan, nbin, profiles, hits);
+}
+
+uint64_t orc_pipeline_c1 (const uint8_t* in, uint64_t ndat, const float* lut,
+                          const float* response, unsigned nfft, unsigned nfilt_pos,
+                          unsigned nfilt_neg, double phi, double phase_per_sample,
+                          unsigned nbin, float* profile, uint32_t* hits, int nthreads)
+{
+  typedef std::complex<float> C;
+  const uint64_t nsamp_overlap = nfilt_pos + nfilt_neg;
+  const uint64_t nsamp_step = nfft - nsamp_overlap;
+  if (ndat < nfft) return 0;
+  const uint64_t npart = (ndat - nsamp_overlap) / nsamp_step;
+  const uint64_t nout = npart * nsamp_step;
+  std::vector<uint32_t> binplan (nout);
+  orc_fold_binplan (phi, phase_per_sample, nout, nbin, binplan.data ());
+  for (uint64_t i = 0; i < nout; i++) hits[binplan[i]]++;
+  const int nt = nthreads > 0 ? nthreads : 1;
+  std::vector<std::vector<float>> partial (nt, std::vector<float> (nbin, 0.0f));
+#pragma omp parallel num_threads(nt)
+  {
+    int tid = 0;
+#ifdef _OPENMP
+    tid = omp_get_thread_num ();
+#endif
+    std::vector<C> win (nfft), spec (nfft), tim[2] = {std::vector<C> (nfft), std::vector<C> (nfft)};
+    float* prof = partial[tid].data ();
+#pragma omp for schedule(dynamic, 1)
+    for (int64_t ipart = 0; ipart < int64_t (npart); ipart++)
+    {
+      for (int ipol = 0; ipol < 2; ipol++)
+      {
+        const uint8_t* b = in + uint64_t (ipart) * nsamp_step * 4 + 2 * ipol;
+        for (unsigned j = 0; j < nfft; j++)
+          win[j] = C (lut[b[4 * j]], lut[b[4 * j + 1]]);
+        fft<float> (nfft, -1, win.data (), spec.data ());
+        const C* f = reinterpret_cast<const C*> (response);
+        for (unsigned k = 0; k < nfft; k++)
+        {
+          const float d_r = spec[k].real (), d_i = spec[k].imag ();
+          const float f_r = f[k].real (), f_i = f[k].imag ();
+          spec[k] = C (f_r * d_r - f_i * d_i, f_i * d_r + f_r * d_i);
+        }
+        fft<float> (nfft, +1, spec.data (), tim[ipol].data ());
+      }
+      const uint64_t t0 = uint64_t (ipart) * nsamp_step;
+      for (uint64_t j = 0; j < nsamp_step; j++)
+      {
+        const C p = tim[0][nfilt_pos + j], q = tim[1][nfilt_pos + j];
+        float v = p.real () * p.real ();
+        v += p.imag () * p.imag ();
+        v += q.real () * q.real ();
+        v += q.imag () * q.imag ();
+        prof[binplan[t0 + j]] += v;
+      }
+    }
+  }
+  for (int t = 0; t < nt; t++)
+    for (unsigned b = 0; b < nbin; b++) profile[b] += partial[t][b];
+  return nout;
+}
+
+} // extern "C"

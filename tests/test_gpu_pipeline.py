@@ -1,0 +1,203 @@
+"""GPU parity of the fused unpack -> convolve -> detect -> fold pipeline
+against the oracle chain, block by block with the overlap carry
+(InputBuffering) and the per-block fold phase (Fold::fold, Fold.C:685-693)."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+# relative error of each folded profile bin against the oracle chain
+PROFILE_RTOL = 1e-5
+
+START = (60000, 3600, 0.25)
+EPOCH = (59999, 0, 0.0)
+
+
+def oracle_chain(orc, b2, raw_blocks, cfg, fp64=False):
+    """raw_blocks: list of TFPD arrays.  Mirrors SingleThread::run over the
+    blocks: unpack, overlap-save, detect, fold with one phase per block."""
+    nchan, npol = cfg["nchan"], cfg["npol"]
+    kind = cfg["kind"]
+    raw = np.concatenate([r.reshape(-1) for r in raw_blocks])
+    if kind == b2.INT8_TFPD:
+        ndat_tot = raw.size // (nchan * npol * 2)
+        x = orc.unpack8(raw, ndat_tot, nchan, npol, 2, cfg["lut"])
+    elif kind == b2.INT16_TFPD:
+        ndat_tot = raw.size // (nchan * npol * 2)
+        x = orc.unpack16(raw, ndat_tot, nchan, npol, 2, False)
+    else:
+        x = np.concatenate([r for r in raw_blocks], axis=2).view(np.float32)
+        ndat_tot = x.shape[2] // 2
+    x = x.view(np.complex64).reshape(nchan, npol, ndat_tot)
+    nfft, pos, neg = cfg["nfft"], cfg["pos"], cfg["neg"]
+    nk = nfft - pos - neg
+    if fp64:
+        h = orc.dedispersion_response_f64(cfg["cf"], cfg["bw"], cfg["dm"], nchan, nfft,
+                                          input_nchan=nchan)
+        y = orc.convolve(x.astype(np.complex128), h, nfft, pos, neg)
+    else:
+        h = orc.dedispersion_response(cfg["cf"], cfg["bw"], cfg["dm"], nchan, nfft,
+                                      input_nchan=nchan, mode=0)
+        y = orc.convolve(x, h, nfft, pos, neg)
+    if npol == 1:
+        d = (y.real ** 2 + y.imag ** 2)
+        d = d.reshape(nchan, 1, -1)
+    else:
+        d = orc.detect(y, cfg["state"])
+    rate = abs(cfg["bw"]) / nchan * 1e6
+    pps = (1.0 / rate) / cfg["period"]
+    nbin = cfg["nbin"]
+    prof = np.zeros((nchan, d.shape[1], nbin), d.dtype)
+    hits = np.zeros(nbin, np.uint32)
+    in0, carry = 0, 0
+    for r in raw_blocks:
+        nb = r.shape[-1] // 2 if kind == b2.FLOAT_FPT else r.size // (nchan * npol * 2)
+        ndat = carry + nb
+        npart = (ndat - pos - neg) // nk if ndat >= nfft else 0
+        nout = npart * nk
+        if nout:
+            phi = orc.fold_phi(START, EPOCH, in0 + pos, rate, cfg["period"])
+            plan = orc.fold_binplan(phi, pps, nout, nbin)
+            orc.fold_accumulate(np.ascontiguousarray(d[:, :, in0:in0 + nout]), plan, nbin,
+                                prof, hits)
+        in0 += nout
+        carry = ndat - nout
+    return prof, hits, in0
+
+
+def make_blocks(rng, cfg, sizes):
+    nchan, npol = cfg["nchan"], cfg["npol"]
+    blocks = []
+    for n in sizes:
+        if cfg["kind"] == b2mod().INT8_TFPD:
+            v = np.clip(np.round(rng.standard_normal(n * nchan * npol * 2) * 10), -128, 127)
+            blocks.append(v.astype(np.int8).view(np.uint8))
+        elif cfg["kind"] == b2mod().INT16_TFPD:
+            v = np.round(rng.standard_normal(n * nchan * npol * 2) * 300)
+            blocks.append(v.astype(np.int16))
+        else:
+            v = rng.standard_normal((nchan, npol, 2 * n)).astype(np.float32)
+            blocks.append(v)
+    return blocks
+
+
+def b2mod():
+    import dspsr_b200
+    return dspsr_b200
+
+
+def run_pipeline(ctx, b2, blocks, cfg, host=False):
+    c = b2.make_config(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nchan"], cfg["npol"], cfg["nfft"],
+                       cfg["pos"], cfg["neg"], cfg["nbin"], cfg["period"], state=cfg["state"],
+                       input_kind=cfg["kind"], lut=cfg["lut"], start_mjd=START, epoch_mjd=EPOCH,
+                       scratch_bytes=cfg.get("scratch", 0))
+    pl = b2.Pipeline(ctx, c)
+    total = 0
+    for r in blocks:
+        if cfg["kind"] == b2.FLOAT_FPT:
+            n = r.shape[-1] // 2
+            total += pl.run(torch.from_numpy(r).cuda(), n, n)
+        elif host:
+            n = r.size // (cfg["nchan"] * cfg["npol"] * 2)
+            total += pl.run_host(r, n)
+        else:
+            n = r.size // (cfg["nchan"] * cfg["npol"] * 2)
+            total += pl.run(torch.from_numpy(r).cuda(), n)
+    prof, hits = pl.get_profiles()
+    info = pl.info()
+    pl.close()
+    return prof, hits, total, info
+
+
+def base_cfg(b2, **kw):
+    cfg = dict(cf=1400.0, bw=16.0, dm=5.0, nchan=1, npol=2, nbin=256, period=0.0123,
+               state=b2.INTENSITY, kind=b2.INT8_TFPD, lut=b2.bittable8()[0])
+    cfg.update(kw)
+    pos, neg, nfft = b2.dispersion_plan(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nchan"],
+                                        cfg.get("nfft"))
+    cfg.update(pos=pos, neg=neg, nfft=nfft)
+    return cfg
+
+
+def check(prof, hits, total, rprof, rhits, rtotal, rtol=PROFILE_RTOL):
+    assert total == rtotal
+    assert np.array_equal(hits, rhits)
+    denom = np.maximum(np.abs(rprof), 1e-30)
+    scale = np.max(np.abs(rprof))
+    err = np.abs(prof - rprof)
+    # bins of signed products (coherence, Stokes) are compared against the
+    # largest bin of the same profile
+    rel = err / np.maximum(denom, 1e-3 * scale)
+    assert np.max(rel) < rtol, float(np.max(rel))
+
+
+CASES = {
+    # single-kernel path (nfft 8192), intensity, int8
+    "fused8k_int8": dict(dm=5.0),
+    # four-step path at the C1 physics (DM 67.99, 16 MHz, nfft 2^17)
+    "c1_fourstep": dict(dm=67.99, nfft=1 << 17, nbin=1024, period=0.08933),
+    # coherence products with int16 input, 4 channels, four-step 2^14
+    "coherence_int16": dict(dm=20.0, bw=64.0, nchan=4, nfft=1 << 14, state=2, kind=1, nbin=128),
+    # full Stokes on float FPT input, small scratch (many batches)
+    "stokes_float": dict(dm=3.0, bw=32.0, nchan=2, nfft=1 << 15, state=3, kind=2, nbin=512,
+                         scratch=8 << 20),
+    # one polarisation, intensity, fused 4096
+    "onepol_4096": dict(dm=1.0, npol=1, nfft=4096),
+}
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_pipeline_matches_oracle_chain(ctx, b2, orc, name):
+    cfg = base_cfg(b2, **CASES[name])
+    rng = np.random.default_rng(abs(hash(name)) % 1000)
+    nk = cfg["nfft"] - cfg["pos"] - cfg["neg"]
+    # three uneven blocks: the carry spans block boundaries
+    sizes = [cfg["nfft"] + 3 * nk + 17, 2 * nk - 5, nk + 1234]
+    blocks = make_blocks(rng, cfg, sizes)
+    prof, hits, total, info = run_pipeline(ctx, b2, blocks, cfg)
+    rprof, rhits, rtotal = oracle_chain(orc, b2, blocks, cfg)
+    check(prof, hits, total, rprof, rhits, rtotal)
+    rprof64, rhits64, _ = oracle_chain(orc, b2, blocks, cfg, fp64=True)
+    assert np.array_equal(hits, rhits64)
+
+
+def test_pipeline_host_input_matches_device_input(ctx, b2):
+    cfg = base_cfg(b2, dm=67.99, nfft=1 << 17, nbin=1024, period=0.08933)
+    rng = np.random.default_rng(1)
+    nk = cfg["nfft"] - cfg["pos"] - cfg["neg"]
+    blocks = make_blocks(rng, cfg, [cfg["nfft"] + 2 * nk, nk + 99])
+    a = run_pipeline(ctx, b2, blocks, cfg)
+    b = run_pipeline(ctx, b2, blocks, cfg, host=True)
+    assert a[2] == b[2]
+    assert np.array_equal(a[1], b[1])
+    assert np.max(np.abs(a[0] - b[0]) / a[0]) < 1e-6
+
+
+def test_pipeline_short_blocks_only_carry(ctx, b2):
+    """Blocks shorter than one FFT fold nothing and are carried forward."""
+    cfg = base_cfg(b2, dm=5.0)
+    rng = np.random.default_rng(2)
+    blocks = make_blocks(rng, cfg, [1000, 2000, 3000])
+    prof, hits, total, info = run_pipeline(ctx, b2, blocks, cfg)
+    assert total == 0 and hits.sum() == 0
+    blocks = make_blocks(rng, cfg, [1000, 2000, 3000, 9000])
+    prof, hits, total, info = run_pipeline(ctx, b2, blocks, cfg)
+    assert total > 0 and hits.sum() == total
+
+
+def test_pipeline_restores_dispersed_pulse(ctx, b2):
+    """A pulse train dispersed by an independent FP64 inverse chirp (numpy FFT
+    of the whole block) is restored: the folded profile peaks at the pulse
+    phase with the expected duty cycle."""
+    from dspsr_b200 import synth
+    cfg = base_cfg(b2, dm=67.99, nfft=1 << 17, nbin=256, period=0.005)
+    raw, truth = synth.dispersed_pulse_train(ndat=1 << 21, cf=cfg["cf"], bw=cfg["bw"], dm=cfg["dm"],
+                                             period=cfg["period"], duty=0.03, snr=50.0, sigma=10.0,
+                                             seed=3, start_mjd=START, epoch_mjd=EPOCH)
+    prof, hits, total, info = run_pipeline(ctx, b2, [raw], cfg)
+    p = prof[0, 0] / np.maximum(hits, 1)
+    on = np.argmax(p)
+    assert abs(((on + 0.5) / cfg["nbin"] - truth["phase"] + 0.5) % 1.0 - 0.5) < 0.03
+    assert (p.max() - np.median(p)) > 20 * np.std(p[np.abs(np.arange(256) - on) > 30])
