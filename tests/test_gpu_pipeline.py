@@ -1,6 +1,8 @@
 """GPU parity of the fused unpack -> convolve -> detect -> fold pipeline
 against the oracle chain, block by block with the overlap carry
 (InputBuffering) and the per-block fold phase (Fold::fold, Fold.C:685-693)."""
+import zlib
+
 import numpy as np
 import pytest
 
@@ -139,7 +141,7 @@ CASES = {
     # four-step path at the C1 physics (DM 67.99, 16 MHz, nfft 2^17)
     "c1_fourstep": dict(dm=67.99, nfft=1 << 17, nbin=1024, period=0.08933),
     # coherence products with int16 input, 4 channels, four-step 2^14
-    "coherence_int16": dict(dm=20.0, bw=64.0, nchan=4, nfft=1 << 14, state=2, kind=1, nbin=128),
+    "coherence_int16": dict(dm=5.0, bw=64.0, nchan=4, nfft=1 << 14, state=2, kind=1, nbin=128),
     # full Stokes on float FPT input, small scratch (many batches)
     "stokes_float": dict(dm=3.0, bw=32.0, nchan=2, nfft=1 << 15, state=3, kind=2, nbin=512,
                          scratch=8 << 20),
@@ -151,7 +153,7 @@ CASES = {
 @pytest.mark.parametrize("name", list(CASES))
 def test_pipeline_matches_oracle_chain(ctx, b2, orc, name):
     cfg = base_cfg(b2, **CASES[name])
-    rng = np.random.default_rng(abs(hash(name)) % 1000)
+    rng = np.random.default_rng(zlib.crc32(name.encode()))
     nk = cfg["nfft"] - cfg["pos"] - cfg["neg"]
     # three uneven blocks: the carry spans block boundaries
     sizes = [cfg["nfft"] + 3 * nk + 17, 2 * nk - 5, nk + 1234]
