@@ -228,7 +228,7 @@ def test_convolution_matches_oracle(ctx, b2, orc, nfft, nchan, pos, neg):
     c.close()
 
 
-@pytest.mark.parametrize("nchan,nfft,dm,bw", [(1, 1 << 17, 67.99, 16.0), (4, 8192, 30.0, 64.0),
+@pytest.mark.parametrize("nchan,nfft,dm,bw", [(1, 1 << 17, 67.99, 16.0), (4, 1 << 15, 30.0, 64.0),
                                               (2, 1 << 16, 500.0, -8.0)])
 def test_dedispersion_response_matches_oracle(ctx, b2, orc, nchan, nfft, dm, bw):
     pos = orc.smearing_samples(1400.0, bw, dm, nchan, 1)
@@ -249,6 +249,30 @@ def test_dedispersion_response_matches_oracle(ctx, b2, orc, nchan, nfft, dm, bw)
     assert np.max(np.abs(got - ref)) < 2 * 2.0 ** -24 * scale
     ref64 = orc.dedispersion_response_f64(1400.0, bw, dm, nchan, nfft, input_nchan=nchan)
     assert np.max(np.abs(got - ref64)) < 2.0 ** -23 * scale
+    c.close()
+
+
+@pytest.mark.parametrize("nchan,nfft,dm,bw", [(1, 1 << 17, 67.99, 16.0), (1, 8192, 5.0, 16.0),
+                                              (4, 1 << 15, 30.0, 64.0)])
+def test_dedispersed_voltages_within_2e6_of_fp64(ctx, b2, orc, nchan, nfft, dm, bw):
+    """Dedispersed voltages with the FP64-phase chirp against the all-FP64
+    oracle (FP64 response and FFT): relative RMS error <= 2e-6."""
+    rng = np.random.default_rng(nfft + nchan)
+    pos = orc.smearing_samples(1400.0, bw, dm, nchan, 1)
+    neg = orc.smearing_samples(1400.0, bw, dm, nchan, -1)
+    nk = nfft - pos - neg
+    ndat = nfft + 3 * nk
+    x = (np.round(rng.standard_normal((nchan, 2, ndat)) * 10)
+         + 1j * np.round(rng.standard_normal((nchan, 2, ndat)) * 10)).astype(np.complex64)
+    h64 = orc.dedispersion_response_f64(1400.0, bw, dm, nchan, nfft, input_nchan=nchan)
+    ref = orc.convolve(x.astype(np.complex128), h64, nfft, pos, neg)
+    c = b2.Convolution(ctx, nchan, 2, nfft, pos, neg)
+    c.set_dedispersion(1400.0, bw, dm, chirp_mode=b2.CHIRP_FP64)
+    out = torch.zeros((nchan, 2, 4 * nk), dtype=torch.complex64, device="cuda")
+    assert c.perform(dev(x), ndat, ndat, out, 4 * nk) == 4
+    ctx.synchronize()
+    got = out.cpu().numpy()
+    assert rel_rms(got, ref) < VOLTAGE_RTOL_FP64, rel_rms(got, ref)
     c.close()
 
 

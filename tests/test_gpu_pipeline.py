@@ -12,6 +12,8 @@ pytestmark = pytest.mark.gpu
 
 # relative error of each folded profile bin against the oracle chain
 PROFILE_RTOL = 1e-5
+# FP64-chirp pipeline against the all-FP64 oracle chain
+PROFILE_RTOL_FP64 = 5e-6
 
 START = (60000, 3600, 0.25)
 EPOCH = (59999, 0, 0.0)
@@ -94,7 +96,8 @@ def run_pipeline(ctx, b2, blocks, cfg, host=False):
     c = b2.make_config(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nchan"], cfg["npol"], cfg["nfft"],
                        cfg["pos"], cfg["neg"], cfg["nbin"], cfg["period"], state=cfg["state"],
                        input_kind=cfg["kind"], lut=cfg["lut"], start_mjd=START, epoch_mjd=EPOCH,
-                       scratch_bytes=cfg.get("scratch", 0))
+                       scratch_bytes=cfg.get("scratch", 0),
+                       chirp_mode=cfg.get("chirp", b2.CHIRP_REFERENCE))
     pl = b2.Pipeline(ctx, c)
     total = 0
     for r in blocks:
@@ -123,15 +126,27 @@ def base_cfg(b2, **kw):
     return cfg
 
 
-def check(prof, hits, total, rprof, rhits, rtotal, rtol=PROFILE_RTOL):
+def profile_scale(rprof, state):
+    """Per-(chan, bin) power scale of a folded profile: the profile itself for
+    intensity-like products, the total power PP+QQ (or Stokes I) for the
+    signed cross products, whose bins are sums with cancellation."""
+    if state in (0, 1):
+        return np.abs(rprof)
+    if state == 2:
+        s = rprof[:, 0:1] + rprof[:, 1:2]
+    else:
+        s = rprof[:, 0:1]
+    return np.broadcast_to(s, rprof.shape)
+
+
+def check(prof, hits, total, rprof, rhits, rtotal, state, rtol=PROFILE_RTOL):
     assert total == rtotal
     assert np.array_equal(hits, rhits)
-    denom = np.maximum(np.abs(rprof), 1e-30)
-    scale = np.max(np.abs(rprof))
-    err = np.abs(prof - rprof)
-    # bins of signed products (coherence, Stokes) are compared against the
-    # largest bin of the same profile
-    rel = err / np.maximum(denom, 1e-3 * scale)
+    scale = profile_scale(rprof.astype(np.float64), state)
+    empty = hits == 0
+    assert np.all(prof[..., empty] == 0)
+    err = np.abs(prof.astype(np.float64) - rprof)[..., ~empty]
+    rel = err / scale[..., ~empty]
     assert np.max(rel) < rtol, float(np.max(rel))
 
 
@@ -160,9 +175,13 @@ def test_pipeline_matches_oracle_chain(ctx, b2, orc, name):
     blocks = make_blocks(rng, cfg, sizes)
     prof, hits, total, info = run_pipeline(ctx, b2, blocks, cfg)
     rprof, rhits, rtotal = oracle_chain(orc, b2, blocks, cfg)
-    check(prof, hits, total, rprof, rhits, rtotal)
+    check(prof, hits, total, rprof, rhits, rtotal, cfg["state"])
+    # the FP64-chirp form against the FP64 oracle chain (FP64 response, FFT,
+    # detection and sums).  The reference-mode chirp rounds |phase| ~ 1e4 rad
+    # to float, which alone moves profiles by ~1e-5, so it is not compared here.
+    prof64, hits64, total64, _ = run_pipeline(ctx, b2, blocks, dict(cfg, chirp=b2.CHIRP_FP64))
     rprof64, rhits64, _ = oracle_chain(orc, b2, blocks, cfg, fp64=True)
-    assert np.array_equal(hits, rhits64)
+    check(prof64, hits64, total64, rprof64, rhits64, rtotal, cfg["state"], rtol=PROFILE_RTOL_FP64)
 
 
 def test_pipeline_host_input_matches_device_input(ctx, b2):
@@ -174,7 +193,7 @@ def test_pipeline_host_input_matches_device_input(ctx, b2):
     b = run_pipeline(ctx, b2, blocks, cfg, host=True)
     assert a[2] == b[2]
     assert np.array_equal(a[1], b[1])
-    assert np.max(np.abs(a[0] - b[0]) / a[0]) < 1e-6
+    check(a[0], a[1], a[2], b[0].astype(np.float64), b[1], b[2], cfg["state"], rtol=1e-6)
 
 
 def test_pipeline_short_blocks_only_carry(ctx, b2):
