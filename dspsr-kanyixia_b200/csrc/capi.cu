@@ -112,9 +112,11 @@ struct dspsr_b200_convolution
 {
   dspsr_b200_context* ctx = nullptr;
   ConvShape shape {};
-  DevBuf<float2> tw2, tw4, H, tmp, scratch;
+  DevBuf<float2> tw2, tw4, ptab, H, tmp, scratch;
   DevBuf<double> chan_par;
   DevBuf<float> lut;
+  DevBuf<int> err;
+  int nsm = 148;
   bool have_response = false;
   unsigned max_batch = 1;
 
@@ -125,9 +127,35 @@ struct dspsr_b200_convolution
     ConvTables t;
     t.tw2 = tw2.ptr;
     t.tw4 = tw4.ptr;
+    t.ptab = ptab.ptr;
     t.H = H.ptr;
     t.lut = lut.ptr;
+    t.err = err.ptr;
+    t.nsm = nsm;
     return t;
+  }
+  void release ()
+  {
+    tw2.release ();
+    tw4.release ();
+    ptab.release ();
+    H.release ();
+    tmp.release ();
+    scratch.release ();
+    chan_par.release ();
+    lut.release ();
+    err.release ();
+  }
+  // ESTATE when a bounded device wait of the row kernel gave up
+  int status ()
+  {
+    if (!err.ptr) return DSPSR_B200_OK;
+    int h = 0;
+    B200_CHECK (ctx, cudaMemcpyAsync (&h, err.ptr, sizeof (int), cudaMemcpyDeviceToHost,
+                                      ctx->stream), "read device status");
+    B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "device status sync");
+    if (h) return fail (ctx, DSPSR_B200_ESTATE, "a device-side wait timed out");
+    return DSPSR_B200_OK;
   }
 };
 
@@ -170,11 +198,33 @@ int dspsr_b200_convolution::init (dspsr_b200_context* c, unsigned nchan, unsigne
     std::vector<float2> t4 = make_tw4 (shape.n1, shape.n2);
     B200_CHECK (ctx, cudaMemcpy (tw4.ptr, t4.data (), t4.size () * sizeof (float2),
                                  cudaMemcpyHostToDevice), "copy tw4");
-    // parts in flight: keep the scratch near the L2 size unless told otherwise
+    const unsigned ntab = pass_tables_count (shape.n2);
+    std::vector<float2> pt (ntab);
+    make_pass_tables (shape.n2, pt.data (), ntab);
+    B200_CHECK (ctx, ptab.reserve (ntab), "cudaMalloc pass tables");
+    B200_CHECK (ctx, cudaMemcpy (ptab.ptr, pt.data (), ntab * sizeof (float2),
+                                 cudaMemcpyHostToDevice), "copy pass tables");
+    B200_CHECK (ctx, err.reserve (1), "cudaMalloc status flag");
+    B200_CHECK (ctx, cudaMemset (err.ptr, 0, sizeof (int)), "clear status flag");
+    int dev = 0;
+    B200_CHECK (ctx, cudaGetDevice (&dev), "cudaGetDevice");
+    B200_CHECK (ctx, cudaDeviceGetAttribute (&nsm, cudaDevAttrMultiProcessorCount, dev),
+                "multiprocessor count");
+    // Parts in flight: the scratch stays near the L2 size unless told
+    // otherwise, and the batch is chosen so that its rows spread evenly over
+    // the persistent row kernel's CTAs.
     const uint64_t per_part = uint64_t (nchan) * npol * nfft * sizeof (float2);
-    const uint64_t budget = scratch_bytes ? scratch_bytes : (uint64_t (48) << 20);
-    max_batch = unsigned (std::max<uint64_t> (1, budget / per_part));
-    if (max_batch > 65535) max_batch = 65535;
+    const uint64_t budget = scratch_bytes ? scratch_bytes : (uint64_t (96) << 20);
+    const uint64_t bmax = std::max<uint64_t> (1, std::min<uint64_t> (65535, budget / per_part));
+    const uint64_t rows_per_part = uint64_t (shape.n1) * nchan * npol;
+    const uint64_t ctas = uint64_t (nsm) * (shape.n2 >= 8192 ? 1 : 2);
+    max_batch = unsigned (bmax);
+    for (uint64_t b = bmax; b >= std::max<uint64_t> (1, bmax / 2); b--)
+      if ((b * rows_per_part) % ctas == 0)
+      {
+        max_batch = unsigned (b);
+        break;
+      }
     B200_CHECK (ctx, scratch.reserve (uint64_t (max_batch) * nchan * npol * nfft),
                 "cudaMalloc scratch");
   }
@@ -611,15 +661,16 @@ int dspsr_b200_convolution_create (dspsr_b200_context* ctx, unsigned nchan, unsi
 int dspsr_b200_convolution_destroy (dspsr_b200_convolution* c)
 {
   if (!c) return DSPSR_B200_EINVAL;
-  c->tw2.release ();
-  c->tw4.release ();
-  c->H.release ();
-  c->tmp.release ();
-  c->scratch.release ();
-  c->chan_par.release ();
-  c->lut.release ();
+  if (c->ctx) cudaStreamSynchronize (c->ctx->stream);
+  c->release ();
   delete c;
   return DSPSR_B200_OK;
+}
+
+int dspsr_b200_convolution_status (dspsr_b200_convolution* c)
+{
+  if (!c) return DSPSR_B200_EINVAL;
+  return c->status ();
 }
 
 int dspsr_b200_convolution_copy_response (dspsr_b200_convolution* c, const float* response)
@@ -884,13 +935,7 @@ int dspsr_b200_pipeline_destroy (dspsr_b200_pipeline* pl)
 {
   if (!pl) return DSPSR_B200_EINVAL;
   if (pl->ctx) cudaStreamSynchronize (pl->ctx->stream);
-  pl->conv.tw2.release ();
-  pl->conv.tw4.release ();
-  pl->conv.H.release ();
-  pl->conv.tmp.release ();
-  pl->conv.scratch.release ();
-  pl->conv.chan_par.release ();
-  pl->conv.lut.release ();
+  pl->conv.release ();
   pl->fold.release ();
   pl->carry[0].release ();
   pl->carry[1].release ();
@@ -927,7 +972,9 @@ int dspsr_b200_pipeline_run_host (dspsr_b200_pipeline* pl, const void* h_in, uin
 int dspsr_b200_pipeline_get_profiles (dspsr_b200_pipeline* pl, float* profiles, uint32_t* hits)
 {
   if (!pl) return DSPSR_B200_EINVAL;
-  return dspsr_b200_fold_get_profiles (&pl->fold, profiles, hits);
+  int rc = dspsr_b200_fold_get_profiles (&pl->fold, profiles, hits);
+  if (rc) return rc;
+  return pl->conv.status ();
 }
 
 int dspsr_b200_pipeline_reset (dspsr_b200_pipeline* pl)

@@ -13,6 +13,7 @@
 #include <stdint.h>
 
 #define B200_HD __host__ __device__ __forceinline__
+#define B200_CE __host__ __device__ constexpr
 
 namespace b200 {
 
@@ -30,7 +31,7 @@ B200_HD float2 cmulc (float2 a, float2 b)
 B200_HD float2 cscale (float2 a, float s) { return make_float2 (a.x * s, a.y * s); }
 
 // cos(2 pi j / 64) for j = 0..16, correctly rounded decimal expansions.
-B200_HD constexpr float quarter_cos64 (int j)
+B200_CE float quarter_cos64 (int j)
 {
   return j == 0 ? 1.0f
        : j == 1 ? 0.99518472667219692873f
@@ -52,14 +53,14 @@ B200_HD constexpr float quarter_cos64 (int j)
 }
 
 // cos and sin of 2 pi j / 64 for any integer j (reduced to the first quadrant)
-B200_HD constexpr float cos64 (int j)
+B200_CE float cos64 (int j)
 {
   return (j & 63) <= 16 ? quarter_cos64 (j & 63)
        : (j & 63) <= 32 ? -quarter_cos64 (32 - (j & 63))
        : (j & 63) <= 48 ? -quarter_cos64 ((j & 63) - 32)
        : quarter_cos64 (64 - (j & 63));
 }
-B200_HD constexpr float sin64 (int j) { return cos64 (j - 16); }
+B200_CE float sin64 (int j) { return cos64 (j - 16); }
 
 // v * w_R^k with w_R = exp(D 2 pi i / R); k is a compile-time constant after
 // unrolling, so the special cases cost nothing.
@@ -132,12 +133,12 @@ struct RegDFT<1, D>
 // Shared-memory index padding: one float2 of padding per 16 entries keeps the
 // strided Stockham stores of the early passes off a single bank.
 B200_HD int spad (int i) { return i + (i >> 4); }
-B200_HD constexpr int spad_size (int n) { return n + (n >> 4); }
+B200_CE int spad_size (int n) { return n + (n >> 4); }
 
 // Stockham pass schedule for an N-point transform run by T = N/16 threads:
 // every pass leaves each thread exactly 16 complex values in registers.
 // Returns the radix of pass p (0 when there is no such pass).
-B200_HD constexpr int stockham_radix (int N, int p)
+B200_CE int stockham_radix (int N, int p)
 {
   return N == 16384 ? (p < 3 ? 16 : p == 3 ? 4 : 0)
        : N == 8192 ? (p < 3 ? 16 : p == 3 ? 2 : 0)
@@ -149,7 +150,7 @@ B200_HD constexpr int stockham_radix (int N, int p)
        : 0;
 }
 
-B200_HD constexpr int stockham_npass (int N)
+B200_CE int stockham_npass (int N)
 {
   return stockham_radix (N, 0) == 0 ? 0
        : stockham_radix (N, 1) == 0 ? 1
@@ -158,13 +159,13 @@ B200_HD constexpr int stockham_npass (int N)
 }
 
 // product of the radices of passes before p
-B200_HD constexpr int stockham_ns (int N, int p)
+B200_CE int stockham_ns (int N, int p)
 {
   return p == 0 ? 1 : stockham_ns (N, p - 1) * stockham_radix (N, p - 1);
 }
 
 // threads of an N-point transform
-B200_HD constexpr int stockham_threads (int N) { return N / 16; }
+B200_CE int stockham_threads (int N) { return N / 16; }
 
 // One radix-R Stockham pass (Govindaraju et al., SC08, "High performance
 // discrete Fourier transforms on graphics processors"): butterfly j reads
@@ -213,6 +214,73 @@ struct StockhamPass
 #pragma unroll
       for (int r = 0; r < R; r++)
         s[spad (idxD + r * Ns)] = x[r];
+    }
+  }
+};
+
+// Per-pass twiddle tables: pass p >= 1 of an N-point schedule uses
+// w_{Ns R}^{a r} for a < Ns, 1 <= r < R, stored [r-1][a] (a fastest) so that
+// lanes holding consecutive butterflies read consecutive entries.
+B200_CE int pass_table_size (int N, int p)
+{
+  return p == 0 ? 0 : stockham_ns (N, p) * (stockham_radix (N, p) - 1);
+}
+B200_CE int pass_table_offset (int N, int p)
+{
+  return p <= 1 ? 0 : pass_table_offset (N, p - 1) + pass_table_size (N, p - 1);
+}
+B200_CE int pass_tables_size (int N)
+{
+  return pass_table_offset (N, stockham_npass (N) - 1)
+         + pass_table_size (N, stockham_npass (N) - 1);
+}
+
+// The same radix-R pass with its twiddles from a per-pass table and with the
+// source / destination layouts chosen by the caller: PADI/PADO select the
+// padded shared-memory layout (spad) for input/output; an unpadded side may
+// be a staging buffer or global memory.
+template <int N, int R, int T, int D, bool PADI, bool PADO>
+struct StockhamPassT
+{
+  static constexpr int NB = N / R;
+  static constexpr int BPT = NB / T;
+  static_assert (BPT >= 1 && BPT * T == NB, "thread count does not tile the pass");
+
+  B200_HD static void load (int tid, const float2* s, float2* v)
+  {
+#pragma unroll
+    for (int b = 0; b < BPT; b++)
+    {
+      const int j = tid + b * T;
+#pragma unroll
+      for (int r = 0; r < R; r++)
+        v[b * R + r] = s[PADI ? spad (j + r * NB) : j + r * NB];
+    }
+  }
+
+  // twp: this pass's table ([r-1][a], Ns entries per r) or null when Ns == 1
+  B200_HD static void compute_store (int tid, int Ns, float2* v, float2* s, const float2* twp)
+  {
+#pragma unroll
+    for (int b = 0; b < BPT; b++)
+    {
+      const int j = tid + b * T;
+      const int a = j & (Ns - 1);
+      float2* x = v + b * R;
+      if (Ns > 1)
+      {
+#pragma unroll
+        for (int r = 1; r < R; r++)
+        {
+          const float2 w = twp[(r - 1) * Ns + a];
+          x[r] = D < 0 ? cmul (x[r], w) : cmulc (x[r], w);
+        }
+      }
+      RegDFT<R, D>::run (x);
+      const int idxD = (j - a) * R + a;
+#pragma unroll
+      for (int r = 0; r < R; r++)
+        s[PADO ? spad (idxD + r * Ns) : idxD + r * Ns] = x[r];
     }
   }
 };

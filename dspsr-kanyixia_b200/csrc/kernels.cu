@@ -25,6 +25,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 
 namespace b200 {
@@ -256,9 +257,10 @@ __device__ __forceinline__ void smem_fft (float2* s, const float2* tw)
 // --------------------------------------------------------------------------
 
 template <int N1, int KIND>
-__global__ void __launch_bounds__ (128, 4)
+__global__ void __launch_bounds__ (128, 2)
 k_fwd_cols (const InputView in, const float* __restrict__ lut, const uint64_t nkeep,
-            const uint64_t part0, const unsigned n2, float2* __restrict__ scratch)
+            const uint64_t part0, const unsigned n2, const float2* __restrict__ tw4,
+            float2* __restrict__ scratch)
 {
   __shared__ float s_lut[256];
   load_lut (in, lut, s_lut);
@@ -275,6 +277,10 @@ k_fwd_cols (const InputView in, const float* __restrict__ lut, const uint64_t nk
     for (int k = 0; k < N1; k++)
       v[k] = fetch<KIND> (in, s_lut, c, p, t0 + uint64_t (k) * n2);
     RegDFT<N1, -1>::run (v);
+    // four-step twiddle w_N^{k1 n2} (row k1 of the [n1][n2] table; coalesced)
+#pragma unroll
+    for (int k = 1; k < N1; k++)
+      v[k] = cmul (v[k], __ldg (tw4 + uint64_t (k) * n2 + i2));
     float2* dst = scratch + ((uint64_t (b) * in.nchan + c) * in.npol + p) * N + i2;
 #pragma unroll
     for (int k = 0; k < N1; k++)
@@ -283,39 +289,178 @@ k_fwd_cols (const InputView in, const float* __restrict__ lut, const uint64_t nk
 }
 
 // --------------------------------------------------------------------------
-// K2: rows -- twiddle, FFT, response, inverse FFT, conjugate twiddle
+// K2 (persistent): one CTA per SM walks the rows.  The next row is fetched
+// into a staging buffer by the bulk-copy engine (cp.async.bulk, completion on
+// an mbarrier) while the current row is transformed; the per-pass twiddle
+// tables stay resident in shared memory.  Row r holds n2 contiguous values,
+// r = ((b*nchan + c)*npol + p)*n1 + k1.
 // --------------------------------------------------------------------------
 
-template <int N2, int T>
-__global__ void __launch_bounds__ (T, 512 / T)
-k_rows (float2* __restrict__ scratch, const float2* __restrict__ tw4,
-        const float2* __restrict__ tw2, const float2* __restrict__ H, const unsigned n1,
-        const unsigned nchan, const unsigned npol)
+__device__ __forceinline__ uint32_t smem_u32 (const void* p)
 {
-  extern __shared__ float2 s[];
-  const unsigned k1 = blockIdx.x;
-  const unsigned b = blockIdx.y;
-  const unsigned cp = blockIdx.z;
-  const unsigned c = cp / npol;
-  const uint64_t N = uint64_t (n1) * N2;
-  float2* row = scratch + (uint64_t (b) * nchan * npol + cp) * N + uint64_t (k1) * N2;
-  const float2* twr = tw4 + uint64_t (k1) * N2;
-  for (int i = threadIdx.x; i < N2; i += T)
-    s[spad (i)] = cmul (row[i], __ldg (twr + i));
-  __syncthreads ();
-  smem_fft<N2, T, -1> (s, tw2);
-  const float2* h = H + (uint64_t (c) * n1 + k1) * N2;
-  for (int i = threadIdx.x; i < N2; i += T)
+  return static_cast<uint32_t> (__cvta_generic_to_shared (p));
+}
+
+__device__ __forceinline__ void mbar_init (uint64_t* bar, unsigned count)
+{
+  asm volatile ("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32 (bar)), "r"(count)
+                : "memory");
+  asm volatile ("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx (uint64_t* bar, unsigned bytes)
+{
+  asm volatile ("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32 (bar)),
+                "r"(bytes)
+                : "memory");
+}
+
+// global -> shared bulk copy (16-byte aligned, multiple of 16 bytes),
+// completing `bytes` transactions on the mbarrier; no multicast
+__device__ __forceinline__ void bulk_g2s (void* dst, const void* src, unsigned bytes,
+                                          uint64_t* bar)
+{
+  asm volatile (
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32 (dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32 (bar))
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait (uint64_t* bar, unsigned parity)
+{
+  uint32_t ok;
+  asm volatile (
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32 (bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: gives up after ~2^21 polls (about a second) and reports it.
+__device__ __forceinline__ bool mbar_wait_bounded (uint64_t* bar, unsigned parity)
+{
+  for (int it = 0; it < (1 << 21); it++)
+    if (mbar_try_wait (bar, parity)) return true;
+  return false;
+}
+
+template <int N>
+constexpr size_t rows_smem_bytes ()
+{
+  return size_t (N + spad_size (N) + pass_tables_size (N)) * sizeof (float2);
+}
+
+template <int N, int D, int P, bool PI, bool PO>
+__device__ __forceinline__ void tpass (const float2* src, float2* dst, float2* v,
+                                       const float2* tab)
+{
+  if constexpr (P < stockham_npass (N))
   {
-    // Response::operate (Response.C:662-726): (f_r d_r - f_i d_i, f_i d_r + f_r d_i)
-    const float2 d = s[spad (i)];
-    const float2 f = __ldg (h + i);
-    s[spad (i)] = make_float2 (d.x * f.x - d.y * f.y, d.x * f.y + d.y * f.x);
+    constexpr int T = stockham_threads (N);
+    constexpr int R = stockham_radix (N, P);
+    constexpr int Ns = stockham_ns (N, P);
+    StockhamPassT<N, R, T, D, PI, PO>::load (threadIdx.x, src, v);
+    __syncthreads ();
+    StockhamPassT<N, R, T, D, PI, PO>::compute_store (
+        threadIdx.x, Ns, v, dst, P ? tab + pass_table_offset (N, P) : nullptr);
+    __syncthreads ();
   }
+}
+
+template <int N2>
+__global__ void __launch_bounds__ (stockham_threads (N2), 1)
+k_rows_tma (float2* __restrict__ scratch, const float2* __restrict__ ptab,
+            const float2* __restrict__ H, const unsigned n1, const unsigned nchan,
+            const unsigned npol, const unsigned nrows, int* __restrict__ err)
+{
+  constexpr int T = stockham_threads (N2);
+  constexpr int NP = stockham_npass (N2);
+  constexpr int TABN = pass_tables_size (N2);
+  constexpr unsigned ROW_BYTES = N2 * sizeof (float2);
+  constexpr unsigned CHUNK = 16384;
+  static_assert (NP == 3 || NP == 4, "row kernel supports 3 or 4 Stockham passes");
+  extern __shared__ __align__ (128) unsigned char smraw[];
+  float2* stage = reinterpret_cast<float2*> (smraw);
+  float2* work = stage + N2;
+  float2* tab = work + spad_size (N2);
+  __shared__ __align__ (8) uint64_t bar;
+  const int tid = threadIdx.x;
+
+  for (int i = tid; i < TABN; i += T) tab[i] = __ldg (ptab + i);
+  if (tid == 0) mbar_init (&bar, 1);
   __syncthreads ();
-  smem_fft<N2, T, +1> (s, tw2);
-  for (int i = threadIdx.x; i < N2; i += T)
-    row[i] = cmulc (s[spad (i)], __ldg (twr + i));
+
+  unsigned row = blockIdx.x;
+  if (tid == 0 && row < nrows)
+  {
+    mbar_expect_tx (&bar, ROW_BYTES);
+    const char* src = reinterpret_cast<const char*> (scratch + uint64_t (row) * N2);
+    for (unsigned o = 0; o < ROW_BYTES; o += CHUNK)
+      bulk_g2s (reinterpret_cast<char*> (stage) + o, src + o, CHUNK, &bar);
+  }
+  unsigned parity = 0;
+  float2 v[16];
+  for (; row < nrows; row += gridDim.x)
+  {
+    if (!mbar_wait_bounded (&bar, parity))
+    {
+      if (tid == 0) atomicExch (err, 1);
+      mbar_wait_bounded (&bar, parity);   // let the copy in flight land
+      return;
+    }
+    parity ^= 1;
+    const unsigned k1 = row % n1;
+    const unsigned c = (row / n1 / npol) % nchan;
+    float2* grow = scratch + uint64_t (row) * N2;
+
+    // forward pass 0 reads the staged row; once every thread has its values
+    // the staging buffer is refilled with the next row in the background
+    {
+      constexpr int R0 = stockham_radix (N2, 0);
+      StockhamPassT<N2, R0, T, -1, false, true>::load (tid, stage, v);
+      __syncthreads ();
+      const unsigned next = row + gridDim.x;
+      if (tid == 0 && next < nrows)
+      {
+        mbar_expect_tx (&bar, ROW_BYTES);
+        const char* src = reinterpret_cast<const char*> (scratch + uint64_t (next) * N2);
+        for (unsigned o = 0; o < ROW_BYTES; o += CHUNK)
+          bulk_g2s (reinterpret_cast<char*> (stage) + o, src + o, CHUNK, &bar);
+      }
+      StockhamPassT<N2, R0, T, -1, false, true>::compute_store (tid, 1, v, work, nullptr);
+      __syncthreads ();
+    }
+    tpass<N2, -1, 1, true, true> (work, work, v, tab);
+    tpass<N2, -1, 2, true, true> (work, work, v, tab);
+    tpass<N2, -1, 3, true, true> (work, work, v, tab);
+
+    // Response::operate (Response.C:662-726): (f_r d_r - f_i d_i, f_i d_r + f_r d_i)
+    const float2* h = H + (uint64_t (c) * n1 + k1) * N2;
+#pragma unroll
+    for (int q = 0; q < 16; q++)
+    {
+      const int i = tid + q * T;
+      const float2 d = work[spad (i)];
+      const float2 f = __ldg (h + i);
+      work[spad (i)] = make_float2 (d.x * f.x - d.y * f.y, d.x * f.y + d.y * f.x);
+    }
+    __syncthreads ();
+
+    // inverse: all but the last pass in shared memory, the last straight to HBM
+    tpass<N2, +1, 0, true, true> (work, work, v, tab);
+    tpass<N2, +1, 1, true, true> (work, work, v, tab);
+    if constexpr (NP == 3)
+      tpass<N2, +1, 2, true, false> (work, grow, v, tab);
+    else
+    {
+      tpass<N2, +1, 2, true, true> (work, work, v, tab);
+      tpass<N2, +1, 3, true, false> (work, grow, v, tab);
+    }
+  }
 }
 
 // --------------------------------------------------------------------------
@@ -326,12 +471,16 @@ template <int N1, int NPOL, int MODE, int NOUT>
 __global__ void __launch_bounds__ (128, 4)
 k_inv_cols (const float2* __restrict__ scratch, const unsigned n2, const unsigned nchan,
             const uint64_t nkeep, const unsigned nfilt_pos, const uint64_t part0,
-            const FoldView fv, const VoltView vv)
+            const float2* __restrict__ tw4, const FoldView fv, const VoltView vv)
 {
   const unsigned i2 = blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned b = blockIdx.y;
   const unsigned c = blockIdx.z;
   const uint64_t N = uint64_t (N1) * n2;
+  float2 w[N1];
+#pragma unroll
+  for (int k = 1; k < N1; k++)
+    w[k] = __ldg (tw4 + uint64_t (k) * n2 + i2);
   float2 v[NPOL][N1];
 #pragma unroll
   for (int p = 0; p < NPOL; p++)
@@ -340,6 +489,10 @@ k_inv_cols (const float2* __restrict__ scratch, const unsigned n2, const unsigne
 #pragma unroll
     for (int k = 0; k < N1; k++)
       v[p][k] = src[uint64_t (k) * n2];
+    // conjugate four-step twiddle, then the inverse n1-point DFT
+#pragma unroll
+    for (int k = 1; k < N1; k++)
+      v[p][k] = cmulc (v[p][k], w[k]);
     RegDFT<N1, +1>::run (v[p]);
   }
   const uint64_t tbase = (part0 + b) * nkeep;
@@ -573,19 +726,23 @@ __global__ void k_binplan (const FoldSegment* __restrict__ segs, const int nseg,
 
 template <int N1, int NPOL, int MODE, int NOUT>
 void launch_inv (const ConvShape& sh, dim3 grid, float2* scratch, uint64_t part0,
-                 const FoldView& fv, const VoltView& vv, cudaStream_t st)
+                 const ConvTables& tb, const FoldView& fv, const VoltView& vv, cudaStream_t st)
 {
   k_inv_cols<N1, NPOL, MODE, NOUT><<<grid, 128, 0, st>>> (scratch, sh.n2, sh.nchan, sh.nkeep,
-                                                          sh.nfilt_pos, part0, fv, vv);
+                                                          sh.nfilt_pos, part0, tb.tw4, fv, vv);
 }
 
 template <int N2>
-void launch_rows (dim3 grid, float2* scratch, const ConvTables& tb, unsigned n1,
+void launch_rows (unsigned nrows, float2* scratch, const ConvTables& tb, unsigned n1,
                   const ConvShape& sh, cudaStream_t st)
 {
   constexpr int T = stockham_threads (N2);
-  const size_t smem = spad_size (N2) * sizeof (float2);
-  k_rows<N2, T><<<grid, T, smem, st>>> (scratch, tb.tw4, tb.tw2, tb.H, n1, sh.nchan, sh.npol);
+  // persistent: as many CTAs as fit at once (shared memory allows 1 per SM at
+  // n2 = 8192 and 2 at n2 = 4096)
+  const unsigned per_sm = N2 >= 8192 ? 1 : 2;
+  const unsigned grid = std::min<unsigned> (nrows, per_sm * unsigned (tb.nsm));
+  k_rows_tma<N2><<<grid, T, rows_smem_bytes<N2> (), st>>> (scratch, tb.ptab, tb.H, n1, sh.nchan,
+                                                           sh.npol, nrows, tb.err);
 }
 
 template <int N1>
@@ -598,34 +755,43 @@ cudaError_t run_fourstep_n1 (const ConvShape& sh, const ConvTables& tb, const In
   {
   ClockScope cs (clk, KK_FWD_COLS, st);
   if (in.kind == IN_INT8)
-    k_fwd_cols<N1, IN_INT8><<<gcol, 128, 0, st>>> (in, tb.lut, sh.nkeep, part0, sh.n2, scratch);
+    k_fwd_cols<N1, IN_INT8><<<gcol, 128, 0, st>>> (in, tb.lut, sh.nkeep, part0, sh.n2, tb.tw4,
+                                                   scratch);
   else if (in.kind == IN_INT16)
-    k_fwd_cols<N1, IN_INT16><<<gcol, 128, 0, st>>> (in, tb.lut, sh.nkeep, part0, sh.n2, scratch);
+    k_fwd_cols<N1, IN_INT16><<<gcol, 128, 0, st>>> (in, tb.lut, sh.nkeep, part0, sh.n2, tb.tw4,
+                                                    scratch);
   else
-    k_fwd_cols<N1, IN_FLOAT><<<gcol, 128, 0, st>>> (in, tb.lut, sh.nkeep, part0, sh.n2, scratch);
+    k_fwd_cols<N1, IN_FLOAT><<<gcol, 128, 0, st>>> (in, tb.lut, sh.nkeep, part0, sh.n2, tb.tw4,
+                                                    scratch);
   }
-  const dim3 grow (N1, nbatch, sh.nchan * sh.npol);
+  const unsigned nrows = N1 * nbatch * sh.nchan * sh.npol;
   {
   ClockScope cs (clk, KK_ROWS, st);
   if (sh.n2 == 8192)
-    launch_rows<8192> (grow, scratch, tb, N1, sh, st);
+    launch_rows<8192> (nrows, scratch, tb, N1, sh, st);
   else if (sh.n2 == 4096)
-    launch_rows<4096> (grow, scratch, tb, N1, sh, st);
+    launch_rows<4096> (nrows, scratch, tb, N1, sh, st);
   else
     return cudaErrorInvalidValue;
   }
   ClockScope cs (clk, KK_INV_COLS, st);
   if (sh.npol == 2)
   {
-    if (mode == OUT_VOLTAGE) launch_inv<N1, 2, OUT_VOLTAGE, 1> (sh, gcol, scratch, part0, fv, vv, st);
-    else if (fv.nout == 1) launch_inv<N1, 2, OUT_FOLD, 1> (sh, gcol, scratch, part0, fv, vv, st);
-    else if (fv.nout == 2) launch_inv<N1, 2, OUT_FOLD, 2> (sh, gcol, scratch, part0, fv, vv, st);
-    else launch_inv<N1, 2, OUT_FOLD, 4> (sh, gcol, scratch, part0, fv, vv, st);
+    if (mode == OUT_VOLTAGE)
+      launch_inv<N1, 2, OUT_VOLTAGE, 1> (sh, gcol, scratch, part0, tb, fv, vv, st);
+    else if (fv.nout == 1)
+      launch_inv<N1, 2, OUT_FOLD, 1> (sh, gcol, scratch, part0, tb, fv, vv, st);
+    else if (fv.nout == 2)
+      launch_inv<N1, 2, OUT_FOLD, 2> (sh, gcol, scratch, part0, tb, fv, vv, st);
+    else
+      launch_inv<N1, 2, OUT_FOLD, 4> (sh, gcol, scratch, part0, tb, fv, vv, st);
   }
   else
   {
-    if (mode == OUT_VOLTAGE) launch_inv<N1, 1, OUT_VOLTAGE, 1> (sh, gcol, scratch, part0, fv, vv, st);
-    else launch_inv<N1, 1, OUT_FOLD, 1> (sh, gcol, scratch, part0, fv, vv, st);
+    if (mode == OUT_VOLTAGE)
+      launch_inv<N1, 1, OUT_VOLTAGE, 1> (sh, gcol, scratch, part0, tb, fv, vv, st);
+    else
+      launch_inv<N1, 1, OUT_FOLD, 1> (sh, gcol, scratch, part0, tb, fv, vv, st);
   }
   return cudaGetLastError ();
 }
@@ -676,14 +842,42 @@ cudaError_t run_fused (const ConvShape& sh, const ConvTables& tb, const InputVie
 template <int N2>
 cudaError_t set_rows_smem ()
 {
-  const int smem = spad_size (N2) * sizeof (float2);
-  return cudaFuncSetAttribute (k_rows<N2, stockham_threads (N2)>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  return cudaFuncSetAttribute (k_rows_tma<N2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int (rows_smem_bytes<N2> ()));
 }
 
 } // namespace
 
 uint64_t kernel_launches () { return g_launches.load (); }
+
+unsigned pass_tables_count (unsigned n)
+{
+  switch (n)
+  {
+    case 4096: return pass_tables_size (4096);
+    case 8192: return pass_tables_size (8192);
+    default: return 0;
+  }
+}
+
+// w_{Ns R}^{a r} rounded once from double precision, [r-1][a] per pass
+void make_pass_tables (unsigned n, float2* out, unsigned capacity)
+{
+  const int N = int (n);
+  for (int p = 1; p < stockham_npass (N); p++)
+  {
+    const int Ns = stockham_ns (N, p), R = stockham_radix (N, p);
+    const int off = pass_table_offset (N, p);
+    for (int r = 1; r < R; r++)
+      for (int a = 0; a < Ns; a++)
+      {
+        const unsigned idx = unsigned (off + (r - 1) * Ns + a);
+        if (idx >= capacity) return;
+        const double ang = -2.0 * 3.14159265358979323846 * double (a) * r / (double (Ns) * R);
+        out[idx] = make_float2 (float (cos (ang)), float (sin (ang)));
+      }
+  }
+}
 
 cudaError_t launch_convolution (const ConvShape& sh, const ConvTables& tb, const InputView& in,
                                 uint64_t part0, unsigned nbatch, float2* scratch, int mode,
@@ -700,13 +894,16 @@ cudaError_t launch_convolution (const ConvShape& sh, const ConvTables& tb, const
       default: return cudaErrorInvalidValue;
     }
   }
-  static bool attr_done = false;
-  if (!attr_done)
+  // the shared-memory opt-in is per device
+  static unsigned attr_done = 0;
+  int dev = 0;
+  cudaGetDevice (&dev);
+  if (dev < 32 && !(attr_done & (1u << dev)))
   {
     cudaError_t e = set_rows_smem<8192> ();
     if (e == cudaSuccess) e = set_rows_smem<4096> ();
     if (e != cudaSuccess) return e;
-    attr_done = true;
+    attr_done |= 1u << dev;
   }
   switch (sh.n1)
   {

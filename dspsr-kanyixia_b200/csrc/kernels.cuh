@@ -57,9 +57,17 @@ struct ConvTables
 {
   const float2* tw2;         // n2-point table exp(-2 pi i m / n2)
   const float2* tw4;         // [n1][n2] exp(-2 pi i k1 n2 / nfft), null when n1 == 1
+  const float2* ptab;        // per-pass Stockham twiddle tables of the n2-point FFT
   const float2* H;           // [nchan][n1][n2] response in four-step order
   const float* lut;          // 8-bit lookup table (device), 256 floats
+  int* err;                  // device flag: set when a bounded wait gave up
+  int nsm;                   // multiprocessors of the device
 };
+
+// Per-pass Stockham twiddle tables of an n-point transform, as the row
+// kernel reads them (fft_core.cuh pass_table_offset layout).
+void make_pass_tables (unsigned n, float2* out, unsigned capacity);
+unsigned pass_tables_count (unsigned n);
 
 // Kernels of the convolution path, for per-kernel timing.
 enum KernelKind { KK_FWD_COLS = 0, KK_ROWS = 1, KK_INV_COLS = 2, KK_FUSED = 3, KK_COUNT = 4 };

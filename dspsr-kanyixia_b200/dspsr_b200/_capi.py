@@ -83,6 +83,7 @@ SIGNATURES = {
     "dspsr_b200_convolution_set_dedispersion": (c_int, [c_vp, c_dbl, c_dbl, c_dbl, c_int, c_int,
                                                         c_int, c_int, c_uint]),
     "dspsr_b200_convolution_get_response": (c_int, [c_vp, c_fp]),
+    "dspsr_b200_convolution_status": (c_int, [c_vp]),
     "dspsr_b200_convolution_perform": (c_int, [c_vp, c_vp, c_u64, c_u64, c_vp, c_u64, c_u64p]),
     "dspsr_b200_detect": (c_int, [c_vp, c_vp, c_u64, c_u64, c_uint, c_int, c_vp, c_u64]),
     "dspsr_b200_fold_create": (c_int, [c_vp, c_uint, c_uint, c_uint, ctypes.POINTER(c_vp)]),

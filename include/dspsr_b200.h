@@ -141,6 +141,10 @@ int dspsr_b200_convolution_set_dedispersion (dspsr_b200_convolution* conv,
                                              double dm, int input_nchan, int dual_sideband,
                                              int dc_centred, int chirp_mode,
                                              unsigned norm_nfft);
+/* Blocks until the engine's queued work is done and returns DSPSR_B200_ESTATE
+   if one of its device-side waits gave up (each wait is bounded to about a
+   second; see the row kernel), DSPSR_B200_OK otherwise. */
+int dspsr_b200_convolution_status (dspsr_b200_convolution* conv);
 /* copies the response (FFT order) back to host memory, nchan*nfft complex */
 int dspsr_b200_convolution_get_response (dspsr_b200_convolution* conv, float* response);
 /* Engine::perform(input, output, npart): complex FPT in (span in complex
