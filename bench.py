@@ -323,15 +323,17 @@ def run_b200(args, cfg, world, rank, local):
 
     # ---- device-resident timed region --------------------------------------
     pl = b2.Pipeline(ctx, c)
+    # the clock sampler starts before the warm-up so that nvidia-smi's own
+    # start-up (NVML initialisation) is over before the timed region
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(1.0)
     for i in range(args.warmup):
         pl.run(blocks[i % NBLOCKS], ndat)
     torch.cuda.synchronize()
     pl.profile(True)
     barrier(world)
     torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    clocks.start()
-    time.sleep(0.3)
     launches0 = b2.kernel_launches()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record()

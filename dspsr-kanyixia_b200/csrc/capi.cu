@@ -245,11 +245,14 @@ struct dspsr_b200_fold
   unsigned nbin = 0, nchan = 0, npol = 0;
   DevBuf<float> profiles;
   DevBuf<unsigned> hits;
-  // double-buffered plan upload
-  DevBuf<FoldSegment> d_segs[2];
-  FoldSegment* h_segs[2] = {nullptr, nullptr};
-  size_t h_cap[2] = {0, 0};
-  cudaEvent_t done[2] = {nullptr, nullptr};
+  // Ring of plan buffers: the host builds block b+1's plan while the GPU still
+  // folds earlier blocks; it waits only when all NRING slots are in flight.
+  static constexpr int NRING = 8;
+  static constexpr size_t INITIAL_SEGMENTS = 16384;
+  DevBuf<FoldSegment> d_segs[NRING];
+  FoldSegment* h_segs[NRING] = {};
+  size_t h_cap[NRING] = {};
+  cudaEvent_t done[NRING] = {};
   int cur = 0;
   int nseg = 0;
   uint64_t ndat = 0;
@@ -266,9 +269,16 @@ struct dspsr_b200_fold
                    nchan, npol);
     B200_CHECK (ctx, profiles.reserve (uint64_t (nchan) * npol * nbin), "cudaMalloc profiles");
     B200_CHECK (ctx, hits.reserve (nbin), "cudaMalloc hits");
-    for (int i = 0; i < 2; i++)
+    for (int i = 0; i < NRING; i++)
+    {
       B200_CHECK (ctx, cudaEventCreateWithFlags (&done[i], cudaEventDisableTiming),
                   "cudaEventCreate");
+      B200_CHECK (ctx, cudaMallocHost (&h_segs[i], INITIAL_SEGMENTS * sizeof (FoldSegment)),
+                  "cudaMallocHost plan");
+      h_cap[i] = INITIAL_SEGMENTS;
+      B200_CHECK (ctx, d_segs[i].reserve (INITIAL_SEGMENTS), "cudaMalloc plan");
+    }
+    plan.reserve (INITIAL_SEGMENTS);
     return reset ();
   }
   int reset ()
@@ -286,8 +296,8 @@ struct dspsr_b200_fold
     build_fold_plan (phi, pps, n, &plan);
     ndat = n;
     nseg = int (plan.size ());
-    cur ^= 1;
-    // the buffer about to be overwritten was last read by work queued before `done[cur]`
+    cur = (cur + 1) % NRING;
+    // the slot about to be overwritten was last read by work queued before `done[cur]`
     B200_CHECK (ctx, cudaEventSynchronize (done[cur]), "cudaEventSynchronize");
     if (h_cap[cur] < plan.size ())
     {
@@ -331,7 +341,7 @@ struct dspsr_b200_fold
   {
     profiles.release ();
     hits.release ();
-    for (int i = 0; i < 2; i++)
+    for (int i = 0; i < NRING; i++)
     {
       d_segs[i].release ();
       if (h_segs[i]) cudaFreeHost (h_segs[i]);
@@ -922,6 +932,15 @@ int dspsr_b200_pipeline_create (dspsr_b200_context* ctx, const dspsr_b200_pipeli
     if (e != cudaSuccess) rc = cuda_fail (ctx, e, "upload lut");
   }
   if (!rc) rc = pl->fold.init (ctx, cfg->nbin, cfg->nchan, pl->nout);
+  // the carry never exceeds nfft samples: size both carry buffers once
+  for (int i = 0; i < 2 && !rc; i++)
+  {
+    const uint64_t bytes = cfg->input_kind == DSPSR_B200_FLOAT_FPT
+                             ? uint64_t (cfg->nchan) * cfg->npol * cfg->nfft * sizeof (float2)
+                             : uint64_t (cfg->nfft) * pl->bytes_per_sample;
+    cudaError_t e = pl->carry[i].reserve (bytes);
+    if (e != cudaSuccess) rc = cuda_fail (ctx, e, "cudaMalloc carry");
+  }
   if (rc)
   {
     dspsr_b200_pipeline_destroy (pl);

@@ -150,9 +150,9 @@ __device__ __forceinline__ void detect_values (int state, unsigned npol, float2 
 // fold
 // --------------------------------------------------------------------------
 
-// Exact bin of plan sample t (see host_rules.cpp for the segment algebra).
-__device__ __forceinline__ unsigned fold_bin (const FoldSegment* __restrict__ segs, int nseg,
-                                              uint64_t t, unsigned nbin)
+// Index of the plan segment holding sample t (segments are sorted by start).
+__device__ __forceinline__ int seg_search (const FoldSegment* __restrict__ segs, int nseg,
+                                           uint64_t t)
 {
   int lo = 0, hi = nseg - 1;
   while (lo < hi)
@@ -160,12 +160,43 @@ __device__ __forceinline__ unsigned fold_bin (const FoldSegment* __restrict__ se
     const int mid = (lo + hi + 1) >> 1;
     if (__ldg (&segs[mid].start) <= t) lo = mid; else hi = mid - 1;
   }
-  const uint64_t start = __ldg (&segs[lo].start);
-  const int64_t m0 = __ldg (&segs[lo].m0);
-  const int64_t dm = __ldg (&segs[lo].dm);
-  const double g = __ldg (&segs[lo].g);
+  return lo;
+}
+
+// Exact bin of plan sample t in segment s (see host_rules.cpp for the algebra):
+// y = (m0 + j*dm) * g in integer arithmetic, then one rounded multiply by nbin.
+__device__ __forceinline__ unsigned seg_bin (const FoldSegment* __restrict__ segs, int s,
+                                             uint64_t t, unsigned nbin)
+{
+  const uint64_t start = __ldg (&segs[s].start);
+  const int64_t m0 = __ldg (&segs[s].m0);
+  const int64_t dm = __ldg (&segs[s].dm);
+  const double g = __ldg (&segs[s].g);
   const double y = __dmul_rn (double (m0 + int64_t (t - start) * dm), g);
   return __double2uint_rz (__dmul_rn (y, double (nbin)));
+}
+
+__device__ __forceinline__ unsigned fold_bin (const FoldSegment* __restrict__ segs, int nseg,
+                                              uint64_t t, unsigned nbin)
+{
+  return seg_bin (segs, seg_search (segs, nseg, t), t, nbin);
+}
+
+// Bins of a warp whose active lanes hold increasing sample indices: one binary
+// search by the first active lane, then each lane steps forward over the (few)
+// segment boundaries between it and that lane.  All 32 lanes call this.
+__device__ __forceinline__ unsigned warp_fold_bin (const FoldSegment* __restrict__ segs,
+                                                   int nseg, bool ok, uint64_t t, unsigned nbin)
+{
+  const unsigned act = __ballot_sync (FULL, ok);
+  if (!act) return 0;
+  const int leader = __ffs (act) - 1;
+  int s = 0;
+  if ((threadIdx.x & 31) == leader) s = seg_search (segs, nseg, t);
+  s = __shfl_sync (FULL, s, leader);
+  if (!ok) return 0;
+  while (s + 1 < nseg && __ldg (&segs[s + 1].start) <= t) s++;
+  return seg_bin (segs, s, t, nbin);
 }
 
 // All 32 lanes call this together.  Lanes holding consecutive time samples
@@ -213,11 +244,10 @@ __device__ __forceinline__ void emit_fold (const FoldView& fv, unsigned c, unsig
                                            uint64_t t, float2 p, float2 q)
 {
   float v[4] = {0.f, 0.f, 0.f, 0.f};
-  unsigned bin = 0;
+  unsigned bin = warp_fold_bin (fv.segs, fv.nseg, ok, t, fv.nbin);
   if (ok)
   {
     detect_values (fv.state, npol, p, q, v);
-    bin = fold_bin (fv.segs, fv.nseg, t, fv.nbin);
     ok = bin < fv.nbin;
   }
   warp_fold<NOUT> (ok, bin, v, fv.profiles + uint64_t (c) * NOUT * fv.nbin, fv.nbin,
@@ -698,12 +728,8 @@ __global__ void k_fold (const float* __restrict__ in, const uint64_t in_span,
   const uint64_t t = uint64_t (blockIdx.x) * blockDim.x + threadIdx.x;
   const unsigned c = blockIdx.y;
   bool ok = t < ndat;
-  unsigned bin = 0;
-  if (ok)
-  {
-    bin = fold_bin (fv.segs, fv.nseg, t, fv.nbin);
-    ok = bin < fv.nbin;
-  }
+  const unsigned bin = warp_fold_bin (fv.segs, fv.nseg, ok, t, fv.nbin);
+  ok = ok && bin < fv.nbin;
   for (unsigned p = 0; p < npol; p++)
   {
     float v = ok ? in[(uint64_t (c) * npol + p) * in_span + t] : 0.f;
