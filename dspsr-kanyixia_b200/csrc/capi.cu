@@ -235,6 +235,44 @@ int dspsr_b200_convolution::init (dspsr_b200_context* c, unsigned nchan, unsigne
   return DSPSR_B200_OK;
 }
 
+namespace {
+
+// Dedispersion response for channels centred at freq[c] (MHz), channel width
+// bw/nchan, each channel complex-sampled with DC at FFT bin 0 when swap_halves
+// (Response::doswap per channel).  Per channel the coefficient of
+// Dedispersion::build_compute (Dedispersion.C:168-173) is formed on the host
+// in double; the GPU evaluates the phase of every bin in FP64.
+int build_response (dspsr_b200_convolution* c, const double* freq, double bw, double dm,
+                    int swap_halves, int chirp_mode, unsigned norm_nfft)
+{
+  dspsr_b200_context* ctx = c->ctx;
+  const ConvShape& sh = c->shape;
+  const unsigned nchan = sh.nchan;
+  std::vector<double> par (2 * nchan);
+  const double sign = bw / std::fabs (bw);
+  const double dispersion_per_MHz = 1e6 * dm / 2.41e-4;
+  for (unsigned ic = 0; ic < nchan; ic++)
+  {
+    par[ic] = freq[ic];
+    par[nchan + ic] = -sign * 2 * M_PI * dispersion_per_MHz / (freq[ic] * freq[ic]);
+  }
+  const double chanwidth = bw / double (nchan);
+  const double binwidth = chanwidth / double (sh.nfft);
+  const float scale = float (1.0 / std::sqrt (double (norm_nfft ? norm_nfft : sh.nfft)));
+  B200_CHECK (ctx, c->chan_par.reserve (2 * nchan), "cudaMalloc channel table");
+  B200_CHECK (ctx, cudaMemcpyAsync (c->chan_par.ptr, par.data (), par.size () * sizeof (double),
+                                    cudaMemcpyHostToDevice, ctx->stream), "upload channels");
+  B200_CHECK (ctx, launch_build_chirp (c->H.ptr, c->chan_par.ptr, c->chan_par.ptr + nchan, nchan,
+                                       sh.nfft, sh.n1, sh.n2, binwidth, 0.5 * chanwidth,
+                                       swap_halves, chirp_mode, scale, ctx->stream),
+              "build chirp");
+  B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "set_dedispersion sync");
+  c->have_response = true;
+  return DSPSR_B200_OK;
+}
+
+} // namespace
+
 // ---------------------------------------------------------------------------
 // fold engine
 // ---------------------------------------------------------------------------
@@ -405,7 +443,9 @@ struct dspsr_b200_pipeline
   int cur_carry = 0;
   uint64_t in0 = 0;                 // global input index of the first sample of the block
   DevBuf<uint8_t> staging;          // host->device staging for run_host
-  double rate = 0;
+  double rate = 0;                  // complex sampling rate of the convolved channels
+  unsigned fb_nsub = 0;             // filterbank channels per input channel (0: none)
+  DevBuf<float2> fbbuf;             // filterbank output, FPT
 };
 
 namespace {
@@ -418,18 +458,18 @@ int pipeline_block (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat_new
   const auto& cfg = pl->cfg;
   const uint64_t nfilt = uint64_t (sh.nfilt_pos) + sh.nfilt_neg;
   const uint64_t ndat = pl->ncarry + ndat_new;
-  const bool fpt = cfg.input_kind == DSPSR_B200_FLOAT_FPT;
+  // after a filterbank stage the convolution reads complex-float channels
+  const bool fpt = pl->fb_nsub > 1 || cfg.input_kind == DSPSR_B200_FLOAT_FPT;
   if (ndat_folded) *ndat_folded = 0;
 
   InputView in;
-  in.kind = cfg.input_kind == DSPSR_B200_INT8_TFPD ? IN_INT8
-          : cfg.input_kind == DSPSR_B200_INT16_TFPD ? IN_INT16 : IN_FLOAT;
+  in.kind = fpt ? IN_FLOAT : cfg.input_kind == DSPSR_B200_INT8_TFPD ? IN_INT8 : IN_INT16;
   in.pre = pl->carry[pl->cur_carry].ptr;
   in.main = d_in;
   in.npre = pl->ncarry;
   in.pre_span = pl->carry_span;
   in.main_span = fpt ? in_span : 0;
-  in.nchan = cfg.nchan;
+  in.nchan = sh.nchan;
   in.npol = cfg.npol;
   in.offset_binary = cfg.offset_binary;
 
@@ -491,7 +531,7 @@ int pipeline_block (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat_new
   }
   else
   {
-    const uint64_t rows = uint64_t (cfg.nchan) * cfg.npol;
+    const uint64_t rows = uint64_t (sh.nchan) * cfg.npol;
     const uint64_t span = std::max<uint64_t> (keep, 1);
     B200_CHECK (ctx, pl->carry[next].reserve (rows * span * sizeof (float2)), "cudaMalloc carry");
     uint64_t done = 0;
@@ -522,6 +562,35 @@ int pipeline_block (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat_new
   pl->in0 += nout;
   if (ndat_folded) *ndat_folded = nout;
   return DSPSR_B200_OK;
+}
+
+// A block of the operation chain: with a filterbank stage the raw input is
+// first channelised (Filterbank, freq_res = 1) into complex-float channels,
+// which then feed the overlap-save stage.  Blocks are whole filterbank
+// transforms (ndat a multiple of the channel count).
+int pipeline_input (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat, uint64_t in_span,
+                    uint64_t* ndat_folded)
+{
+  if (!pl->fb_nsub) return pipeline_block (pl, d_in, ndat, in_span, ndat_folded);
+  dspsr_b200_context* ctx = pl->ctx;
+  const auto& cfg = pl->cfg;
+  if (ndat % pl->fb_nsub)
+    return fail (ctx, DSPSR_B200_EINVAL, "pipeline: block of %llu samples is not a multiple of "
+                 "the %u filterbank channels", (unsigned long long) ndat, pl->fb_nsub);
+  const uint64_t nb = ndat / pl->fb_nsub;
+  const uint64_t rows = uint64_t (pl->conv.shape.nchan) * cfg.npol;
+  B200_CHECK (ctx, pl->fbbuf.reserve (std::max<uint64_t> (rows * nb, 1)), "cudaMalloc filterbank");
+  InputView in {};
+  in.kind = cfg.input_kind;
+  in.main = d_in;
+  in.main_span = in_span;
+  in.nchan = cfg.nchan;
+  in.npol = cfg.npol;
+  in.offset_binary = cfg.offset_binary;
+  const float scale = float (1.0 / std::sqrt (double (pl->fb_nsub)));
+  B200_CHECK (ctx, launch_filterbank (in, pl->conv.lut.ptr, pl->fb_nsub, nb, scale, pl->fbbuf.ptr,
+                                      nb, ctx->stream), "filterbank");
+  return pipeline_block (pl, pl->fbbuf.ptr, nb, nb, ndat_folded);
 }
 
 } // namespace
@@ -712,32 +781,63 @@ int dspsr_b200_convolution_set_dedispersion (dspsr_b200_convolution* c, double c
   if (dc_centred && input_nchan > 1)
     return fail (ctx, DSPSR_B200_EINVAL, "set_dedispersion: DC-centred channels not supported");
   const unsigned nchan = sh.nchan;
-  // Observation::get_centre_frequency(ichan) (Observation.C:521-534) and the
-  // per-channel coefficient of Dedispersion::build_compute (Dedispersion.C:168-173)
-  std::vector<double> par (2 * nchan);
-  const double sign = bw / std::fabs (bw);
-  const double dispersion_per_MHz = 1e6 * dm / 2.41e-4;
+  // Observation::get_centre_frequency(ichan) (Observation.C:521-534)
+  std::vector<double> freq (nchan);
   for (unsigned ic = 0; ic < nchan; ic++)
-  {
-    const double base = cf - 0.5 * bw + 0.5 * bw / double (nchan);
-    const double chan_freq = base + double (ic) * bw / double (nchan);
-    par[ic] = chan_freq;
-    par[nchan + ic] = -sign * 2 * M_PI * dispersion_per_MHz / (chan_freq * chan_freq);
-  }
-  const double chanwidth = bw / double (nchan);
-  const double binwidth = chanwidth / double (sh.nfft);
+    freq[ic] = channel_centre (cf, bw, nchan, ic, false, false);
   // Response::swap_as_needed (Response.C:325-400) for the supported states
   const int swap = (input_nchan == 1 && nchan == 1 && dual_sideband > 0)
                 || (input_nchan > 1 && unsigned (input_nchan) == nchan && dual_sideband != 0);
-  const float scale = float (1.0 / std::sqrt (double (norm_nfft ? norm_nfft : sh.nfft)));
-  B200_CHECK (ctx, c->chan_par.reserve (2 * nchan), "cudaMalloc channel table");
-  B200_CHECK (ctx, cudaMemcpyAsync (c->chan_par.ptr, par.data (), par.size () * sizeof (double),
-                                    cudaMemcpyHostToDevice, ctx->stream), "upload channels");
-  B200_CHECK (ctx, launch_build_chirp (c->H.ptr, c->chan_par.ptr, c->chan_par.ptr + nchan, nchan,
-                                       sh.nfft, sh.n1, sh.n2, binwidth, 0.5 * chanwidth, swap,
-                                       chirp_mode, scale, ctx->stream), "build chirp");
-  B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "set_dedispersion sync");
-  c->have_response = true;
+  return build_response (c, freq.data (), bw, dm, swap, chirp_mode, norm_nfft);
+}
+
+int dspsr_b200_convolution_set_dedispersion_channels (dspsr_b200_convolution* c,
+                                                      const double* chan_freq, double bw,
+                                                      double dm, int chirp_mode,
+                                                      unsigned norm_nfft)
+{
+  if (!c) return DSPSR_B200_EINVAL;
+  if (!chan_freq || bw == 0)
+    return fail (c->ctx, DSPSR_B200_EINVAL, "set_dedispersion_channels: invalid argument");
+  for (unsigned ic = 0; ic < c->shape.nchan; ic++)
+    if (!(chan_freq[ic] > 0))
+      return fail (c->ctx, DSPSR_B200_EINVAL, "set_dedispersion_channels: bad frequency");
+  return build_response (c, chan_freq, bw, dm, 1, chirp_mode, norm_nfft);
+}
+
+int dspsr_b200_filterbank (dspsr_b200_context* ctx, int input_kind, const void* d_in,
+                           uint64_t ndat, uint64_t in_span, unsigned nchan_in, unsigned npol,
+                           unsigned nsub, const float* lut256, int offset_binary, float* d_out,
+                           uint64_t out_span, uint64_t* ndat_out)
+{
+  if (!ctx) return DSPSR_B200_EINVAL;
+  if (ndat_out) *ndat_out = 0;
+  if (!d_in || !d_out || nchan_in == 0 || npol == 0 || npol > 2)
+    return fail (ctx, DSPSR_B200_EINVAL, "filterbank: invalid argument");
+  if (input_kind < 0 || input_kind > 2 || (input_kind == DSPSR_B200_INT8_TFPD && !lut256))
+    return fail (ctx, DSPSR_B200_EINVAL, "filterbank: invalid input kind or missing table");
+  if (!(nsub == 4 || nsub == 8 || nsub == 16 || nsub == 32 || nsub == 64))
+    return fail (ctx, DSPSR_B200_EINVAL, "filterbank: nsub=%u not in {4,...,64}", nsub);
+  if (input_kind == DSPSR_B200_FLOAT_FPT && in_span < ndat)
+    return fail (ctx, DSPSR_B200_EINVAL, "filterbank: in_span < ndat");
+  const uint64_t nblk = ndat / nsub;
+  if (out_span < nblk)
+    return fail (ctx, DSPSR_B200_EINVAL, "filterbank: out_span < ndat/nsub");
+  if (input_kind == DSPSR_B200_INT8_TFPD)
+    B200_CHECK (ctx, cudaMemcpyAsync (ctx->d_lut, lut256, 256 * sizeof (float),
+                                      cudaMemcpyHostToDevice, ctx->stream), "upload lut");
+  InputView in {};
+  in.kind = input_kind;
+  in.main = d_in;
+  in.main_span = in_span;
+  in.nchan = nchan_in;
+  in.npol = npol;
+  in.offset_binary = offset_binary;
+  const float scale = float (1.0 / std::sqrt (double (nsub)));
+  B200_CHECK (ctx, launch_filterbank (in, ctx->d_lut, nsub, nblk, scale,
+                                      reinterpret_cast<float2*> (d_out), out_span, ctx->stream),
+              "filterbank");
+  if (ndat_out) *ndat_out = nblk;
   return DSPSR_B200_OK;
 }
 
@@ -917,27 +1017,48 @@ int dspsr_b200_pipeline_create (dspsr_b200_context* ctx, const dspsr_b200_pipeli
   pl->nout = detect_nout (cfg->state);
   const uint64_t bytes_per_value = cfg->input_kind == DSPSR_B200_INT16_TFPD ? 2 : 1;
   pl->bytes_per_sample = uint64_t (cfg->nchan) * cfg->npol * 2 * bytes_per_value;
-  pl->rate = std::fabs (cfg->bandwidth_mhz) / double (cfg->nchan) * 1e6;
-  int rc = pl->conv.init (ctx, cfg->nchan, cfg->npol, cfg->nfft, cfg->nfilt_pos, cfg->nfilt_neg,
+  const unsigned fb = cfg->filterbank_nchan > 1 ? cfg->filterbank_nchan : 0;
+  if (fb && !(fb == 4 || fb == 8 || fb == 16 || fb == 32 || fb == 64))
+  {
+    delete pl;
+    return fail (ctx, DSPSR_B200_EINVAL, "pipeline: filterbank_nchan=%u not in {4,...,64}", fb);
+  }
+  pl->fb_nsub = fb;
+  // channels the convolution sees
+  const unsigned nchan = fb ? cfg->nchan * fb : cfg->nchan;
+  pl->rate = std::fabs (cfg->bandwidth_mhz) / double (nchan) * 1e6;
+  int rc = pl->conv.init (ctx, nchan, cfg->npol, cfg->nfft, cfg->nfilt_pos, cfg->nfilt_neg,
                           cfg->scratch_bytes);
-  if (!rc)
+  if (!rc && !fb)
     rc = dspsr_b200_convolution_set_dedispersion (&pl->conv, cfg->centre_freq_mhz,
                                                   cfg->bandwidth_mhz, cfg->dm, cfg->nchan,
                                                   cfg->dual_sideband, cfg->dc_centred,
                                                   cfg->chirp_mode, cfg->nfft);
+  else if (!rc)
+  {
+    // Filterbank::prepare_output (Filterbank.C:352-381) with freq_res = 1: the
+    // output channels are DC-centred and, for dual-sideband input, swapped
+    std::vector<double> freq (nchan);
+    for (unsigned ic = 0; ic < nchan; ic++)
+      freq[ic] = channel_centre (cfg->centre_freq_mhz, cfg->bandwidth_mhz, nchan, ic,
+                                 cfg->dual_sideband != 0, true);
+    rc = dspsr_b200_convolution_set_dedispersion_channels (&pl->conv, freq.data (),
+                                                           cfg->bandwidth_mhz, cfg->dm,
+                                                           cfg->chirp_mode, cfg->nfft);
+  }
   if (!rc && cfg->input_kind == DSPSR_B200_INT8_TFPD)
   {
     cudaError_t e = cudaMemcpy (pl->conv.lut.ptr, cfg->lut, 256 * sizeof (float),
                                 cudaMemcpyHostToDevice);
     if (e != cudaSuccess) rc = cuda_fail (ctx, e, "upload lut");
   }
-  if (!rc) rc = pl->fold.init (ctx, cfg->nbin, cfg->nchan, pl->nout);
+  if (!rc) rc = pl->fold.init (ctx, cfg->nbin, nchan, pl->nout);
   // the carry never exceeds nfft samples: size both carry buffers once
   for (int i = 0; i < 2 && !rc; i++)
   {
-    const uint64_t bytes = cfg->input_kind == DSPSR_B200_FLOAT_FPT
-                             ? uint64_t (cfg->nchan) * cfg->npol * cfg->nfft * sizeof (float2)
-                             : uint64_t (cfg->nfft) * pl->bytes_per_sample;
+    const bool fpt = fb || cfg->input_kind == DSPSR_B200_FLOAT_FPT;
+    const uint64_t bytes = fpt ? uint64_t (nchan) * cfg->npol * cfg->nfft * sizeof (float2)
+                               : uint64_t (cfg->nfft) * pl->bytes_per_sample;
     cudaError_t e = pl->carry[i].reserve (bytes);
     if (e != cudaSuccess) rc = cuda_fail (ctx, e, "cudaMalloc carry");
   }
@@ -959,6 +1080,7 @@ int dspsr_b200_pipeline_destroy (dspsr_b200_pipeline* pl)
   pl->carry[0].release ();
   pl->carry[1].release ();
   pl->staging.release ();
+  pl->fbbuf.release ();
   delete pl;
   return DSPSR_B200_OK;
 }
@@ -970,7 +1092,7 @@ int dspsr_b200_pipeline_run (dspsr_b200_pipeline* pl, const void* d_in, uint64_t
   if (!d_in && ndat) return fail (pl->ctx, DSPSR_B200_EINVAL, "pipeline_run: null input");
   if (pl->cfg.input_kind == DSPSR_B200_FLOAT_FPT && in_span < ndat)
     return fail (pl->ctx, DSPSR_B200_EINVAL, "pipeline_run: in_span < ndat");
-  return pipeline_block (pl, d_in, ndat, in_span, ndat_folded);
+  return pipeline_input (pl, d_in, ndat, in_span, ndat_folded);
 }
 
 int dspsr_b200_pipeline_run_host (dspsr_b200_pipeline* pl, const void* h_in, uint64_t ndat,
@@ -985,7 +1107,7 @@ int dspsr_b200_pipeline_run_host (dspsr_b200_pipeline* pl, const void* h_in, uin
   B200_CHECK (ctx, pl->staging.reserve (std::max<uint64_t> (bytes, 16)), "cudaMalloc staging");
   B200_CHECK (ctx, cudaMemcpyAsync (pl->staging.ptr, h_in, bytes, cudaMemcpyHostToDevice,
                                     ctx->stream), "upload block");
-  return pipeline_block (pl, pl->staging.ptr, ndat, 0, ndat_folded);
+  return pipeline_input (pl, pl->staging.ptr, ndat, 0, ndat_folded);
 }
 
 int dspsr_b200_pipeline_get_profiles (dspsr_b200_pipeline* pl, float* profiles, uint32_t* hits)

@@ -47,6 +47,17 @@ unsigned smearing_samples (double centre_frequency, double bandwidth, double dm,
   return unsigned (std::ceil (tsmear * sampling_rate));
 }
 
+// Observation::get_centre_frequency (Observation.C:521-534): the base frequency
+// is the centre of channel 0 (its lower edge when the channels are DC-centred);
+// swapped channel orders are undone first (get_unswapped_ichan, :495-518).
+double channel_centre (double cf, double bw, unsigned nchan, unsigned ichan, bool swap,
+                       bool dc_centred)
+{
+  const unsigned ch = swap ? (ichan + nchan / 2) % nchan : ichan;
+  const double base = dc_centred ? cf - 0.5 * bw : cf - 0.5 * bw + 0.5 * bw / double (nchan);
+  return base + double (ch) * bw / double (nchan);
+}
+
 // Response::get_minimum_ndat (Response.C:529-545): the smallest power of two
 // strictly greater than impulse_pos + impulse_neg.
 unsigned minimum_ndat (unsigned impulse_pos, unsigned impulse_neg)

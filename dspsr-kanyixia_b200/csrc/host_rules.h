@@ -19,6 +19,9 @@ struct FoldSegment
 unsigned smearing_samples (double centre_frequency, double bandwidth, double dm,
                            unsigned nchan, int half);
 unsigned minimum_ndat (unsigned impulse_pos, unsigned impulse_neg);
+// Observation::get_centre_frequency(ichan) with get_unswapped_ichan (swap only)
+double channel_centre (double centre_frequency, double bandwidth, unsigned nchan,
+                       unsigned ichan, bool swap, bool dc_centred);
 int64_t optimal_fft_length (uint64_t nbad, uint64_t nfft_max, unsigned factor);
 void bittable8 (double spacing, bool twos_complement, float* lut, double* scale);
 double fold_phi (int64_t start_day, int64_t start_sec, double start_frac,

@@ -669,6 +669,35 @@ __global__ void k_permute (float2* __restrict__ dst, const float2* __restrict__ 
 // standalone engines
 // --------------------------------------------------------------------------
 
+// FFT filterbank without convolution (Filterbank with freq_res = 1,
+// FilterbankEngineCPU.C:379-535): every block of NSUB input samples becomes one
+// sample in each of NSUB output channels, channel k = FFT bin k scaled by the
+// normaliser 1/sqrt(NSUB) (Filterbank.C:171-180).  The unpack is fused into
+// the load; one thread transforms one block of one polarisation in registers.
+template <int NSUB, int KIND>
+__global__ void __launch_bounds__ (128)
+k_filterbank (const InputView in, const float* __restrict__ lut, const uint64_t nblk,
+              const float scale, float2* __restrict__ out, const uint64_t out_span)
+{
+  __shared__ float s_lut[256];
+  load_lut (in, lut, s_lut);
+  __syncthreads ();
+  const uint64_t blk = uint64_t (blockIdx.x) * blockDim.x + threadIdx.x;
+  const unsigned p = blockIdx.y;
+  const unsigned cin = blockIdx.z;
+  if (blk >= nblk) return;
+  float2 v[NSUB];
+#pragma unroll
+  for (int k = 0; k < NSUB; k++)
+    v[k] = fetch<KIND> (in, s_lut, cin, p, blk * NSUB + k);
+  RegDFT<NSUB, -1>::run (v);
+  float2* o = out + (uint64_t (cin) * NSUB * in.npol + p) * out_span + blk;
+#pragma unroll
+  for (int k = 0; k < NSUB; k++)
+    o[uint64_t (k) * in.npol * out_span] = make_float2 (__fmul_rn (scale, v[k].x),
+                                                         __fmul_rn (scale, v[k].y));
+}
+
 __global__ void k_unpack8 (const uint8_t* __restrict__ in, const uint64_t ndat,
                            const unsigned nchan, const unsigned npol, const unsigned ndim,
                            const float* __restrict__ lut, float* __restrict__ out,
@@ -970,6 +999,39 @@ cudaError_t launch_unpermute_response (float2* dst, const float2* H, unsigned nc
   g_launches++;
   k_permute<<<dim3 (unsigned ((N + 255) / 256), nchan), 256, 0, st>>> (dst, H, n1, n2, 1);
   return cudaGetLastError ();
+}
+
+namespace {
+template <int NSUB>
+cudaError_t run_filterbank (const InputView& in, const float* d_lut, uint64_t nblk, float scale,
+                            float2* out, uint64_t out_span, cudaStream_t st)
+{
+  const dim3 grid (unsigned ((nblk + 127) / 128), in.npol, in.nchan);
+  g_launches++;
+  if (in.kind == IN_INT8)
+    k_filterbank<NSUB, IN_INT8><<<grid, 128, 0, st>>> (in, d_lut, nblk, scale, out, out_span);
+  else if (in.kind == IN_INT16)
+    k_filterbank<NSUB, IN_INT16><<<grid, 128, 0, st>>> (in, d_lut, nblk, scale, out, out_span);
+  else
+    k_filterbank<NSUB, IN_FLOAT><<<grid, 128, 0, st>>> (in, d_lut, nblk, scale, out, out_span);
+  return cudaGetLastError ();
+}
+} // namespace
+
+cudaError_t launch_filterbank (const InputView& in, const float* d_lut, unsigned nsub,
+                               uint64_t nblk, float scale, float2* out, uint64_t out_span,
+                               cudaStream_t st)
+{
+  if (nblk == 0) return cudaSuccess;
+  switch (nsub)
+  {
+    case 4: return run_filterbank<4> (in, d_lut, nblk, scale, out, out_span, st);
+    case 8: return run_filterbank<8> (in, d_lut, nblk, scale, out, out_span, st);
+    case 16: return run_filterbank<16> (in, d_lut, nblk, scale, out, out_span, st);
+    case 32: return run_filterbank<32> (in, d_lut, nblk, scale, out, out_span, st);
+    case 64: return run_filterbank<64> (in, d_lut, nblk, scale, out, out_span, st);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 cudaError_t launch_unpack8 (const uint8_t* in, uint64_t ndat, unsigned nchan, unsigned npol,

@@ -105,6 +105,13 @@ cudaError_t launch_permute_response (float2* H, const float2* src, unsigned ncha
 cudaError_t launch_unpermute_response (float2* dst, const float2* H, unsigned nchan,
                                        unsigned n1, unsigned n2, cudaStream_t stream);
 
+// FFT filterbank, freq_res = 1: nsub in {4, 8, 16, 32, 64}; nblk blocks of
+// nsub input samples per (input channel, pol); output FPT with channel
+// cin*nsub + k, span out_span.
+cudaError_t launch_filterbank (const InputView& in, const float* d_lut, unsigned nsub,
+                               uint64_t nblk, float scale, float2* out, uint64_t out_span,
+                               cudaStream_t stream);
+
 cudaError_t launch_unpack8 (const uint8_t* in, uint64_t ndat, unsigned nchan, unsigned npol,
                             unsigned ndim, const float* d_lut, float* out, uint64_t span,
                             cudaStream_t stream);

@@ -128,6 +128,18 @@ class Context:
                                                  int(offset_binary), _ptr(d_out), out_span),
                    "unpack16")
 
+    # ---- Filterbank engine (freq_res = 1) -------------------------------------------
+    def filterbank(self, input_kind, d_in, ndat, nchan_in, npol, nsub, d_out, out_span,
+                   in_span=0, lut=None, offset_binary=False):
+        """Returns the output samples per channel (ndat // nsub)."""
+        n = ctypes.c_uint64()
+        lp = _fptr(np.ascontiguousarray(lut, np.float32)) if lut is not None else None
+        self.check(self._lib.dspsr_b200_filterbank(self.handle, input_kind, _ptr(d_in), ndat,
+                                                   in_span, nchan_in, npol, nsub, lp,
+                                                   int(offset_binary), _ptr(d_out), out_span,
+                                                   ctypes.byref(n)), "filterbank")
+        return n.value
+
     # ---- Detection engine ----------------------------------------------------------
     def detect(self, d_in, in_span, ndat, nchan, state, d_out, out_span):
         self.check(self._lib.dspsr_b200_detect(self.handle, _ptr(d_in), in_span, ndat, nchan,
@@ -161,6 +173,17 @@ class Convolution:
             self.handle, centre_freq, bandwidth, dm,
             self.nchan if input_nchan is None else input_nchan, dual_sideband, dc_centred,
             chirp_mode, norm_nfft or self.nfft), "set_dedispersion")
+
+    def set_dedispersion_channels(self, chan_freq, bandwidth, dm, chirp_mode=CHIRP_REFERENCE,
+                                  norm_nfft=None):
+        f = np.ascontiguousarray(chan_freq, np.float64)
+        assert f.size == self.nchan
+        self.ctx.check(self._lib.dspsr_b200_convolution_set_dedispersion_channels(
+            self.handle, f.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), bandwidth, dm,
+            chirp_mode, norm_nfft or self.nfft), "set_dedispersion_channels")
+
+    def status(self):
+        self.ctx.check(self._lib.dspsr_b200_convolution_status(self.handle), "status")
 
     def get_response(self):
         out = np.empty(self.nchan * self.nfft, np.complex64)
@@ -267,7 +290,8 @@ class Pipeline:
 
     def get_profiles(self):
         c = self.config
-        prof = np.empty((c.nchan, self.nout, c.nbin), np.float32)
+        nchan = c.nchan * (c.filterbank_nchan if c.filterbank_nchan > 1 else 1)
+        prof = np.empty((nchan, self.nout, c.nbin), np.float32)
         hits = np.empty(c.nbin, np.uint32)
         self.ctx.check(self._lib.dspsr_b200_pipeline_get_profiles(
             self.handle, _fptr(prof), hits.ctypes.data_as(_capi.c_u32p)), "get_profiles")
@@ -311,9 +335,12 @@ class Pipeline:
 def make_config(centre_freq, bandwidth, dm, nchan, npol, nfft, nfilt_pos, nfilt_neg, nbin,
                 period, state=INTENSITY, input_kind=INT8_TFPD, lut=None, chirp_mode=CHIRP_REFERENCE,
                 start_mjd=(60000, 0, 0.0), epoch_mjd=(60000, 0, 0.0), reference_phase=0.0,
-                dual_sideband=1, offset_binary=0, scratch_bytes=0):
-    """Fill a PipelineConfig (the fields DedispersionPipe / LoadToFold set up)."""
+                dual_sideband=1, offset_binary=0, scratch_bytes=0, filterbank_nchan=0):
+    """Fill a PipelineConfig (the fields DedispersionPipe / LoadToFold set up).
+    With filterbank_nchan > 1, nchan counts input channels, and nfft and the
+    smearing (nfilt_pos, nfilt_neg) refer to the filterbank's output channels."""
     cfg = PipelineConfig()
+    cfg.filterbank_nchan = filterbank_nchan
     cfg.centre_freq_mhz = centre_freq
     cfg.bandwidth_mhz = bandwidth
     cfg.dm = dm

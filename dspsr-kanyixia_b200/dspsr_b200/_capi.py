@@ -56,6 +56,7 @@ class PipelineConfig(ctypes.Structure):
         ("start_sec", c_i64),
         ("start_frac", c_dbl),
         ("scratch_bytes", c_u64),
+        ("filterbank_nchan", c_uint),
     ]
 
 
@@ -84,6 +85,10 @@ SIGNATURES = {
                                                         c_int, c_int, c_uint]),
     "dspsr_b200_convolution_get_response": (c_int, [c_vp, c_fp]),
     "dspsr_b200_convolution_status": (c_int, [c_vp]),
+    "dspsr_b200_convolution_set_dedispersion_channels": (c_int, [c_vp, ctypes.POINTER(c_dbl),
+                                                                 c_dbl, c_dbl, c_int, c_uint]),
+    "dspsr_b200_filterbank": (c_int, [c_vp, c_int, c_vp, c_u64, c_u64, c_uint, c_uint, c_uint,
+                                      c_fp, c_int, c_vp, c_u64, c_u64p]),
     "dspsr_b200_convolution_perform": (c_int, [c_vp, c_vp, c_u64, c_u64, c_vp, c_u64, c_u64p]),
     "dspsr_b200_detect": (c_int, [c_vp, c_vp, c_u64, c_u64, c_uint, c_int, c_vp, c_u64]),
     "dspsr_b200_fold_create": (c_int, [c_vp, c_uint, c_uint, c_uint, ctypes.POINTER(c_vp)]),

@@ -141,6 +141,15 @@ int dspsr_b200_convolution_set_dedispersion (dspsr_b200_convolution* conv,
                                              double dm, int input_nchan, int dual_sideband,
                                              int dc_centred, int chirp_mode,
                                              unsigned norm_nfft);
+/* The same response for channels whose centre frequencies the caller supplies
+   (the values PlasmaResponse::configure stores in frequency_input from
+   Observation::get_centre_frequency(ichan), PlasmaResponse.C:73-80), each
+   channel complex-sampled with DC at its FFT bin 0 (the per-channel
+   Response::doswap of Response.C:375-387); bandwidth is the whole band's. */
+int dspsr_b200_convolution_set_dedispersion_channels (dspsr_b200_convolution* conv,
+                                                      const double* chan_freq_mhz,
+                                                      double bandwidth_mhz, double dm,
+                                                      int chirp_mode, unsigned norm_nfft);
 /* Blocks until the engine's queued work is done and returns DSPSR_B200_ESTATE
    if one of its device-side waits gave up (each wait is bounded to about a
    second; see the row kernel), DSPSR_B200_OK otherwise. */
@@ -153,6 +162,23 @@ int dspsr_b200_convolution_get_response (dspsr_b200_convolution* conv, float* re
 int dspsr_b200_convolution_perform (dspsr_b200_convolution* conv, const float* d_in,
                                     uint64_t in_span, uint64_t ndat, float* d_out,
                                     uint64_t out_span, uint64_t* npart);
+
+/* ---------------------------------------------------------------------- */
+/* Filterbank::Engine without convolution (freq_res = 1): CUDA::FilterbankEngine*/
+/* (Signal/General/FilterbankEngineCUDA.cu:353-480), FilterbankEngineCPU     */
+/* (FilterbankEngineCPU.C:379-535); callers Filterbank.C:454-570            */
+/* ---------------------------------------------------------------------- */
+
+/* Every block of nsub input samples of each (input channel, pol) becomes one
+   sample in nsub output channels: out channel cin*nsub + k = FFT bin k scaled
+   by 1/sqrt(nsub) (Filterbank::prepare_normalizer).  Input as input_kind
+   (TFPD int8/int16 or complex-float FPT with in_span); the unpack is fused.
+   Output complex-float FPT, (chan*npol + pol)*out_span.  nsub in {4,...,64}.
+   Returns ndat/nsub output samples; a trailing partial block is ignored. */
+int dspsr_b200_filterbank (dspsr_b200_context* ctx, int input_kind, const void* d_in,
+                           uint64_t ndat, uint64_t in_span, unsigned nchan_in, unsigned npol,
+                           unsigned nsub, const float* lut256, int offset_binary,
+                           float* d_out, uint64_t out_span, uint64_t* ndat_out);
 
 /* ---------------------------------------------------------------------- */
 /* Detection::Engine (CUDA::DetectionEngine, Signal/General/DetectionCUDA.cu;*/
@@ -222,6 +248,10 @@ typedef struct
   int64_t start_day, start_sec; double start_frac;   /* MJD of input sample 0 */
   /* tuning: maximum scratch bytes for in-flight FFT parts (0 = default) */
   uint64_t scratch_bytes;
+  /* FFT filterbank stage in front of the dedispersion (Filterbank with
+     freq_res = 1, Filterbank.C:75-570): channels per input channel, 0 or 1 =
+     none, else 4..64; blocks must then be multiples of it */
+  unsigned filterbank_nchan;
 } dspsr_b200_pipeline_config;
 
 int dspsr_b200_pipeline_create (dspsr_b200_context* ctx,

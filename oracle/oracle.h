@@ -72,6 +72,33 @@ void orc_dedispersion_response_f64 (double centre_freq, double bandwidth, double
 void orc_tukey_response (unsigned impulse_neg, unsigned impulse_pos, unsigned ndat,
                          float* spectral, float* temporal);
 
+/* Observation::get_centre_frequency(ichan) with get_unswapped_ichan
+   (Kernel/Classes/Observation.C:495-534) */
+double orc_channel_centre (double centre_freq, double bandwidth, unsigned nchan,
+                           unsigned ichan, int swap, int dc_centred);
+/* Response for channels with explicit centre frequencies (what
+   PlasmaResponse::configure stores in frequency_input, PlasmaResponse.C:73-80),
+   each channel complex-sampled with its DC at FFT bin 0: the within-channel
+   bins are half-swapped into FFT order.  mode as above; f64 variant writes
+   double complex. */
+void orc_dedispersion_response_channels (const double* chan_freq, unsigned nchan,
+                                         double bandwidth, double dm, unsigned ndat,
+                                         int mode, unsigned norm_nfft, float* out);
+void orc_dedispersion_response_channels_f64 (const double* chan_freq, unsigned nchan,
+                                             double bandwidth, double dm, unsigned ndat,
+                                             unsigned norm_nfft, double* out);
+
+/* ---- FFT filterbank without convolution (freq_res = 1):
+        Filterbank::do_prepare / prepare_output (Filterbank.C:75-380) and
+        FilterbankEngineCPU::perform (FilterbankEngineCPU.C:379-535) --------- */
+/* in: complex FPT, nchan_in spans of npol; out: nchan_in*nchan_sub channels of
+   ndat/nchan_sub samples, channel k of subband s = FFT bin k of each block of
+   nchan_sub samples, scaled by 1/sqrt(nchan_sub).  Returns output ndat. */
+uint64_t orc_filterbank_f32 (const float* in, uint64_t ndat, uint64_t in_span, int nchan_in,
+                             int npol, unsigned nchan_sub, float* out, uint64_t out_span);
+uint64_t orc_filterbank_f64 (const double* in, uint64_t ndat, uint64_t in_span, int nchan_in,
+                             int npol, unsigned nchan_sub, double* out, uint64_t out_span);
+
 /* ---- overlap-save convolution (Signal/General/Convolution.C:316-813) ----- */
 /* in/out FPT: (ichan*npol+ipol)*span complex values; response nchan*nfft complex
    (one filter for all polns).  Returns npart.  out holds npart*(nfft-nfilt) values. */

@@ -55,7 +55,48 @@ _SIGS = {
                                        f64p, u32p]),
     "orc_pipeline_c1": (c_u64, [u8p, c_u64, f32p, f32p, c_uint, c_uint, c_uint, c_dbl, c_dbl,
                                 c_uint, f32p, u32p, c_int]),
+    "orc_channel_centre": (c_dbl, [c_dbl, c_dbl, c_uint, c_uint, c_int, c_int]),
+    "orc_dedispersion_response_channels": (None, [f64p, c_uint, c_dbl, c_dbl, c_uint, c_int,
+                                                  c_uint, f32p]),
+    "orc_dedispersion_response_channels_f64": (None, [f64p, c_uint, c_dbl, c_dbl, c_uint,
+                                                      c_uint, f64p]),
+    "orc_filterbank_f32": (c_u64, [f32p, c_u64, c_u64, c_int, c_int, c_uint, f32p, c_u64]),
+    "orc_filterbank_f64": (c_u64, [f64p, c_u64, c_u64, c_int, c_int, c_uint, f64p, c_u64]),
 }
+
+
+def channel_centres(cf, bw, nchan, swap=False, dc_centred=False):
+    return np.array([lib().orc_channel_centre(cf, bw, nchan, i, int(swap), int(dc_centred))
+                     for i in range(nchan)], np.float64)
+
+
+def dedispersion_response_channels(chan_freq, bw, dm, ndat, mode=0, norm_nfft=None, fp64=False):
+    chan_freq = np.ascontiguousarray(chan_freq, np.float64)
+    nchan = chan_freq.size
+    if fp64:
+        out = np.empty(nchan * ndat, np.complex128)
+        lib().orc_dedispersion_response_channels_f64(chan_freq, nchan, bw, dm, ndat,
+                                                     norm_nfft or ndat, out.view(np.float64))
+    else:
+        out = np.empty(nchan * ndat, np.complex64)
+        lib().orc_dedispersion_response_channels(chan_freq, nchan, bw, dm, ndat, mode,
+                                                 norm_nfft or ndat, out.view(np.float32))
+    return out.reshape(nchan, ndat)
+
+
+def filterbank(x, nsub):
+    """x: complex (nchan_in, npol, ndat) -> (nchan_in*nsub, npol, ndat//nsub)."""
+    nchan, npol, ndat = x.shape
+    nout = ndat // nsub
+    if x.dtype == np.complex64:
+        out = np.zeros((nchan * nsub, npol, nout), np.complex64)
+        lib().orc_filterbank_f32(np.ascontiguousarray(x).view(np.float32).ravel(), ndat, ndat,
+                                 nchan, npol, nsub, out.view(np.float32).ravel(), nout)
+    else:
+        out = np.zeros((nchan * nsub, npol, nout), np.complex128)
+        lib().orc_filterbank_f64(np.ascontiguousarray(x, np.complex128).view(np.float64).ravel(),
+                                 ndat, ndat, nchan, npol, nsub, out.view(np.float64).ravel(), nout)
+    return out
 
 
 def build():

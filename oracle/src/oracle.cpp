@@ -560,6 +560,114 @@ void orc_tukey_response (unsigned impulse_neg, unsigned impulse_pos, unsigned nd
   std::memcpy (temporal_out, temporal.data (), size * sizeof (std::complex<float>));
 }
 
+double orc_channel_centre (double cf, double bw, unsigned nchan, unsigned ichan, int swap,
+                           int dc_centred)
+{
+  // Observation::get_unswapped_ichan (Observation.C:495-518), swap only
+  unsigned ch = ichan;
+  if (swap) ch = (ch + nchan / 2) % nchan;
+  return channel_centre (cf, bw, nchan, ch, dc_centred != 0);
+}
+
+} // extern "C"
+
+namespace {
+template <typename T>
+void response_channels (const double* chan_freq, unsigned nchan, double bw, double dm,
+                        unsigned ndat, int mode, unsigned norm_nfft, std::complex<T>* h)
+{
+  const double chanwidth = bw / double (nchan);
+  const double binwidth = chanwidth / double (ndat);
+  const double sign = bw / std::fabs (bw);
+  const double dispersion_per_MHz = 1e6 * dm / dm_dispersion;
+  const T s = sizeof (T) == 4 ? T (float (1.0 / std::sqrt (double (norm_nfft))))
+                              : T (1.0 / std::sqrt (double (norm_nfft)));
+  for (unsigned c = 0; c < nchan; c++)
+  {
+    const double f0 = chan_freq[c];
+    const double coeff = -sign * 2 * M_PI * dispersion_per_MHz / sqr (f0);
+    for (unsigned k = 0; k < ndat; k++)
+    {
+      // FFT-order bin k holds natural bin (k + ndat/2) mod ndat
+      const unsigned ipt = (k + ndat / 2) % ndat;
+      const double freq = double (ipt) * binwidth - 0.5 * chanwidth;
+      const double phase = coeff * sqr (freq) / (f0 + freq) + (-2.0 * M_PI * freq * 0.0);
+      std::complex<T>& o = h[uint64_t (c) * ndat + k];
+      if (sizeof (T) == 8)
+        o = std::complex<T> (T (std::cos (phase) * s), T (std::sin (phase) * s));
+      else if (mode == 0)
+      {
+        const float ph = float (phase);
+        o = std::complex<T> (T (std::cos (ph) * float (s)), T (std::sin (ph) * float (s)));
+      }
+      else
+      {
+        const double ph = phase - 2.0 * M_PI * std::nearbyint (phase / (2.0 * M_PI));
+        o = std::complex<T> (T (float (std::cos (ph)) * float (s)),
+                             T (float (std::sin (ph)) * float (s)));
+      }
+    }
+  }
+}
+
+template <typename T>
+uint64_t filterbank (const T* in, uint64_t ndat, uint64_t in_span, int nchan_in, int npol,
+                     unsigned nsub, T* out, uint64_t out_span)
+{
+  typedef std::complex<T> C;
+  const uint64_t npart = ndat / nsub;
+  // Filterbank::prepare_normalizer(1/sqrt(nsamp_fft * freq_res)), freq_res = 1,
+  // applied as a complex<float> product with (s, 0) by Response::operate
+  const T s = T (1.0 / std::sqrt (double (nsub)));
+  std::vector<C> spec (nsub);
+  for (int ic = 0; ic < nchan_in; ic++)
+    for (uint64_t ipart = 0; ipart < npart; ipart++)
+      for (int p = 0; p < npol; p++)
+      {
+        const C* x = reinterpret_cast<const C*> (in) + (uint64_t (ic) * npol + p) * in_span
+                     + ipart * nsub;
+        fft<T> (int (nsub), -1, x, spec.data ());
+        for (unsigned k = 0; k < nsub; k++)
+        {
+          const T d_r = spec[k].real (), d_i = spec[k].imag ();
+          C* o = reinterpret_cast<C*> (out) + ((uint64_t (ic) * nsub + k) * npol + p) * out_span;
+          o[ipart] = C (s * d_r - T (0) * d_i, T (0) * d_r + s * d_i);
+        }
+      }
+  return npart;
+}
+} // namespace
+
+extern "C" {
+
+void orc_dedispersion_response_channels (const double* chan_freq, unsigned nchan, double bw,
+                                         double dm, unsigned ndat, int mode, unsigned norm_nfft,
+                                         float* out)
+{
+  response_channels<float> (chan_freq, nchan, bw, dm, ndat, mode, norm_nfft,
+                            reinterpret_cast<std::complex<float>*> (out));
+}
+
+void orc_dedispersion_response_channels_f64 (const double* chan_freq, unsigned nchan, double bw,
+                                             double dm, unsigned ndat, unsigned norm_nfft,
+                                             double* out)
+{
+  response_channels<double> (chan_freq, nchan, bw, dm, ndat, 1, norm_nfft,
+                             reinterpret_cast<std::complex<double>*> (out));
+}
+
+uint64_t orc_filterbank_f32 (const float* in, uint64_t ndat, uint64_t in_span, int nchan_in,
+                             int npol, unsigned nsub, float* out, uint64_t out_span)
+{
+  return filterbank<float> (in, ndat, in_span, nchan_in, npol, nsub, out, out_span);
+}
+
+uint64_t orc_filterbank_f64 (const double* in, uint64_t ndat, uint64_t in_span, int nchan_in,
+                             int npol, unsigned nsub, double* out, uint64_t out_span)
+{
+  return filterbank<double> (in, ndat, in_span, nchan_in, npol, nsub, out, out_span);
+}
+
 uint64_t orc_convolve_f32 (const float* in, uint64_t ndat, uint64_t in_span, int nchan,
                            int npol, const float* response, unsigned nfft, unsigned nfilt_pos,
                            unsigned nfilt_neg, float* out, uint64_t out_span, int nthreads)

@@ -91,6 +91,58 @@ def test_detect_closed_forms(ctx, b2):
     assert np.array_equal(out.cpu().numpy()[:, 0], 2 * f[:, 0] ** 2 + 2 * f[:, 1] ** 2)
 
 
+# ---------------------------------------------------------------- filterbank
+
+@pytest.mark.parametrize("nsub,kind", [(64, 0), (64, 2), (16, 1), (4, 2), (32, 0)])
+def test_filterbank_matches_oracle(ctx, b2, orc, nsub, kind):
+    """Filterbank with freq_res = 1 (FilterbankEngineCPU.C:379-535) through
+    dspsr_b200_filterbank, unpack fused for int8/int16 input."""
+    rng = np.random.default_rng(nsub + kind)
+    nchan, npol, ndat = 2, 2, nsub * 3001 + 7
+    lut, _ = b2.bittable8()
+    if kind == b2.INT8_TFPD:
+        raw = rng.integers(0, 256, ndat * nchan * npol * 2, dtype=np.uint8)
+        x = orc.unpack8(raw, ndat, nchan, npol, 2, lut)
+        d_in = dev(raw)
+    elif kind == b2.INT16_TFPD:
+        raw = rng.integers(-3000, 3000, ndat * nchan * npol * 2).astype(np.int16)
+        x = orc.unpack16(raw, ndat, nchan, npol, 2)
+        d_in = dev(raw)
+    else:
+        x = rng.standard_normal((nchan, npol, 2 * ndat)).astype(np.float32)
+        d_in = dev(x)
+    x = x.view(np.complex64).reshape(nchan, npol, ndat)
+    ref = orc.filterbank(x, nsub)
+    ref64 = orc.filterbank(x.astype(np.complex128), nsub)
+    nb = ndat // nsub
+    out = torch.zeros((nchan * nsub, npol, nb), dtype=torch.complex64, device="cuda")
+    assert ctx.filterbank(kind, d_in, ndat, nchan, npol, nsub, out, nb, in_span=ndat,
+                          lut=lut) == nb
+    ctx.synchronize()
+    got = out.cpu().numpy()
+    assert rel_rms(got, ref64) < 3e-7
+    assert rel_rms(got, ref) < 3e-7
+
+
+def test_channel_response_matches_oracle(ctx, b2, orc):
+    """Per-channel response of the filterbank's DC-centred, swapped channels."""
+    nchan, nfft, bw, dm = 64, 1 << 13, 256.0, 50.0
+    freqs = orc.channel_centres(1400.0, bw, nchan, swap=True, dc_centred=True)
+    pos = orc.smearing_samples(1400.0, bw, dm, nchan, 1)
+    neg = orc.smearing_samples(1400.0, bw, dm, nchan, -1)
+    c = b2.Convolution(ctx, nchan, 2, nfft, pos, neg)
+    c.set_dedispersion_channels(freqs, bw, dm, chirp_mode=b2.CHIRP_REFERENCE)
+    got = c.get_response()
+    ref = orc.dedispersion_response_channels(freqs, bw, dm, nfft, mode=0)
+    scale = np.float32(1 / np.sqrt(nfft))
+    assert np.max(np.abs(got - ref)) < 4 * 2.0 ** -24 * scale
+    c.set_dedispersion_channels(freqs, bw, dm, chirp_mode=b2.CHIRP_FP64)
+    got = c.get_response()
+    ref64 = orc.dedispersion_response_channels(freqs, bw, dm, nfft, fp64=True)
+    assert np.max(np.abs(got - ref64)) < 2.0 ** -23 * scale
+    c.close()
+
+
 # ---------------------------------------------------------------- fold
 
 FOLD_CASES = [

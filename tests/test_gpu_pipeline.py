@@ -37,7 +37,17 @@ def oracle_chain(orc, b2, raw_blocks, cfg, fp64=False):
     x = x.view(np.complex64).reshape(nchan, npol, ndat_tot)
     nfft, pos, neg = cfg["nfft"], cfg["pos"], cfg["neg"]
     nk = nfft - pos - neg
-    if fp64:
+    fb = cfg.get("fb", 0)
+    if fb:
+        # Filterbank (freq_res = 1): DC-centred, swapped output channels
+        x = orc.filterbank(x.astype(np.complex128) if fp64 else x, fb)
+        nchan *= fb
+        ndat_tot //= fb
+        freqs = orc.channel_centres(cfg["cf"], cfg["bw"], nchan, swap=True, dc_centred=True)
+        h = orc.dedispersion_response_channels(freqs, cfg["bw"], cfg["dm"], nfft, mode=0,
+                                               fp64=fp64)
+        y = orc.convolve(x, h, nfft, pos, neg)
+    elif fp64:
         h = orc.dedispersion_response_f64(cfg["cf"], cfg["bw"], cfg["dm"], nchan, nfft,
                                           input_nchan=nchan)
         y = orc.convolve(x.astype(np.complex128), h, nfft, pos, neg)
@@ -57,7 +67,9 @@ def oracle_chain(orc, b2, raw_blocks, cfg, fp64=False):
     hits = np.zeros(nbin, np.uint32)
     in0, carry = 0, 0
     for r in raw_blocks:
-        nb = r.shape[-1] // 2 if kind == b2.FLOAT_FPT else r.size // (nchan * npol * 2)
+        nb = r.shape[-1] // 2 if kind == b2.FLOAT_FPT else r.size // (cfg["nchan"] * npol * 2)
+        if fb:
+            nb //= fb
         ndat = carry + nb
         npart = (ndat - pos - neg) // nk if ndat >= nfft else 0
         nout = npart * nk
@@ -97,7 +109,8 @@ def run_pipeline(ctx, b2, blocks, cfg, host=False):
                        cfg["pos"], cfg["neg"], cfg["nbin"], cfg["period"], state=cfg["state"],
                        input_kind=cfg["kind"], lut=cfg["lut"], start_mjd=START, epoch_mjd=EPOCH,
                        scratch_bytes=cfg.get("scratch", 0),
-                       chirp_mode=cfg.get("chirp", b2.CHIRP_REFERENCE))
+                       chirp_mode=cfg.get("chirp", b2.CHIRP_REFERENCE),
+                       filterbank_nchan=cfg.get("fb", 0))
     pl = b2.Pipeline(ctx, c)
     total = 0
     for r in blocks:
@@ -120,7 +133,9 @@ def base_cfg(b2, **kw):
     cfg = dict(cf=1400.0, bw=16.0, dm=5.0, nchan=1, npol=2, nbin=256, period=0.0123,
                state=b2.INTENSITY, kind=b2.INT8_TFPD, lut=b2.bittable8()[0])
     cfg.update(kw)
-    pos, neg, nfft = b2.dispersion_plan(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nchan"],
+    # with a filterbank the smearing is that of its output channels
+    nchan_conv = cfg["nchan"] * (cfg.get("fb", 0) or 1)
+    pos, neg, nfft = b2.dispersion_plan(cfg["cf"], cfg["bw"], cfg["dm"], nchan_conv,
                                         cfg.get("nfft"))
     cfg.update(pos=pos, neg=neg, nfft=nfft)
     return cfg
@@ -162,6 +177,11 @@ CASES = {
                          scratch=8 << 20),
     # one polarisation, intensity, fused 4096
     "onepol_4096": dict(dm=1.0, npol=1, nfft=4096),
+    # C2 shape: 64-channel FFT filterbank of 256 MHz, per-channel dedispersion,
+    # full Stokes, single-kernel path (DM 50 -> 8192) and four-step (DM 500 -> 2^16)
+    "c2_filterbank_8k": dict(dm=50.0, bw=256.0, fb=64, state=3, nbin=2048, period=5.757e-3),
+    "c2_filterbank_64k": dict(dm=500.0, bw=256.0, fb=64, nfft=1 << 16, state=3, nbin=2048,
+                              period=5.757e-3),
 }
 
 
@@ -172,6 +192,10 @@ def test_pipeline_matches_oracle_chain(ctx, b2, orc, name):
     nk = cfg["nfft"] - cfg["pos"] - cfg["neg"]
     # three uneven blocks: the carry spans block boundaries
     sizes = [cfg["nfft"] + 3 * nk + 17, 2 * nk - 5, nk + 1234]
+    if cfg.get("fb"):
+        # whole filterbank transforms per block; fewer parts for the CPU oracle
+        fb = cfg["fb"]
+        sizes = [(cfg["nfft"] + nk + 17) * fb, (nk - 5) * fb, (nk // 2 + 1234) * fb]
     blocks = make_blocks(rng, cfg, sizes)
     prof, hits, total, info = run_pipeline(ctx, b2, blocks, cfg)
     rprof, rhits, rtotal = oracle_chain(orc, b2, blocks, cfg)
