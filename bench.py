@@ -41,7 +41,14 @@ CONFIGS = {
                   "2 pol int8, DM 67.99, FFT 2^17 (2^15 is below the reference's minimum), "
                   "Intensity, 1024-bin fold, P=89.33 ms, 2^24 samples/pol per block"),
         cf=1400.0, bw=16.0, dm=67.99, nchan=1, npol=2, nfft=1 << 17, nbin=1024,
-        period=0.08933, state=0, ndat=1 << 24, duty=0.03, snr=20.0, sigma=10.0),
+        period=0.08933, state=0, ndat=1 << 24, duty=0.03, snr=20.0, sigma=10.0, fb=0),
+    "c2": dict(
+        workload=("filterbank + coherent dedispersion: 256 MHz complex baseband at 1400 MHz, "
+                  "2 pol int8, FFT filterbank to 64 x 4 MHz channels, DM 500, per-channel FFT "
+                  "2^16, full Stokes, 2048-bin fold, P=5.757 ms, 2^26 samples/pol per block "
+                  "(four blocks = the 2^28-sample data set)"),
+        cf=1400.0, bw=256.0, dm=500.0, nchan=1, npol=2, nfft=1 << 16, nbin=2048,
+        period=5.757e-3, state=3, ndat=1 << 26, duty=0.03, snr=10.0, sigma=12.0, fb=64),
 }
 
 NBLOCKS = 4
@@ -149,15 +156,17 @@ def measured_peaks():
 
 
 def ncu_traffic(kernel):
-    """DRAM bytes per unit of work of a kernel from a committed ncu summary
-    (profiles/ncu_traffic.txt: 'kernel=<name> bytes_per_part=<B>')."""
+    """DRAM bytes per input sample of a kernel from a committed ncu summary
+    (profiles/ncu_traffic.txt lines 'kernel=<config>:<name> bytes_per_sample=<B>',
+    each from one ncu capture, dram__bytes_read.sum + dram__bytes_write.sum of a
+    launch divided by the input samples that launch covered)."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
     if not os.path.exists(p):
         return None
     for line in open(p):
         parts = dict(kv.split("=", 1) for kv in line.split() if "=" in kv)
-        if parts.get("kernel") == kernel and "bytes_per_part" in parts:
-            return float(parts["bytes_per_part"])
+        if parts.get("kernel") == kernel and "bytes_per_sample" in parts:
+            return float(parts["bytes_per_sample"])
     return None
 
 
@@ -209,39 +218,61 @@ def make_blocks(cfg, seed, device):
 # reference's CPU path; test infrastructure, timed here as the CPU baseline)
 # ---------------------------------------------------------------------------
 
+def nchan_conv(cfg):
+    """Channels the dedispersion sees (after the filterbank, if any)."""
+    return cfg["nchan"] * (cfg["fb"] or 1)
+
+
 def cpu_prepare(cfg):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
     orc.lib()
-    pos = orc.smearing_samples(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nchan"], 1)
-    neg = orc.smearing_samples(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nchan"], -1)
+    nc = nchan_conv(cfg)
+    pos = orc.smearing_samples(cfg["cf"], cfg["bw"], cfg["dm"], nc, 1)
+    neg = orc.smearing_samples(cfg["cf"], cfg["bw"], cfg["dm"], nc, -1)
     lut, _ = orc.bittable8(0.0308)
-    h = orc.dedispersion_response(cfg["cf"], cfg["bw"], cfg["dm"], 1, cfg["nfft"], mode=0)
+    if cfg["fb"]:
+        freqs = orc.channel_centres(cfg["cf"], cfg["bw"], nc, swap=True, dc_centred=True)
+        h = orc.dedispersion_response_channels(freqs, cfg["bw"], cfg["dm"], cfg["nfft"], mode=0)
+    else:
+        h = orc.dedispersion_response(cfg["cf"], cfg["bw"], cfg["dm"], 1, cfg["nfft"], mode=0)
     return orc, pos, neg, lut, h
 
 
 def cpu_sample(cfg, orc, pos, neg, lut, h, nparts, seed=1):
-    """Bounded sample: nparts FFT parts of the block (int8 noise + pulse)."""
+    """Bounded sample: nparts FFT parts (of every channel) of a block, int8 noise."""
     from dspsr_b200 import synth
     nk = cfg["nfft"] - pos - neg
-    ndat = cfg["nfft"] + (nparts - 1) * nk
-    raw = synth.noise_block(ndat, 1, cfg["npol"], cfg["sigma"], seed)
+    ndat = (cfg["nfft"] + (nparts - 1) * nk) * (cfg["fb"] or 1)
+    raw = synth.noise_block(ndat, cfg["nchan"], cfg["npol"], cfg["sigma"], seed)
     return raw, ndat
 
 
 def cpu_run(cfg, orc, pos, neg, lut, h, raw, ndat, threads):
-    rate = abs(cfg["bw"]) * 1e6
+    """The reference's CPU chain on one sample: unpack -> (filterbank) ->
+    overlap-save -> detection -> fold (oracle/, all host threads in the FFTs)."""
+    nc = nchan_conv(cfg)
+    rate = abs(cfg["bw"]) / nc * 1e6
     phi = orc.fold_phi(START_MJD, EPOCH_MJD, pos, rate, cfg["period"])
+    pps = (1 / rate) / cfg["period"]
     t0 = time.perf_counter()
-    orc.pipeline_c1(raw, ndat, lut, h, cfg["nfft"], pos, neg, phi, (1 / rate) / cfg["period"],
-                    cfg["nbin"], threads)
+    if not cfg["fb"]:
+        orc.pipeline_c1(raw, ndat, lut, h, cfg["nfft"], pos, neg, phi, pps, cfg["nbin"], threads)
+    else:
+        x = orc.unpack8(raw, ndat, cfg["nchan"], cfg["npol"], 2, lut)
+        x = x.view(np.complex64).reshape(cfg["nchan"], cfg["npol"], ndat)
+        y = orc.filterbank(x, cfg["fb"])
+        z = orc.convolve(y, h, cfg["nfft"], pos, neg, nthreads=threads)
+        d = orc.detect(z, cfg["state"])
+        plan = orc.fold_binplan(phi, pps, z.shape[2], cfg["nbin"])
+        orc.fold_accumulate(d, plan, cfg["nbin"])
     return time.perf_counter() - t0
 
 
 def block_parts(cfg, pos, neg):
-    """FFT parts one block of the workload holds."""
+    """FFT parts (per channel) one block of the workload holds."""
     nk = cfg["nfft"] - pos - neg
-    return (cfg["ndat"] - pos - neg) // nk
+    return (cfg["ndat"] // (cfg["fb"] or 1) - pos - neg) // nk
 
 
 def cpu_baseline(cfg, target_s=15.0):
@@ -259,7 +290,7 @@ def cpu_baseline(cfg, target_s=15.0):
     msps = ndat * cfg["npol"] * reps / total / 1e6
     return {"value": round(msps, 3), "unit": "complex Msamples/s", "cores": threads,
             "kind": "port",
-            "sample": (f"one workload block ({nparts} FFT parts, {ndat} samples/pol, "
+            "sample": (f"{nparts} FFT parts per channel ({ndat} input samples/pol, "
                        f"{cfg['npol']} pol) x {reps} through the oracle CPU restatement "
                        f"(self-written FP32 FFT, OpenMP over parts), {total:.1f} s")}
 
@@ -309,13 +340,13 @@ def run_b200(args, cfg, world, rank, local):
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
     ctx = b2.Context(local)
-    pos, neg, nfft = b2.dispersion_plan(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nchan"],
-                                        cfg["nfft"])
+    nc = nchan_conv(cfg)
+    pos, neg, nfft = b2.dispersion_plan(cfg["cf"], cfg["bw"], cfg["dm"], nc, cfg["nfft"])
     nk = nfft - pos - neg
     lut, _ = b2.bittable8()
     c = b2.make_config(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nchan"], cfg["npol"], nfft, pos,
                        neg, cfg["nbin"], cfg["period"], state=cfg["state"], lut=lut,
-                       start_mjd=START_MJD, epoch_mjd=EPOCH_MJD)
+                       start_mjd=START_MJD, epoch_mjd=EPOCH_MJD, filterbank_nchan=cfg["fb"])
     blocks = make_blocks(cfg, 1234 + rank, device)
     ndat = cfg["ndat"]
     samples_per_step = ndat * cfg["npol"]   # complex samples consumed per step (all pols)
@@ -331,7 +362,6 @@ def run_b200(args, cfg, world, rank, local):
     for i in range(args.warmup):
         pl.run(blocks[i % NBLOCKS], ndat)
     torch.cuda.synchronize()
-    pl.profile(True)
     barrier(world)
     torch.cuda.synchronize()
     launches0 = b2.kernel_launches()
@@ -347,12 +377,19 @@ def run_b200(args, cfg, world, rank, local):
     barrier(world)
     ms = ev0.elapsed_time(ev1)
     ms_max = max_over_ranks(ms, world)
+    value = samples_per_step * args.steps * world / (ms_max / 1e3) / 1e6
+
+    # the same K steps again with CUDA events around every kernel, for the
+    # per-kernel durations of the roofline (the events themselves cost ~10 %,
+    # so `value` above is taken without them)
+    pl.profile(True)
+    for i in range(args.steps):
+        pl.run(blocks[(args.warmup + i) % NBLOCKS], ndat)
     ktimes = pl.kernel_times()
     pl.profile(False)
     info = pl.info()
     prof, hits = pl.get_profiles()
     pl.close()
-    value = samples_per_step * args.steps * world / (ms_max / 1e3) / 1e6
 
     # ---- end to end through the public API from pinned host memory ----------
     host = [b.cpu().pin_memory() for b in blocks]
@@ -379,21 +416,24 @@ def run_b200(args, cfg, world, rank, local):
     # ---- roofline of the dominant kernel -----------------------------------
     hbm_peak, bf16_peak, peak_src = measured_peaks()
     name, (kms, kn) = max(ktimes.items(), key=lambda kv: kv[1][0])
-    # parts processed in the timed region = output samples / nkeep
-    parts = folded // nk
-    parts_per_launch = parts / max(kn, 1)
-    # algorithmic bytes per part: the int8 input of the new samples it
-    # dedisperses (2 bytes per complex sample per pol)
-    alg_bytes = 2.0 * cfg["npol"] * nk * parts_per_launch
+    # Algorithmic bytes: the int8 input, 2 bytes per complex sample per pol.
+    # Each kernel kind covers all input of the timed region over its kn
+    # launches (a batch of FFT parts of every channel, or a whole block).
+    samples_per_launch = ndat * args.steps / max(kn, 1)
+    alg_bytes = 2.0 * cfg["npol"] * samples_per_launch
     avg_s = kms / 1e3 / max(kn, 1)
     achieved = alg_bytes / avg_s / 1e9
-    tb = ncu_traffic(name)
-    traffic = tb * parts_per_launch if tb else None
+    tb = ncu_traffic(f"{args.config}:{name}")
+    # committed summaries give DRAM bytes per input sample of the kernel
+    traffic = tb * samples_per_launch if tb else None
     # FP32 view: flops per output sample of the FFT convolution (log2 N radix-2
-    # count, both transforms, overlap included) + detection + fold
+    # count, both transforms, overlap included) + detection + fold (+ the
+    # filterbank's own FFT when there is one)
     import math
     flop_per_sample = (nfft / nk) * (2 * 5 * math.log2(nfft) + 6) + 5
-    fp32_tflops = flop_per_sample * folded * cfg["npol"] / (ms / 1e3) / 1e12
+    if cfg["fb"]:
+        flop_per_sample += 5 * math.log2(cfg["fb"]) + 2
+    fp32_tflops = flop_per_sample * folded * nc * cfg["npol"] / (ms / 1e3) / 1e12
     fp32_peak = 148 * 128 * 2 * (clk["sm_mhz"] or 1965.0) * 1e6 / 1e12
 
     line = {
@@ -404,6 +444,7 @@ def run_b200(args, cfg, world, rank, local):
         "data": "synthetic (seeded Gaussian noise + FP64-dispersed pulse train, int8)",
         "config": {"workload": cfg["workload"], "nfft": nfft, "nfilt_pos": pos,
                    "nfilt_neg": neg, "nkeep": nk, "fft_split": [info["n1"], info["n2"]],
+                   "filterbank_nchan": cfg["fb"], "nchan_dedispersed": nc,
                    "parts_per_batch": info["max_batch"],
                    "l2": f"inputs larger than L2: {NBLOCKS} distinct {bytes_per_block >> 20} MiB "
                          "blocks cycled",

@@ -588,8 +588,10 @@ int pipeline_input (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat, ui
   in.npol = cfg.npol;
   in.offset_binary = cfg.offset_binary;
   const float scale = float (1.0 / std::sqrt (double (pl->fb_nsub)));
+  KernelClock kc {&PipeClock::mark, &pl->clock};
   B200_CHECK (ctx, launch_filterbank (in, pl->conv.lut.ptr, pl->fb_nsub, nb, scale, pl->fbbuf.ptr,
-                                      nb, ctx->stream), "filterbank");
+                                      nb, ctx->stream, pl->clock.on ? &kc : nullptr),
+              "filterbank");
   return pipeline_block (pl, pl->fbbuf.ptr, nb, nb, ndat_folded);
 }
 

@@ -1004,10 +1004,11 @@ cudaError_t launch_unpermute_response (float2* dst, const float2* H, unsigned nc
 namespace {
 template <int NSUB>
 cudaError_t run_filterbank (const InputView& in, const float* d_lut, uint64_t nblk, float scale,
-                            float2* out, uint64_t out_span, cudaStream_t st)
+                            float2* out, uint64_t out_span, cudaStream_t st,
+                            const KernelClock* clk)
 {
   const dim3 grid (unsigned ((nblk + 127) / 128), in.npol, in.nchan);
-  g_launches++;
+  ClockScope cs (clk, KK_FILTERBANK, st);
   if (in.kind == IN_INT8)
     k_filterbank<NSUB, IN_INT8><<<grid, 128, 0, st>>> (in, d_lut, nblk, scale, out, out_span);
   else if (in.kind == IN_INT16)
@@ -1020,16 +1021,16 @@ cudaError_t run_filterbank (const InputView& in, const float* d_lut, uint64_t nb
 
 cudaError_t launch_filterbank (const InputView& in, const float* d_lut, unsigned nsub,
                                uint64_t nblk, float scale, float2* out, uint64_t out_span,
-                               cudaStream_t st)
+                               cudaStream_t st, const KernelClock* clk)
 {
   if (nblk == 0) return cudaSuccess;
   switch (nsub)
   {
-    case 4: return run_filterbank<4> (in, d_lut, nblk, scale, out, out_span, st);
-    case 8: return run_filterbank<8> (in, d_lut, nblk, scale, out, out_span, st);
-    case 16: return run_filterbank<16> (in, d_lut, nblk, scale, out, out_span, st);
-    case 32: return run_filterbank<32> (in, d_lut, nblk, scale, out, out_span, st);
-    case 64: return run_filterbank<64> (in, d_lut, nblk, scale, out, out_span, st);
+    case 4: return run_filterbank<4> (in, d_lut, nblk, scale, out, out_span, st, clk);
+    case 8: return run_filterbank<8> (in, d_lut, nblk, scale, out, out_span, st, clk);
+    case 16: return run_filterbank<16> (in, d_lut, nblk, scale, out, out_span, st, clk);
+    case 32: return run_filterbank<32> (in, d_lut, nblk, scale, out, out_span, st, clk);
+    case 64: return run_filterbank<64> (in, d_lut, nblk, scale, out, out_span, st, clk);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -70,7 +70,10 @@ void make_pass_tables (unsigned n, float2* out, unsigned capacity);
 unsigned pass_tables_count (unsigned n);
 
 // Kernels of the convolution path, for per-kernel timing.
-enum KernelKind { KK_FWD_COLS = 0, KK_ROWS = 1, KK_INV_COLS = 2, KK_FUSED = 3, KK_COUNT = 4 };
+enum KernelKind
+{
+  KK_FWD_COLS = 0, KK_ROWS = 1, KK_INV_COLS = 2, KK_FUSED = 3, KK_FILTERBANK = 4, KK_COUNT = 5
+};
 
 // Optional per-kernel clock: mark(self, kind, 0|1, stream) is called right
 // before (0) and after (1) each kernel launch of the convolution path.
@@ -110,7 +113,7 @@ cudaError_t launch_unpermute_response (float2* dst, const float2* H, unsigned nc
 // cin*nsub + k, span out_span.
 cudaError_t launch_filterbank (const InputView& in, const float* d_lut, unsigned nsub,
                                uint64_t nblk, float scale, float2* out, uint64_t out_span,
-                               cudaStream_t stream);
+                               cudaStream_t stream, const KernelClock* clock = nullptr);
 
 cudaError_t launch_unpack8 (const uint8_t* in, uint64_t ndat, unsigned nchan, unsigned npol,
                             unsigned ndim, const float* d_lut, float* out, uint64_t span,

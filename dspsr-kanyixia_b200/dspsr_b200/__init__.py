@@ -304,12 +304,12 @@ class Pipeline:
         self.ctx.check(self._lib.dspsr_b200_pipeline_profile(self.handle, int(enable)),
                        "pipeline_profile")
 
-    KERNELS = ("fwd_cols", "rows", "inv_cols_detect_fold", "fused")
+    KERNELS = ("fwd_cols", "rows", "inv_cols_detect_fold", "fused", "filterbank")
 
     def kernel_times(self):
         """{kernel: (milliseconds, launches)} since the last call."""
-        ms = (ctypes.c_double * 4)()
-        n = (ctypes.c_uint64 * 4)()
+        ms = (ctypes.c_double * 5)()
+        n = (ctypes.c_uint64 * 5)()
         self.ctx.check(self._lib.dspsr_b200_pipeline_kernel_times(self.handle, ms, n),
                        "kernel_times")
         return {k: (ms[i], n[i]) for i, k in enumerate(self.KERNELS)}

@@ -277,7 +277,8 @@ int dspsr_b200_pipeline_reset (dspsr_b200_pipeline* pipe);
    inverse column pass with detect+fold, single-kernel path). */
 int dspsr_b200_pipeline_profile (dspsr_b200_pipeline* pipe, int enable);
 /* Milliseconds and launch counts per kernel kind since the last call
-   (ms[4], launches[4]: columns, rows, inverse columns, single-kernel). */
+   (ms[5], launches[5]: columns, rows, inverse columns, single-kernel,
+   filterbank). */
 int dspsr_b200_pipeline_kernel_times (dspsr_b200_pipeline* pipe, double* ms,
                                       uint64_t* launches);
 /* Kernels launched by this library since it was loaded. */
