@@ -1,0 +1,198 @@
+// dsp_b200_engines.cpp -- C++ engines over the C ABI (see dsp_b200_engines.h)
+
+#include "dsp_b200_engines.h"
+
+#include <string>
+
+namespace b200 {
+
+namespace {
+std::string message (dspsr_b200_context* ctx, const char* where)
+{
+  std::string m = where;
+  if (ctx)
+  {
+    m += ": ";
+    m += dspsr_b200_last_error (ctx);
+  }
+  return m;
+}
+} // namespace
+
+Context::Context (int device, void* stream)
+{
+  const int rc = dspsr_b200_context_create (device, stream, &ctx);
+  if (rc)
+    throw Error (rc, rc == DSPSR_B200_ENODEV ? "Context: no CUDA device"
+                                             : "Context: dspsr_b200_context_create failed");
+}
+
+Context::~Context ()
+{
+  if (ctx) dspsr_b200_context_destroy (ctx);
+}
+
+void Context::check (int rc, const char* where) const
+{
+  if (rc) throw Error (rc, message (ctx, where));
+}
+
+void Context::synchronize () { check (dspsr_b200_synchronize (ctx), "synchronize"); }
+
+// ---- convolution ------------------------------------------------------------
+
+ConvolutionEngine::~ConvolutionEngine ()
+{
+  if (conv) dspsr_b200_convolution_destroy (conv);
+}
+
+void ConvolutionEngine::prepare (unsigned nchan, unsigned npol, unsigned nfft,
+                                 unsigned nfilt_pos, unsigned nfilt_neg)
+{
+  if (conv) dspsr_b200_convolution_destroy (conv);
+  conv = nullptr;
+  ctx.check (dspsr_b200_convolution_create (ctx.handle (), nchan, npol, nfft, nfilt_pos,
+                                            nfilt_neg, &conv),
+             "ConvolutionEngine::prepare");
+}
+
+void ConvolutionEngine::copy_response (const float* response)
+{
+  ctx.check (dspsr_b200_convolution_copy_response (conv, response),
+             "ConvolutionEngine::copy_response");
+}
+
+void ConvolutionEngine::set_dedispersion (double cf, double bw, double dm, int input_nchan,
+                                          int dual_sideband, int chirp_mode)
+{
+  ctx.check (dspsr_b200_convolution_set_dedispersion (conv, cf, bw, dm, input_nchan,
+                                                      dual_sideband, 0, chirp_mode, 0),
+             "ConvolutionEngine::set_dedispersion");
+}
+
+uint64_t ConvolutionEngine::perform (const TimeSeriesView& in, TimeSeriesView& out)
+{
+  if (in.ndim != 2 || out.ndim != 2)
+    throw Error (DSPSR_B200_ESTATE, "ConvolutionEngine::perform: complex data required");
+  uint64_t npart = 0;
+  ctx.check (dspsr_b200_convolution_perform (conv, in.base, in.span_floats / 2, in.ndat,
+                                             out.base, out.span_floats / 2, &npart),
+             "ConvolutionEngine::perform");
+  return npart;
+}
+
+// ---- filterbank ---------------------------------------------------------------
+
+uint64_t FilterbankEngine::perform (const TimeSeriesView& in, TimeSeriesView& out)
+{
+  if (out.nchan != in.nchan * nsub)
+    throw Error (DSPSR_B200_ESTATE, "FilterbankEngine::perform: output nchan mismatch");
+  uint64_t n = 0;
+  ctx.check (dspsr_b200_filterbank (ctx.handle (), DSPSR_B200_FLOAT_FPT, in.base, in.ndat,
+                                    in.span_floats / 2, in.nchan, in.npol, nsub, nullptr, 0,
+                                    out.base, out.span_floats / 2, &n),
+             "FilterbankEngine::perform");
+  out.ndat = n;
+  return n;
+}
+
+// ---- detection -------------------------------------------------------------
+
+void DetectionEngine::square_law (const TimeSeriesView& in, TimeSeriesView& out)
+{
+  ctx.check (dspsr_b200_detect (ctx.handle (), in.base, in.span_floats / 2, in.ndat, in.nchan,
+                                DSPSR_B200_INTENSITY, out.base, out.span_floats),
+             "DetectionEngine::square_law");
+}
+
+void DetectionEngine::polarimetry (unsigned ndim, const TimeSeriesView& in, TimeSeriesView& out,
+                                   int state)
+{
+  (void) ndim;   // output is FPT with one float per product (ndim 1)
+  ctx.check (dspsr_b200_detect (ctx.handle (), in.base, in.span_floats / 2, in.ndat, in.nchan,
+                                state, out.base, out.span_floats),
+             "DetectionEngine::polarimetry");
+}
+
+// ---- fold -------------------------------------------------------------------
+
+FoldEngine::~FoldEngine ()
+{
+  if (fold_) dspsr_b200_fold_destroy (fold_);
+}
+
+void FoldEngine::ensure (unsigned nc, unsigned np)
+{
+  if (fold_ && nc == nchan && np == npol) return;
+  if (fold_) dspsr_b200_fold_destroy (fold_);
+  fold_ = nullptr;
+  nchan = nc;
+  npol = np;
+  ctx.check (dspsr_b200_fold_create (ctx.handle (), nbin, nchan, npol, &fold_),
+             "FoldEngine::setup");
+}
+
+void FoldEngine::setup (unsigned nc, unsigned np) { ensure (nc, np); }
+
+void FoldEngine::set_nbin (unsigned n)
+{
+  if (n != nbin && fold_)
+  {
+    dspsr_b200_fold_destroy (fold_);
+    fold_ = nullptr;
+  }
+  nbin = n;
+}
+
+void FoldEngine::set_ndat (uint64_t n, uint64_t idat_start)
+{
+  (void) idat_start;
+  ndat = n;
+}
+
+uint64_t FoldEngine::set_bins (double phi, double pps, uint64_t n, uint64_t idat_start)
+{
+  if (!fold_) ensure (nchan ? nchan : 1, npol ? npol : 1);
+  ctx.check (dspsr_b200_fold_set_bins (fold_, phi, pps, n, idat_start, &ndat_folded),
+             "FoldEngine::set_bins");
+  hits_valid = false;
+  return ndat_folded;
+}
+
+unsigned FoldEngine::get_bin_hits (unsigned ibin)
+{
+  if (!hits_valid)
+  {
+    std::vector<float> p;
+    synch (p, hits_cache);
+  }
+  return ibin < hits_cache.size () ? hits_cache[ibin] : 0;
+}
+
+void FoldEngine::fold (const TimeSeriesView& in)
+{
+  ensure (in.nchan, in.npol);
+  ctx.check (dspsr_b200_fold_fold (fold_, in.base, in.span_floats), "FoldEngine::fold");
+  hits_valid = false;
+}
+
+void FoldEngine::synch (std::vector<float>& profiles, std::vector<uint32_t>& hits)
+{
+  profiles.assign (uint64_t (nchan) * npol * nbin, 0.f);
+  hits.assign (nbin, 0u);
+  ctx.check (dspsr_b200_fold_get_profiles (fold_, profiles.data (), hits.data ()),
+             "FoldEngine::synch");
+  hits_cache = hits;
+  hits_valid = true;
+}
+
+// ---- unpack -----------------------------------------------------------------
+
+void unpack8 (Context& ctx, const void* d_bytes, const float lut256[256], TimeSeriesView& out)
+{
+  ctx.check (dspsr_b200_unpack8 (ctx.handle (), d_bytes, out.ndat, out.nchan, out.npol,
+                                 out.ndim, lut256, out.base, out.span_floats),
+             "unpack8");
+}
+
+} // namespace b200

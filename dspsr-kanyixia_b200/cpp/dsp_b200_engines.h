@@ -1,0 +1,144 @@
+// dsp_b200_engines.h -- C++ engines with the shapes of DSPSR's CUDA engines,
+// implemented over the C ABI of libdspsr_b200.so (include/dspsr_b200.h).
+//
+// DSPSR's operations (dsp::Convolution, dsp::Detection, dsp::Fold,
+// dsp::Filterbank, dsp::GenericEightBitUnpacker) keep all bookkeeping and
+// call a pluggable Engine with raw device pointers, strides and counts.  The
+// classes here have the method names and argument meanings of those engines
+// (recovered from their call sites, because the reference's Signal/General
+// headers are not part of the snapshot):
+//
+//   Convolution::Engine  prepare / copy_response / perform      Convolution.C:446-452, 656-698
+//   Filterbank::Engine   setup / perform                        Filterbank.C:245-256, 549-565
+//   Detection::Engine    square_law / polarimetry               Detection.C:237-242, 483-489
+//   Fold::Engine         set_nbin / set_ndat / set_bins / fold  Fold.C:760-887, 1011-1035
+//                        get_bin_hits / synch
+//
+// A TimeSeriesView carries what those call sites read from a dsp::TimeSeries
+// (get_datptr(0,0), get_nfloat_span(), get_ndat(), get_nchan(), get_npol()).
+// Every failure throws b200::Error carrying the C ABI's status and message,
+// as the reference throws its Error (InvalidParam / InvalidState / FailedCall).
+#pragma once
+
+#include "dspsr_b200.h"
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace b200 {
+
+class Error : public std::runtime_error
+{
+public:
+  Error (int code, const std::string& what) : std::runtime_error (what), code (code) {}
+  int code;
+};
+
+// The fields of a dsp::TimeSeries that the engines use.  FPT order: the data
+// of (chan, pol) start at base + (chan*npol + pol) * span_floats.
+struct TimeSeriesView
+{
+  float* base = nullptr;        // get_datptr (0, 0), device memory
+  uint64_t span_floats = 0;     // get_nfloat_span ()
+  uint64_t ndat = 0;            // get_ndat ()
+  unsigned nchan = 1;
+  unsigned npol = 1;
+  unsigned ndim = 2;            // 2 = complex (Signal::Analytic)
+};
+
+// One device + stream (CUDA::DeviceMemory(stream) in SingleThread::construct)
+class Context
+{
+public:
+  explicit Context (int device = 0, void* stream = nullptr);
+  ~Context ();
+  Context (const Context&) = delete;
+  Context& operator= (const Context&) = delete;
+  dspsr_b200_context* handle () const { return ctx; }
+  void check (int rc, const char* where) const;
+  void synchronize ();
+private:
+  dspsr_b200_context* ctx = nullptr;
+};
+
+// CUDA::ConvolutionEngine
+class ConvolutionEngine
+{
+public:
+  explicit ConvolutionEngine (Context& ctx) : ctx (ctx) {}
+  ~ConvolutionEngine ();
+  // Engine::prepare(Convolution*): the sizes Convolution::prepare computed
+  void prepare (unsigned nchan, unsigned npol, unsigned nfft, unsigned nfilt_pos,
+                unsigned nfilt_neg);
+  // Engine::copy_response(const Response*): nchan*nfft complex floats, FFT order
+  void copy_response (const float* response);
+  // Dedispersion built on the device (FP64 phase); chirp_mode as in the C ABI
+  void set_dedispersion (double centre_freq, double bandwidth, double dm, int input_nchan,
+                         int dual_sideband, int chirp_mode = DSPSR_B200_CHIRP_REFERENCE);
+  // Engine::perform(input, output, npart); returns npart
+  uint64_t perform (const TimeSeriesView& input, TimeSeriesView& output);
+private:
+  Context& ctx;
+  dspsr_b200_convolution* conv = nullptr;
+};
+
+// CUDA::FilterbankEngine for freq_res = 1 (no "During" convolution)
+class FilterbankEngine
+{
+public:
+  FilterbankEngine (Context& ctx, unsigned nchan_subband) : ctx (ctx), nsub (nchan_subband) {}
+  // Engine::perform(in, out, npart, in_step, out_step) with in_step = nsub and
+  // out_step = 1 per part; returns the output samples per channel
+  uint64_t perform (const TimeSeriesView& input, TimeSeriesView& output);
+private:
+  Context& ctx;
+  unsigned nsub;
+};
+
+// CUDA::DetectionEngine
+class DetectionEngine
+{
+public:
+  explicit DetectionEngine (Context& ctx) : ctx (ctx) {}
+  void square_law (const TimeSeriesView& input, TimeSeriesView& output);           // Intensity
+  void polarimetry (unsigned ndim, const TimeSeriesView& input, TimeSeriesView& output,
+                    int state = DSPSR_B200_COHERENCE);
+private:
+  Context& ctx;
+};
+
+// CUDA::FoldEngine with use_set_bins = true
+class FoldEngine
+{
+public:
+  explicit FoldEngine (Context& ctx) : ctx (ctx) {}
+  ~FoldEngine ();
+  const bool use_set_bins = true;
+  // Engine::setup (Fold.C:1011-1035): the input's channels and polarisations
+  void setup (unsigned nchan, unsigned npol);
+  void set_nbin (unsigned nbin);
+  void set_ndat (uint64_t ndat, uint64_t idat_start);
+  // Engine::set_bins(phi, phase_per_sample, ndat, idat_start): returns ndat_folded
+  uint64_t set_bins (double phi, double phase_per_sample, uint64_t ndat, uint64_t idat_start);
+  unsigned get_bin_hits (unsigned ibin);
+  void fold (const TimeSeriesView& input);
+  // Engine::synch(PhaseSeries*): profiles [chan][pol][bin] and hits
+  void synch (std::vector<float>& profiles, std::vector<uint32_t>& hits);
+  uint64_t get_ndat_folded () const { return ndat_folded; }
+private:
+  void ensure (unsigned nchan, unsigned npol);
+  Context& ctx;
+  dspsr_b200_fold* fold_ = nullptr;
+  unsigned nbin = 0, nchan = 0, npol = 0;
+  uint64_t ndat = 0, ndat_folded = 0;
+  std::vector<uint32_t> hits_cache;
+  bool hits_valid = false;
+};
+
+// GenericEightBitUnpacker::unpack_on_gpu: TFPD bytes on the device -> FPT
+void unpack8 (Context& ctx, const void* d_bytes, const float lut256[256],
+              TimeSeriesView& output);
+
+} // namespace b200
