@@ -63,8 +63,9 @@ int main ()
     conv.copy_response (unit.data ());
     b200::TimeSeriesView y = x;
     y.base = d_y;
+    // npart = (ndat - nfilt) / nkeep (Convolution.C:486-487) = (nfft + 3 nkeep - nfilt) / nkeep
     const uint64_t npart = conv.perform (x, y);
-    CHECK (npart == 3, "npart=%llu", (unsigned long long) npart);
+    CHECK (npart == 4, "npart=%llu", (unsigned long long) npart);
     std::vector<float> hx (ndat * npol * 2), hy (ndat * npol * 2);
     ctx.synchronize ();
     cudaMemcpy (hx.data (), d_x, hx.size () * 4, cudaMemcpyDeviceToHost);
