@@ -209,6 +209,8 @@ def make_blocks(cfg, seed, device):
         blocks.append(out.reshape(-1).view(torch.uint8))
         del ph, on
     del chirp
+    # hand the synthesis buffers back so that only the pipeline's memory stays
+    torch.cuda.empty_cache()
     torch.cuda.synchronize()
     return blocks
 
@@ -480,9 +482,15 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="c1", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ndat", type=int, default=0,
+                    help="samples per pol per block (default: the workload's); smaller blocks "
+                         "are for profiling captures only")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
-    cfg = CONFIGS[args.config]
+    cfg = dict(CONFIGS[args.config])
+    if args.ndat:
+        cfg["ndat"] = args.ndat
+        cfg["workload"] += f" [profiling size: {args.ndat} samples/pol per block]"
     world, rank, local = dist_init()
     try:
         if args.impl == "reference":
