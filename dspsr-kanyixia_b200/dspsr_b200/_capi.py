@@ -12,7 +12,8 @@ PKG_ROOT = os.path.dirname(_HERE)
 LIB_PATH = os.path.join(PKG_ROOT, "lib", "libdspsr_b200.so")
 HEADER_PATH = os.path.join(os.path.dirname(PKG_ROOT), "include", "dspsr_b200.h")
 
-OK, EINVAL, ESTATE, ECUDA, ENOMEM, ENODEV = 0, 1, 2, 3, 4, 5
+OK, EINVAL, ESTATE, ECUDA, ENOMEM, ENODEV, ETOOBIG = 0, 1, 2, 3, 4, 5, 6
+NOALLOC_SCRATCH_BYTES = 32 << 20
 INTENSITY, PPQQ, COHERENCE, STOKES = 0, 1, 2, 3
 INT8_TFPD, INT16_TFPD, FLOAT_FPT = 0, 1, 2
 CHIRP_REFERENCE, CHIRP_FP64 = 0, 1
@@ -85,6 +86,9 @@ SIGNATURES = {
                                                         c_int, c_int, c_uint]),
     "dspsr_b200_convolution_get_response": (c_int, [c_vp, c_fp]),
     "dspsr_b200_convolution_status": (c_int, [c_vp]),
+    "dspsr_b200_convolution_perform_noalloc": (c_int, [c_vp, c_vp, c_u64, c_u64, c_uint, c_uint,
+                                                       c_uint, c_uint, c_uint, c_vp, c_vp, c_u64,
+                                                       c_u64p]),
     "dspsr_b200_convolution_set_dedispersion_channels": (c_int, [c_vp, ctypes.POINTER(c_dbl),
                                                                  c_dbl, c_dbl, c_int, c_uint]),
     "dspsr_b200_filterbank": (c_int, [c_vp, c_int, c_vp, c_u64, c_u64, c_uint, c_uint, c_uint,

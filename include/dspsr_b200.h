@@ -31,6 +31,8 @@ extern "C" {
 #define DSPSR_B200_ECUDA     3   /* FailedCall (CUDA runtime) */
 #define DSPSR_B200_ENOMEM    4
 #define DSPSR_B200_ENODEV    5   /* no CUDA device: the library never falls back to the CPU */
+#define DSPSR_B200_ETOOBIG   6   /* the sizes need more than the fixed scratch of
+                                    dspsr_b200_convolution_perform_noalloc */
 
 /* Signal::State values accepted by detection and the fused path
    (Signal/General/Detection.C:225-630) */
@@ -150,6 +152,29 @@ int dspsr_b200_convolution_set_dedispersion_channels (dspsr_b200_convolution* co
                                                       const double* chan_freq_mhz,
                                                       double bandwidth_mhz, double dm,
                                                       int chirp_mode, unsigned norm_nfft);
+/* The same overlap-save convolution without allocating anything.  This entry
+   point has no counterpart in the reference: it exists for callers that
+   cannot call cudaMalloc while they run -- code inside a CUDA stream capture
+   that others replay, real-time processes that fix all memory at start-up,
+   hosts whose device memory is owned by another allocator.  It takes no
+   context or engine object: stream (a cudaStream_t, NULL for the legacy
+   default stream), the complex FPT input (in_span complex samples per
+   (chan, pol)), the response (nchan*nfft complex floats in FFT order, in
+   device memory, normaliser applied), and the output; sizes as for
+   dspsr_b200_convolution_create.  Its tables and FFT scratch live in one
+   static device array of DSPSR_B200_NOALLOC_SCRATCH_BYTES that every GPU
+   loading the library keeps until exit; shapes needing more (roughly
+   nchan*(npol+1)*nfft*8 bytes plus nfft*8 for FFTs above 8192 points) return
+   DSPSR_B200_ETOOBIG.  The array's address is set up on the first call made
+   on each device (make that call before any stream capture).  All calls
+   share the one array: calls whose work overlaps on the GPU race.  Returns
+   the status; *npart as for dspsr_b200_convolution_perform. */
+#define DSPSR_B200_NOALLOC_SCRATCH_BYTES (32ull << 20)
+int dspsr_b200_convolution_perform_noalloc (void* stream, const float* d_in, uint64_t in_span,
+                                            uint64_t ndat, unsigned nchan, unsigned npol,
+                                            unsigned nfft, unsigned nfilt_pos,
+                                            unsigned nfilt_neg, const float* d_response,
+                                            float* d_out, uint64_t out_span, uint64_t* npart);
 /* Blocks until the engine's queued work is done and returns DSPSR_B200_ESTATE
    if one of its device-side waits gave up (each wait is bounded to about a
    second; see the row kernel), DSPSR_B200_OK otherwise. */
