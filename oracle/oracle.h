@@ -138,6 +138,25 @@ void orc_fold_accumulate_f64 (const double* in, uint64_t ndat, uint64_t in_span,
                               int nchan, int npol, int ndim, const uint32_t* binplan,
                               unsigned nbin, double* profiles, uint32_t* hits);
 
+/* ---- SpectralKurtosis, one resolution, noverlap = 1
+        (Signal/General/SpectralKurtosis.C:251-281, 674-798, 1105-1222, 1465-1566) */
+/* complex FPT input; sums[(ipart*nchan + ichan)*npol + ipol][2] = (S1, S2) as
+   float from double accumulation; counts[ipart*nchan + ichan]. Returns npart. */
+uint64_t orc_sk_compute (const float* in, uint64_t ndat, uint64_t in_span, int nchan, int npol,
+                         unsigned M, int zero_is_valid, float* sums, uint32_t* counts);
+/* mask[ipart*nchan + ichan] = 1 where any pol's SK estimator lies outside
+   [lower, upper] (or fewer than 3 samples counted); returns zapped count */
+uint64_t orc_sk_detect (const float* sums, const uint32_t* counts, uint64_t npart, int nchan,
+                        int npol, unsigned Nd, float lower, float upper, uint8_t* mask);
+/* out = in, with every masked M-sample block of every pol set to zero */
+void orc_sk_mask (const float* in, uint64_t in_span, float* out, uint64_t out_span,
+                  const uint8_t* mask, uint64_t npart, int nchan, int npol, unsigned M);
+/* SKLimits::calc_limits (Signal/Statistics/SKLimits.C:136-229): lower and
+   upper SK thresholds for M samples of Nd integrated intensities, std_devs
+   sigma, ntest tests; Romberg-integrated Pearson IV / VI CDFs. 0 on success. */
+int orc_sk_limits (unsigned M, unsigned Nd, float std_devs, unsigned ntest, float* lower,
+                   float* upper);
+
 /* ---- the whole single-channel path, for the timed CPU baseline ----------- */
 /* int8 TFPD (nchan=1, npol=2, ndim=2) -> unpack -> convolve -> Intensity ->
    fold.  Returns the number of output samples folded per pol. */

@@ -53,6 +53,12 @@ _SIGS = {
                                    f32p, u32p]),
     "orc_fold_accumulate_f64": (None, [f64p, c_u64, c_u64, c_int, c_int, c_int, u32p, c_uint,
                                        f64p, u32p]),
+    "orc_sk_compute": (c_u64, [f32p, c_u64, c_u64, c_int, c_int, c_uint, c_int, f32p, u32p]),
+    "orc_sk_detect": (c_u64, [f32p, u32p, c_u64, c_int, c_int, c_uint, ctypes.c_float,
+                              ctypes.c_float, u8p]),
+    "orc_sk_mask": (None, [f32p, c_u64, f32p, c_u64, u8p, c_u64, c_int, c_int, c_uint]),
+    "orc_sk_limits": (c_int, [c_uint, c_uint, ctypes.c_float, c_uint,
+                              ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
     "orc_pipeline_c1": (c_u64, [u8p, c_u64, f32p, f32p, c_uint, c_uint, c_uint, c_dbl, c_dbl,
                                 c_uint, f32p, u32p, c_int]),
     "orc_channel_centre": (c_dbl, [c_dbl, c_dbl, c_uint, c_uint, c_int, c_int]),
@@ -63,6 +69,38 @@ _SIGS = {
     "orc_filterbank_f32": (c_u64, [f32p, c_u64, c_u64, c_int, c_int, c_uint, f32p, c_u64]),
     "orc_filterbank_f64": (c_u64, [f64p, c_u64, c_u64, c_int, c_int, c_uint, f64p, c_u64]),
 }
+
+
+def sk(x, M, lower, upper, Nd=1, zero_is_valid=True, ndat=None):
+    """x: complex64 (nchan, npol, span); the first ndat (default span) samples
+    of each span are used.  Returns sums (npart, nchan, npol, 2), counts
+    (npart, nchan), mask (npart, nchan) uint8 and a copy of x whose first
+    npart*M samples are masked."""
+    nchan, npol, span = x.shape
+    ndat = span if ndat is None else ndat
+    x = np.ascontiguousarray(x, np.complex64)
+    xf = x.view(np.float32).ravel()
+    npart = ndat // M
+    sums = np.zeros((npart, nchan, npol, 2), np.float32)
+    counts = np.zeros((npart, nchan), np.uint32)
+    lib().orc_sk_compute(xf, ndat, span, nchan, npol, M, int(zero_is_valid), sums.ravel(),
+                         counts.ravel())
+    mask = np.zeros((npart, nchan), np.uint8)
+    lib().orc_sk_detect(sums.ravel(), counts.ravel(), npart, nchan, npol, Nd, lower, upper,
+                        mask.ravel())
+    out = x.copy()
+    lib().orc_sk_mask(xf, span, out.view(np.float32).ravel(), span, mask.ravel(), npart, nchan,
+                      npol, M)
+    return sums, counts, mask, out
+
+
+def sk_limits(M, Nd=1, std_devs=3.0, ntest=1):
+    """(lower, upper) float32 thresholds of SKLimits::calc_limits."""
+    lo, hi = ctypes.c_float(), ctypes.c_float()
+    rc = lib().orc_sk_limits(M, Nd, std_devs, ntest, ctypes.byref(lo), ctypes.byref(hi))
+    if rc != 0:
+        raise ValueError(f"sk_limits: invalid M={M} Nd={Nd} std_devs={std_devs} (rc {rc})")
+    return np.float32(lo.value), np.float32(hi.value)
 
 
 def channel_centres(cf, bw, nchan, swap=False, dc_centred=False):

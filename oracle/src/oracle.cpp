@@ -745,6 +745,325 @@ void orc_fold_accumulate_f64 (const double* in, uint64_t ndat, uint64_t in_span,
   fold_accumulate<double> (in, ndat, in_span, nchan, npol, ndim, binplan, nbin, profiles, hits);
 }
 
+// SpectralKurtosis::compute (SpectralKurtosis.C:674-798), FPT, noverlap = 1:
+// square-law detect each sample in float, accumulate S1 and S2 in double,
+// store them as float.
+uint64_t orc_sk_compute (const float* in, uint64_t ndat, uint64_t in_span, int nchan, int npol,
+                         unsigned M, int zero_is_valid, float* sums, uint32_t* counts)
+{
+  const uint64_t npart = ndat / M;   // Resolution::prepare with noverlap = 1
+  // every (part, chan) is independent; threads only split the outer loop
+#pragma omp parallel for schedule(static)
+  for (int64_t ipart = 0; ipart < int64_t (npart); ipart++)
+    for (int ichan = 0; ichan < nchan; ichan++)
+      for (int ipol = 0; ipol < npol; ipol++)
+      {
+        const float* indat = in + 2 * ((uint64_t (ichan) * npol + ipol) * in_span + ipart * M);
+        double S1_sum = 0, S2_sum = 0;
+        unsigned count = 0;
+        for (unsigned i = 0; i < M; i++)
+        {
+          const float re = indat[2 * i];
+          const float im = indat[2 * i + 1];
+          const float sqld = (re * re) + (im * im);
+          if (zero_is_valid || sqld != 0)
+          {
+            S1_sum += sqld;
+            S2_sum += sqld * sqld;
+            count++;
+          }
+        }
+        const uint64_t o = (ipart * nchan + ichan) * npol + ipol;
+        sums[2 * o] = float (S1_sum);
+        sums[2 * o + 1] = float (S2_sum);
+        if (ipol == 0) counts[ipart * nchan + ichan] = count;
+      }
+  return npart;
+}
+
+// SpectralKurtosis::detect_skfb (SpectralKurtosis.C:1105-1222), one resolution
+uint64_t orc_sk_detect (const float* sums, const uint32_t* counts, uint64_t npart, int nchan,
+                        int npol, unsigned Nd, float lower, float upper, uint8_t* mask)
+{
+  uint64_t zapped = 0;
+  for (uint64_t ipart = 0; ipart < npart; ipart++)
+    for (int ichan = 0; ichan < nchan; ichan++)
+    {
+      const unsigned Mprime = counts[ipart * nchan + ichan];
+      uint8_t& out = mask[ipart * nchan + ichan];
+      out = 0;
+      if (Mprime == 0) continue;
+      bool zap = true;
+      if (Mprime > 2)
+      {
+        const float M_fac = (float) (Mprime * Nd + 1) / (Mprime - 1);
+        zap = false;
+        for (int ipol = 0; ipol < npol; ipol++)
+        {
+          const uint64_t o = (ipart * nchan + ichan) * npol + ipol;
+          const float S1_sum = sums[2 * o];
+          const float S2_sum = sums[2 * o + 1];
+          const float V = M_fac * (Mprime * (S2_sum / (S1_sum * S1_sum)) - 1);
+          if (V > upper || V < lower) zap = true;
+        }
+      }
+      if (zap)
+      {
+        out = 1;
+        zapped++;
+      }
+    }
+  return zapped;
+}
+
+// SpectralKurtosis::mask (SpectralKurtosis.C:1465-1566), one resolution
+void orc_sk_mask (const float* in, uint64_t in_span, float* out, uint64_t out_span,
+                  const uint8_t* mask, uint64_t npart, int nchan, int npol, unsigned M)
+{
+#pragma omp parallel for schedule(static)
+  for (int ichan = 0; ichan < nchan; ichan++)
+    for (int ipol = 0; ipol < npol; ipol++)
+    {
+      const float* indat = in + 2 * (uint64_t (ichan) * npol + ipol) * in_span;
+      float* outdat = out + 2 * (uint64_t (ichan) * npol + ipol) * out_span;
+      for (uint64_t ipart = 0; ipart < npart; ipart++)
+      {
+        const bool z = mask[ipart * nchan + ichan] != 0;
+        for (unsigned j = 0; j < 2 * M; j++)
+          outdat[j] = z ? 0.0f : indat[j];
+        indat += 2 * M;
+        outdat += 2 * M;
+      }
+    }
+}
+
+} // extern "C"
+
+namespace {
+
+// Pearson IV / VI densities of the SK estimator (PearsonIV.C:37-134,
+// PearsonVI.C:22-95)
+struct SkDensity
+{
+  bool type6 = false;
+  double m = 0, nu = 0, a = 0, lamda = 0, alpha = 0, beta = 0, delta = 0, logk = 0;
+  double operator() (double x) const
+  {
+    if (type6)
+    {
+      x -= delta;
+      if (x < 0) return 0;
+      return std::exp (logk + (alpha - 1) * std::log (x) - (alpha + beta) * std::log (1 + x));
+    }
+    const double t = (x - lamda) / a;
+    return std::exp (logk - m * std::log (1 + t * t) - nu * std::atan (t));
+  }
+};
+
+// log |Gamma(x+iy)/Gamma(x)|^2 from the product prod_k (1 + y^2/(x+k)^2)^-1:
+// the logs are summed for k < K with x+K >= max(1e5, 1e3 |y|), and the rest
+// by Euler-Maclaurin on f(t) = y^2/(x+t)^2 - y^4/(2(x+t)^4) from D = x+K:
+// y^2/D + f(D)/2 + y^2/(6D^3) - y^4/(6D^3).
+double sk_log_gamma_ratio2 (double x, double y)
+{
+  const double y2 = y * y;
+  const double dmax = std::max (1e5, 1e3 * std::fabs (y));
+  double s = 0, d = x;
+  for (; d < dmax; d += 1) s += std::log1p (y2 / (d * d));
+  const double D = d;
+  s += y2 / D + 0.5 * (y2 / (D * D)) + (y2 - y2 * y2) / (6 * D * D * D);
+  return -s;
+}
+
+// Romberg integration (Romberg.h:63-104): stage j of the extended midpoint
+// (step / 3) or trapezoid (step / 2) rule, polynomial extrapolation of the
+// last five stages to step 0, absolute tolerance 1e-12.
+template <typename F>
+double sk_romberg (const F& f, double a, double b, bool midpoint)
+{
+  const int K = 5, JMAX = 18;
+  const double ratio = midpoint ? 9.0 : 4.0;
+  double h[JMAX + 1], s[JMAX];
+  double stage = 0;
+  h[0] = 1;
+  for (int j = 0; j < JMAX; j++)
+  {
+    if (midpoint)
+    {
+      if (j == 0)
+        stage = (b - a) * f (0.5 * (a + b));
+      else
+      {
+        const double n = std::pow (3.0, j - 1);   // new points: 2 * 3^(j-1)
+        const double del = (b - a) / (3 * n);
+        double x = a + 0.5 * del, sum = 0;
+        for (uint64_t i = 0; i < uint64_t (n); i++)
+        {
+          sum += f (x);
+          x += 2 * del;
+          sum += f (x);
+          x += del;
+        }
+        stage = (stage + (b - a) * sum / n) / 3;
+      }
+    }
+    else
+    {
+      if (j == 0)
+        stage = 0.5 * (b - a) * (f (a) + f (b));
+      else
+      {
+        const double n = std::pow (2.0, j - 1);
+        const double del = (b - a) / n;
+        double x = a + 0.5 * del, sum = 0;
+        for (uint64_t i = 0; i < uint64_t (n); i++, x += del) sum += f (x);
+        stage = 0.5 * (stage + (b - a) * sum / n);
+      }
+    }
+    s[j] = stage;
+    if (j >= K)
+    {
+      // Neville's algorithm at step 0 through (h, s) of stages j-K..j-1
+      double p[K];
+      for (int i = 0; i < K; i++) p[i] = s[j - K + i];
+      double last = 0;
+      for (int m = 1; m < K; m++)
+        for (int i = 0; i < K - m; i++)
+        {
+          const double hi = h[j - K + i], hm = h[j - K + i + m];
+          const double np = (hm * p[i] - hi * p[i + 1]) / (hm - hi);
+          if (i == 0) last = np - p[0];
+          p[i] = np;
+        }
+      if (std::fabs (last) <= double (1.0e-12f)) return p[0];
+    }
+    h[j + 1] = h[j] / ratio;
+  }
+  return s[JMAX - 1];
+}
+
+struct SkCumulative
+{
+  const SkDensity& pdf;
+  // CumulativeDistribution.C:10-24: the tail beyond -1 (or +1) through u = 1/x
+  double cf (double x) const
+  {
+    auto tail = [this] (double u) { return u == 0 ? 0.0 : pdf (-1.0 / u) / (u * u); };
+    if (x < -1) return sk_romberg (tail, 0.0, -1.0 / x, true);
+    return sk_romberg (tail, 0.0, 1.0, true) + sk_romberg (pdf, -1.0, x, false);
+  }
+  double ccf (double x) const
+  {
+    auto tail = [this] (double u) { return u == 0 ? 0.0 : pdf (1.0 / u) / (u * u); };
+    if (x > 1) return sk_romberg (tail, 0.0, 1.0 / x, true);
+    return sk_romberg (tail, 0.0, 1.0, true) + sk_romberg (pdf, x, 1.0, false);
+  }
+};
+
+} // namespace
+
+extern "C" {
+
+// SKLimits::calc_limits (SKLimits.C:136-229) with SKLimits::parametersIV/VI
+// (:71-134), NewtonRaphson.h (100 iterations, 1e-12 relative, clamped to
+// 1 +- 2 sym).  The inverse error function is found by bisection.
+int orc_sk_limits (unsigned M, unsigned Nd, float std_devs, unsigned ntest, float* lower,
+                   float* upper)
+{
+  const double fwer = 1.0 - erf ((float) std_devs / sqrt (2));
+  if (M < 2 || fwer <= 0 || ntest == 0 || Nd == 0) return -1;
+  const double pcer = 1.0 - pow (1 - fwer, 1.0 / ntest);
+  const double target = pcer / 2.0;
+  // ierf(1 - pcer) by bisection on erf
+  double lo_e = 0, hi_e = 10;
+  for (int i = 0; i < 200; i++)
+  {
+    const double mid = 0.5 * (lo_e + hi_e);
+    if (erf (mid) < 1.0 - pcer) lo_e = mid; else hi_e = mid;
+  }
+  const double psd = 0.5 * (lo_e + hi_e) * sqrt (2);
+  if (M >= 32768)
+  {
+    const double factor = sqrt (4.0 / (double) M) * psd;
+    *lower = (float) (1.0f - factor);
+    *upper = (float) (1.0f + factor);
+    return 0;
+  }
+  const double Mx = M, N = Nd;
+  const double b = Mx / (Mx - 1);
+  const double lg = lgamma (Mx * N + 2);
+  const double mu2_6 = 2 * N * (N + 1) * Mx * b * exp (lg - lgamma (Mx * N + 4));
+  const double mu3_6 = 8 * N * (N + 1) * Mx * b * b * exp (lg - lgamma (Mx * N + 6))
+                       * ((N + 4) * Mx * N - 5 * N - 2);
+  const double mu4_6 = 12 * N * (N + 1) * Mx * b * b * b * exp (lg - lgamma (Mx * N + 8))
+      * ((Mx * Mx * Mx + 3 * Mx * Mx) * N * N * N * N
+         + (Mx * Mx * Mx + 68 * Mx * Mx - 93 * Mx) * N * N * N
+         + (125 * Mx * Mx - 245 * Mx + 84) * N * N + (48 - 32 * Mx) * N + 24);
+  double mu2, beta1, beta2;
+  if (Nd == 1)
+  {
+    mu2 = (4 * Mx * Mx) / ((Mx - 1) * (Mx + 2) * (Mx + 3));
+    beta1 = 4 * (Mx + 2) * (Mx + 3) * (5 * Mx - 7) * (5 * Mx - 7)
+            / ((Mx - 1) * (Mx + 4) * (Mx + 4) * (Mx + 5) * (Mx + 5));
+    beta2 = 3 * (Mx + 2) * (Mx + 3) * (Mx * Mx * Mx + 98 * Mx * Mx - 185 * Mx + 78)
+            / ((Mx - 1) * (Mx + 4) * (Mx + 5) * (Mx + 6) * (Mx + 7));
+  }
+  else
+  {
+    mu2 = mu2_6;
+    beta1 = mu3_6 * mu3_6 / (mu2_6 * mu2_6 * mu2_6);
+    beta2 = mu4_6 / (mu2_6 * mu2_6);
+  }
+  const double kappa = beta1 * (beta2 + 3) * (beta2 + 3)
+                       / (4 * (4 * beta2 - 3 * beta1) * (2 * beta2 - 3 * beta1 - 6));
+  if (kappa < 0) return -2;
+  SkDensity pdf;
+  if (kappa > 1)
+  {
+    pdf.type6 = true;
+    const double root = sqrt (16 * pow (mu2_6, 4) + (4 * mu2_6 + 1) * mu3_6 * mu3_6);
+    pdf.alpha = (32 * pow (mu2_6, 5) - 4 * mu3_6 * pow (mu2_6, 3)
+                 + 8 * mu3_6 * mu3_6 * mu2_6 * mu2_6 + mu3_6 * mu3_6 * mu2_6 - pow (mu3_6, 3)
+                 + (8 * pow (mu2_6, 3) - mu3_6 * mu2_6 + mu3_6 * mu3_6) * root)
+                / pow (mu3_6, 3);
+    pdf.beta = 3 + 2 * mu2_6 / (mu3_6 * mu3_6) * (4 * mu2_6 * mu2_6 + root);
+    pdf.delta = (pdf.beta - pdf.alpha - 1) / (pdf.beta - 1);
+    pdf.logk = lgamma (pdf.alpha + pdf.beta) - lgamma (pdf.alpha) - lgamma (pdf.beta);
+  }
+  else
+  {
+    const double r = 6 * (beta2 - beta1 - 1) / (2 * beta2 - 3 * beta1 - 6);
+    pdf.m = (r + 2) / 2;
+    pdf.nu = -r * (r - 2) * sqrt (beta1) / sqrt (16 * (r - 1) - beta1 * (r - 2) * (r - 2));
+    pdf.a = 0.25 * sqrt (mu2 * (16 * (r - 1) - beta1 * (r - 2) * (r - 2)));
+    pdf.lamda = 1 - 0.25 * (r - 2) * sqrt (mu2) * sqrt (beta1);
+    pdf.logk = sk_log_gamma_ratio2 (pdf.m, 0.5 * pdf.nu) - log (pdf.a)
+               - (lgamma (pdf.m - 0.5) + 0.5 * log (M_PI) - lgamma (pdf.m));
+  }
+  const SkCumulative cdf {pdf};
+  const double sym = sqrt (mu2) * psd;
+  const double xmin = 1 - 2 * sym, xmax = 1 + 2 * sym;
+  for (int side = 0; side < 2; side++)
+  {
+    double x = side == 0 ? 1 - sym : 1 + sym;
+    const double guess = x;
+    bool ok = false;
+    for (unsigned it = 0; it < 100 && !ok; it++)
+    {
+      const double c = side == 0 ? cdf.cf (x) : cdf.ccf (x);
+      const double dlog = (side == 0 ? pdf (x) : -pdf (x)) / c;
+      const double dx = (log (c) - log (target)) / dlog;
+      x -= dx;
+      if (x < xmin) x = xmin;
+      if (x > xmax) x = xmax;
+      ok = dx * dx <= (x * 1e-12) * (x * 1e-12);
+    }
+    const double t = ok ? x : guess;
+    if (side == 0) *lower = (float) t; else *upper = (float) t;
+  }
+  return 0;
+}
+
 uint64_t orc_pipeline_c1 (const uint8_t* in, uint64_t ndat, const float* lut,
                           const float* response, unsigned nfft, unsigned nfilt_pos,
                           unsigned nfilt_neg, double phi, double phase_per_sample,
