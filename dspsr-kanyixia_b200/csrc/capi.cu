@@ -685,6 +685,59 @@ int64_t dspsr_b200_fold_plan_count (double phi, double pps, uint64_t ndat)
   return build_fold_plan (phi, pps, ndat, nullptr);
 }
 
+int dspsr_b200_sk_limits (unsigned M, unsigned Nd, float std_devs, unsigned ntest, float* lower,
+                          float* upper)
+{
+  if (!lower || !upper) return DSPSR_B200_EINVAL;
+  const int rc = sk_limits (M, Nd, std_devs, ntest, lower, upper);
+  return rc == 0 ? DSPSR_B200_OK : rc == -2 ? DSPSR_B200_ESTATE : DSPSR_B200_EINVAL;
+}
+
+// ---- spectral kurtosis -------------------------------------------------------
+
+int dspsr_b200_sk (dspsr_b200_context* ctx, const float* d_in, uint64_t in_span, uint64_t ndat,
+                   unsigned nchan, unsigned npol, unsigned M, int zero_is_valid, unsigned Nd,
+                   float lower, float upper, float* d_out, uint64_t out_span, float* d_sums,
+                   uint32_t* d_counts, uint8_t* d_mask, uint64_t* d_zapped, uint64_t* npart_out)
+{
+  if (!ctx) return DSPSR_B200_EINVAL;
+  if (npart_out) *npart_out = 0;
+  if (!d_in || !d_out || nchan == 0 || nchan > 65535 || Nd == 0)
+    return fail (ctx, DSPSR_B200_EINVAL, "sk: invalid argument");
+  if (npol != 1 && npol != 2)
+    return fail (ctx, DSPSR_B200_EINVAL, "sk: npol must be 1 or 2 (got %u)", npol);
+  if (M < 2 || (M & 1) || (in_span & 1) || (out_span & 1))
+    return fail (ctx, DSPSR_B200_EINVAL, "sk: M and the spans must be even (M=%u)", M);
+  if ((reinterpret_cast<uintptr_t> (d_in) | reinterpret_cast<uintptr_t> (d_out)) & 15)
+    return fail (ctx, DSPSR_B200_EINVAL, "sk: buffers must be 16-byte aligned");
+  if (M > (1u << 20) || sk_smem_bytes (npol, M, 1) > SK_SMEM_MAX)
+    return fail (ctx, DSPSR_B200_EINVAL, "sk: npol*M = %u exceeds the shared-memory block",
+                 npol * M);
+  const uint64_t npart = ndat / M;
+  if (in_span < npart * M || out_span < npart * M)
+    return fail (ctx, DSPSR_B200_EINVAL, "sk: span smaller than the blocks");
+  if (npart > 0x7fffffffull) return fail (ctx, DSPSR_B200_EINVAL, "sk: too many blocks");
+  if (d_in != d_out)
+  {
+    // partial overlap of input and output is not supported
+    const char* a = reinterpret_cast<const char*> (d_in);
+    const char* b = reinterpret_cast<const char*> (d_out);
+    const uint64_t na = (uint64_t (nchan) * npol * in_span) * 8;
+    const uint64_t nb = (uint64_t (nchan) * npol * out_span) * 8;
+    if (a < b + nb && b < a + na)
+      return fail (ctx, DSPSR_B200_EINVAL, "sk: input and output overlap without being equal");
+  }
+  if (d_in == d_out && in_span != out_span)
+    return fail (ctx, DSPSR_B200_EINVAL, "sk: in-place masking needs equal spans");
+  B200_CHECK (ctx, launch_sk (reinterpret_cast<const float2*> (d_in), in_span,
+                              reinterpret_cast<float2*> (d_out), out_span, npart, nchan, npol, M,
+                              zero_is_valid, Nd, lower, upper, d_sums, d_counts, d_mask,
+                              reinterpret_cast<unsigned long long*> (d_zapped), ctx->stream),
+              "spectral kurtosis");
+  if (npart_out) *npart_out = npart;
+  return DSPSR_B200_OK;
+}
+
 // ---- unpack ----------------------------------------------------------------
 
 int dspsr_b200_unpack8 (dspsr_b200_context* ctx, const void* d_in, uint64_t ndat,

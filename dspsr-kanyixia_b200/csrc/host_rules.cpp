@@ -9,6 +9,7 @@
 #include "host_rules.h"
 
 #include <cmath>
+#include <complex>
 #include <cstdint>
 #include <vector>
 
@@ -138,6 +139,299 @@ double fold_phi (int64_t start_day, int64_t start_sec, double start_frac,
   const double seconds = double ((day - epoch_day) * 86400 + (sec - epoch_sec))
                          + (frac - epoch_frac);
   return std::fmod (seconds, period) / period - reference_phase;
+}
+
+// ---------------------------------------------------------------------------
+// Spectral-kurtosis thresholds: SKLimits::calc_limits
+// (Signal/Statistics/SKLimits.C:136-229) with the Pearson type IV / VI
+// densities of PearsonIV.C / PearsonVI.C (Nita & Gary 2010a,b; Nagahara
+// 1999).  The cumulative distributions are integrated by adaptive Gauss-Kronrod
+// quadrature (the reference uses Romberg on the midpoint rule) with the same
+// split of the real line: the tails beyond -1 and +1 through t = -1/u and
+// t = 1/u, the middle directly.  The inversion is the reference's
+// Newton-Raphson on log CF / log CCF (NewtonRaphson.h).
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct SKPdf
+{
+  bool vi = false;
+  // Pearson IV
+  double m = 0, nu = 0, a = 0, lamda = 0;
+  // Pearson VI
+  double alpha = 0, beta = 0, delta = 0;
+  double logk = 0;
+  double operator() (double x) const
+  {
+    if (vi)
+    {
+      x -= delta;
+      return x >= 0 ? std::exp (logk + (alpha - 1) * std::log (x) - (alpha + beta) * std::log1p (x))
+                    : 0.0;
+    }
+    const double a1 = (x - lamda) / a;
+    return std::exp (logk - m * std::log1p (a1 * a1) - nu * std::atan (a1));
+  }
+};
+
+// log |Gamma(x+iy) / Gamma(x)|^2 for x > 0 (Nagahara 1999, Eq. 27).  The
+// argument is raised to X = x+n >= 16 by Gamma(z+1) = z Gamma(z), which
+// contributes -sum_k log(1 + y^2/(x+k)^2); at X the Stirling series of
+// log Gamma (Bernoulli terms to w^-9, error below 1e-16 for |w| >= 16) is
+// differenced between w = X+iy and X analytically, so nothing cancels.
+double log_gamma_ratio2 (double x, double y)
+{
+  double acc = 0;
+  while (x < 16)
+  {
+    const double t = y / x;
+    acc -= std::log1p (t * t);
+    x += 1;
+  }
+  // Re[(w - 1/2) log w - w] - [(X - 1/2) log X - X]
+  const double lead = (x - 0.5) * 0.5 * std::log1p ((y / x) * (y / x)) - y * std::atan2 (y, x);
+  // Re S(w) - S(X) with S(w) = 1/(12w) - 1/(360w^3) + 1/(1260w^5) - 1/(1680w^7) + 1/(1188w^9)
+  static const double coef[5] = {1.0 / 12, -1.0 / 360, 1.0 / 1260, -1.0 / 1680, 1.0 / 1188};
+  const std::complex<double> w (x, y), w2inv = 1.0 / (w * w);
+  std::complex<double> pw = 1.0 / w;
+  double px = 1.0 / x, sw = 0, sx = 0;
+  for (int k = 0; k < 5; k++)
+  {
+    sw += coef[k] * pw.real ();
+    sx += coef[k] * px;
+    pw *= w2inv;
+    px /= x * x;
+  }
+  return acc + 2 * (lead + sw - sx);
+}
+
+// 7-point Gauss / 15-point Kronrod pair on [a, b] (abscissae and weights of
+// Kronrod 1965 as tabulated in QUADPACK); returns the Kronrod estimate and
+// |Kronrod - Gauss| as its error.
+template <typename F>
+double gauss_kronrod15 (const F& f, double a, double b, double* err)
+{
+  static const double xk[8] = {0.991455371120812639206854697526329, 0.949107912342758524526189684047851,
+                               0.864864423359769072789712788640926, 0.741531185599394439863864773280788,
+                               0.586087235467691130294144845693013, 0.405845151377397166906606412076961,
+                               0.207784955007898467600689403773245, 0.0};
+  static const double wk[8] = {0.022935322010529224963732008058970, 0.063092092629978553290700663189204,
+                               0.104790010322250183839876322541518, 0.140653259715525918745189590510238,
+                               0.169004726639267902826583426598550, 0.190350578064785409913256402421014,
+                               0.204432940075298892414161999234649, 0.209482141084727828012999174891714};
+  static const double wg[4] = {0.129484966168869693270611432679082, 0.279705391489276667901467771423780,
+                               0.381830050505118944950369775488975, 0.417959183673469387755102040816327};
+  const double c = 0.5 * (a + b), h = 0.5 * (b - a);
+  const double fc = f (c);
+  double rk = wk[7] * fc, rg = wg[3] * fc;
+  for (int i = 0; i < 7; i++)
+  {
+    const double s = f (c - h * xk[i]) + f (c + h * xk[i]);
+    rk += wk[i] * s;
+    if (i & 1) rg += wg[i / 2] * s;
+  }
+  *err = std::fabs ((rk - rg) * h);
+  return rk * h;
+}
+
+// Globally adaptive quadrature: bisect the sub-interval with the largest
+// error estimate until the summed error is below 1e-13 of the integral (or
+// 4000 sub-intervals); an optional break point (a kink of the density) is
+// made an interval end from the start.
+template <typename F>
+double integrate (const F& f, double a, double b, double kink = NAN)
+{
+  if (a == b) return 0;
+  struct Piece { double a, b, v, e; };
+  std::vector<Piece> pieces;
+  auto add = [&] (double lo, double hi) {
+    Piece q {lo, hi, 0, 0};
+    q.v = gauss_kronrod15 (f, lo, hi, &q.e);
+    pieces.push_back (q);
+  };
+  if (kink > std::fmin (a, b) && kink < std::fmax (a, b))
+  {
+    add (a, kink);
+    add (kink, b);
+  }
+  else
+    add (a, b);
+  for (int iter = 0; iter < 4000; iter++)
+  {
+    double total = 0, error = 0;
+    size_t worst = 0;
+    for (size_t i = 0; i < pieces.size (); i++)
+    {
+      total += pieces[i].v;
+      error += pieces[i].e;
+      if (pieces[i].e > pieces[worst].e) worst = i;
+    }
+    if (error <= 1e-13 * std::fabs (total) || error < 1e-300) return total;
+    const Piece w = pieces[worst];
+    const double m = 0.5 * (w.a + w.b);
+    if (!(m > std::fmin (w.a, w.b) && m < std::fmax (w.a, w.b))) return total;
+    pieces[worst] = pieces.back ();
+    pieces.pop_back ();
+    add (w.a, m);
+    add (m, w.b);
+  }
+  double total = 0;
+  for (const Piece& q : pieces) total += q.v;
+  return total;
+}
+
+struct SKCdf
+{
+  const SKPdf& p;
+  // tail integrands through t = -1/u and t = 1/u; zero at u = 0
+  double left_tail (double u) const { return u > 0 ? p (-1.0 / u) / (u * u) : 0.0; }
+  double right_tail (double u) const { return u > 0 ? p (1.0 / u) / (u * u) : 0.0; }
+  // the Pearson VI density starts at x = delta
+  double kink_x () const { return p.vi ? p.delta : NAN; }
+  double kink_u (double sign) const
+  {
+    return p.vi && sign * p.delta > 1 ? sign / p.delta : NAN;
+  }
+  double cf (double x) const
+  {
+    auto lt = [this] (double u) { return left_tail (u); };
+    if (x < -1) return integrate (lt, 0.0, -1.0 / x, kink_u (-1));
+    return integrate (lt, 0.0, 1.0, kink_u (-1)) + integrate (p, -1.0, x, kink_x ());
+  }
+  double ccf (double x) const
+  {
+    auto rt = [this] (double u) { return right_tail (u); };
+    if (x > 1) return integrate (rt, 0.0, 1.0 / x, kink_u (1));
+    return integrate (rt, 0.0, 1.0, kink_u (1)) + integrate (p, x, 1.0, kink_x ());
+  }
+};
+
+// NewtonRaphson.h: x -= (f(x)-y)/f'(x), clamped to [lo, hi], until dx^2 <= (x 1e-12)^2
+template <typename F, typename D>
+bool newton (const F& f, const D& df, double y, double& x, double lo, double hi)
+{
+  for (unsigned i = 0; i < 100; i++)
+  {
+    const double dx = (f (x) - y) / df (x);
+    x -= dx;
+    if (lo != hi)
+    {
+      if (x < lo) x = lo;
+      if (x > hi) x = hi;
+    }
+    if (dx * dx <= (x * 1e-12) * (x * 1e-12)) return true;
+  }
+  return false;
+}
+
+// inverse error function by Newton iteration on erf (to double precision)
+double inverse_erf (double y)
+{
+  if (!(y > -1 && y < 1)) return y > 0 ? INFINITY : -INFINITY;
+  double x = 0;
+  for (int i = 0; i < 100; i++)
+  {
+    const double dx = (std::erf (x) - y) / (2.0 / std::sqrt (M_PI) * std::exp (-x * x));
+    x -= dx;
+    if (std::fabs (dx) <= 1e-16 * std::fabs (x)) break;
+  }
+  return x;
+}
+
+} // namespace
+
+int sk_limits (unsigned M, unsigned Nd, float std_devs, unsigned ntest, float* lower, float* upper)
+{
+  const double fwer = 1.0 - std::erf (double (std_devs) / std::sqrt (2.0));
+  if (M < 2 || !(fwer > 0) || Nd == 0 || ntest == 0) return -1;
+  const double pcer = 1.0 - std::pow (1 - fwer, 1.0 / ntest);
+  const double target = pcer / 2.0;
+  const double psd = inverse_erf (1.0 - pcer) * std::sqrt (2.0);
+  if (M >= 32768)
+  {
+    const double factor = std::sqrt (4.0 / double (M)) * psd;
+    *lower = float (1.0f - factor);
+    *upper = float (1.0f + factor);
+    return 0;
+  }
+  const double Md = M, N = Nd;
+  // SKLimits::parametersIV / parametersVI
+  double mu2, beta1, beta2;
+  double vmu2 = 0, vmu3 = 0, vmu4 = 0;
+  {
+    const double b = Md / (Md - 1);
+    const double lg = std::lgamma (Md * N + 2);
+    vmu2 = 2 * N * (N + 1) * Md * b * std::exp (lg - std::lgamma (Md * N + 4));
+    vmu3 = 8 * N * (N + 1) * Md * b * b * std::exp (lg - std::lgamma (Md * N + 6))
+           * ((N + 4) * Md * N - 5 * N - 2);
+    vmu4 = 12 * N * (N + 1) * Md * b * b * b * std::exp (lg - std::lgamma (Md * N + 8))
+           * ((Md * Md * Md + 3 * Md * Md) * std::pow (N, 4)
+              + (Md * Md * Md + 68 * Md * Md - 93 * Md) * std::pow (N, 3)
+              + (125 * Md * Md - 245 * Md + 84) * N * N + (48 - 32 * Md) * N + 24);
+  }
+  if (Nd == 1)
+  {
+    mu2 = (4 * Md * Md) / ((Md - 1) * (Md + 2) * (Md + 3));
+    beta1 = (4 * (Md + 2) * (Md + 3) * (5 * Md - 7) * (5 * Md - 7))
+            / ((Md - 1) * (Md + 4) * (Md + 4) * (Md + 5) * (Md + 5));
+    beta2 = 3 * (Md + 2) * (Md + 3) * (Md * Md * Md + 98 * Md * Md - 185 * Md + 78)
+            / ((Md - 1) * (Md + 4) * (Md + 5) * (Md + 6) * (Md + 7));
+  }
+  else
+  {
+    mu2 = vmu2;
+    beta1 = vmu3 * vmu3 / (vmu2 * vmu2 * vmu2);
+    beta2 = vmu4 / (vmu2 * vmu2);
+  }
+  const double kappa = beta1 * (beta2 + 3) * (beta2 + 3)
+                       / (4 * (4 * beta2 - 3 * beta1) * (2 * beta2 - 3 * beta1 - 6));
+  if (kappa < 0) return -2;   // Pearson type I: not implemented in the reference either
+  SKPdf pdf;
+  if (kappa > 1)
+  {
+    // PearsonVI::prepare with Equation (14) of Nita & Gary (2010b)
+    pdf.vi = true;
+    const double sq = std::sqrt (16 * std::pow (vmu2, 4) + (4 * vmu2 + 1) * vmu3 * vmu3);
+    pdf.alpha = std::pow (vmu3, -3)
+                * (32 * std::pow (vmu2, 5) - 4 * vmu3 * std::pow (vmu2, 3)
+                   + 8 * vmu3 * vmu3 * vmu2 * vmu2 + vmu3 * vmu3 * vmu2 - std::pow (vmu3, 3)
+                   + (8 * std::pow (vmu2, 3) - vmu3 * vmu2 + vmu3 * vmu3) * sq);
+    pdf.beta = 3 + 2 * vmu2 * std::pow (vmu3, -2) * (4 * vmu2 * vmu2 + sq);
+    pdf.delta = (pdf.beta - pdf.alpha - 1) / (pdf.beta - 1);
+    pdf.logk = std::lgamma (pdf.alpha + pdf.beta) - std::lgamma (pdf.alpha) - std::lgamma (pdf.beta);
+  }
+  else
+  {
+    // PearsonIV::prepare, Equation (57) of Nita & Gary (2010a)
+    const double r = (6 * (beta2 - beta1 - 1)) / (2 * beta2 - 3 * beta1 - 6);
+    pdf.m = (r + 2) / 2;
+    pdf.nu = -(r * (r - 2) * std::sqrt (beta1)) / std::sqrt (16 * (r - 1) - beta1 * (r - 2) * (r - 2));
+    pdf.a = 0.25 * std::sqrt (mu2 * ((16 * (r - 1)) - (beta1 * (r - 2) * (r - 2))));
+    pdf.lamda = 1.0 - 0.25 * (r - 2) * std::sqrt (mu2) * std::sqrt (beta1);
+    const double log_beta = std::lgamma (pdf.m - 0.5) + 0.5 * std::log (M_PI) - std::lgamma (pdf.m);
+    pdf.logk = log_gamma_ratio2 (pdf.m, 0.5 * pdf.nu) - std::log (pdf.a) - log_beta;
+  }
+  SKCdf cdf {pdf};
+  const double sym = std::sqrt (mu2) * psd;
+  const double lo = 1 - 2 * sym, hi = 1 + 2 * sym;
+  double xl = 1 - sym;
+  {
+    double x = xl;
+    auto f = [&] (double v) { return std::log (cdf.cf (v)); };
+    auto df = [&] (double v) { return pdf (v) / cdf.cf (v); };
+    if (newton (f, df, std::log (target), x, lo, hi)) xl = x;
+  }
+  double xu = 1 + sym;
+  {
+    double x = xu;
+    auto f = [&] (double v) { return std::log (cdf.ccf (v)); };
+    auto df = [&] (double v) { return -pdf (v) / cdf.ccf (v); };
+    if (newton (f, df, std::log (target), x, lo, hi)) xu = x;
+  }
+  *lower = float (xl);
+  *upper = float (xu);
+  return 0;
 }
 
 // ---------------------------------------------------------------------------

@@ -27,6 +27,11 @@ void bittable8 (double spacing, bool twos_complement, float* lut, double* scale)
 double fold_phi (int64_t start_day, int64_t start_sec, double start_frac,
                  int64_t epoch_day, int64_t epoch_sec, double epoch_frac,
                  uint64_t idat_start, double rate, double period, double reference_phase);
+// SKLimits::calc_limits: lower/upper thresholds of the SK estimator for M
+// samples (Nd integrated), std_devs sigma, ntest tests.  0 on success, -1 for
+// invalid arguments, -2 where a Pearson type I density would be needed.
+int sk_limits (unsigned M, unsigned Nd, float std_devs, unsigned ntest, float* lower,
+               float* upper);
 // Returns the number of segments; fills *out when non-null.
 int64_t build_fold_plan (double phi, double phase_per_sample, uint64_t ndat,
                          std::vector<FoldSegment>* out);

@@ -698,6 +698,180 @@ k_filterbank (const InputView in, const float* __restrict__ lut, const uint64_t 
                                                          __fmul_rn (scale, v[k].y));
 }
 
+// SpectralKurtosis::transformation for one resolution with noverlap = 1:
+// compute (SpectralKurtosis.C:674-798), detect_skfb (:1105-1222) and mask
+// (:1465-1566).  A CTA takes up to U consecutive M-sample blocks of one
+// channel:
+//
+//   1. all threads stream the blocks in (16-byte loads, both pols in flight
+//      together), square-law detect them in float as the reference does and
+//      keep sqld per (block, pol) in shared memory; out of place the voltages
+//      are written through to the output at the same time;
+//   2. warp 0 forms the reference's two sequential double sums per (block,
+//      pol) -- S1 of sqld, S2 of sqld*sqld -- one lane per sum, 4U lanes in
+//      all, so that each conversion to double serves 4U values.  The
+//      additions run in the reference's order: the sums (and hence the mask)
+//      equal the CPU's bit for bit.  Many CTAs per SM keep the loads of some
+//      in flight while others add;
+//   3. the SK estimator of each block is tested and zapped blocks of the
+//      output are overwritten with zeros (in place, only they are written).
+//
+// Uncounted samples (sqld == 0 with zero_is_valid unset) add +0.0, which
+// leaves a sum of non-negative terms unchanged exactly; they are counted by a
+// shared atomic as they are met.  Shared memory holds U * npol columns of
+// Ms floats, Ms = M rounded up to a multiple of 4 plus 4 (so that the
+// columns read together fall on different banks).
+constexpr int SK_THREADS = 128;
+
+__host__ __device__ inline unsigned sk_column (unsigned M) { return ((M + 3) & ~3u) + 4; }
+
+template <int U>
+__global__ void __launch_bounds__ (SK_THREADS, 12)
+k_sk (const float2* __restrict__ in, const uint64_t in_span, float2* out, const uint64_t out_span,
+      const uint64_t npart, const unsigned nchan, const unsigned npol, const unsigned M,
+      const int zero_is_valid, const unsigned Nd, const float lower,
+      const float upper, float* __restrict__ sums, unsigned* __restrict__ counts,
+      uint8_t* __restrict__ mask, unsigned long long* __restrict__ nzap)
+{
+  extern __shared__ __align__ (16) float s_sqld[];   // [unit][pol][Ms]
+  __shared__ double s_sum[U][2][2];
+  __shared__ unsigned s_zero[U];
+  __shared__ int s_zap[U];
+  const uint64_t part0 = uint64_t (blockIdx.x) * U;
+  const unsigned c = blockIdx.y;
+  const unsigned nu = unsigned (min (uint64_t (U), npart - part0));
+  const unsigned Ms = sk_column (M);
+  const unsigned n4 = M / 2;                      // float4 (two samples) per (block, pol)
+  const bool through = !(out == in && out_span == in_span);
+  const bool two = npol == 2;
+  if (threadIdx.x < U) s_zero[threadIdx.x] = 0;
+  // both pols of the CTA's blocks are contiguous runs of nu*M samples
+  const float4* src0 = reinterpret_cast<const float4*> (in + uint64_t (c) * npol * in_span
+                                                        + part0 * M);
+  const float4* src1 = src0 + (two ? in_span / 2 : 0);
+  float4* dst0 = reinterpret_cast<float4*> (out + uint64_t (c) * npol * out_span + part0 * M);
+  float4* dst1 = dst0 + (two ? out_span / 2 : 0);
+  __syncthreads ();
+  const unsigned total = nu * n4;
+#pragma unroll 4
+  for (unsigned f = threadIdx.x; f < total; f += SK_THREADS)
+  {
+    const unsigned u = f / n4, i = f - u * n4;
+    const float4 a = __ldcs (src0 + f);
+    float4 b = a;
+    if (two) b = __ldcs (src1 + f);
+    if (through)
+    {
+      __stcs (dst0 + f, a);
+      if (two) __stcs (dst1 + f, b);
+    }
+    const float a0 = __fadd_rn (__fmul_rn (a.x, a.x), __fmul_rn (a.y, a.y));
+    const float a1 = __fadd_rn (__fmul_rn (a.z, a.z), __fmul_rn (a.w, a.w));
+    float2* q0 = reinterpret_cast<float2*> (s_sqld + (u * npol) * Ms);
+    q0[i] = make_float2 (a0, a1);
+    // Mprime counts pol 0, as detect_skfb reads it
+    if (!zero_is_valid && (a0 == 0.0f || a1 == 0.0f))
+      atomicAdd (&s_zero[u], unsigned (a0 == 0.0f) + unsigned (a1 == 0.0f));
+    if (two)
+    {
+      float2* q1 = reinterpret_cast<float2*> (s_sqld + (u * npol + 1) * Ms);
+      q1[i] = make_float2 (__fadd_rn (__fmul_rn (b.x, b.x), __fmul_rn (b.y, b.y)),
+                           __fadd_rn (__fmul_rn (b.z, b.z), __fmul_rn (b.w, b.w)));
+    }
+  }
+  __syncthreads ();
+  if (threadIdx.x < 4 * U)
+  {
+    // lane = unit*4 + pol*2 + (S2 ? 1 : 0)
+    const unsigned u = threadIdx.x >> 2, p = (threadIdx.x >> 1) & 1;
+    const bool sq = threadIdx.x & 1;
+    const bool live = u < nu && p < npol;
+    const float* xf = s_sqld + (live ? u * npol + p : 0) * Ms;
+    const float4* x = reinterpret_cast<const float4*> (xf);
+    const unsigned nq = M / 4;
+    double acc = 0.0;
+    unsigned i = 0;
+    if (nq >= 4)
+    {
+      float4 q[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) q[k] = x[k];
+      for (i = 4; i + 4 <= nq; i += 4)
+      {
+        double t[16];
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+        {
+          t[4 * k] = double (sq ? __fmul_rn (q[k].x, q[k].x) : q[k].x);
+          t[4 * k + 1] = double (sq ? __fmul_rn (q[k].y, q[k].y) : q[k].y);
+          t[4 * k + 2] = double (sq ? __fmul_rn (q[k].z, q[k].z) : q[k].z);
+          t[4 * k + 3] = double (sq ? __fmul_rn (q[k].w, q[k].w) : q[k].w);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) q[k] = x[i + k];
+#pragma unroll
+        for (int k = 0; k < 16; k++) acc = __dadd_rn (acc, t[k]);
+      }
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+      {
+        acc = __dadd_rn (acc, double (sq ? __fmul_rn (q[k].x, q[k].x) : q[k].x));
+        acc = __dadd_rn (acc, double (sq ? __fmul_rn (q[k].y, q[k].y) : q[k].y));
+        acc = __dadd_rn (acc, double (sq ? __fmul_rn (q[k].z, q[k].z) : q[k].z));
+        acc = __dadd_rn (acc, double (sq ? __fmul_rn (q[k].w, q[k].w) : q[k].w));
+      }
+    }
+    for (unsigned jj = 4 * i; jj < M; jj++)
+      acc = __dadd_rn (acc, double (sq ? __fmul_rn (xf[jj], xf[jj]) : xf[jj]));
+    if (live) s_sum[u][p][sq] = acc;
+  }
+  __syncthreads ();
+  if (threadIdx.x < nu)
+  {
+    const unsigned u = threadIdx.x;
+    const uint64_t unit = (part0 + u) * nchan + c;
+    const unsigned Mprime = M - s_zero[u];
+    bool zap = false;
+    if (Mprime > 0)
+    {
+      zap = true;
+      if (Mprime > 2)
+      {
+        // Equation (8) of Nita & Gary (2010b), as detect_skfb evaluates it in float
+        const float M_fac = __fdiv_rn (float (Mprime * Nd + 1), float (Mprime - 1));
+        zap = false;
+        for (unsigned p = 0; p < npol; p++)
+        {
+          const float S1 = __double2float_rn (s_sum[u][p][0]);
+          const float S2 = __double2float_rn (s_sum[u][p][1]);
+          const float r = __fdiv_rn (S2, __fmul_rn (S1, S1));
+          const float V = __fmul_rn (M_fac, __fsub_rn (__fmul_rn (float (Mprime), r), 1.0f));
+          if (V > upper || V < lower) zap = true;
+        }
+      }
+    }
+    if (sums)
+      for (unsigned p = 0; p < npol; p++)
+      {
+        sums[2 * (unit * npol + p)] = __double2float_rn (s_sum[u][p][0]);
+        sums[2 * (unit * npol + p) + 1] = __double2float_rn (s_sum[u][p][1]);
+      }
+    if (counts) counts[unit] = Mprime;
+    if (mask) mask[unit] = zap ? 1 : 0;
+    if (zap && nzap) atomicAdd (nzap, 1ull);
+    s_zap[u] = zap;
+  }
+  __syncthreads ();
+  // zero the zapped blocks; each thread overwrites exactly the float4s it wrote through
+  const float4 zero = make_float4 (0.f, 0.f, 0.f, 0.f);
+  for (unsigned f = threadIdx.x; f < total; f += SK_THREADS)
+    if (s_zap[f / n4])
+    {
+      __stcs (dst0 + f, zero);
+      if (two) __stcs (dst1 + f, zero);
+    }
+}
+
 __global__ void k_unpack8 (const uint8_t* __restrict__ in, const uint64_t ndat,
                            const unsigned nchan, const unsigned npol, const unsigned ndim,
                            const float* __restrict__ lut, float* __restrict__ out,
@@ -1033,6 +1207,34 @@ cudaError_t launch_filterbank (const InputView& in, const float* d_lut, unsigned
     case 64: return run_filterbank<64> (in, d_lut, nblk, scale, out, out_span, st, clk);
     default: return cudaErrorInvalidValue;
   }
+}
+
+size_t sk_smem_bytes (unsigned npol, unsigned M, unsigned units)
+{
+  return size_t (units) * npol * sk_column (M) * sizeof (float);
+}
+
+cudaError_t launch_sk (const float2* in, uint64_t in_span, float2* out, uint64_t out_span,
+                       uint64_t npart, unsigned nchan, unsigned npol, unsigned M,
+                       int zero_is_valid, unsigned Nd, float lower, float upper, float* sums,
+                       unsigned* counts, uint8_t* mask, unsigned long long* nzap, cudaStream_t st)
+{
+  if (npart == 0) return cudaSuccess;
+  // two blocks per CTA while they fit in a modest footprint, else one
+  const unsigned units = sk_smem_bytes (npol, M, 2) <= (48u << 10) ? 2 : 1;
+  const size_t smem = sk_smem_bytes (npol, M, units);
+  if (smem > SK_SMEM_MAX) return cudaErrorInvalidValue;
+  const uint64_t nblk = (npart + units - 1) / units;
+  if (nblk > 0x7fffffffull || nchan > 65535) return cudaErrorInvalidValue;
+  auto kern = units == 2 ? k_sk<2> : k_sk<1>;
+  cudaError_t e = cudaFuncSetAttribute (kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        int (smem));
+  if (e != cudaSuccess) return e;
+  g_launches++;
+  kern<<<dim3 (unsigned (nblk), nchan), SK_THREADS, smem, st>>> (
+      in, in_span, out, out_span, npart, nchan, npol, M, zero_is_valid, Nd, lower, upper, sums,
+      counts, mask, nzap);
+  return cudaGetLastError ();
 }
 
 cudaError_t launch_unpack8 (const uint8_t* in, uint64_t ndat, unsigned nchan, unsigned npol,

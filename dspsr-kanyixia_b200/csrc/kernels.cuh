@@ -115,6 +115,19 @@ cudaError_t launch_filterbank (const InputView& in, const float* d_lut, unsigned
                                uint64_t nblk, float scale, float2* out, uint64_t out_span,
                                cudaStream_t stream, const KernelClock* clock = nullptr);
 
+// SpectralKurtosis (one resolution, noverlap 1): statistics, test and masked
+// copy (out may equal in: then only zapped blocks are written).  sums
+// [npart][nchan][npol][2], counts and mask [npart][nchan] are optional.
+// in/out spans are complex samples; M and the spans must be even, npol 1 or 2,
+// and sk_smem_bytes(npol, M, 1) at most SK_SMEM_MAX.
+constexpr size_t SK_SMEM_MAX = 224u << 10;
+size_t sk_smem_bytes (unsigned npol, unsigned M, unsigned units);
+cudaError_t launch_sk (const float2* in, uint64_t in_span, float2* out, uint64_t out_span,
+                       uint64_t npart, unsigned nchan, unsigned npol, unsigned M,
+                       int zero_is_valid, unsigned Nd, float lower, float upper, float* sums,
+                       unsigned* counts, uint8_t* mask, unsigned long long* nzap,
+                       cudaStream_t stream);
+
 cudaError_t launch_unpack8 (const uint8_t* in, uint64_t ndat, unsigned nchan, unsigned npol,
                             unsigned ndim, const float* d_lut, float* out, uint64_t span,
                             cudaStream_t stream);

@@ -22,6 +22,7 @@ from ._capi import (B200Error, PipelineConfig, INTENSITY, PPQQ, COHERENCE, STOKE
 
 __all__ = ["Context", "Convolution", "Fold", "Pipeline", "PipelineConfig", "B200Error",
            "smearing_samples", "minimum_ndat", "optimal_fft_length", "bittable8", "fold_phi",
+           "sk_limits",
            "fold_plan_count", "INTENSITY", "PPQQ", "COHERENCE", "STOKES", "INT8_TFPD",
            "INT16_TFPD", "FLOAT_FPT", "CHIRP_REFERENCE", "CHIRP_FP64", "NOUT"]
 
@@ -65,6 +66,16 @@ def bittable8(spacing=JA98_SPACING_8BIT, twos_complement=True):
     if rc:
         raise B200Error(rc, "bittable8: invalid spacing")
     return lut, scale.value
+
+
+def sk_limits(M, Nd=1, std_devs=3.0, ntest=1):
+    """SKLimits::calc_limits -> (lower, upper) float32 thresholds."""
+    lo = np.zeros(1, np.float32)
+    hi = np.zeros(1, np.float32)
+    rc = _capi.lib().dspsr_b200_sk_limits(M, Nd, std_devs, ntest, _fptr(lo), _fptr(hi))
+    if rc != _capi.OK:
+        raise B200Error(rc, f"sk_limits: no thresholds for M={M} Nd={Nd} std_devs={std_devs}")
+    return lo[0], hi[0]
 
 
 def fold_phi(start_mjd, epoch_mjd, idat_start, rate, period, reference_phase=0.0):
@@ -144,6 +155,17 @@ class Context:
     def detect(self, d_in, in_span, ndat, nchan, state, d_out, out_span):
         self.check(self._lib.dspsr_b200_detect(self.handle, _ptr(d_in), in_span, ndat, nchan,
                                                state, _ptr(d_out), out_span), "detect")
+
+    # ---- SpectralKurtosis engine (one resolution, noverlap 1) -----------------------
+    def sk(self, d_in, in_span, ndat, nchan, npol, M, lower, upper, d_out, out_span,
+           d_sums=None, d_counts=None, d_mask=None, d_zapped=None, Nd=1, zero_is_valid=True):
+        """compute + detect_ft + mask in one pass; returns npart = ndat // M."""
+        n = ctypes.c_uint64()
+        self.check(self._lib.dspsr_b200_sk(self.handle, _ptr(d_in), in_span, ndat, nchan, npol, M,
+                                           int(zero_is_valid), Nd, lower, upper, _ptr(d_out),
+                                           out_span, _ptr(d_sums), _ptr(d_counts), _ptr(d_mask),
+                                           _ptr(d_zapped), ctypes.byref(n)), "sk")
+        return n.value
 
 
 class Convolution:

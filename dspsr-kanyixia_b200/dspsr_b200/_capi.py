@@ -75,6 +75,7 @@ SIGNATURES = {
     "dspsr_b200_fold_phi": (c_dbl, [c_i64, c_i64, c_dbl, c_i64, c_i64, c_dbl, c_u64, c_dbl,
                                     c_dbl, c_dbl]),
     "dspsr_b200_fold_plan_count": (c_i64, [c_dbl, c_dbl, c_u64]),
+    "dspsr_b200_sk_limits": (c_int, [c_uint, c_uint, ctypes.c_float, c_uint, c_fp, c_fp]),
     "dspsr_b200_unpack8": (c_int, [c_vp, c_vp, c_u64, c_uint, c_uint, c_uint, c_fp, c_vp, c_u64]),
     "dspsr_b200_unpack16": (c_int, [c_vp, c_vp, c_u64, c_uint, c_uint, c_uint, c_int, c_vp,
                                     c_u64]),
@@ -95,6 +96,9 @@ SIGNATURES = {
                                       c_fp, c_int, c_vp, c_u64, c_u64p]),
     "dspsr_b200_convolution_perform": (c_int, [c_vp, c_vp, c_u64, c_u64, c_vp, c_u64, c_u64p]),
     "dspsr_b200_detect": (c_int, [c_vp, c_vp, c_u64, c_u64, c_uint, c_int, c_vp, c_u64]),
+    "dspsr_b200_sk": (c_int, [c_vp, c_vp, c_u64, c_u64, c_uint, c_uint, c_uint, c_int, c_uint,
+                              ctypes.c_float, ctypes.c_float, c_vp, c_u64, c_vp, c_vp, c_vp, c_vp,
+                              c_u64p]),
     "dspsr_b200_fold_create": (c_int, [c_vp, c_uint, c_uint, c_uint, ctypes.POINTER(c_vp)]),
     "dspsr_b200_fold_destroy": (c_int, [c_vp]),
     "dspsr_b200_fold_set_bins": (c_int, [c_vp, c_dbl, c_dbl, c_u64, c_u64, c_u64p]),

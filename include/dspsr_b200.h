@@ -97,6 +97,15 @@ double dspsr_b200_fold_phi (int64_t start_day, int64_t start_sec, double start_f
                             int64_t epoch_day, int64_t epoch_sec, double epoch_frac,
                             uint64_t idat_start, double rate, double period,
                             double reference_phase);
+/* SKLimits::calc_limits (Signal/Statistics/SKLimits.C:136-229) as
+   SpectralKurtosis::get_limits calls it (SpectralKurtosis.C:989-1007): the
+   float thresholds of the SK estimator for M intensities of Nd integrated
+   samples, std_devs sigma, ntest tests (the number of polarisations).
+   DSPSR_B200_EINVAL for M < 2, Nd = 0, ntest = 0 or std_devs giving no error
+   rate; DSPSR_B200_ESTATE where the moments call for a Pearson type I density
+   (which the reference does not implement either). */
+int dspsr_b200_sk_limits (unsigned M, unsigned Nd, float std_devs, unsigned ntest,
+                          float* lower, float* upper);
 /* Number of arithmetic segments the exact fold-bin plan needs for a block
    (see dspsr_b200_fold_set_bins); lets a caller size buffers. */
 int64_t dspsr_b200_fold_plan_count (double phi, double phase_per_sample,
@@ -215,6 +224,32 @@ int dspsr_b200_filterbank (dspsr_b200_context* ctx, int input_kind, const void* 
 int dspsr_b200_detect (dspsr_b200_context* ctx, const float* d_in, uint64_t in_span,
                        uint64_t ndat, unsigned nchan, int state, float* d_out,
                        uint64_t out_span);
+
+/* ---------------------------------------------------------------------- */
+/* SpectralKurtosis::Engine compute / detect_ft / mask for one resolution  */
+/* with noverlap 1 (CUDA::SpectralKurtosisEngine,                           */
+/* Signal/General/SpectralKurtosisCUDA.cu:45-99; host loop                  */
+/* SpectralKurtosis.C:542-671, 674-798, 1105-1222, 1465-1566)               */
+/* ---------------------------------------------------------------------- */
+
+/* Complex FPT input (span in complex samples), npart = ndat / M blocks of M
+   samples per channel.  Per (block, channel): S1 and S2 of every pol summed
+   as the reference does, the SK estimator of each pol tested against
+   [lower, upper] (a block with 1 or 2 counted samples is zapped, one with
+   none is not), and the block of every pol copied to d_out with zapped
+   blocks set to zero.  d_out may equal d_in (same span): only zapped blocks
+   are then written.  Optional device outputs (null to skip):
+   d_sums[(ipart*nchan + ichan)*npol + ipol][2] = (S1, S2) as float,
+   d_counts[ipart*nchan + ichan] = samples counted (zero_is_valid = 0 skips
+   zero samples), d_mask[ipart*nchan + ichan] = 1 where zapped, *d_zapped
+   (device uint64) += zapped blocks.  npol is 1 or 2; M and the spans are
+   even; d_in and d_out are 16-byte aligned; npol*4*(M + 8) bytes at most
+   224 KiB, i.e. M <= 28664 for two pols. */
+int dspsr_b200_sk (dspsr_b200_context* ctx, const float* d_in, uint64_t in_span,
+                   uint64_t ndat, unsigned nchan, unsigned npol, unsigned M, int zero_is_valid,
+                   unsigned Nd, float lower, float upper, float* d_out, uint64_t out_span,
+                   float* d_sums, uint32_t* d_counts, uint8_t* d_mask, uint64_t* d_zapped,
+                   uint64_t* npart_out);
 
 /* ---------------------------------------------------------------------- */
 /* Fold::Engine (CUDA::FoldEngine, Signal/Pulsar/FoldCUDA.cu:78-704;        */
