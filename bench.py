@@ -3,7 +3,7 @@
 dedispersion -> detection -> fold, in complex Msamples/s.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                  [--config c1]
+                  [--config c1|c2|c4]
 
 One step = one block of the workload processed end to end (unpack -> fold),
 the InputBuffering overlap carried from block to block.  Inputs are seeded
@@ -49,6 +49,13 @@ CONFIGS = {
                   "(four blocks = the 2^28-sample data set)"),
         cf=1400.0, bw=256.0, dm=500.0, nchan=1, npol=2, nfft=1 << 16, nbin=2048,
         period=5.757e-3, state=3, ndat=1 << 26, duty=0.03, snr=10.0, sigma=12.0, fb=64),
+    "c4": dict(
+        kind="sk",
+        workload=("spectral kurtosis RFI excision: 512 channels x 2^20 samples x 2 pol complex "
+                  "FP32 voltages (sigma 1) with 20 CW tones (0.5-5 sigma), 1 %-duty broadband "
+                  "bursts (1-64 samples, 3-30 sigma) and one drifting chirp; M = 1024, "
+                  "3 sigma thresholds (SKLimits), sums + mask + masked copy"),
+        nchan=512, npol=2, ndat=1 << 20, M=1024, std_devs=3.0),
 }
 
 NBLOCKS = 4
@@ -474,6 +481,220 @@ def run_b200(args, cfg, world, rank, local):
     ctx.close()
 
 
+# ---------------------------------------------------------------------------
+# SpectralKurtosis workload
+# ---------------------------------------------------------------------------
+
+def make_sk_block(cfg, seed, device):
+    """Complex FPT voltages [nchan][npol][ndat] with injected RFI, generated on
+    the GPU (torch is the synthesis tool here, not the product path)."""
+    import torch
+    nchan, npol, ndat, M = cfg["nchan"], cfg["npol"], cfg["ndat"], cfg["M"]
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    x = torch.randn((nchan, npol, ndat, 2), generator=gen, device=device) * (1 / np.sqrt(2))
+    rng = np.random.default_rng(seed)
+    t = torch.arange(ndat, device=device, dtype=torch.float64)
+    for _ in range(20):                                   # CW tones
+        c = int(rng.integers(nchan))
+        amp, f = rng.uniform(0.5, 5.0), rng.uniform(-0.5, 0.5)
+        ph = 2 * np.pi * f * t
+        for p in range(npol):
+            x[c, p, :, 0] += (amp * torch.cos(ph)).float()
+            x[c, p, :, 1] += (amp * torch.sin(ph)).float()
+    nburst = int(0.01 * ndat / 32.5)                      # 1 % duty, widths 1..64
+    for _ in range(nburst):
+        w = int(rng.integers(1, 65))
+        t0 = int(rng.integers(0, ndat - w))
+        x[:, :, t0:t0 + w, :] *= float(rng.uniform(3.0, 30.0))
+    nblk = ndat // M                                      # drifting chirp, 3 sigma
+    ph = 2 * np.pi * (0.05 * t[:M] + 1e-5 * t[:M] * t[:M])
+    for b in range(nblk):
+        c = (b * nchan) // nblk
+        seg = slice(b * M, (b + 1) * M)
+        for p in range(npol):
+            x[c, p, seg, 0] += (3 * torch.cos(ph)).float()
+            x[c, p, seg, 1] += (3 * torch.sin(ph)).float()
+    torch.cuda.synchronize()
+    return x.reshape(-1)
+
+
+def sk_bytes_per_sample(inplace):
+    # read 8 B per complex sample; write it back (out of place) or nothing
+    return 8.0 if inplace else 16.0
+
+
+def sk_cpu_sample(cfg):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    M, npol = cfg["M"], cfg["npol"]
+    lo, hi = orc.sk_limits(M, 1, cfg["std_devs"], npol)
+    # bounded sample: 16 channels of the block, all of their time
+    nchan_s = max(1, min(cfg["nchan"], 16))
+    rng = np.random.default_rng(7)
+    x = (rng.standard_normal((nchan_s, npol, cfg["ndat"])) +
+         1j * rng.standard_normal((nchan_s, npol, cfg["ndat"]))).astype(np.complex64)
+    return orc, lo, hi, nchan_s, x
+
+
+def run_reference_sk(args, cfg, world, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    orc, lo, hi, nchan_s, x = sk_cpu_sample(cfg)
+    M, npol = cfg["M"], cfg["npol"]
+
+    def step():
+        t0 = time.perf_counter()
+        orc.sk(x, M, lo, hi)
+        return time.perf_counter() - t0
+    for _ in range(args.warmup):
+        step()
+    total = sum(step() for _ in range(args.steps))
+    msps = nchan_s * npol * cfg["ndat"] * args.steps / total / 1e6
+    line = {
+        "impl": "reference", "metric": "complex Msamples/s spectral kurtosis",
+        "value": round(msps, 3), "unit": "complex Msamples/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * total / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64",
+        "data": "synthetic (seeded Gaussian complex voltages)",
+        "config": {"workload": cfg["workload"], "sample_channels_per_step": nchan_s},
+        "cpu_baseline": {"value": round(msps, 3), "unit": "complex Msamples/s", "cores": threads,
+                         "kind": "port",
+                         "sample": (f"{nchan_s} of {cfg['nchan']} channels x {cfg['ndat']} "
+                                    f"samples x {npol} pol per step through the oracle "
+                                    "restatement of SpectralKurtosis compute/detect/mask "
+                                    "(OpenMP over blocks)")},
+        "e2e": {"value": round(msps, 3), "unit": "complex Msamples/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_sk(cfg, target_s=12.0):
+    threads = os.cpu_count() or 1
+    orc, lo, hi, nchan_s, x = sk_cpu_sample(cfg)
+    M, npol = cfg["M"], cfg["npol"]
+    orc.sk(x, M, lo, hi)
+    total, reps = 0.0, 0
+    while total < target_s:
+        t0 = time.perf_counter()
+        orc.sk(x, M, lo, hi)
+        total += time.perf_counter() - t0
+        reps += 1
+    msps = nchan_s * npol * cfg["ndat"] * reps / total / 1e6
+    return {"value": round(msps, 3), "unit": "complex Msamples/s", "cores": threads,
+            "kind": "port",
+            "sample": (f"{nchan_s} channels x {cfg['ndat']} samples x {npol} pol x {reps} "
+                       f"through the oracle SK restatement (OpenMP over blocks), {total:.1f} s")}
+
+
+def run_b200_sk(args, cfg, world, rank, local):
+    import torch
+    import dspsr_b200 as b2
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    ctx = b2.Context(local)
+    nchan, npol, ndat, M = cfg["nchan"], cfg["npol"], cfg["ndat"], cfg["M"]
+    lo, hi = b2.sk_limits(M, 1, cfg["std_devs"], npol)
+    x = make_sk_block(cfg, 4321 + rank, device)
+    npart = ndat // M
+    out = torch.empty_like(x)
+    sums = torch.empty(npart * nchan * npol * 2, dtype=torch.float32, device=device)
+    counts = torch.empty(npart * nchan, dtype=torch.int32, device=device)
+    mask = torch.empty(npart * nchan, dtype=torch.uint8, device=device)
+    zapped = torch.zeros(1, dtype=torch.int64, device=device)
+    samples_per_step = nchan * npol * ndat
+    inplace = args.sk_inplace
+
+    def step(src, dst):
+        ctx.sk(src, ndat, ndat, nchan, npol, M, lo, hi, dst, ndat, sums, counts, mask, zapped)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(1.0)
+    # an in-place step masks its own input; later steps then see masked data,
+    # which reads the same bytes (the input exceeds L2 many times per step)
+    for _ in range(args.warmup):
+        step(x, x if inplace else out)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    launches0 = b2.kernel_launches()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    evs[0].record()
+    for i in range(args.steps):
+        step(x, x if inplace else out)
+        evs[i + 1].record()
+    torch.cuda.synchronize()
+    launches = b2.kernel_launches() - launches0
+    clk = clocks.stop()
+    barrier(world)
+    ms = evs[0].elapsed_time(evs[-1])
+    ms_max = max_over_ranks(ms, world)
+    value = samples_per_step * args.steps * world / (ms_max / 1e3) / 1e6
+    per_launch = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
+    zap_frac = float(mask.float().mean().item())
+
+    # ---- end to end: pinned host voltages in, masked voltages and mask out --
+    hx = torch.empty(x.shape, dtype=x.dtype, pin_memory=True)
+    hx.copy_(x)
+    hout = torch.empty(x.shape, dtype=x.dtype, pin_memory=True)
+    hmask = torch.empty(mask.shape, dtype=mask.dtype, pin_memory=True)
+    for _ in range(max(1, args.warmup)):
+        x.copy_(hx, non_blocking=True)
+        step(x, x if inplace else out)
+        hout.copy_(x if inplace else out, non_blocking=True)
+        hmask.copy_(mask, non_blocking=True)
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        x.copy_(hx, non_blocking=True)
+        step(x, x if inplace else out)
+        hout.copy_(x if inplace else out, non_blocking=True)
+        hmask.copy_(mask, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    e2e_ms = max_over_ranks(max(e0.elapsed_time(e1), 1e3 * wall), world)
+    e2e = samples_per_step * args.steps * world / (e2e_ms / 1e3) / 1e6
+
+    hbm_peak, _, peak_src = measured_peaks()
+    bps = sk_bytes_per_sample(inplace)
+    avg_s = statistics.mean(per_launch) / 1e3
+    achieved = bps * samples_per_step / avg_s / 1e9
+    tb = ncu_traffic(f"{args.config}:sk")
+    line = {
+        "metric": "complex Msamples/s spectral kurtosis", "value": round(value, 3),
+        "unit": "complex Msamples/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64",
+        "data": "synthetic (seeded Gaussian complex voltages + injected RFI)",
+        "config": {"workload": cfg["workload"], "M": M, "thresholds": [float(lo), float(hi)],
+                   "in_place": inplace, "zapped_fraction": round(zap_frac, 5),
+                   "l2": f"input {x.numel() * 4 >> 30} GiB per step, larger than L2",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "clocks": clk,
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "k_sk", "achieved": round(achieved, 2),
+                     "peak": hbm_peak, "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
+                     "traffic": tb * samples_per_step if tb else None,
+                     "peak_source": peak_src, "bytes_per_sample": bps},
+        "e2e": {"value": round(e2e, 3), "unit": "complex Msamples/s",
+                "h2d_bytes_per_step": int(hx.numel() * 4),
+                "d2h_bytes_per_step": int(hout.numel() * 4 + hmask.numel())},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sk(cfg)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -482,6 +703,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="c1", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sk-inplace", action="store_true",
+                    help="c4: mask the voltages in place (only zapped blocks are written)")
     ap.add_argument("--ndat", type=int, default=0,
                     help="samples per pol per block (default: the workload's); smaller blocks "
                          "are for profiling captures only")
@@ -493,10 +716,11 @@ def main():
         cfg["workload"] += f" [profiling size: {args.ndat} samples/pol per block]"
     world, rank, local = dist_init()
     try:
+        sk = cfg.get("kind") == "sk"
         if args.impl == "reference":
-            run_reference(args, cfg, world, rank)
+            (run_reference_sk if sk else run_reference)(args, cfg, world, rank)
         else:
-            run_b200(args, cfg, world, rank, local)
+            (run_b200_sk if sk else run_b200)(args, cfg, world, rank, local)
     finally:
         if world > 1:
             import torch.distributed as dist
