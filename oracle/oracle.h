@@ -157,6 +157,33 @@ void orc_sk_mask (const float* in, uint64_t in_span, float* out, uint64_t out_sp
 int orc_sk_limits (unsigned M, unsigned Nd, float std_devs, unsigned ntest, float* lower,
                    float* upper);
 
+/* ---- InverseFilterbank (Signal/General/InverseFilterbank.C:129-454,
+        InverseFilterbankEngineCPU.C:46-792), complex FPT input ---------------- */
+typedef struct orc_ifb_config
+{
+  unsigned input_nchan;        /* fine channels */
+  unsigned output_nchan;       /* divides input_nchan */
+  unsigned pfb_nchan;          /* fine channels per coarse (PFB) channel */
+  unsigned npol;
+  unsigned input_fft_length;   /* forward FFT per fine channel */
+  unsigned os_num, os_den;     /* oversampling factor, e.g. 4/3 */
+  unsigned output_discard_pos, output_discard_neg;
+  int pfb_dc_chan, pfb_all_chan, dual_sideband;
+} orc_ifb_config;
+/* in [input_nchan][npol][in_span] complex; out [output_nchan][npol][out_span]
+   complex; response [output_nchan][Lout] complex, temporal [Lin] and
+   spectral [Lout] real windows, each optional (null).  Lout =
+   (input_nchan/output_nchan) * Lin*os_den/os_num.  Returns npart, or -1 for
+   an invalid configuration. */
+int64_t orc_inverse_filterbank_f32 (const orc_ifb_config* cfg, const float* in, uint64_t ndat,
+                                    uint64_t in_span, const float* response,
+                                    const float* temporal, const float* spectral, float* out,
+                                    uint64_t out_span);
+int64_t orc_inverse_filterbank_f64 (const orc_ifb_config* cfg, const double* in, uint64_t ndat,
+                                    uint64_t in_span, const double* response,
+                                    const double* temporal, const double* spectral, double* out,
+                                    uint64_t out_span);
+
 /* ---- the whole single-channel path, for the timed CPU baseline ----------- */
 /* int8 TFPD (nchan=1, npol=2, ndim=2) -> unpack -> convolve -> Intensity ->
    fold.  Returns the number of output samples folded per pol. */

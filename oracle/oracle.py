@@ -59,6 +59,10 @@ _SIGS = {
     "orc_sk_mask": (None, [f32p, c_u64, f32p, c_u64, u8p, c_u64, c_int, c_int, c_uint]),
     "orc_sk_limits": (c_int, [c_uint, c_uint, ctypes.c_float, c_uint,
                               ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
+    "orc_inverse_filterbank_f32": (c_i64, [ctypes.c_void_p, f32p, c_u64, c_u64, ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_void_p, f32p, c_u64]),
+    "orc_inverse_filterbank_f64": (c_i64, [ctypes.c_void_p, f64p, c_u64, c_u64, ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_void_p, f64p, c_u64]),
     "orc_pipeline_c1": (c_u64, [u8p, c_u64, f32p, f32p, c_uint, c_uint, c_uint, c_dbl, c_dbl,
                                 c_uint, f32p, u32p, c_int]),
     "orc_channel_centre": (c_dbl, [c_dbl, c_dbl, c_uint, c_uint, c_int, c_int]),
@@ -101,6 +105,54 @@ def sk_limits(M, Nd=1, std_devs=3.0, ntest=1):
     if rc != 0:
         raise ValueError(f"sk_limits: invalid M={M} Nd={Nd} std_devs={std_devs} (rc {rc})")
     return np.float32(lo.value), np.float32(hi.value)
+
+
+class IfbConfig(ctypes.Structure):
+    """orc_ifb_config (oracle.h)."""
+    _fields_ = [("input_nchan", c_uint), ("output_nchan", c_uint), ("pfb_nchan", c_uint),
+                ("npol", c_uint), ("input_fft_length", c_uint), ("os_num", c_uint),
+                ("os_den", c_uint), ("output_discard_pos", c_uint),
+                ("output_discard_neg", c_uint), ("pfb_dc_chan", c_int), ("pfb_all_chan", c_int),
+                ("dual_sideband", c_int)]
+
+
+def ifb_sizes(cfg):
+    """(keep, Lout, input_discard_pos, input_discard_neg, in_step, out_step)."""
+    keep = cfg["input_fft_length"] * cfg["os_den"] // cfg["os_num"]
+    lout = cfg["input_nchan"] // cfg["output_nchan"] * keep
+    scale = cfg["output_nchan"] * cfg["os_num"], cfg["input_nchan"] * cfg["os_den"]
+    ipos = cfg["output_discard_pos"] * scale[0] // scale[1]
+    ineg = cfg["output_discard_neg"] * scale[0] // scale[1]
+    return (keep, lout, ipos, ineg, cfg["input_fft_length"] - ipos - ineg,
+            lout - cfg["output_discard_pos"] - cfg["output_discard_neg"])
+
+
+def inverse_filterbank(x, cfg, response=None, temporal=None, spectral=None, fp64=False):
+    """x: complex (input_nchan, npol, ndat).  cfg: dict of orc_ifb_config
+    fields.  Returns complex (output_nchan, npol, npart*out_step)."""
+    nin, npol, ndat = x.shape
+    c = IfbConfig(**{k: int(v) for k, v in cfg.items()})
+    keep, lout, ipos, ineg, in_step, out_step = ifb_sizes(cfg)
+    npart = (ndat - ipos - ineg) // in_step if ndat > ipos + ineg else 0
+    cdt, rdt = (np.complex128, np.float64) if fp64 else (np.complex64, np.float32)
+    xin = np.ascontiguousarray(x, cdt)
+    out = np.zeros((cfg["output_nchan"], npol, max(1, npart * out_step)), cdt)
+
+    def opt(a, dt):
+        if a is None:
+            return None, None
+        a = np.ascontiguousarray(a, dt)
+        return a, a.ctypes.data
+    r, rp = opt(response, cdt)
+    t, tp = opt(temporal, rdt)
+    sp_, spp = opt(spectral, rdt)
+    f = lib().orc_inverse_filterbank_f64 if fp64 else lib().orc_inverse_filterbank_f32
+    n = f(ctypes.addressof(c), xin.view(rdt).ravel(), ndat, ndat, rp, tp, spp,
+          out.view(rdt).ravel(), out.shape[2])
+    if n < 0:
+        raise ValueError("inverse_filterbank: invalid configuration")
+    assert n == npart
+    return out[:, :, :npart * out_step]
 
 
 def channel_centres(cf, bw, nchan, swap=False, dc_centred=False):

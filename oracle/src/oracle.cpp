@@ -1064,6 +1064,242 @@ int orc_sk_limits (unsigned M, unsigned Nd, float std_devs, unsigned ntest, floa
   return 0;
 }
 
+} // extern "C"
+
+namespace {
+
+// FFT of any length 2^a 3^b (FFTW conventions, unnormalised): recursive
+// decimation in time by 2 or 3, twiddles from double; plain DFT otherwise.
+// Power-of-two lengths go to the radix-2 routine above.
+template <typename T>
+void fft_any (int n, int sign, const std::complex<T>* in, std::complex<T>* out)
+{
+  typedef std::complex<T> C;
+  if ((n & (n - 1)) == 0)
+  {
+    fft<T> (n, sign, in, out);
+    return;
+  }
+  const int r = n % 2 == 0 ? 2 : n % 3 == 0 ? 3 : n;
+  if (r == n)
+  {
+    for (int k = 0; k < n; k++)
+    {
+      std::complex<double> acc (0, 0);
+      for (int j = 0; j < n; j++)
+      {
+        const double a = sign * 2.0 * M_PI * double ((int64_t (j) * k) % n) / double (n);
+        acc += std::complex<double> (in[j].real (), in[j].imag ()) *
+               std::complex<double> (std::cos (a), std::sin (a));
+      }
+      out[k] = C (T (acc.real ()), T (acc.imag ()));
+    }
+    return;
+  }
+  const int m = n / r;
+  std::vector<C> sub (n), res (n);
+  for (int q = 0; q < r; q++)
+  {
+    for (int j = 0; j < m; j++) sub[q * m + j] = in[j * r + q];
+    fft_any<T> (m, sign, sub.data () + q * m, res.data () + q * m);
+  }
+  for (int k = 0; k < m; k++)
+  {
+    C t[3];
+    for (int q = 0; q < r; q++)
+    {
+      const double a = sign * 2.0 * M_PI * double (int64_t (q) * k) / double (n);
+      const C w (T (std::cos (a)), T (std::sin (a)));
+      const C v = res[q * m + k];
+      t[q] = C (v.real () * w.real () - v.imag () * w.imag (),
+                v.real () * w.imag () + v.imag () * w.real ());
+    }
+    for (int p = 0; p < r; p++)
+    {
+      C acc = t[0];
+      for (int q = 1; q < r; q++)
+      {
+        const double a = sign * 2.0 * M_PI * double ((p * q) % r) / double (r);
+        const C w (T (std::cos (a)), T (std::sin (a)));
+        acc += C (t[q].real () * w.real () - t[q].imag () * w.imag (),
+                  t[q].real () * w.imag () + t[q].imag () * w.real ());
+      }
+      out[p * m + k] = acc;
+    }
+  }
+}
+
+// InverseFilterbankEngineCPU::build_fine_channel_plan (InverseFilterbankEngineCPU.C:378-425):
+// input channel feeding stitched position ichan when several coarse channels
+// are combined into one output channel.
+std::vector<unsigned> ifb_fine_channel_plan (unsigned input_nchan, unsigned fine_per_coarse)
+{
+  std::vector<unsigned> idx (input_nchan), plan (input_nchan);
+  const unsigned half_band = input_nchan / 2, half_coarse = fine_per_coarse / 2;
+  for (unsigned i = 0; i < input_nchan; i++) idx[i] = (i + input_nchan - half_coarse) % input_nchan;
+  for (unsigned i = 0; i < half_band; i++) std::swap (idx[i], idx[i + half_band]);
+  for (unsigned ic = 0; ic < input_nchan / fine_per_coarse; ic++)
+    for (unsigned i = ic * fine_per_coarse; i < ic * fine_per_coarse + half_coarse; i++)
+      std::swap (idx[i], idx[i + half_coarse]);
+  for (unsigned i = 0; i < input_nchan; i++) plan[idx[i]] = i;
+  return plan;
+}
+
+// InverseFilterbankEngineCPU::perform (InverseFilterbankEngineCPU.C:309-366)
+// with stitch / stitch_one (:443-616), filter (:620-700) and invert (:703-779)
+// for complex (analytic) FPT input.
+template <typename T>
+int64_t inverse_filterbank (const orc_ifb_config* cfg, const T* in, uint64_t ndat,
+                            uint64_t in_span, const T* response, const T* temporal,
+                            const T* spectral, T* out, uint64_t out_span)
+{
+  typedef std::complex<T> C;
+  const unsigned nin = cfg->input_nchan, nout = cfg->output_nchan, pfb = cfg->pfb_nchan;
+  const unsigned Lin = cfg->input_fft_length;
+  if (!nin || !nout || !pfb || nin % nout || nin % pfb || !cfg->os_num || !cfg->os_den) return -1;
+  if ((uint64_t (Lin) * cfg->os_den) % cfg->os_num) return -1;
+  const unsigned keep = unsigned (uint64_t (Lin) * cfg->os_den / cfg->os_num);  // Rational::normalize
+  if ((Lin - keep) % 2 || keep % 2) return -1;
+  const unsigned fine_per_out = nin / nout;
+  const unsigned Lout = fine_per_out * keep;
+  // output_to_input of the output discards (InverseFilterbank.C:285-288)
+  auto to_input = [&] (uint64_t n) -> int64_t {
+    const uint64_t a = n * nout * cfg->os_num, b = uint64_t (nin) * cfg->os_den;
+    return a % b ? -1 : int64_t (a / b);
+  };
+  const int64_t in_pos = to_input (cfg->output_discard_pos), in_neg = to_input (cfg->output_discard_neg);
+  if (in_pos < 0 || in_neg < 0) return -1;
+  const uint64_t in_step = Lin - uint64_t (in_pos + in_neg);
+  const uint64_t out_step = Lout - uint64_t (cfg->output_discard_pos + cfg->output_discard_neg);
+  const unsigned coarse = nin / pfb;
+  unsigned coarse_per_out = 1, out_per_coarse = 1, steps = coarse, out_per_step = 1;
+  std::vector<unsigned> plan;
+  if (fine_per_out > pfb)
+  {
+    if (fine_per_out % pfb) return -1;
+    coarse_per_out = fine_per_out / pfb;
+    steps = coarse / coarse_per_out;
+    plan = ifb_fine_channel_plan (nin, pfb);
+  }
+  else if (fine_per_out < pfb)
+  {
+    if (pfb % fine_per_out) return -1;
+    out_per_coarse = pfb / fine_per_out;
+    steps = nout / out_per_coarse;
+    out_per_step = out_per_coarse;
+  }
+  const bool shift = cfg->pfb_dc_chan != 0;
+  const unsigned keep2 = keep / 2;
+  uint64_t npart = 0;
+  if (ndat > uint64_t (in_pos + in_neg)) npart = (ndat - (in_pos + in_neg)) / in_step;
+  const unsigned spec_len = out_per_step * Lout;   // stitched spectrum of one step
+  std::vector<C> time (Lin), fine (Lin), spec (spec_len), tout (Lout);
+  for (unsigned ipol = 0; ipol < cfg->npol; ipol++)
+    for (uint64_t ipart = 0; ipart < npart; ipart++)
+      for (unsigned istep = 0; istep < steps; istep++)
+      {
+        const unsigned fine_offset = istep * coarse_per_out * pfb;
+        const unsigned out_offset = istep * out_per_coarse;
+        std::fill (spec.begin (), spec.end (), C (0, 0));
+        // stitch
+        for (unsigned icoarse = 0; icoarse < coarse_per_out; icoarse++)
+        {
+          const unsigned start = fine_offset + icoarse * pfb;
+          const uint64_t soff = uint64_t (icoarse) * keep * pfb;
+          for (unsigned ich = 0; ich < pfb; ich++)
+          {
+            unsigned jch = ich + start;
+            if (coarse_per_out > 1) jch = plan[jch];
+            const C* src = reinterpret_cast<const C*> (in) + (uint64_t (jch) * cfg->npol + ipol) * in_span
+                           + ipart * in_step;
+            for (unsigned i = 0; i < Lin; i++)
+              time[i] = temporal ? C (src[i].real () * temporal[i], src[i].imag () * temporal[i])
+                                 : src[i];
+            fft<T> (int (Lin), -1, time.data (), fine.data ());
+            uint64_t neg, pos;
+            if (shift)
+            {
+              if (ich == 0)
+              {
+                neg = uint64_t (keep) * pfb - keep2;
+                pos = 0;
+              }
+              else
+              {
+                neg = uint64_t (keep) * ich - keep2;
+                pos = neg + keep2;
+              }
+            }
+            else
+            {
+              neg = uint64_t (keep) * ich;
+              pos = neg + keep2;
+            }
+            const C* pneg = fine.data () + (Lin - keep2);
+            const C* ppos = fine.data ();
+            if (!cfg->dual_sideband)
+            {
+              pneg = fine.data () + (Lin - keep) / 2;
+              ppos = pneg + keep2;
+            }
+            for (unsigned j = 0; j < keep2; j++)
+            {
+              spec[soff + neg + j] = pneg[j];
+              spec[soff + pos + j] = ppos[j];
+            }
+          }
+        }
+        // filter
+        if (!cfg->pfb_all_chan && cfg->pfb_dc_chan)
+          for (unsigned j = 0; j < keep2; j++) spec[spec_len - keep2 + j] = C (0, 0);
+        for (unsigned io = 0; io < out_per_step; io++)
+        {
+          C* s = spec.data () + uint64_t (io) * Lout;
+          if (response)
+          {
+            // Response::operate: (f_r d_r - f_i d_i, f_i d_r + f_r d_i)
+            const C* f = reinterpret_cast<const C*> (response) + uint64_t (out_offset + io) * Lout;
+            for (unsigned k = 0; k < Lout; k++)
+            {
+              const T d_r = s[k].real (), d_i = s[k].imag ();
+              const T f_r = f[k].real (), f_i = f[k].imag ();
+              s[k] = C (f_r * d_r - f_i * d_i, f_i * d_r + f_r * d_i);
+            }
+          }
+          if (spectral)
+            for (unsigned k = 0; k < Lout; k++)
+              s[k] = C (s[k].real () * spectral[k], s[k].imag () * spectral[k]);
+          // invert
+          fft_any<T> (int (Lout), +1, s, tout.data ());
+          C* dst = reinterpret_cast<C*> (out) + (uint64_t (out_offset + io) * cfg->npol + ipol) * out_span
+                   + ipart * out_step;
+          for (uint64_t t = 0; t < out_step; t++) dst[t] = tout[cfg->output_discard_pos + t];
+        }
+      }
+  return int64_t (npart);
+}
+
+} // namespace
+
+extern "C" {
+
+int64_t orc_inverse_filterbank_f32 (const orc_ifb_config* cfg, const float* in, uint64_t ndat,
+                                    uint64_t in_span, const float* response, const float* temporal,
+                                    const float* spectral, float* out, uint64_t out_span)
+{
+  return inverse_filterbank<float> (cfg, in, ndat, in_span, response, temporal, spectral, out,
+                                    out_span);
+}
+
+int64_t orc_inverse_filterbank_f64 (const orc_ifb_config* cfg, const double* in, uint64_t ndat,
+                                    uint64_t in_span, const double* response,
+                                    const double* temporal, const double* spectral, double* out,
+                                    uint64_t out_span)
+{
+  return inverse_filterbank<double> (cfg, in, ndat, in_span, response, temporal, spectral, out,
+                                     out_span);
+}
+
 uint64_t orc_pipeline_c1 (const uint8_t* in, uint64_t ndat, const float* lut,
                           const float* response, unsigned nfft, unsigned nfilt_pos,
                           unsigned nfilt_neg, double phi, double phase_per_sample,
