@@ -601,6 +601,375 @@ int pipeline_input (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat, ui
 // exported functions
 // ---------------------------------------------------------------------------
 
+// ---------------------------------------------------------------------------
+// inverse filterbank engine
+// ---------------------------------------------------------------------------
+
+struct dspsr_b200_inverse_filterbank
+{
+  dspsr_b200_context* ctx = nullptr;
+  IfbShape shape {};
+  unsigned in_discard_pos = 0, in_discard_neg = 0;
+  DevBuf<int4> map;
+  DevBuf<float2> tw_lin, tw4, ptab, response, scratch;
+  DevBuf<float> temporal, spectral;
+  DevBuf<int> err;
+  bool have_response = false, have_temporal = false, have_spectral = false;
+  int nsm = 148;
+  unsigned max_batch = 1;
+
+  int init (dspsr_b200_context* c, const dspsr_b200_ifb_config& cfg);
+  IfbTables tables () const
+  {
+    IfbTables t;
+    t.map = map.ptr;
+    t.tw_lin = tw_lin.ptr;
+    t.tw4 = tw4.ptr;
+    t.ptab = ptab.ptr;
+    t.response = have_response ? response.ptr : nullptr;
+    t.temporal = have_temporal ? temporal.ptr : nullptr;
+    t.spectral = have_spectral ? spectral.ptr : nullptr;
+    t.lut = ctx->d_lut;
+    t.err = err.ptr;
+    t.nsm = nsm;
+    return t;
+  }
+  void release ()
+  {
+    map.release ();
+    tw_lin.release ();
+    tw4.release ();
+    ptab.release ();
+    response.release ();
+    scratch.release ();
+    temporal.release ();
+    spectral.release ();
+    err.release ();
+  }
+};
+
+namespace {
+
+// The stitching of InverseFilterbankEngineCPU::perform / stitch / stitch_one /
+// filter (InverseFilterbankEngineCPU.C:309-366, 443-616, 620-650), evaluated
+// once on the host: where each fine channel's two kept halves land in the
+// output channels' spectra, and which half the DC-channel rule zeroes.
+// Returns an empty message on success.
+std::string ifb_build_map (const dspsr_b200_ifb_config& cfg, unsigned keep, unsigned lout,
+                           std::vector<int4>& map)
+{
+  const unsigned nin = cfg.input_nchan, nout = cfg.output_nchan, pfb = cfg.pfb_nchan;
+  const unsigned fine_per_out = nin / nout, coarse = nin / pfb;
+  unsigned coarse_per_out = 1, out_per_coarse = 1, steps = coarse, out_per_step = 1;
+  std::vector<unsigned> plan;
+  if (fine_per_out > pfb)
+  {
+    if (fine_per_out % pfb) return "output channels do not hold whole coarse channels";
+    coarse_per_out = fine_per_out / pfb;
+    steps = coarse / coarse_per_out;
+    plan = ifb_fine_channel_plan (nin, pfb);
+  }
+  else if (fine_per_out < pfb)
+  {
+    if (pfb % fine_per_out) return "coarse channels do not split into whole output channels";
+    out_per_coarse = pfb / fine_per_out;
+    steps = nout / out_per_coarse;
+    out_per_step = out_per_coarse;
+  }
+  const unsigned keep2 = keep / 2;
+  const uint64_t spec_len = uint64_t (out_per_step) * lout;
+  map.assign (nin, make_int4 (-1, -1, -1, -1));
+  for (unsigned istep = 0; istep < steps; istep++)
+  {
+    const unsigned fine_offset = istep * coarse_per_out * pfb;
+    const unsigned out_offset = istep * out_per_coarse;
+    std::vector<char> covered (spec_len / keep2, 0);
+    for (unsigned icoarse = 0; icoarse < coarse_per_out; icoarse++)
+    {
+      const uint64_t soff = uint64_t (icoarse) * keep * pfb;
+      for (unsigned ich = 0; ich < pfb; ich++)
+      {
+        unsigned jch = fine_offset + icoarse * pfb + ich;
+        if (coarse_per_out > 1) jch = plan[jch];
+        uint64_t neg, pos;
+        if (cfg.pfb_dc_chan)
+        {
+          neg = ich == 0 ? uint64_t (keep) * pfb - keep2 : uint64_t (keep) * ich - keep2;
+          pos = ich == 0 ? 0 : neg + keep2;
+        }
+        else
+        {
+          neg = uint64_t (keep) * ich;
+          pos = neg + keep2;
+        }
+        neg += soff;
+        pos += soff;
+        if (map[jch].x >= 0) return "an input channel is stitched twice";
+        for (uint64_t at : {neg, pos})
+        {
+          if (at % keep2 || at >= spec_len || covered[at / keep2]) return "stitched halves overlap";
+          covered[at / keep2] = 1;
+        }
+        map[jch] = make_int4 (int (out_offset + neg / lout), int (neg % lout),
+                              int (out_offset + pos / lout), int (pos % lout));
+      }
+    }
+    for (char c : covered)
+      if (!c) return "stitched spectrum has gaps";
+    // filter: without every PFB channel, the last half channel is zeroed
+    if (!cfg.pfb_all_chan && cfg.pfb_dc_chan)
+    {
+      const uint64_t z = spec_len - keep2;
+      const int zo = int (out_offset + z / lout), zk = int (z % lout);
+      for (int4& m : map)
+      {
+        if (m.x == zo && m.y == zk) m.y |= IFB_ZERO;
+        if (m.z == zo && m.w == zk) m.w |= IFB_ZERO;
+      }
+    }
+  }
+  return std::string ();
+}
+
+} // namespace
+
+int dspsr_b200_inverse_filterbank::init (dspsr_b200_context* c, const dspsr_b200_ifb_config& cfg)
+{
+  ctx = c;
+  const unsigned nin = cfg.input_nchan, nout = cfg.output_nchan, pfb = cfg.pfb_nchan;
+  if (!nin || !nout || !pfb || nin % nout || nin % pfb || cfg.npol == 0 || cfg.npol > 2 ||
+      nin > 65535)
+    return fail (ctx, DSPSR_B200_EINVAL,
+                 "inverse filterbank: invalid channels (in %u, out %u, pfb %u, npol %u)", nin,
+                 nout, pfb, cfg.npol);
+  const unsigned lin = cfg.input_fft_length;
+  if (!ifb_supported_lin (lin))
+    return fail (ctx, DSPSR_B200_EINVAL,
+                 "inverse filterbank: input FFT length %u not a power of two in [64, 4096]", lin);
+  // Rational::normalize (Rational.C:83-90): the kept bins of each fine channel
+  if (!cfg.os_num || !cfg.os_den || (uint64_t (lin) * cfg.os_den) % cfg.os_num)
+    return fail (ctx, DSPSR_B200_EINVAL, "inverse filterbank: %u * %u/%u is not an integer", lin,
+                 cfg.os_den, cfg.os_num);
+  const unsigned keep = unsigned (uint64_t (lin) * cfg.os_den / cfg.os_num);
+  if (keep == 0 || keep > lin || keep % 2 || (lin - keep) % 2)
+    return fail (ctx, DSPSR_B200_EINVAL, "inverse filterbank: kept bins %u must be even", keep);
+  const unsigned lout = nin / nout * keep;
+  // output_to_input (InverseFilterbank.C:128-142) of the output discards
+  const uint64_t num = uint64_t (nout) * cfg.os_num, den = uint64_t (nin) * cfg.os_den;
+  if ((uint64_t (cfg.output_discard_pos) * num) % den ||
+      (uint64_t (cfg.output_discard_neg) * num) % den)
+    return fail (ctx, DSPSR_B200_EINVAL,
+                 "inverse filterbank: output discards do not map to whole input samples");
+  in_discard_pos = unsigned (uint64_t (cfg.output_discard_pos) * num / den);
+  in_discard_neg = unsigned (uint64_t (cfg.output_discard_neg) * num / den);
+  if (uint64_t (cfg.output_discard_pos) + cfg.output_discard_neg >= lout ||
+      uint64_t (in_discard_pos) + in_discard_neg >= lin)
+    return fail (ctx, DSPSR_B200_EINVAL, "inverse filterbank: discards exceed the FFT length");
+  unsigned n2 = 0, n1 = 0;
+  for (unsigned cand : {8192u, 4096u})
+  {
+    if (lout % cand) continue;
+    const unsigned r = lout / cand;
+    if (r == 2 || r == 3 || r == 4 || r == 6 || r == 8 || r == 12 || r == 16 || r == 24 ||
+        r == 32)
+    {
+      n2 = cand;
+      n1 = r;
+      break;
+    }
+  }
+  if (!n2)
+    return fail (ctx, DSPSR_B200_EINVAL,
+                 "inverse filterbank: output FFT length %u is not n1 x 4096 or n1 x 8192 with "
+                 "n1 in {2,3,4,6,8,12,16,24,32}", lout);
+  std::vector<int4> m;
+  const std::string why = ifb_build_map (cfg, keep, lout, m);
+  if (!why.empty ()) return fail (ctx, DSPSR_B200_EINVAL, "inverse filterbank: %s", why.c_str ());
+  shape.nin = nin;
+  shape.nout = nout;
+  shape.npol = cfg.npol;
+  shape.lin = lin;
+  shape.keep = keep;
+  shape.lout = lout;
+  shape.n1 = n1;
+  shape.n2 = n2;
+  shape.in_step = lin - in_discard_pos - in_discard_neg;
+  shape.out_step = lout - cfg.output_discard_pos - cfg.output_discard_neg;
+  shape.out_discard_pos = cfg.output_discard_pos;
+  shape.dual_sideband = cfg.dual_sideband;
+  B200_CHECK (ctx, map.reserve (nin), "cudaMalloc stitch map");
+  B200_CHECK (ctx, cudaMemcpy (map.ptr, m.data (), nin * sizeof (int4), cudaMemcpyHostToDevice),
+              "copy stitch map");
+  std::vector<float2> t = make_tw2 (lin);
+  B200_CHECK (ctx, tw_lin.reserve (lin), "cudaMalloc twiddles");
+  B200_CHECK (ctx, cudaMemcpy (tw_lin.ptr, t.data (), lin * sizeof (float2),
+                               cudaMemcpyHostToDevice), "copy twiddles");
+  t = make_tw4 (n1, n2);
+  B200_CHECK (ctx, tw4.reserve (lout), "cudaMalloc four-step twiddles");
+  B200_CHECK (ctx, cudaMemcpy (tw4.ptr, t.data (), lout * sizeof (float2),
+                               cudaMemcpyHostToDevice), "copy four-step twiddles");
+  const unsigned ntab = pass_tables_count (n2);
+  t.assign (ntab, make_float2 (0.f, 0.f));
+  make_pass_tables (n2, t.data (), ntab);
+  B200_CHECK (ctx, ptab.reserve (ntab), "cudaMalloc pass tables");
+  B200_CHECK (ctx, cudaMemcpy (ptab.ptr, t.data (), ntab * sizeof (float2),
+                               cudaMemcpyHostToDevice), "copy pass tables");
+  B200_CHECK (ctx, err.reserve (1), "cudaMalloc status flag");
+  B200_CHECK (ctx, cudaMemset (err.ptr, 0, sizeof (int)), "clear status flag");
+  int dev = 0;
+  B200_CHECK (ctx, cudaGetDevice (&dev), "cudaGetDevice");
+  B200_CHECK (ctx, cudaDeviceGetAttribute (&nsm, cudaDevAttrMultiProcessorCount, dev),
+              "multiprocessor count");
+  const uint64_t per_part = uint64_t (nout) * cfg.npol * lout * sizeof (float2);
+  const uint64_t budget = cfg.scratch_bytes ? cfg.scratch_bytes : (uint64_t (96) << 20);
+  max_batch = unsigned (std::max<uint64_t> (1, std::min<uint64_t> (65535, budget / per_part)));
+  B200_CHECK (ctx, scratch.reserve (size_t (max_batch) * nout * cfg.npol * lout),
+              "cudaMalloc scratch");
+  return DSPSR_B200_OK;
+}
+
+extern "C" {
+
+int dspsr_b200_inverse_filterbank_create (dspsr_b200_context* ctx,
+                                          const dspsr_b200_ifb_config* cfg,
+                                          dspsr_b200_inverse_filterbank** out)
+{
+  if (!ctx || !cfg || !out) return DSPSR_B200_EINVAL;
+  *out = nullptr;
+  dspsr_b200_inverse_filterbank* f = new (std::nothrow) dspsr_b200_inverse_filterbank;
+  if (!f) return fail (ctx, DSPSR_B200_ENOMEM, "inverse filterbank: out of host memory");
+  const int rc = f->init (ctx, *cfg);
+  if (rc)
+  {
+    f->release ();
+    delete f;
+    return rc;
+  }
+  *out = f;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_inverse_filterbank_destroy (dspsr_b200_inverse_filterbank* f)
+{
+  if (!f) return DSPSR_B200_EINVAL;
+  cudaStreamSynchronize (f->ctx->stream);
+  f->release ();
+  delete f;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_inverse_filterbank_info (dspsr_b200_inverse_filterbank* f, uint64_t* info)
+{
+  if (!f || !info) return DSPSR_B200_EINVAL;
+  const IfbShape& s = f->shape;
+  const uint64_t v[10] = {s.keep, s.lout, s.in_step, s.out_step, f->in_discard_pos,
+                          f->in_discard_neg, s.n1, s.n2, f->max_batch, s.lin};
+  for (int i = 0; i < 10; i++) info[i] = v[i];
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_inverse_filterbank_copy_response (dspsr_b200_inverse_filterbank* f,
+                                                 const float* response)
+{
+  if (!f) return DSPSR_B200_EINVAL;
+  if (!response)
+  {
+    f->have_response = false;
+    return DSPSR_B200_OK;
+  }
+  const size_t n = size_t (f->shape.nout) * f->shape.lout;
+  B200_CHECK (f->ctx, f->response.reserve (n), "cudaMalloc response");
+  B200_CHECK (f->ctx, cudaMemcpy (f->response.ptr, response, n * sizeof (float2),
+                                  cudaMemcpyHostToDevice), "copy response");
+  f->have_response = true;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_inverse_filterbank_set_apodization (dspsr_b200_inverse_filterbank* f,
+                                                   const float* temporal, const float* spectral)
+{
+  if (!f) return DSPSR_B200_EINVAL;
+  f->have_temporal = f->have_spectral = false;
+  if (temporal)
+  {
+    B200_CHECK (f->ctx, f->temporal.reserve (f->shape.lin), "cudaMalloc temporal window");
+    B200_CHECK (f->ctx, cudaMemcpy (f->temporal.ptr, temporal, f->shape.lin * sizeof (float),
+                                    cudaMemcpyHostToDevice), "copy temporal window");
+    f->have_temporal = true;
+  }
+  if (spectral)
+  {
+    B200_CHECK (f->ctx, f->spectral.reserve (f->shape.lout), "cudaMalloc spectral window");
+    B200_CHECK (f->ctx, cudaMemcpy (f->spectral.ptr, spectral, f->shape.lout * sizeof (float),
+                                    cudaMemcpyHostToDevice), "copy spectral window");
+    f->have_spectral = true;
+  }
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_inverse_filterbank_perform (dspsr_b200_inverse_filterbank* f, int input_kind,
+                                           const void* d_in, uint64_t ndat, uint64_t in_span,
+                                           const float* lut256, int offset_binary, float* d_out,
+                                           uint64_t out_span, uint64_t* npart_out)
+{
+  if (!f) return DSPSR_B200_EINVAL;
+  dspsr_b200_context* ctx = f->ctx;
+  if (npart_out) *npart_out = 0;
+  if (!d_in || !d_out) return fail (ctx, DSPSR_B200_EINVAL, "inverse filterbank: null buffer");
+  if (input_kind < 0 || input_kind > 2 || (input_kind == DSPSR_B200_INT8_TFPD && !lut256))
+    return fail (ctx, DSPSR_B200_EINVAL, "inverse filterbank: invalid input kind or missing table");
+  if (input_kind == DSPSR_B200_FLOAT_FPT && in_span < ndat)
+    return fail (ctx, DSPSR_B200_EINVAL, "inverse filterbank: in_span < ndat");
+  const IfbShape& s = f->shape;
+  const uint64_t disc = uint64_t (f->in_discard_pos) + f->in_discard_neg;
+  // InverseFilterbank::resize_output (InverseFilterbank.C:599-634)
+  const uint64_t npart = ndat > disc ? (ndat - disc) / s.in_step : 0;
+  if (npart && npart * s.in_step + disc > ndat) return fail (ctx, DSPSR_B200_EINVAL, "bad npart");
+  if (out_span < npart * s.out_step)
+    return fail (ctx, DSPSR_B200_EINVAL, "inverse filterbank: out_span < npart * out_step");
+  if (input_kind == DSPSR_B200_INT8_TFPD)
+    B200_CHECK (ctx, cudaMemcpyAsync (ctx->d_lut, lut256, 256 * sizeof (float),
+                                      cudaMemcpyHostToDevice, ctx->stream), "upload lut");
+  InputView in {};
+  in.kind = input_kind;
+  in.main = d_in;
+  in.main_span = in_span;
+  in.nchan = s.nin;
+  in.npol = s.npol;
+  in.offset_binary = offset_binary;
+  VoltView vv {reinterpret_cast<float2*> (d_out), out_span};
+  const IfbTables tb = f->tables ();
+  for (uint64_t p0 = 0; p0 < npart; p0 += f->max_batch)
+  {
+    const unsigned nb = unsigned (std::min<uint64_t> (f->max_batch, npart - p0));
+    B200_CHECK (ctx, launch_inverse_filterbank (s, tb, in, p0, nb, f->scratch.ptr, vv,
+                                                ctx->stream), "inverse filterbank kernels");
+  }
+  if (npart_out) *npart_out = npart;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_inverse_filterbank_status (dspsr_b200_inverse_filterbank* f)
+{
+  if (!f) return DSPSR_B200_EINVAL;
+  int h = 0;
+  B200_CHECK (f->ctx, cudaMemcpyAsync (&h, f->err.ptr, sizeof (int), cudaMemcpyDeviceToHost,
+                                       f->ctx->stream), "read device status");
+  B200_CHECK (f->ctx, cudaStreamSynchronize (f->ctx->stream), "device status sync");
+  if (h) return fail (f->ctx, DSPSR_B200_ESTATE, "a device-side wait timed out");
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_apodization (int type, unsigned ndat, unsigned transition_start,
+                            unsigned transition_end, int swap_halves, float* window)
+{
+  if (!window) return DSPSR_B200_EINVAL;
+  return apodization (type, ndat, transition_start, transition_end, swap_halves != 0, window)
+             ? DSPSR_B200_EINVAL : DSPSR_B200_OK;
+}
+
+} // extern "C"
+
 extern "C" {
 
 int dspsr_b200_version (void) { return 100; }

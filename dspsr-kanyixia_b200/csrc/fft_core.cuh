@@ -130,6 +130,103 @@ struct RegDFT<1, D>
   B200_HD static void run (float2*) {}
 };
 
+// cos(2 pi j / 96) for j = 0..24 (decimal expansions to 22 digits), for the
+// twiddles of transforms whose length has a factor 3.
+B200_CE float quarter_cos96 (int j)
+{
+  return j == 0 ? 1.0f
+       : j == 1 ? 0.9978589232386035067380f
+       : j == 2 ? 0.9914448613738104111445f
+       : j == 3 ? 0.9807852804032304491261f
+       : j == 4 ? 0.9659258262890682867497f
+       : j == 5 ? 0.9469301294951056642558f
+       : j == 6 ? 0.9238795325112867561281f
+       : j == 7 ? 0.8968727415326883038941f
+       : j == 8 ? 0.8660254037844386467637f
+       : j == 9 ? 0.8314696123025452370787f
+       : j == 10 ? 0.7933533402912351645797f
+       : j == 11 ? 0.7518398074789773964075f
+       : j == 12 ? 0.7071067811865475244008f
+       : j == 13 ? 0.6593458151000688684251f
+       : j == 14 ? 0.6087614290087206394160f
+       : j == 15 ? 0.5555702330196022247428f
+       : j == 16 ? 0.5f
+       : j == 17 ? 0.4422886902190012819952f
+       : j == 18 ? 0.3826834323650897717284f
+       : j == 19 ? 0.3214394653031615807010f
+       : j == 20 ? 0.2588190451025207623488f
+       : j == 21 ? 0.1950903220161282678482f
+       : j == 22 ? 0.1305261922200515915484f
+       : j == 23 ? 0.0654031292301430668153f
+       : 0.0f;
+}
+
+B200_CE float cos96 (int j)
+{
+  const int m = ((j % 96) + 96) % 96;
+  return m <= 24 ? quarter_cos96 (m)
+       : m <= 48 ? -quarter_cos96 (48 - m)
+       : m <= 72 ? -quarter_cos96 (m - 48)
+       : quarter_cos96 (96 - m);
+}
+B200_CE float sin96 (int j) { return cos96 (j - 24); }
+
+// v * w_R^k, w_R = exp(D 2 pi i / R), for R dividing 96
+template <int R, int D>
+B200_HD float2 tw_mul96 (int k, float2 v)
+{
+  const int j = (k * (96 / R)) % 96;
+  if (j == 0) return v;
+  if (j == 24) return D < 0 ? make_float2 (v.y, -v.x) : make_float2 (-v.y, v.x);
+  if (j == 48) return make_float2 (-v.x, -v.y);
+  if (j == 72) return D < 0 ? make_float2 (-v.y, v.x) : make_float2 (v.y, -v.x);
+  const float c = cos96 (j);
+  const float s = D < 0 ? -sin96 (j) : sin96 (j);
+  return make_float2 (v.x * c - v.y * s, v.x * s + v.y * c);
+}
+
+// In-register DFT of size R = 2^a or 3 * 2^a (R <= 96), natural order in and
+// out.  A factor 3 is split off first (decimation in time: three interleaved
+// sub-sequences of length R/3, twiddled, then 3-point butterflies); powers of
+// two go to RegDFT.
+template <int R, int D>
+struct RegDFTm
+{
+  B200_HD static void run (float2* v)
+  {
+    if constexpr (R % 3 != 0)
+      RegDFT<R, D>::run (v);
+    else
+    {
+      constexpr int M = R / 3;
+      float2 e[3][M];
+#pragma unroll
+      for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int m = 0; m < M; m++) e[r][m] = v[3 * m + r];
+#pragma unroll
+      for (int r = 0; r < 3; r++) RegDFT<M, D>::run (e[r]);
+      // sin(2 pi / 3)
+      const float h = 0.8660254037844386467637f;
+#pragma unroll
+      for (int k = 0; k < M; k++)
+      {
+        const float2 a = e[0][k];
+        const float2 b = tw_mul96<R, D> (k, e[1][k]);
+        const float2 c = tw_mul96<R, D> (2 * k, e[2][k]);
+        const float2 s = cadd (b, c);
+        const float2 d = csub (b, c);
+        const float2 m = make_float2 (a.x - 0.5f * s.x, a.y - 0.5f * s.y);
+        // D * i * h * d
+        const float2 r = D < 0 ? make_float2 (h * d.y, -h * d.x) : make_float2 (-h * d.y, h * d.x);
+        v[k] = cadd (a, s);
+        v[k + M] = cadd (m, r);
+        v[k + 2 * M] = csub (m, r);
+      }
+    }
+  }
+};
+
 // Shared-memory index padding: one float2 of padding per 16 entries keeps the
 // strided Stockham stores of the early passes off a single bank.
 B200_HD int spad (int i) { return i + (i >> 4); }
@@ -147,6 +244,8 @@ B200_CE int stockham_radix (int N, int p)
        : N == 1024 ? (p < 2 ? 16 : p == 2 ? 4 : 0)
        : N == 512 ? (p < 2 ? 16 : p == 2 ? 2 : 0)
        : N == 256 ? (p < 2 ? 16 : 0)
+       : N == 128 ? (p < 1 ? 16 : p == 1 ? 8 : 0)
+       : N == 64 ? (p < 1 ? 16 : p == 1 ? 4 : 0)
        : 0;
 }
 

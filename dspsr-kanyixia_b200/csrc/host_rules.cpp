@@ -8,6 +8,7 @@
 
 #include "host_rules.h"
 
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdint>
@@ -139,6 +140,84 @@ double fold_phi (int64_t start_day, int64_t start_sec, double start_frac,
   const double seconds = double ((day - epoch_day) * 86400 + (sec - epoch_sec))
                          + (frac - epoch_frac);
   return std::fmod (seconds, period) / period - reference_phase;
+}
+
+// InverseFilterbankEngineCPU::build_fine_channel_plan (InverseFilterbankEngineCPU.C:378-425):
+// when one output channel combines several coarse channels, the input channel
+// that lands at stitched position i.  The stitched order rolls the band by half
+// a coarse channel, swaps the two halves of the band and the two halves of
+// every coarse channel; the plan is the inverse of that re-ordering.
+std::vector<unsigned> ifb_fine_channel_plan (unsigned nchan, unsigned per_coarse)
+{
+  std::vector<unsigned> order (nchan);
+  for (unsigned i = 0; i < nchan; i++) order[i] = (i + nchan - per_coarse / 2) % nchan;
+  std::vector<unsigned> tmp (order);
+  for (unsigned i = 0; i < nchan; i++) order[i] = tmp[(i + nchan / 2) % nchan];
+  for (unsigned start = 0; start < nchan; start += per_coarse)
+    for (unsigned i = 0; i < per_coarse / 2; i++)
+      std::swap (order[start + i], order[start + i + per_coarse / 2]);
+  std::vector<unsigned> plan (nchan);
+  for (unsigned i = 0; i < nchan; i++) plan[order[i]] = i;
+  return plan;
+}
+
+// Apodization::build (Apodization.C:60-146) and swap (:168-178); the
+// arithmetic keeps the reference's float and double steps.
+int apodization (int type, unsigned ndat, unsigned t_start, unsigned t_end, bool swap,
+                 float* w)
+{
+  if (ndat == 0) return -1;
+  switch (type)
+  {
+    case 0:   // top hat
+      for (unsigned i = 0; i < ndat; i++) w[i] = 1.0f;
+      break;
+    case 1:   // Hanning
+    {
+      const double denom = ndat - 1.0;
+      for (unsigned i = 0; i < ndat; i++)
+        w[i] = float (0.5 * (1 - std::cos (2.0 * M_PI * double (i) / denom)));
+      break;
+    }
+    case 2:   // Welch
+    {
+      const float centre = 0.5 * (ndat - 1);
+      const float denominator = 0.5 * (ndat + 1);
+      for (unsigned i = 0; i < ndat; i++)
+      {
+        const float q = (float (i) - centre) / denominator;
+        w[i] = float (1.0 - q * q);
+      }
+      break;
+    }
+    case 3:   // Bartlett
+    {
+      const float centre = 0.5 * (ndat - 1);
+      const float denominator = 0.5 * (ndat - 1);
+      for (unsigned i = 0; i < ndat; i++)
+        w[i] = float (1.0 - std::fabs ((float (i) - centre) / denominator));
+      break;
+    }
+    case 4:   // Tukey
+    {
+      const float ds = 2 * t_start, de = 2 * t_end;
+      for (unsigned i = 0; i < ndat; i++)
+      {
+        if (i < t_start)
+          w[i] = float (0.5 * (1 - std::cos (2.0 * M_PI * float (i) / ds)));
+        else if (i + 1 > ndat - t_end)
+          w[i] = float (0.5 * (1 - std::cos (2.0 * M_PI * float (ndat - i - 1) / de)));
+        else
+          w[i] = 1.0f;
+      }
+      break;
+    }
+    default:
+      return -1;
+  }
+  if (swap)
+    for (unsigned i = 0; i < ndat / 2; i++) std::swap (w[i], w[i + ndat / 2]);
+  return 0;
 }
 
 // ---------------------------------------------------------------------------

@@ -32,6 +32,12 @@ double fold_phi (int64_t start_day, int64_t start_sec, double start_frac,
 // invalid arguments, -2 where a Pearson type I density would be needed.
 int sk_limits (unsigned M, unsigned Nd, float std_devs, unsigned ntest, float* lower,
                float* upper);
+// InverseFilterbank fine-channel plan for combined coarse channels
+std::vector<unsigned> ifb_fine_channel_plan (unsigned nchan, unsigned per_coarse);
+// Apodization::build: type 0 top hat, 1 Hanning, 2 Welch, 3 Bartlett, 4 Tukey
+// (transitions t_start, t_end); swap exchanges the halves.  0 on success.
+int apodization (int type, unsigned ndat, unsigned t_start, unsigned t_end, bool swap,
+                 float* window);
 // Returns the number of segments; fills *out when non-null.
 int64_t build_fold_plan (double phi, double phase_per_sample, uint64_t ndat,
                          std::vector<FoldSegment>* out);

@@ -401,7 +401,9 @@ __device__ __forceinline__ void tpass (const float2* src, float2* dst, float2* v
   }
 }
 
-template <int N2>
+// CONV: the convolution row (forward FFT, x H, inverse FFT).  Otherwise the
+// inverse FFT of the row alone (the inverse filterbank's stitched spectra).
+template <int N2, bool CONV>
 __global__ void __launch_bounds__ (stockham_threads (N2), 1)
 k_rows_tma (float2* __restrict__ scratch, const float2* __restrict__ ptab,
             const float2* __restrict__ H, const unsigned n1, const unsigned nchan,
@@ -447,11 +449,12 @@ k_rows_tma (float2* __restrict__ scratch, const float2* __restrict__ ptab,
     const unsigned c = (row / n1 / npol) % nchan;
     float2* grow = scratch + uint64_t (row) * N2;
 
-    // forward pass 0 reads the staged row; once every thread has its values
-    // the staging buffer is refilled with the next row in the background
+    // pass 0 reads the staged row; once every thread has its values the
+    // staging buffer is refilled with the next row in the background
     {
       constexpr int R0 = stockham_radix (N2, 0);
-      StockhamPassT<N2, R0, T, -1, false, true>::load (tid, stage, v);
+      constexpr int D0 = CONV ? -1 : +1;
+      StockhamPassT<N2, R0, T, D0, false, true>::load (tid, stage, v);
       __syncthreads ();
       const unsigned next = row + gridDim.x;
       if (tid == 0 && next < nrows)
@@ -461,27 +464,30 @@ k_rows_tma (float2* __restrict__ scratch, const float2* __restrict__ ptab,
         for (unsigned o = 0; o < ROW_BYTES; o += CHUNK)
           bulk_g2s (reinterpret_cast<char*> (stage) + o, src + o, CHUNK, &bar);
       }
-      StockhamPassT<N2, R0, T, -1, false, true>::compute_store (tid, 1, v, work, nullptr);
+      StockhamPassT<N2, R0, T, D0, false, true>::compute_store (tid, 1, v, work, nullptr);
       __syncthreads ();
     }
-    tpass<N2, -1, 1, true, true> (work, work, v, tab);
-    tpass<N2, -1, 2, true, true> (work, work, v, tab);
-    tpass<N2, -1, 3, true, true> (work, work, v, tab);
-
-    // Response::operate (Response.C:662-726): (f_r d_r - f_i d_i, f_i d_r + f_r d_i)
-    const float2* h = H + (uint64_t (c) * n1 + k1) * N2;
-#pragma unroll
-    for (int q = 0; q < 16; q++)
+    if constexpr (CONV)
     {
-      const int i = tid + q * T;
-      const float2 d = work[spad (i)];
-      const float2 f = __ldg (h + i);
-      work[spad (i)] = make_float2 (d.x * f.x - d.y * f.y, d.x * f.y + d.y * f.x);
+      tpass<N2, -1, 1, true, true> (work, work, v, tab);
+      tpass<N2, -1, 2, true, true> (work, work, v, tab);
+      tpass<N2, -1, 3, true, true> (work, work, v, tab);
+
+      // Response::operate (Response.C:662-726): (f_r d_r - f_i d_i, f_i d_r + f_r d_i)
+      const float2* h = H + (uint64_t (c) * n1 + k1) * N2;
+#pragma unroll
+      for (int q = 0; q < 16; q++)
+      {
+        const int i = tid + q * T;
+        const float2 d = work[spad (i)];
+        const float2 f = __ldg (h + i);
+        work[spad (i)] = make_float2 (d.x * f.x - d.y * f.y, d.x * f.y + d.y * f.x);
+      }
+      __syncthreads ();
+      tpass<N2, +1, 0, true, true> (work, work, v, tab);
     }
-    __syncthreads ();
 
     // inverse: all but the last pass in shared memory, the last straight to HBM
-    tpass<N2, +1, 0, true, true> (work, work, v, tab);
     tpass<N2, +1, 1, true, true> (work, work, v, tab);
     if constexpr (NP == 3)
       tpass<N2, +1, 2, true, false> (work, grow, v, tab);
@@ -602,6 +608,103 @@ k_fused (const InputView in, const float* __restrict__ lut, const float2* __rest
     }
     else
       emit_fold<NOUT> (fv, c, npol, ok, tbase + j, pv, qv);
+  }
+}
+
+// --------------------------------------------------------------------------
+// inverse filterbank (InverseFilterbankEngineCPU.C:309-779 restructured)
+// --------------------------------------------------------------------------
+
+// One CTA per (fine channel, pol, part): unpack on load and temporal window
+// (Apodization::operate), lin-point forward FFT in shared memory, then the
+// kept bins of both halves -- stitch_one's placement, precomputed per channel
+// on the host -- times the response and the spectral window, written into the
+// output channel's spectrum in four-step order (bin k at row k mod n1,
+// column k div n1) for the row kernel.
+template <int LIN, int KIND>
+__global__ void __launch_bounds__ (stockham_threads (LIN))
+k_ifb_stitch (const InputView in, const IfbShape sh, const IfbTables tb, const uint64_t part0,
+              float2* __restrict__ scratch)
+{
+  constexpr int T = stockham_threads (LIN);
+  __shared__ float2 s[spad_size (LIN)];
+  __shared__ float s_lut[256];
+  const unsigned jch = blockIdx.x, p = blockIdx.y, b = blockIdx.z;
+  load_lut (in, tb.lut, s_lut);
+  __syncthreads ();
+  const uint64_t t0 = (part0 + b) * sh.in_step;
+  for (int i = threadIdx.x; i < LIN; i += T)
+  {
+    float2 x = fetch<KIND> (in, s_lut, jch, p, t0 + i);
+    if (tb.temporal)
+    {
+      const float w = __ldg (tb.temporal + i);
+      x = make_float2 (__fmul_rn (x.x, w), __fmul_rn (x.y, w));
+    }
+    s[spad (i)] = x;
+  }
+  __syncthreads ();
+  smem_fft<LIN, T, -1> (s, tb.tw_lin);
+  const int4 m = __ldg (tb.map + jch);
+  const unsigned keep2 = sh.keep / 2;
+  const unsigned skip2 = (LIN - sh.keep) / 2;
+  const unsigned src_neg = sh.dual_sideband ? LIN - keep2 : skip2;
+  const unsigned src_pos = sh.dual_sideband ? 0 : skip2 + keep2;
+  for (unsigned i = threadIdx.x; i < sh.keep; i += T)
+  {
+    const bool neg = i < keep2;
+    const unsigned j = neg ? i : i - keep2;
+    const int o = neg ? m.x : m.z;
+    const int off = neg ? m.y : m.w;
+    const unsigned k = unsigned (off & (IFB_ZERO - 1)) + j;
+    float2 y = (off & IFB_ZERO) ? make_float2 (0.f, 0.f) : s[spad ((neg ? src_neg : src_pos) + j)];
+    if (tb.response)
+    {
+      // Response::operate: (f_r d_r - f_i d_i, f_i d_r + f_r d_i)
+      const float2 f = __ldg (tb.response + uint64_t (o) * sh.lout + k);
+      y = make_float2 (__fsub_rn (__fmul_rn (f.x, y.x), __fmul_rn (f.y, y.y)),
+                       __fadd_rn (__fmul_rn (f.y, y.x), __fmul_rn (f.x, y.y)));
+    }
+    if (tb.spectral)
+    {
+      const float w = __ldg (tb.spectral + k);
+      y = make_float2 (__fmul_rn (y.x, w), __fmul_rn (y.y, w));
+    }
+    float2* dst = scratch + ((uint64_t (b) * sh.nout + o) * sh.npol + p) * sh.lout;
+    dst[uint64_t (k % sh.n1) * sh.n2 + k / sh.n1] = y;
+  }
+}
+
+// Inverse column DFTs of the lout-point transforms (after the row kernel):
+// conjugate four-step twiddle, n1-point inverse DFT in registers (n1 may
+// carry a factor 3), output discard, voltages out.  Pols one after another.
+template <int N1>
+__global__ void __launch_bounds__ (128)
+k_ifb_cols (const float2* __restrict__ scratch, const IfbShape sh, const float2* __restrict__ tw4,
+            const uint64_t part0, const VoltView vv)
+{
+  const unsigned i2 = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned b = blockIdx.y;
+  const unsigned o = blockIdx.z;
+  const uint64_t N = uint64_t (N1) * sh.n2;
+  const uint64_t tbase = (part0 + b) * sh.out_step;
+  for (unsigned p = 0; p < sh.npol; p++)
+  {
+    const float2* src = scratch + ((uint64_t (b) * sh.nout + o) * sh.npol + p) * N + i2;
+    float2 v[N1];
+#pragma unroll
+    for (int k = 0; k < N1; k++) v[k] = src[uint64_t (k) * sh.n2];
+#pragma unroll
+    for (int k = 1; k < N1; k++) v[k] = cmulc (v[k], __ldg (tw4 + uint64_t (k) * sh.n2 + i2));
+    RegDFTm<N1, +1>::run (v);
+    float2* dst = vv.out + (uint64_t (o) * sh.npol + p) * vv.span + tbase;
+#pragma unroll
+    for (int k = 0; k < N1; k++)
+    {
+      const uint64_t tl = uint64_t (k) * sh.n2 + i2;
+      if (tl >= sh.out_discard_pos && tl < sh.out_discard_pos + sh.out_step)
+        dst[tl - sh.out_discard_pos] = v[k];
+    }
   }
 }
 
@@ -970,8 +1073,8 @@ void launch_rows (unsigned nrows, float2* scratch, const ConvTables& tb, unsigne
   // n2 = 8192 and 2 at n2 = 4096)
   const unsigned per_sm = N2 >= 8192 ? 1 : 2;
   const unsigned grid = std::min<unsigned> (nrows, per_sm * unsigned (tb.nsm));
-  k_rows_tma<N2><<<grid, T, rows_smem_bytes<N2> (), st>>> (scratch, tb.ptab, tb.H, n1, sh.nchan,
-                                                           sh.npol, nrows, tb.err);
+  k_rows_tma<N2, true><<<grid, T, rows_smem_bytes<N2> (), st>>> (scratch, tb.ptab, tb.H, n1,
+                                                                 sh.nchan, sh.npol, nrows, tb.err);
 }
 
 template <int N1>
@@ -1068,10 +1171,49 @@ cudaError_t run_fused (const ConvShape& sh, const ConvTables& tb, const InputVie
   return run_fused_k<N, IN_FLOAT> (sh, tb, in, part0, nbatch, mode, fv, vv, st, clk);
 }
 
+template <int LIN, int KIND>
+void launch_ifb_stitch (const IfbShape& sh, const IfbTables& tb, const InputView& in,
+                        uint64_t part0, unsigned nbatch, float2* scratch, cudaStream_t st)
+{
+  k_ifb_stitch<LIN, KIND><<<dim3 (sh.nin, sh.npol, nbatch), stockham_threads (LIN), 0, st>>> (
+      in, sh, tb, part0, scratch);
+}
+
+template <int LIN>
+void launch_ifb_stitch_k (const IfbShape& sh, const IfbTables& tb, const InputView& in,
+                          uint64_t part0, unsigned nbatch, float2* scratch, cudaStream_t st)
+{
+  if (in.kind == IN_INT8)
+    launch_ifb_stitch<LIN, IN_INT8> (sh, tb, in, part0, nbatch, scratch, st);
+  else if (in.kind == IN_INT16)
+    launch_ifb_stitch<LIN, IN_INT16> (sh, tb, in, part0, nbatch, scratch, st);
+  else
+    launch_ifb_stitch<LIN, IN_FLOAT> (sh, tb, in, part0, nbatch, scratch, st);
+}
+
+template <int N1>
+void launch_ifb_cols (const IfbShape& sh, const IfbTables& tb, uint64_t part0, unsigned nbatch,
+                      const float2* scratch, const VoltView& vv, cudaStream_t st)
+{
+  k_ifb_cols<N1><<<dim3 (sh.n2 / 128, nbatch, sh.nout), 128, 0, st>>> (scratch, sh, tb.tw4, part0,
+                                                                       vv);
+}
+
 template <int N2>
+void launch_rows_inv (unsigned nrows, float2* scratch, const IfbTables& tb, unsigned n1,
+                      unsigned npol, cudaStream_t st)
+{
+  constexpr int T = stockham_threads (N2);
+  const unsigned per_sm = N2 >= 8192 ? 1 : 2;
+  const unsigned grid = std::min<unsigned> (nrows, per_sm * unsigned (tb.nsm));
+  k_rows_tma<N2, false><<<grid, T, rows_smem_bytes<N2> (), st>>> (scratch, tb.ptab, nullptr, n1,
+                                                                  1, npol, nrows, tb.err);
+}
+
+template <int N2, bool CONV = true>
 cudaError_t set_rows_smem ()
 {
-  return cudaFuncSetAttribute (k_rows_tma<N2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  return cudaFuncSetAttribute (k_rows_tma<N2, CONV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                int (rows_smem_bytes<N2> ()));
 }
 
@@ -1143,6 +1285,68 @@ cudaError_t launch_convolution (const ConvShape& sh, const ConvTables& tb, const
     case 32: return run_fourstep_n1<32> (sh, tb, in, part0, nbatch, scratch, mode, fv, vv, st, clk);
     default: return cudaErrorInvalidValue;
   }
+}
+
+bool ifb_supported_lin (unsigned lin)
+{
+  return lin == 64 || lin == 128 || lin == 256 || lin == 512 || lin == 1024 || lin == 2048 ||
+         lin == 4096;
+}
+
+cudaError_t launch_inverse_filterbank (const IfbShape& sh, const IfbTables& tb,
+                                       const InputView& in, uint64_t part0, unsigned nbatch,
+                                       float2* scratch, const VoltView& vv, cudaStream_t st,
+                                       const KernelClock* clk)
+{
+  if (nbatch == 0) return cudaSuccess;
+  if (sh.n2 != 8192 && sh.n2 != 4096) return cudaErrorInvalidValue;
+  static unsigned attr_done = 0;
+  int dev = 0;
+  cudaGetDevice (&dev);
+  if (dev < 32 && !(attr_done & (1u << dev)))
+  {
+    cudaError_t e = set_rows_smem<8192, false> ();
+    if (e == cudaSuccess) e = set_rows_smem<4096, false> ();
+    if (e != cudaSuccess) return e;
+    attr_done |= 1u << dev;
+  }
+  {
+    ClockScope cs (clk, KK_FWD_COLS, st);
+    switch (sh.lin)
+    {
+      case 64: launch_ifb_stitch_k<64> (sh, tb, in, part0, nbatch, scratch, st); break;
+      case 128: launch_ifb_stitch_k<128> (sh, tb, in, part0, nbatch, scratch, st); break;
+      case 256: launch_ifb_stitch_k<256> (sh, tb, in, part0, nbatch, scratch, st); break;
+      case 512: launch_ifb_stitch_k<512> (sh, tb, in, part0, nbatch, scratch, st); break;
+      case 1024: launch_ifb_stitch_k<1024> (sh, tb, in, part0, nbatch, scratch, st); break;
+      case 2048: launch_ifb_stitch_k<2048> (sh, tb, in, part0, nbatch, scratch, st); break;
+      case 4096: launch_ifb_stitch_k<4096> (sh, tb, in, part0, nbatch, scratch, st); break;
+      default: return cudaErrorInvalidValue;
+    }
+  }
+  const unsigned nrows = sh.n1 * nbatch * sh.nout * sh.npol;
+  {
+    ClockScope cs (clk, KK_ROWS, st);
+    if (sh.n2 == 8192)
+      launch_rows_inv<8192> (nrows, scratch, tb, sh.n1, sh.npol, st);
+    else
+      launch_rows_inv<4096> (nrows, scratch, tb, sh.n1, sh.npol, st);
+  }
+  ClockScope cs (clk, KK_INV_COLS, st);
+  switch (sh.n1)
+  {
+    case 2: launch_ifb_cols<2> (sh, tb, part0, nbatch, scratch, vv, st); break;
+    case 3: launch_ifb_cols<3> (sh, tb, part0, nbatch, scratch, vv, st); break;
+    case 4: launch_ifb_cols<4> (sh, tb, part0, nbatch, scratch, vv, st); break;
+    case 6: launch_ifb_cols<6> (sh, tb, part0, nbatch, scratch, vv, st); break;
+    case 8: launch_ifb_cols<8> (sh, tb, part0, nbatch, scratch, vv, st); break;
+    case 12: launch_ifb_cols<12> (sh, tb, part0, nbatch, scratch, vv, st); break;
+    case 16: launch_ifb_cols<16> (sh, tb, part0, nbatch, scratch, vv, st); break;
+    case 24: launch_ifb_cols<24> (sh, tb, part0, nbatch, scratch, vv, st); break;
+    case 32: launch_ifb_cols<32> (sh, tb, part0, nbatch, scratch, vv, st); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError ();
 }
 
 cudaError_t launch_build_chirp (float2* H, const double* d_chan_freq, const double* d_coeff,

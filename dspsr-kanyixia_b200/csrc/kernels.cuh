@@ -115,6 +115,45 @@ cudaError_t launch_filterbank (const InputView& in, const float* d_lut, unsigned
                                uint64_t nblk, float scale, float2* out, uint64_t out_span,
                                cudaStream_t stream, const KernelClock* clock = nullptr);
 
+// InverseFilterbank: per part, forward FFT of lin samples of every fine
+// channel, the kept bins stitched into the spectra of the output channels
+// (lout = n1 * n2 bins each, n2 in {4096, 8192}), times the response and the
+// spectral window, then the inverse lout-point FFT with the output discard.
+struct IfbShape
+{
+  unsigned nin, nout, npol;
+  unsigned lin, keep, lout, n1, n2;
+  uint64_t in_step, out_step;
+  unsigned out_discard_pos;
+  int dual_sideband;
+};
+
+struct IfbTables
+{
+  // per input channel: (output channel of the negative half, its first bin,
+  // output channel of the positive half, its first bin); bit 30 of a first
+  // bin marks a half that is zeroed instead
+  const int4* map;
+  const float2* tw_lin;      // lin-point table exp(-2 pi i m / lin)
+  const float2* tw4;         // [n1][n2] four-step table of the lout-point transform
+  const float2* ptab;        // per-pass tables of the n2-point row transform
+  const float2* response;    // [nout][lout] or null
+  const float* temporal;     // [lin] or null
+  const float* spectral;     // [lout] or null
+  const float* lut;          // 8-bit table for int8 input
+  int* err;
+  int nsm;
+};
+
+constexpr int IFB_ZERO = 1 << 30;
+
+// Parts [part0, part0 + nbatch); scratch holds nbatch*nout*npol*lout values.
+cudaError_t launch_inverse_filterbank (const IfbShape& shape, const IfbTables& tables,
+                                       const InputView& in, uint64_t part0, unsigned nbatch,
+                                       float2* scratch, const VoltView& out, cudaStream_t stream,
+                                       const KernelClock* clock = nullptr);
+bool ifb_supported_lin (unsigned lin);
+
 // SpectralKurtosis (one resolution, noverlap 1): statistics, test and masked
 // copy (out may equal in: then only zapped blocks are written).  sums
 // [npart][nchan][npol][2], counts and mask [npart][nchan] are optional.

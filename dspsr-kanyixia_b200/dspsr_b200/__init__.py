@@ -20,7 +20,7 @@ from . import _capi
 from ._capi import (B200Error, PipelineConfig, INTENSITY, PPQQ, COHERENCE, STOKES, INT8_TFPD,
                     INT16_TFPD, FLOAT_FPT, CHIRP_REFERENCE, CHIRP_FP64)
 
-__all__ = ["Context", "Convolution", "Fold", "Pipeline", "PipelineConfig", "B200Error",
+__all__ = ["Context", "Convolution", "InverseFilterbank", "Fold", "apodization", "Pipeline", "PipelineConfig", "B200Error",
            "smearing_samples", "minimum_ndat", "optimal_fft_length", "bittable8", "fold_phi",
            "sk_limits",
            "fold_plan_count", "INTENSITY", "PPQQ", "COHERENCE", "STOKES", "INT8_TFPD",
@@ -76,6 +76,19 @@ def sk_limits(M, Nd=1, std_devs=3.0, ntest=1):
     if rc != _capi.OK:
         raise B200Error(rc, f"sk_limits: no thresholds for M={M} Nd={Nd} std_devs={std_devs}")
     return lo[0], hi[0]
+
+
+APOD_TOPHAT, APOD_HANNING, APOD_WELCH, APOD_BARTLETT, APOD_TUKEY = range(5)
+
+
+def apodization(kind, ndat, transition_start=0, transition_end=0, swap_halves=False):
+    """Apodization::build: the float window of ndat points."""
+    w = np.zeros(ndat, np.float32)
+    rc = _capi.lib().dspsr_b200_apodization(kind, ndat, transition_start, transition_end,
+                                           int(swap_halves), _fptr(w))
+    if rc != _capi.OK:
+        raise B200Error(rc, f"apodization: invalid type {kind} or size {ndat}")
+    return w
 
 
 def fold_phi(start_mjd, epoch_mjd, idat_start, rate, period, reference_phase=0.0):
@@ -228,6 +241,77 @@ class Convolution:
     def close(self):
         if self.handle:
             self._lib.dspsr_b200_convolution_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class InverseFilterbank:
+    """InverseFilterbank::Engine: fine-channel FFTs, stitch, response, inverse FFT."""
+
+    INFO = ("keep", "lout", "in_step", "out_step", "in_discard_pos", "in_discard_neg", "n1",
+            "n2", "max_batch", "lin")
+
+    def __init__(self, ctx, input_nchan, output_nchan, pfb_nchan, npol, input_fft_length,
+                 os=(4, 3), output_discard=(0, 0), pfb_dc_chan=True, pfb_all_chan=True,
+                 dual_sideband=True, scratch_bytes=0):
+        self.ctx = ctx
+        self._lib = ctx._lib
+        cfg = _capi.IfbConfig(input_nchan, output_nchan, pfb_nchan, npol, input_fft_length,
+                              os[0], os[1], output_discard[0], output_discard[1],
+                              int(pfb_dc_chan), int(pfb_all_chan), int(dual_sideband),
+                              scratch_bytes)
+        h = ctypes.c_void_p()
+        ctx.check(self._lib.dspsr_b200_inverse_filterbank_create(ctx.handle, ctypes.byref(cfg),
+                                                                 ctypes.byref(h)),
+                  "inverse_filterbank_create")
+        self.handle = h
+        info = (ctypes.c_uint64 * 10)()
+        ctx.check(self._lib.dspsr_b200_inverse_filterbank_info(h, info), "inverse_filterbank_info")
+        self.info = dict(zip(self.INFO, list(info)))
+        self.nin, self.nout, self.npol = input_nchan, output_nchan, npol
+
+    def copy_response(self, response):
+        if response is None:
+            self.ctx.check(self._lib.dspsr_b200_inverse_filterbank_copy_response(self.handle, None),
+                           "copy_response")
+            return
+        r = np.ascontiguousarray(response, np.complex64)
+        assert r.size == self.nout * self.info["lout"]
+        self.ctx.check(self._lib.dspsr_b200_inverse_filterbank_copy_response(
+            self.handle, _fptr(r.view(np.float32))), "copy_response")
+
+    def set_apodization(self, temporal=None, spectral=None):
+        t = None if temporal is None else np.ascontiguousarray(temporal, np.float32)
+        sp = None if spectral is None else np.ascontiguousarray(spectral, np.float32)
+        self.ctx.check(self._lib.dspsr_b200_inverse_filterbank_set_apodization(
+            self.handle, None if t is None else _fptr(t), None if sp is None else _fptr(sp)),
+            "set_apodization")
+
+    def npart(self, ndat):
+        d = self.info["in_discard_pos"] + self.info["in_discard_neg"]
+        return (ndat - d) // self.info["in_step"] if ndat > d else 0
+
+    def perform(self, d_in, ndat, d_out, out_span, input_kind=FLOAT_FPT, in_span=None, lut=None,
+                offset_binary=False):
+        n = ctypes.c_uint64()
+        lp = _fptr(np.ascontiguousarray(lut, np.float32)) if lut is not None else None
+        self.ctx.check(self._lib.dspsr_b200_inverse_filterbank_perform(
+            self.handle, input_kind, _ptr(d_in), ndat, ndat if in_span is None else in_span, lp,
+            int(offset_binary), _ptr(d_out), out_span, ctypes.byref(n)),
+            "inverse_filterbank_perform")
+        return n.value
+
+    def status(self):
+        self.ctx.check(self._lib.dspsr_b200_inverse_filterbank_status(self.handle), "status")
+
+    def close(self):
+        if self.handle:
+            self._lib.dspsr_b200_inverse_filterbank_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -61,6 +61,25 @@ class PipelineConfig(ctypes.Structure):
     ]
 
 
+class IfbConfig(ctypes.Structure):
+    """dspsr_b200_ifb_config"""
+    _fields_ = [
+        ("input_nchan", c_uint),
+        ("output_nchan", c_uint),
+        ("pfb_nchan", c_uint),
+        ("npol", c_uint),
+        ("input_fft_length", c_uint),
+        ("os_num", c_uint),
+        ("os_den", c_uint),
+        ("output_discard_pos", c_uint),
+        ("output_discard_neg", c_uint),
+        ("pfb_dc_chan", c_int),
+        ("pfb_all_chan", c_int),
+        ("dual_sideband", c_int),
+        ("scratch_bytes", c_u64),
+    ]
+
+
 SIGNATURES = {
     "dspsr_b200_version": (c_int, []),
     "dspsr_b200_context_create": (c_int, [c_int, c_vp, ctypes.POINTER(c_vp)]),
@@ -96,6 +115,16 @@ SIGNATURES = {
                                       c_fp, c_int, c_vp, c_u64, c_u64p]),
     "dspsr_b200_convolution_perform": (c_int, [c_vp, c_vp, c_u64, c_u64, c_vp, c_u64, c_u64p]),
     "dspsr_b200_detect": (c_int, [c_vp, c_vp, c_u64, c_u64, c_uint, c_int, c_vp, c_u64]),
+    "dspsr_b200_inverse_filterbank_create": (c_int, [c_vp, ctypes.POINTER(IfbConfig),
+                                                     ctypes.POINTER(c_vp)]),
+    "dspsr_b200_inverse_filterbank_destroy": (c_int, [c_vp]),
+    "dspsr_b200_inverse_filterbank_info": (c_int, [c_vp, c_u64p]),
+    "dspsr_b200_inverse_filterbank_copy_response": (c_int, [c_vp, c_fp]),
+    "dspsr_b200_inverse_filterbank_set_apodization": (c_int, [c_vp, c_fp, c_fp]),
+    "dspsr_b200_inverse_filterbank_perform": (c_int, [c_vp, c_int, c_vp, c_u64, c_u64, c_fp, c_int,
+                                                      c_vp, c_u64, c_u64p]),
+    "dspsr_b200_inverse_filterbank_status": (c_int, [c_vp]),
+    "dspsr_b200_apodization": (c_int, [c_int, c_uint, c_uint, c_uint, c_int, c_fp]),
     "dspsr_b200_sk": (c_int, [c_vp, c_vp, c_u64, c_u64, c_uint, c_uint, c_uint, c_int, c_uint,
                               ctypes.c_float, ctypes.c_float, c_vp, c_u64, c_vp, c_vp, c_vp, c_vp,
                               c_u64p]),

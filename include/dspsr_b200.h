@@ -56,6 +56,7 @@ typedef struct dspsr_b200_context dspsr_b200_context;
 typedef struct dspsr_b200_convolution dspsr_b200_convolution;
 typedef struct dspsr_b200_fold dspsr_b200_fold;
 typedef struct dspsr_b200_pipeline dspsr_b200_pipeline;
+typedef struct dspsr_b200_inverse_filterbank dspsr_b200_inverse_filterbank;
 
 /* ---------------------------------------------------------------------- */
 /* Library and context                                                     */
@@ -106,6 +107,17 @@ double dspsr_b200_fold_phi (int64_t start_day, int64_t start_sec, double start_f
    (which the reference does not implement either). */
 int dspsr_b200_sk_limits (unsigned M, unsigned Nd, float std_devs, unsigned ntest,
                           float* lower, float* upper);
+/* Apodization::build (Signal/General/Apodization.C:60-146) and swap
+   (:168-178): the window of ndat points, type DSPSR_B200_APOD_*; Tukey uses
+   transition_start / transition_end.  swap_halves exchanges the two halves
+   (spectral windows of dual-sideband data). */
+#define DSPSR_B200_APOD_TOPHAT   0
+#define DSPSR_B200_APOD_HANNING  1
+#define DSPSR_B200_APOD_WELCH    2
+#define DSPSR_B200_APOD_BARTLETT 3
+#define DSPSR_B200_APOD_TUKEY    4
+int dspsr_b200_apodization (int type, unsigned ndat, unsigned transition_start,
+                            unsigned transition_end, int swap_halves, float* window);
 /* Number of arithmetic segments the exact fold-bin plan needs for a block
    (see dspsr_b200_fold_set_bins); lets a caller size buffers. */
 int64_t dspsr_b200_fold_plan_count (double phi, double phase_per_sample,
@@ -213,6 +225,65 @@ int dspsr_b200_filterbank (dspsr_b200_context* ctx, int input_kind, const void* 
                            uint64_t ndat, uint64_t in_span, unsigned nchan_in, unsigned npol,
                            unsigned nsub, const float* lut256, int offset_binary,
                            float* d_out, uint64_t out_span, uint64_t* ndat_out);
+
+/* ---------------------------------------------------------------------- */
+/* InverseFilterbank::Engine (InverseFilterbankEngineCPU.C:46-792,          */
+/* InverseFilterbankEngineCUDA.cu:58-529; caller InverseFilterbank.C:129-454) */
+/* ---------------------------------------------------------------------- */
+
+/* Shape of InverseFilterbank::make_preparations (InverseFilterbank.C:225-330):
+   input_nchan fine channels (pfb_nchan per coarse PFB channel), output_nchan
+   dividing input_nchan; each fine channel is transformed in
+   input_fft_length-point FFTs of which Lin*os_den/os_num bins are kept and
+   stitched; output FFT length Lout = (input_nchan/output_nchan) * kept bins,
+   which must be n1 * 4096 or n1 * 8192 with n1 in {2,3,4,6,8,12,16,24,32}.
+   Output discards are given (from the response); the input discards follow
+   by output_to_input (InverseFilterbank.C:128-142).  scratch_bytes bounds the
+   device scratch (0 = 96 MiB). */
+typedef struct dspsr_b200_ifb_config
+{
+  unsigned input_nchan;
+  unsigned output_nchan;
+  unsigned pfb_nchan;
+  unsigned npol;
+  unsigned input_fft_length;
+  unsigned os_num, os_den;
+  unsigned output_discard_pos, output_discard_neg;
+  int pfb_dc_chan;          /* channel 0 of the PFB is centred on DC */
+  int pfb_all_chan;         /* all PFB channels present (else the last half channel is zeroed) */
+  int dual_sideband;
+  uint64_t scratch_bytes;
+} dspsr_b200_ifb_config;
+
+/* Engine::setup (InverseFilterbankEngineCPU.C:46-278) */
+int dspsr_b200_inverse_filterbank_create (dspsr_b200_context* ctx,
+                                          const dspsr_b200_ifb_config* cfg,
+                                          dspsr_b200_inverse_filterbank** ifb);
+int dspsr_b200_inverse_filterbank_destroy (dspsr_b200_inverse_filterbank* ifb);
+/* info[10] = {kept bins, Lout, input step, output step, input discard pos,
+   input discard neg, n1, n2, parts per batch, input FFT length} */
+int dspsr_b200_inverse_filterbank_info (dspsr_b200_inverse_filterbank* ifb, uint64_t* info);
+/* the response applied by filter() (Response::operate, e.g. the deripple of
+   InverseFilterbankResponse::build or a dedispersion response): host complex
+   [output_nchan][Lout] interleaved re/im; NULL removes it */
+int dspsr_b200_inverse_filterbank_copy_response (dspsr_b200_inverse_filterbank* ifb,
+                                                 const float* response);
+/* temporal window of input_fft_length points applied before each forward FFT
+   and spectral window of Lout points applied after the response (either may
+   be NULL), as set_temporal_apodization / set_spectral_apodization do */
+int dspsr_b200_inverse_filterbank_set_apodization (dspsr_b200_inverse_filterbank* ifb,
+                                                   const float* temporal, const float* spectral);
+/* Engine::perform (InverseFilterbankEngineCPU.C:309-366): npart =
+   (ndat - input discards) / input step parts; output FPT complex
+   [output_nchan][npol] spans of out_span complex samples, npart * output step
+   written per span.  Input as dspsr_b200_filterbank takes it (int8 / int16
+   TFPD or complex-float FPT with in_span). */
+int dspsr_b200_inverse_filterbank_perform (dspsr_b200_inverse_filterbank* ifb, int input_kind,
+                                           const void* d_in, uint64_t ndat, uint64_t in_span,
+                                           const float* lut256, int offset_binary, float* d_out,
+                                           uint64_t out_span, uint64_t* npart);
+/* DSPSR_B200_ESTATE when a bounded device wait of the row kernel gave up */
+int dspsr_b200_inverse_filterbank_status (dspsr_b200_inverse_filterbank* ifb);
 
 /* ---------------------------------------------------------------------- */
 /* Detection::Engine (CUDA::DetectionEngine, Signal/General/DetectionCUDA.cu;*/
