@@ -3,7 +3,7 @@
 dedispersion -> detection -> fold, in complex Msamples/s.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                  [--config c1|c2|c4]
+                  [--config c1|c2|c4|c5]
 
 One step = one block of the workload processed end to end (unpack -> fold),
 the InputBuffering overlap carried from block to block.  Inputs are seeded
@@ -56,6 +56,14 @@ CONFIGS = {
                   "bursts (1-64 samples, 3-30 sigma) and one drifting chirp; M = 1024, "
                   "3 sigma thresholds (SKLimits), sums + mask + masked copy"),
         nchan=512, npol=2, ndat=1 << 20, M=1024, std_devs=3.0),
+    "c5": dict(
+        kind="ifb",
+        workload=("inverse filterbank stage: 256 critically spaced 4/3-oversampled PFB "
+                  "channels of int16 complex dual-pol voltages (seeded Gaussian), 1024-point "
+                  "input FFTs, 768 kept bins, stitched into one 196608-point spectrum, "
+                  "12288-sample output discards each side; 1 s of 800 MHz per block "
+                  "(4.17 M samples per fine channel)"),
+        nin=256, npol=2, lin=1024, disc=12288, ndat=4166784),
 }
 
 NBLOCKS = 4
@@ -695,6 +703,140 @@ def run_b200_sk(args, cfg, world, rank, local):
     ctx.close()
 
 
+# ---------------------------------------------------------------------------
+# InverseFilterbank workload
+# ---------------------------------------------------------------------------
+
+def ifb_cfg_dict(cfg):
+    return dict(input_nchan=cfg["nin"], output_nchan=1, pfb_nchan=cfg["nin"], npol=cfg["npol"],
+                input_fft_length=cfg["lin"], os_num=4, os_den=3,
+                output_discard_pos=cfg["disc"], output_discard_neg=cfg["disc"], pfb_dc_chan=1,
+                pfb_all_chan=1, dual_sideband=1)
+
+
+def run_reference_ifb(args, cfg, world, rank):
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    threads = os.cpu_count() or 1
+    c = ifb_cfg_dict(cfg)
+    keep, lout, ipos, ineg, in_step, out_step = orc.ifb_sizes(c)
+    nparts = 4
+    ndat = nparts * in_step + ipos + ineg
+    rng = np.random.default_rng(3)
+    x = (rng.standard_normal((cfg["nin"], cfg["npol"], ndat)) * 100 +
+         1j * rng.standard_normal((cfg["nin"], cfg["npol"], ndat)) * 100).astype(np.complex64)
+
+    def step():
+        t0 = time.perf_counter()
+        orc.inverse_filterbank(x, c)
+        return time.perf_counter() - t0
+    for _ in range(args.warmup):
+        step()
+    total = sum(step() for _ in range(args.steps))
+    msps = cfg["nin"] * cfg["npol"] * nparts * in_step * args.steps / total / 1e6
+    line = {
+        "impl": "reference", "metric": "complex Msamples/s inverse filterbank",
+        "value": round(msps, 3), "unit": "complex Msamples/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * total / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Gaussian complex voltages)",
+        "config": {"workload": cfg["workload"], "sample_parts_per_step": nparts},
+        "cpu_baseline": {"value": round(msps, 3), "unit": "complex Msamples/s", "cores": 1,
+                         "kind": "port",
+                         "sample": (f"{nparts} parts of {cfg['nin']} fine channels x "
+                                    f"{cfg['npol']} pol through the oracle restatement of "
+                                    "InverseFilterbankEngineCPU (single thread, FP32)")},
+        "e2e": {"value": round(msps, 3), "unit": "complex Msamples/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_b200_ifb(args, cfg, world, rank, local):
+    import torch
+    import dspsr_b200 as b2
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    ctx = b2.Context(local)
+    ifb = b2.InverseFilterbank(ctx, cfg["nin"], 1, cfg["nin"], cfg["npol"], cfg["lin"],
+                               os=(4, 3), output_discard=(cfg["disc"], cfg["disc"]))
+    info = ifb.info
+    in_step, out_step = info["in_step"], info["out_step"]
+    disc_in = info["in_discard_pos"] + info["in_discard_neg"]
+    ndat = cfg["ndat"]
+    npart = ifb.npart(ndat)
+    # int16 TFPD voltages (seeded Gaussian, sigma 100), generated on the GPU
+    gen = torch.Generator(device=device)
+    gen.manual_seed(99 + rank)
+    raw = torch.empty((ndat, cfg["nin"], cfg["npol"], 2), dtype=torch.int16, device=device)
+    chunk = 1 << 18
+    for t0 in range(0, ndat, chunk):
+        n = min(chunk, ndat - t0)
+        raw[t0:t0 + n] = (torch.randn((n, cfg["nin"], cfg["npol"], 2), generator=gen,
+                                      device=device) * 100).round().to(torch.int16)
+    raw = raw.reshape(-1)
+    out = torch.empty((1, cfg["npol"], npart * out_step, 2), dtype=torch.float32, device=device)
+    samples_per_step = cfg["nin"] * cfg["npol"] * npart * in_step
+
+    def step():
+        ifb.perform(raw, ndat, out, npart * out_step, input_kind=b2.INT16_TFPD)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(1.0)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    launches0 = b2.kernel_launches()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    evs[0].record()
+    for i in range(args.steps):
+        step()
+        evs[i + 1].record()
+    torch.cuda.synchronize()
+    launches = b2.kernel_launches() - launches0
+    clk = clocks.stop()
+    barrier(world)
+    ms = evs[0].elapsed_time(evs[-1])
+    ms_max = max_over_ranks(ms, world)
+    value = samples_per_step * args.steps * world / (ms_max / 1e3) / 1e6
+    ifb.status()
+    hbm_peak, _, peak_src = measured_peaks()
+    # algorithmic bytes per step: int16 input once (4 B per complex sample per pol)
+    # and the complex-float output once
+    alg = raw.numel() * 2 + out.numel() * 4
+    achieved = alg / (ms / args.steps / 1e3) / 1e9
+    line = {
+        "metric": "complex Msamples/s inverse filterbank", "value": round(value, 3),
+        "unit": "complex Msamples/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Gaussian int16 PFB-channel voltages)",
+        "config": {"workload": cfg["workload"], "npart": npart, "input_fft_length": cfg["lin"],
+                   "output_fft_length": info["lout"], "fft_split": [info["n1"], info["n2"]],
+                   "parts_per_batch": info["max_batch"],
+                   "l2": f"input {raw.numel() * 2 >> 20} MiB per step, larger than L2",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "clocks": clk,
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "inverse filterbank (3 kernels)",
+                     "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
+                     "frac": round(achieved / hbm_peak, 4), "traffic": None,
+                     "peak_source": peak_src,
+                     "note": "algorithmic bytes: int16 in + complex-float out, once"},
+        "e2e": None,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ifb.close()
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -716,11 +858,13 @@ def main():
         cfg["workload"] += f" [profiling size: {args.ndat} samples/pol per block]"
     world, rank, local = dist_init()
     try:
-        sk = cfg.get("kind") == "sk"
+        kind = cfg.get("kind", "path")
         if args.impl == "reference":
-            (run_reference_sk if sk else run_reference)(args, cfg, world, rank)
+            {"sk": run_reference_sk, "ifb": run_reference_ifb}.get(kind, run_reference)(
+                args, cfg, world, rank)
         else:
-            (run_b200_sk if sk else run_b200)(args, cfg, world, rank, local)
+            {"sk": run_b200_sk, "ifb": run_b200_ifb}.get(kind, run_b200)(
+                args, cfg, world, rank, local)
     finally:
         if world > 1:
             import torch.distributed as dist

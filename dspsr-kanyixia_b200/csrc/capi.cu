@@ -114,10 +114,10 @@ struct dspsr_b200_convolution
   ConvShape shape {};
   DevBuf<float2> tw2, tw4, ptab, H, tmp, scratch;
   DevBuf<double> chan_par;
-  DevBuf<float> lut;
+  DevBuf<float> lut, apod;
   DevBuf<int> err;
   int nsm = 148;
-  bool have_response = false;
+  bool have_response = false, have_apod = false;
   unsigned max_batch = 1;
 
   int init (dspsr_b200_context* c, unsigned nchan, unsigned npol, unsigned nfft,
@@ -132,10 +132,12 @@ struct dspsr_b200_convolution
     t.lut = lut.ptr;
     t.err = err.ptr;
     t.nsm = nsm;
+    t.apod = have_apod ? apod.ptr : nullptr;
     return t;
   }
   void release ()
   {
+    apod.release ();
     tw2.release ();
     tw4.release ();
     ptab.release ();
@@ -1262,6 +1264,23 @@ int dspsr_b200_filterbank (dspsr_b200_context* ctx, int input_kind, const void* 
                                       reinterpret_cast<float2*> (d_out), out_span, ctx->stream),
               "filterbank");
   if (ndat_out) *ndat_out = nblk;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_convolution_set_temporal_apodization (dspsr_b200_convolution* c,
+                                                     const float* window)
+{
+  if (!c) return DSPSR_B200_EINVAL;
+  if (!window)
+  {
+    c->have_apod = false;
+    return DSPSR_B200_OK;
+  }
+  B200_CHECK (c->ctx, cudaStreamSynchronize (c->ctx->stream), "sync before window upload");
+  B200_CHECK (c->ctx, c->apod.reserve (c->shape.nfft), "cudaMalloc temporal window");
+  B200_CHECK (c->ctx, cudaMemcpy (c->apod.ptr, window, c->shape.nfft * sizeof (float),
+                                  cudaMemcpyHostToDevice), "copy temporal window");
+  c->have_apod = true;
   return DSPSR_B200_OK;
 }
 

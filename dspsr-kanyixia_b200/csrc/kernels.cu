@@ -290,7 +290,7 @@ template <int N1, int KIND>
 __global__ void __launch_bounds__ (128, 2)
 k_fwd_cols (const InputView in, const float* __restrict__ lut, const uint64_t nkeep,
             const uint64_t part0, const unsigned n2, const float2* __restrict__ tw4,
-            float2* __restrict__ scratch)
+            float2* __restrict__ scratch, const float* __restrict__ apod)
 {
   __shared__ float s_lut[256];
   load_lut (in, lut, s_lut);
@@ -306,6 +306,16 @@ k_fwd_cols (const InputView in, const float* __restrict__ lut, const uint64_t nk
 #pragma unroll
     for (int k = 0; k < N1; k++)
       v[k] = fetch<KIND> (in, s_lut, c, p, t0 + uint64_t (k) * n2);
+    if (apod)
+    {
+      // Apodization::operate on the part before the forward FFT (Convolution.C:739-743)
+#pragma unroll
+      for (int k = 0; k < N1; k++)
+      {
+        const float w = __ldg (apod + uint64_t (k) * n2 + i2);
+        v[k] = make_float2 (__fmul_rn (v[k].x, w), __fmul_rn (v[k].y, w));
+      }
+    }
     RegDFT<N1, -1>::run (v);
     // four-step twiddle w_N^{k1 n2} (row k1 of the [n1][n2] table; coalesced)
 #pragma unroll
@@ -560,7 +570,8 @@ template <int N, int T, int KIND, int MODE, int NOUT>
 __global__ void __launch_bounds__ (T, 512 / T)
 k_fused (const InputView in, const float* __restrict__ lut, const float2* __restrict__ tw,
          const float2* __restrict__ H, const uint64_t nkeep, const unsigned nfilt_pos,
-         const uint64_t part0, const FoldView fv, const VoltView vv)
+         const uint64_t part0, const FoldView fv, const VoltView vv,
+         const float* __restrict__ apod)
 {
   extern __shared__ float2 s[];
   __shared__ float s_lut[256];
@@ -573,7 +584,15 @@ k_fused (const InputView in, const float* __restrict__ lut, const float2* __rest
   __syncthreads ();
   for (unsigned p = 0; p < npol; p++)
     for (int i = threadIdx.x; i < N; i += T)
-      s[p * SP + spad (i)] = fetch<KIND> (in, s_lut, c, p, part * nkeep + i);
+    {
+      float2 x = fetch<KIND> (in, s_lut, c, p, part * nkeep + i);
+      if (apod)
+      {
+        const float w = __ldg (apod + i);
+        x = make_float2 (__fmul_rn (x.x, w), __fmul_rn (x.y, w));
+      }
+      s[p * SP + spad (i)] = x;
+    }
   __syncthreads ();
   const float2* h = H + uint64_t (c) * N;
   for (unsigned p = 0; p < npol; p++)
@@ -1088,13 +1107,13 @@ cudaError_t run_fourstep_n1 (const ConvShape& sh, const ConvTables& tb, const In
   ClockScope cs (clk, KK_FWD_COLS, st);
   if (in.kind == IN_INT8)
     k_fwd_cols<N1, IN_INT8><<<gcol, 128, 0, st>>> (in, tb.lut, sh.nkeep, part0, sh.n2, tb.tw4,
-                                                   scratch);
+                                                   scratch, tb.apod);
   else if (in.kind == IN_INT16)
     k_fwd_cols<N1, IN_INT16><<<gcol, 128, 0, st>>> (in, tb.lut, sh.nkeep, part0, sh.n2, tb.tw4,
-                                                    scratch);
+                                                    scratch, tb.apod);
   else
     k_fwd_cols<N1, IN_FLOAT><<<gcol, 128, 0, st>>> (in, tb.lut, sh.nkeep, part0, sh.n2, tb.tw4,
-                                                    scratch);
+                                                    scratch, tb.apod);
   }
   const unsigned nrows = N1 * nbatch * sh.nchan * sh.npol;
   {
@@ -1141,7 +1160,7 @@ cudaError_t run_fused_t (const ConvShape& sh, const ConvTables& tb, const InputV
   if (err != cudaSuccess) return err;
   ClockScope cs (clk, KK_FUSED, st);
   kern<<<dim3 (nbatch, sh.nchan), T, smem, st>>> (in, tb.lut, tb.tw2, tb.H, sh.nkeep,
-                                                  sh.nfilt_pos, part0, fv, vv);
+                                                  sh.nfilt_pos, part0, fv, vv, tb.apod);
   return cudaGetLastError ();
 }
 

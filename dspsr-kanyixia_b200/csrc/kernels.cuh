@@ -62,6 +62,7 @@ struct ConvTables
   const float* lut;          // 8-bit lookup table (device), 256 floats
   int* err;                  // device flag: set when a bounded wait gave up
   int nsm;                   // multiprocessors of the device
+  const float* apod;         // temporal window [nfft] applied to each part, or null
 };
 
 // Per-pass Stockham twiddle tables of an n-point transform, as the row

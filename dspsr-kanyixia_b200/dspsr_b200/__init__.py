@@ -217,6 +217,12 @@ class Convolution:
             self.handle, f.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), bandwidth, dm,
             chirp_mode, norm_nfft or self.nfft), "set_dedispersion_channels")
 
+    def set_temporal_apodization(self, window):
+        w = None if window is None else np.ascontiguousarray(window, np.float32)
+        assert w is None or w.size == self.nfft
+        self.ctx.check(self._lib.dspsr_b200_convolution_set_temporal_apodization(
+            self.handle, None if w is None else _fptr(w)), "set_temporal_apodization")
+
     def status(self):
         self.ctx.check(self._lib.dspsr_b200_convolution_status(self.handle), "status")
 

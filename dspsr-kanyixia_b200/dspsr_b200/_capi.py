@@ -106,6 +106,7 @@ SIGNATURES = {
                                                         c_int, c_int, c_uint]),
     "dspsr_b200_convolution_get_response": (c_int, [c_vp, c_fp]),
     "dspsr_b200_convolution_status": (c_int, [c_vp]),
+    "dspsr_b200_convolution_set_temporal_apodization": (c_int, [c_vp, c_fp]),
     "dspsr_b200_convolution_perform_noalloc": (c_int, [c_vp, c_vp, c_u64, c_u64, c_uint, c_uint,
                                                        c_uint, c_uint, c_uint, c_vp, c_vp, c_u64,
                                                        c_u64p]),

@@ -202,6 +202,12 @@ int dspsr_b200_convolution_perform_noalloc (void* stream, const float* d_in, uin
 int dspsr_b200_convolution_status (dspsr_b200_convolution* conv);
 /* copies the response (FFT order) back to host memory, nchan*nfft complex */
 int dspsr_b200_convolution_get_response (dspsr_b200_convolution* conv, float* response);
+/* Convolution::set_temporal_apodization (Convolution.C:144-147, 222-250,
+   applied at :739-743): a window of nfft floats (dspsr_b200_apodization, e.g.
+   Tukey with transitions nfilt_pos / nfilt_neg) multiplied into every part
+   before its forward FFT; NULL removes it. */
+int dspsr_b200_convolution_set_temporal_apodization (dspsr_b200_convolution* conv,
+                                                     const float* window);
 /* Engine::perform(input, output, npart): complex FPT in (span in complex
    samples per (chan, pol)), complex FPT out; returns npart
    = (ndat - nfilt_pos - nfilt_neg)/(nfft - nfilt_pos - nfilt_neg). */

@@ -184,6 +184,17 @@ int64_t orc_inverse_filterbank_f64 (const orc_ifb_config* cfg, const double* in,
                                     const double* temporal, const double* spectral, double* out,
                                     uint64_t out_span);
 
+/* overlap-save as orc_convolve_f32 with the temporal apodization window
+   (nfft floats) applied to every part before its forward FFT */
+uint64_t orc_convolve_window_f32 (const float* in, uint64_t ndat, uint64_t in_span, int nchan,
+                                  int npol, const float* response, unsigned nfft,
+                                  unsigned nfilt_pos, unsigned nfilt_neg, float* out,
+                                  uint64_t out_span, int nthreads, const float* window);
+/* Apodization::build (Signal/General/Apodization.C:60-178): 0 top hat,
+   1 Hanning, 2 Welch, 3 Bartlett, 4 Tukey; swap exchanges the halves */
+int orc_apodization (int type, unsigned ndat, unsigned transition_start,
+                     unsigned transition_end, int swap, float* window);
+
 /* ---- the whole single-channel path, for the timed CPU baseline ----------- */
 /* int8 TFPD (nchan=1, npol=2, ndim=2) -> unpack -> convolve -> Intensity ->
    fold.  Returns the number of output samples folded per pol. */

@@ -63,6 +63,9 @@ _SIGS = {
                                            ctypes.c_void_p, ctypes.c_void_p, f32p, c_u64]),
     "orc_inverse_filterbank_f64": (c_i64, [ctypes.c_void_p, f64p, c_u64, c_u64, ctypes.c_void_p,
                                            ctypes.c_void_p, ctypes.c_void_p, f64p, c_u64]),
+    "orc_convolve_window_f32": (c_u64, [f32p, c_u64, c_u64, c_int, c_int, f32p, c_uint, c_uint,
+                                        c_uint, f32p, c_u64, c_int, f32p]),
+    "orc_apodization": (c_int, [c_int, c_uint, c_uint, c_uint, c_int, f32p]),
     "orc_pipeline_c1": (c_u64, [u8p, c_u64, f32p, f32p, c_uint, c_uint, c_uint, c_dbl, c_dbl,
                                 c_uint, f32p, u32p, c_int]),
     "orc_channel_centre": (c_dbl, [c_dbl, c_dbl, c_uint, c_uint, c_int, c_int]),
@@ -300,6 +303,28 @@ def convolve(x, response, nfft, nfilt_pos, nfilt_neg, nthreads=8):
                                nfilt_pos, nfilt_neg, out.view(np.float64).ravel(),
                                npart * nkeep, nthreads)
     return out
+
+
+def convolve_window(x, response, nfft, nfilt_pos, nfilt_neg, window, nthreads=8):
+    """convolve() with a temporal window (nfft floats) on every part."""
+    nchan, npol, ndat = x.shape
+    nkeep = nfft - nfilt_pos - nfilt_neg
+    npart = (ndat - nfilt_pos - nfilt_neg) // nkeep if ndat >= nfft else 0
+    out = np.zeros((nchan, npol, npart * nkeep), np.complex64)
+    r = np.ascontiguousarray(response, np.complex64)
+    lib().orc_convolve_window_f32(np.ascontiguousarray(x, np.complex64).view(np.float32).ravel(),
+                                  ndat, ndat, nchan, npol, r.view(np.float32).ravel(), nfft,
+                                  nfilt_pos, nfilt_neg, out.view(np.float32).ravel(),
+                                  npart * nkeep, nthreads,
+                                  np.ascontiguousarray(window, np.float32))
+    return out
+
+
+def apodization(kind, ndat, transition_start=0, transition_end=0, swap=False):
+    w = np.zeros(ndat, np.float32)
+    if lib().orc_apodization(kind, ndat, transition_start, transition_end, int(swap), w) != 0:
+        raise ValueError("apodization: invalid type or size")
+    return w
 
 
 STATES = {"Intensity": 0, "PPQQ": 1, "Coherence": 2, "Stokes": 3}

@@ -201,7 +201,7 @@ void dedispersion_phases (double cf, double bw, double dm, unsigned nchan,
 template <typename T>
 uint64_t convolve (const T* in, uint64_t ndat, uint64_t in_span, int nchan, int npol,
                    const T* response, unsigned nfft, unsigned nfilt_pos, unsigned nfilt_neg,
-                   T* out, uint64_t out_span, int nthreads)
+                   T* out, uint64_t out_span, int nthreads, const T* window = nullptr)
 {
   typedef std::complex<T> C;
   const uint64_t nsamp_overlap = nfilt_pos + nfilt_neg;
@@ -213,7 +213,7 @@ uint64_t convolve (const T* in, uint64_t ndat, uint64_t in_span, int nchan, int 
   (void) nthreads;
 #pragma omp parallel num_threads(nthreads > 0 ? nthreads : 1)
   {
-    std::vector<C> spectrum (nfft), complex_time (nfft);
+    std::vector<C> spectrum (nfft), complex_time (nfft), windowed (window ? nfft : 0);
 #pragma omp for schedule(static)
     for (int64_t task = 0; task < ntask; task++)
     {
@@ -222,6 +222,13 @@ uint64_t convolve (const T* in, uint64_t ndat, uint64_t in_span, int nchan, int 
       const int ichan = int (uint64_t (task) / npart / npol);
       const C* ptr = reinterpret_cast<const C*> (in) + (uint64_t (ichan) * npol + ipol) * in_span
                      + ipart * nsamp_step;
+      if (window)
+      {
+        // Apodization::operate on the part (Convolution.C:739-743)
+        for (unsigned i = 0; i < nfft; i++)
+          windowed[i] = C (ptr[i].real () * window[i], ptr[i].imag () * window[i]);
+        ptr = windowed.data ();
+      }
       fft<T> (nfft, -1, ptr, spectrum.data ());
       // Response::operate (Response.C:662-726)
       const C* f = reinterpret_cast<const C*> (response) + uint64_t (ichan) * nfft;
@@ -674,6 +681,62 @@ uint64_t orc_convolve_f32 (const float* in, uint64_t ndat, uint64_t in_span, int
 {
   return convolve<float> (in, ndat, in_span, nchan, npol, response, nfft, nfilt_pos,
                           nfilt_neg, out, out_span, nthreads);
+}
+
+uint64_t orc_convolve_window_f32 (const float* in, uint64_t ndat, uint64_t in_span, int nchan,
+                                  int npol, const float* response, unsigned nfft,
+                                  unsigned nfilt_pos, unsigned nfilt_neg, float* out,
+                                  uint64_t out_span, int nthreads, const float* window)
+{
+  return convolve<float> (in, ndat, in_span, nchan, npol, response, nfft, nfilt_pos,
+                          nfilt_neg, out, out_span, nthreads, window);
+}
+
+// Apodization::build (Apodization.C:60-146): window types 0 top hat, 1
+// Hanning, 2 Welch, 3 Bartlett, 4 Tukey; swap exchanges halves (:168-178)
+int orc_apodization (int type, unsigned ndat, unsigned transition_start,
+                     unsigned transition_end, int swap, float* buffer)
+{
+  if (!ndat) return -1;
+  for (unsigned idat = 0; idat < ndat; idat++)
+  {
+    if (type == 0)
+      buffer[idat] = 1.0;
+    else if (type == 1)
+    {
+      double denom = ndat - 1.0;
+      buffer[idat] = 0.5 * (1 - cos (2.0 * M_PI * double (idat) / denom));
+    }
+    else if (type == 2)
+    {
+      float centre = 0.5 * (ndat - 1);
+      float denominator = 0.5 * (ndat + 1);
+      float tosquare = (float (idat) - centre) / denominator;
+      buffer[idat] = 1.0 - tosquare * tosquare;
+    }
+    else if (type == 3)
+    {
+      float centre = 0.5 * (ndat - 1);
+      float denominator = 0.5 * (ndat - 1);
+      buffer[idat] = 1.0 - fabs ((float (idat) - centre) / denominator);
+    }
+    else if (type == 4)
+    {
+      float denom_start = 2 * transition_start;
+      float denom_end = 2 * transition_end;
+      if (idat < transition_start)
+        buffer[idat] = 0.5 * (1 - cos (2.0 * M_PI * float (idat) / denom_start));
+      else if (idat + 1 > ndat - transition_end)
+        buffer[idat] = 0.5 * (1 - cos (2.0 * M_PI * float (ndat - idat - 1) / denom_end));
+      else
+        buffer[idat] = 1.0;
+    }
+    else
+      return -1;
+  }
+  if (swap)
+    for (unsigned i = 0; i < ndat / 2; i++) std::swap (buffer[i], buffer[i + ndat / 2]);
+  return 0;
 }
 
 uint64_t orc_convolve_f64 (const double* in, uint64_t ndat, uint64_t in_span, int nchan,
