@@ -363,7 +363,8 @@ def run_b200(args, cfg, world, rank, local):
     lut, _ = b2.bittable8()
     c = b2.make_config(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nchan"], cfg["npol"], nfft, pos,
                        neg, cfg["nbin"], cfg["period"], state=cfg["state"], lut=lut,
-                       start_mjd=START_MJD, epoch_mjd=EPOCH_MJD, filterbank_nchan=cfg["fb"])
+                       start_mjd=START_MJD, epoch_mjd=EPOCH_MJD, filterbank_nchan=cfg["fb"],
+                       scratch_bytes=args.scratch_mib << 20)
     blocks = make_blocks(cfg, 1234 + rank, device)
     ndat = cfg["ndat"]
     samples_per_step = ndat * cfg["npol"]   # complex samples consumed per step (all pols)
@@ -845,6 +846,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scratch-mib", type=int, default=0,
+                    help="device scratch of the four-step FFT batches (0: the library default)")
     ap.add_argument("--sk-inplace", action="store_true",
                     help="c4: mask the voltages in place (only zapped blocks are written)")
     ap.add_argument("--ndat", type=int, default=0,

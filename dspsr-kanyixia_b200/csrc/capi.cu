@@ -216,7 +216,7 @@ int dspsr_b200_convolution::init (dspsr_b200_context* c, unsigned nchan, unsigne
     // otherwise, and the batch is chosen so that its rows spread evenly over
     // the persistent row kernel's CTAs.
     const uint64_t per_part = uint64_t (nchan) * npol * nfft * sizeof (float2);
-    const uint64_t budget = scratch_bytes ? scratch_bytes : (uint64_t (96) << 20);
+    const uint64_t budget = scratch_bytes ? scratch_bytes : (uint64_t (512) << 20);
     const uint64_t bmax = std::max<uint64_t> (1, std::min<uint64_t> (65535, budget / per_part));
     const uint64_t rows_per_part = uint64_t (shape.n1) * nchan * npol;
     const uint64_t ctas = uint64_t (nsm) * (shape.n2 >= 8192 ? 1 : 2);
@@ -444,7 +444,10 @@ struct dspsr_b200_pipeline
   uint64_t ncarry = 0;
   int cur_carry = 0;
   uint64_t in0 = 0;                 // global input index of the first sample of the block
-  DevBuf<uint8_t> staging;          // host->device staging for run_host
+  DevBuf<uint8_t> staging[2];       // host->device staging for run_host (double buffer)
+  cudaStream_t copy_stream = nullptr;   // run_host uploads, overlapping the kernels
+  cudaEvent_t copied[2] = {nullptr, nullptr}, consumed[2] = {nullptr, nullptr};
+  bool consumed_pending[2] = {false, false};
   double rate = 0;                  // complex sampling rate of the convolved channels
   unsigned fb_nsub = 0;             // filterbank channels per input channel (0: none)
   DevBuf<float2> fbbuf;             // filterbank output, FPT
@@ -625,7 +628,7 @@ struct dspsr_b200_inverse_filterbank
   {
     IfbTables t;
     t.map = map.ptr;
-    t.tw_lin = tw_lin.ptr;
+    t.ptab_lin = tw_lin.ptr;
     t.tw4 = tw4.ptr;
     t.ptab = ptab.ptr;
     t.response = have_response ? response.ptr : nullptr;
@@ -802,9 +805,11 @@ int dspsr_b200_inverse_filterbank::init (dspsr_b200_context* c, const dspsr_b200
   B200_CHECK (ctx, map.reserve (nin), "cudaMalloc stitch map");
   B200_CHECK (ctx, cudaMemcpy (map.ptr, m.data (), nin * sizeof (int4), cudaMemcpyHostToDevice),
               "copy stitch map");
-  std::vector<float2> t = make_tw2 (lin);
-  B200_CHECK (ctx, tw_lin.reserve (lin), "cudaMalloc twiddles");
-  B200_CHECK (ctx, cudaMemcpy (tw_lin.ptr, t.data (), lin * sizeof (float2),
+  const unsigned ntab_lin = pass_tables_count (lin);
+  std::vector<float2> t (std::max (ntab_lin, 1u), make_float2 (0.f, 0.f));
+  make_pass_tables (lin, t.data (), ntab_lin);
+  B200_CHECK (ctx, tw_lin.reserve (t.size ()), "cudaMalloc twiddles");
+  B200_CHECK (ctx, cudaMemcpy (tw_lin.ptr, t.data (), t.size () * sizeof (float2),
                                cudaMemcpyHostToDevice), "copy twiddles");
   t = make_tw4 (n1, n2);
   B200_CHECK (ctx, tw4.reserve (lout), "cudaMalloc four-step twiddles");
@@ -823,7 +828,7 @@ int dspsr_b200_inverse_filterbank::init (dspsr_b200_context* c, const dspsr_b200
   B200_CHECK (ctx, cudaDeviceGetAttribute (&nsm, cudaDevAttrMultiProcessorCount, dev),
               "multiprocessor count");
   const uint64_t per_part = uint64_t (nout) * cfg.npol * lout * sizeof (float2);
-  const uint64_t budget = cfg.scratch_bytes ? cfg.scratch_bytes : (uint64_t (96) << 20);
+  const uint64_t budget = cfg.scratch_bytes ? cfg.scratch_bytes : (uint64_t (512) << 20);
   max_batch = unsigned (std::max<uint64_t> (1, std::min<uint64_t> (65535, budget / per_part)));
   B200_CHECK (ctx, scratch.reserve (size_t (max_batch) * nout * cfg.npol * lout),
               "cudaMalloc scratch");
@@ -1522,7 +1527,15 @@ int dspsr_b200_pipeline_destroy (dspsr_b200_pipeline* pl)
   pl->fold.release ();
   pl->carry[0].release ();
   pl->carry[1].release ();
-  pl->staging.release ();
+  pl->staging[0].release ();
+  pl->staging[1].release ();
+  if (pl->copy_stream) cudaStreamSynchronize (pl->copy_stream);
+  for (int i = 0; i < 2; i++)
+  {
+    if (pl->copied[i]) cudaEventDestroy (pl->copied[i]);
+    if (pl->consumed[i]) cudaEventDestroy (pl->consumed[i]);
+  }
+  if (pl->copy_stream) cudaStreamDestroy (pl->copy_stream);
   pl->fbbuf.release ();
   delete pl;
   return DSPSR_B200_OK;
@@ -1546,11 +1559,52 @@ int dspsr_b200_pipeline_run_host (dspsr_b200_pipeline* pl, const void* h_in, uin
   if (pl->cfg.input_kind == DSPSR_B200_FLOAT_FPT)
     return fail (ctx, DSPSR_B200_EINVAL, "pipeline_run_host: TFPD input only");
   if (!h_in && ndat) return fail (ctx, DSPSR_B200_EINVAL, "pipeline_run_host: null input");
-  const uint64_t bytes = ndat * pl->bytes_per_sample;
-  B200_CHECK (ctx, pl->staging.reserve (std::max<uint64_t> (bytes, 16)), "cudaMalloc staging");
-  B200_CHECK (ctx, cudaMemcpyAsync (pl->staging.ptr, h_in, bytes, cudaMemcpyHostToDevice,
-                                    ctx->stream), "upload block");
-  return pipeline_input (pl, pl->staging.ptr, ndat, 0, ndat_folded);
+  if (ndat_folded) *ndat_folded = 0;
+  if (!pl->copy_stream)
+  {
+    B200_CHECK (ctx, cudaStreamCreateWithFlags (&pl->copy_stream, cudaStreamNonBlocking),
+                "create upload stream");
+    for (int i = 0; i < 2; i++)
+    {
+      B200_CHECK (ctx, cudaEventCreateWithFlags (&pl->copied[i], cudaEventDisableTiming),
+                  "create event");
+      B200_CHECK (ctx, cudaEventCreateWithFlags (&pl->consumed[i], cudaEventDisableTiming),
+                  "create event");
+    }
+  }
+  // The block is uploaded in up to four pieces on a stream of its own, each
+  // into one of two staging buffers, so that the upload of a piece overlaps
+  // the kernels of the one before; the carried overlap joins the pieces as it
+  // joins blocks.  Pieces are whole filterbank transforms.
+  const uint64_t unit = pl->fb_nsub ? pl->fb_nsub : 1;
+  const uint64_t min_piece = uint64_t (pl->conv.shape.nfft) * unit * 2;
+  const uint64_t npiece = ndat >= 4 * min_piece ? 4 : ndat >= 2 * min_piece ? 2 : 1;
+  const uint64_t piece = ((ndat + npiece - 1) / npiece + unit - 1) / unit * unit;
+  const uint64_t bps = pl->bytes_per_sample;
+  uint64_t total = 0;
+  for (uint64_t j = 0, off = 0; off < ndat || (ndat == 0 && j == 0); j++, off += piece)
+  {
+    const uint64_t n = std::min<uint64_t> (piece, ndat - off);
+    const int b = int (j & 1);
+    if (pl->consumed_pending[b])
+      B200_CHECK (ctx, cudaStreamWaitEvent (pl->copy_stream, pl->consumed[b], 0), "wait staging");
+    B200_CHECK (ctx, pl->staging[b].reserve (std::max<uint64_t> (piece * bps, 16)),
+                "cudaMalloc staging");
+    B200_CHECK (ctx, cudaMemcpyAsync (pl->staging[b].ptr, static_cast<const uint8_t*> (h_in) + off * bps,
+                                      n * bps, cudaMemcpyHostToDevice, pl->copy_stream),
+                "upload block");
+    B200_CHECK (ctx, cudaEventRecord (pl->copied[b], pl->copy_stream), "record upload");
+    B200_CHECK (ctx, cudaStreamWaitEvent (ctx->stream, pl->copied[b], 0), "wait upload");
+    uint64_t folded = 0;
+    const int rc = pipeline_input (pl, pl->staging[b].ptr, n, 0, &folded);
+    if (rc) return rc;
+    total += folded;
+    B200_CHECK (ctx, cudaEventRecord (pl->consumed[b], ctx->stream), "record consumed");
+    pl->consumed_pending[b] = true;
+    if (ndat == 0) break;
+  }
+  if (ndat_folded) *ndat_folded = total;
+  return DSPSR_B200_OK;
 }
 
 int dspsr_b200_pipeline_get_profiles (dspsr_b200_pipeline* pl, float* profiles, uint32_t* hits)

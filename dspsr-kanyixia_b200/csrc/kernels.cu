@@ -634,42 +634,178 @@ k_fused (const InputView in, const float* __restrict__ lut, const float2* __rest
 // inverse filterbank (InverseFilterbankEngineCPU.C:309-779 restructured)
 // --------------------------------------------------------------------------
 
-// One CTA per (fine channel, pol, part): unpack on load and temporal window
-// (Apodization::operate), lin-point forward FFT in shared memory, then the
-// kept bins of both halves -- stitch_one's placement, precomputed per channel
-// on the host -- times the response and the spectral window, written into the
-// output channel's spectrum in four-step order (bin k at row k mod n1,
-// column k div n1) for the row kernel.
+// Stockham FFT of N points run by a group of T = N/16 threads (tid within the
+// group) on the group's own shared-memory array; every group of the CTA runs
+// the same passes, so the CTA-wide barriers line up.
+// Twiddles come from the per-pass tables (pass_table_offset layout) that the
+// caller holds in shared memory.
+template <int N, int T, int D, int P>
+__device__ __forceinline__ void group_fft_pass (float2* s, float2* v, const float2* tab, int tid)
+{
+  if constexpr (P < stockham_npass (N))
+  {
+    constexpr int R = stockham_radix (N, P);
+    constexpr int Ns = stockham_ns (N, P);
+    StockhamPassT<N, R, T, D, true, true>::load (tid, s, v);
+    __syncthreads ();
+    StockhamPassT<N, R, T, D, true, true>::compute_store (
+        tid, Ns, v, s, P ? tab + pass_table_offset (N, P) : nullptr);
+    __syncthreads ();
+    group_fft_pass<N, T, D, P + 1> (s, v, tab, tid);
+  }
+}
+
+// A CTA of IFB_THREADS threads transforms F = 8192/LIN (channel, pol) slots of
+// one part: CG = F/npol consecutive fine channels, both pols.  The input tile
+// is read so that consecutive threads touch consecutive bytes (for TFPD input
+// the slots of one time sample are contiguous; for FPT input the samples of
+// one slot are), unpacked and windowed (Apodization::operate) into shared
+// memory; each group of LIN/16 threads runs the forward FFT of its slot; then
+// the kept bins of both halves -- stitch_one's placement, precomputed per
+// channel on the host -- times the response and the spectral window go to the
+// output channel's spectrum in four-step order (bin k at row k mod n1, column
+// k div n1) for the row kernel.
+constexpr int IFB_THREADS = 512;
+
 template <int LIN, int KIND>
-__global__ void __launch_bounds__ (stockham_threads (LIN))
+__global__ void __launch_bounds__ (IFB_THREADS)
 k_ifb_stitch (const InputView in, const IfbShape sh, const IfbTables tb, const uint64_t part0,
               float2* __restrict__ scratch)
 {
-  constexpr int T = stockham_threads (LIN);
-  __shared__ float2 s[spad_size (LIN)];
+  constexpr int TF = stockham_threads (LIN);     // threads per transform
+  constexpr int F = IFB_THREADS / TF;             // slots per CTA
+  // slot stride: the padded transform plus 32 bytes, so that the slots of one
+  // time sample written together fall on different banks
+  constexpr int SP = spad_size (LIN) + 4;
+  constexpr int TABN = pass_tables_size (LIN);
+  extern __shared__ float2 s_ifb[];               // [F][SP], then the pass tables
+  float2* s_tab = s_ifb + F * SP;
   __shared__ float s_lut[256];
-  const unsigned jch = blockIdx.x, p = blockIdx.y, b = blockIdx.z;
+  const unsigned npol = sh.npol;
+  const unsigned cg = F / npol;                   // channels per CTA
+  const unsigned c0 = blockIdx.x * cg;
+  const unsigned b = blockIdx.y;
   load_lut (in, tb.lut, s_lut);
+  for (int i = threadIdx.x; i < TABN; i += IFB_THREADS) s_tab[i] = __ldg (tb.ptab_lin + i);
   __syncthreads ();
   const uint64_t t0 = (part0 + b) * sh.in_step;
-  for (int i = threadIdx.x; i < LIN; i += T)
+  // all PER loads of a thread are issued before any is used
+  constexpr int PER = F * LIN / IFB_THREADS;
+  const unsigned nslot = min (unsigned (F), (sh.nin - c0) * npol);   // live slots
+  const uint64_t row = uint64_t (sh.nin) * npol;                       // TFPD values per sample
+  uint32_t word[PER];
+  float2 fv[KIND == IN_FLOAT ? PER : 1];
+#pragma unroll
+  for (int k = 0; k < PER; k++)
   {
-    float2 x = fetch<KIND> (in, s_lut, jch, p, t0 + i);
+    const unsigned e = threadIdx.x + k * IFB_THREADS;
+    if constexpr (KIND == IN_FLOAT)
+    {
+      const unsigned slot = e / LIN, t = e % LIN;
+      fv[k] = slot < nslot ? __ldg (static_cast<const float2*> (in.main)
+                                    + (uint64_t (c0) * npol + slot) * in.main_span + t0 + t)
+                           : make_float2 (0.f, 0.f);
+    }
+    else
+    {
+      const unsigned slot = e % F, t = e / F;
+      const uint64_t idx = (t0 + t) * row + uint64_t (c0) * npol + slot;
+      if constexpr (KIND == IN_INT16)
+        word[k] = slot < nslot ? __ldg (static_cast<const uint32_t*> (in.main) + idx) : 0u;
+      else
+        word[k] = slot < nslot ? __ldg (static_cast<const unsigned short*> (in.main) + idx) : 0u;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < PER; k++)
+  {
+    const unsigned e = threadIdx.x + k * IFB_THREADS;
+    unsigned slot, t;
+    float2 x;
+    if constexpr (KIND == IN_FLOAT)
+    {
+      slot = e / LIN;
+      t = e % LIN;
+      x = fv[k];
+    }
+    else
+    {
+      slot = e % F;
+      t = e / F;
+      if constexpr (KIND == IN_INT16)
+      {
+        short re = short (word[k] & 0xffff), im = short (word[k] >> 16);
+        if (in.offset_binary)
+        {
+          re = short (re ^ 0x8000);
+          im = short (im ^ 0x8000);
+        }
+        // SixteenBitUnpacker.C:69: float(x) + 0.5
+        x = make_float2 (__fadd_rn (float (re), 0.5f), __fadd_rn (float (im), 0.5f));
+      }
+      else
+        x = make_float2 (s_lut[word[k] & 0xff], s_lut[word[k] >> 8]);
+      if (slot >= nslot) x = make_float2 (0.f, 0.f);
+    }
     if (tb.temporal)
     {
-      const float w = __ldg (tb.temporal + i);
+      const float w = __ldg (tb.temporal + t);
       x = make_float2 (__fmul_rn (x.x, w), __fmul_rn (x.y, w));
     }
-    s[spad (i)] = x;
+    s_ifb[slot * SP + spad (t)] = x;
   }
   __syncthreads ();
-  smem_fft<LIN, T, -1> (s, tb.tw_lin);
-  const int4 m = __ldg (tb.map + jch);
+  const unsigned group = threadIdx.x / TF, tid = threadIdx.x % TF;
+  float2* s = s_ifb + group * SP;
+  {
+    float2 v[LIN / TF];
+    group_fft_pass<LIN, TF, -1, 0> (s, v, s_tab, tid);
+  }
+  const unsigned c = c0 + group / npol, p = group % npol;
+  if (c >= sh.nin) return;
+  const int4 m = __ldg (tb.map + c);
   const unsigned keep2 = sh.keep / 2;
   const unsigned skip2 = (LIN - sh.keep) / 2;
   const unsigned src_neg = sh.dual_sideband ? LIN - keep2 : skip2;
   const unsigned src_pos = sh.dual_sideband ? 0 : skip2 + keep2;
-  for (unsigned i = threadIdx.x; i < sh.keep; i += T)
+  if (keep2 % sh.n1 == 0)
+  {
+    // n1 divides keep/2, so every half starts on a multiple of n1 and its
+    // bins fill per_row consecutive columns of each four-step row: threads
+    // walk them row by row, consecutive threads writing consecutive columns.
+    const unsigned per_row = keep2 / sh.n1;
+    const bool pow2 = (per_row & (per_row - 1)) == 0;
+    const unsigned lg = __ffs (per_row) - 1;
+    for (int h = 0; h < 2; h++)
+    {
+      const int o = h ? m.z : m.x;
+      const int offz = h ? m.w : m.y;
+      const unsigned off = unsigned (offz & (IFB_ZERO - 1));
+      const unsigned src0 = h ? src_pos : src_neg;
+      float2* dst = scratch + ((uint64_t (b) * sh.nout + o) * sh.npol + p) * sh.lout + off / sh.n1;
+      for (unsigned r = tid; r < keep2; r += TF)
+      {
+        const unsigned a = pow2 ? r >> lg : r / per_row;
+        const unsigned q = r - a * per_row;
+        const unsigned j = q * sh.n1 + a;
+        float2 y = (offz & IFB_ZERO) ? make_float2 (0.f, 0.f) : s[spad (src0 + j)];
+        if (tb.response)
+        {
+          const float2 f = __ldg (tb.response + uint64_t (o) * sh.lout + off + j);
+          y = make_float2 (__fsub_rn (__fmul_rn (f.x, y.x), __fmul_rn (f.y, y.y)),
+                           __fadd_rn (__fmul_rn (f.y, y.x), __fmul_rn (f.x, y.y)));
+        }
+        if (tb.spectral)
+        {
+          const float w = __ldg (tb.spectral + off + j);
+          y = make_float2 (__fmul_rn (y.x, w), __fmul_rn (y.y, w));
+        }
+        dst[uint64_t (a) * sh.n2 + q] = y;
+      }
+    }
+    return;
+  }
+  for (unsigned i = tid; i < sh.keep; i += TF)
   {
     const bool neg = i < keep2;
     const unsigned j = neg ? i : i - keep2;
@@ -1194,8 +1330,13 @@ template <int LIN, int KIND>
 void launch_ifb_stitch (const IfbShape& sh, const IfbTables& tb, const InputView& in,
                         uint64_t part0, unsigned nbatch, float2* scratch, cudaStream_t st)
 {
-  k_ifb_stitch<LIN, KIND><<<dim3 (sh.nin, sh.npol, nbatch), stockham_threads (LIN), 0, st>>> (
-      in, sh, tb, part0, scratch);
+  constexpr int F = IFB_THREADS / stockham_threads (LIN);
+  const size_t smem = (size_t (F) * (spad_size (LIN) + 4) + pass_tables_size (LIN)) * sizeof (float2);
+  auto kern = k_ifb_stitch<LIN, KIND>;
+  cudaFuncSetAttribute (kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int (smem));
+  const unsigned cg = F / sh.npol;
+  kern<<<dim3 ((sh.nin + cg - 1) / cg, nbatch), IFB_THREADS, smem, st>>> (in, sh, tb, part0,
+                                                                         scratch);
 }
 
 template <int LIN>
@@ -1244,6 +1385,12 @@ unsigned pass_tables_count (unsigned n)
 {
   switch (n)
   {
+    case 64: return pass_tables_size (64);
+    case 128: return pass_tables_size (128);
+    case 256: return pass_tables_size (256);
+    case 512: return pass_tables_size (512);
+    case 1024: return pass_tables_size (1024);
+    case 2048: return pass_tables_size (2048);
     case 4096: return pass_tables_size (4096);
     case 8192: return pass_tables_size (8192);
     default: return 0;

@@ -135,7 +135,7 @@ struct IfbTables
   // output channel of the positive half, its first bin); bit 30 of a first
   // bin marks a half that is zeroed instead
   const int4* map;
-  const float2* tw_lin;      // lin-point table exp(-2 pi i m / lin)
+  const float2* ptab_lin;    // per-pass Stockham tables of the lin-point transform
   const float2* tw4;         // [n1][n2] four-step table of the lout-point transform
   const float2* ptab;        // per-pass tables of the n2-point row transform
   const float2* response;    // [nout][lout] or null

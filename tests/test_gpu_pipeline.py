@@ -220,6 +220,22 @@ def test_pipeline_host_input_matches_device_input(ctx, b2):
     check(a[0], a[1], a[2], b[0].astype(np.float64), b[1], b[2], cfg["state"], rtol=1e-6)
 
 
+@pytest.mark.parametrize("nfft_mult", [9, 17])
+def test_pipeline_host_upload_in_pieces(ctx, b2, nfft_mult):
+    """Large host blocks are uploaded in 2 or 4 pieces that overlap the
+    kernels; the carried overlap joins them, so the result equals the
+    device-input run."""
+    cfg = base_cfg(b2, dm=20.0, nfft=1 << 15, nbin=512, period=0.08933)
+    rng = np.random.default_rng(nfft_mult)
+    blocks = make_blocks(rng, cfg, [nfft_mult * cfg["nfft"] + 12345, 3 * cfg["nfft"] + 7,
+                                    nfft_mult * cfg["nfft"]])
+    a = run_pipeline(ctx, b2, blocks, cfg)
+    b = run_pipeline(ctx, b2, blocks, cfg, host=True)
+    assert a[2] == b[2]
+    assert np.array_equal(a[1], b[1])
+    check(a[0], a[1], a[2], b[0].astype(np.float64), b[1], b[2], cfg["state"], rtol=1e-6)
+
+
 def test_pipeline_short_blocks_only_carry(ctx, b2):
     """Blocks shorter than one FFT fold nothing and are carried forward."""
     cfg = base_cfg(b2, dm=5.0)
