@@ -3,7 +3,7 @@
 dedispersion -> detection -> fold, in complex Msamples/s.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                  [--config c1|c2|c4|c5]
+                  [--config c1|c2|c3|c4|c5]
 
 One step = one block of the workload processed end to end (unpack -> fold),
 the InputBuffering overlap carried from block to block.  Inputs are seeded
@@ -49,6 +49,13 @@ CONFIGS = {
                   "(four blocks = the 2^28-sample data set)"),
         cf=1400.0, bw=256.0, dm=500.0, nchan=1, npol=2, nfft=1 << 16, nbin=2048,
         period=5.757e-3, state=3, ndat=1 << 26, duty=0.03, snr=10.0, sigma=12.0, fb=64),
+    "c3": dict(
+        kind="c3",
+        workload=("48 independent streams at once (beams / DM trials): dual-pol int8 complex "
+                  "baseband at 1400 MHz, DM ~ U[10, 2000], bandwidth in {16, 32, 64, 128} MHz, "
+                  "channels in {1, 8, 32}, FFT 2^12..2^18 per channel (optimal_fft_length), "
+                  "Intensity, 512-4096 bins, 2^24 samples/pol per stream per step"),
+        nstream=48, cf=1400.0, samples=1 << 24, seed=2024),
     "c4": dict(
         kind="sk",
         workload=("spectral kurtosis RFI excision: 512 channels x 2^20 samples x 2 pol complex "
@@ -838,6 +845,281 @@ def run_b200_ifb(args, cfg, world, rank, local):
     ctx.close()
 
 
+# ---------------------------------------------------------------------------
+# Multi-stream workload: many independent beams / DM trials at once
+# ---------------------------------------------------------------------------
+
+def c3_streams(cfg, b2):
+    """The seeded stream list: DM ~ U[10, 2000], bandwidth in {16, 32, 64,
+    128} MHz, channels in {1, 8, 32}, redrawn until the reference's minimum
+    FFT fits 2^18; FFT length by optimal_fft_length within [2^12, 2^18];
+    nbin in {512, 1024, 2048, 4096}; period in [2, 500] ms."""
+    rng = np.random.default_rng(cfg["seed"])
+    out = []
+    while len(out) < cfg["nstream"]:
+        dm = float(rng.uniform(10.0, 2000.0))
+        bw = float(rng.choice([16.0, 32.0, 64.0, 128.0]))
+        nchan = int(rng.choice([1, 8, 32]))
+        pos = b2.smearing_samples(cfg["cf"], bw, dm, nchan, 1)
+        neg = b2.smearing_samples(cfg["cf"], bw, dm, nchan, -1)
+        nmin = b2.minimum_ndat(pos, neg)
+        if nmin > (1 << 18):
+            continue
+        nfft = b2.optimal_fft_length(pos + neg, 1 << 18)
+        nfft = int(min(max(nfft if nfft > 0 else nmin, nmin, 1 << 12), 1 << 18))
+        ndat = cfg["samples"] // nchan
+        if ndat < 2 * nfft:
+            continue
+        out.append(dict(dm=dm, bw=bw, nchan=nchan, pos=pos, neg=neg, nfft=nfft, ndat=ndat,
+                        nbin=int(rng.choice([512, 1024, 2048, 4096])),
+                        period=float(rng.uniform(0.002, 0.5))))
+    return out
+
+
+def c3_cpu_sample(cfg, b2, orc, nstream=4):
+    """Bounded CPU sample: two FFT parts of each of the first streams through
+    the oracle chain unpack -> convolve -> detect -> fold."""
+    streams = c3_streams(cfg, b2)[:nstream]
+    lut, _ = orc.bittable8(0.0308)
+    work = []
+    for k, s in enumerate(streams):
+        nk = s["nfft"] - s["pos"] - s["neg"]
+        ndat = s["nfft"] + nk
+        from dspsr_b200 import synth
+        raw = synth.noise_block(ndat, s["nchan"], 2, 10.0, 10 + k)
+        h = orc.dedispersion_response(cfg["cf"], s["bw"], s["dm"], s["nchan"], s["nfft"],
+                                      input_nchan=s["nchan"])
+        work.append((s, raw, ndat, h))
+
+    def run(threads):
+        t0 = time.perf_counter()
+        n = 0
+        for s, raw, ndat, h in work:
+            x = orc.unpack8(raw, ndat, s["nchan"], 2, 2, lut)
+            x = x.view(np.complex64).reshape(s["nchan"], 2, ndat)
+            z = orc.convolve(x, h, s["nfft"], s["pos"], s["neg"], nthreads=threads)
+            d = orc.detect(z, 0)
+            plan = orc.fold_binplan(0.1, 1e-7, z.shape[2], s["nbin"])
+            orc.fold_accumulate(d, plan, s["nbin"])
+            n += ndat * s["nchan"] * 2
+        return time.perf_counter() - t0, n
+    return run, len(work)
+
+
+def run_reference_c3(args, cfg, world, rank):
+    if rank != 0:
+        return
+    import dspsr_b200 as b2
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    threads = os.cpu_count() or 1
+    run, ns = c3_cpu_sample(cfg, b2, orc)
+    for _ in range(args.warmup):
+        run(threads)
+    total, n = 0.0, 0
+    for _ in range(args.steps):
+        t, k = run(threads)
+        total += t
+        n += k
+    msps = n / total / 1e6
+    line = {
+        "impl": "reference", "metric": "complex Msamples/s unpack->fold, many streams",
+        "value": round(msps, 3), "unit": "complex Msamples/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * total / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Gaussian noise, int8)",
+        "config": {"workload": cfg["workload"], "sample_streams": ns},
+        "cpu_baseline": {"value": round(msps, 3), "unit": "complex Msamples/s", "cores": threads,
+                         "kind": "port",
+                         "sample": (f"two FFT parts of each of the first {ns} streams through "
+                                    "the oracle chain (unpack, overlap-save, detect, fold)")},
+        "e2e": {"value": round(msps, 3), "unit": "complex Msamples/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_b200_c3(args, cfg, world, rank, local):
+    import math
+    import torch
+    import dspsr_b200 as b2
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    streams = c3_streams(cfg, b2)
+    lut, _ = b2.bittable8()
+    gen = torch.Generator(device=device)
+    gen.manual_seed(777 + rank)
+    nblk = 2
+    for s in streams:
+        nbytes = s["ndat"] * s["nchan"] * 2 * 2
+        s["blocks"] = [torch.randint(-40, 40, (nbytes,), generator=gen, device=device,
+                                     dtype=torch.int8).view(torch.uint8) for _ in range(nblk)]
+        s["tstream"] = torch.cuda.Stream(device=device)
+        s["ctx"] = b2.Context(local, s["tstream"].cuda_stream)
+
+    def make_pipe(s, scratch):
+        c = b2.make_config(cfg["cf"], s["bw"], s["dm"], s["nchan"], 2, s["nfft"], s["pos"],
+                           s["neg"], s["nbin"], s["period"], state=b2.INTENSITY, lut=lut,
+                           start_mjd=START_MJD, epoch_mjd=EPOCH_MJD, scratch_bytes=scratch)
+        return b2.Pipeline(s["ctx"], c)
+
+    # autotuner: per shape class (FFT length, channels) the FFT-batch scratch
+    # that runs one block fastest, timed alone on the stream
+    tuned = {}
+    candidates = [64 << 20, 256 << 20, 1024 << 20]
+    t_tune = time.perf_counter()
+    for s in streams:
+        key = (s["nfft"], s["nchan"])
+        if key not in tuned:
+            best = None
+            for sc in candidates:
+                pl = make_pipe(s, sc)
+                for w in range(2):
+                    pl.run(s["blocks"][w % nblk], s["ndat"])
+                st = s["tstream"]
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                pl.run(s["blocks"][0], s["ndat"])
+                e1.record(st)
+                e1.synchronize()
+                ms = e0.elapsed_time(e1)
+                pl.close()
+                if best is None or ms < best[0]:
+                    best = (ms, sc)
+            tuned[key] = best[1]
+        s["scratch"] = tuned[key]
+        s["pipe"] = make_pipe(s, s["scratch"])
+    t_tune = time.perf_counter() - t_tune
+    torch.cuda.synchronize()
+    samples_per_step = sum(s["ndat"] * s["nchan"] * 2 for s in streams)
+
+    def step_batched(i, default):
+        for s in streams:
+            s["tstream"].wait_stream(default)
+        for s in streams:
+            s["pipe"].run(s["blocks"][i % nblk], s["ndat"])
+        for s in streams:
+            default.wait_stream(s["tstream"])
+
+    default = torch.cuda.current_stream()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(1.0)
+    for i in range(args.warmup):
+        step_batched(i, default)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    launches0 = b2.kernel_launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(default)
+    for i in range(args.steps):
+        step_batched(args.warmup + i, default)
+    ev1.record(default)
+    torch.cuda.synchronize()
+    launches = b2.kernel_launches() - launches0
+    clk = clocks.stop()
+    barrier(world)
+    ms = ev0.elapsed_time(ev1)
+    ms_max = max_over_ranks(ms, world)
+    value = samples_per_step * args.steps * world / (ms_max / 1e3) / 1e6
+
+    # the plain path for comparison: the same streams one after another
+    ev0.record(default)
+    for i in range(args.steps):
+        for s in streams:
+            s["tstream"].wait_stream(default)
+            s["pipe"].run(s["blocks"][i % nblk], s["ndat"])
+            default.wait_stream(s["tstream"])
+    ev1.record(default)
+    torch.cuda.synchronize()
+    ms_seq = ev0.elapsed_time(ev1)
+    seq_value = samples_per_step * args.steps / (ms_seq / 1e3) / 1e6
+
+    # end to end: pinned host blocks uploaded by each stream's pipeline
+    host = [s["blocks"][0].cpu().pin_memory() for s in streams]
+    for s, h in zip(streams, host):
+        s["pipe"].run_host(h, s["ndat"])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(default)
+    for i in range(args.steps):
+        for s in streams:
+            s["tstream"].wait_stream(default)
+        for s, h in zip(streams, host):
+            s["pipe"].run_host(h, s["ndat"])
+        for s in streams:
+            default.wait_stream(s["tstream"])
+        profs = [s["pipe"].get_profiles() for s in streams]
+    e1.record(default)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    e2e_ms = max_over_ranks(max(e0.elapsed_time(e1), 1e3 * wall), world)
+    e2e = samples_per_step * args.steps * world / (e2e_ms / 1e3) / 1e6
+    d2h = sum(p.nbytes + h_.nbytes for p, h_ in profs)
+
+    flops = 0.0
+    for s in streams:
+        nk = s["nfft"] - s["pos"] - s["neg"]
+        fps = (s["nfft"] / nk) * (2 * 5 * math.log2(s["nfft"]) + 6) + 5
+        flops += fps * s["ndat"] * s["nchan"] * 2
+    fp32_tflops = flops * args.steps / (ms / 1e3) / 1e12
+    fp32_peak = 148 * 128 * 2 * (clk["sm_mhz"] or 1965.0) * 1e6 / 1e12
+    hbm_peak, _, peak_src = measured_peaks()
+    alg_gbs = 2.0 * samples_per_step * args.steps / (ms / 1e3) / 1e9
+    shapes = sorted({(s["nfft"], s["nchan"]) for s in streams})
+    line = {
+        "metric": "complex Msamples/s unpack->fold, many streams", "value": round(value, 3),
+        "unit": "complex Msamples/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Gaussian noise, int8)",
+        "config": {"workload": cfg["workload"], "streams": len(streams),
+                   "shape_classes": [list(x) for x in shapes],
+                   "tuned_scratch_mib": {f"{k[0]}x{k[1]}": v >> 20 for k, v in tuned.items()},
+                   "autotune_s": round(t_tune, 2),
+                   "plain_sequential_value": round(seq_value, 3),
+                   "batched_over_sequential": round(value / seq_value, 3),
+                   "l2": f"{nblk} distinct blocks per stream ({samples_per_step * 2 >> 20} MiB "
+                         "per step), larger than L2",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "clocks": clk,
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "whole step", "achieved": round(alg_gbs, 2),
+                     "peak": hbm_peak, "unit": "GB/s", "frac": round(alg_gbs / hbm_peak, 4),
+                     "traffic": None, "peak_source": peak_src,
+                     "note": "path is FP32-ALU bound (2 B/sample in); see roofline_fp32"},
+        "roofline_fp32": {"achieved": round(fp32_tflops, 3), "unit": "TFLOP/s",
+                          "peak": round(fp32_peak, 1), "frac": round(fp32_tflops / fp32_peak, 4)},
+        "e2e": {"value": round(e2e, 3), "unit": "complex Msamples/s",
+                "h2d_bytes_per_step": int(sum(h.numel() for h in host)),
+                "d2h_bytes_per_step": int(d2h)},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as orc
+        run, ns = c3_cpu_sample(cfg, b2, orc)
+        threads = os.cpu_count() or 1
+        run(threads)
+        total, n, reps = 0.0, 0, 0
+        while total < 12.0:
+            t, k = run(threads)
+            total += t
+            n += k
+            reps += 1
+        line["cpu_baseline"] = {"value": round(n / total / 1e6, 3), "unit": "complex Msamples/s",
+                                "cores": threads, "kind": "port",
+                                "sample": (f"two FFT parts of each of the first {ns} streams x "
+                                           f"{reps} through the oracle chain, {total:.1f} s")}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for s in streams:
+        s["pipe"].close()
+        s["ctx"].close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -863,10 +1145,10 @@ def main():
     try:
         kind = cfg.get("kind", "path")
         if args.impl == "reference":
-            {"sk": run_reference_sk, "ifb": run_reference_ifb}.get(kind, run_reference)(
-                args, cfg, world, rank)
+            {"sk": run_reference_sk, "ifb": run_reference_ifb, "c3": run_reference_c3}.get(
+                kind, run_reference)(args, cfg, world, rank)
         else:
-            {"sk": run_b200_sk, "ifb": run_b200_ifb}.get(kind, run_b200)(
+            {"sk": run_b200_sk, "ifb": run_b200_ifb, "c3": run_b200_c3}.get(kind, run_b200)(
                 args, cfg, world, rank, local)
     finally:
         if world > 1:
