@@ -1343,6 +1343,32 @@ int dspsr_b200_convolution_perform (dspsr_b200_convolution* c, const float* d_in
   return DSPSR_B200_OK;
 }
 
+int dspsr_b200_convolution_perform_zero_dm (dspsr_b200_convolution* c, const float* d_in,
+                                            uint64_t in_span, uint64_t ndat, float* d_out,
+                                            uint64_t out_span, float* d_zero_dm,
+                                            uint64_t zero_dm_span, uint64_t* npart_out)
+{
+  if (!c) return DSPSR_B200_EINVAL;
+  dspsr_b200_context* ctx = c->ctx;
+  if (!d_zero_dm) return fail (ctx, DSPSR_B200_EINVAL, "perform_zero_dm: null zero-DM output");
+  uint64_t npart = 0;
+  const int rc = dspsr_b200_convolution_perform (c, d_in, in_span, ndat, d_out, out_span, &npart);
+  if (npart_out) *npart_out = npart;
+  if (rc) return rc;
+  const ConvShape& sh = c->shape;
+  const uint64_t n = npart * sh.nkeep;
+  if (zero_dm_span < n)
+    return fail (ctx, DSPSR_B200_EINVAL, "perform_zero_dm: zero_dm_span < npart*nkeep");
+  if (n)
+    // Convolution.C:789-796: the input samples aligned with the output
+    B200_CHECK (ctx, cudaMemcpy2DAsync (d_zero_dm, zero_dm_span * sizeof (float2),
+                                        d_in + 2 * uint64_t (sh.nfilt_pos),
+                                        in_span * sizeof (float2), n * sizeof (float2),
+                                        uint64_t (sh.nchan) * sh.npol, cudaMemcpyDeviceToDevice,
+                                        ctx->stream), "zero-DM copy");
+  return DSPSR_B200_OK;
+}
+
 // ---- detection -------------------------------------------------------------
 
 int dspsr_b200_detect (dspsr_b200_context* ctx, const float* d_in, uint64_t in_span,

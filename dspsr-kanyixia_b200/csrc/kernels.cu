@@ -479,22 +479,48 @@ k_rows_tma (float2* __restrict__ scratch, const float2* __restrict__ ptab,
     }
     if constexpr (CONV)
     {
+      // forward passes but the last
       tpass<N2, -1, 1, true, true> (work, work, v, tab);
-      tpass<N2, -1, 2, true, true> (work, work, v, tab);
-      tpass<N2, -1, 3, true, true> (work, work, v, tab);
-
+      if constexpr (NP == 4) tpass<N2, -1, 2, true, true> (work, work, v, tab);
+      // The last forward pass leaves in thread tid exactly the 16 values that
+      // the first inverse pass needs in that thread (x[tid + m T], m < 16), so
+      // the response multiply and the inverse pass-0 butterfly follow in
+      // registers, with no shared-memory round trip between them.
+      constexpr int PL = NP - 1;
+      constexpr int RL = stockham_radix (N2, PL);
+      constexpr int NsL = stockham_ns (N2, PL);
+      constexpr int BPT = (N2 / RL) / T;
+      StockhamPassT<N2, RL, T, -1, true, true>::load (tid, work, v);
+      __syncthreads ();
+      const float2* twp = tab + pass_table_offset (N2, PL);
+#pragma unroll
+      for (int bb = 0; bb < BPT; bb++)
+      {
+        const int j = tid + bb * T;
+        const int a = j & (NsL - 1);
+        float2* x = v + bb * RL;
+#pragma unroll
+        for (int r = 1; r < RL; r++) x[r] = cmul (x[r], twp[(r - 1) * NsL + a]);
+        RegDFT<RL, -1>::run (x);
+      }
       // Response::operate (Response.C:662-726): (f_r d_r - f_i d_i, f_i d_r + f_r d_i)
       const float2* h = H + (uint64_t (c) * n1 + k1) * N2;
+      float2 u[16];
 #pragma unroll
-      for (int q = 0; q < 16; q++)
-      {
-        const int i = tid + q * T;
-        const float2 d = work[spad (i)];
-        const float2 f = __ldg (h + i);
-        work[spad (i)] = make_float2 (d.x * f.x - d.y * f.y, d.x * f.y + d.y * f.x);
-      }
+      for (int bb = 0; bb < BPT; bb++)
+#pragma unroll
+        for (int r = 0; r < RL; r++)
+        {
+          const int m = bb + r * (16 / RL);
+          const float2 d = v[bb * RL + r];
+          const float2 f = __ldg (h + tid + m * T);
+          u[m] = make_float2 (d.x * f.x - d.y * f.y, d.x * f.y + d.y * f.x);
+        }
+      static_assert (stockham_radix (N2, 0) == 16, "inverse pass 0 must be radix 16");
+      RegDFT<16, +1>::run (u);
+#pragma unroll
+      for (int r = 0; r < 16; r++) work[spad (tid * 16 + r)] = u[r];
       __syncthreads ();
-      tpass<N2, +1, 0, true, true> (work, work, v, tab);
     }
 
     // inverse: all but the last pass in shared memory, the last straight to HBM

@@ -244,6 +244,13 @@ class Convolution:
             "convolution_perform")
         return n.value
 
+    def perform_zero_dm(self, d_in, in_span, ndat, d_out, out_span, d_zero_dm, zero_dm_span):
+        n = ctypes.c_uint64()
+        self.ctx.check(self._lib.dspsr_b200_convolution_perform_zero_dm(
+            self.handle, _ptr(d_in), in_span, ndat, _ptr(d_out), out_span, _ptr(d_zero_dm),
+            zero_dm_span, ctypes.byref(n)), "convolution_perform_zero_dm")
+        return n.value
+
     def close(self):
         if self.handle:
             self._lib.dspsr_b200_convolution_destroy(self.handle)

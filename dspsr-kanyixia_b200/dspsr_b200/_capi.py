@@ -115,6 +115,8 @@ SIGNATURES = {
     "dspsr_b200_filterbank": (c_int, [c_vp, c_int, c_vp, c_u64, c_u64, c_uint, c_uint, c_uint,
                                       c_fp, c_int, c_vp, c_u64, c_u64p]),
     "dspsr_b200_convolution_perform": (c_int, [c_vp, c_vp, c_u64, c_u64, c_vp, c_u64, c_u64p]),
+    "dspsr_b200_convolution_perform_zero_dm": (c_int, [c_vp, c_vp, c_u64, c_u64, c_vp, c_u64, c_vp,
+                                                       c_u64, c_u64p]),
     "dspsr_b200_detect": (c_int, [c_vp, c_vp, c_u64, c_u64, c_uint, c_int, c_vp, c_u64]),
     "dspsr_b200_inverse_filterbank_create": (c_int, [c_vp, ctypes.POINTER(IfbConfig),
                                                      ctypes.POINTER(c_vp)]),

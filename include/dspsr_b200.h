@@ -214,6 +214,15 @@ int dspsr_b200_convolution_set_temporal_apodization (dspsr_b200_convolution* con
 int dspsr_b200_convolution_perform (dspsr_b200_convolution* conv, const float* d_in,
                                     uint64_t in_span, uint64_t ndat, float* d_out,
                                     uint64_t out_span, uint64_t* npart);
+/* Engine::perform(input, output, zero_DM_output, npart) (Convolution.C:690-698,
+   789-796): as dspsr_b200_convolution_perform, and the zero-DM output -- the
+   undispersed input samples aligned with the output, nfilt_pos after the
+   start of each part -- copied to d_zero_dm (complex FPT spans of
+   zero_dm_span samples). */
+int dspsr_b200_convolution_perform_zero_dm (dspsr_b200_convolution* conv, const float* d_in,
+                                            uint64_t in_span, uint64_t ndat, float* d_out,
+                                            uint64_t out_span, float* d_zero_dm,
+                                            uint64_t zero_dm_span, uint64_t* npart);
 
 /* ---------------------------------------------------------------------- */
 /* Filterbank::Engine without convolution (freq_res = 1): CUDA::FilterbankEngine*/

@@ -343,3 +343,31 @@ def test_convolution_rejects_bad_shapes(ctx, b2):
         c.perform(x, 5000, 5000, out, 10)               # output too small
     assert c.perform(x, 5000, 100, out, 10) == 0       # fewer samples than one FFT
     c.close()
+
+
+@pytest.mark.parametrize("nfft,pos,neg", [(8192, 100, 200), (1 << 15, 0, 0), (1 << 16, 3000, 1000)])
+def test_convolution_zero_dm_output_is_input(ctx, b2, orc, nfft, pos, neg):
+    """test_Convolution.cpp:151-186: the zero-DM output equals the input,
+    sample for sample (here: the input samples aligned with the output)."""
+    nchan, npol = 2, 2
+    nk = nfft - pos - neg
+    ndat = 3 * nk + pos + neg + 17
+    rng = np.random.default_rng(nfft)
+    x = (rng.standard_normal((nchan, npol, ndat)) +
+         1j * rng.standard_normal((nchan, npol, ndat))).astype(np.complex64)
+    resp = np.exp(1j * rng.uniform(0, 2 * np.pi, (nchan, nfft))).astype(np.complex64)
+    conv = b2.Convolution(ctx, nchan, npol, nfft, pos, neg)
+    conv.copy_response(resp)
+    d_in = dev(x.view(np.float32))
+    out = torch.zeros((nchan, npol, 3 * nk, 2), device="cuda")
+    zdm = torch.full((nchan, npol, 3 * nk + 5, 2), float("nan"), device="cuda")
+    out2 = torch.zeros_like(out)
+    n = conv.perform_zero_dm(d_in, ndat, ndat, out, 3 * nk, zdm, 3 * nk + 5)
+    conv.perform(d_in, ndat, ndat, out2, 3 * nk)
+    ctx.synchronize()
+    assert n == 3
+    z = zdm.cpu().numpy().view(np.complex64)[..., 0]
+    assert z[:, :, :3 * nk].tobytes() == x[:, :, pos:pos + 3 * nk].tobytes()
+    assert np.isnan(z[:, :, 3 * nk:].view(np.float32)).all()
+    assert out.cpu().numpy().tobytes() == out2.cpu().numpy().tobytes()
+    conv.close()
