@@ -26,6 +26,8 @@ struct dspsr_b200_context
   cudaStream_t stream = nullptr;
   std::string error;
   float* d_lut = nullptr;     // scratch LUT for the standalone unpacker
+  float2* d_fb_tab = nullptr; // pass tables of the standalone filterbank's FFT
+  unsigned fb_tab_n = 0;      // ... for this transform length
 };
 
 namespace {
@@ -53,6 +55,26 @@ int cuda_fail (dspsr_b200_context* ctx, cudaError_t err, const char* where)
   } while (0)
 
 bool is_pow2 (uint64_t x) { return x && !(x & (x - 1)); }
+
+// Per-pass Stockham tables of an n-point transform uploaded into a device
+// buffer (the shared-memory filterbank's twiddles).
+cudaError_t upload_pass_tables (unsigned n, float2** dst, size_t* cap)
+{
+  const unsigned cnt = pass_tables_count (n);
+  std::vector<float2> t (std::max (cnt, 1u), make_float2 (0.f, 0.f));
+  make_pass_tables (n, t.data (), cnt);
+  if (*cap < t.size ())
+  {
+    if (*dst) cudaFree (*dst);
+    *dst = nullptr;
+    *cap = 0;
+    cudaError_t e = cudaMalloc (dst, t.size () * sizeof (float2));
+    if (e != cudaSuccess) return e;
+    *cap = t.size ();
+  }
+  return cudaMemcpy (*dst, t.data (), t.size () * sizeof (float2), cudaMemcpyHostToDevice);
+}
+
 
 // Device buffer owned by an engine object.
 template <typename T>
@@ -451,6 +473,8 @@ struct dspsr_b200_pipeline
   double rate = 0;                  // complex sampling rate of the convolved channels
   unsigned fb_nsub = 0;             // filterbank channels per input channel (0: none)
   DevBuf<float2> fbbuf;             // filterbank output, FPT
+  float2* fb_tab = nullptr;         // pass tables of the filterbank FFT (fb_nsub >= 128)
+  size_t fb_tab_cap = 0;
 };
 
 namespace {
@@ -595,7 +619,7 @@ int pipeline_input (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat, ui
   const float scale = float (1.0 / std::sqrt (double (pl->fb_nsub)));
   KernelClock kc {&PipeClock::mark, &pl->clock};
   B200_CHECK (ctx, launch_filterbank (in, pl->conv.lut.ptr, pl->fb_nsub, nb, scale, pl->fbbuf.ptr,
-                                      nb, ctx->stream, pl->clock.on ? &kc : nullptr),
+                                      nb, ctx->stream, pl->clock.on ? &kc : nullptr, pl->fb_tab),
               "filterbank");
   return pipeline_block (pl, pl->fbbuf.ptr, nb, nb, ndat_folded);
 }
@@ -1007,6 +1031,7 @@ int dspsr_b200_context_destroy (dspsr_b200_context* ctx)
 {
   if (!ctx) return DSPSR_B200_EINVAL;
   if (ctx->d_lut) cudaFree (ctx->d_lut);
+  if (ctx->d_fb_tab) cudaFree (ctx->d_fb_tab);
   delete ctx;
   return DSPSR_B200_OK;
 }
@@ -1247,8 +1272,16 @@ int dspsr_b200_filterbank (dspsr_b200_context* ctx, int input_kind, const void* 
     return fail (ctx, DSPSR_B200_EINVAL, "filterbank: invalid argument");
   if (input_kind < 0 || input_kind > 2 || (input_kind == DSPSR_B200_INT8_TFPD && !lut256))
     return fail (ctx, DSPSR_B200_EINVAL, "filterbank: invalid input kind or missing table");
-  if (!(nsub == 4 || nsub == 8 || nsub == 16 || nsub == 32 || nsub == 64))
-    return fail (ctx, DSPSR_B200_EINVAL, "filterbank: nsub=%u not in {4,...,64}", nsub);
+  if (!is_pow2 (nsub) || nsub < 4 || nsub > 4096)
+    return fail (ctx, DSPSR_B200_EINVAL, "filterbank: nsub=%u not a power of two in [4, 4096]",
+                 nsub);
+  if (nsub >= 128 && ctx->fb_tab_n != nsub)
+  {
+    size_t cap = ctx->fb_tab_n ? pass_tables_count (ctx->fb_tab_n) : 0;
+    B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "sync before table upload");
+    B200_CHECK (ctx, upload_pass_tables (nsub, &ctx->d_fb_tab, &cap), "filterbank tables");
+    ctx->fb_tab_n = nsub;
+  }
   if (input_kind == DSPSR_B200_FLOAT_FPT && in_span < ndat)
     return fail (ctx, DSPSR_B200_EINVAL, "filterbank: in_span < ndat");
   const uint64_t nblk = ndat / nsub;
@@ -1266,8 +1299,8 @@ int dspsr_b200_filterbank (dspsr_b200_context* ctx, int input_kind, const void* 
   in.offset_binary = offset_binary;
   const float scale = float (1.0 / std::sqrt (double (nsub)));
   B200_CHECK (ctx, launch_filterbank (in, ctx->d_lut, nsub, nblk, scale,
-                                      reinterpret_cast<float2*> (d_out), out_span, ctx->stream),
-              "filterbank");
+                                      reinterpret_cast<float2*> (d_out), out_span, ctx->stream,
+                                      nullptr, ctx->d_fb_tab), "filterbank");
   if (ndat_out) *ndat_out = nblk;
   return DSPSR_B200_OK;
 }
@@ -1492,12 +1525,18 @@ int dspsr_b200_pipeline_create (dspsr_b200_context* ctx, const dspsr_b200_pipeli
   const uint64_t bytes_per_value = cfg->input_kind == DSPSR_B200_INT16_TFPD ? 2 : 1;
   pl->bytes_per_sample = uint64_t (cfg->nchan) * cfg->npol * 2 * bytes_per_value;
   const unsigned fb = cfg->filterbank_nchan > 1 ? cfg->filterbank_nchan : 0;
-  if (fb && !(fb == 4 || fb == 8 || fb == 16 || fb == 32 || fb == 64))
+  if (fb && (!is_pow2 (fb) || fb < 4 || fb > 4096))
   {
     delete pl;
-    return fail (ctx, DSPSR_B200_EINVAL, "pipeline: filterbank_nchan=%u not in {4,...,64}", fb);
+    return fail (ctx, DSPSR_B200_EINVAL,
+                 "pipeline: filterbank_nchan=%u not a power of two in [4, 4096]", fb);
   }
   pl->fb_nsub = fb;
+  if (fb >= 128 && upload_pass_tables (fb, &pl->fb_tab, &pl->fb_tab_cap) != cudaSuccess)
+  {
+    delete pl;
+    return fail (ctx, DSPSR_B200_ECUDA, "pipeline: filterbank tables");
+  }
   // channels the convolution sees
   const unsigned nchan = fb ? cfg->nchan * fb : cfg->nchan;
   pl->rate = std::fabs (cfg->bandwidth_mhz) / double (nchan) * 1e6;
@@ -1555,6 +1594,7 @@ int dspsr_b200_pipeline_destroy (dspsr_b200_pipeline* pl)
   pl->carry[1].release ();
   pl->staging[0].release ();
   pl->staging[1].release ();
+  if (pl->fb_tab) cudaFree (pl->fb_tab);
   if (pl->copy_stream) cudaStreamSynchronize (pl->copy_stream);
   for (int i = 0; i < 2; i++)
   {

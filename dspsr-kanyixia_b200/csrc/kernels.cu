@@ -982,6 +982,119 @@ k_filterbank (const InputView in, const float* __restrict__ lut, const uint64_t 
                                                          __fmul_rn (scale, v[k].y));
 }
 
+// The same filterbank for NSUB = 128 .. 4096 with the transforms in shared
+// memory: a CTA of FB_THREADS threads takes F = 8192/NSUB (block, pol) slots of
+// one input channel, reads their samples in address order (coalesced), runs
+// one NSUB-point FFT per group of NSUB/16 threads (per-pass twiddle tables in
+// shared memory), and writes the bins channel by channel, consecutive threads
+// on consecutive output samples.
+constexpr int FB_THREADS = 512;
+
+template <int NSUB, int KIND>
+__global__ void __launch_bounds__ (FB_THREADS)
+k_filterbank_smem (const InputView in, const float* __restrict__ lut, const float2* __restrict__ ptab,
+                   const uint64_t nblk, const float scale, float2* __restrict__ out,
+                   const uint64_t out_span)
+{
+  constexpr int TF = stockham_threads (NSUB);
+  constexpr int F = FB_THREADS / TF;
+  // odd slot stride (in float2): the output loop reads one bin of consecutive
+  // slots, which then fall on different banks
+  constexpr int SP = spad_size (NSUB) + 1;
+  constexpr int TABN = pass_tables_size (NSUB);
+  extern __shared__ float2 s_fb[];                 // [F][SP], then the pass tables
+  float2* s_tab = s_fb + F * SP;
+  __shared__ float s_lut[256];
+  const unsigned npol = in.npol;
+  const unsigned bpc = F / npol;                    // blocks per CTA
+  const uint64_t blk0 = uint64_t (blockIdx.x) * bpc;
+  const unsigned cin = blockIdx.y;
+  const unsigned nb = unsigned (min (uint64_t (bpc), nblk - blk0));
+  load_lut (in, lut, s_lut);
+  for (int i = threadIdx.x; i < TABN; i += FB_THREADS) s_tab[i] = __ldg (ptab + i);
+  __syncthreads ();
+  const uint64_t t0 = blk0 * NSUB;
+  // element e in address order: TFPD (t, pol) pairs, FPT (pol, t); all PER
+  // loads of a thread are issued before any is used
+  constexpr int PER = F * NSUB / FB_THREADS;
+  constexpr unsigned HALF = F * NSUB / 2;          // samples per pol when npol == 2
+  const bool two = npol == 2;
+  const uint64_t rowv = uint64_t (in.nchan) * npol;  // TFPD values per time sample
+  uint32_t word[PER];
+  float2 fv[KIND == IN_FLOAT ? PER : 1];
+#pragma unroll
+  for (int k = 0; k < PER; k++)
+  {
+    const unsigned e = threadIdx.x + k * FB_THREADS;
+    if constexpr (KIND == IN_FLOAT)
+    {
+      const unsigned p = two ? e / HALF : 0, t = two ? e % HALF : e;
+      fv[k] = t / NSUB < nb ? __ldg (static_cast<const float2*> (in.main)
+                                     + (uint64_t (cin) * npol + p) * in.main_span + t0 + t)
+                            : make_float2 (0.f, 0.f);
+    }
+    else
+    {
+      const unsigned p = two ? (e & 1) : 0, t = two ? e >> 1 : e;
+      const uint64_t idx = (t0 + t) * rowv + uint64_t (cin) * npol + p;
+      if constexpr (KIND == IN_INT16)
+        word[k] = t / NSUB < nb ? __ldg (static_cast<const uint32_t*> (in.main) + idx) : 0u;
+      else
+        word[k] = t / NSUB < nb ? __ldg (static_cast<const unsigned short*> (in.main) + idx) : 0u;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < PER; k++)
+  {
+    const unsigned e = threadIdx.x + k * FB_THREADS;
+    unsigned p, t;
+    float2 x;
+    if constexpr (KIND == IN_FLOAT)
+    {
+      p = two ? e / HALF : 0;
+      t = two ? e % HALF : e;
+      x = fv[k];
+    }
+    else
+    {
+      p = two ? (e & 1) : 0;
+      t = two ? e >> 1 : e;
+      if constexpr (KIND == IN_INT16)
+      {
+        short re = short (word[k] & 0xffff), im = short (word[k] >> 16);
+        if (in.offset_binary)
+        {
+          re = short (re ^ 0x8000);
+          im = short (im ^ 0x8000);
+        }
+        // SixteenBitUnpacker.C:69: float(x) + 0.5
+        x = make_float2 (__fadd_rn (float (re), 0.5f), __fadd_rn (float (im), 0.5f));
+      }
+      else
+        x = make_float2 (s_lut[word[k] & 0xff], s_lut[word[k] >> 8]);
+    }
+    const unsigned blk = t / NSUB, i = t % NSUB;
+    if (blk >= nb) x = make_float2 (0.f, 0.f);
+    s_fb[(blk * npol + p) * SP + spad (i)] = x;
+  }
+  __syncthreads ();
+  const unsigned group = threadIdx.x / TF, tid = threadIdx.x % TF;
+  {
+    float2 v[NSUB / TF];
+    group_fft_pass<NSUB, TF, -1, 0> (s_fb + group * SP, v, s_tab, tid);
+  }
+  // bins out: channel cin*NSUB + k of pol p, sample blk0 + blk
+  for (unsigned e = threadIdx.x; e < unsigned (F * NSUB); e += FB_THREADS)
+  {
+    const unsigned blk = e % bpc, rest = e / bpc;
+    const unsigned p = rest % npol, k = rest / npol;
+    if (blk >= nb || k >= NSUB) continue;
+    const float2 y = s_fb[(blk * npol + p) * SP + spad (k)];
+    out[((uint64_t (cin) * NSUB + k) * npol + p) * out_span + blk0 + blk] =
+        make_float2 (__fmul_rn (scale, y.x), __fmul_rn (scale, y.y));
+  }
+}
+
 // SpectralKurtosis::transformation for one resolution with noverlap = 1:
 // compute (SpectralKurtosis.C:674-798), detect_skfb (:1105-1222) and mask
 // (:1465-1566).  A CTA takes up to U consecutive M-sample blocks of one
@@ -1587,13 +1700,67 @@ cudaError_t run_filterbank (const InputView& in, const float* d_lut, uint64_t nb
     k_filterbank<NSUB, IN_FLOAT><<<grid, 128, 0, st>>> (in, d_lut, nblk, scale, out, out_span);
   return cudaGetLastError ();
 }
+template <int NSUB>
+cudaError_t run_filterbank_smem (const InputView& in, const float* d_lut, const float2* ptab,
+                                 uint64_t nblk, float scale, float2* out, uint64_t out_span,
+                                 cudaStream_t st, const KernelClock* clk)
+{
+  constexpr int F = FB_THREADS / stockham_threads (NSUB);
+  const unsigned bpc = F / in.npol;
+  const size_t smem = (size_t (F) * (spad_size (NSUB) + 1) + pass_tables_size (NSUB)) *
+                      sizeof (float2);
+  const dim3 grid (unsigned ((nblk + bpc - 1) / bpc), in.nchan);
+  ClockScope cs (clk, KK_FILTERBANK, st);
+  cudaError_t e;
+  if (in.kind == IN_INT8)
+  {
+    e = cudaFuncSetAttribute (k_filterbank_smem<NSUB, IN_INT8>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, int (smem));
+    if (e == cudaSuccess)
+      k_filterbank_smem<NSUB, IN_INT8><<<grid, FB_THREADS, smem, st>>> (in, d_lut, ptab, nblk,
+                                                                        scale, out, out_span);
+  }
+  else if (in.kind == IN_INT16)
+  {
+    e = cudaFuncSetAttribute (k_filterbank_smem<NSUB, IN_INT16>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, int (smem));
+    if (e == cudaSuccess)
+      k_filterbank_smem<NSUB, IN_INT16><<<grid, FB_THREADS, smem, st>>> (in, d_lut, ptab, nblk,
+                                                                         scale, out, out_span);
+  }
+  else
+  {
+    e = cudaFuncSetAttribute (k_filterbank_smem<NSUB, IN_FLOAT>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, int (smem));
+    if (e == cudaSuccess)
+      k_filterbank_smem<NSUB, IN_FLOAT><<<grid, FB_THREADS, smem, st>>> (in, d_lut, ptab, nblk,
+                                                                         scale, out, out_span);
+  }
+  if (e != cudaSuccess) return e;
+  return cudaGetLastError ();
+}
 } // namespace
 
 cudaError_t launch_filterbank (const InputView& in, const float* d_lut, unsigned nsub,
                                uint64_t nblk, float scale, float2* out, uint64_t out_span,
-                               cudaStream_t st, const KernelClock* clk)
+                               cudaStream_t st, const KernelClock* clk, const float2* ptab)
 {
   if (nblk == 0) return cudaSuccess;
+  // up to 64 channels the one-thread-per-block register transform is faster
+  if (nsub >= 128)
+  {
+    if (!ptab) return cudaErrorInvalidValue;
+    switch (nsub)
+    {
+      case 128: return run_filterbank_smem<128> (in, d_lut, ptab, nblk, scale, out, out_span, st, clk);
+      case 256: return run_filterbank_smem<256> (in, d_lut, ptab, nblk, scale, out, out_span, st, clk);
+      case 512: return run_filterbank_smem<512> (in, d_lut, ptab, nblk, scale, out, out_span, st, clk);
+      case 1024: return run_filterbank_smem<1024> (in, d_lut, ptab, nblk, scale, out, out_span, st, clk);
+      case 2048: return run_filterbank_smem<2048> (in, d_lut, ptab, nblk, scale, out, out_span, st, clk);
+      case 4096: return run_filterbank_smem<4096> (in, d_lut, ptab, nblk, scale, out, out_span, st, clk);
+      default: return cudaErrorInvalidValue;
+    }
+  }
   switch (nsub)
   {
     case 4: return run_filterbank<4> (in, d_lut, nblk, scale, out, out_span, st, clk);

@@ -109,12 +109,14 @@ cudaError_t launch_permute_response (float2* H, const float2* src, unsigned ncha
 cudaError_t launch_unpermute_response (float2* dst, const float2* H, unsigned nchan,
                                        unsigned n1, unsigned n2, cudaStream_t stream);
 
-// FFT filterbank, freq_res = 1: nsub in {4, 8, 16, 32, 64}; nblk blocks of
-// nsub input samples per (input channel, pol); output FPT with channel
-// cin*nsub + k, span out_span.
+// FFT filterbank, freq_res = 1: nsub a power of two in [4, 4096]; nblk blocks
+// of nsub input samples per (input channel, pol); output FPT with channel
+// cin*nsub + k, span out_span.  nsub >= 128 runs the transforms in shared
+// memory and needs the per-pass tables of the nsub-point FFT (ptab).
 cudaError_t launch_filterbank (const InputView& in, const float* d_lut, unsigned nsub,
                                uint64_t nblk, float scale, float2* out, uint64_t out_span,
-                               cudaStream_t stream, const KernelClock* clock = nullptr);
+                               cudaStream_t stream, const KernelClock* clock = nullptr,
+                               const float2* ptab = nullptr);
 
 // InverseFilterbank: per part, forward FFT of lin samples of every fine
 // channel, the kept bins stitched into the spectra of the output channels

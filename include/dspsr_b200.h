@@ -234,7 +234,8 @@ int dspsr_b200_convolution_perform_zero_dm (dspsr_b200_convolution* conv, const 
    sample in nsub output channels: out channel cin*nsub + k = FFT bin k scaled
    by 1/sqrt(nsub) (Filterbank::prepare_normalizer).  Input as input_kind
    (TFPD int8/int16 or complex-float FPT with in_span); the unpack is fused.
-   Output complex-float FPT, (chan*npol + pol)*out_span.  nsub in {4,...,64}.
+   Output complex-float FPT, (chan*npol + pol)*out_span.  nsub a power of two
+   in [4, 4096].
    Returns ndat/nsub output samples; a trailing partial block is ignored. */
 int dspsr_b200_filterbank (dspsr_b200_context* ctx, int input_kind, const void* d_in,
                            uint64_t ndat, uint64_t in_span, unsigned nchan_in, unsigned npol,
@@ -254,7 +255,7 @@ int dspsr_b200_filterbank (dspsr_b200_context* ctx, int input_kind, const void* 
    which must be n1 * 4096 or n1 * 8192 with n1 in {2,3,4,6,8,12,16,24,32}.
    Output discards are given (from the response); the input discards follow
    by output_to_input (InverseFilterbank.C:128-142).  scratch_bytes bounds the
-   device scratch (0 = 96 MiB). */
+   device scratch (0 = 512 MiB). */
 typedef struct dspsr_b200_ifb_config
 {
   unsigned input_nchan;
@@ -396,7 +397,8 @@ typedef struct
   uint64_t scratch_bytes;
   /* FFT filterbank stage in front of the dedispersion (Filterbank with
      freq_res = 1, Filterbank.C:75-570): channels per input channel, 0 or 1 =
-     none, else 4..64; blocks must then be multiples of it */
+     none, else a power of two in [4, 4096]; blocks must then be multiples
+     of it */
   unsigned filterbank_nchan;
 } dspsr_b200_pipeline_config;
 
