@@ -3,7 +3,7 @@
 dedispersion -> detection -> fold, in complex Msamples/s.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                  [--config c1|c2|c3|c4|c5]
+                  [--config c1|c2|c3|c4|c5|c5ifb]
 
 One step = one block of the workload processed end to end (unpack -> fold),
 the InputBuffering overlap carried from block to block.  Inputs are seeded
@@ -64,12 +64,20 @@ CONFIGS = {
                   "3 sigma thresholds (SKLimits), sums + mask + masked copy"),
         nchan=512, npol=2, ndat=1 << 20, M=1024, std_devs=3.0),
     "c5": dict(
+        kind="c5",
+        workload=("inverse PFB then re-channelised coherent dedispersion: 256 critically "
+                  "spaced 4/3-oversampled PFB channels of int16 complex dual-pol voltages "
+                  "(seeded Gaussian), 1024-point input FFTs stitched into 196608-point "
+                  "spectra (12288-sample discards), FFT filterbank to 1024 channels, DM 1000 "
+                  "at 1400 MHz over 800 MHz, per-channel overlap-save, full Stokes, "
+                  "4096-bin fold, P=1.6 ms; 1 s of 800 MHz per block (4.17 M samples per "
+                  "PFB channel)"),
+        nin=256, npol=2, lin=1024, disc=12288, ndat=4166784, cf=1400.0, bw=800.0, dm=1000.0,
+        fb=1024, nbin=4096, period=1.6e-3),
+    "c5ifb": dict(
         kind="ifb",
-        workload=("inverse filterbank stage: 256 critically spaced 4/3-oversampled PFB "
-                  "channels of int16 complex dual-pol voltages (seeded Gaussian), 1024-point "
-                  "input FFTs, 768 kept bins, stitched into one 196608-point spectrum, "
-                  "12288-sample output discards each side; 1 s of 800 MHz per block "
-                  "(4.17 M samples per fine channel)"),
+        workload=("inverse filterbank stage of C5 alone: 256 PFB channels int16 dual-pol, "
+                  "1024-point input FFTs, 196608-point output spectra, 1 s of 800 MHz"),
         nin=256, npol=2, lin=1024, disc=12288, ndat=4166784),
 }
 
@@ -1120,6 +1128,180 @@ def run_b200_c3(args, cfg, world, rank, local):
         s["ctx"].close()
 
 
+def c5_plan(cfg, b2):
+    """Re-channelised dedispersion plan of the C5 chain (per output channel)."""
+    nc = cfg["fb"]
+    pos = b2.smearing_samples(cfg["cf"], cfg["bw"], cfg["dm"], nc, 1)
+    neg = b2.smearing_samples(cfg["cf"], cfg["bw"], cfg["dm"], nc, -1)
+    nmin = b2.minimum_ndat(pos, neg)
+    nfft = b2.optimal_fft_length(pos + neg, 1 << 16)
+    nfft = int(min(max(nfft if nfft > 0 else nmin, nmin, 8192), 1 << 16))
+    return pos, neg, nfft
+
+
+def run_reference_c5(args, cfg, world, rank):
+    """The chain on the CPU for a bounded sample: inverse filterbank (oracle,
+    all threads over parts) -> 1024-channel filterbank -> overlap-save ->
+    Stokes -> fold."""
+    if rank != 0:
+        return
+    import dspsr_b200 as b2
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    threads = os.cpu_count() or 1
+    c = ifb_cfg_dict(cfg)
+    keep, lout, ipos, ineg, in_step, out_step = orc.ifb_sizes(c)
+    pos, neg, nfft = c5_plan(cfg, b2)
+    nc = cfg["fb"]
+    need = (nfft + 16) * nc                     # one FFT part per channel
+    nparts = -(-need // out_step)
+    ndat = nparts * in_step + ipos + ineg
+    rng = np.random.default_rng(3)
+    x = (rng.standard_normal((cfg["nin"], cfg["npol"], ndat)) * 100 +
+         1j * rng.standard_normal((cfg["nin"], cfg["npol"], ndat)) * 100).astype(np.complex64)
+    freqs = orc.channel_centres(cfg["cf"], cfg["bw"], nc, swap=True, dc_centred=True)
+    h = orc.dedispersion_response_channels(freqs, cfg["bw"], cfg["dm"], nfft, mode=0)
+
+    def step():
+        t0 = time.perf_counter()
+        w = orc.inverse_filterbank(x, c)
+        n = (w.shape[2] // nc) * nc
+        y = orc.filterbank(w[:, :, :n], nc)
+        z = orc.convolve(y, h, nfft, pos, neg, nthreads=threads)
+        d = orc.detect(z, 3)
+        plan = orc.fold_binplan(0.2, 1e-6, z.shape[2], cfg["nbin"])
+        orc.fold_accumulate(d, plan, cfg["nbin"])
+        return time.perf_counter() - t0
+    for _ in range(args.warmup):
+        step()
+    total = sum(step() for _ in range(args.steps))
+    msps = cfg["nin"] * cfg["npol"] * nparts * in_step * args.steps / total / 1e6
+    line = {
+        "impl": "reference", "metric": "complex Msamples/s inverse filterbank->fold",
+        "value": round(msps, 3), "unit": "complex Msamples/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * total / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Gaussian complex voltages)",
+        "config": {"workload": cfg["workload"], "sample_ifb_parts_per_step": nparts},
+        "cpu_baseline": {"value": round(msps, 3), "unit": "complex Msamples/s", "cores": threads,
+                         "kind": "port",
+                         "sample": (f"{nparts} inverse-filterbank parts of {cfg['nin']} "
+                                    f"channels x {cfg['npol']} pol (one FFT part per output "
+                                    "channel) through the oracle chain")},
+        "e2e": {"value": round(msps, 3), "unit": "complex Msamples/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_b200_c5(args, cfg, world, rank, local):
+    import math
+    import torch
+    import dspsr_b200 as b2
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    ctx = b2.Context(local)
+    ifb = b2.InverseFilterbank(ctx, cfg["nin"], 1, cfg["nin"], cfg["npol"], cfg["lin"],
+                               os=(4, 3), output_discard=(cfg["disc"], cfg["disc"]))
+    info = ifb.info
+    in_step, out_step = info["in_step"], info["out_step"]
+    ndat = cfg["ndat"]
+    npart = ifb.npart(ndat)
+    nwide = npart * out_step
+    pos, neg, nfft = c5_plan(cfg, b2)
+    pcfg = b2.make_config(cfg["cf"], cfg["bw"], cfg["dm"], 1, cfg["npol"], nfft, pos, neg,
+                          cfg["nbin"], cfg["period"], state=b2.STOKES, input_kind=b2.FLOAT_FPT,
+                          start_mjd=START_MJD, epoch_mjd=EPOCH_MJD, filterbank_nchan=cfg["fb"])
+    pipe = b2.Pipeline(ctx, pcfg)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(99 + rank)
+    raw = torch.empty((ndat, cfg["nin"], cfg["npol"], 2), dtype=torch.int16, device=device)
+    chunk = 1 << 18
+    for t0 in range(0, ndat, chunk):
+        n = min(chunk, ndat - t0)
+        raw[t0:t0 + n] = (torch.randn((n, cfg["nin"], cfg["npol"], 2), generator=gen,
+                                      device=device) * 100).round().to(torch.int16)
+    raw = raw.reshape(-1)
+    wide = torch.empty((1, cfg["npol"], nwide, 2), dtype=torch.float32, device=device)
+    samples_per_step = cfg["nin"] * cfg["npol"] * npart * in_step
+    default = torch.cuda.current_stream()
+
+    def step(evs=None):
+        if evs:
+            evs[0].record(default)
+        ifb.perform(raw, ndat, wide, nwide, input_kind=b2.INT16_TFPD)
+        if evs:
+            evs[1].record(default)
+        pipe.run(wide, nwide, nwide)
+        if evs:
+            evs[2].record(default)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(1.0)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    launches0 = b2.kernel_launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(default)
+    for _ in range(args.steps):
+        step()
+    ev1.record(default)
+    torch.cuda.synchronize()
+    launches = b2.kernel_launches() - launches0
+    clk = clocks.stop()
+    barrier(world)
+    ms = ev0.elapsed_time(ev1)
+    ms_max = max_over_ranks(ms, world)
+    value = samples_per_step * args.steps * world / (ms_max / 1e3) / 1e6
+    # stage split, and the pipeline's kernels
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    pipe.profile(True)
+    step(evs)
+    torch.cuda.synchronize()
+    ktimes = pipe.kernel_times()
+    pipe.profile(False)
+    ifb_ms = evs[0].elapsed_time(evs[1])
+    chain_ms = evs[1].elapsed_time(evs[2])
+    prof, hits = pipe.get_profiles()
+    ifb.status()
+    hbm_peak, _, peak_src = measured_peaks()
+    alg = raw.numel() * 2          # int16 input once
+    achieved = alg / (ms / args.steps / 1e3) / 1e9
+    line = {
+        "metric": "complex Msamples/s inverse filterbank->fold", "value": round(value, 3),
+        "unit": "complex Msamples/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Gaussian int16 PFB-channel voltages)",
+        "config": {"workload": cfg["workload"], "ifb_parts": npart,
+                   "ifb_fft": [cfg["lin"], info["lout"]], "rechannels": cfg["fb"],
+                   "nfft": nfft, "nfilt_pos": pos, "nfilt_neg": neg,
+                   "stage_ms": {"inverse_filterbank": round(ifb_ms, 3),
+                                "filterbank_dedisperse_detect_fold": round(chain_ms, 3)},
+                   "l2": f"input {raw.numel() * 2 >> 20} MiB per step, larger than L2",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "clocks": clk,
+        "gpu_launches": int(launches),
+        "kernel_ms": {k: round(v[0], 3) for k, v in ktimes.items() if v[1]},
+        "roofline": {"bound": "hbm", "kernel": "whole step", "achieved": round(achieved, 2),
+                     "peak": hbm_peak, "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
+                     "traffic": None, "peak_source": peak_src,
+                     "note": "algorithmic bytes: the int16 input once; FFT-bound chain"},
+        "e2e": None,
+        "check": {"hits_total": int(hits.sum())},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    pipe.close()
+    ifb.close()
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1145,11 +1327,11 @@ def main():
     try:
         kind = cfg.get("kind", "path")
         if args.impl == "reference":
-            {"sk": run_reference_sk, "ifb": run_reference_ifb, "c3": run_reference_c3}.get(
-                kind, run_reference)(args, cfg, world, rank)
+            {"sk": run_reference_sk, "ifb": run_reference_ifb, "c3": run_reference_c3,
+             "c5": run_reference_c5}.get(kind, run_reference)(args, cfg, world, rank)
         else:
-            {"sk": run_b200_sk, "ifb": run_b200_ifb, "c3": run_b200_c3}.get(kind, run_b200)(
-                args, cfg, world, rank, local)
+            {"sk": run_b200_sk, "ifb": run_b200_ifb, "c3": run_b200_c3,
+             "c5": run_b200_c5}.get(kind, run_b200)(args, cfg, world, rank, local)
     finally:
         if world > 1:
             import torch.distributed as dist

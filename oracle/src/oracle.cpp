@@ -1256,9 +1256,16 @@ int64_t inverse_filterbank (const orc_ifb_config* cfg, const T* in, uint64_t nda
   uint64_t npart = 0;
   if (ndat > uint64_t (in_pos + in_neg)) npart = (ndat - (in_pos + in_neg)) / in_step;
   const unsigned spec_len = out_per_step * Lout;   // stitched spectrum of one step
+  // (pol, part) pairs are independent: threads take whole pairs
+  const int64_t ntask = int64_t (cfg->npol) * int64_t (npart);
+#pragma omp parallel
+  {
   std::vector<C> time (Lin), fine (Lin), spec (spec_len), tout (Lout);
-  for (unsigned ipol = 0; ipol < cfg->npol; ipol++)
-    for (uint64_t ipart = 0; ipart < npart; ipart++)
+#pragma omp for schedule(dynamic, 1)
+  for (int64_t task = 0; task < ntask; task++)
+  {
+    const unsigned ipol = unsigned (task / int64_t (npart));
+    const uint64_t ipart = uint64_t (task % int64_t (npart));
       for (unsigned istep = 0; istep < steps; istep++)
       {
         const unsigned fine_offset = istep * coarse_per_out * pfb;
@@ -1339,6 +1346,8 @@ int64_t inverse_filterbank (const orc_ifb_config* cfg, const T* in, uint64_t nda
           for (uint64_t t = 0; t < out_step; t++) dst[t] = tout[cfg->output_discard_pos + t];
         }
       }
+  }
+  }
   return int64_t (npart);
 }
 
