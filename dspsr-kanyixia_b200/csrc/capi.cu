@@ -5,6 +5,7 @@
 #include "dspsr_b200.h"
 #include "kernels.cuh"
 #include "host_rules.h"
+#include "dada.h"
 
 #include <cuda_runtime.h>
 
@@ -353,9 +354,9 @@ struct dspsr_b200_fold
     return DSPSR_B200_OK;
   }
   // builds the exact plan on the host and uploads it on the context's stream
-  int set_bins (double phi, double pps, uint64_t n)
+  int set_bins (double phi, double pps, uint64_t n, double* x_end = nullptr)
   {
-    build_fold_plan (phi, pps, n, &plan);
+    build_fold_plan (phi, pps, n, &plan, x_end);
     ndat = n;
     nseg = int (plan.size ());
     cur = (cur + 1) % NRING;
@@ -475,6 +476,15 @@ struct dspsr_b200_pipeline
   DevBuf<float2> fbbuf;             // filterbank output, FPT
   float2* fb_tab = nullptr;         // pass tables of the filterbank FFT (fb_nsub >= 128)
   size_t fb_tab_cap = 0;
+  // run_host folds a block in pieces: the first piece that folds starts the
+  // block's phase with Fold::get_phase, later pieces go on with the block's
+  // own phase recurrence, exactly as one fold of the whole block would
+  bool in_pieces = false, phase_continue = false;
+  double phase_next = 0;
+  void* pinned[2] = {nullptr, nullptr};   // run_dada: file blocks in page-locked memory
+  uint64_t pinned_bytes = 0;
+  cudaEvent_t host_free[2] = {nullptr, nullptr};   // uploads of pinned[b] done
+  bool host_free_pending[2] = {false, false};
 };
 
 namespace {
@@ -510,13 +520,16 @@ int pipeline_block (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat_new
   {
     // Fold::fold (Fold.C:685-693): phase of the first output sample's midpoint;
     // the output starts nfilt_pos samples after the input (Convolution.C:599)
-    const double phi = fold_phi (cfg.start_day, cfg.start_sec, cfg.start_frac, cfg.epoch_day,
+    const double phi = pl->phase_continue
+                     ? pl->phase_next
+                     : fold_phi (cfg.start_day, cfg.start_sec, cfg.start_frac, cfg.epoch_day,
                                  cfg.epoch_sec, cfg.epoch_frac, pl->in0 + sh.nfilt_pos,
                                  pl->rate, cfg.period_s, cfg.reference_phase);
     const double sampling_interval = 1.0 / pl->rate;
     const double pps = sampling_interval / cfg.period_s;   // Fold.C:754-756
-    int rc = pl->fold.set_bins (phi, pps, nout);
+    int rc = pl->fold.set_bins (phi, pps, nout, &pl->phase_next);
     if (rc) return rc;
+    pl->phase_continue = pl->in_pieces;
     FoldView fv = pl->fold.view (cfg.state, pl->nout, cfg.nchan);
     VoltView vv {nullptr, 0};
     const ConvTables tb = pl->conv.tables ();
@@ -1602,6 +1615,11 @@ int dspsr_b200_pipeline_destroy (dspsr_b200_pipeline* pl)
     if (pl->consumed[i]) cudaEventDestroy (pl->consumed[i]);
   }
   if (pl->copy_stream) cudaStreamDestroy (pl->copy_stream);
+  for (int i = 0; i < 2; i++)
+  {
+    if (pl->pinned[i]) cudaFreeHost (pl->pinned[i]);
+    if (pl->host_free[i]) cudaEventDestroy (pl->host_free[i]);
+  }
   pl->fbbuf.release ();
   delete pl;
   return DSPSR_B200_OK;
@@ -1648,6 +1666,13 @@ int dspsr_b200_pipeline_run_host (dspsr_b200_pipeline* pl, const void* h_in, uin
   const uint64_t piece = ((ndat + npiece - 1) / npiece + unit - 1) / unit * unit;
   const uint64_t bps = pl->bytes_per_sample;
   uint64_t total = 0;
+  // one block: its pieces share one fold phase recurrence
+  struct PieceScope
+  {
+    dspsr_b200_pipeline* p;
+    explicit PieceScope (dspsr_b200_pipeline* q) : p (q) { p->in_pieces = true; p->phase_continue = false; }
+    ~PieceScope () { p->in_pieces = false; p->phase_continue = false; }
+  } scope (pl);
   for (uint64_t j = 0, off = 0; off < ndat || (ndat == 0 && j == 0); j++, off += piece)
   {
     const uint64_t n = std::min<uint64_t> (piece, ndat - off);
@@ -1670,6 +1695,91 @@ int dspsr_b200_pipeline_run_host (dspsr_b200_pipeline* pl, const void* h_in, uin
     if (ndat == 0) break;
   }
   if (ndat_folded) *ndat_folded = total;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_pipeline_run_dada (dspsr_b200_pipeline* pl, dspsr_b200_dada_file* file,
+                                  uint64_t start_sample, uint64_t nsamp, uint64_t block_ndat,
+                                  uint64_t* ndat_read, uint64_t* ndat_folded)
+{
+  if (!pl) return DSPSR_B200_EINVAL;
+  dspsr_b200_context* ctx = pl->ctx;
+  if (ndat_read) *ndat_read = 0;
+  if (ndat_folded) *ndat_folded = 0;
+  if (!file) return fail (ctx, DSPSR_B200_EINVAL, "pipeline_run_dada: null file");
+  const dspsr_b200_dada_info& info = dspsr_b200_host::dada_info (file);
+  const auto& cfg = pl->cfg;
+  const unsigned nbit = cfg.input_kind == DSPSR_B200_INT8_TFPD ? 8
+                      : cfg.input_kind == DSPSR_B200_INT16_TFPD ? 16 : 0;
+  if (!nbit)
+    return fail (ctx, DSPSR_B200_EINVAL, "pipeline_run_dada: TFPD input only");
+  // GenericEightBitUnpacker::matches / the 16-bit unpacker: complex TFPD of
+  // the pipeline's shape
+  if (info.nchan != cfg.nchan || info.npol != cfg.npol || info.ndim != 2 || info.nbit != nbit)
+    return fail (ctx, DSPSR_B200_EINVAL,
+                 "pipeline_run_dada: file has NCHAN=%u NPOL=%u NDIM=%u NBIT=%u, the pipeline "
+                 "takes NCHAN=%u NPOL=%u NDIM=2 NBIT=%u", info.nchan, info.npol, info.ndim,
+                 info.nbit, cfg.nchan, cfg.npol, nbit);
+  const uint64_t unit = pl->fb_nsub ? pl->fb_nsub : 1;
+  if (block_ndat == 0 || block_ndat % unit)
+    return fail (ctx, DSPSR_B200_EINVAL,
+                 "pipeline_run_dada: block_ndat=%llu must be a positive multiple of %llu",
+                 (unsigned long long) block_ndat, (unsigned long long) unit);
+  const uint64_t end = std::min (info.ndat, info.file_ndat);
+  const uint64_t avail = start_sample < end ? end - start_sample : 0;
+  uint64_t total = nsamp ? std::min (nsamp, avail) : avail;
+  total -= total % unit;
+
+  const uint64_t bytes = block_ndat * pl->bytes_per_sample;
+  if (pl->pinned_bytes < bytes)
+  {
+    for (int i = 0; i < 2; i++)
+    {
+      if (pl->host_free_pending[i])
+        B200_CHECK (ctx, cudaEventSynchronize (pl->host_free[i]), "wait upload");
+      pl->host_free_pending[i] = false;
+      if (pl->pinned[i]) cudaFreeHost (pl->pinned[i]);
+      pl->pinned[i] = nullptr;
+    }
+    pl->pinned_bytes = 0;
+    for (int i = 0; i < 2; i++)
+      B200_CHECK (ctx, cudaHostAlloc (&pl->pinned[i], bytes, cudaHostAllocDefault),
+                  "cudaHostAlloc file block");
+    pl->pinned_bytes = bytes;
+  }
+  for (int i = 0; i < 2; i++)
+    if (!pl->host_free[i])
+      B200_CHECK (ctx, cudaEventCreateWithFlags (&pl->host_free[i], cudaEventDisableTiming),
+                  "create event");
+
+  // File::load_bytes into one buffer while the other block's upload and
+  // kernels run (the reference's File::load_bytes_device,
+  // File.C:280-339, uploads one pinned block at a time)
+  uint64_t done = 0, folded = 0;
+  int b = 0;
+  while (done < total)
+  {
+    const uint64_t n = std::min (block_ndat, total - done);
+    if (pl->host_free_pending[b])
+      B200_CHECK (ctx, cudaEventSynchronize (pl->host_free[b]), "wait upload");
+    pl->host_free_pending[b] = false;
+    uint64_t got = 0;
+    int rc = dspsr_b200_dada_read (file, start_sample + done, n, pl->pinned[b], &got);
+    if (rc) return fail (ctx, rc, "pipeline_run_dada: %s", dspsr_b200_host_error ());
+    if (got != n)
+      return fail (ctx, DSPSR_B200_ESTATE, "pipeline_run_dada: read %llu of %llu samples",
+                   (unsigned long long) got, (unsigned long long) n);
+    uint64_t f = 0;
+    rc = dspsr_b200_pipeline_run_host (pl, pl->pinned[b], n, &f);
+    if (rc) return rc;
+    B200_CHECK (ctx, cudaEventRecord (pl->host_free[b], pl->copy_stream), "record upload");
+    pl->host_free_pending[b] = true;
+    folded += f;
+    done += n;
+    b ^= 1;
+  }
+  if (ndat_read) *ndat_read = done;
+  if (ndat_folded) *ndat_folded = folded;
   return DSPSR_B200_OK;
 }
 

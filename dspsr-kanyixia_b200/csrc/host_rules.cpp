@@ -552,7 +552,8 @@ static void single (std::vector<FoldSegment>& out, uint64_t k, double y)
   out.push_back (s);
 }
 
-int64_t build_fold_plan (double phi, double p, uint64_t ndat, std::vector<FoldSegment>* out)
+int64_t build_fold_plan (double phi, double p, uint64_t ndat, std::vector<FoldSegment>* out,
+                         double* x_end)
 {
   std::vector<FoldSegment> local;
   std::vector<FoldSegment>& segs = out ? *out : local;
@@ -610,6 +611,7 @@ int64_t build_fold_plan (double phi, double p, uint64_t ndat, std::vector<FoldSe
     x = ylast + p;                     // the reference's own rounding step
     k += len;
   }
+  if (x_end) *x_end = x;
   return int64_t (segs.size ());
 }
 

@@ -38,8 +38,10 @@ std::vector<unsigned> ifb_fine_channel_plan (unsigned nchan, unsigned per_coarse
 // (transitions t_start, t_end); swap exchanges the halves.  0 on success.
 int apodization (int type, unsigned ndat, unsigned t_start, unsigned t_end, bool swap,
                  float* window);
-// Returns the number of segments; fills *out when non-null.
+// Returns the number of segments; fills *out when non-null.  *x_end, when
+// non-null, receives the recurrence's phase after the last sample: the phi
+// with which the sequence goes on for the samples that follow.
 int64_t build_fold_plan (double phi, double phase_per_sample, uint64_t ndat,
-                         std::vector<FoldSegment>* out);
+                         std::vector<FoldSegment>* out, double* x_end = nullptr);
 
 } // namespace b200

@@ -8,11 +8,14 @@ C ABI of libdspsr_b200.so (include/dspsr_b200.h):
   Detection engine   -> detect                  (CUDA::DetectionEngine)
   Fold engine        -> Fold                    (CUDA::FoldEngine with use_set_bins)
   SingleThread loop  -> Pipeline                (unpack -> convolve -> detect -> fold)
+  DADAFile / header  -> DADAFile, dada_parse, ascii_header_get/_set (file source of the loop)
 
 Device buffers are torch CUDA tensors (torch is only the allocator and stream
 provider here); every computation runs in the library's sm_100a kernels.
 """
 import ctypes
+import os
+import weakref
 
 import numpy as np
 
@@ -22,7 +25,8 @@ from ._capi import (B200Error, PipelineConfig, INTENSITY, PPQQ, COHERENCE, STOKE
 
 __all__ = ["Context", "Convolution", "InverseFilterbank", "Fold", "apodization", "Pipeline", "PipelineConfig", "B200Error",
            "smearing_samples", "minimum_ndat", "optimal_fft_length", "bittable8", "fold_phi",
-           "sk_limits",
+           "sk_limits", "DADAFile", "dada_parse", "dada_is_valid", "ascii_header_get",
+           "ascii_header_set", "write_dada",
            "fold_plan_count", "INTENSITY", "PPQQ", "COHERENCE", "STOKES", "INT8_TFPD",
            "INT16_TFPD", "FLOAT_FPT", "CHIRP_REFERENCE", "CHIRP_FP64", "NOUT"]
 
@@ -118,6 +122,11 @@ class Context:
         if rc:
             raise B200Error(rc, f"context_create(device={device}) failed")
         self.handle = h
+        # engines made on this context: released before it
+        self._children = weakref.WeakSet()
+
+    def _adopt(self, child):
+        self._children.add(child)
 
     def check(self, rc, what=""):
         if rc:
@@ -132,6 +141,8 @@ class Context:
 
     def close(self):
         if self.handle:
+            for child in list(self._children):
+                child.close()
             self._lib.dspsr_b200_context_destroy(self.handle)
             self.handle = None
 
@@ -192,6 +203,7 @@ class Convolution:
                                                           nfilt_pos, nfilt_neg, ctypes.byref(h)),
                   "convolution_create")
         self.handle = h
+        ctx._adopt(self)
         self.nchan, self.npol, self.nfft = nchan, npol, nfft
         self.nfilt_pos, self.nfilt_neg = nfilt_pos, nfilt_neg
         self.nkeep = nfft - nfilt_pos - nfilt_neg
@@ -283,6 +295,7 @@ class InverseFilterbank:
                                                                  ctypes.byref(h)),
                   "inverse_filterbank_create")
         self.handle = h
+        ctx._adopt(self)
         info = (ctypes.c_uint64 * 10)()
         ctx.check(self._lib.dspsr_b200_inverse_filterbank_info(h, info), "inverse_filterbank_info")
         self.info = dict(zip(self.INFO, list(info)))
@@ -344,6 +357,7 @@ class Fold:
         ctx.check(self._lib.dspsr_b200_fold_create(ctx.handle, nbin, nchan, npol, ctypes.byref(h)),
                   "fold_create")
         self.handle = h
+        ctx._adopt(self)
         self.nbin, self.nchan, self.npol = nbin, nchan, npol
 
     def set_bins(self, phi, phase_per_sample, ndat, idat_start=0):
@@ -391,6 +405,7 @@ class Pipeline:
         ctx.check(self._lib.dspsr_b200_pipeline_create(ctx.handle, ctypes.byref(config),
                                                        ctypes.byref(h)), "pipeline_create")
         self.handle = h
+        ctx._adopt(self)
         self.nout = NOUT[config.state]
 
     def run(self, d_in, ndat, in_span=0):
@@ -406,6 +421,16 @@ class Pipeline:
         self.ctx.check(self._lib.dspsr_b200_pipeline_run_host(self.handle, addr, ndat,
                                                               ctypes.byref(n)), "pipeline_run_host")
         return n.value
+
+    def run_dada(self, dada, block_ndat, start_sample=0, nsamp=0):
+        """Feed a DADAFile through the pipeline in blocks of block_ndat
+        (nsamp 0 = to the end of the data); returns (samples read, folded)."""
+        nread = ctypes.c_uint64()
+        nfold = ctypes.c_uint64()
+        self.ctx.check(self._lib.dspsr_b200_pipeline_run_dada(
+            self.handle, dada.handle, start_sample, nsamp, block_ndat, ctypes.byref(nread),
+            ctypes.byref(nfold)), "pipeline_run_dada")
+        return nread.value, nfold.value
 
     def get_profiles(self):
         c = self.config
@@ -449,6 +474,140 @@ class Pipeline:
             self.close()
         except Exception:
             pass
+
+
+def _host_check(rc, what):
+    if rc != 0:
+        msg = _capi.lib().dspsr_b200_host_error()
+        raise B200Error(rc, f"{what}: {msg.decode() if msg else ''}")
+
+
+def _cstr(text):
+    return text.encode() if isinstance(text, str) else bytes(text)
+
+
+def ascii_header_get(header, keyword):
+    """ascii_header_get with a "%s" code (ascii_header.c:117-142): the value
+    token after KEYWORD, or None when the keyword or its value is absent."""
+    buf = ctypes.create_string_buffer(4096)
+    rc = _capi.lib().dspsr_b200_ascii_header_get(_cstr(header), _cstr(keyword), buf, len(buf))
+    return buf.value.decode() if rc == 1 else None
+
+
+def ascii_header_set(header, keyword, value, header_size=4096):
+    """ascii_header_set (ascii_header.c:58-115) on a copy of HEADER inside a
+    buffer of header_size bytes; returns the new header text."""
+    h = _cstr(header)
+    buf = ctypes.create_string_buffer(h, max(header_size, len(h) + 1))
+    _host_check(_capi.lib().dspsr_b200_ascii_header_set(buf, header_size, _cstr(keyword),
+                                                        _cstr(str(value))), "ascii_header_set")
+    return buf.value.decode()
+
+
+def _info_dict(info):
+    d = {}
+    for name, _ in _capi.DadaInfo._fields_:
+        v = getattr(info, name)
+        d[name] = v.decode() if isinstance(v, bytes) else v
+    return d
+
+
+def dada_parse(header, header_bytes=4096):
+    """ASCIIObservation::load over a header text: the observation as a dict."""
+    info = _capi.DadaInfo()
+    _host_check(_capi.lib().dspsr_b200_dada_parse(_cstr(header), header_bytes,
+                                                  ctypes.byref(info)), "dada_parse")
+    return _info_dict(info)
+
+
+def dada_is_valid(filename):
+    """DADAFile::is_valid: the header loads and names HDR_VERSION and INSTRUMENT."""
+    return bool(_capi.lib().dspsr_b200_dada_is_valid(_cstr(os.fspath(filename))))
+
+
+class DADAFile:
+    """A DADA file (DADAFile::open_file, File::open): header, observation
+    parameters and whole-sample reads."""
+
+    def __init__(self, filename):
+        self._lib = _capi.lib()
+        self.filename = os.fspath(filename)
+        info = _capi.DadaInfo()
+        h = ctypes.c_void_p()
+        _host_check(self._lib.dspsr_b200_dada_open(_cstr(self.filename), ctypes.byref(h),
+                                                   ctypes.byref(info)), "dada_open")
+        self.handle = h
+        self.info = _info_dict(info)
+        text = ctypes.c_char_p()
+        size = ctypes.c_uint64()
+        _host_check(self._lib.dspsr_b200_dada_header(self.handle, ctypes.byref(text),
+                                                     ctypes.byref(size)), "dada_header")
+        self.header = text.value.decode(errors="replace")
+
+    @property
+    def ndat(self):
+        return min(self.info["ndat"], self.info["file_ndat"])
+
+    @property
+    def bytes_per_sample(self):
+        return self.info["bits_per_sample"] // 8
+
+    @property
+    def dual_sideband(self):
+        """Observation::get_dual_sideband: DSB, else true for analytic (NDIM 2) data."""
+        dsb = self.info["dual_sideband"]
+        return dsb if dsb >= 0 else int(self.info["ndim"] == 2)
+
+    def read(self, start_sample, nsamp):
+        """nsamp samples from start_sample as raw bytes (uint8), fewer at the end."""
+        out = np.empty(nsamp * self.info["bits_per_sample"] // 8, np.uint8)
+        n = ctypes.c_uint64()
+        _host_check(self._lib.dspsr_b200_dada_read(self.handle, start_sample, nsamp,
+                                                   out.ctypes.data, ctypes.byref(n)), "dada_read")
+        return out[: n.value * self.info["bits_per_sample"] // 8]
+
+    def pipeline_config(self, dm, nfft, nfilt_pos, nfilt_neg, nbin, period, **kw):
+        """make_config with the file's FREQ, BW, NCHAN, NPOL, NBIT, start time
+        and sideband filled in."""
+        i = self.info
+        if i["ndim"] != 2 or i["nbit"] not in (8, 16):
+            raise B200Error(_capi.EINVAL, f"the pipeline takes NDIM 2 with NBIT 8 or 16, the "
+                                          f"file has NDIM {i['ndim']} NBIT {i['nbit']}")
+        kw.setdefault("input_kind", INT8_TFPD if i["nbit"] == 8 else INT16_TFPD)
+        kw.setdefault("start_mjd", (i["start_day"], i["start_sec"], i["start_frac"]))
+        kw.setdefault("dual_sideband", self.dual_sideband)
+        return make_config(i["centre_freq_mhz"], i["bandwidth_mhz"], dm, i["nchan"], i["npol"],
+                           nfft, nfilt_pos, nfilt_neg, nbin, period, **kw)
+
+    def close(self):
+        if self.handle:
+            self._lib.dspsr_b200_dada_close(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def write_dada(filename, keys, data, header_size=4096):
+    """Write a DADA file: a header of header_size bytes holding HDR_SIZE and
+    KEYS (set in order with ascii_header_set), then the raw bytes of DATA."""
+    text = ""
+    text = ascii_header_set(text, "HDR_SIZE", header_size, header_size)
+    for k, v in keys.items():
+        text = ascii_header_set(text, k, v, header_size)
+    raw = text.encode()
+    with open(filename, "wb") as f:
+        f.write(raw + b"\0" * (header_size - len(raw)))
+        f.write(np.ascontiguousarray(data).view(np.uint8).tobytes())
 
 
 def make_config(centre_freq, bandwidth, dm, nchan, npol, nfft, nfilt_pos, nfilt_neg, nbin,

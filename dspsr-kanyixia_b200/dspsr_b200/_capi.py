@@ -80,6 +80,33 @@ class IfbConfig(ctypes.Structure):
     ]
 
 
+class DadaInfo(ctypes.Structure):
+    """dspsr_b200_dada_info"""
+    _fields_ = [
+        ("header_bytes", c_u64),
+        ("ndat", c_u64),
+        ("file_ndat", c_u64),
+        ("bits_per_sample", c_u64),
+        ("obs_offset", c_u64),
+        ("picoseconds", c_i64),
+        ("start_day", c_i64),
+        ("start_sec", c_i64),
+        ("start_frac", c_dbl),
+        ("centre_freq_mhz", c_dbl),
+        ("bandwidth_mhz", c_dbl),
+        ("tsamp_us", c_dbl),
+        ("rate_hz", c_dbl),
+        ("hdr_version", c_dbl),
+        ("nchan", c_uint),
+        ("npol", c_uint),
+        ("nbit", c_uint),
+        ("ndim", c_uint),
+        ("dual_sideband", c_int),
+        ("adjacent_header", c_int),
+    ] + [(k, ctypes.c_char * 64) for k in ("telescope", "receiver", "source", "mode",
+                                            "instrument", "utc_start", "state", "basis")]
+
+
 SIGNATURES = {
     "dspsr_b200_version": (c_int, []),
     "dspsr_b200_context_create": (c_int, [c_int, c_vp, ctypes.POINTER(c_vp)]),
@@ -149,6 +176,17 @@ SIGNATURES = {
     "dspsr_b200_pipeline_profile": (c_int, [c_vp, c_int]),
     "dspsr_b200_pipeline_kernel_times": (c_int, [c_vp, ctypes.POINTER(c_dbl), c_u64p]),
     "dspsr_b200_kernel_launches": (c_u64, []),
+    "dspsr_b200_host_error": (ctypes.c_char_p, []),
+    "dspsr_b200_ascii_header_get": (c_int, [ctypes.c_char_p, ctypes.c_char_p, c_vp, c_u64]),
+    "dspsr_b200_ascii_header_set": (c_int, [c_vp, c_u64, ctypes.c_char_p, ctypes.c_char_p]),
+    "dspsr_b200_dada_parse": (c_int, [ctypes.c_char_p, c_u64, ctypes.POINTER(DadaInfo)]),
+    "dspsr_b200_dada_open": (c_int, [ctypes.c_char_p, ctypes.POINTER(c_vp),
+                                     ctypes.POINTER(DadaInfo)]),
+    "dspsr_b200_dada_is_valid": (c_int, [ctypes.c_char_p]),
+    "dspsr_b200_dada_header": (c_int, [c_vp, ctypes.POINTER(ctypes.c_char_p), c_u64p]),
+    "dspsr_b200_dada_read": (c_int, [c_vp, c_u64, c_u64, c_vp, c_u64p]),
+    "dspsr_b200_dada_close": (c_int, [c_vp]),
+    "dspsr_b200_pipeline_run_dada": (c_int, [c_vp, c_vp, c_u64, c_u64, c_u64, c_u64p, c_u64p]),
 }
 
 _lib = None

@@ -434,6 +434,89 @@ uint64_t dspsr_b200_kernel_launches (void);
 /* shape of the plan: nfft, nkeep, FFT split n1 x n2, parts per batch */
 int dspsr_b200_pipeline_info (dspsr_b200_pipeline* pipe, uint64_t* info8);
 
+/* ---------------------------------------------------------------------- */
+/* DADA file source (host only, no GPU needed except for _pipeline_run_dada) */
+/* ---------------------------------------------------------------------- */
+
+typedef struct dspsr_b200_dada_file dspsr_b200_dada_file;
+
+/* The observation parameters DADAFile::open_file (Kernel/Classes/DADAFile.C:
+   48-68) loads through ASCIIObservation::load (ASCIIObservation.C:88-410)
+   and File::open (File.C:175-190, fstat_file_ndat :366-390). */
+typedef struct
+{
+  uint64_t header_bytes;     /* bytes before the first sample (HDR_SIZE; 0 with
+                                an adjacent header file that defines none) */
+  uint64_t ndat;             /* NDAT when the header gives it, else file_ndat */
+  uint64_t file_ndat;        /* samples the file holds after the header */
+  uint64_t bits_per_sample;  /* nbit * npol * nchan * ndim */
+  uint64_t obs_offset;       /* OBS_OFFSET (or OFFSET) in bytes */
+  int64_t picoseconds;       /* PICOSECONDS, 0 when absent */
+  int64_t start_day, start_sec;  /* MJD of sample 0: UTC_START + PICOSECONDS */
+  double start_frac;             /* + the samples in OBS_OFFSET; 0 for TBD */
+  double centre_freq_mhz;    /* FREQ */
+  double bandwidth_mhz;      /* BW */
+  double tsamp_us;           /* TSAMP, microseconds */
+  double rate_hz;            /* 1 / (TSAMP * 1e-6) */
+  double hdr_version;        /* HDR_VERSION, 0 when absent */
+  unsigned nchan, npol, nbit, ndim;   /* defaults 1, 1, 2, 1 when absent */
+  int dual_sideband;         /* DSB: 1, 0, or -1 when absent */
+  int adjacent_header;       /* the header came from an adjacent .hdr file */
+  char telescope[64], receiver[64], source[64], mode[64];
+  char instrument[64], utc_start[64], state[64], basis[64];
+} dspsr_b200_dada_info;
+
+/* Message of the calling thread's last failed host-only call (the DADA and
+   header calls below, which have no context). */
+const char* dspsr_b200_host_error (void);
+
+/* ascii_header_get with a "%s" code (Kernel/Classes/ascii_header.c:34-56,
+   117-142): copies the whitespace-delimited value after KEYWORD (a keyword
+   at the start of the header, or after a newline or backslash and followed
+   by a blank) into value (at most value_cap-1 bytes).  Returns 1, or -1 when
+   the keyword or its value is absent. */
+int dspsr_b200_ascii_header_get (const char* header, const char* keyword, char* value,
+                                 uint64_t value_cap);
+/* ascii_header_set (ascii_header.c:58-115): replaces the keyword's value in
+   place, or inserts the line before "DATA\n" or at the end.  header_cap is the
+   size of the buffer; ETOOBIG when the result would not fit. */
+int dspsr_b200_ascii_header_set (char* header, uint64_t header_cap, const char* keyword,
+                                 const char* value);
+/* ASCIIObservation::load over a NUL-terminated header; header_bytes goes to
+   info->header_bytes and file_ndat stays 0.  EINVAL names the first missing
+   required keyword (TELESCOPE SOURCE FREQ BW NPOL NBIT TSAMP UTC_START
+   OBS_OFFSET) or the invalid NDIM. */
+int dspsr_b200_dada_parse (const char* header, uint64_t header_bytes, dspsr_b200_dada_info* info);
+/* DADAFile::open_file + File::open: DADAHeader::load_header (DADAHeader.C:
+   56-139; HDR_SIZE grows the read until the whole header is in, an absent
+   HDR_SIZE sends it to the adjacent .hdr file), then the parse above and the
+   sample count from the file size when NDAT is absent. */
+int dspsr_b200_dada_open (const char* filename, dspsr_b200_dada_file** file,
+                          dspsr_b200_dada_info* info);
+/* DADAFile::is_valid (DADAFile.C:32-43, DADAHeader::valid :146-174): 1 when
+   the header loads and defines HDR_VERSION and INSTRUMENT, else 0. */
+int dspsr_b200_dada_is_valid (const char* filename);
+/* the loaded header text (NUL-terminated) and its buffer size */
+int dspsr_b200_dada_header (const dspsr_b200_dada_file* file, const char** text, uint64_t* size);
+/* File::load_bytes (File.C:248-300): nsamp samples from sample start_sample
+   into host memory dst, stopping at the end of the data (NDAT or the file);
+   *nread = samples read.  Sample boundaries must fall on whole bytes. */
+int dspsr_b200_dada_read (dspsr_b200_dada_file* file, uint64_t start_sample, uint64_t nsamp,
+                          void* dst, uint64_t* nread);
+int dspsr_b200_dada_close (dspsr_b200_dada_file* file);
+
+/* The file-driven SingleThread loop: nsamp samples (0 = to the end of the
+   data) from start_sample, in blocks of block_ndat, through two pinned host
+   buffers: the read of one block overlaps the upload and kernels of the block
+   before.  The file must match the pipeline: NCHAN, NPOL, NDIM 2 and NBIT 8
+   (INT8_TFPD) or 16 (INT16_TFPD).  With a filterbank stage block_ndat must be
+   a multiple of its channel count and a short last block is cut to one.
+   *ndat_read = samples passed to the pipeline, *ndat_folded = output samples
+   folded.  Returns after queueing the last block, like _pipeline_run_host. */
+int dspsr_b200_pipeline_run_dada (dspsr_b200_pipeline* pipe, dspsr_b200_dada_file* file,
+                                  uint64_t start_sample, uint64_t nsamp, uint64_t block_ndat,
+                                  uint64_t* ndat_read, uint64_t* ndat_folded);
+
 #ifdef __cplusplus
 }
 #endif

@@ -262,3 +262,96 @@ def test_pipeline_restores_dispersed_pulse(ctx, b2):
     on = np.argmax(p)
     assert abs(((on + 0.5) / cfg["nbin"] - truth["phase"] + 0.5) % 1.0 - 0.5) < 0.03
     assert (p.max() - np.median(p)) > 20 * np.std(p[np.abs(np.arange(256) - on) > 30])
+
+
+def dada_keys(cfg, ndat_hint=None):
+    """A header for cfg's observation whose start time is START."""
+    keys = {"HDR_VERSION": "1.0", "TELESCOPE": "PKS", "SOURCE": "J0437-4715",
+            "INSTRUMENT": "CASPSR", "FREQ": cfg["cf"], "BW": cfg["bw"], "NCHAN": cfg["nchan"],
+            "NPOL": cfg["npol"], "NBIT": 8 if cfg["kind"] == 0 else 16, "NDIM": 2,
+            "TSAMP": cfg["nchan"] / abs(cfg["bw"]), "UTC_START": "2023-02-25-01:00:00",
+            "PICOSECONDS": 250000000000, "OBS_OFFSET": 0}
+    return keys
+
+
+def run_file(ctx, b2, path, cfg, block_ndat, start=0, nsamp=0):
+    with b2.DADAFile(path) as f:
+        c = f.pipeline_config(cfg["dm"], cfg["nfft"], cfg["pos"], cfg["neg"], cfg["nbin"],
+                              cfg["period"], state=cfg["state"], lut=cfg["lut"],
+                              epoch_mjd=EPOCH, filterbank_nchan=cfg.get("fb", 0))
+        assert (c.start_day, c.start_sec, c.start_frac) == START
+        pl = b2.Pipeline(ctx, c)
+        nread, nfold = pl.run_dada(f, block_ndat, start, nsamp)
+        prof, hits = pl.get_profiles()
+        pl.close()
+    return prof, hits, nread, nfold
+
+
+@pytest.mark.parametrize("name,kw,block", [
+    ("int8_4chan", dict(dm=20.0, bw=64.0, nchan=4, nfft=1 << 16, nbin=256, period=0.00557),
+     2 * (1 << 16) + 123),
+    ("int16_coherence", dict(dm=5.0, bw=32.0, nchan=2, nfft=1 << 13, state=2, kind=1, nbin=128),
+     50000),
+    ("filterbank16", dict(dm=30.0, bw=64.0, fb=16, nfft=1 << 13, state=3, nbin=512,
+                          period=0.0041), 16 * 9000),
+])
+def test_pipeline_reads_dada_file(ctx, b2, orc, tmp_path, name, kw, block):
+    """A recorded DADA file through pipeline_run_dada (blocks read into two
+    pinned buffers, each read overlapping the previous block's upload and
+    kernels): the same profiles as run_host with the same blocks, and the
+    oracle chain's within PROFILE_RTOL."""
+    cfg = base_cfg(b2, **kw)
+    rng = np.random.default_rng(zlib.crc32(name.encode()))
+    unit = cfg.get("fb", 0) or 1
+    ndat = 5 * cfg["nfft"] * unit + 999
+    raw = make_blocks(rng, cfg, [ndat])[0]
+    path = tmp_path / f"{name}.dada"
+    b2.write_dada(path, dada_keys(cfg), raw)
+    prof, hits, nread, nfold = run_file(ctx, b2, path, cfg, block)
+    used = ndat - ndat % unit
+    assert nread == used
+    bps = cfg["nchan"] * cfg["npol"] * 2
+    flat = raw.reshape(-1)[: used * bps]
+    blocks = [flat[i * bps:(i + block) * bps] for i in range(0, used, block)]
+    hprof, hhits, htotal, _ = run_pipeline(ctx, b2, blocks, cfg, host=True)
+    assert nfold == htotal > 0
+    # the fold's float sums are not order-deterministic between runs
+    check(prof, hits, nfold, hprof.astype(np.float64), hhits, htotal, cfg["state"], rtol=1e-6)
+    rprof, rhits, rtotal = oracle_chain(orc, b2, blocks, cfg)
+    check(prof, hits, nfold, rprof, rhits, rtotal, cfg["state"])
+
+
+def test_pipeline_dada_window_and_rejects(ctx, b2, tmp_path):
+    """start_sample / nsamp select a window of the file; a file whose shape
+    differs from the pipeline's, or a block that splits a filterbank
+    transform, is refused."""
+    cfg = base_cfg(b2, dm=5.0, nchan=2, bw=32.0, nfft=1 << 13)
+    rng = np.random.default_rng(5)
+    ndat = 6 * cfg["nfft"]
+    raw = make_blocks(rng, cfg, [ndat])[0]
+    path = tmp_path / "w.dada"
+    b2.write_dada(path, dada_keys(cfg), raw)
+    prof, hits, nread, nfold = run_file(ctx, b2, path, cfg, 10000, start=4000,
+                                        nsamp=3 * cfg["nfft"])
+    assert nread == 3 * cfg["nfft"]
+    bps = cfg["nchan"] * cfg["npol"] * 2
+    win = raw.reshape(-1)[4000 * bps:(4000 + nread) * bps]
+    blocks = [win[i * bps:(i + 10000) * bps] for i in range(0, nread, 10000)]
+    hprof, hhits, htotal, _ = run_pipeline(ctx, b2, blocks, cfg, host=True)
+    check(prof, hits, nfold, hprof.astype(np.float64), hhits, htotal, cfg["state"], rtol=1e-6)
+    # past the end: nothing read
+    assert run_file(ctx, b2, path, cfg, 10000, start=ndat + 5)[2:] == (0, 0)
+    # shape mismatch: the pipeline takes 4 channels, the file has 2
+    with b2.DADAFile(path) as f:
+        c = f.pipeline_config(cfg["dm"], cfg["nfft"], cfg["pos"], cfg["neg"], 64, 0.01)
+        c.nchan = 4
+        pl = b2.Pipeline(ctx, c)
+        with pytest.raises(b2.B200Error, match="NCHAN=2"):
+            pl.run_dada(f, 10000)
+        pl.close()
+        pos, neg, nfft = b2.dispersion_plan(cfg["cf"], cfg["bw"], cfg["dm"], 32, 4096)
+        c = f.pipeline_config(cfg["dm"], nfft, pos, neg, 64, 0.01, filterbank_nchan=16)
+        pl = b2.Pipeline(ctx, c)
+        with pytest.raises(b2.B200Error, match="multiple of 16"):
+            pl.run_dada(f, 10008)
+        pl.close()
