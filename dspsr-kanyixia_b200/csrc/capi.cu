@@ -6,6 +6,7 @@
 #include "kernels.cuh"
 #include "host_rules.h"
 #include "dada.h"
+#include "subint.h"
 
 #include <cuda_runtime.h>
 
@@ -15,6 +16,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <new>
 #include <string>
 #include <vector>
@@ -321,17 +323,21 @@ struct dspsr_b200_fold
   uint64_t ndat = 0;
   std::vector<FoldSegment> plan;
 
-  int init (dspsr_b200_context* c, unsigned nb, unsigned nc, unsigned np)
+  unsigned slots = 1;                 // sub-integrations held side by side
+  int init (dspsr_b200_context* c, unsigned nb, unsigned nc, unsigned np, unsigned ns = 1)
   {
     ctx = c;
     nbin = nb;
     nchan = nc;
     npol = np;
-    if (nbin == 0 || nchan == 0 || npol == 0)
-      return fail (ctx, DSPSR_B200_EINVAL, "fold: invalid nbin=%u nchan=%u npol=%u", nbin,
-                   nchan, npol);
-    B200_CHECK (ctx, profiles.reserve (uint64_t (nchan) * npol * nbin), "cudaMalloc profiles");
-    B200_CHECK (ctx, hits.reserve (nbin), "cudaMalloc hits");
+    slots = ns;
+    if (nbin == 0 || nchan == 0 || npol == 0 || slots == 0
+        || uint64_t (nbin) * slots >= FOLD_SKIP)
+      return fail (ctx, DSPSR_B200_EINVAL, "fold: invalid nbin=%u nchan=%u npol=%u slots=%u",
+                   nbin, nchan, npol, slots);
+    B200_CHECK (ctx, profiles.reserve (uint64_t (nchan) * npol * nbin * slots),
+                "cudaMalloc profiles");
+    B200_CHECK (ctx, hits.reserve (uint64_t (nbin) * slots), "cudaMalloc hits");
     for (int i = 0; i < NRING; i++)
     {
       B200_CHECK (ctx, cudaEventCreateWithFlags (&done[i], cudaEventDisableTiming),
@@ -347,16 +353,52 @@ struct dspsr_b200_fold
   int reset ()
   {
     B200_CHECK (ctx, cudaMemsetAsync (profiles.ptr, 0,
-                                      uint64_t (nchan) * npol * nbin * sizeof (float),
+                                      uint64_t (nchan) * npol * nbin * slots * sizeof (float),
                                       ctx->stream), "memset profiles");
-    B200_CHECK (ctx, cudaMemsetAsync (hits.ptr, 0, nbin * sizeof (unsigned), ctx->stream),
-                "memset hits");
+    B200_CHECK (ctx, cudaMemsetAsync (hits.ptr, 0, uint64_t (nbin) * slots * sizeof (unsigned),
+                                      ctx->stream), "memset hits");
     return DSPSR_B200_OK;
+  }
+  // zeroes one sub-integration slot
+  int reset_slot (unsigned k)
+  {
+    const size_t pitch = size_t (nbin) * slots * sizeof (float);
+    B200_CHECK (ctx, cudaMemset2DAsync (profiles.ptr + size_t (k) * nbin, pitch, 0,
+                                        nbin * sizeof (float), size_t (nchan) * npol, ctx->stream),
+                "memset slot");
+    B200_CHECK (ctx, cudaMemsetAsync (hits.ptr + size_t (k) * nbin, 0, nbin * sizeof (unsigned),
+                                      ctx->stream), "memset slot hits");
+    return DSPSR_B200_OK;
+  }
+  // copies one slot to host memory ([chan*npol][nbin] and [nbin]) on the stream
+  int download_slot (unsigned k, float* h_prof, uint32_t* h_hits)
+  {
+    const size_t pitch = size_t (nbin) * slots * sizeof (float);
+    if (h_prof)
+      B200_CHECK (ctx, cudaMemcpy2DAsync (h_prof, nbin * sizeof (float),
+                                          profiles.ptr + size_t (k) * nbin, pitch,
+                                          nbin * sizeof (float), size_t (nchan) * npol,
+                                          cudaMemcpyDeviceToHost, ctx->stream), "download slot");
+    if (h_hits)
+      B200_CHECK (ctx, cudaMemcpyAsync (h_hits, hits.ptr + size_t (k) * nbin,
+                                        nbin * sizeof (unsigned), cudaMemcpyDeviceToHost,
+                                        ctx->stream), "download slot hits");
+    return DSPSR_B200_OK;
+  }
+  // installs a plan built by the caller (segments over ndat samples)
+  int set_plan (std::vector<FoldSegment>& segs, uint64_t n)
+  {
+    plan.swap (segs);
+    return upload_plan (n);
   }
   // builds the exact plan on the host and uploads it on the context's stream
   int set_bins (double phi, double pps, uint64_t n, double* x_end = nullptr)
   {
     build_fold_plan (phi, pps, n, &plan, x_end);
+    return upload_plan (n);
+  }
+  int upload_plan (uint64_t n)
+  {
     ndat = n;
     nseg = int (plan.size ());
     cur = (cur + 1) % NRING;
@@ -396,6 +438,7 @@ struct dspsr_b200_fold
     v.profiles = profiles.ptr;
     v.hits = hits.ptr;
     v.nbin = nbin;
+    v.stride = nbin * slots;
     v.state = state;
     v.nout = nout;
     return v;
@@ -481,6 +524,25 @@ struct dspsr_b200_pipeline
   // own phase recurrence, exactly as one fold of the whole block would
   bool in_pieces = false, phase_continue = false;
   double phase_next = 0;
+  // sub-integrations (Subint<Fold>): each division folds into its own slot of
+  // the fold's profiles; closed slots wait in sub_ready for the unloader or
+  // pop_subint, then are zeroed and reused
+  bool sub_on = false;
+  b200::SubintPlanner planner;
+  b200::SubintPlanner planner_init;            // the configured, unstarted divider
+  std::vector<b200::SubintAction> sub_actions;
+  struct SubSlot
+  {
+    bool used = false;
+    dspsr_b200_subint info {};
+  };
+  std::vector<SubSlot> sub_slots;
+  int sub_cur = -1;
+  std::deque<int> sub_ready;
+  dspsr_b200_unload_fn unload_fn = nullptr;
+  void* unload_user = nullptr;
+  std::vector<float> h_subprof;
+  std::vector<uint32_t> h_subhits;
   void* pinned[2] = {nullptr, nullptr};   // run_dada: file blocks in page-locked memory
   uint64_t pinned_bytes = 0;
   cudaEvent_t host_free[2] = {nullptr, nullptr};   // uploads of pinned[b] done
@@ -488,6 +550,147 @@ struct dspsr_b200_pipeline
 };
 
 namespace {
+
+// Subint<Fold>::transformation over one block's nout output samples
+// (Subint.h:258-332): the divider splits the block into ranges, each range
+// folds with its own phase (Fold::fold at its idat_start, Fold.C:685-693)
+// into the slot of its division, and a closed division joins sub_ready.
+// Samples outside every range are not folded.
+void subint_close (dspsr_b200_pipeline* pl)
+{
+  if (pl->sub_cur < 0) return;
+  auto& slot = pl->sub_slots[pl->sub_cur];
+  if (slot.info.ndat_folded > 0)
+    pl->sub_ready.push_back (pl->sub_cur);
+  else
+    slot.used = false;                 // nothing folded: still zero
+  pl->sub_cur = -1;
+}
+
+int pipeline_subint_plan (dspsr_b200_pipeline* pl, uint64_t nout, double pps)
+{
+  dspsr_b200_context* ctx = pl->ctx;
+  const auto& cfg = pl->cfg;
+  const ConvShape& sh = pl->conv.shape;
+  // the detected block's start: Convolution shifts its output by nfilt_pos
+  // samples (Convolution.C:611, Observation::change_start_time)
+  b200::Mjd start0;
+  start0.day = cfg.start_day;
+  start0.sec = cfg.start_sec;
+  start0.frac = cfg.start_frac;
+  const b200::Mjd start = b200::mjd_add (start0, double (pl->in0 + sh.nfilt_pos) / pl->rate);
+  b200::SubintPlanner trial = pl->planner;
+  const char* err = nullptr;
+  if (!trial.block (start, nout, pl->rate, &pl->sub_actions, &err))
+    return fail (ctx, DSPSR_B200_ESTATE, "pipeline sub-integrations: %s", err);
+  // every division the block opens needs a free slot now
+  unsigned need = 0, nfree = 0;
+  bool open = pl->sub_cur >= 0;
+  for (const auto& a : pl->sub_actions)
+  {
+    if (a.kind != b200::SubintAction::FOLD) { open = false; continue; }
+    if (!open) { need++; open = true; }
+  }
+  for (const auto& sl : pl->sub_slots) nfree += sl.used ? 0 : 1;
+  if (need > nfree)
+    return fail (ctx, DSPSR_B200_ESTATE,
+                 "pipeline: the block opens %u sub-integrations and %u of %zu slots are free "
+                 "(pop closed sub-integrations, set an unloader, raise subint_slots or pass "
+                 "shorter blocks)", need, nfree, pl->sub_slots.size ());
+  pl->planner = trial;
+
+  std::vector<FoldSegment> plan, part;
+  uint64_t cursor = 0;
+  auto skip = [&plan] (uint64_t at) {
+    FoldSegment g;
+    g.start = at;
+    g.m0 = 0;
+    g.dm = 0;
+    g.g = 1.0;
+    g.base = FOLD_SKIP;
+    plan.push_back (g);
+  };
+  for (const auto& a : pl->sub_actions)
+  {
+    if (a.kind != b200::SubintAction::FOLD)
+    {
+      subint_close (pl);
+      continue;
+    }
+    if (pl->sub_cur < 0)
+    {
+      int k = 0;
+      while (pl->sub_slots[k].used) k++;
+      auto& sl = pl->sub_slots[k];
+      sl.used = true;
+      sl.info = dspsr_b200_subint {};
+      sl.info.division = a.division;
+      sl.info.first_sample = pl->in0 + a.idat_start;
+      sl.info.lower_day = a.lower.day;
+      sl.info.lower_sec = a.lower.sec;
+      sl.info.lower_frac = a.lower.frac;
+      sl.info.upper_day = a.upper.day;
+      sl.info.upper_sec = a.upper.sec;
+      sl.info.upper_frac = a.upper.frac;
+      pl->sub_cur = k;
+    }
+    auto& sl = pl->sub_slots[pl->sub_cur];
+    sl.info.ndat_folded += a.ndat;
+    sl.info.integration_length = double (sl.info.ndat_folded) / pl->rate;
+    sl.info.complete = a.end_reached ? 1 : 0;
+    if (a.idat_start > cursor) skip (cursor);
+    const double phi = fold_phi (cfg.start_day, cfg.start_sec, cfg.start_frac, cfg.epoch_day,
+                                 cfg.epoch_sec, cfg.epoch_frac,
+                                 pl->in0 + sh.nfilt_pos + a.idat_start, pl->rate, cfg.period_s,
+                                 cfg.reference_phase);
+    build_fold_plan (phi, pps, a.ndat, &part);
+    const uint32_t base = uint32_t (pl->sub_cur) * pl->fold.nbin;
+    for (FoldSegment g : part)
+    {
+      g.start += a.idat_start;
+      g.base = base;
+      plan.push_back (g);
+    }
+    cursor = a.idat_start + a.ndat;
+  }
+  if (cursor < nout || plan.empty ()) skip (cursor);
+  return pl->fold.set_plan (plan, nout);
+}
+
+// hands closed sub-integration slot k to the caller's buffers (or to the
+// pipeline's own, for the unloader), then zeroes and frees the slot
+int subint_take (dspsr_b200_pipeline* pl, int k, dspsr_b200_subint* info, float* prof,
+                 uint32_t* hits)
+{
+  dspsr_b200_context* ctx = pl->ctx;
+  int rc = pl->fold.download_slot (unsigned (k), prof, hits);
+  if (rc) return rc;
+  B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "download sub-integration");
+  if (info) *info = pl->sub_slots[k].info;
+  rc = pl->fold.reset_slot (unsigned (k));
+  if (rc) return rc;
+  pl->sub_slots[k].used = false;
+  return DSPSR_B200_OK;
+}
+
+// PhaseSeriesUnloader::unload for every closed sub-integration, in order
+int subint_drain (dspsr_b200_pipeline* pl)
+{
+  if (!pl->unload_fn) return DSPSR_B200_OK;
+  const size_t nprof = size_t (pl->fold.nchan) * pl->fold.npol * pl->fold.nbin;
+  pl->h_subprof.resize (nprof);
+  pl->h_subhits.resize (pl->fold.nbin);
+  while (!pl->sub_ready.empty ())
+  {
+    const int k = pl->sub_ready.front ();
+    pl->sub_ready.pop_front ();
+    dspsr_b200_subint info;
+    int rc = subint_take (pl, k, &info, pl->h_subprof.data (), pl->h_subhits.data ());
+    if (rc) return rc;
+    pl->unload_fn (pl->unload_user, &info, pl->h_subprof.data (), pl->h_subhits.data ());
+  }
+  return DSPSR_B200_OK;
+}
 
 int pipeline_block (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat_new,
                     uint64_t in_span, uint64_t* ndat_folded)
@@ -520,16 +723,25 @@ int pipeline_block (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat_new
   {
     // Fold::fold (Fold.C:685-693): phase of the first output sample's midpoint;
     // the output starts nfilt_pos samples after the input (Convolution.C:599)
-    const double phi = pl->phase_continue
-                     ? pl->phase_next
-                     : fold_phi (cfg.start_day, cfg.start_sec, cfg.start_frac, cfg.epoch_day,
-                                 cfg.epoch_sec, cfg.epoch_frac, pl->in0 + sh.nfilt_pos,
-                                 pl->rate, cfg.period_s, cfg.reference_phase);
     const double sampling_interval = 1.0 / pl->rate;
     const double pps = sampling_interval / cfg.period_s;   // Fold.C:754-756
-    int rc = pl->fold.set_bins (phi, pps, nout, &pl->phase_next);
-    if (rc) return rc;
-    pl->phase_continue = pl->in_pieces;
+    int rc;
+    if (pl->sub_on)
+    {
+      rc = pipeline_subint_plan (pl, nout, pps);
+      if (rc) return rc;
+    }
+    else
+    {
+      const double phi = pl->phase_continue
+                       ? pl->phase_next
+                       : fold_phi (cfg.start_day, cfg.start_sec, cfg.start_frac, cfg.epoch_day,
+                                   cfg.epoch_sec, cfg.epoch_frac, pl->in0 + sh.nfilt_pos,
+                                   pl->rate, cfg.period_s, cfg.reference_phase);
+      rc = pl->fold.set_bins (phi, pps, nout, &pl->phase_next);
+      if (rc) return rc;
+      pl->phase_continue = pl->in_pieces;
+    }
     FoldView fv = pl->fold.view (cfg.state, pl->nout, cfg.nchan);
     VoltView vv {nullptr, 0};
     const ConvTables tb = pl->conv.tables ();
@@ -543,6 +755,11 @@ int pipeline_block (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat_new
     }
     rc = pl->fold.release_plan ();
     if (rc) return rc;
+    if (pl->sub_on)
+    {
+      rc = subint_drain (pl);
+      if (rc) return rc;
+    }
   }
 
   // InputBuffering (InputBuffering.C:66-174): samples [nout, ndat) carry over
@@ -1578,7 +1795,31 @@ int dspsr_b200_pipeline_create (dspsr_b200_context* ctx, const dspsr_b200_pipeli
                                 cudaMemcpyHostToDevice);
     if (e != cudaSuccess) rc = cuda_fail (ctx, e, "upload lut");
   }
-  if (!rc) rc = pl->fold.init (ctx, cfg->nbin, nchan, pl->nout);
+  // sub-integrations: Subint<Fold>::prepare hands the divider the folding
+  // period for divisions in turns (Subint.h:230-242)
+  if (!rc && (cfg->subint_seconds != 0 || cfg->subint_turns != 0))
+  {
+    if (cfg->subint_seconds < 0 || cfg->subint_turns < 0
+        || (cfg->subint_seconds > 0 && cfg->subint_turns > 0))
+      rc = fail (ctx, DSPSR_B200_EINVAL,
+                 "pipeline: subint_seconds=%g, subint_turns=%g: give one positive length",
+                 cfg->subint_seconds, cfg->subint_turns);
+    else
+    {
+      pl->sub_on = true;
+      b200::TimeDivide& d = pl->planner_init.divider;
+      d.division_seconds = cfg->subint_seconds;
+      d.division_turns = cfg->subint_turns;
+      d.period = cfg->period_s;
+      d.reference_epoch.day = cfg->subint_epoch_day;
+      d.reference_epoch.sec = cfg->subint_epoch_sec;
+      d.reference_epoch.frac = cfg->subint_epoch_frac;
+      pl->planner = pl->planner_init;
+      pl->sub_slots.resize (cfg->subint_slots ? cfg->subint_slots : 4);
+    }
+  }
+  if (!rc) rc = pl->fold.init (ctx, cfg->nbin, nchan, pl->nout,
+                               pl->sub_on ? unsigned (pl->sub_slots.size ()) : 1);
   // the carry never exceeds nfft samples: size both carry buffers once
   for (int i = 0; i < 2 && !rc; i++)
   {
@@ -1662,7 +1903,8 @@ int dspsr_b200_pipeline_run_host (dspsr_b200_pipeline* pl, const void* h_in, uin
   // joins blocks.  Pieces are whole filterbank transforms.
   const uint64_t unit = pl->fb_nsub ? pl->fb_nsub : 1;
   const uint64_t min_piece = uint64_t (pl->conv.shape.nfft) * unit * 2;
-  const uint64_t npiece = ndat >= 4 * min_piece ? 4 : ndat >= 2 * min_piece ? 2 : 1;
+  // (sub-integrations divide each block as a whole: no pieces)
+  const uint64_t npiece = pl->sub_on ? 1 : ndat >= 4 * min_piece ? 4 : ndat >= 2 * min_piece ? 2 : 1;
   const uint64_t piece = ((ndat + npiece - 1) / npiece + unit - 1) / unit * unit;
   const uint64_t bps = pl->bytes_per_sample;
   uint64_t total = 0;
@@ -1786,9 +2028,50 @@ int dspsr_b200_pipeline_run_dada (dspsr_b200_pipeline* pl, dspsr_b200_dada_file*
 int dspsr_b200_pipeline_get_profiles (dspsr_b200_pipeline* pl, float* profiles, uint32_t* hits)
 {
   if (!pl) return DSPSR_B200_EINVAL;
+  if (pl->sub_on)
+    return fail (pl->ctx, DSPSR_B200_ESTATE,
+                 "pipeline_get_profiles: the pipeline folds sub-integrations; take them with "
+                 "pop_subint or an unloader");
   int rc = dspsr_b200_fold_get_profiles (&pl->fold, profiles, hits);
   if (rc) return rc;
   return pl->conv.status ();
+}
+
+int dspsr_b200_pipeline_set_unloader (dspsr_b200_pipeline* pl, dspsr_b200_unload_fn fn,
+                                      void* user)
+{
+  if (!pl) return DSPSR_B200_EINVAL;
+  pl->unload_fn = fn;
+  pl->unload_user = user;
+  return pl->sub_on ? subint_drain (pl) : DSPSR_B200_OK;
+}
+
+int dspsr_b200_pipeline_subints_ready (dspsr_b200_pipeline* pl, uint64_t* n)
+{
+  if (!pl || !n) return DSPSR_B200_EINVAL;
+  *n = pl->sub_ready.size ();
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_pipeline_pop_subint (dspsr_b200_pipeline* pl, dspsr_b200_subint* subint,
+                                    float* profiles, uint32_t* hits)
+{
+  if (!pl) return DSPSR_B200_EINVAL;
+  if (!pl->sub_on)
+    return fail (pl->ctx, DSPSR_B200_ESTATE, "pop_subint: no sub-integrations configured");
+  if (pl->sub_ready.empty ())
+    return fail (pl->ctx, DSPSR_B200_ESTATE, "pop_subint: no closed sub-integration");
+  const int k = pl->sub_ready.front ();
+  pl->sub_ready.pop_front ();
+  return subint_take (pl, k, subint, profiles, hits);
+}
+
+int dspsr_b200_pipeline_finish (dspsr_b200_pipeline* pl)
+{
+  if (!pl) return DSPSR_B200_EINVAL;
+  if (!pl->sub_on) return DSPSR_B200_OK;
+  subint_close (pl);
+  return subint_drain (pl);
 }
 
 int dspsr_b200_pipeline_reset (dspsr_b200_pipeline* pl)
@@ -1796,6 +2079,13 @@ int dspsr_b200_pipeline_reset (dspsr_b200_pipeline* pl)
   if (!pl) return DSPSR_B200_EINVAL;
   pl->ncarry = 0;
   pl->in0 = 0;
+  if (pl->sub_on)
+  {
+    pl->planner = pl->planner_init;
+    for (auto& sl : pl->sub_slots) sl.used = false;
+    pl->sub_cur = -1;
+    pl->sub_ready.clear ();
+  }
   return pl->fold.reset ();
 }
 

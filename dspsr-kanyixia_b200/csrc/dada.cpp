@@ -5,6 +5,7 @@
 // (Kernel/Classes/File.C).  Host code only: blocks read here go to the
 // device through dspsr_b200_pipeline_run_dada (capi.cu).
 #include "dada.h"
+#include "subint.h"
 
 #include <algorithm>
 #include <cerrno>
@@ -20,9 +21,8 @@
 #include <sys/stat.h>
 #include <unistd.h>
 
-namespace
+namespace dspsr_b200_host
 {
-
 thread_local std::string host_error;
 
 int host_fail (int code, const char* fmt, ...)
@@ -35,6 +35,14 @@ int host_fail (int code, const char* fmt, ...)
   host_error = buf;
   return code;
 }
+}  // namespace dspsr_b200_host
+
+using dspsr_b200_host::host_fail;
+using dspsr_b200_host::host_error;
+using b200::mjd_add;
+
+namespace
+{
 
 // DADAHeader::default_header_size (DADAHeader.C:22)
 constexpr uint64_t DEFAULT_HEADER_SIZE = 4096;
@@ -149,18 +157,17 @@ bool utc_to_mjd (const char* text, int64_t* day, int64_t* sec)
   return true;
 }
 
-// MJD += seconds, keeping the fraction in [0, 1) and the seconds in [0, 86400)
+// MJD += seconds on the info's (day, sec, frac) fields
 void mjd_add (int64_t* day, int64_t* sec, double* frac, double seconds)
 {
-  const double f = *frac + seconds;
-  const double whole = std::floor (f);
-  *frac = f - whole;
-  int64_t s = *sec + int64_t (whole);
-  int64_t d = s / 86400;
-  s -= d * 86400;
-  if (s < 0) { s += 86400; d -= 1; }
-  *sec = s;
-  *day += d;
+  b200::Mjd m;
+  m.day = *day;
+  m.sec = *sec;
+  m.frac = *frac;
+  m = b200::mjd_add (m, seconds);
+  *day = m.day;
+  *sec = m.sec;
+  *frac = m.frac;
 }
 
 // replace_extension (psrchive's Util/genutil, used by DADAHeader.C:89): the

@@ -7,14 +7,19 @@
 namespace b200 {
 
 // One arithmetic segment of the exact fold-bin plan: sample start+j (j below
-// the next segment's start) has frac(phi) = (m0 + j*dm) * g exactly.
+// the next segment's start) has frac(phi) = (m0 + j*dm) * g exactly, and
+// folds into profile column base + bin (base = sub-integration slot * nbin;
+// FOLD_SKIP: the samples are not folded).
 struct FoldSegment
 {
   uint64_t start;
   int64_t m0;
   int64_t dm;
   double g;
+  uint32_t base = 0;
+  uint32_t pad = 0;
 };
+constexpr uint32_t FOLD_SKIP = 0xffffffffu;
 
 unsigned smearing_samples (double centre_frequency, double bandwidth, double dm,
                            unsigned nchan, int half);

@@ -182,21 +182,26 @@ __device__ __forceinline__ unsigned fold_bin (const FoldSegment* __restrict__ se
   return seg_bin (segs, seg_search (segs, nseg, t), t, nbin);
 }
 
-// Bins of a warp whose active lanes hold increasing sample indices: one binary
-// search by the first active lane, then each lane steps forward over the (few)
-// segment boundaries between it and that lane.  All 32 lanes call this.
+// Profile columns of a warp whose active lanes hold increasing sample
+// indices: one binary search by the first active lane, then each lane steps
+// forward over the (few) segment boundaries between it and that lane.  The
+// column is the segment's base plus the bin; NO_COLUMN for skipped samples
+// and bins outside [0, nbin).  All 32 lanes call this.
+constexpr unsigned NO_COLUMN = 0xffffffffu;
 __device__ __forceinline__ unsigned warp_fold_bin (const FoldSegment* __restrict__ segs,
                                                    int nseg, bool ok, uint64_t t, unsigned nbin)
 {
   const unsigned act = __ballot_sync (FULL, ok);
-  if (!act) return 0;
+  if (!act) return NO_COLUMN;
   const int leader = __ffs (act) - 1;
   int s = 0;
   if ((threadIdx.x & 31) == leader) s = seg_search (segs, nseg, t);
   s = __shfl_sync (FULL, s, leader);
-  if (!ok) return 0;
+  if (!ok) return NO_COLUMN;
   while (s + 1 < nseg && __ldg (&segs[s + 1].start) <= t) s++;
-  return seg_bin (segs, s, t, nbin);
+  const unsigned base = __ldg (&segs[s].base);
+  const unsigned bin = seg_bin (segs, s, t, nbin);
+  return (base == FOLD_SKIP || bin >= nbin) ? NO_COLUMN : base + bin;
 }
 
 // All 32 lanes call this together.  Lanes holding consecutive time samples
@@ -248,9 +253,9 @@ __device__ __forceinline__ void emit_fold (const FoldView& fv, unsigned c, unsig
   if (ok)
   {
     detect_values (fv.state, npol, p, q, v);
-    ok = bin < fv.nbin;
+    ok = bin < fv.stride;
   }
-  warp_fold<NOUT> (ok, bin, v, fv.profiles + uint64_t (c) * NOUT * fv.nbin, fv.nbin,
+  warp_fold<NOUT> (ok, bin, v, fv.profiles + uint64_t (c) * NOUT * fv.stride, fv.stride,
                    c == 0 ? fv.hits : nullptr);
 }
 
@@ -1329,11 +1334,11 @@ __global__ void k_fold (const float* __restrict__ in, const uint64_t in_span,
   const unsigned c = blockIdx.y;
   bool ok = t < ndat;
   const unsigned bin = warp_fold_bin (fv.segs, fv.nseg, ok, t, fv.nbin);
-  ok = ok && bin < fv.nbin;
+  ok = ok && bin < fv.stride;
   for (unsigned p = 0; p < npol; p++)
   {
     float v = ok ? in[(uint64_t (c) * npol + p) * in_span + t] : 0.f;
-    warp_fold<1> (ok, bin, &v, fv.profiles + (uint64_t (c) * npol + p) * fv.nbin, fv.nbin,
+    warp_fold<1> (ok, bin, &v, fv.profiles + (uint64_t (c) * npol + p) * fv.stride, fv.stride,
                   (c == 0 && p == 0) ? fv.hits : nullptr);
   }
 }

@@ -30,9 +30,10 @@ struct FoldView
 {
   const FoldSegment* segs;
   int nseg;
-  float* profiles;       // [chan][nout][nbin]
-  unsigned* hits;        // [nbin]
+  float* profiles;       // [chan][nout][stride]
+  unsigned* hits;        // [stride]
   unsigned nbin;
+  unsigned stride;       // profile columns: nbin times the sub-integration slots
   int state;
   int nout;
 };

@@ -26,7 +26,7 @@ from ._capi import (B200Error, PipelineConfig, INTENSITY, PPQQ, COHERENCE, STOKE
 __all__ = ["Context", "Convolution", "InverseFilterbank", "Fold", "apodization", "Pipeline", "PipelineConfig", "B200Error",
            "smearing_samples", "minimum_ndat", "optimal_fft_length", "bittable8", "fold_phi",
            "sk_limits", "DADAFile", "dada_parse", "dada_is_valid", "ascii_header_get",
-           "ascii_header_set", "write_dada",
+           "ascii_header_set", "write_dada", "TimeDivide",
            "fold_plan_count", "INTENSITY", "PPQQ", "COHERENCE", "STOKES", "INT8_TFPD",
            "INT16_TFPD", "FLOAT_FPT", "CHIRP_REFERENCE", "CHIRP_FP64", "NOUT"]
 
@@ -432,6 +432,44 @@ class Pipeline:
             ctypes.byref(nfold)), "pipeline_run_dada")
         return nread.value, nfold.value
 
+    def set_unloader(self, fn):
+        """PhaseSeriesUnloader: fn(info: dict, profiles [chan][nout][nbin], hits [nbin])
+        is called for every closed sub-integration (copies of the arrays)."""
+        c = self.config
+        nchan = c.nchan * (c.filterbank_nchan if c.filterbank_nchan > 1 else 1)
+        shape = (nchan, self.nout, c.nbin)
+
+        def tramp(user, info, prof, hits):
+            p = np.ctypeslib.as_array(prof, shape=(int(np.prod(shape)),)).reshape(shape).copy()
+            h = np.ctypeslib.as_array(hits, shape=(c.nbin,)).copy()
+            fn(_struct_dict(info.contents), p, h)
+
+        self._unload = _capi.UNLOAD_FN(tramp) if fn is not None else _capi.UNLOAD_FN()
+        self.ctx.check(self._lib.dspsr_b200_pipeline_set_unloader(self.handle, self._unload, None),
+                       "set_unloader")
+
+    def subints_ready(self):
+        n = ctypes.c_uint64()
+        self.ctx.check(self._lib.dspsr_b200_pipeline_subints_ready(self.handle, ctypes.byref(n)),
+                       "subints_ready")
+        return n.value
+
+    def pop_subint(self):
+        """The oldest closed sub-integration: (info dict, profiles, hits)."""
+        c = self.config
+        nchan = c.nchan * (c.filterbank_nchan if c.filterbank_nchan > 1 else 1)
+        prof = np.empty((nchan, self.nout, c.nbin), np.float32)
+        hits = np.empty(c.nbin, np.uint32)
+        info = _capi.Subint()
+        self.ctx.check(self._lib.dspsr_b200_pipeline_pop_subint(
+            self.handle, ctypes.byref(info), _fptr(prof), hits.ctypes.data_as(_capi.c_u32p)),
+            "pop_subint")
+        return _struct_dict(info), prof, hits
+
+    def finish(self):
+        """Subint::finish: close the open sub-integration."""
+        self.ctx.check(self._lib.dspsr_b200_pipeline_finish(self.handle), "pipeline_finish")
+
     def get_profiles(self):
         c = self.config
         nchan = c.nchan * (c.filterbank_nchan if c.filterbank_nchan > 1 else 1)
@@ -502,6 +540,44 @@ def ascii_header_set(header, keyword, value, header_size=4096):
     _host_check(_capi.lib().dspsr_b200_ascii_header_set(buf, header_size, _cstr(keyword),
                                                         _cstr(str(value))), "ascii_header_set")
     return buf.value.decode()
+
+
+def _struct_dict(st):
+    return {name: getattr(st, name) for name, _ in st._fields_}
+
+
+class TimeDivide:
+    """TimeDivide + the block loop of Subint<Fold> on the host: the ranges of
+    each block that fold into each division, and where divisions close."""
+
+    def __init__(self, seconds=0.0, turns=0.0, period=0.0, reference_epoch=(0, 0, 0.0)):
+        self._lib = _capi.lib()
+        h = ctypes.c_void_p()
+        _host_check(self._lib.dspsr_b200_time_divide_create(seconds, turns, period,
+                                                             *reference_epoch, ctypes.byref(h)),
+                    "time_divide_create")
+        self.handle = h
+
+    def block(self, start_mjd, ndat, rate, cap=4096):
+        """Actions for a block of ndat samples at rate starting at start_mjd:
+        a list of dicts (kind 0 fold, 1 close partial, 2 close complete)."""
+        acts = (_capi.SubintAction * cap)()
+        n = ctypes.c_uint64()
+        _host_check(self._lib.dspsr_b200_time_divide_block(self.handle, *start_mjd, ndat, rate,
+                                                            acts, cap, ctypes.byref(n)),
+                    "time_divide_block")
+        return [_struct_dict(acts[i]) for i in range(n.value)]
+
+    def close(self):
+        if self.handle:
+            self._lib.dspsr_b200_time_divide_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _info_dict(info):
@@ -613,7 +689,9 @@ def write_dada(filename, keys, data, header_size=4096):
 def make_config(centre_freq, bandwidth, dm, nchan, npol, nfft, nfilt_pos, nfilt_neg, nbin,
                 period, state=INTENSITY, input_kind=INT8_TFPD, lut=None, chirp_mode=CHIRP_REFERENCE,
                 start_mjd=(60000, 0, 0.0), epoch_mjd=(60000, 0, 0.0), reference_phase=0.0,
-                dual_sideband=1, offset_binary=0, scratch_bytes=0, filterbank_nchan=0):
+                dual_sideband=1, offset_binary=0, scratch_bytes=0, filterbank_nchan=0,
+                subint_seconds=0.0, subint_turns=0.0, subint_slots=0,
+                subint_epoch=(0, 0, 0.0)):
     """Fill a PipelineConfig (the fields DedispersionPipe / LoadToFold set up).
     With filterbank_nchan > 1, nchan counts input channels, and nfft and the
     smearing (nfilt_pos, nfilt_neg) refer to the filterbank's output channels."""
@@ -643,6 +721,10 @@ def make_config(centre_freq, bandwidth, dm, nchan, npol, nfft, nfilt_pos, nfilt_
     cfg.epoch_day, cfg.epoch_sec, cfg.epoch_frac = epoch_mjd
     cfg.start_day, cfg.start_sec, cfg.start_frac = start_mjd
     cfg.scratch_bytes = scratch_bytes
+    cfg.subint_seconds = subint_seconds
+    cfg.subint_turns = subint_turns
+    cfg.subint_slots = subint_slots
+    cfg.subint_epoch_day, cfg.subint_epoch_sec, cfg.subint_epoch_frac = subint_epoch
     return cfg
 
 

@@ -58,7 +58,52 @@ class PipelineConfig(ctypes.Structure):
         ("start_frac", c_dbl),
         ("scratch_bytes", c_u64),
         ("filterbank_nchan", c_uint),
+        ("subint_seconds", c_dbl),
+        ("subint_turns", c_dbl),
+        ("subint_epoch_day", c_i64),
+        ("subint_epoch_sec", c_i64),
+        ("subint_epoch_frac", c_dbl),
+        ("subint_slots", c_uint),
     ]
+
+
+class SubintAction(ctypes.Structure):
+    """dspsr_b200_subint_action"""
+    _fields_ = [
+        ("kind", c_int),
+        ("end_reached", c_int),
+        ("idat_start", c_u64),
+        ("ndat", c_u64),
+        ("division", c_u64),
+        ("lower_day", c_i64),
+        ("lower_sec", c_i64),
+        ("lower_frac", c_dbl),
+        ("upper_day", c_i64),
+        ("upper_sec", c_i64),
+        ("upper_frac", c_dbl),
+    ]
+
+
+class Subint(ctypes.Structure):
+    """dspsr_b200_subint"""
+    _fields_ = [
+        ("division", c_u64),
+        ("ndat_folded", c_u64),
+        ("first_sample", c_u64),
+        ("lower_day", c_i64),
+        ("lower_sec", c_i64),
+        ("lower_frac", c_dbl),
+        ("upper_day", c_i64),
+        ("upper_sec", c_i64),
+        ("upper_frac", c_dbl),
+        ("integration_length", c_dbl),
+        ("complete", c_int),
+    ]
+
+
+UNLOAD_FN = ctypes.CFUNCTYPE(None, c_vp, ctypes.POINTER(Subint), ctypes.POINTER(ctypes.c_float),
+                             ctypes.POINTER(ctypes.c_uint32))
+SUBINT_FOLD, SUBINT_CLOSE_PARTIAL, SUBINT_CLOSE_COMPLETE = 0, 1, 2
 
 
 class IfbConfig(ctypes.Structure):
@@ -177,6 +222,15 @@ SIGNATURES = {
     "dspsr_b200_pipeline_kernel_times": (c_int, [c_vp, ctypes.POINTER(c_dbl), c_u64p]),
     "dspsr_b200_kernel_launches": (c_u64, []),
     "dspsr_b200_host_error": (ctypes.c_char_p, []),
+    "dspsr_b200_time_divide_create": (c_int, [c_dbl, c_dbl, c_dbl, c_i64, c_i64, c_dbl,
+                                              ctypes.POINTER(c_vp)]),
+    "dspsr_b200_time_divide_block": (c_int, [c_vp, c_i64, c_i64, c_dbl, c_u64, c_dbl,
+                                             ctypes.POINTER(SubintAction), c_u64, c_u64p]),
+    "dspsr_b200_time_divide_destroy": (c_int, [c_vp]),
+    "dspsr_b200_pipeline_set_unloader": (c_int, [c_vp, UNLOAD_FN, c_vp]),
+    "dspsr_b200_pipeline_subints_ready": (c_int, [c_vp, c_u64p]),
+    "dspsr_b200_pipeline_pop_subint": (c_int, [c_vp, ctypes.POINTER(Subint), c_fp, c_u32p]),
+    "dspsr_b200_pipeline_finish": (c_int, [c_vp]),
     "dspsr_b200_ascii_header_get": (c_int, [ctypes.c_char_p, ctypes.c_char_p, c_vp, c_u64]),
     "dspsr_b200_ascii_header_set": (c_int, [c_vp, c_u64, ctypes.c_char_p, ctypes.c_char_p]),
     "dspsr_b200_dada_parse": (c_int, [ctypes.c_char_p, c_u64, ctypes.POINTER(DadaInfo)]),

@@ -400,6 +400,16 @@ typedef struct
      none, else a power of two in [4, 4096]; blocks must then be multiples
      of it */
   unsigned filterbank_nchan;
+  /* sub-integrations (Subint<Fold> with TimeDivide, Signal/Pulsar/dsp/
+     Subint.h:206-332, TimeDivide.C): both zero = one integration, read by
+     _get_profiles; otherwise each division is folded into its own profiles
+     and handed out when closed (_set_unloader, or _pop_subint) */
+  double subint_seconds;    /* TimeDivide::set_seconds (division length) */
+  double subint_turns;      /* TimeDivide::set_turns, of period_s */
+  int64_t subint_epoch_day, subint_epoch_sec;   /* TimeDivide::set_reference_epoch; */
+  double subint_epoch_frac;                     /* all zero = none */
+  unsigned subint_slots;    /* divisions held on the device at once (0 = 4); one
+                               block may touch at most this many */
 } dspsr_b200_pipeline_config;
 
 int dspsr_b200_pipeline_create (dspsr_b200_context* ctx,
@@ -433,6 +443,73 @@ int dspsr_b200_pipeline_kernel_times (dspsr_b200_pipeline* pipe, double* ms,
 uint64_t dspsr_b200_kernel_launches (void);
 /* shape of the plan: nfft, nkeep, FFT split n1 x n2, parts per batch */
 int dspsr_b200_pipeline_info (dspsr_b200_pipeline* pipe, uint64_t* info8);
+
+/* ---------------------------------------------------------------------- */
+/* Sub-integrations                                                        */
+/* ---------------------------------------------------------------------- */
+
+#define DSPSR_B200_SUBINT_FOLD           0   /* fold a range of the block */
+#define DSPSR_B200_SUBINT_CLOSE_PARTIAL  1   /* Subint::unload_partial */
+#define DSPSR_B200_SUBINT_CLOSE_COMPLETE 2   /* Subint::transformation's unload */
+
+/* one step of Subint<Fold>::transformation for a block (Subint.h:258-332) */
+typedef struct
+{
+  int kind;                          /* DSPSR_B200_SUBINT_* */
+  int end_reached;                   /* FOLD: the range ends its division */
+  uint64_t idat_start, ndat;         /* FOLD: samples of the block */
+  uint64_t division;                 /* FOLD: TimeDivide::get_division */
+  int64_t lower_day, lower_sec;      /* FOLD: the division's start ... */
+  double lower_frac;
+  int64_t upper_day, upper_sec;      /* ... and end, rounded to whole samples */
+  double upper_frac;
+} dspsr_b200_subint_action;
+
+typedef struct dspsr_b200_time_divide dspsr_b200_time_divide;
+
+/* TimeDivide with a division length in seconds, or in turns of a constant
+   period (TimeDivide.C:40-537 without a Pulsar::Predictor), driven by the
+   per-block loop of Subint<Fold>.  Host only. */
+int dspsr_b200_time_divide_create (double seconds, double turns, double period_s,
+                                   int64_t epoch_day, int64_t epoch_sec, double epoch_frac,
+                                   dspsr_b200_time_divide** td);
+/* The actions for one block of ndat samples at rate (Hz) starting at the MJD
+   (start_day, start_sec, start_frac): up to cap into actions, *n = count. */
+int dspsr_b200_time_divide_block (dspsr_b200_time_divide* td, int64_t start_day,
+                                  int64_t start_sec, double start_frac, uint64_t ndat,
+                                  double rate, dspsr_b200_subint_action* actions, uint64_t cap,
+                                  uint64_t* n);
+int dspsr_b200_time_divide_destroy (dspsr_b200_time_divide* td);
+
+/* A closed sub-integration of the pipeline (the PhaseSeries handed to
+   PhaseSeriesUnloader::unload / partial) */
+typedef struct
+{
+  uint64_t division;             /* TimeDivide division index */
+  uint64_t ndat_folded;          /* output samples folded into it */
+  uint64_t first_sample;         /* global output index of the first of them */
+  int64_t lower_day, lower_sec;  /* division start */
+  double lower_frac;
+  int64_t upper_day, upper_sec;  /* division end */
+  double upper_frac;
+  double integration_length;     /* ndat_folded / rate, seconds */
+  int complete;                  /* its end was reached (else the data stopped) */
+} dspsr_b200_subint;
+
+/* PhaseSeriesUnloader::unload: called in division order on the calling
+   thread, during _run, _run_host, _run_dada or _finish, with profiles
+   [chan][nout][nbin] and hits[nbin] in host memory valid for the call */
+typedef void (*dspsr_b200_unload_fn) (void* user, const dspsr_b200_subint* subint,
+                                      const float* profiles, const uint32_t* hits);
+int dspsr_b200_pipeline_set_unloader (dspsr_b200_pipeline* pipe, dspsr_b200_unload_fn fn,
+                                      void* user);
+/* closed sub-integrations waiting (when no unloader is set) */
+int dspsr_b200_pipeline_subints_ready (dspsr_b200_pipeline* pipe, uint64_t* n);
+/* the oldest closed sub-integration into host memory; ESTATE when none */
+int dspsr_b200_pipeline_pop_subint (dspsr_b200_pipeline* pipe, dspsr_b200_subint* subint,
+                                    float* profiles, uint32_t* hits);
+/* Subint::finish (Subint.h:345-362): closes the open division (partial) */
+int dspsr_b200_pipeline_finish (dspsr_b200_pipeline* pipe);
 
 /* ---------------------------------------------------------------------- */
 /* DADA file source (host only, no GPU needed except for _pipeline_run_dada) */

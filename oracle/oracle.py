@@ -382,3 +382,126 @@ def pipeline_c1(raw, ndat, lut, response, nfft, nfilt_pos, nfilt_neg, phi, pps, 
                               np.ascontiguousarray(response, np.complex64).view(np.float32).ravel(),
                               nfft, nfilt_pos, nfilt_neg, phi, pps, nbin, prof, hits, nthreads)
     return prof, hits, n
+
+
+# ---------------------------------------------------------------------------
+# TimeDivide (Signal/Pulsar/TimeDivide.C) and the block loop of Subint<Fold>
+# (Signal/Pulsar/dsp/Subint.h:206-362), pure Python.  MJDs are
+# (day, second, fraction) tuples; the arithmetic follows PSRCHIVE's MJD
+# (whole days and seconds plus a fraction), which is not in the reference
+# tree, so it is restated, not pinned.
+# ---------------------------------------------------------------------------
+
+import math
+
+
+def mjd_add(m, seconds):
+    day, sec, frac = m
+    f = frac + seconds
+    whole = math.floor(f)
+    frac = f - whole
+    d, s = divmod(sec + int(whole), 86400)
+    return (day + d, s, frac)
+
+
+def mjd_diff(a, b):
+    """(a - b).in_seconds()"""
+    return float((a[0] - b[0]) * 86400 + (a[1] - b[1])) + (a[2] - b[2])
+
+
+def _rint(x):
+    return int(round(x))          # half to even, as rint / lrint
+
+
+class TimeDivideOracle:
+    """TimeDivide with a length in seconds, or in turns of a constant period."""
+
+    def __init__(self, seconds=0.0, turns=0.0, period=0.0, reference_epoch=(0, 0, 0.0)):
+        self.seconds, self.turns, self.period = seconds, turns, period
+        self.reference_epoch = tuple(reference_epoch)
+        self.start_time = (0, 0, 0.0)
+        self.lower = self.upper = self.current_end = (0, 0, 0.0)
+        self.is_valid = False
+        self.division = 0
+
+    # TimeDivide.C:40-76
+    def set_start_time(self, t):
+        if self.start_time == tuple(t):
+            return
+        self.start_time = tuple(t)
+        self.is_valid = False
+        if self.reference_epoch != (0, 0, 0.0):
+            self.start_time = self.reference_epoch
+        elif self.seconds and self.seconds == float(int(self.seconds)):
+            isec = int(self.seconds)
+            day, sec, _ = self.start_time
+            self.start_time = (day, (sec // isec) * isec, 0.0)
+
+    # TimeDivide.C:503-537
+    def _round_bounds(self, m1, m2, obs_start, rate):
+        samples = _rint(mjd_diff(m1, obs_start) * rate)
+        self.lower = mjd_add(obs_start, samples / rate)
+        self.division_ndat = _rint(mjd_diff(m2, self.lower) * rate)
+        self.upper = mjd_add(self.lower, self.division_ndat / rate)
+
+    # TimeDivide.C:349-501 (no predictor)
+    def _set_boundaries(self, t, obs_start, rate):
+        divide_start = max(self.start_time, t)
+        spi = self.seconds if not self.turns else self.period * self.turns
+        self.division = int(mjd_diff(divide_start, self.start_time) / spi)
+        self._round_bounds(mjd_add(self.start_time, self.division * spi),
+                           mjd_add(self.start_time, (self.division + 1) * spi), obs_start, rate)
+
+    # TimeDivide.C:130-333
+    def set_bounds(self, start, ndat, rate):
+        start = tuple(start)
+        end = mjd_add(start, ndat / rate) if ndat else start
+        divide_start = max(self.current_end, start) if self.is_valid else start
+        self.new_division = self.end_reached = self.in_next = False
+        if end < self.lower or self.upper < mjd_add(divide_start, 0.5 / rate):
+            self.new_division = True
+            self._set_boundaries(mjd_add(divide_start, 0.55 / rate), start, rate)
+        divide_start = max(self.lower, divide_start)
+        self.idat_start = _rint(mjd_diff(divide_start, start) * rate)
+        if self.idat_start >= ndat:
+            self.is_valid = False
+            return
+        divide_end = min(end, self.upper)
+        idat_end = _rint(mjd_diff(divide_end, start) * rate)
+        assert idat_end > self.idat_start
+        if idat_end > ndat:
+            idat_end = ndat
+        elif idat_end < ndat:
+            self.in_next = True
+        self.ndat = idat_end - self.idat_start
+        if mjd_diff(self.upper, divide_end) * rate < 0.5:
+            self.end_reached = True
+        self.is_valid = True
+        self.current_end = mjd_add(start, idat_end / rate)
+
+
+def subint_block_actions(td, start, ndat, rate):
+    """Subint<Fold>::transformation for one block (Subint.h:258-332): a list
+    of ("fold", idat_start, ndat, division, end_reached) and ("close", kind)
+    steps, kind "partial" or "complete"."""
+    if td.start_time == (0, 0, 0.0):
+        td.set_start_time(start)
+    out = []
+    more, first = True, True
+    while more:
+        td.set_bounds(start, ndat, rate)
+        more = td.in_next
+        if first and td.new_division:
+            out.append(("close", "partial"))
+        if not td.is_valid:
+            continue
+        out.append(("fold", td.idat_start, td.ndat, td.division, td.end_reached,
+                    td.lower, td.upper))
+        if not td.end_reached:
+            continue
+        if first:
+            out.append(("close", "partial"))
+            first = False
+            continue
+        out.append(("close", "complete"))
+    return out

@@ -22,6 +22,12 @@ EPOCH = (59999, 0, 0.0)
 def oracle_chain(orc, b2, raw_blocks, cfg, fp64=False):
     """raw_blocks: list of TFPD arrays.  Mirrors SingleThread::run over the
     blocks: unpack, overlap-save, detect, fold with one phase per block."""
+    d, nchan = oracle_detected(orc, b2, raw_blocks, cfg, fp64)
+    return oracle_fold(orc, b2, raw_blocks, cfg, d, nchan)
+
+
+def oracle_detected(orc, b2, raw_blocks, cfg, fp64=False):
+    """The detected output of the whole stream: (d [chan][nout][t], nchan)."""
     nchan, npol = cfg["nchan"], cfg["npol"]
     kind = cfg["kind"]
     raw = np.concatenate([r.reshape(-1) for r in raw_blocks])
@@ -60,6 +66,70 @@ def oracle_chain(orc, b2, raw_blocks, cfg, fp64=False):
         d = d.reshape(nchan, 1, -1)
     else:
         d = orc.detect(y, cfg["state"])
+    return d, nchan
+
+
+def block_outputs(b2, raw_blocks, cfg):
+    """(in0, nout) of each block: the parts the overlap carry completes."""
+    nk = cfg["nfft"] - cfg["pos"] - cfg["neg"]
+    fb = cfg.get("fb", 0)
+    out, in0, carry = [], 0, 0
+    for r in raw_blocks:
+        nb = r.shape[-1] // 2 if cfg["kind"] == b2.FLOAT_FPT else r.size // (cfg["nchan"] * cfg["npol"] * 2)
+        if fb:
+            nb //= fb
+        ndat = carry + nb
+        npart = (ndat - cfg["pos"] - cfg["neg"]) // nk if ndat >= cfg["nfft"] else 0
+        out.append((in0, npart * nk))
+        in0 += npart * nk
+        carry = ndat - npart * nk
+    return out
+
+
+def oracle_subints(orc, b2, raw_blocks, cfg, td_kw):
+    """Subint<Fold> over the blocks: each range folds with its own phase into
+    its division; closed divisions with data are returned in order as
+    (division, first_sample, ndat_folded, profiles, hits)."""
+    d, nchan = oracle_detected(orc, b2, raw_blocks, cfg)
+    rate = abs(cfg["bw"]) / nchan * 1e6
+    pps = (1.0 / rate) / cfg["period"]
+    nbin = cfg["nbin"]
+    td = orc.TimeDivideOracle(**td_kw)
+    subs, cur = [], None
+
+    def close():
+        nonlocal cur
+        if cur is not None and cur[2] > 0:
+            subs.append(tuple(cur))
+        cur = None
+
+    for in0, nout in block_outputs(b2, raw_blocks, cfg):
+        if nout == 0:
+            continue
+        start = orc.mjd_add(START, (in0 + cfg["pos"]) / rate)
+        for a in orc.subint_block_actions(td, start, nout, rate):
+            if a[0] == "close":
+                close()
+                continue
+            _, i0, n, div = a[:4]
+            if cur is None:
+                cur = [div, in0 + i0, 0, np.zeros((nchan, d.shape[1], nbin), d.dtype),
+                       np.zeros(nbin, np.uint32)]
+            phi = orc.fold_phi(START, EPOCH, in0 + cfg["pos"] + i0, rate, cfg["period"])
+            plan = orc.fold_binplan(phi, pps, n, nbin)
+            orc.fold_accumulate(np.ascontiguousarray(d[:, :, in0 + i0:in0 + i0 + n]), plan, nbin,
+                                cur[3], cur[4])
+            cur[2] += n
+    close()
+    return subs
+
+
+def oracle_fold(orc, b2, raw_blocks, cfg, d, nchan):
+    npol = cfg["npol"]
+    kind = cfg["kind"]
+    nfft, pos, neg = cfg["nfft"], cfg["pos"], cfg["neg"]
+    nk = nfft - pos - neg
+    fb = cfg.get("fb", 0)
     rate = abs(cfg["bw"]) / nchan * 1e6
     pps = (1.0 / rate) / cfg["period"]
     nbin = cfg["nbin"]
@@ -355,3 +425,100 @@ def test_pipeline_dada_window_and_rejects(ctx, b2, tmp_path):
         with pytest.raises(b2.B200Error, match="multiple of 16"):
             pl.run_dada(f, 10008)
         pl.close()
+
+
+def run_subints(ctx, b2, blocks, cfg, td_kw, slots=0, pop=False, host=False):
+    """The pipeline with sub-integrations: closed divisions as (info, prof, hits)."""
+    kw = dict(subint_seconds=td_kw.get("seconds", 0.0), subint_turns=td_kw.get("turns", 0.0),
+              subint_slots=slots)
+    if "reference_epoch" in td_kw:
+        kw["subint_epoch"] = td_kw["reference_epoch"]
+    c = b2.make_config(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nchan"], cfg["npol"], cfg["nfft"],
+                       cfg["pos"], cfg["neg"], cfg["nbin"], cfg["period"], state=cfg["state"],
+                       input_kind=cfg["kind"], lut=cfg["lut"], start_mjd=START, epoch_mjd=EPOCH,
+                       filterbank_nchan=cfg.get("fb", 0), **kw)
+    pl = b2.Pipeline(ctx, c)
+    got = []
+    if not pop:
+        pl.set_unloader(lambda info, prof, hits: got.append((info, prof, hits)))
+    for r in blocks:
+        n = r.size // (cfg["nchan"] * cfg["npol"] * 2)
+        if host:
+            pl.run_host(r, n)
+        else:
+            pl.run(torch.from_numpy(r).cuda(), n)
+        if pop:
+            while pl.subints_ready():
+                got.append(pl.pop_subint())
+    pl.finish()
+    while pop and pl.subints_ready():
+        got.append(pl.pop_subint())
+    with pytest.raises(b2.B200Error, match="sub-integrations"):
+        pl.get_profiles()
+    pl.close()
+    return got
+
+
+def check_subints(got, want, cfg, rate):
+    assert len(got) == len(want) > 1
+    for (info, prof, hits), (div, first, n, rprof, rhits) in zip(got, want):
+        assert (info["division"], info["first_sample"], info["ndat_folded"]) == (div, first, n)
+        assert info["integration_length"] == n / rate
+        check(prof, hits, int(hits.sum()), rprof.astype(np.float64), rhits, int(rhits.sum()),
+              cfg["state"])
+
+
+SUBINT_CASES = {
+    # seconds: three blocks of ~3.3 ms at 16 MHz over 1 ms divisions, fused path
+    "seconds_fused": (dict(dm=5.0, nbin=128, period=0.00123), dict(seconds=0.001), 0),
+    # single-pulse mode (one turn per division), four-step path, Stokes, 2 channels
+    "turns_fourstep": (dict(dm=3.0, bw=32.0, nchan=2, nfft=1 << 15, state=3, nbin=256,
+                            period=0.0009), dict(turns=1.0, period=0.0009), 16),
+    # a reference epoch and a 16-channel filterbank in front
+    "epoch_filterbank": (dict(dm=30.0, bw=64.0, fb=16, nfft=1 << 13, state=3, nbin=256,
+                              period=0.0041), dict(seconds=0.002,
+                                                   reference_epoch=(60000, 3599, 0.9993)), 8),
+}
+
+
+@pytest.mark.parametrize("name", list(SUBINT_CASES))
+def test_pipeline_subints_match_oracle(ctx, b2, orc, name):
+    """Subint<Fold>: every closed division's profiles, hits and sample count
+    against the oracle's TimeDivide + fold, delivered through the unloader;
+    the same through pop_subint from host input."""
+    kw, td_kw, slots = SUBINT_CASES[name]
+    cfg = base_cfg(b2, **kw)
+    rng = np.random.default_rng(zlib.crc32(name.encode()))
+    nk = cfg["nfft"] - cfg["pos"] - cfg["neg"]
+    unit = cfg.get("fb", 0) or 1
+    sizes = [(cfg["nfft"] + 3 * nk + 17) * unit, (2 * nk - 5) * unit, (nk + 1234) * unit]
+    blocks = make_blocks(rng, cfg, sizes)
+    td = dict(td_kw)
+    if "turns" in td:
+        td["period"] = cfg["period"]
+    got = run_subints(ctx, b2, blocks, cfg, td, slots=slots)
+    want = oracle_subints(orc, b2, blocks, cfg, td)
+    rate = abs(cfg["bw"]) / (cfg["nchan"] * unit) * 1e6
+    check_subints(got, want, cfg, rate)
+    got2 = run_subints(ctx, b2, blocks, cfg, td, slots=slots, pop=True, host=True)
+    check_subints(got2, want, cfg, rate)
+
+
+def test_pipeline_subint_slots_exhausted(ctx, b2):
+    """A block that opens more divisions than there are free slots is refused
+    before any work is queued, and the pipeline goes on once slots free up."""
+    cfg = base_cfg(b2, dm=5.0, nbin=64, period=0.00123)
+    rng = np.random.default_rng(3)
+    blocks = make_blocks(rng, cfg, [5 * cfg["nfft"]])
+    c = b2.make_config(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nchan"], cfg["npol"], cfg["nfft"],
+                       cfg["pos"], cfg["neg"], cfg["nbin"], cfg["period"], lut=cfg["lut"],
+                       start_mjd=START, epoch_mjd=EPOCH, subint_seconds=0.0005, subint_slots=2)
+    pl = b2.Pipeline(ctx, c)
+    n = blocks[0].size // 4
+    with pytest.raises(b2.B200Error, match="slots are free"):
+        pl.run(torch.from_numpy(blocks[0]).cuda(), n)
+    pl.close()
+    with pytest.raises(b2.B200Error, match="one positive length"):
+        b2.Pipeline(ctx, b2.make_config(cfg["cf"], cfg["bw"], cfg["dm"], 1, 2, cfg["nfft"],
+                                        cfg["pos"], cfg["neg"], 64, 0.001, subint_seconds=1.0,
+                                        subint_turns=1.0))
