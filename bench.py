@@ -446,6 +446,85 @@ def run_b200(args, cfg, world, rank, local):
     e2e = samples_per_step * args.steps * world / (e2e_ms / 1e3) / 1e6
     d2h = p2.nbytes + h2.nbytes
 
+    # ---- optional: sub-integrations, and end to end from a DADA file ---------
+    extra = {}
+    if args.subint_seconds > 0:
+        cs = b2.make_config(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nchan"], cfg["npol"], nfft,
+                            pos, neg, cfg["nbin"], cfg["period"], state=cfg["state"], lut=lut,
+                            start_mjd=START_MJD, epoch_mjd=EPOCH_MJD, filterbank_nchan=cfg["fb"],
+                            scratch_bytes=args.scratch_mib << 20,
+                            subint_seconds=args.subint_seconds, subint_slots=64)
+        pl = b2.Pipeline(ctx, cs)
+        nsub = [0]
+        pl.set_unloader(lambda info, prof_, hits_: nsub.__setitem__(0, nsub[0] + 1))
+        for i in range(args.warmup):
+            pl.run(blocks[i % NBLOCKS], ndat)
+        torch.cuda.synchronize()
+        nsub[0] = 0
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record()
+        for i in range(args.steps):
+            pl.run(blocks[(args.warmup + i) % NBLOCKS], ndat)
+        s1.record()
+        torch.cuda.synchronize()
+        sms = max_over_ranks(s0.elapsed_time(s1), world)
+        pl.finish()
+        pl.close()
+        extra["subint"] = {"seconds": args.subint_seconds, "subints_unloaded": nsub[0],
+                           "value": round(samples_per_step * args.steps * world / (sms / 1e3) / 1e6, 3),
+                           "ms_per_step": round(sms / args.steps, 4),
+                           "note": "device-resident input; every closed sub-integration is "
+                                   "copied to the host and handed to the unloader callback"}
+    if args.dada:
+        import tempfile
+        with tempfile.TemporaryDirectory() as tmpd:
+            path = os.path.join(tmpd, "c.dada")
+            keys = {"HDR_VERSION": "1.0", "TELESCOPE": "synthetic", "SOURCE": "synthetic",
+                    "INSTRUMENT": "dspsr_b200", "FREQ": cfg["cf"], "BW": cfg["bw"],
+                    "NCHAN": cfg["nchan"], "NPOL": cfg["npol"], "NBIT": 8, "NDIM": 2,
+                    "TSAMP": cfg["nchan"] / abs(cfg["bw"]), "UTC_START": "2023-02-25-01:00:00",
+                    "OBS_OFFSET": 0}
+            with open(path, "wb") as fh:
+                text = b""
+                hdr = b2.ascii_header_set("", "HDR_SIZE", 4096)
+                for k, v in keys.items():
+                    hdr = b2.ascii_header_set(hdr, k, v)
+                text = hdr.encode()
+                fh.write(text + b"\0" * (4096 - len(text)))
+                for hb in host:
+                    fh.write(hb.numpy().tobytes())
+            f = b2.DADAFile(path)
+            pl = b2.Pipeline(ctx, f.pipeline_config(cfg["dm"], nfft, pos, neg, cfg["nbin"],
+                                                    cfg["period"], state=cfg["state"], lut=lut,
+                                                    epoch_mjd=EPOCH_MJD,
+                                                    filterbank_nchan=cfg["fb"],
+                                                    scratch_bytes=args.scratch_mib << 20))
+            # each call streams the whole file (NBLOCKS blocks), so every
+            # block's read overlaps the previous block's upload and kernels
+            nfile = f.ndat // ndat
+            pl.run_dada(f, ndat)
+            pl.get_profiles()
+            torch.cuda.synchronize()
+            barrier(world)
+            ncall = max(1, args.steps // nfile)
+            d0 = time.perf_counter()
+            for i in range(ncall):
+                pl.run_dada(f, ndat)
+                pd, hd = pl.get_profiles()
+            torch.cuda.synchronize()
+            dms = max_over_ranks(1e3 * (time.perf_counter() - d0), world) / (ncall * nfile) * args.steps
+            pl.close()
+            f.close()
+            extra["dada_e2e"] = {"value": round(samples_per_step * args.steps * world / (dms / 1e3) / 1e6, 3),
+                                 "unit": "complex Msamples/s", "ms_per_step": round(dms / args.steps, 4),
+                                 "file_bytes": int(os.path.getsize(path)) if os.path.exists(path) else None,
+                                 "block_ndat": ndat,
+                                 "note": "pipeline_run_dada over a DADA file of the same blocks "
+                                         "(one call per pass over the file, profiles read back "
+                                         "after each), read through two pinned buffers; the "
+                                         "file was just written, so reads come from the page "
+                                         "cache"}
+
     # ---- roofline of the dominant kernel -----------------------------------
     hbm_peak, bf16_peak, peak_src = measured_peaks()
     name, (kms, kn) = max(ktimes.items(), key=lambda kv: kv[1][0])
@@ -498,6 +577,7 @@ def run_b200(args, cfg, world, rank, local):
         "check": {"samples_folded": int(folded), "hits_total": int(hits.sum()),
                   "profile_peak_over_median": float(np.max(prof) / max(np.median(prof), 1e-30))},
     }
+    line.update(extra)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg)
     if rank == 0:
@@ -1310,6 +1390,13 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--subint-seconds", type=float, default=0.0,
+                    help="also time the device-resident run folding sub-integrations of this "
+                         "length (TimeDivide), unloaded through the callback (c1/c2)")
+    ap.add_argument("--dada", action="store_true",
+                    help="also time end to end from a DADA file holding the blocks "
+                         "(pipeline_run_dada; the file is written first, so it is read from "
+                         "the page cache) (c1/c2)")
     ap.add_argument("--scratch-mib", type=int, default=0,
                     help="device scratch of the four-step FFT batches (0: the library default)")
     ap.add_argument("--sk-inplace", action="store_true",

@@ -541,8 +541,17 @@ struct dspsr_b200_pipeline
   std::deque<int> sub_ready;
   dspsr_b200_unload_fn unload_fn = nullptr;
   void* unload_user = nullptr;
-  std::vector<float> h_subprof;
-  std::vector<uint32_t> h_subhits;
+  // unloads in flight: the slot's copy into page-locked memory was queued,
+  // the callback runs once its event has completed
+  struct PendingUnload
+  {
+    dspsr_b200_subint info;
+    float* prof;
+    uint32_t* hits;
+    cudaEvent_t ev;
+  };
+  std::deque<PendingUnload> sub_pending;
+  std::vector<PendingUnload> sub_spare;      // host buffers and events for reuse
   void* pinned[2] = {nullptr, nullptr};   // run_dada: file blocks in page-locked memory
   uint64_t pinned_bytes = 0;
   cudaEvent_t host_free[2] = {nullptr, nullptr};   // uploads of pinned[b] done
@@ -673,21 +682,59 @@ int subint_take (dspsr_b200_pipeline* pl, int k, dspsr_b200_subint* info, float*
   return DSPSR_B200_OK;
 }
 
-// PhaseSeriesUnloader::unload for every closed sub-integration, in order
-int subint_drain (dspsr_b200_pipeline* pl)
+// PhaseSeriesUnloader::unload for every closed sub-integration, in order.
+// Each closed slot is copied to page-locked memory and zeroed on the stream
+// (the slot is free again at once: later folds into it queue behind the
+// copy); the callback runs when the copy has landed -- now if wait, else at
+// the first call that finds it done.
+int subint_drain (dspsr_b200_pipeline* pl, bool wait)
 {
   if (!pl->unload_fn) return DSPSR_B200_OK;
+  dspsr_b200_context* ctx = pl->ctx;
   const size_t nprof = size_t (pl->fold.nchan) * pl->fold.npol * pl->fold.nbin;
-  pl->h_subprof.resize (nprof);
-  pl->h_subhits.resize (pl->fold.nbin);
   while (!pl->sub_ready.empty ())
   {
     const int k = pl->sub_ready.front ();
     pl->sub_ready.pop_front ();
-    dspsr_b200_subint info;
-    int rc = subint_take (pl, k, &info, pl->h_subprof.data (), pl->h_subhits.data ());
-    if (rc) return rc;
-    pl->unload_fn (pl->unload_user, &info, pl->h_subprof.data (), pl->h_subhits.data ());
+    dspsr_b200_pipeline::PendingUnload u {};
+    if (!pl->sub_spare.empty ())
+    {
+      u = pl->sub_spare.back ();
+      pl->sub_spare.pop_back ();
+    }
+    else
+    {
+      B200_CHECK (ctx, cudaMallocHost (&u.prof, nprof * sizeof (float)), "cudaMallocHost unload");
+      B200_CHECK (ctx, cudaMallocHost (&u.hits, pl->fold.nbin * sizeof (uint32_t)),
+                  "cudaMallocHost unload");
+      B200_CHECK (ctx, cudaEventCreateWithFlags (&u.ev, cudaEventDisableTiming), "create event");
+    }
+    u.info = pl->sub_slots[k].info;
+    int rc = pl->fold.download_slot (unsigned (k), u.prof, u.hits);
+    if (!rc) rc = pl->fold.reset_slot (unsigned (k));
+    if (rc)
+    {
+      pl->sub_spare.push_back (u);
+      return rc;
+    }
+    B200_CHECK (ctx, cudaEventRecord (u.ev, ctx->stream), "record unload");
+    pl->sub_slots[k].used = false;
+    pl->sub_pending.push_back (u);
+  }
+  while (!pl->sub_pending.empty ())
+  {
+    auto& u = pl->sub_pending.front ();
+    if (wait)
+      B200_CHECK (ctx, cudaEventSynchronize (u.ev), "wait unload");
+    else
+    {
+      const cudaError_t e = cudaEventQuery (u.ev);
+      if (e == cudaErrorNotReady) break;
+      B200_CHECK (ctx, e, "unload copy");
+    }
+    pl->unload_fn (pl->unload_user, &u.info, u.prof, u.hits);
+    pl->sub_spare.push_back (u);
+    pl->sub_pending.pop_front ();
   }
   return DSPSR_B200_OK;
 }
@@ -757,7 +804,7 @@ int pipeline_block (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat_new
     if (rc) return rc;
     if (pl->sub_on)
     {
-      rc = subint_drain (pl);
+      rc = subint_drain (pl, false);
       if (rc) return rc;
     }
   }
@@ -1861,6 +1908,13 @@ int dspsr_b200_pipeline_destroy (dspsr_b200_pipeline* pl)
     if (pl->pinned[i]) cudaFreeHost (pl->pinned[i]);
     if (pl->host_free[i]) cudaEventDestroy (pl->host_free[i]);
   }
+  for (auto& u : pl->sub_pending) pl->sub_spare.push_back (u);   // undelivered: dropped
+  for (auto& u : pl->sub_spare)
+  {
+    if (u.prof) cudaFreeHost (u.prof);
+    if (u.hits) cudaFreeHost (u.hits);
+    if (u.ev) cudaEventDestroy (u.ev);
+  }
   pl->fbbuf.release ();
   delete pl;
   return DSPSR_B200_OK;
@@ -2041,9 +2095,14 @@ int dspsr_b200_pipeline_set_unloader (dspsr_b200_pipeline* pl, dspsr_b200_unload
                                       void* user)
 {
   if (!pl) return DSPSR_B200_EINVAL;
+  if (pl->sub_on && pl->unload_fn)
+  {
+    const int rc = subint_drain (pl, true);   // the old unloader takes what it started
+    if (rc) return rc;
+  }
   pl->unload_fn = fn;
   pl->unload_user = user;
-  return pl->sub_on ? subint_drain (pl) : DSPSR_B200_OK;
+  return pl->sub_on ? subint_drain (pl, true) : DSPSR_B200_OK;
 }
 
 int dspsr_b200_pipeline_subints_ready (dspsr_b200_pipeline* pl, uint64_t* n)
@@ -2071,7 +2130,7 @@ int dspsr_b200_pipeline_finish (dspsr_b200_pipeline* pl)
   if (!pl) return DSPSR_B200_EINVAL;
   if (!pl->sub_on) return DSPSR_B200_OK;
   subint_close (pl);
-  return subint_drain (pl);
+  return subint_drain (pl, true);
 }
 
 int dspsr_b200_pipeline_reset (dspsr_b200_pipeline* pl)
@@ -2081,6 +2140,8 @@ int dspsr_b200_pipeline_reset (dspsr_b200_pipeline* pl)
   pl->in0 = 0;
   if (pl->sub_on)
   {
+    const int rc = subint_drain (pl, true);      // unloads already started complete
+    if (rc) return rc;
     pl->planner = pl->planner_init;
     for (auto& sl : pl->sub_slots) sl.used = false;
     pl->sub_cur = -1;

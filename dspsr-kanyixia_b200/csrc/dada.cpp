@@ -16,6 +16,8 @@
 #include <cstring>
 #include <ctime>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include <fcntl.h>
 #include <sys/stat.h>
@@ -514,19 +516,53 @@ int dspsr_b200_dada_read (dspsr_b200_dada_file* file, uint64_t start_sample, uin
   const uint64_t bytes = std::min<uint64_t> (nsamp * bits / 8, file->data_end - begin);
   // only whole samples are handed on
   const uint64_t want = bytes * 8 / bits * bits / 8;
-  uint64_t done = 0;
   char* out = static_cast<char*> (dst);
-  while (done < want)
-  {
-    const ssize_t r = pread (file->fd, out + done, size_t (want - done), off_t (begin + done));
-    if (r < 0)
+  // Large reads are split over threads: one thread copying out of the page
+  // cache moves ~6 GB/s, below the host link the blocks go to next.
+  constexpr uint64_t CHUNK_MIN = 16ull << 20;
+  const unsigned hw = std::max (1u, std::thread::hardware_concurrency ());
+  const unsigned nthr = unsigned (std::min<uint64_t> ({8, hw, std::max<uint64_t> (1, want / CHUNK_MIN)}));
+  const uint64_t per = (want / nthr + 4095) / 4096 * 4096;
+  std::vector<uint64_t> got (nthr, 0);
+  std::vector<int> err (nthr, 0);
+  auto work = [&] (unsigned i) {
+    const uint64_t lo = std::min<uint64_t> (want, i * per);
+    const uint64_t hi = i + 1 == nthr ? want : std::min<uint64_t> (want, lo + per);
+    uint64_t done = 0;
+    while (lo + done < hi)
     {
-      if (errno == EINTR) continue;
-      return host_fail (DSPSR_B200_EINVAL, "dada_read: pread: %s", strerror (errno));
+      const ssize_t r = pread (file->fd, out + lo + done, size_t (hi - lo - done),
+                               off_t (begin + lo + done));
+      if (r < 0)
+      {
+        if (errno == EINTR) continue;
+        err[i] = errno;
+        break;
+      }
+      if (r == 0)
+        break;
+      done += uint64_t (r);
     }
-    if (r == 0)
-      break;
-    done += uint64_t (r);
+    got[i] = done;
+  };
+  if (nthr == 1)
+    work (0);
+  else
+  {
+    std::vector<std::thread> pool;
+    for (unsigned i = 0; i < nthr; i++) pool.emplace_back (work, i);
+    for (auto& t : pool) t.join ();
+  }
+  // the samples read: the prefix up to the first short chunk
+  uint64_t done = 0;
+  for (unsigned i = 0; i < nthr; i++)
+  {
+    if (err[i])
+      return host_fail (DSPSR_B200_EINVAL, "dada_read: pread: %s", strerror (err[i]));
+    done += got[i];
+    const uint64_t lo = std::min<uint64_t> (want, i * per);
+    const uint64_t hi = i + 1 == nthr ? want : std::min<uint64_t> (want, lo + per);
+    if (got[i] < hi - lo) break;
   }
   if (nread) *nread = done * 8 / bits;
   return DSPSR_B200_OK;

@@ -497,8 +497,11 @@ typedef struct
 } dspsr_b200_subint;
 
 /* PhaseSeriesUnloader::unload: called in division order on the calling
-   thread, during _run, _run_host, _run_dada or _finish, with profiles
-   [chan][nout][nbin] and hits[nbin] in host memory valid for the call */
+   thread with profiles [chan][nout][nbin] and hits[nbin] in host memory valid
+   for the call.  A closed division's copy to the host is queued behind the
+   block's kernels and its callback runs in the first later _run, _run_host,
+   _run_dada, _set_unloader, _reset or _finish call that finds the copy done;
+   _finish delivers all that remain. */
 typedef void (*dspsr_b200_unload_fn) (void* user, const dspsr_b200_subint* subint,
                                       const float* profiles, const uint32_t* hits);
 int dspsr_b200_pipeline_set_unloader (dspsr_b200_pipeline* pipe, dspsr_b200_unload_fn fn,
