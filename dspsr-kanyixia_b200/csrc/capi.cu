@@ -516,6 +516,7 @@ struct dspsr_b200_pipeline
   bool consumed_pending[2] = {false, false};
   double rate = 0;                  // complex sampling rate of the convolved channels
   unsigned fb_nsub = 0;             // filterbank channels per input channel (0: none)
+  bool fb_fused = false;            // filterbank computed inside the column pass
   DevBuf<float2> fbbuf;             // filterbank output, FPT
   float2* fb_tab = nullptr;         // pass tables of the filterbank FFT (fb_nsub >= 128)
   size_t fb_tab_cap = 0;
@@ -747,8 +748,11 @@ int pipeline_block (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat_new
   const auto& cfg = pl->cfg;
   const uint64_t nfilt = uint64_t (sh.nfilt_pos) + sh.nfilt_neg;
   const uint64_t ndat = pl->ncarry + ndat_new;
-  // after a filterbank stage the convolution reads complex-float channels
-  const bool fpt = pl->fb_nsub > 1 || cfg.input_kind == DSPSR_B200_FLOAT_FPT;
+  // after a filterbank stage the convolution reads complex-float channels,
+  // unless the filterbank runs inside the column pass: then the block and the
+  // carry stay raw TFPD, counted in filterbank samples of fb_nsub raw samples
+  const bool fbraw = pl->fb_fused;
+  const bool fpt = !fbraw && (pl->fb_nsub > 1 || cfg.input_kind == DSPSR_B200_FLOAT_FPT);
   if (ndat_folded) *ndat_folded = 0;
 
   InputView in;
@@ -758,9 +762,10 @@ int pipeline_block (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat_new
   in.npre = pl->ncarry;
   in.pre_span = pl->carry_span;
   in.main_span = fpt ? in_span : 0;
-  in.nchan = sh.nchan;
+  in.nchan = fbraw ? cfg.nchan : sh.nchan;
   in.npol = cfg.npol;
   in.offset_binary = cfg.offset_binary;
+  in.fb_nsub = fbraw ? pl->fb_nsub : 0;
 
   uint64_t npart = 0;
   if (ndat >= sh.nfft) npart = (ndat - nfilt) / sh.nkeep;   // Convolution.C:486-487
@@ -814,7 +819,7 @@ int pipeline_block (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat_new
   const int next = pl->cur_carry ^ 1;
   if (!fpt)
   {
-    const uint64_t bps = pl->bytes_per_sample;
+    const uint64_t bps = pl->bytes_per_sample * (fbraw ? pl->fb_nsub : 1);
     B200_CHECK (ctx, pl->carry[next].reserve (std::max<uint64_t> (keep * bps, 16)),
                 "cudaMalloc carry");
     uint64_t done = 0;
@@ -883,6 +888,8 @@ int pipeline_input (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat, ui
   if (ndat % pl->fb_nsub)
     return fail (ctx, DSPSR_B200_EINVAL, "pipeline: block of %llu samples is not a multiple of "
                  "the %u filterbank channels", (unsigned long long) ndat, pl->fb_nsub);
+  if (pl->fb_fused)
+    return pipeline_block (pl, d_in, ndat / pl->fb_nsub, 0, ndat_folded);
   const uint64_t nb = ndat / pl->fb_nsub;
   const uint64_t rows = uint64_t (pl->conv.shape.nchan) * cfg.npol;
   B200_CHECK (ctx, pl->fbbuf.reserve (std::max<uint64_t> (rows * nb, 1)), "cudaMalloc filterbank");
@@ -1867,12 +1874,19 @@ int dspsr_b200_pipeline_create (dspsr_b200_context* ctx, const dspsr_b200_pipeli
   }
   if (!rc) rc = pl->fold.init (ctx, cfg->nbin, nchan, pl->nout,
                                pl->sub_on ? unsigned (pl->sub_slots.size ()) : 1);
+  // C2's shape -- a 64-channel filterbank of one dual-polarisation int8 or
+  // int16 channel with four-step parts of 8 x n2 -- runs the filterbank
+  // inside the forward column pass: its output never goes through memory
+  pl->fb_fused = !rc && fb == 64 && cfg->nchan == 1 && cfg->npol == 2
+                 && cfg->input_kind != DSPSR_B200_FLOAT_FPT && pl->conv.shape.n1 == 8
+                 && cfg->fused_filterbank >= 0;
   // the carry never exceeds nfft samples: size both carry buffers once
   for (int i = 0; i < 2 && !rc; i++)
   {
-    const bool fpt = fb || cfg->input_kind == DSPSR_B200_FLOAT_FPT;
+    const bool fpt = !pl->fb_fused && (fb || cfg->input_kind == DSPSR_B200_FLOAT_FPT);
     const uint64_t bytes = fpt ? uint64_t (nchan) * cfg->npol * cfg->nfft * sizeof (float2)
-                               : uint64_t (cfg->nfft) * pl->bytes_per_sample;
+                               : uint64_t (cfg->nfft) * pl->bytes_per_sample
+                                     * (pl->fb_fused ? fb : 1);
     cudaError_t e = pl->carry[i].reserve (bytes);
     if (e != cudaSuccess) rc = cuda_fail (ctx, e, "cudaMalloc carry");
   }

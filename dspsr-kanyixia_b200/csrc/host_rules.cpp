@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <complex>
 #include <cstdint>
 #include <vector>

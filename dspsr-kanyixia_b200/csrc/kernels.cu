@@ -334,6 +334,175 @@ k_fwd_cols (const InputView in, const float* __restrict__ lut, const uint64_t nk
 }
 
 // --------------------------------------------------------------------------
+// K1 with the filterbank in front (Filterbank with freq_res 1 and 64 channels,
+// FilterbankEngineCPU.C:379-535, then the first four-step pass of each
+// channel's convolution), for raw TFPD input of one channel and two
+// polarisations and n1 = 8.  The filterbank's own output never reaches
+// memory: a warp takes one column i2 of one part and computes, for the eight
+// filterbank samples t0 + j*n2 of that column, all 64 channels of both
+// polarisations, then each channel's 8-point column DFT.
+//
+// Lane (j, q), j = lane/4, q = lane%4, reads raw samples s = q + 4m (m < 16)
+// of filterbank sample j: a 16-point DFT over m, the twiddle w64^(q k),
+// then, after an exchange inside the quad, 4-point DFTs over q give channel
+// c = 4q + e + 16 kb for e, kb < 4.  A second exchange inside each group of
+// lanes with equal q gathers the eight j of four (channel, pol) pairs per
+// lane for the 8-point DFTs.  The block's warps (consecutive columns) stage
+// their outputs in shared memory and write each scratch row in runs of one
+// value per column.  Both exchanges swizzle their shared-memory columns so
+// that every access is free of bank conflicts.
+// --------------------------------------------------------------------------
+
+constexpr int FBC_THREADS = 128;
+constexpr int FBC_COLS = FBC_THREADS / 32;      // columns per block, one per warp
+constexpr int FBC_XSTRIDE = 1056;               // float2 per warp exchange buffer
+constexpr int FBC_SROW = FBC_COLS + 1;          // staging row stride (float2)
+constexpr size_t FBC_SMEM =
+    (size_t (FBC_SROW) * 1024 > size_t (FBC_COLS) * FBC_XSTRIDE ? size_t (FBC_SROW) * 1024
+                                                                : size_t (FBC_COLS) * FBC_XSTRIDE)
+    * sizeof (float2);
+
+template <int KIND>
+__device__ __forceinline__ void fetch_raw2 (const InputView& in, const float* s_lut, uint64_t r,
+                                            float2& p0, float2& p1)
+{
+  const void* base = in.main;
+  const uint64_t npre = in.npre * 64;
+  if (r < npre)
+    base = in.pre;
+  else
+    r -= npre;
+  if constexpr (KIND == IN_INT8)
+  {
+    const unsigned w = __ldg (static_cast<const unsigned*> (base) + r);
+    p0 = make_float2 (s_lut[w & 0xff], s_lut[(w >> 8) & 0xff]);
+    p1 = make_float2 (s_lut[(w >> 16) & 0xff], s_lut[w >> 24]);
+  }
+  else
+  {
+    const uint2 w = __ldg (static_cast<const uint2*> (base) + r);
+    short a = short (w.x & 0xffff), b = short (w.x >> 16);
+    short c = short (w.y & 0xffff), d = short (w.y >> 16);
+    if (in.offset_binary)
+    {
+      a = short (a ^ 0x8000);
+      b = short (b ^ 0x8000);
+      c = short (c ^ 0x8000);
+      d = short (d ^ 0x8000);
+    }
+    p0 = make_float2 (__fadd_rn (float (a), 0.5f), __fadd_rn (float (b), 0.5f));
+    p1 = make_float2 (__fadd_rn (float (c), 0.5f), __fadd_rn (float (d), 0.5f));
+  }
+}
+
+template <int KIND>
+__global__ void __launch_bounds__ (FBC_THREADS, 512 / FBC_THREADS)
+k_fwd_cols_fb64 (const InputView in, const float* __restrict__ lut, const uint64_t nkeep,
+                 const uint64_t part0, const unsigned n2, const float2* __restrict__ tw4,
+                 float2* __restrict__ scratch)
+{
+  extern __shared__ float2 s_fbc[];
+  __shared__ float s_lut[256];
+  __shared__ float2 s_tw64[64];
+  load_lut (in, lut, s_lut);
+  if (threadIdx.x < 64)
+    s_tw64[threadIdx.x] = make_float2 (cos64 (int (threadIdx.x)), -sin64 (int (threadIdx.x)));
+  __syncthreads ();
+  const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned j = lane >> 2, q = lane & 3;
+  const unsigned i0 = blockIdx.x * FBC_COLS;
+  const unsigned i2 = i0 + warp;
+  const unsigned b = blockIdx.y;
+  const uint64_t N = 8ull * n2;
+  float2* xb = s_fbc + warp * FBC_XSTRIDE;
+
+  // raw samples q + 4m of filterbank sample t, both polarisations
+  const uint64_t t = (part0 + b) * nkeep + i2 + uint64_t (j) * n2;
+  float2 x0[16], x1[16];
+#pragma unroll
+  for (int m = 0; m < 16; m++)
+    fetch_raw2<KIND> (in, s_lut, t * 64 + q + 4 * m, x0[m], x1[m]);
+  RegDFT<16, -1>::run (x0);
+  RegDFT<16, -1>::run (x1);
+  // twiddle w64^(q ka), then the quad exchange: column q ^ (ka >> 2)
+#pragma unroll
+  for (int ka = 0; ka < 16; ka++)
+  {
+    const float2 w = s_tw64[(q * ka) & 63];
+    const unsigned col = q ^ unsigned (ka >> 2);
+    xb[j * 132 + (0 * 16 + ka) * 4 + col] = cmul (x0[ka], w);
+    xb[j * 132 + (1 * 16 + ka) * 4 + col] = cmul (x1[ka], w);
+  }
+  __syncwarp ();
+  // 4-point DFTs over the quad: channel 4q + e + 16 kb
+  float2 y[2][4][4];
+#pragma unroll
+  for (int pol = 0; pol < 2; pol++)
+#pragma unroll
+    for (int e = 0; e < 4; e++)
+    {
+#pragma unroll
+      for (int qq = 0; qq < 4; qq++)
+        y[pol][e][qq] = xb[j * 132 + (pol * 16 + 4 * q + e) * 4 + (unsigned (qq) ^ q)];
+      RegDFT<4, -1>::run (y[pol][e]);
+    }
+  __syncwarp ();
+  // gather the eight j of (channel, pol) pairs v = 4j + f of this quad group:
+  // pair v = pol*16 + e*4 + kb is stored at column j ^ (v >> 2)
+#pragma unroll
+  for (int pol = 0; pol < 2; pol++)
+#pragma unroll
+    for (int e = 0; e < 4; e++)
+#pragma unroll
+      for (int kb = 0; kb < 4; kb++)
+      {
+        const unsigned v = pol * 16 + e * 4 + kb;
+        xb[q * 260 + v * 8 + (j ^ (v >> 2))] = y[pol][e][kb];
+      }
+  __syncwarp ();
+  float2 z[4][8];
+#pragma unroll
+  for (int f = 0; f < 4; f++)
+  {
+#pragma unroll
+    for (int jj = 0; jj < 8; jj++)
+      z[f][jj] = xb[q * 260 + (4 * j + f) * 8 + (unsigned (jj) ^ j)];
+    RegDFT<8, -1>::run (z[f]);
+  }
+  // four-step twiddle w_N^(k1 n2) of column i2, and the filterbank
+  // normaliser 1/sqrt(64) (exact)
+  float2 tw[8];
+  tw[0] = make_float2 (1.f, 0.f);
+#pragma unroll
+  for (int k1 = 1; k1 < 8; k1++) tw[k1] = __ldg (tw4 + uint64_t (k1) * n2 + i2);
+  __syncthreads ();                    // every warp is done with its exchange buffer
+  // pair f of lane (j, q): channel c = 4q + (j & 3) + 16 f, pol = j >> 2;
+  // staging row k1*128 + c*2 + pol, column = warp
+#pragma unroll
+  for (int f = 0; f < 4; f++)
+  {
+    const unsigned c = 4 * q + (j & 3) + 16 * f, pol = j >> 2;
+#pragma unroll
+    for (int k1 = 0; k1 < 8; k1++)
+    {
+      float2 o = k1 ? cmul (z[f][k1], tw[k1]) : z[f][k1];
+      o = make_float2 (__fmul_rn (o.x, 0.125f), __fmul_rn (o.y, 0.125f));
+      s_fbc[(k1 * 128 + c * 2 + pol) * FBC_SROW + warp] = o;
+    }
+  }
+  __syncthreads ();
+  // scratch row ((b*64 + c)*2 + pol)*N + k1*n2, columns i0 .. i0+FBC_COLS-1
+#pragma unroll 4
+  for (unsigned idx = threadIdx.x; idx < 1024 * FBC_COLS; idx += FBC_THREADS)
+  {
+    const unsigned row = idx / FBC_COLS, w = idx % FBC_COLS;
+    const unsigned k1 = row >> 7, c = (row & 127) >> 1, pol = row & 1;
+    scratch[((uint64_t (b) * 64 + c) * 2 + pol) * N + uint64_t (k1) * n2 + i0 + w] =
+        s_fbc[row * FBC_SROW + w];
+  }
+}
+
+// --------------------------------------------------------------------------
 // K2 (persistent): one CTA per SM walks the rows.  The next row is fetched
 // into a staging buffer by the bulk-copy engine (cp.async.bulk, completion on
 // an mbarrier) while the current row is transformed; the per-pass twiddle
@@ -1383,6 +1552,22 @@ cudaError_t run_fourstep_n1 (const ConvShape& sh, const ConvTables& tb, const In
                              const KernelClock* clk)
 {
   const dim3 gcol (sh.n2 / 128, nbatch, sh.nchan);
+  if (in.fb_nsub)
+  {
+    // the 64-channel filterbank inside the column pass
+    if (N1 != 8 || in.fb_nsub != 64 || sh.nchan != 64 || in.nchan != 1 || in.npol != 2
+        || sh.npol != 2 || tb.apod || (in.kind != IN_INT8 && in.kind != IN_INT16))
+      return cudaErrorInvalidValue;
+    ClockScope cs (clk, KK_FWD_COLS, st);
+    const dim3 g (sh.n2 / FBC_COLS, nbatch);
+    if (in.kind == IN_INT8)
+      k_fwd_cols_fb64<IN_INT8><<<g, FBC_THREADS, FBC_SMEM, st>>> (in, tb.lut, sh.nkeep, part0,
+                                                                   sh.n2, tb.tw4, scratch);
+    else
+      k_fwd_cols_fb64<IN_INT16><<<g, FBC_THREADS, FBC_SMEM, st>>> (in, tb.lut, sh.nkeep, part0,
+                                                                    sh.n2, tb.tw4, scratch);
+  }
+  else
   {
   ClockScope cs (clk, KK_FWD_COLS, st);
   if (in.kind == IN_INT8)
@@ -1583,6 +1768,12 @@ cudaError_t launch_convolution (const ConvShape& sh, const ConvTables& tb, const
   {
     cudaError_t e = set_rows_smem<8192> ();
     if (e == cudaSuccess) e = set_rows_smem<4096> ();
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute (k_fwd_cols_fb64<IN_INT8>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, int (FBC_SMEM));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute (k_fwd_cols_fb64<IN_INT16>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, int (FBC_SMEM));
     if (e != cudaSuccess) return e;
     attr_done |= 1u << dev;
   }

@@ -23,6 +23,12 @@ struct InputView
   uint64_t main_span;    // FPT span of the main block
   unsigned nchan, npol;
   int offset_binary;     // int16 encoding
+  // 64: the input is raw TFPD (one input channel, two polarisations) and the
+  // convolution's 64 channels come from a 64-point filterbank computed inside
+  // the forward column pass; times (and npre) then count filterbank samples
+  // of 64 raw samples, npre_raw = 64 * npre.  0: the input holds the
+  // convolution's channels.
+  unsigned fb_nsub = 0;
 };
 
 // Fold / detection epilogue

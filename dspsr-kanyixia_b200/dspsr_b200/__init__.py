@@ -691,7 +691,7 @@ def make_config(centre_freq, bandwidth, dm, nchan, npol, nfft, nfilt_pos, nfilt_
                 start_mjd=(60000, 0, 0.0), epoch_mjd=(60000, 0, 0.0), reference_phase=0.0,
                 dual_sideband=1, offset_binary=0, scratch_bytes=0, filterbank_nchan=0,
                 subint_seconds=0.0, subint_turns=0.0, subint_slots=0,
-                subint_epoch=(0, 0, 0.0)):
+                subint_epoch=(0, 0, 0.0), fused_filterbank=0):
     """Fill a PipelineConfig (the fields DedispersionPipe / LoadToFold set up).
     With filterbank_nchan > 1, nchan counts input channels, and nfft and the
     smearing (nfilt_pos, nfilt_neg) refer to the filterbank's output channels."""
@@ -725,6 +725,7 @@ def make_config(centre_freq, bandwidth, dm, nchan, npol, nfft, nfilt_pos, nfilt_
     cfg.subint_turns = subint_turns
     cfg.subint_slots = subint_slots
     cfg.subint_epoch_day, cfg.subint_epoch_sec, cfg.subint_epoch_frac = subint_epoch
+    cfg.fused_filterbank = fused_filterbank
     return cfg
 
 

@@ -64,6 +64,7 @@ class PipelineConfig(ctypes.Structure):
         ("subint_epoch_sec", c_i64),
         ("subint_epoch_frac", c_dbl),
         ("subint_slots", c_uint),
+        ("fused_filterbank", c_int),
     ]
 
 

@@ -410,6 +410,11 @@ typedef struct
   double subint_epoch_frac;                     /* all zero = none */
   unsigned subint_slots;    /* divisions held on the device at once (0 = 4); one
                                block may touch at most this many */
+  /* tuning: 0 = compute a 64-channel filterbank of one dual-polarisation
+     int8/int16 channel inside the convolution's first FFT pass where the
+     FFT split allows it (its output then never goes through memory);
+     -1 = always run the filterbank as a stage of its own */
+  int fused_filterbank;
 } dspsr_b200_pipeline_config;
 
 int dspsr_b200_pipeline_create (dspsr_b200_context* ctx,

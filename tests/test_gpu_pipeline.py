@@ -252,6 +252,12 @@ CASES = {
     "c2_filterbank_8k": dict(dm=50.0, bw=256.0, fb=64, state=3, nbin=2048, period=5.757e-3),
     "c2_filterbank_64k": dict(dm=500.0, bw=256.0, fb=64, nfft=1 << 16, state=3, nbin=2048,
                               period=5.757e-3),
+    # a table that is not (x + 0.5) * scale: looked up, not computed
+    "c2_fb64k_table": dict(dm=500.0, bw=256.0, fb=64, nfft=1 << 16, state=3, nbin=2048,
+                           period=5.757e-3, lut=(np.asarray(__import__("dspsr_b200").bittable8()[0])
+                                                 * (1 + 1e-3 * np.cos(np.arange(256)))).astype(np.float32)),
+    "fused8k_table": dict(dm=5.0, lut=(np.asarray(__import__("dspsr_b200").bittable8()[0])
+                                       * (1 + 1e-3 * np.sin(np.arange(256)))).astype(np.float32)),
 }
 
 
@@ -522,3 +528,41 @@ def test_pipeline_subint_slots_exhausted(ctx, b2):
         b2.Pipeline(ctx, b2.make_config(cfg["cf"], cfg["bw"], cfg["dm"], 1, 2, cfg["nfft"],
                                         cfg["pos"], cfg["neg"], 64, 0.001, subint_seconds=1.0,
                                         subint_turns=1.0))
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_pipeline_fused_filterbank_matches_stage(ctx, b2, orc, kind):
+    """The 64-channel filterbank computed inside the column pass (C2's shape)
+    against the filterbank as a stage of its own and against the oracle
+    chain, over blocks whose carry crosses parts, from device and host
+    memory."""
+    cfg = base_cfg(b2, dm=500.0, bw=256.0, fb=64, nfft=1 << 16, state=3, nbin=512,
+                   period=5.757e-3, kind=kind)
+    rng = np.random.default_rng(77 + kind)
+    nk = cfg["nfft"] - cfg["pos"] - cfg["neg"]
+    blocks = make_blocks(rng, cfg, [(cfg["nfft"] + 2 * nk + 321) * 64, (nk - 17) * 64,
+                                    (3 * nk + 5) * 64])
+
+    def run(fused, host=False):
+        c = b2.make_config(cfg["cf"], cfg["bw"], cfg["dm"], 1, 2, cfg["nfft"], cfg["pos"],
+                           cfg["neg"], cfg["nbin"], cfg["period"], state=cfg["state"],
+                           input_kind=kind, lut=cfg["lut"], start_mjd=START, epoch_mjd=EPOCH,
+                           filterbank_nchan=64, fused_filterbank=0 if fused else -1)
+        pl = b2.Pipeline(ctx, c)
+        tot = 0
+        for r in blocks:
+            n = r.size // 4
+            tot += pl.run_host(r, n) if host else pl.run(torch.from_numpy(r).cuda(), n)
+        prof, hits = pl.get_profiles()
+        pl.close()
+        return prof, hits, tot
+
+    fused = run(True)
+    stage = run(False)
+    check(fused[0], fused[1], fused[2], stage[0].astype(np.float64), stage[1], stage[2],
+          cfg["state"], rtol=2e-6)
+    rprof, rhits, rtotal = oracle_chain(orc, b2, blocks, cfg)
+    check(fused[0], fused[1], fused[2], rprof, rhits, rtotal, cfg["state"])
+    hostrun = run(True, host=True)
+    check(hostrun[0], hostrun[1], hostrun[2], fused[0].astype(np.float64), fused[1], fused[2],
+          cfg["state"], rtol=2e-6)
