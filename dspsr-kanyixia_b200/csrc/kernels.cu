@@ -347,10 +347,11 @@ k_fwd_cols (const InputView in, const float* __restrict__ lut, const uint64_t nk
 // then, after an exchange inside the quad, 4-point DFTs over q give channel
 // c = 4q + e + 16 kb for e, kb < 4.  A second exchange inside each group of
 // lanes with equal q gathers the eight j of four (channel, pol) pairs per
-// lane for the 8-point DFTs.  The block's warps (consecutive columns) stage
-// their outputs in shared memory and write each scratch row in runs of one
-// value per column.  Both exchanges swizzle their shared-memory columns so
-// that every access is free of bank conflicts.
+// lane for the 8-point DFTs.  The block's four warps (four consecutive
+// columns) stage their outputs in shared memory and write each scratch row
+// in runs of one 32-byte sector (blocks of two or eight warps measured
+// slower).  Both exchanges swizzle their shared-memory columns against bank
+// conflicts.
 // --------------------------------------------------------------------------
 
 constexpr int FBC_THREADS = 128;
