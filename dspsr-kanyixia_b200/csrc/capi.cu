@@ -270,26 +270,29 @@ namespace {
 // Dedispersion::build_compute (Dedispersion.C:168-173) is formed on the host
 // in double; the GPU evaluates the phase of every bin in FP64.
 int build_response (dspsr_b200_convolution* c, const double* freq, double bw, double dm,
-                    int swap_halves, int chirp_mode, unsigned norm_nfft)
+                    int swap_halves, int chirp_mode, unsigned norm_nfft,
+                    const double* frac_us = nullptr)
 {
   dspsr_b200_context* ctx = c->ctx;
   const ConvShape& sh = c->shape;
   const unsigned nchan = sh.nchan;
-  std::vector<double> par (2 * nchan);
+  std::vector<double> par (3 * nchan, 0.0);
   const double sign = bw / std::fabs (bw);
   const double dispersion_per_MHz = 1e6 * dm / 2.41e-4;
   for (unsigned ic = 0; ic < nchan; ic++)
   {
     par[ic] = freq[ic];
     par[nchan + ic] = -sign * 2 * M_PI * dispersion_per_MHz / (freq[ic] * freq[ic]);
+    if (frac_us) par[2 * nchan + ic] = frac_us[ic];
   }
   const double chanwidth = bw / double (nchan);
   const double binwidth = chanwidth / double (sh.nfft);
   const float scale = float (1.0 / std::sqrt (double (norm_nfft ? norm_nfft : sh.nfft)));
-  B200_CHECK (ctx, c->chan_par.reserve (2 * nchan), "cudaMalloc channel table");
+  B200_CHECK (ctx, c->chan_par.reserve (3 * nchan), "cudaMalloc channel table");
   B200_CHECK (ctx, cudaMemcpyAsync (c->chan_par.ptr, par.data (), par.size () * sizeof (double),
                                     cudaMemcpyHostToDevice, ctx->stream), "upload channels");
-  B200_CHECK (ctx, launch_build_chirp (c->H.ptr, c->chan_par.ptr, c->chan_par.ptr + nchan, nchan,
+  B200_CHECK (ctx, launch_build_chirp (c->H.ptr, c->chan_par.ptr, c->chan_par.ptr + nchan,
+                                       frac_us ? c->chan_par.ptr + 2 * nchan : nullptr, nchan,
                                        sh.nfft, sh.n1, sh.n2, binwidth, 0.5 * chanwidth,
                                        swap_halves, chirp_mode, scale, ctx->stream),
               "build chirp");
@@ -517,6 +520,16 @@ struct dspsr_b200_pipeline
   double rate = 0;                  // complex sampling rate of the convolved channels
   unsigned fb_nsub = 0;             // filterbank channels per input channel (0: none)
   bool fb_fused = false;            // filterbank computed inside the column pass
+  // inter-channel dedispersion: SampleDelay between the convolution and the
+  // fold, its voltages in sd_buf[sd_cur] (rows [chan][pol], sd_span values)
+  bool sd_on = false;
+  InterchannelDelays sd;
+  DevBuf<int> sd_applied;
+  DevBuf<float2> sd_buf[2];
+  uint64_t sd_span = 0;
+  int sd_cur = 0;
+  uint64_t sd_ncarry = 0;           // voltages carried per row
+  uint64_t sd_out0 = 0;             // SampleDelay output samples before this block
   DevBuf<float2> fbbuf;             // filterbank output, FPT
   float2* fb_tab = nullptr;         // pass tables of the filterbank FFT (fb_nsub >= 128)
   size_t fb_tab_cap = 0;
@@ -577,18 +590,20 @@ void subint_close (dspsr_b200_pipeline* pl)
   pl->sub_cur = -1;
 }
 
-int pipeline_subint_plan (dspsr_b200_pipeline* pl, uint64_t nout, double pps)
+// out_base: global index of the fold input's first sample; time_base: the
+// input sample whose time that is (the convolution shifts its output by
+// nfilt_pos samples, Convolution.C:611, and SampleDelay by zero_delay more,
+// SampleDelay.C:221)
+int pipeline_subint_plan (dspsr_b200_pipeline* pl, uint64_t out_base, uint64_t time_base,
+                          uint64_t nout, double pps)
 {
   dspsr_b200_context* ctx = pl->ctx;
   const auto& cfg = pl->cfg;
-  const ConvShape& sh = pl->conv.shape;
-  // the detected block's start: Convolution shifts its output by nfilt_pos
-  // samples (Convolution.C:611, Observation::change_start_time)
   b200::Mjd start0;
   start0.day = cfg.start_day;
   start0.sec = cfg.start_sec;
   start0.frac = cfg.start_frac;
-  const b200::Mjd start = b200::mjd_add (start0, double (pl->in0 + sh.nfilt_pos) / pl->rate);
+  const b200::Mjd start = b200::mjd_add (start0, double (time_base) / pl->rate);
   b200::SubintPlanner trial = pl->planner;
   const char* err = nullptr;
   if (!trial.block (start, nout, pl->rate, &pl->sub_actions, &err))
@@ -635,7 +650,7 @@ int pipeline_subint_plan (dspsr_b200_pipeline* pl, uint64_t nout, double pps)
       sl.used = true;
       sl.info = dspsr_b200_subint {};
       sl.info.division = a.division;
-      sl.info.first_sample = pl->in0 + a.idat_start;
+      sl.info.first_sample = out_base + a.idat_start;
       sl.info.lower_day = a.lower.day;
       sl.info.lower_sec = a.lower.sec;
       sl.info.lower_frac = a.lower.frac;
@@ -650,9 +665,8 @@ int pipeline_subint_plan (dspsr_b200_pipeline* pl, uint64_t nout, double pps)
     sl.info.complete = a.end_reached ? 1 : 0;
     if (a.idat_start > cursor) skip (cursor);
     const double phi = fold_phi (cfg.start_day, cfg.start_sec, cfg.start_frac, cfg.epoch_day,
-                                 cfg.epoch_sec, cfg.epoch_frac,
-                                 pl->in0 + sh.nfilt_pos + a.idat_start, pl->rate, cfg.period_s,
-                                 cfg.reference_phase);
+                                 cfg.epoch_sec, cfg.epoch_frac, time_base + a.idat_start,
+                                 pl->rate, cfg.period_s, cfg.reference_phase);
     build_fold_plan (phi, pps, a.ndat, &part);
     const uint32_t base = uint32_t (pl->sub_cur) * pl->fold.nbin;
     for (FoldSegment g : part)
@@ -740,6 +754,102 @@ int subint_drain (dspsr_b200_pipeline* pl, bool wait)
   return DSPSR_B200_OK;
 }
 
+// The fold plan of nout fold-input samples starting at global index out_base,
+// whose first sample has the time of input sample time_base: one range with
+// the block's phase (continued across the pieces of one host block), or the
+// sub-integration ranges.
+int pipeline_fold_plan (dspsr_b200_pipeline* pl, uint64_t out_base, uint64_t time_base,
+                        uint64_t nout)
+{
+  const auto& cfg = pl->cfg;
+  const double sampling_interval = 1.0 / pl->rate;
+  const double pps = sampling_interval / cfg.period_s;   // Fold.C:754-756
+  if (pl->sub_on) return pipeline_subint_plan (pl, out_base, time_base, nout, pps);
+  const double phi = pl->phase_continue
+                   ? pl->phase_next
+                   : fold_phi (cfg.start_day, cfg.start_sec, cfg.start_frac, cfg.epoch_day,
+                               cfg.epoch_sec, cfg.epoch_frac, time_base, pl->rate, cfg.period_s,
+                               cfg.reference_phase);
+  const int rc = pl->fold.set_bins (phi, pps, nout, &pl->phase_next);
+  if (rc) return rc;
+  pl->phase_continue = pl->in_pieces;
+  return DSPSR_B200_OK;
+}
+
+// SampleDelay with its InputBuffering (SampleDelay.C:166-298) between the
+// convolution and the fold: the block's voltages land after the carried ones,
+// output sample t of channel c is voltage t + applied[c], and the last
+// total_delay voltages of every (chan, pol) carry over.  *folded = outputs.
+int pipeline_sd_block (dspsr_b200_pipeline* pl, const InputView& in, uint64_t npart,
+                       uint64_t nout, const KernelClock* clk, uint64_t* folded)
+{
+  dspsr_b200_context* ctx = pl->ctx;
+  const ConvShape& sh = pl->conv.shape;
+  const auto& cfg = pl->cfg;
+  const uint64_t rows = uint64_t (sh.nchan) * cfg.npol;
+  const uint64_t len = pl->sd_ncarry + nout;
+  if (len > pl->sd_span)
+  {
+    const uint64_t span = len + len / 4;
+    DevBuf<float2> nb[2];
+    for (int i = 0; i < 2; i++)
+      B200_CHECK (ctx, nb[i].reserve (rows * span), "cudaMalloc sample delay");
+    if (pl->sd_ncarry)
+      B200_CHECK (ctx, cudaMemcpy2DAsync (nb[0].ptr, span * sizeof (float2),
+                                          pl->sd_buf[pl->sd_cur].ptr, pl->sd_span * sizeof (float2),
+                                          pl->sd_ncarry * sizeof (float2), rows,
+                                          cudaMemcpyDeviceToDevice, ctx->stream),
+                  "sample delay carry");
+    B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "sample delay resize");
+    for (int i = 0; i < 2; i++)
+    {
+      pl->sd_buf[i].release ();
+      std::swap (pl->sd_buf[i], nb[i]);
+    }
+    pl->sd_span = span;
+    pl->sd_cur = 0;
+  }
+  float2* cur = pl->sd_buf[pl->sd_cur].ptr;
+  FoldView fv0 {};
+  VoltView vv {cur + pl->sd_ncarry, pl->sd_span};
+  const ConvTables tb = pl->conv.tables ();
+  for (uint64_t p0 = 0; p0 < npart; p0 += pl->conv.max_batch)
+  {
+    const unsigned nb = unsigned (std::min<uint64_t> (pl->conv.max_batch, npart - p0));
+    B200_CHECK (ctx, launch_convolution (sh, tb, in, p0, nb, pl->conv.scratch.ptr, OUT_VOLTAGE,
+                                         fv0, vv, ctx->stream, clk), "convolution kernels");
+  }
+  const uint64_t total = pl->sd.total_delay;
+  const uint64_t out_n = len > total ? len - total : 0;
+  if (out_n)
+  {
+    const uint64_t time_base = pl->sd_out0 + sh.nfilt_pos + uint64_t (pl->sd.zero_delay);
+    int rc = pipeline_fold_plan (pl, pl->sd_out0, time_base, out_n);
+    if (rc) return rc;
+    const FoldView fv = pl->fold.view (cfg.state, pl->nout, cfg.nchan);
+    B200_CHECK (ctx, launch_delay_fold (cur, pl->sd_span, pl->sd_applied.ptr, out_n, sh.nchan,
+                                        cfg.npol, fv, ctx->stream, clk), "sample delay fold");
+    rc = pl->fold.release_plan ();
+    if (rc) return rc;
+    if (pl->sub_on)
+    {
+      rc = subint_drain (pl, false);
+      if (rc) return rc;
+    }
+  }
+  const uint64_t keep = len - out_n;
+  if (keep)
+    B200_CHECK (ctx, cudaMemcpy2DAsync (pl->sd_buf[pl->sd_cur ^ 1].ptr, pl->sd_span * sizeof (float2),
+                                        cur + out_n, pl->sd_span * sizeof (float2),
+                                        keep * sizeof (float2), rows, cudaMemcpyDeviceToDevice,
+                                        ctx->stream), "sample delay carry");
+  pl->sd_cur ^= 1;
+  pl->sd_ncarry = keep;
+  pl->sd_out0 += out_n;
+  *folded = out_n;
+  return DSPSR_B200_OK;
+}
+
 int pipeline_block (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat_new,
                     uint64_t in_span, uint64_t* ndat_folded)
 {
@@ -771,29 +881,19 @@ int pipeline_block (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat_new
   if (ndat >= sh.nfft) npart = (ndat - nfilt) / sh.nkeep;   // Convolution.C:486-487
   const uint64_t nout = npart * sh.nkeep;
 
-  if (npart > 0)
+  uint64_t nfolded = nout;
+  if (npart > 0 && pl->sd_on)
+  {
+    KernelClock kc {&PipeClock::mark, &pl->clock};
+    int rc = pipeline_sd_block (pl, in, npart, nout, pl->clock.on ? &kc : nullptr, &nfolded);
+    if (rc) return rc;
+  }
+  else if (npart > 0)
   {
     // Fold::fold (Fold.C:685-693): phase of the first output sample's midpoint;
     // the output starts nfilt_pos samples after the input (Convolution.C:599)
-    const double sampling_interval = 1.0 / pl->rate;
-    const double pps = sampling_interval / cfg.period_s;   // Fold.C:754-756
-    int rc;
-    if (pl->sub_on)
-    {
-      rc = pipeline_subint_plan (pl, nout, pps);
-      if (rc) return rc;
-    }
-    else
-    {
-      const double phi = pl->phase_continue
-                       ? pl->phase_next
-                       : fold_phi (cfg.start_day, cfg.start_sec, cfg.start_frac, cfg.epoch_day,
-                                   cfg.epoch_sec, cfg.epoch_frac, pl->in0 + sh.nfilt_pos,
-                                   pl->rate, cfg.period_s, cfg.reference_phase);
-      rc = pl->fold.set_bins (phi, pps, nout, &pl->phase_next);
-      if (rc) return rc;
-      pl->phase_continue = pl->in_pieces;
-    }
+    int rc = pipeline_fold_plan (pl, pl->in0, pl->in0 + sh.nfilt_pos, nout);
+    if (rc) return rc;
     FoldView fv = pl->fold.view (cfg.state, pl->nout, cfg.nchan);
     VoltView vv {nullptr, 0};
     const ConvTables tb = pl->conv.tables ();
@@ -871,7 +971,7 @@ int pipeline_block (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat_new
   pl->cur_carry = next;
   pl->ncarry = keep;
   pl->in0 += nout;
-  if (ndat_folded) *ndat_folded = nout;
+  if (ndat_folded) *ndat_folded = nfolded;
   return DSPSR_B200_OK;
 }
 
@@ -1365,6 +1465,24 @@ double dspsr_b200_fold_phi (int64_t sd, int64_t ss, double sf, int64_t ed, int64
   return fold_phi (sd, ss, sf, ed, es, ef, idat_start, rate, period, ref_phase);
 }
 
+int dspsr_b200_interchannel_delays (double cf, double dm, double rate, const double* freq,
+                                    unsigned nchan, int64_t* delay, double* frac,
+                                    int64_t* applied, int64_t* zero_delay, uint64_t* total_delay)
+{
+  if (!freq || nchan == 0 || !(rate > 0) || !(cf > 0)) return DSPSR_B200_EINVAL;
+  InterchannelDelays d;
+  interchannel_delays (cf, dm, rate, freq, nchan, &d);
+  for (unsigned c = 0; c < nchan; c++)
+  {
+    if (delay) delay[c] = d.delay[c];
+    if (frac) frac[c] = d.frac[c];
+    if (applied) applied[c] = d.applied[c];
+  }
+  if (zero_delay) *zero_delay = d.zero_delay;
+  if (total_delay) *total_delay = d.total_delay;
+  return DSPSR_B200_OK;
+}
+
 int64_t dspsr_b200_fold_plan_count (double phi, double pps, uint64_t ndat)
 {
   return build_fold_plan (phi, pps, ndat, nullptr);
@@ -1826,7 +1944,48 @@ int dspsr_b200_pipeline_create (dspsr_b200_context* ctx, const dspsr_b200_pipeli
   pl->rate = std::fabs (cfg->bandwidth_mhz) / double (nchan) * 1e6;
   int rc = pl->conv.init (ctx, nchan, cfg->npol, cfg->nfft, cfg->nfilt_pos, cfg->nfilt_neg,
                           cfg->scratch_bytes);
-  if (!rc && !fb)
+  if (!rc && cfg->interchannel)
+  {
+    // DedispersionPipe::construct_interchan (DedispersionPipe.C:435-470): the
+    // response takes each channel's fractional delay (Dedispersion::build,
+    // Dedispersion.C:84-97 with build_setup :141-162), SampleDelay the whole
+    // samples; channel centres as Observation::get_centre_frequency gives them
+    std::vector<double> freq (nchan), frac (nchan);
+    for (unsigned ic = 0; ic < nchan; ic++)
+      freq[ic] = fb ? channel_centre (cfg->centre_freq_mhz, cfg->bandwidth_mhz, nchan, ic,
+                                      cfg->dual_sideband != 0, true)
+                    : channel_centre (cfg->centre_freq_mhz, cfg->bandwidth_mhz, nchan, ic,
+                                      false, false);
+    interchannel_delays (cfg->centre_freq_mhz, cfg->dm, pl->rate, freq.data (), nchan, &pl->sd);
+    bool ok = nchan > 1 && !(cfg->dc_centred && !fb);
+    std::vector<int> applied (nchan);
+    for (unsigned ic = 0; ic < nchan && ok; ic++)
+    {
+      ok = pl->sd.applied[ic] >= 0 && uint64_t (pl->sd.applied[ic]) <= pl->sd.total_delay;
+      applied[ic] = int (pl->sd.applied[ic]);
+      frac[ic] = pl->sd.frac[ic] / (cfg->bandwidth_mhz / double (nchan));   // microseconds
+    }
+    if (!ok)
+      rc = fail (ctx, DSPSR_B200_EINVAL,
+                 "pipeline: inter-channel dedispersion needs several channels whose delays "
+                 "lie within the span SampleDelay buffers");
+    else
+    {
+      const int swap = fb ? 1 : cfg->dual_sideband != 0;
+      rc = build_response (&pl->conv, freq.data (), cfg->bandwidth_mhz, cfg->dm, swap,
+                           cfg->chirp_mode, cfg->nfft, frac.data ());
+    }
+    if (!rc)
+    {
+      cudaError_t e = pl->sd_applied.reserve (nchan);
+      if (e == cudaSuccess)
+        e = cudaMemcpy (pl->sd_applied.ptr, applied.data (), nchan * sizeof (int),
+                        cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) rc = cuda_fail (ctx, e, "upload delays");
+    }
+    pl->sd_on = !rc;
+  }
+  else if (!rc && !fb)
     rc = dspsr_b200_convolution_set_dedispersion (&pl->conv, cfg->centre_freq_mhz,
                                                   cfg->bandwidth_mhz, cfg->dm, cfg->nchan,
                                                   cfg->dual_sideband, cfg->dc_centred,
@@ -1930,6 +2089,9 @@ int dspsr_b200_pipeline_destroy (dspsr_b200_pipeline* pl)
     if (u.ev) cudaEventDestroy (u.ev);
   }
   pl->fbbuf.release ();
+  pl->sd_applied.release ();
+  pl->sd_buf[0].release ();
+  pl->sd_buf[1].release ();
   delete pl;
   return DSPSR_B200_OK;
 }
@@ -2152,6 +2314,8 @@ int dspsr_b200_pipeline_reset (dspsr_b200_pipeline* pl)
   if (!pl) return DSPSR_B200_EINVAL;
   pl->ncarry = 0;
   pl->in0 = 0;
+  pl->sd_ncarry = 0;
+  pl->sd_out0 = 0;
   if (pl->sub_on)
   {
     const int rc = subint_drain (pl, true);      // unloads already started complete

@@ -122,6 +122,38 @@ void bittable8 (double spacing, bool twos_complement, float* lut, double* scale_
   if (scale_out) *scale_out = scale;
 }
 
+void interchannel_delays (double cf, double dm, double rate, const double* freq, unsigned nchan,
+                          InterchannelDelays* o)
+{
+  const double dispersion = dm / 2.41e-4;   // Dedispersion::dm_dispersion
+  o->delay.assign (nchan, 0);
+  o->frac.assign (nchan, 0.0);
+  o->applied.assign (nchan, 0);
+  for (unsigned c = 0; c < nchan; c++)
+  {
+    const double time_delay = dispersion * (1.0 / (cf * cf) - 1.0 / (freq[c] * freq[c]));
+    const double sample_delay = time_delay * rate;
+    o->delay[c] = int64_t (std::floor (sample_delay + 0.5));
+    o->frac[c] = sample_delay - double (o->delay[c]);
+  }
+  // get_delay_range over all channels (DedispersionSampleDelay.C:130-140):
+  // the delay at the mean of the end channels' centres
+  const double f = (freq[0] + freq[nchan - 1]) / 2;
+  const double d = dispersion * (1.0 / (cf * cf) - 1.0 / (f * f));
+  o->span_centre = int64_t (std::floor (d * rate + 0.5));
+  o->zero_delay = 0;
+  for (unsigned c = 0; c < nchan; c++)
+    o->zero_delay = std::max (o->zero_delay, o->delay[c] - o->span_centre);
+  o->total_delay = 0;
+  for (unsigned c = 0; c < nchan; c++)
+  {
+    const int64_t zd = o->span_centre + o->zero_delay;
+    if (zd - o->delay[c] > int64_t (o->total_delay)) o->total_delay = uint64_t (zd - o->delay[c]);
+    // SampleDelay::transformation (SampleDelay.C:277-285)
+    o->applied[c] = o->zero_delay ? zd - o->delay[c] : o->delay[c];
+  }
+}
+
 // Fold::get_phi with a constant period (Fold.C:685-693, 975-979):
 //   t   = start + (idat_start + 0.5) / rate          (MJD + seconds)
 //   phi = fmod((t - epoch) in seconds, P) / P - reference_phase

@@ -43,6 +43,23 @@ std::vector<unsigned> ifb_fine_channel_plan (unsigned nchan, unsigned per_coarse
 // (transitions t_start, t_end); swap exchanges the halves.  0 on success.
 int apodization (int type, unsigned ndat, unsigned t_start, unsigned t_end, bool swap,
                  float* window);
+// Inter-channel dispersion delays (DedispersionPipe -K): the integer sample
+// delay of each channel and its fractional remainder
+// (Dedispersion::SampleDelay::get_sample_delay, DedispersionSampleDelay.C:
+// 82-100), and SampleDelay::build's relative delays (SampleDelay.C:65-141):
+// zero_delay, total_delay and the delay applied to each channel.
+struct InterchannelDelays
+{
+  std::vector<int64_t> delay;      // floor(sample delay + 0.5)
+  std::vector<double> frac;        // sample delay - delay, in samples
+  std::vector<int64_t> applied;    // output sample t of channel c reads input t + applied[c]
+  int64_t span_centre = 0;
+  int64_t zero_delay = 0;
+  uint64_t total_delay = 0;
+};
+void interchannel_delays (double centre_frequency, double dm, double rate, const double* freq,
+                          unsigned nchan, InterchannelDelays* out);
+
 // Returns the number of segments; fills *out when non-null.  *x_end, when
 // non-null, receives the recurrence's phase after the last sample: the phi
 // with which the sequence goes on for the samples that follow.

@@ -1075,10 +1075,10 @@ k_ifb_cols (const float2* __restrict__ scratch, const IfbShape sh, const float2*
 // (Response::doswap, Response.C:998-1050).  Written in four-step order
 // H[c][k1][k2] for k = k1 + n1*k2.
 __global__ void k_build_chirp (float2* __restrict__ H, const double* __restrict__ chan_freq,
-                               const double* __restrict__ coeff, const unsigned nfft,
-                               const unsigned n1, const unsigned n2, const double binwidth,
-                               const double half_chanwidth, const int swap_halves,
-                               const int chirp_mode, const float scale)
+                               const double* __restrict__ coeff, const double* __restrict__ frac_us,
+                               const unsigned nfft, const unsigned n1, const unsigned n2,
+                               const double binwidth, const double half_chanwidth,
+                               const int swap_halves, const int chirp_mode, const float scale)
 {
   const uint64_t idx = uint64_t (blockIdx.x) * blockDim.x + threadIdx.x;
   const unsigned c = blockIdx.y;
@@ -1089,7 +1089,14 @@ __global__ void k_build_chirp (float2* __restrict__ H, const double* __restrict_
   const double cf = chan_freq[c];
   const double freq = __dsub_rn (__dmul_rn (double (ipt), binwidth), half_chanwidth);
   const double num = __dmul_rn (coeff[c], __dmul_rn (freq, freq));
-  const double phase = __ddiv_rn (num, __dadd_rn (cf, freq));
+  double phase = __ddiv_rn (num, __dadd_rn (cf, freq));
+  if (frac_us)
+  {
+    // Dedispersion::build_compute (Dedispersion.C:176-179): the phase of the
+    // channel's fractional-sample inter-channel delay
+    const double minus_two_pi = -6.283185307179586476925286766559;
+    phase = __dadd_rn (phase, __dmul_rn (__dmul_rn (minus_two_pi, freq), frac_us[c]));
+  }
   float re, im;
   if (chirp_mode == 0)
   {
@@ -1513,6 +1520,27 @@ __global__ void k_fold (const float* __restrict__ in, const uint64_t in_span,
   }
 }
 
+// SampleDelay::transformation (SampleDelay.C:247-298) fused with detection and
+// the fold: output sample t of channel c is voltage t + applied[c] of that
+// channel (rows [chan][pol] of span values).
+template <int NOUT>
+__global__ void k_delay_fold (const float2* __restrict__ v, const uint64_t span,
+                              const int* __restrict__ applied, const uint64_t ndat,
+                              const unsigned npol, const FoldView fv)
+{
+  const uint64_t t = uint64_t (blockIdx.x) * blockDim.x + threadIdx.x;
+  const unsigned c = blockIdx.y;
+  const bool ok = t < ndat;
+  float2 p = make_float2 (0.f, 0.f), q = make_float2 (0.f, 0.f);
+  if (ok)
+  {
+    const uint64_t i = t + uint64_t (__ldg (applied + c));
+    p = v[(uint64_t (c) * npol) * span + i];
+    if (npol == 2) q = v[(uint64_t (c) * npol + 1) * span + i];
+  }
+  emit_fold<NOUT> (fv, c, npol, ok, t, p, q);
+}
+
 __global__ void k_binplan (const FoldSegment* __restrict__ segs, const int nseg,
                            const uint64_t ndat, const unsigned nbin, uint32_t* __restrict__ out)
 {
@@ -1852,14 +1880,14 @@ cudaError_t launch_inverse_filterbank (const IfbShape& sh, const IfbTables& tb,
 }
 
 cudaError_t launch_build_chirp (float2* H, const double* d_chan_freq, const double* d_coeff,
-                                unsigned nchan, unsigned nfft, unsigned n1, unsigned n2,
-                                double binwidth, double half_chanwidth, int swap_halves,
-                                int chirp_mode, float scale, cudaStream_t st)
+                                const double* d_frac_us, unsigned nchan, unsigned nfft,
+                                unsigned n1, unsigned n2, double binwidth, double half_chanwidth,
+                                int swap_halves, int chirp_mode, float scale, cudaStream_t st)
 {
   const dim3 grid ((nfft + 255) / 256, nchan);
   g_launches++;
-  k_build_chirp<<<grid, 256, 0, st>>> (H, d_chan_freq, d_coeff, nfft, n1, n2, binwidth,
-                                        half_chanwidth, swap_halves, chirp_mode, scale);
+  k_build_chirp<<<grid, 256, 0, st>>> (H, d_chan_freq, d_coeff, d_frac_us, nfft, n1, n2,
+                                        binwidth, half_chanwidth, swap_halves, chirp_mode, scale);
   return cudaGetLastError ();
 }
 
@@ -2036,6 +2064,22 @@ cudaError_t launch_fold (const float* in, uint64_t in_span, uint64_t ndat, unsig
   g_launches++;
   k_fold<<<dim3 (unsigned ((ndat + 255) / 256), nchan), 256, 0, st>>> (in, in_span, ndat, npol,
                                                                         fv);
+  return cudaGetLastError ();
+}
+
+cudaError_t launch_delay_fold (const float2* v, uint64_t span, const int* applied, uint64_t ndat,
+                               unsigned nchan, unsigned npol, const FoldView& fv, cudaStream_t st,
+                               const KernelClock* clk)
+{
+  if (ndat == 0) return cudaSuccess;
+  const dim3 grid (unsigned ((ndat + 255) / 256), nchan);
+  ClockScope cs (clk, KK_INV_COLS, st);
+  if (fv.nout == 1)
+    k_delay_fold<1><<<grid, 256, 0, st>>> (v, span, applied, ndat, npol, fv);
+  else if (fv.nout == 2)
+    k_delay_fold<2><<<grid, 256, 0, st>>> (v, span, applied, ndat, npol, fv);
+  else
+    k_delay_fold<4><<<grid, 256, 0, st>>> (v, span, applied, ndat, npol, fv);
   return cudaGetLastError ();
 }
 

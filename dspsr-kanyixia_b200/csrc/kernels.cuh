@@ -104,11 +104,10 @@ cudaError_t launch_convolution (const ConvShape& shape, const ConvTables& tables
 
 // Builds the dispersion response directly in four-step order on the device.
 // chan_freq/coeff per response channel computed on the host in double.
-cudaError_t launch_build_chirp (float2* H, const double* d_chan_freq,
-                                const double* d_coeff, unsigned nchan, unsigned nfft,
-                                unsigned n1, unsigned n2, double binwidth,
-                                double half_chanwidth, int swap_halves, int chirp_mode,
-                                float scale, cudaStream_t stream);
+cudaError_t launch_build_chirp (float2* H, const double* d_chan_freq, const double* d_coeff,
+                                const double* d_frac_us, unsigned nchan, unsigned nfft,
+                                unsigned n1, unsigned n2, double binwidth, double half_chanwidth,
+                                int swap_halves, int chirp_mode, float scale, cudaStream_t st);
 // Reorders an FFT-order response [nchan][nfft] into four-step order.
 cudaError_t launch_permute_response (float2* H, const float2* src, unsigned nchan,
                                      unsigned n1, unsigned n2, cudaStream_t stream);
@@ -189,6 +188,10 @@ cudaError_t launch_fold (const float* in, uint64_t in_span, uint64_t ndat, unsig
                          unsigned npol, const FoldView& fold, cudaStream_t stream);
 cudaError_t launch_binplan (const FoldSegment* segs, int nseg, uint64_t ndat, unsigned nbin,
                             uint32_t* out, cudaStream_t stream);
+// SampleDelay + detection + fold over voltages [chan][pol] (span values a row)
+cudaError_t launch_delay_fold (const float2* v, uint64_t span, const int* applied, uint64_t ndat,
+                               unsigned nchan, unsigned npol, const FoldView& fv, cudaStream_t st,
+                               const KernelClock* clk);
 
 // number of detected output polarisations for a detection state
 __host__ __device__ inline int detect_nout (int state) { return state == 0 ? 1 : state == 1 ? 2 : 4; }

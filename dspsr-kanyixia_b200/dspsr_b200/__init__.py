@@ -26,7 +26,7 @@ from ._capi import (B200Error, PipelineConfig, INTENSITY, PPQQ, COHERENCE, STOKE
 __all__ = ["Context", "Convolution", "InverseFilterbank", "Fold", "apodization", "Pipeline", "PipelineConfig", "B200Error",
            "smearing_samples", "minimum_ndat", "optimal_fft_length", "bittable8", "fold_phi",
            "sk_limits", "DADAFile", "dada_parse", "dada_is_valid", "ascii_header_get",
-           "ascii_header_set", "write_dada", "TimeDivide",
+           "ascii_header_set", "write_dada", "TimeDivide", "interchannel_delays",
            "fold_plan_count", "INTENSITY", "PPQQ", "COHERENCE", "STOKES", "INT8_TFPD",
            "INT16_TFPD", "FLOAT_FPT", "CHIRP_REFERENCE", "CHIRP_FP64", "NOUT"]
 
@@ -99,6 +99,27 @@ def fold_phi(start_mjd, epoch_mjd, idat_start, rate, period, reference_phase=0.0
     return _capi.lib().dspsr_b200_fold_phi(start_mjd[0], start_mjd[1], start_mjd[2],
                                            epoch_mjd[0], epoch_mjd[1], epoch_mjd[2], idat_start,
                                            rate, period, reference_phase)
+
+
+def interchannel_delays(centre_freq, dm, rate, chan_freq):
+    """Dedispersion::SampleDelay + SampleDelay::build for channels centred at
+    chan_freq: dict of delay, frac, applied (arrays), zero_delay, total_delay."""
+    f = np.ascontiguousarray(chan_freq, np.float64)
+    n = f.size
+    delay = np.empty(n, np.int64)
+    frac = np.empty(n, np.float64)
+    applied = np.empty(n, np.int64)
+    zd = ctypes.c_int64()
+    td = ctypes.c_uint64()
+    P64 = ctypes.POINTER(ctypes.c_int64)
+    PD = ctypes.POINTER(ctypes.c_double)
+    rc = _capi.lib().dspsr_b200_interchannel_delays(
+        centre_freq, dm, rate, f.ctypes.data_as(PD), n, delay.ctypes.data_as(P64),
+        frac.ctypes.data_as(PD), applied.ctypes.data_as(P64), ctypes.byref(zd), ctypes.byref(td))
+    if rc:
+        raise B200Error(rc, "interchannel_delays: invalid argument")
+    return dict(delay=delay, frac=frac, applied=applied, zero_delay=zd.value,
+                total_delay=td.value)
 
 
 def kernel_launches():
@@ -691,7 +712,7 @@ def make_config(centre_freq, bandwidth, dm, nchan, npol, nfft, nfilt_pos, nfilt_
                 start_mjd=(60000, 0, 0.0), epoch_mjd=(60000, 0, 0.0), reference_phase=0.0,
                 dual_sideband=1, offset_binary=0, scratch_bytes=0, filterbank_nchan=0,
                 subint_seconds=0.0, subint_turns=0.0, subint_slots=0,
-                subint_epoch=(0, 0, 0.0), fused_filterbank=0):
+                subint_epoch=(0, 0, 0.0), fused_filterbank=0, interchannel=0):
     """Fill a PipelineConfig (the fields DedispersionPipe / LoadToFold set up).
     With filterbank_nchan > 1, nchan counts input channels, and nfft and the
     smearing (nfilt_pos, nfilt_neg) refer to the filterbank's output channels."""
@@ -726,6 +747,7 @@ def make_config(centre_freq, bandwidth, dm, nchan, npol, nfft, nfilt_pos, nfilt_
     cfg.subint_slots = subint_slots
     cfg.subint_epoch_day, cfg.subint_epoch_sec, cfg.subint_epoch_frac = subint_epoch
     cfg.fused_filterbank = fused_filterbank
+    cfg.interchannel = interchannel
     return cfg
 
 

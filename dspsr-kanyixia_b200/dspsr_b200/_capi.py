@@ -65,6 +65,7 @@ class PipelineConfig(ctypes.Structure):
         ("subint_epoch_frac", c_dbl),
         ("subint_slots", c_uint),
         ("fused_filterbank", c_int),
+        ("interchannel", c_int),
     ]
 
 
@@ -167,6 +168,10 @@ SIGNATURES = {
     "dspsr_b200_fold_phi": (c_dbl, [c_i64, c_i64, c_dbl, c_i64, c_i64, c_dbl, c_u64, c_dbl,
                                     c_dbl, c_dbl]),
     "dspsr_b200_fold_plan_count": (c_i64, [c_dbl, c_dbl, c_u64]),
+    "dspsr_b200_interchannel_delays": (c_int, [c_dbl, c_dbl, c_dbl, ctypes.POINTER(c_dbl), c_uint,
+                                               ctypes.POINTER(c_i64), ctypes.POINTER(c_dbl),
+                                               ctypes.POINTER(c_i64), ctypes.POINTER(c_i64),
+                                               c_u64p]),
     "dspsr_b200_sk_limits": (c_int, [c_uint, c_uint, ctypes.c_float, c_uint, c_fp, c_fp]),
     "dspsr_b200_unpack8": (c_int, [c_vp, c_vp, c_u64, c_uint, c_uint, c_uint, c_fp, c_vp, c_u64]),
     "dspsr_b200_unpack16": (c_int, [c_vp, c_vp, c_u64, c_uint, c_uint, c_uint, c_int, c_vp,

@@ -118,6 +118,17 @@ int dspsr_b200_sk_limits (unsigned M, unsigned Nd, float std_devs, unsigned ntes
 #define DSPSR_B200_APOD_TUKEY    4
 int dspsr_b200_apodization (int type, unsigned ndat, unsigned transition_start,
                             unsigned transition_end, int swap_halves, float* window);
+/* Inter-channel dispersion delays for channels centred at freq_mhz[nchan],
+   sampled at rate_hz, relative to the band centre centre_freq_mhz:
+   Dedispersion::SampleDelay (DedispersionSampleDelay.C:26-140) gives delay[c]
+   (the nearest whole-sample delay) and frac[c] (the remainder, samples);
+   SampleDelay::build (SampleDelay.C:65-141) gives zero_delay, total_delay and
+   applied[c], the shift SampleDelay::transformation (:247-298) applies:
+   output sample t of channel c = input sample t + applied[c]. */
+int dspsr_b200_interchannel_delays (double centre_freq_mhz, double dm, double rate_hz,
+                                    const double* freq_mhz, unsigned nchan, int64_t* delay,
+                                    double* frac, int64_t* applied, int64_t* zero_delay,
+                                    uint64_t* total_delay);
 /* Number of arithmetic segments the exact fold-bin plan needs for a block
    (see dspsr_b200_fold_set_bins); lets a caller size buffers. */
 int64_t dspsr_b200_fold_plan_count (double phi, double phase_per_sample,
@@ -415,6 +426,12 @@ typedef struct
      FFT split allows it (its output then never goes through memory);
      -1 = always run the filterbank as a stage of its own */
   int fused_filterbank;
+  /* DedispersionPipe's inter-channel dedispersion (-K, DedispersionPipe.C:
+     435-470): each channel's response takes the fractional-sample remainder of
+     its dispersion delay (Dedispersion.C:141-187) and a SampleDelay stage
+     (SampleDelay.C:65-304) shifts the channels by whole samples before
+     detection, so the channels' profiles line up; 0 = off */
+  int interchannel;
 } dspsr_b200_pipeline_config;
 
 int dspsr_b200_pipeline_create (dspsr_b200_context* ctx,

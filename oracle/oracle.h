@@ -84,6 +84,12 @@ double orc_channel_centre (double centre_freq, double bandwidth, unsigned nchan,
 void orc_dedispersion_response_channels (const double* chan_freq, unsigned nchan,
                                          double bandwidth, double dm, unsigned ndat,
                                          int mode, unsigned norm_nfft, float* out);
+/* the same with the fractional inter-channel delay of each channel in
+   microseconds (Dedispersion.C:141-187) */
+void orc_dedispersion_response_channels_delay (const double* chan_freq, unsigned nchan,
+                                               double bw, double dm, unsigned ndat, int mode,
+                                               unsigned norm_nfft, const double* frac_delay_us,
+                                               float* out);
 void orc_dedispersion_response_channels_f64 (const double* chan_freq, unsigned nchan,
                                              double bandwidth, double dm, unsigned ndat,
                                              unsigned norm_nfft, double* out);

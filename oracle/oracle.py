@@ -71,6 +71,8 @@ _SIGS = {
     "orc_channel_centre": (c_dbl, [c_dbl, c_dbl, c_uint, c_uint, c_int, c_int]),
     "orc_dedispersion_response_channels": (None, [f64p, c_uint, c_dbl, c_dbl, c_uint, c_int,
                                                   c_uint, f32p]),
+    "orc_dedispersion_response_channels_delay": (None, [f64p, c_uint, c_dbl, c_dbl, c_uint, c_int,
+                                                         c_uint, f64p, f32p]),
     "orc_dedispersion_response_channels_f64": (None, [f64p, c_uint, c_dbl, c_dbl, c_uint,
                                                       c_uint, f64p]),
     "orc_filterbank_f32": (c_u64, [f32p, c_u64, c_u64, c_int, c_int, c_uint, f32p, c_u64]),
@@ -163,9 +165,17 @@ def channel_centres(cf, bw, nchan, swap=False, dc_centred=False):
                      for i in range(nchan)], np.float64)
 
 
-def dedispersion_response_channels(chan_freq, bw, dm, ndat, mode=0, norm_nfft=None, fp64=False):
+def dedispersion_response_channels(chan_freq, bw, dm, ndat, mode=0, norm_nfft=None, fp64=False,
+                                   frac_delay_us=None):
     chan_freq = np.ascontiguousarray(chan_freq, np.float64)
     nchan = chan_freq.size
+    if frac_delay_us is not None:
+        assert not fp64
+        out = np.empty(nchan * ndat, np.complex64)
+        lib().orc_dedispersion_response_channels_delay(
+            chan_freq, nchan, bw, dm, ndat, mode, norm_nfft or ndat,
+            np.ascontiguousarray(frac_delay_us, np.float64), out.view(np.float32))
+        return out.reshape(nchan, ndat)
     if fp64:
         out = np.empty(nchan * ndat, np.complex128)
         lib().orc_dedispersion_response_channels_f64(chan_freq, nchan, bw, dm, ndat,
@@ -504,4 +514,40 @@ def subint_block_actions(td, start, ndat, rate):
             first = False
             continue
         out.append(("close", "complete"))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Inter-channel dispersion delays: Dedispersion::SampleDelay
+# (Signal/General/DedispersionSampleDelay.C:26-140) and SampleDelay::build /
+# transformation (Signal/General/SampleDelay.C:65-298), pure Python.
+# ---------------------------------------------------------------------------
+
+def interchannel_delays(cf, dm, rate, chan_freq):
+    dispersion = dm / 2.41e-4
+    delay, frac = [], []
+    for f in chan_freq:
+        sample_delay = dispersion * (1.0 / (cf * cf) - 1.0 / (f * f)) * rate
+        d = math.floor(sample_delay + 0.5)
+        delay.append(int(d))
+        frac.append(sample_delay - d)
+    fm = (chan_freq[0] + chan_freq[-1]) / 2
+    span = int(math.floor(dispersion * (1.0 / (cf * cf) - 1.0 / (fm * fm)) * rate + 0.5))
+    zero = max([0] + [d - span for d in delay])
+    zd = span + zero
+    total = max([0] + [zd - d for d in delay])
+    applied = [zd - d if zero else d for d in delay]
+    return dict(delay=np.array(delay, np.int64), frac=np.array(frac), applied=np.array(applied),
+                zero_delay=zero, total_delay=total)
+
+
+def sample_delay_block(y, applied, total):
+    """SampleDelay::transformation on one block y [chan][pol][t]: output
+    [chan][pol][t] = y[chan][pol][t + applied[chan]] for t < ndat - total."""
+    n = y.shape[2] - total
+    if n <= 0:
+        return y[:, :, :0]
+    out = np.empty(y.shape[:2] + (n,), y.dtype)
+    for c in range(y.shape[0]):
+        out[c] = y[c, :, applied[c]:applied[c] + n]
     return out

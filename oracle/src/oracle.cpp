@@ -581,7 +581,8 @@ double orc_channel_centre (double cf, double bw, unsigned nchan, unsigned ichan,
 namespace {
 template <typename T>
 void response_channels (const double* chan_freq, unsigned nchan, double bw, double dm,
-                        unsigned ndat, int mode, unsigned norm_nfft, std::complex<T>* h)
+                        unsigned ndat, int mode, unsigned norm_nfft, std::complex<T>* h,
+                        const double* frac_delay_us = nullptr)
 {
   const double chanwidth = bw / double (nchan);
   const double binwidth = chanwidth / double (ndat);
@@ -593,12 +594,15 @@ void response_channels (const double* chan_freq, unsigned nchan, double bw, doub
   {
     const double f0 = chan_freq[c];
     const double coeff = -sign * 2 * M_PI * dispersion_per_MHz / sqr (f0);
+    // Dedispersion::build_setup / build_compute (Dedispersion.C:141-187): the
+    // fractional-sample inter-channel delay, microseconds
+    const double fd = frac_delay_us ? frac_delay_us[c] : 0.0;
     for (unsigned k = 0; k < ndat; k++)
     {
       // FFT-order bin k holds natural bin (k + ndat/2) mod ndat
       const unsigned ipt = (k + ndat / 2) % ndat;
       const double freq = double (ipt) * binwidth - 0.5 * chanwidth;
-      const double phase = coeff * sqr (freq) / (f0 + freq) + (-2.0 * M_PI * freq * 0.0);
+      const double phase = coeff * sqr (freq) / (f0 + freq) + (-2.0 * M_PI * freq * fd);
       std::complex<T>& o = h[uint64_t (c) * ndat + k];
       if (sizeof (T) == 8)
         o = std::complex<T> (T (std::cos (phase) * s), T (std::sin (phase) * s));
@@ -653,6 +657,15 @@ void orc_dedispersion_response_channels (const double* chan_freq, unsigned nchan
 {
   response_channels<float> (chan_freq, nchan, bw, dm, ndat, mode, norm_nfft,
                             reinterpret_cast<std::complex<float>*> (out));
+}
+
+void orc_dedispersion_response_channels_delay (const double* chan_freq, unsigned nchan,
+                                               double bw, double dm, unsigned ndat, int mode,
+                                               unsigned norm_nfft, const double* frac_delay_us,
+                                               float* out)
+{
+  response_channels<float> (chan_freq, nchan, bw, dm, ndat, mode, norm_nfft,
+                            reinterpret_cast<std::complex<float>*> (out), frac_delay_us);
 }
 
 void orc_dedispersion_response_channels_f64 (const double* chan_freq, unsigned nchan, double bw,

@@ -28,6 +28,19 @@ def oracle_chain(orc, b2, raw_blocks, cfg, fp64=False):
 
 def oracle_detected(orc, b2, raw_blocks, cfg, fp64=False):
     """The detected output of the whole stream: (d [chan][nout][t], nchan)."""
+    y, nchan = oracle_voltages(orc, b2, raw_blocks, cfg, fp64)
+    if cfg["npol"] == 1:
+        d = (y.real ** 2 + y.imag ** 2)
+        d = d.reshape(nchan, 1, -1)
+    else:
+        d = orc.detect(y, cfg["state"])
+    return d, nchan
+
+
+def oracle_voltages(orc, b2, raw_blocks, cfg, fp64=False, interchannel=None):
+    """The dedispersed voltages of the whole stream: (y [chan][pol][t], nchan).
+    interchannel: a dict to receive the inter-channel delays, whose fractional
+    parts then enter the response (Dedispersion.C:141-187)."""
     nchan, npol = cfg["nchan"], cfg["npol"]
     kind = cfg["kind"]
     raw = np.concatenate([r.reshape(-1) for r in raw_blocks])
@@ -44,7 +57,21 @@ def oracle_detected(orc, b2, raw_blocks, cfg, fp64=False):
     nfft, pos, neg = cfg["nfft"], cfg["pos"], cfg["neg"]
     nk = nfft - pos - neg
     fb = cfg.get("fb", 0)
-    if fb:
+    if interchannel is not None:
+        if fb:
+            x = orc.filterbank(x, fb)
+            nchan *= fb
+            freqs = orc.channel_centres(cfg["cf"], cfg["bw"], nchan, swap=True, dc_centred=True)
+        else:
+            freqs = orc.channel_centres(cfg["cf"], cfg["bw"], nchan)
+        rate = abs(cfg["bw"]) / nchan * 1e6
+        delays = orc.interchannel_delays(cfg["cf"], cfg["dm"], rate, list(freqs))
+        interchannel.update(delays)
+        frac_us = delays["frac"] / (cfg["bw"] / nchan)
+        h = orc.dedispersion_response_channels(freqs, cfg["bw"], cfg["dm"], nfft, mode=0,
+                                               frac_delay_us=frac_us)
+        y = orc.convolve(x, h, nfft, pos, neg)
+    elif fb:
         # Filterbank (freq_res = 1): DC-centred, swapped output channels
         x = orc.filterbank(x.astype(np.complex128) if fp64 else x, fb)
         nchan *= fb
@@ -61,12 +88,7 @@ def oracle_detected(orc, b2, raw_blocks, cfg, fp64=False):
         h = orc.dedispersion_response(cfg["cf"], cfg["bw"], cfg["dm"], nchan, nfft,
                                       input_nchan=nchan, mode=0)
         y = orc.convolve(x, h, nfft, pos, neg)
-    if npol == 1:
-        d = (y.real ** 2 + y.imag ** 2)
-        d = d.reshape(nchan, 1, -1)
-    else:
-        d = orc.detect(y, cfg["state"])
-    return d, nchan
+    return y, nchan
 
 
 def block_outputs(b2, raw_blocks, cfg):
@@ -566,3 +588,68 @@ def test_pipeline_fused_filterbank_matches_stage(ctx, b2, orc, kind):
     hostrun = run(True, host=True)
     check(hostrun[0], hostrun[1], hostrun[2], fused[0].astype(np.float64), fused[1], fused[2],
           cfg["state"], rtol=2e-6)
+
+
+def oracle_interchannel_chain(orc, b2, raw_blocks, cfg):
+    """DedispersionPipe with -K: the convolution's voltages pass SampleDelay
+    (with its InputBuffering of total_delay samples) before detection and the
+    fold; the fold's phase is taken at each block's first SampleDelay output,
+    zero_delay samples later than the convolution's."""
+    delays = {}
+    y, nchan = oracle_voltages(orc, b2, raw_blocks, cfg, interchannel=delays)
+    rate = abs(cfg["bw"]) / nchan * 1e6
+    pps = (1.0 / rate) / cfg["period"]
+    nbin = cfg["nbin"]
+    nout = 4 if cfg["state"] in (2, 3) else (2 if cfg["state"] == 1 else 1)
+    prof = np.zeros((nchan, nout, nbin), np.float32)
+    hits = np.zeros(nbin, np.uint32)
+    g0, total = 0, 0
+    tot = delays["total_delay"]
+    for in0, n in block_outputs(b2, raw_blocks, cfg):
+        seg = y[:, :, g0:in0 + n]
+        out = orc.sample_delay_block(seg, delays["applied"], tot)
+        m = out.shape[2]
+        if m:
+            d = orc.detect(np.ascontiguousarray(out), cfg["state"])
+            phi = orc.fold_phi(START, EPOCH, g0 + cfg["pos"] + delays["zero_delay"], rate,
+                               cfg["period"])
+            plan = orc.fold_binplan(phi, pps, m, nbin)
+            orc.fold_accumulate(np.ascontiguousarray(d), plan, nbin, prof, hits)
+        g0 += m
+        total += m
+    return prof, hits, total, delays
+
+
+@pytest.mark.parametrize("name,kw", [
+    # C2's shape: 64-channel filterbank (computed in the column pass), DM 500
+    # (DM 5: at C2's DM 500 the channels span 0.39 s, more data than the
+    # oracle should chew through here)
+    ("c2_fb64", dict(dm=5.0, bw=256.0, fb=64, nfft=1 << 16, state=3, nbin=1024,
+                     period=5.757e-3)),
+    # eight int16 channels straight from the input, coherence products
+    ("nchan8_int16", dict(dm=10.0, bw=64.0, nchan=8, nfft=1 << 14, state=2, kind=1,
+                          nbin=256, period=0.0031)),
+])
+def test_pipeline_interchannel_matches_oracle(ctx, b2, orc, name, kw):
+    """-K: fractional delays in the response and SampleDelay's whole-sample
+    shifts before the fold, against the oracle chain; the channels' pulse
+    then lines up."""
+    cfg = base_cfg(b2, **kw)
+    rng = np.random.default_rng(zlib.crc32(name.encode()))
+    nk = cfg["nfft"] - cfg["pos"] - cfg["neg"]
+    unit = cfg.get("fb", 0) or 1
+    blocks = make_blocks(rng, cfg, [(cfg["nfft"] + 2 * nk + 77) * unit, (nk - 3) * unit,
+                                    (2 * nk + 999) * unit])
+    c = b2.make_config(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nchan"], cfg["npol"], cfg["nfft"],
+                       cfg["pos"], cfg["neg"], cfg["nbin"], cfg["period"], state=cfg["state"],
+                       input_kind=cfg["kind"], lut=cfg["lut"], start_mjd=START, epoch_mjd=EPOCH,
+                       filterbank_nchan=cfg.get("fb", 0), interchannel=1)
+    pl = b2.Pipeline(ctx, c)
+    total = 0
+    for r in blocks:
+        total += pl.run(torch.from_numpy(r).cuda(), r.size // (cfg["nchan"] * cfg["npol"] * 2))
+    prof, hits = pl.get_profiles()
+    pl.close()
+    rprof, rhits, rtotal, delays = oracle_interchannel_chain(orc, b2, blocks, cfg)
+    assert delays["total_delay"] > 0
+    check(prof, hits, total, rprof, rhits, rtotal, cfg["state"])
