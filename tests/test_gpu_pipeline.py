@@ -653,3 +653,37 @@ def test_pipeline_interchannel_matches_oracle(ctx, b2, orc, name, kw):
     rprof, rhits, rtotal, delays = oracle_interchannel_chain(orc, b2, blocks, cfg)
     assert delays["total_delay"] > 0
     check(prof, hits, total, rprof, rhits, rtotal, cfg["state"])
+
+
+def test_pipeline_interchannel_aligns_channels(ctx, b2):
+    """A pulse train dispersed across 64 MHz (DM 30: 5.8 ms across the band,
+    more than the 5 ms period) through a 16-channel filterbank: without -K
+    the channels' profiles peak at phases spread by the inter-channel delays,
+    with -K they line up.  (The DC-centred filterbank's channel 8 holds the
+    Nyquist bin: half of it is the other band edge, so it is left out.)"""
+    from dspsr_b200 import synth
+    cf, bw, dm, period, nbin = 1400.0, 64.0, 30.0, 0.005, 256
+    raw, truth = synth.dispersed_pulse_train(ndat=1 << 22, cf=cf, bw=bw, dm=dm, period=period,
+                                             duty=0.03, snr=30.0, sigma=10.0, seed=11,
+                                             start_mjd=START, epoch_mjd=EPOCH)
+    pos, neg, nfft = b2.dispersion_plan(cf, bw, dm, 16, 1 << 14)
+
+    def peaks(interchannel):
+        c = b2.make_config(cf, bw, dm, 1, 2, nfft, pos, neg, nbin, period, start_mjd=START,
+                           epoch_mjd=EPOCH, filterbank_nchan=16, interchannel=interchannel)
+        pl = b2.Pipeline(ctx, c)
+        pl.run(torch.from_numpy(raw).cuda(), raw.size // 4)
+        prof, hits = pl.get_profiles()
+        pl.close()
+        p = prof[:, 0] / np.maximum(hits, 1)
+        return np.delete(np.argmax(p, axis=1), 8)
+
+    def spread(b):
+        # circular spread of the peak bins around their circular mean
+        ang = 2 * np.pi * b / nbin
+        mean = np.angle(np.mean(np.exp(1j * ang)))
+        d = np.angle(np.exp(1j * (ang - mean))) * nbin / (2 * np.pi)
+        return np.max(np.abs(d))
+
+    assert spread(peaks(0)) > 20
+    assert spread(peaks(1)) <= 2
