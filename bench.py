@@ -475,6 +475,29 @@ def run_b200(args, cfg, world, rank, local):
                            "ms_per_step": round(sms / args.steps, 4),
                            "note": "device-resident input; every closed sub-integration is "
                                    "copied to the host and handed to the unloader callback"}
+    if args.interchannel:
+        ck = b2.make_config(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nchan"], cfg["npol"], nfft,
+                            pos, neg, cfg["nbin"], cfg["period"], state=cfg["state"], lut=lut,
+                            start_mjd=START_MJD, epoch_mjd=EPOCH_MJD, filterbank_nchan=cfg["fb"],
+                            scratch_bytes=args.scratch_mib << 20, interchannel=1)
+        pl = b2.Pipeline(ctx, ck)
+        for i in range(args.warmup):
+            pl.run(blocks[i % NBLOCKS], ndat)
+        torch.cuda.synchronize()
+        k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k0.record()
+        kfold = 0
+        for i in range(args.steps):
+            kfold += pl.run(blocks[(args.warmup + i) % NBLOCKS], ndat)
+        k1.record()
+        torch.cuda.synchronize()
+        kms = max_over_ranks(k0.elapsed_time(k1), world)
+        pl.close()
+        extra["interchannel"] = {
+            "value": round(samples_per_step * args.steps * world / (kms / 1e3) / 1e6, 3),
+            "ms_per_step": round(kms / args.steps, 4), "samples_folded": int(kfold),
+            "note": "device-resident input; the convolution's voltages go through memory to "
+                    "SampleDelay + detect + fold (one extra round trip)"}
     if args.dada:
         import tempfile
         with tempfile.TemporaryDirectory() as tmpd:
@@ -1393,6 +1416,10 @@ def main():
     ap.add_argument("--subint-seconds", type=float, default=0.0,
                     help="also time the device-resident run folding sub-integrations of this "
                          "length (TimeDivide), unloaded through the callback (c1/c2)")
+    ap.add_argument("--interchannel", action="store_true",
+                    help="also time the device-resident run with inter-channel dedispersion "
+                         "(-K: fractional delays in the response, SampleDelay before the fold) "
+                         "(c1/c2)")
     ap.add_argument("--dada", action="store_true",
                     help="also time end to end from a DADA file holding the blocks "
                          "(pipeline_run_dada; the file is written first, so it is read from "
