@@ -685,5 +685,6 @@ def test_pipeline_interchannel_aligns_channels(ctx, b2):
         d = np.angle(np.exp(1j * (ang - mean))) * nbin / (2 * np.pi)
         return np.max(np.abs(d))
 
+    # the pulse is 0.03 x 256 = 7.7 bins wide: its peak bin wanders inside it
     assert spread(peaks(0)) > 20
-    assert spread(peaks(1)) <= 2
+    assert spread(peaks(1)) <= 5
