@@ -318,6 +318,11 @@ struct dspsr_b200_fold
   static constexpr int NRING = 8;
   static constexpr size_t INITIAL_SEGMENTS = 16384;
   DevBuf<FoldSegment> d_segs[NRING];
+  // with many channels the column of each sample is computed once per block
+  // (k_colplan) instead of from the segments in every channel
+  bool use_cols = false;
+  DevBuf<unsigned> d_cols[NRING];
+  uint64_t cols_cap = 0;
   FoldSegment* h_segs[NRING] = {};
   size_t h_cap[NRING] = {};
   cudaEvent_t done[NRING] = {};
@@ -424,6 +429,22 @@ struct dspsr_b200_fold
       B200_CHECK (ctx, cudaMemcpyAsync (d_segs[cur].ptr, h_segs[cur],
                                         plan.size () * sizeof (FoldSegment),
                                         cudaMemcpyHostToDevice, ctx->stream), "upload plan");
+    if (use_cols && n && !plan.empty ())
+    {
+      // every ring slot grows at once, with headroom, so that steady blocks
+      // allocate nothing (an allocation would wait for the device)
+      if (n > cols_cap)
+      {
+        cols_cap = n + n / 4;
+        for (int i = 0; i < NRING; i++)
+        {
+          d_cols[i].release ();
+          B200_CHECK (ctx, d_cols[i].reserve (cols_cap), "cudaMalloc fold columns");
+        }
+      }
+      B200_CHECK (ctx, launch_colplan (d_segs[cur].ptr, nseg, n, nbin, d_cols[cur].ptr,
+                                       ctx->stream), "fold columns");
+    }
     return DSPSR_B200_OK;
   }
   // marks the end of the work that reads the current plan buffer
@@ -442,6 +463,7 @@ struct dspsr_b200_fold
     v.hits = hits.ptr;
     v.nbin = nbin;
     v.stride = nbin * slots;
+    v.cols = use_cols && ndat && nseg ? d_cols[cur].ptr : nullptr;
     v.state = state;
     v.nout = nout;
     return v;
@@ -453,6 +475,8 @@ struct dspsr_b200_fold
     for (int i = 0; i < NRING; i++)
     {
       d_segs[i].release ();
+      d_cols[i].release ();
+      cols_cap = 0;
       if (h_segs[i]) cudaFreeHost (h_segs[i]);
       h_segs[i] = nullptr;
       if (done[i]) cudaEventDestroy (done[i]);
@@ -2033,6 +2057,7 @@ int dspsr_b200_pipeline_create (dspsr_b200_context* ctx, const dspsr_b200_pipeli
   }
   if (!rc) rc = pl->fold.init (ctx, cfg->nbin, nchan, pl->nout,
                                pl->sub_on ? unsigned (pl->sub_slots.size ()) : 1);
+  pl->fold.use_cols = nchan >= 4;
   // C2's shape -- a 64-channel filterbank of one dual-polarisation int8 or
   // int16 channel with four-step parts of 8 x n2 -- runs the filterbank
   // inside the forward column pass: its output never goes through memory

@@ -249,7 +249,8 @@ __device__ __forceinline__ void emit_fold (const FoldView& fv, unsigned c, unsig
                                            uint64_t t, float2 p, float2 q)
 {
   float v[4] = {0.f, 0.f, 0.f, 0.f};
-  unsigned bin = warp_fold_bin (fv.segs, fv.nseg, ok, t, fv.nbin);
+  unsigned bin = fv.cols ? (ok ? __ldg (fv.cols + t) : NO_COLUMN)
+                         : warp_fold_bin (fv.segs, fv.nseg, ok, t, fv.nbin);
   if (ok)
   {
     detect_values (fv.state, npol, p, q, v);
@@ -1541,6 +1542,16 @@ __global__ void k_delay_fold (const float2* __restrict__ v, const uint64_t span,
   emit_fold<NOUT> (fv, c, npol, ok, t, p, q);
 }
 
+// one thread per sample: the column warp_fold_bin would give it
+__global__ void k_colplan (const FoldSegment* __restrict__ segs, const int nseg,
+                           const uint64_t ndat, const unsigned nbin, unsigned* __restrict__ cols)
+{
+  const uint64_t t = uint64_t (blockIdx.x) * blockDim.x + threadIdx.x;
+  const bool ok = t < ndat;
+  const unsigned col = warp_fold_bin (segs, nseg, ok, t, nbin);
+  if (ok) cols[t] = col;
+}
+
 __global__ void k_binplan (const FoldSegment* __restrict__ segs, const int nseg,
                            const uint64_t ndat, const unsigned nbin, uint32_t* __restrict__ out)
 {
@@ -2064,6 +2075,15 @@ cudaError_t launch_fold (const float* in, uint64_t in_span, uint64_t ndat, unsig
   g_launches++;
   k_fold<<<dim3 (unsigned ((ndat + 255) / 256), nchan), 256, 0, st>>> (in, in_span, ndat, npol,
                                                                         fv);
+  return cudaGetLastError ();
+}
+
+cudaError_t launch_colplan (const FoldSegment* segs, int nseg, uint64_t ndat, unsigned nbin,
+                            unsigned* cols, cudaStream_t st)
+{
+  if (ndat == 0) return cudaSuccess;
+  g_launches++;
+  k_colplan<<<unsigned ((ndat + 255) / 256), 256, 0, st>>> (segs, nseg, ndat, nbin, cols);
   return cudaGetLastError ();
 }
 

@@ -40,6 +40,9 @@ struct FoldView
   unsigned* hits;        // [stride]
   unsigned nbin;
   unsigned stride;       // profile columns: nbin times the sub-integration slots
+  // when set: the profile column of every sample of the block (or NO_COLUMN),
+  // computed once for all channels instead of from segs in every channel
+  const unsigned* cols = nullptr;
   int state;
   int nout;
 };
@@ -188,6 +191,9 @@ cudaError_t launch_fold (const float* in, uint64_t in_span, uint64_t ndat, unsig
                          unsigned npol, const FoldView& fold, cudaStream_t stream);
 cudaError_t launch_binplan (const FoldSegment* segs, int nseg, uint64_t ndat, unsigned nbin,
                             uint32_t* out, cudaStream_t stream);
+// the profile column (segment base + bin, or 0xffffffff) of samples 0..ndat-1
+cudaError_t launch_colplan (const FoldSegment* segs, int nseg, uint64_t ndat, unsigned nbin,
+                            unsigned* cols, cudaStream_t st);
 // SampleDelay + detection + fold over voltages [chan][pol] (span values a row)
 cudaError_t launch_delay_fold (const float2* v, uint64_t span, const int* applied, uint64_t ndat,
                                unsigned nchan, unsigned npol, const FoldView& fv, cudaStream_t st,
