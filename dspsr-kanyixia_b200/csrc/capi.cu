@@ -394,6 +394,12 @@ struct dspsr_b200_fold
     return DSPSR_B200_OK;
   }
   // installs a plan built by the caller (segments over ndat samples)
+  // Plans go to the device on `up` when set (the stream that carries the
+  // block's own upload), else on the context's stream: an upload from host
+  // memory queued on the compute stream waits behind whatever host copies
+  // another stream has already given the copy engine.
+  cudaStream_t up = nullptr;
+  cudaEvent_t plan_ev = nullptr;
   int set_plan (std::vector<FoldSegment>& segs, uint64_t n)
   {
     plan.swap (segs);
@@ -426,9 +432,20 @@ struct dspsr_b200_fold
                 "cudaMalloc plan");
     std::memcpy (h_segs[cur], plan.data (), plan.size () * sizeof (FoldSegment));
     if (!plan.empty ())
+    {
       B200_CHECK (ctx, cudaMemcpyAsync (d_segs[cur].ptr, h_segs[cur],
                                         plan.size () * sizeof (FoldSegment),
-                                        cudaMemcpyHostToDevice, ctx->stream), "upload plan");
+                                        cudaMemcpyHostToDevice, up ? up : ctx->stream),
+                  "upload plan");
+      if (up)
+      {
+        if (!plan_ev)
+          B200_CHECK (ctx, cudaEventCreateWithFlags (&plan_ev, cudaEventDisableTiming),
+                      "cudaEventCreate");
+        B200_CHECK (ctx, cudaEventRecord (plan_ev, up), "record plan upload");
+        B200_CHECK (ctx, cudaStreamWaitEvent (ctx->stream, plan_ev, 0), "wait plan upload");
+      }
+    }
     if (use_cols && n && !plan.empty ())
     {
       // every ring slot grows at once, with headroom, so that steady blocks
@@ -472,6 +489,8 @@ struct dspsr_b200_fold
   {
     profiles.release ();
     hits.release ();
+    if (plan_ev) cudaEventDestroy (plan_ev);
+    plan_ev = nullptr;
     for (int i = 0; i < NRING; i++)
     {
       d_segs[i].release ();
@@ -2170,6 +2189,13 @@ int dspsr_b200_pipeline_run_host (dspsr_b200_pipeline* pl, const void* h_in, uin
     explicit PieceScope (dspsr_b200_pipeline* q) : p (q) { p->in_pieces = true; p->phase_continue = false; }
     ~PieceScope () { p->in_pieces = false; p->phase_continue = false; }
   } scope (pl);
+  // the pieces' fold plans follow the pieces on the copy stream
+  struct PlanStream
+  {
+    dspsr_b200_fold* f;
+    PlanStream (dspsr_b200_fold* g, cudaStream_t s) : f (g) { f->up = s; }
+    ~PlanStream () { f->up = nullptr; }
+  } plan_stream (&pl->fold, pl->copy_stream);
   for (uint64_t j = 0, off = 0; off < ndat || (ndat == 0 && j == 0); j++, off += piece)
   {
     const uint64_t n = std::min<uint64_t> (piece, ndat - off);
