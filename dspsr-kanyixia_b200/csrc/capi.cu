@@ -2171,14 +2171,17 @@ int dspsr_b200_pipeline_run_host (dspsr_b200_pipeline* pl, const void* h_in, uin
                   "create event");
     }
   }
-  // The block is uploaded in up to four pieces on a stream of its own, each
+  // The block is uploaded in up to eight pieces on a stream of its own, each
   // into one of two staging buffers, so that the upload of a piece overlaps
   // the kernels of the one before; the carried overlap joins the pieces as it
   // joins blocks.  Pieces are whole filterbank transforms.
   const uint64_t unit = pl->fb_nsub ? pl->fb_nsub : 1;
   const uint64_t min_piece = uint64_t (pl->conv.shape.nfft) * unit * 2;
   // (sub-integrations divide each block as a whole: no pieces)
-  const uint64_t npiece = pl->sub_on ? 1 : ndat >= 4 * min_piece ? 4 : ndat >= 2 * min_piece ? 2 : 1;
+  const uint64_t npiece = pl->sub_on ? 1
+                        : ndat >= 8 * min_piece ? 8
+                        : ndat >= 4 * min_piece ? 4
+                        : ndat >= 2 * min_piece ? 2 : 1;
   const uint64_t piece = ((ndat + npiece - 1) / npiece + unit - 1) / unit * unit;
   const uint64_t bps = pl->bytes_per_sample;
   uint64_t total = 0;
