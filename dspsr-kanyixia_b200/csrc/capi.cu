@@ -563,6 +563,7 @@ struct dspsr_b200_pipeline
   double rate = 0;                  // complex sampling rate of the convolved channels
   unsigned fb_nsub = 0;             // filterbank channels per input channel (0: none)
   bool fb_fused = false;            // filterbank computed inside the column pass
+  float lut_scale = 0.f;            // the 8-bit table as (x + 0.5) * scale, or 0
   // inter-channel dedispersion: SampleDelay between the convolution and the
   // fold, its voltages in sd_buf[sd_cur] (rows [chan][pol], sd_span values)
   bool sd_on = false;
@@ -919,6 +920,7 @@ int pipeline_block (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat_new
   in.npol = cfg.npol;
   in.offset_binary = cfg.offset_binary;
   in.fb_nsub = fbraw ? pl->fb_nsub : 0;
+  in.lut_scale = fbraw ? pl->lut_scale : 0.f;
 
   uint64_t npart = 0;
   if (ndat >= sh.nfft) npart = (ndat - nfilt) / sh.nkeep;   // Convolution.C:486-487
@@ -2050,6 +2052,7 @@ int dspsr_b200_pipeline_create (dspsr_b200_context* ctx, const dspsr_b200_pipeli
     cudaError_t e = cudaMemcpy (pl->conv.lut.ptr, cfg->lut, 256 * sizeof (float),
                                 cudaMemcpyHostToDevice);
     if (e != cudaSuccess) rc = cuda_fail (ctx, e, "upload lut");
+    pl->lut_scale = affine_lut_scale (cfg->lut);
   }
   // sub-integrations: Subint<Fold>::prepare hands the divider the folding
   // period for divisions in turns (Subint.h:230-242)

@@ -521,7 +521,7 @@ int dspsr_b200_dada_read (dspsr_b200_dada_file* file, uint64_t start_sample, uin
   // cache moves ~6 GB/s, below the host link the blocks go to next.
   constexpr uint64_t CHUNK_MIN = 16ull << 20;
   const unsigned hw = std::max (1u, std::thread::hardware_concurrency ());
-  const unsigned nthr = unsigned (std::min<uint64_t> ({8, hw, std::max<uint64_t> (1, want / CHUNK_MIN)}));
+  const unsigned nthr = unsigned (std::min<uint64_t> ({16, hw, std::max<uint64_t> (1, want / CHUNK_MIN)}));
   const uint64_t per = (want / nthr + 4095) / 4096 * 4096;
   std::vector<uint64_t> got (nthr, 0);
   std::vector<int> err (nthr, 0);

@@ -154,6 +154,20 @@ void interchannel_delays (double cf, double dm, double rate, const double* freq,
   }
 }
 
+float affine_lut_scale (const float* lut)
+{
+  // entry 0 is x = 0: 0.5f * s, so s = 2 * lut[0] exactly
+  const float s = 2.0f * lut[0];
+  if (!(s > 0.0f) || !std::isfinite (s)) return 0.0f;
+  for (int b = 0; b < 256; b++)
+  {
+    const float x = float (int8_t (uint8_t (b)));
+    const float v = (x + 0.5f) * s;
+    if (std::memcmp (&v, &lut[b], sizeof (float)) != 0) return 0.0f;
+  }
+  return s;
+}
+
 // Fold::get_phi with a constant period (Fold.C:685-693, 975-979):
 //   t   = start + (idat_start + 0.5) / rate          (MJD + seconds)
 //   phi = fmod((t - epoch) in seconds, P) / P - reference_phase

@@ -29,6 +29,10 @@ double channel_centre (double centre_frequency, double bandwidth, unsigned nchan
                        unsigned ichan, bool swap, bool dc_centred);
 int64_t optimal_fft_length (uint64_t nbad, uint64_t nfft_max, unsigned factor);
 void bittable8 (double spacing, bool twos_complement, float* lut, double* scale);
+// s when every entry of a two's-complement 8-bit table equals
+// (float(int8 x) + 0.5f) * s in float arithmetic (BitTable's tables do), so
+// that a kernel may compute the value instead of looking it up; else 0
+float affine_lut_scale (const float* lut256);
 double fold_phi (int64_t start_day, int64_t start_sec, double start_frac,
                  int64_t epoch_day, int64_t epoch_sec, double epoch_frac,
                  uint64_t idat_start, double rate, double period, double reference_phase);

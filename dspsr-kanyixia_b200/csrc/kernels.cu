@@ -364,7 +364,16 @@ constexpr size_t FBC_SMEM =
                                                                 : size_t (FBC_COLS) * FBC_XSTRIDE)
     * sizeof (float2);
 
-template <int KIND>
+// (float(x) + 0.5f) * scale for the two's-complement byte x, bit for bit:
+// 2^22 + (x + 128) has its last mantissa bit worth 0.5, so subtracting
+// 2^22 + 127.5 leaves x + 0.5 exactly; no int -> float conversion
+__device__ __forceinline__ float unpack_affine (unsigned byte, float scale)
+{
+  const float big = __int_as_float (0x4a800000u | (((byte & 0xffu) ^ 0x80u) << 1));
+  return __fmul_rn (__fsub_rn (big, 4194431.5f), scale);
+}
+
+template <int KIND, bool AFFINE>
 __device__ __forceinline__ void fetch_raw2 (const InputView& in, const float* s_lut, uint64_t r,
                                             float2& p0, float2& p1)
 {
@@ -377,8 +386,17 @@ __device__ __forceinline__ void fetch_raw2 (const InputView& in, const float* s_
   if constexpr (KIND == IN_INT8)
   {
     const unsigned w = __ldg (static_cast<const unsigned*> (base) + r);
-    p0 = make_float2 (s_lut[w & 0xff], s_lut[(w >> 8) & 0xff]);
-    p1 = make_float2 (s_lut[(w >> 16) & 0xff], s_lut[w >> 24]);
+    if constexpr (AFFINE)
+    {
+      const float sc = in.lut_scale;
+      p0 = make_float2 (unpack_affine (w, sc), unpack_affine (w >> 8, sc));
+      p1 = make_float2 (unpack_affine (w >> 16, sc), unpack_affine (w >> 24, sc));
+    }
+    else
+    {
+      p0 = make_float2 (s_lut[w & 0xff], s_lut[(w >> 8) & 0xff]);
+      p1 = make_float2 (s_lut[(w >> 16) & 0xff], s_lut[w >> 24]);
+    }
   }
   else
   {
@@ -397,7 +415,7 @@ __device__ __forceinline__ void fetch_raw2 (const InputView& in, const float* s_
   }
 }
 
-template <int KIND>
+template <int KIND, bool AFFINE>
 __global__ void __launch_bounds__ (FBC_THREADS, 512 / FBC_THREADS)
 k_fwd_cols_fb64 (const InputView in, const float* __restrict__ lut, const uint64_t nkeep,
                  const uint64_t part0, const unsigned n2, const float2* __restrict__ tw4,
@@ -406,7 +424,7 @@ k_fwd_cols_fb64 (const InputView in, const float* __restrict__ lut, const uint64
   extern __shared__ float2 s_fbc[];
   __shared__ float s_lut[256];
   __shared__ float2 s_tw64[64];
-  load_lut (in, lut, s_lut);
+  if (!AFFINE) load_lut (in, lut, s_lut);
   if (threadIdx.x < 64)
     s_tw64[threadIdx.x] = make_float2 (cos64 (int (threadIdx.x)), -sin64 (int (threadIdx.x)));
   __syncthreads ();
@@ -423,7 +441,7 @@ k_fwd_cols_fb64 (const InputView in, const float* __restrict__ lut, const uint64
   float2 x0[16], x1[16];
 #pragma unroll
   for (int m = 0; m < 16; m++)
-    fetch_raw2<KIND> (in, s_lut, t * 64 + q + 4 * m, x0[m], x1[m]);
+    fetch_raw2<KIND, AFFINE> (in, s_lut, t * 64 + q + 4 * m, x0[m], x1[m]);
   RegDFT<16, -1>::run (x0);
   RegDFT<16, -1>::run (x1);
   // twiddle w64^(q ka), then the quad exchange: column q ^ (ka >> 2)
@@ -1600,12 +1618,16 @@ cudaError_t run_fourstep_n1 (const ConvShape& sh, const ConvTables& tb, const In
       return cudaErrorInvalidValue;
     ClockScope cs (clk, KK_FWD_COLS, st);
     const dim3 g (sh.n2 / FBC_COLS, nbatch);
-    if (in.kind == IN_INT8)
-      k_fwd_cols_fb64<IN_INT8><<<g, FBC_THREADS, FBC_SMEM, st>>> (in, tb.lut, sh.nkeep, part0,
-                                                                   sh.n2, tb.tw4, scratch);
+    if (in.kind == IN_INT8 && in.lut_scale != 0.f)
+      k_fwd_cols_fb64<IN_INT8, true><<<g, FBC_THREADS, FBC_SMEM, st>>> (in, tb.lut, sh.nkeep, part0,
+                                                                         sh.n2, tb.tw4, scratch);
+    else if (in.kind == IN_INT8)
+      k_fwd_cols_fb64<IN_INT8, false><<<g, FBC_THREADS, FBC_SMEM, st>>> (in, tb.lut, sh.nkeep, part0,
+                                                                          sh.n2, tb.tw4, scratch);
     else
-      k_fwd_cols_fb64<IN_INT16><<<g, FBC_THREADS, FBC_SMEM, st>>> (in, tb.lut, sh.nkeep, part0,
-                                                                    sh.n2, tb.tw4, scratch);
+      k_fwd_cols_fb64<IN_INT16, false><<<g, FBC_THREADS, FBC_SMEM, st>>> (in, tb.lut, sh.nkeep,
+                                                                           part0, sh.n2, tb.tw4,
+                                                                           scratch);
   }
   else
   {
@@ -1809,10 +1831,13 @@ cudaError_t launch_convolution (const ConvShape& sh, const ConvTables& tb, const
     cudaError_t e = set_rows_smem<8192> ();
     if (e == cudaSuccess) e = set_rows_smem<4096> ();
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute (k_fwd_cols_fb64<IN_INT8>,
+      e = cudaFuncSetAttribute (k_fwd_cols_fb64<IN_INT8, false>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int (FBC_SMEM));
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute (k_fwd_cols_fb64<IN_INT16>,
+      e = cudaFuncSetAttribute (k_fwd_cols_fb64<IN_INT8, true>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, int (FBC_SMEM));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute (k_fwd_cols_fb64<IN_INT16, false>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int (FBC_SMEM));
     if (e != cudaSuccess) return e;
     attr_done |= 1u << dev;

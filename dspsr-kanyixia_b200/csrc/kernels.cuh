@@ -29,6 +29,10 @@ struct InputView
   // of 64 raw samples, npre_raw = 64 * npre.  0: the input holds the
   // convolution's channels.
   unsigned fb_nsub = 0;
+  // nonzero: the 8-bit table equals (float(x) + 0.5f) * lut_scale for every
+  // two's-complement x (BitTable's tables do), and the filterbank column pass
+  // computes the values instead of looking them up in shared memory
+  float lut_scale = 0.f;
 };
 
 // Fold / detection epilogue
