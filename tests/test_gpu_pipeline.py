@@ -455,10 +455,10 @@ def test_pipeline_dada_window_and_rejects(ctx, b2, tmp_path):
         pl.close()
 
 
-def run_subints(ctx, b2, blocks, cfg, td_kw, slots=0, pop=False, host=False):
+def run_subints(ctx, b2, blocks, cfg, td_kw, slots=0, pop=False, host=False, interchannel=0):
     """The pipeline with sub-integrations: closed divisions as (info, prof, hits)."""
     kw = dict(subint_seconds=td_kw.get("seconds", 0.0), subint_turns=td_kw.get("turns", 0.0),
-              subint_slots=slots)
+              subint_slots=slots, interchannel=interchannel)
     if "reference_epoch" in td_kw:
         kw["subint_epoch"] = td_kw["reference_epoch"]
     c = b2.make_config(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nchan"], cfg["npol"], cfg["nfft"],
@@ -688,3 +688,65 @@ def test_pipeline_interchannel_aligns_channels(ctx, b2):
     # the pulse is 0.03 x 256 = 7.7 bins wide: its peak bin wanders inside it
     assert spread(peaks(0)) > 20
     assert spread(peaks(1)) <= 5
+
+
+def oracle_interchannel_subints(orc, b2, raw_blocks, cfg, td_kw):
+    """-K and sub-integrations together: SampleDelay's outputs of each block
+    (starting zero_delay samples after the convolution's) are divided by
+    TimeDivide and folded range by range."""
+    delays = {}
+    y, nchan = oracle_voltages(orc, b2, raw_blocks, cfg, interchannel=delays)
+    rate = abs(cfg["bw"]) / nchan * 1e6
+    pps = (1.0 / rate) / cfg["period"]
+    nbin = cfg["nbin"]
+    nout = 4 if cfg["state"] in (2, 3) else (2 if cfg["state"] == 1 else 1)
+    td = orc.TimeDivideOracle(**td_kw)
+    subs, cur = [], None
+    tot, zero = delays["total_delay"], delays["zero_delay"]
+
+    def close():
+        nonlocal cur
+        if cur is not None and cur[2] > 0:
+            subs.append(tuple(cur))
+        cur = None
+
+    g0 = 0
+    for in0, n in block_outputs(b2, raw_blocks, cfg):
+        out = orc.sample_delay_block(y[:, :, g0:in0 + n], delays["applied"], tot)
+        m = out.shape[2]
+        if m == 0:
+            continue
+        d = orc.detect(np.ascontiguousarray(out), cfg["state"])
+        start = orc.mjd_add(START, (g0 + cfg["pos"] + zero) / rate)
+        for a in orc.subint_block_actions(td, start, m, rate):
+            if a[0] == "close":
+                close()
+                continue
+            _, i0, k, div = a[:4]
+            if cur is None:
+                cur = [div, g0 + i0, 0, np.zeros((nchan, nout, nbin), np.float32),
+                       np.zeros(nbin, np.uint32)]
+            phi = orc.fold_phi(START, EPOCH, g0 + cfg["pos"] + zero + i0, rate, cfg["period"])
+            plan = orc.fold_binplan(phi, pps, k, nbin)
+            orc.fold_accumulate(np.ascontiguousarray(d[:, :, i0:i0 + k]), plan, nbin, cur[3],
+                                cur[4])
+            cur[2] += k
+        g0 += m
+    close()
+    return subs
+
+
+def test_pipeline_interchannel_with_subints(ctx, b2, orc):
+    """-K, sub-integrations and host uploads in pieces at once (a 64-channel
+    filterbank computed in the column pass): every division against the
+    oracle."""
+    cfg = base_cfg(b2, dm=5.0, bw=256.0, fb=64, nfft=1 << 16, state=3, nbin=256,
+                   period=5.757e-3)
+    rng = np.random.default_rng(99)
+    nk = cfg["nfft"] - cfg["pos"] - cfg["neg"]
+    blocks = make_blocks(rng, cfg, [(cfg["nfft"] + 2 * nk + 77) * 64, (nk - 3) * 64,
+                                    (2 * nk + 999) * 64])
+    td = dict(seconds=0.02)
+    got = run_subints(ctx, b2, blocks, cfg, td, slots=8, host=True, interchannel=1)
+    want = oracle_interchannel_subints(orc, b2, blocks, cfg, td)
+    check_subints(got, want, cfg, abs(cfg["bw"]) / 64 * 1e6)
