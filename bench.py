@@ -88,7 +88,10 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
-def dist_init():
+def dist_init(backend="nccl"):
+    """One process per GPU (torchrun's RANK / WORLD_SIZE / LOCAL_RANK).  The
+    replicas share nothing but the barriers around the timed region and the
+    max over ranks of its duration; "gloo" runs the same plumbing on CPU."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -96,7 +99,7 @@ def dist_init():
         import datetime
         import torch.distributed as dist
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return world, rank, local
 
 
@@ -111,7 +114,8 @@ def max_over_ranks(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
