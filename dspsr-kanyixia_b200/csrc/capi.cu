@@ -1420,6 +1420,267 @@ int dspsr_b200_inverse_filterbank_status (dspsr_b200_inverse_filterbank* f)
   return DSPSR_B200_OK;
 }
 
+} // extern "C"
+
+// ---------------------------------------------------------------------------
+// filterbank with a response ("During")
+// ---------------------------------------------------------------------------
+
+struct dspsr_b200_filterbank_during
+{
+  dspsr_b200_context* ctx = nullptr;
+  DuringShape shape {};
+  DevBuf<float2> tw4, ptab, ptab_seg, twd, H, tmp, scratch;
+  DevBuf<double> chan_par;
+  bool have_response = false;
+  int nsm = 148;
+  unsigned max_batch = 1;
+
+  DuringTables tables () const
+  {
+    DuringTables t;
+    t.tw4 = tw4.ptr;
+    t.ptab = ptab.ptr;
+    t.ptab_seg = ptab_seg.ptr;
+    t.twd = twd.ptr;
+    t.H = H.ptr;
+    t.lut = ctx->d_lut;
+    t.nsm = nsm;
+    t.apod = nullptr;
+    return t;
+  }
+  void release ()
+  {
+    tw4.release ();
+    ptab.release ();
+    ptab_seg.release ();
+    twd.release ();
+    H.release ();
+    tmp.release ();
+    scratch.release ();
+    chan_par.release ();
+  }
+  int init (dspsr_b200_context* c, const dspsr_b200_fbd_config& cfg);
+};
+
+int dspsr_b200_filterbank_during::init (dspsr_b200_context* c, const dspsr_b200_fbd_config& cfg)
+{
+  ctx = c;
+  if (cfg.input_nchan == 0 || cfg.npol == 0 || cfg.npol > 2)
+    return fail (ctx, DSPSR_B200_EINVAL, "filterbank during: invalid channel or polarisation count");
+  if (!during_supported (cfg.nsub, cfg.freq_res))
+    return fail (ctx, DSPSR_B200_EINVAL,
+                 "filterbank during: nsub=%u freq_res=%u unsupported (nsub a power of two in "
+                 "[2, 128], freq_res a power of two, nsub*freq_res in [16384, 262144])",
+                 cfg.nsub, cfg.freq_res);
+  // Filterbank::do_prepare (Filterbank.C:155-196): nkeep = freq_res - nfilt_tot
+  if (uint64_t (cfg.nfilt_pos) + cfg.nfilt_neg >= cfg.freq_res)
+    return fail (ctx, DSPSR_B200_EINVAL, "filterbank during: freq_res=%u <= nfilt=%u",
+                 cfg.freq_res, cfg.nfilt_pos + cfg.nfilt_neg);
+  DuringShape& s = shape;
+  s.nchan_in = cfg.input_nchan;
+  s.npol = cfg.npol;
+  s.nsub = cfg.nsub;
+  s.freq_res = cfg.freq_res;
+  s.nfilt_pos = cfg.nfilt_pos;
+  s.nfilt_neg = cfg.nfilt_neg;
+  s.n2 = 8192;
+  s.n1 = unsigned (uint64_t (cfg.nsub) * cfg.freq_res / s.n2);
+  s.seg = s.n2 / cfg.nsub;
+  s.nkeep = cfg.freq_res - cfg.nfilt_pos - cfg.nfilt_neg;
+  s.in_step = uint64_t (cfg.nsub) * s.nkeep;
+  const uint64_t N = uint64_t (s.n1) * s.n2;
+  const std::vector<float2> t4 = make_tw4 (s.n1, s.n2);
+  const std::vector<float2> td = make_tw4 (s.n1, s.seg);
+  B200_CHECK (ctx, tw4.reserve (t4.size ()), "cudaMalloc tw4");
+  B200_CHECK (ctx, cudaMemcpy (tw4.ptr, t4.data (), t4.size () * sizeof (float2),
+                               cudaMemcpyHostToDevice), "copy tw4");
+  B200_CHECK (ctx, twd.reserve (td.size ()), "cudaMalloc channel twiddles");
+  B200_CHECK (ctx, cudaMemcpy (twd.ptr, td.data (), td.size () * sizeof (float2),
+                               cudaMemcpyHostToDevice), "copy channel twiddles");
+  for (int which = 0; which < 2; which++)
+  {
+    const unsigned n = which ? s.seg : s.n2;
+    DevBuf<float2>& dst = which ? ptab_seg : ptab;
+    const unsigned cnt = pass_tables_count (n);
+    std::vector<float2> pt (std::max (cnt, 1u), make_float2 (0.f, 0.f));
+    make_pass_tables (n, pt.data (), cnt);
+    B200_CHECK (ctx, dst.reserve (pt.size ()), "cudaMalloc pass tables");
+    B200_CHECK (ctx, cudaMemcpy (dst.ptr, pt.data (), pt.size () * sizeof (float2),
+                                 cudaMemcpyHostToDevice), "copy pass tables");
+  }
+  int dev = 0;
+  B200_CHECK (ctx, cudaGetDevice (&dev), "cudaGetDevice");
+  B200_CHECK (ctx, cudaDeviceGetAttribute (&nsm, cudaDevAttrMultiProcessorCount, dev),
+              "multiprocessor count");
+  const uint64_t per_part = uint64_t (s.nchan_in) * s.npol * N * sizeof (float2);
+  const uint64_t budget = cfg.scratch_bytes ? cfg.scratch_bytes : (uint64_t (512) << 20);
+  max_batch = unsigned (std::max<uint64_t> (1, std::min<uint64_t> (65535, budget / per_part)));
+  B200_CHECK (ctx, scratch.reserve (uint64_t (max_batch) * s.nchan_in * s.npol * N),
+              "cudaMalloc scratch");
+  B200_CHECK (ctx, H.reserve (uint64_t (s.nchan_in) * s.nsub * s.freq_res), "cudaMalloc response");
+  return DSPSR_B200_OK;
+}
+
+extern "C" {
+
+int dspsr_b200_filterbank_during_create (dspsr_b200_context* ctx, const dspsr_b200_fbd_config* cfg,
+                                         dspsr_b200_filterbank_during** out)
+{
+  if (!ctx || !cfg || !out) return DSPSR_B200_EINVAL;
+  *out = nullptr;
+  dspsr_b200_filterbank_during* f = new (std::nothrow) dspsr_b200_filterbank_during;
+  if (!f) return fail (ctx, DSPSR_B200_ENOMEM, "filterbank during: out of host memory");
+  const int rc = f->init (ctx, *cfg);
+  if (rc)
+  {
+    dspsr_b200_filterbank_during_destroy (f);
+    return rc;
+  }
+  *out = f;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_filterbank_during_destroy (dspsr_b200_filterbank_during* f)
+{
+  if (!f) return DSPSR_B200_EINVAL;
+  if (f->ctx) cudaStreamSynchronize (f->ctx->stream);
+  f->release ();
+  delete f;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_filterbank_during_info (dspsr_b200_filterbank_during* f, uint64_t* info)
+{
+  if (!f || !info) return DSPSR_B200_EINVAL;
+  const DuringShape& s = f->shape;
+  info[0] = uint64_t (s.nsub) * s.freq_res;
+  info[1] = s.in_step;
+  info[2] = uint64_t (s.nsub) * (s.nfilt_pos + s.nfilt_neg);
+  info[3] = s.nkeep;
+  info[4] = s.n1;
+  info[5] = f->max_batch;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_filterbank_during_copy_response (dspsr_b200_filterbank_during* f,
+                                                const float* response)
+{
+  if (!f) return DSPSR_B200_EINVAL;
+  dspsr_b200_context* ctx = f->ctx;
+  if (!response) return fail (ctx, DSPSR_B200_EINVAL, "copy_response: null response");
+  const DuringShape& s = f->shape;
+  const unsigned nchan = s.nchan_in * s.nsub;
+  const uint64_t n = uint64_t (nchan) * s.freq_res;
+  B200_CHECK (ctx, f->tmp.reserve (n), "cudaMalloc response staging");
+  B200_CHECK (ctx, cudaMemcpyAsync (f->tmp.ptr, response, n * sizeof (float2),
+                                    cudaMemcpyHostToDevice, ctx->stream), "upload response");
+  // bin k1 + n1*f2 of each channel to [chan][k1][f2]
+  B200_CHECK (ctx, launch_permute_response (f->H.ptr, f->tmp.ptr, nchan, s.n1, s.seg, ctx->stream),
+              "permute response");
+  B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "copy_response sync");
+  f->have_response = true;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_filterbank_during_set_dedispersion (dspsr_b200_filterbank_during* f, double cf,
+                                                   double bw, double dm, int swapped,
+                                                   int chirp_mode)
+{
+  if (!f) return DSPSR_B200_EINVAL;
+  dspsr_b200_context* ctx = f->ctx;
+  if (bw == 0 || !(cf > 0))
+    return fail (ctx, DSPSR_B200_EINVAL, "set_dedispersion: invalid frequency/bandwidth");
+  const DuringShape& s = f->shape;
+  const unsigned nchan = s.nchan_in * s.nsub;
+  // response channel j holds natural channel j, or channel (j + nchan/2) mod
+  // nchan after the whole response is swapped (half of nchan*freq_res points
+  // is nchan/2 whole channels)
+  std::vector<double> par (2 * nchan);
+  const double sign = bw / std::fabs (bw);
+  const double dispersion_per_MHz = 1e6 * dm / 2.41e-4;
+  for (unsigned j = 0; j < nchan; j++)
+  {
+    const double fr = channel_centre (cf, bw, nchan, j, swapped != 0, false);
+    if (!(fr > 0)) return fail (ctx, DSPSR_B200_EINVAL, "set_dedispersion: channel below 0 MHz");
+    par[j] = fr;
+    par[nchan + j] = -sign * 2 * M_PI * dispersion_per_MHz / (fr * fr);
+  }
+  const double chanwidth = bw / double (nchan);
+  const double binwidth = chanwidth / double (s.freq_res);
+  const float scale = float (1.0 / std::sqrt (double (s.nsub) * s.freq_res * double (s.freq_res)));
+  B200_CHECK (ctx, f->chan_par.reserve (2 * nchan), "cudaMalloc channel table");
+  B200_CHECK (ctx, cudaMemcpyAsync (f->chan_par.ptr, par.data (), par.size () * sizeof (double),
+                                    cudaMemcpyHostToDevice, ctx->stream), "upload channels");
+  B200_CHECK (ctx, launch_build_chirp (f->H.ptr, f->chan_par.ptr, f->chan_par.ptr + nchan, nullptr,
+                                       nchan, s.freq_res, s.n1, s.seg, binwidth, 0.5 * chanwidth,
+                                       0, chirp_mode, scale, ctx->stream),
+              "build chirp");
+  B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "set_dedispersion sync");
+  f->have_response = true;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_filterbank_during_get_response (dspsr_b200_filterbank_during* f, float* response)
+{
+  if (!f) return DSPSR_B200_EINVAL;
+  dspsr_b200_context* ctx = f->ctx;
+  if (!response) return fail (ctx, DSPSR_B200_EINVAL, "get_response: null pointer");
+  const DuringShape& s = f->shape;
+  const unsigned nchan = s.nchan_in * s.nsub;
+  const uint64_t n = uint64_t (nchan) * s.freq_res;
+  B200_CHECK (ctx, f->tmp.reserve (n), "cudaMalloc response staging");
+  B200_CHECK (ctx, launch_unpermute_response (f->tmp.ptr, f->H.ptr, nchan, s.n1, s.seg,
+                                              ctx->stream), "unpermute response");
+  B200_CHECK (ctx, cudaMemcpyAsync (response, f->tmp.ptr, n * sizeof (float2),
+                                    cudaMemcpyDeviceToHost, ctx->stream), "download response");
+  B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "get_response sync");
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_filterbank_during_perform (dspsr_b200_filterbank_during* f, int input_kind,
+                                          const void* d_in, uint64_t ndat, uint64_t in_span,
+                                          const float* lut256, int offset_binary, float* d_out,
+                                          uint64_t out_span, uint64_t* npart_out)
+{
+  if (!f) return DSPSR_B200_EINVAL;
+  dspsr_b200_context* ctx = f->ctx;
+  if (npart_out) *npart_out = 0;
+  if (!f->have_response) return fail (ctx, DSPSR_B200_ESTATE, "filterbank during: no response set");
+  if (!d_in || !d_out) return fail (ctx, DSPSR_B200_EINVAL, "filterbank during: null buffer");
+  if (input_kind < 0 || input_kind > 2 || (input_kind == DSPSR_B200_INT8_TFPD && !lut256))
+    return fail (ctx, DSPSR_B200_EINVAL, "filterbank during: invalid input kind or missing table");
+  if (input_kind == DSPSR_B200_FLOAT_FPT && in_span < ndat)
+    return fail (ctx, DSPSR_B200_EINVAL, "filterbank during: in_span < ndat");
+  const DuringShape& s = f->shape;
+  // Filterbank::resize_output (Filterbank.C:398-420)
+  const uint64_t overlap = uint64_t (s.nsub) * (s.nfilt_pos + s.nfilt_neg);
+  const uint64_t npart = ndat > overlap ? (ndat - overlap) / s.in_step : 0;
+  if (out_span < npart * s.nkeep)
+    return fail (ctx, DSPSR_B200_EINVAL, "filterbank during: out_span < npart * nkeep");
+  if (input_kind == DSPSR_B200_INT8_TFPD)
+    B200_CHECK (ctx, cudaMemcpyAsync (ctx->d_lut, lut256, 256 * sizeof (float),
+                                      cudaMemcpyHostToDevice, ctx->stream), "upload lut");
+  InputView in {};
+  in.kind = input_kind;
+  in.main = d_in;
+  in.main_span = in_span;
+  in.nchan = s.nchan_in;
+  in.npol = s.npol;
+  in.offset_binary = offset_binary;
+  VoltView vv {reinterpret_cast<float2*> (d_out), out_span};
+  FoldView fv {};
+  const DuringTables tb = f->tables ();
+  for (uint64_t p0 = 0; p0 < npart; p0 += f->max_batch)
+  {
+    const unsigned nb = unsigned (std::min<uint64_t> (f->max_batch, npart - p0));
+    B200_CHECK (ctx, launch_filterbank_during (s, tb, in, p0, nb, f->scratch.ptr, OUT_VOLTAGE, fv,
+                                               vv, ctx->stream), "filterbank during kernels");
+  }
+  if (npart_out) *npart_out = npart;
+  return DSPSR_B200_OK;
+}
+
 int dspsr_b200_apodization (int type, unsigned ndat, unsigned transition_start,
                             unsigned transition_end, int swap_halves, float* window)
 {

@@ -1084,6 +1084,166 @@ k_ifb_cols (const float2* __restrict__ scratch, const IfbShape sh, const float2*
 }
 
 // --------------------------------------------------------------------------
+// Filterbank with a response ("During")
+// --------------------------------------------------------------------------
+
+// One radix pass of an N-point transform run by the stockham_threads(N)
+// threads of one group (lane = index in the group), both sides in the padded
+// layout relative to the group's base, or the output unpadded (PO false).
+// Every thread of the block calls it: the barriers are block-wide.
+template <int N, int D, int P, bool PO>
+__device__ __forceinline__ void gpass (int lane, const float2* src, float2* dst, float2* v,
+                                       const float2* tab)
+{
+  if constexpr (P < stockham_npass (N))
+  {
+    constexpr int T = stockham_threads (N);
+    constexpr int R = stockham_radix (N, P);
+    constexpr int Ns = stockham_ns (N, P);
+    StockhamPassT<N, R, T, D, true, PO>::load (lane, src, v);
+    __syncthreads ();
+    StockhamPassT<N, R, T, D, true, PO>::compute_store (
+        lane, Ns, v, dst, P ? tab + pass_table_offset (N, P) : nullptr);
+    __syncthreads ();
+  }
+}
+
+constexpr int DUR_N2 = 8192;
+
+template <int SEG>
+constexpr size_t during_rows_smem ()
+{
+  return size_t (spad_size (DUR_N2) + pass_tables_size (DUR_N2) + pass_tables_size (SEG))
+         * sizeof (float2);
+}
+
+// Rows of the big transform (persistent CTAs, one row at a time): the
+// forward n2-point FFT, the response of each output channel on its segment
+// (Response::operate over nchan_subband channels from input_ichan*nchan_subband,
+// FilterbankEngineCPU.C:480-484), then the seg-point inverse FFT of every
+// segment, written back in place.  Row r of the scratch is row k1 = r mod n1
+// of (part, input channel, pol).
+template <int SEG>
+__global__ void __launch_bounds__ (stockham_threads (DUR_N2), 1)
+k_rows_during (float2* __restrict__ scratch, const float2* __restrict__ ptab,
+               const float2* __restrict__ ptab_seg, const float2* __restrict__ H,
+               const unsigned n1, const unsigned nsub, const unsigned npol,
+               const unsigned nchan_in, const unsigned nrows)
+{
+  constexpr int N2 = DUR_N2;
+  constexpr int T = stockham_threads (N2);
+  constexpr int TABN = pass_tables_size (N2);
+  constexpr int TABS = pass_tables_size (SEG);
+  constexpr int TS = stockham_threads (SEG);
+  constexpr int NPS = stockham_npass (SEG);
+  static_assert (stockham_npass (N2) == 4, "row schedule of 8192 points has four passes");
+  static_assert (NPS == 2 || NPS == 3, "segment transforms of 64 .. 4096 points");
+  static_assert (T % TS == 0, "segments tile the block");
+  extern __shared__ __align__ (16) float2 s_dur[];
+  float2* work = s_dur;
+  float2* tab = work + spad_size (N2);
+  float2* tabs = tab + TABN;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < TABN; i += T) tab[i] = __ldg (ptab + i);
+  for (int i = tid; i < TABS; i += T) tabs[i] = __ldg (ptab_seg + i);
+  __syncthreads ();
+  // group g transforms segment g; spad(g*SEG + i) = spad(g*SEG) + spad(i)
+  // because SEG is a multiple of 16
+  const int g = tid / TS, lane = tid % TS;
+  float2* wseg = work + spad (g * SEG);
+  float2 v[16];
+  for (unsigned row = blockIdx.x; row < nrows; row += gridDim.x)
+  {
+    const unsigned k1 = row % n1;
+    const unsigned cin = (row / n1 / npol) % nchan_in;
+    float2* grow = scratch + uint64_t (row) * N2;
+    tpass<N2, -1, 0, false, true> (grow, work, v, tab);
+    tpass<N2, -1, 1, true, true> (work, work, v, tab);
+    tpass<N2, -1, 2, true, true> (work, work, v, tab);
+    tpass<N2, -1, 3, true, true> (work, work, v, tab);
+    // position i = cs*SEG + f2 of row k1 is bin k1 + n1*f2 of output channel
+    // cin*nsub + cs: (f_r d_r - f_i d_i, f_i d_r + f_r d_i), Response.C:662-726
+#pragma unroll
+    for (int m = 0; m < 16; m++)
+    {
+      const int i = tid + m * T;
+      const unsigned cs = unsigned (i) / SEG, f2 = unsigned (i) % SEG;
+      const float2 f = __ldg (H + ((uint64_t (cin) * nsub + cs) * n1 + k1) * SEG + f2);
+      const float2 d = work[spad (i)];
+      work[spad (i)] = make_float2 (d.x * f.x - d.y * f.y, d.x * f.y + d.y * f.x);
+    }
+    __syncthreads ();
+    float2* gseg = grow + g * SEG;
+    if constexpr (NPS == 2)
+    {
+      gpass<SEG, +1, 0, true> (lane, wseg, wseg, v, tabs);
+      gpass<SEG, +1, 1, false> (lane, wseg, gseg, v, tabs);
+    }
+    else
+    {
+      gpass<SEG, +1, 0, true> (lane, wseg, wseg, v, tabs);
+      gpass<SEG, +1, 1, true> (lane, wseg, wseg, v, tabs);
+      gpass<SEG, +1, 2, false> (lane, wseg, gseg, v, tabs);
+    }
+  }
+}
+
+// Inverse column DFTs of the freq_res-point transforms: thread i2 holds
+// sample t2 = i2 mod seg of output channel cin*nsub + i2/seg; conjugate
+// twiddle exp(+2 pi i k1 t2 / freq_res), n1-point inverse DFT giving samples
+// t2 + seg*t1, then the discard of nfilt_pos / nfilt_neg
+// (FilterbankEngineCPU.C:516-523) and voltages out, or detection + fold.
+// seg >= 64, so the 32 lanes of a warp share one output channel.
+template <int N1, int NPOL, int MODE, int NOUT>
+__global__ void __launch_bounds__ (128, 4)
+k_inv_cols_during (const float2* __restrict__ scratch, const DuringShape sh, const uint64_t part0,
+                   const float2* __restrict__ twd, const FoldView fv, const VoltView vv)
+{
+  const unsigned i2 = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned b = blockIdx.y;
+  const unsigned cin = blockIdx.z;
+  const uint64_t N = uint64_t (N1) * sh.n2;
+  const unsigned cs = i2 / sh.seg, t2 = i2 % sh.seg;
+  const unsigned c = cin * sh.nsub + cs;
+  float2 w[N1];
+#pragma unroll
+  for (int k = 1; k < N1; k++)
+    w[k] = __ldg (twd + uint64_t (k) * sh.seg + t2);
+  float2 v[NPOL][N1];
+#pragma unroll
+  for (int p = 0; p < NPOL; p++)
+  {
+    const float2* src = scratch + ((uint64_t (b) * sh.nchan_in + cin) * NPOL + p) * N + i2;
+#pragma unroll
+    for (int k = 0; k < N1; k++)
+      v[p][k] = src[uint64_t (k) * sh.n2];
+#pragma unroll
+    for (int k = 1; k < N1; k++)
+      v[p][k] = cmulc (v[p][k], w[k]);
+    RegDFT<N1, +1>::run (v[p]);
+  }
+  const uint64_t tbase = (part0 + b) * sh.nkeep;
+#pragma unroll
+  for (int k = 0; k < N1; k++)
+  {
+    const uint64_t tl = uint64_t (k) * sh.seg + t2;
+    const bool ok = tl >= sh.nfilt_pos && tl < sh.nfilt_pos + sh.nkeep;
+    const uint64_t t = tbase + (tl - sh.nfilt_pos);
+    if constexpr (MODE == OUT_VOLTAGE)
+    {
+      if (ok)
+      {
+#pragma unroll
+        for (int p = 0; p < NPOL; p++)
+          vv.out[(uint64_t (c) * NPOL + p) * vv.span + t] = v[p][k];
+      }
+    }
+    else
+      emit_fold<NOUT> (fv, c, NPOL, ok, t, v[0][k], v[NPOL - 1][k]);
+  }
+}
+
+// --------------------------------------------------------------------------
 // response construction
 // --------------------------------------------------------------------------
 
@@ -1849,6 +2009,122 @@ cudaError_t launch_convolution (const ConvShape& sh, const ConvTables& tb, const
     case 8: return run_fourstep_n1<8> (sh, tb, in, part0, nbatch, scratch, mode, fv, vv, st, clk);
     case 16: return run_fourstep_n1<16> (sh, tb, in, part0, nbatch, scratch, mode, fv, vv, st, clk);
     case 32: return run_fourstep_n1<32> (sh, tb, in, part0, nbatch, scratch, mode, fv, vv, st, clk);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+namespace {
+
+template <int SEG>
+cudaError_t launch_rows_during (unsigned nrows, float2* scratch, const DuringShape& sh,
+                                const DuringTables& tb, cudaStream_t st)
+{
+  constexpr size_t smem = during_rows_smem<SEG> ();
+  static_assert (smem <= 227u * 1024u, "row kernel shared memory");
+  cudaError_t e = cudaFuncSetAttribute (k_rows_during<SEG>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, int (smem));
+  if (e != cudaSuccess) return e;
+  const unsigned grid = std::min<unsigned> (nrows, unsigned (tb.nsm));
+  k_rows_during<SEG><<<grid, stockham_threads (DUR_N2), smem, st>>> (
+      scratch, tb.ptab, tb.ptab_seg, tb.H, sh.n1, sh.nsub, sh.npol, sh.nchan_in, nrows);
+  return cudaSuccess;
+}
+
+template <int N1, int NPOL, int MODE, int NOUT>
+void launch_inv_during (const DuringShape& sh, dim3 grid, const float2* scratch, uint64_t part0,
+                        const DuringTables& tb, const FoldView& fv, const VoltView& vv,
+                        cudaStream_t st)
+{
+  k_inv_cols_during<N1, NPOL, MODE, NOUT><<<grid, 128, 0, st>>> (scratch, sh, part0, tb.twd, fv,
+                                                                 vv);
+}
+
+template <int N1, int NPOL>
+void launch_inv_during_m (const DuringShape& sh, dim3 grid, const float2* scratch,
+                          uint64_t part0, const DuringTables& tb, int mode, const FoldView& fv,
+                          const VoltView& vv, cudaStream_t st)
+{
+  if (mode == OUT_VOLTAGE)
+    launch_inv_during<N1, NPOL, OUT_VOLTAGE, 1> (sh, grid, scratch, part0, tb, fv, vv, st);
+  else if (NPOL == 1 || fv.nout == 1)
+    launch_inv_during<N1, NPOL, OUT_FOLD, 1> (sh, grid, scratch, part0, tb, fv, vv, st);
+  else if (fv.nout == 2)
+    launch_inv_during<N1, NPOL, OUT_FOLD, 2> (sh, grid, scratch, part0, tb, fv, vv, st);
+  else
+    launch_inv_during<N1, NPOL, OUT_FOLD, 4> (sh, grid, scratch, part0, tb, fv, vv, st);
+}
+
+template <int N1>
+cudaError_t run_during_n1 (const DuringShape& sh, const DuringTables& tb, const InputView& in,
+                           uint64_t part0, unsigned nbatch, float2* scratch, int mode,
+                           const FoldView& fv, const VoltView& vv, cudaStream_t st,
+                           const KernelClock* clk)
+{
+  const dim3 gcol (sh.n2 / 128, nbatch, sh.nchan_in);
+  {
+    ClockScope cs (clk, KK_FWD_COLS, st);
+    if (in.kind == IN_INT8)
+      k_fwd_cols<N1, IN_INT8><<<gcol, 128, 0, st>>> (in, tb.lut, sh.in_step, part0, sh.n2, tb.tw4,
+                                                     scratch, tb.apod);
+    else if (in.kind == IN_INT16)
+      k_fwd_cols<N1, IN_INT16><<<gcol, 128, 0, st>>> (in, tb.lut, sh.in_step, part0, sh.n2,
+                                                      tb.tw4, scratch, tb.apod);
+    else
+      k_fwd_cols<N1, IN_FLOAT><<<gcol, 128, 0, st>>> (in, tb.lut, sh.in_step, part0, sh.n2,
+                                                      tb.tw4, scratch, tb.apod);
+  }
+  const unsigned nrows = N1 * nbatch * sh.nchan_in * sh.npol;
+  cudaError_t e = cudaSuccess;
+  {
+    ClockScope cs (clk, KK_ROWS, st);
+    switch (sh.seg)
+    {
+      case 64: e = launch_rows_during<64> (nrows, scratch, sh, tb, st); break;
+      case 128: e = launch_rows_during<128> (nrows, scratch, sh, tb, st); break;
+      case 256: e = launch_rows_during<256> (nrows, scratch, sh, tb, st); break;
+      case 512: e = launch_rows_during<512> (nrows, scratch, sh, tb, st); break;
+      case 1024: e = launch_rows_during<1024> (nrows, scratch, sh, tb, st); break;
+      case 2048: e = launch_rows_during<2048> (nrows, scratch, sh, tb, st); break;
+      case 4096: e = launch_rows_during<4096> (nrows, scratch, sh, tb, st); break;
+      default: return cudaErrorInvalidValue;
+    }
+  }
+  if (e != cudaSuccess) return e;
+  ClockScope cs (clk, KK_INV_COLS, st);
+  if (sh.npol == 2)
+    launch_inv_during_m<N1, 2> (sh, gcol, scratch, part0, tb, mode, fv, vv, st);
+  else
+    launch_inv_during_m<N1, 1> (sh, gcol, scratch, part0, tb, mode, fv, vv, st);
+  return cudaGetLastError ();
+}
+
+} // namespace
+
+bool during_supported (unsigned nsub, unsigned freq_res)
+{
+  if (nsub < 2 || nsub > 128 || (nsub & (nsub - 1))) return false;
+  const uint64_t n = uint64_t (nsub) * freq_res;
+  return freq_res && (freq_res & (freq_res - 1)) == 0 && n >= 2 * DUR_N2 && n <= 32 * DUR_N2;
+}
+
+cudaError_t launch_filterbank_during (const DuringShape& sh, const DuringTables& tb,
+                                      const InputView& in, uint64_t part0, unsigned nbatch,
+                                      float2* scratch, int mode, const FoldView& fv,
+                                      const VoltView& vv, cudaStream_t st,
+                                      const KernelClock* clk)
+{
+  if (nbatch == 0) return cudaSuccess;
+  if (!during_supported (sh.nsub, sh.freq_res) || sh.n2 != unsigned (DUR_N2)
+      || uint64_t (sh.n1) * sh.n2 != uint64_t (sh.nsub) * sh.freq_res || sh.seg * sh.nsub != sh.n2
+      || sh.npol < 1 || sh.npol > 2 || in.fb_nsub)
+    return cudaErrorInvalidValue;
+  switch (sh.n1)
+  {
+    case 2: return run_during_n1<2> (sh, tb, in, part0, nbatch, scratch, mode, fv, vv, st, clk);
+    case 4: return run_during_n1<4> (sh, tb, in, part0, nbatch, scratch, mode, fv, vv, st, clk);
+    case 8: return run_during_n1<8> (sh, tb, in, part0, nbatch, scratch, mode, fv, vv, st, clk);
+    case 16: return run_during_n1<16> (sh, tb, in, part0, nbatch, scratch, mode, fv, vv, st, clk);
+    case 32: return run_during_n1<32> (sh, tb, in, part0, nbatch, scratch, mode, fv, vv, st, clk);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -170,6 +170,46 @@ cudaError_t launch_inverse_filterbank (const IfbShape& shape, const IfbTables& t
                                        const KernelClock* clock = nullptr);
 bool ifb_supported_lin (unsigned lin);
 
+// Filterbank with a response (the "During" form, -F nchan:D:
+// FilterbankEngineCPU.C:379-535 with Response::operate over the channels of
+// the big spectrum): per part one nsub*freq_res-point forward FFT of every
+// input channel, split as n1 x n2 (n2 = 8192); the response; then one inverse
+// FFT of freq_res = n1*seg points per output channel, seg = n2/nsub.  In the
+// four-step order of the big spectrum output channel cs of an input channel is
+// the contiguous range [cs*seg, (cs+1)*seg) of every row, so its inverse
+// transform is itself a four-step transform: seg-point inverse FFTs inside the
+// row kernel, then n1-point inverse DFTs across the rows.
+struct DuringShape
+{
+  unsigned nchan_in, npol, nsub;
+  unsigned n1, n2, seg;          // nsub * freq_res = n1 * n2, seg = n2 / nsub
+  unsigned freq_res, nfilt_pos, nfilt_neg;
+  uint64_t nkeep;                // freq_res - nfilt_pos - nfilt_neg
+  uint64_t in_step;              // nsub * nkeep input samples between parts
+};
+
+struct DuringTables
+{
+  const float2* tw4;       // [n1][n2] exp(-2 pi i k1 m / (n1 n2))
+  const float2* ptab;      // per-pass tables of the n2-point FFT
+  const float2* ptab_seg;  // per-pass tables of the seg-point FFT
+  const float2* twd;       // [n1][seg] exp(-2 pi i k1 t2 / freq_res)
+  const float2* H;         // [nchan_in*nsub][n1][seg]: bin k1 + n1*f2 of each channel
+  const float* lut;        // 8-bit table for int8 input
+  int nsm;
+  const float* apod;       // temporal window of n1*n2 points, or null
+};
+
+bool during_supported (unsigned nsub, unsigned freq_res);
+// Parts [part0, part0 + nbatch); scratch holds nbatch*nchan_in*npol*n1*n2
+// values.  mode OUT_VOLTAGE writes the output channels (chan*npol + pol)*span;
+// OUT_FOLD detects and folds them (fold.nout products).
+cudaError_t launch_filterbank_during (const DuringShape& shape, const DuringTables& tables,
+                                      const InputView& in, uint64_t part0, unsigned nbatch,
+                                      float2* scratch, int mode, const FoldView& fold,
+                                      const VoltView& out, cudaStream_t stream,
+                                      const KernelClock* clock = nullptr);
+
 // SpectralKurtosis (one resolution, noverlap 1): statistics, test and masked
 // copy (out may equal in: then only zapped blocks are written).  sums
 // [npart][nchan][npol][2], counts and mask [npart][nchan] are optional.

@@ -23,7 +23,7 @@ from . import _capi
 from ._capi import (B200Error, PipelineConfig, INTENSITY, PPQQ, COHERENCE, STOKES, INT8_TFPD,
                     INT16_TFPD, FLOAT_FPT, CHIRP_REFERENCE, CHIRP_FP64)
 
-__all__ = ["Context", "Convolution", "InverseFilterbank", "Fold", "apodization", "Pipeline", "PipelineConfig", "B200Error",
+__all__ = ["Context", "Convolution", "InverseFilterbank", "FilterbankDuring", "Fold", "apodization", "Pipeline", "PipelineConfig", "B200Error",
            "smearing_samples", "minimum_ndat", "optimal_fft_length", "bittable8", "fold_phi",
            "sk_limits", "DADAFile", "dada_parse", "dada_is_valid", "ascii_header_get",
            "ascii_header_set", "write_dada", "TimeDivide", "interchannel_delays",
@@ -359,6 +359,72 @@ class InverseFilterbank:
     def close(self):
         if self.handle:
             self._lib.dspsr_b200_inverse_filterbank_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class FilterbankDuring:
+    """Filterbank::Engine with a response (the "During" filterbank, -F nchan:D):
+    one nsub*freq_res-point FFT per part, the response, then a freq_res-point
+    inverse FFT per output channel (FilterbankEngineCPU.C:379-535)."""
+
+    INFO = ("nsamp_fft", "nsamp_step", "nsamp_overlap", "nkeep", "n1", "max_batch")
+
+    def __init__(self, ctx, input_nchan, npol, nsub, freq_res, nfilt=(0, 0), scratch_bytes=0):
+        self.ctx = ctx
+        self._lib = ctx._lib
+        cfg = _capi.FbdConfig(input_nchan, npol, nsub, freq_res, nfilt[0], nfilt[1],
+                              scratch_bytes)
+        h = ctypes.c_void_p()
+        ctx.check(self._lib.dspsr_b200_filterbank_during_create(ctx.handle, ctypes.byref(cfg),
+                                                                ctypes.byref(h)),
+                  "filterbank_during_create")
+        self.handle = h
+        ctx._adopt(self)
+        info = (ctypes.c_uint64 * 6)()
+        ctx.check(self._lib.dspsr_b200_filterbank_during_info(h, info), "filterbank_during_info")
+        self.info = dict(zip(self.INFO, list(info)))
+        self.nin, self.npol, self.nsub, self.freq_res = input_nchan, npol, nsub, freq_res
+        self.nchan = input_nchan * nsub
+
+    def copy_response(self, response):
+        r = np.ascontiguousarray(response, np.complex64)
+        assert r.size == self.nchan * self.freq_res
+        self.ctx.check(self._lib.dspsr_b200_filterbank_during_copy_response(
+            self.handle, _fptr(r.view(np.float32))), "copy_response")
+
+    def set_dedispersion(self, centre_freq, bandwidth, dm, swapped=True, chirp_mode=0):
+        self.ctx.check(self._lib.dspsr_b200_filterbank_during_set_dedispersion(
+            self.handle, centre_freq, bandwidth, dm, int(swapped), chirp_mode), "set_dedispersion")
+
+    def get_response(self):
+        out = np.empty(self.nchan * self.freq_res, np.complex64)
+        self.ctx.check(self._lib.dspsr_b200_filterbank_during_get_response(
+            self.handle, _fptr(out.view(np.float32))), "get_response")
+        return out.reshape(self.nchan, self.freq_res)
+
+    def npart(self, ndat):
+        o = self.info["nsamp_overlap"]
+        return (ndat - o) // self.info["nsamp_step"] if ndat > o else 0
+
+    def perform(self, d_in, ndat, d_out, out_span, input_kind=FLOAT_FPT, in_span=None, lut=None,
+                offset_binary=False):
+        n = ctypes.c_uint64()
+        lp = _fptr(np.ascontiguousarray(lut, np.float32)) if lut is not None else None
+        self.ctx.check(self._lib.dspsr_b200_filterbank_during_perform(
+            self.handle, input_kind, _ptr(d_in), ndat, ndat if in_span is None else in_span, lp,
+            int(offset_binary), _ptr(d_out), out_span, ctypes.byref(n)),
+            "filterbank_during_perform")
+        return n.value
+
+    def close(self):
+        if self.handle:
+            self._lib.dspsr_b200_filterbank_during_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

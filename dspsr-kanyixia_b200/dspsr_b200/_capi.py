@@ -108,6 +108,19 @@ UNLOAD_FN = ctypes.CFUNCTYPE(None, c_vp, ctypes.POINTER(Subint), ctypes.POINTER(
 SUBINT_FOLD, SUBINT_CLOSE_PARTIAL, SUBINT_CLOSE_COMPLETE = 0, 1, 2
 
 
+class FbdConfig(ctypes.Structure):
+    """dspsr_b200_fbd_config"""
+    _fields_ = [
+        ("input_nchan", c_uint),
+        ("npol", c_uint),
+        ("nsub", c_uint),
+        ("freq_res", c_uint),
+        ("nfilt_pos", c_uint),
+        ("nfilt_neg", c_uint),
+        ("scratch_bytes", ctypes.c_uint64),
+    ]
+
+
 class IfbConfig(ctypes.Structure):
     """dspsr_b200_ifb_config"""
     _fields_ = [
@@ -205,6 +218,16 @@ SIGNATURES = {
     "dspsr_b200_inverse_filterbank_perform": (c_int, [c_vp, c_int, c_vp, c_u64, c_u64, c_fp, c_int,
                                                       c_vp, c_u64, c_u64p]),
     "dspsr_b200_inverse_filterbank_status": (c_int, [c_vp]),
+    "dspsr_b200_filterbank_during_create": (c_int, [c_vp, ctypes.POINTER(FbdConfig),
+                                                    ctypes.POINTER(c_vp)]),
+    "dspsr_b200_filterbank_during_destroy": (c_int, [c_vp]),
+    "dspsr_b200_filterbank_during_info": (c_int, [c_vp, c_u64p]),
+    "dspsr_b200_filterbank_during_copy_response": (c_int, [c_vp, c_fp]),
+    "dspsr_b200_filterbank_during_set_dedispersion": (c_int, [c_vp, c_dbl, c_dbl, c_dbl,
+                                                              c_int, c_int]),
+    "dspsr_b200_filterbank_during_get_response": (c_int, [c_vp, c_fp]),
+    "dspsr_b200_filterbank_during_perform": (c_int, [c_vp, c_int, c_vp, c_u64, c_u64, c_fp, c_int,
+                                                     c_vp, c_u64, c_u64p]),
     "dspsr_b200_apodization": (c_int, [c_int, c_uint, c_uint, c_uint, c_int, c_fp]),
     "dspsr_b200_sk": (c_int, [c_vp, c_vp, c_u64, c_u64, c_uint, c_uint, c_uint, c_int, c_uint,
                               ctypes.c_float, ctypes.c_float, c_vp, c_u64, c_vp, c_vp, c_vp, c_vp,

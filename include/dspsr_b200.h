@@ -313,6 +313,68 @@ int dspsr_b200_inverse_filterbank_perform (dspsr_b200_inverse_filterbank* ifb, i
 int dspsr_b200_inverse_filterbank_status (dspsr_b200_inverse_filterbank* ifb);
 
 /* ---------------------------------------------------------------------- */
+/* Filterbank::Engine with a response: the "During" filterbank (-F N:D;     */
+/* Filterbank::do_prepare with a response, Filterbank.C:98-198;             */
+/* FilterbankEngineCPU::perform, FilterbankEngineCPU.C:379-535;             */
+/* CUDA::FilterbankEngine::perform, FilterbankEngineCUDA.cu:353-480)        */
+/* ---------------------------------------------------------------------- */
+
+/* Each part of nsamp_fft = nsub * freq_res input samples of every input
+   channel is transformed forward, multiplied by the response of its nsub
+   output channels (channel cin*nsub + k takes bins [k*freq_res,
+   (k+1)*freq_res) of the FFT-order spectrum), and each output channel is
+   transformed back in freq_res points, of which nkeep = freq_res - nfilt_pos
+   - nfilt_neg from nfilt_pos are kept.  Parts start nsamp_step = nsub * nkeep
+   input samples apart; npart = (ndat - nsub*(nfilt_pos+nfilt_neg)) /
+   nsamp_step (Filterbank::resize_output, Filterbank.C:398-420).  Supported:
+   nsub a power of two in [2, 128], freq_res a power of two, nsub * freq_res
+   in [16384, 262144]. */
+typedef struct dspsr_b200_filterbank_during dspsr_b200_filterbank_during;
+typedef struct dspsr_b200_fbd_config
+{
+  unsigned input_nchan;
+  unsigned npol;
+  unsigned nsub;            /* output channels per input channel (nchan_subband) */
+  unsigned freq_res;        /* points per output channel: the response's ndat */
+  unsigned nfilt_pos, nfilt_neg;
+  uint64_t scratch_bytes;   /* device scratch bound, 0 = 512 MiB */
+} dspsr_b200_fbd_config;
+
+/* Engine::setup (FilterbankEngineCUDA.cu:62-150) */
+int dspsr_b200_filterbank_during_create (dspsr_b200_context* ctx,
+                                         const dspsr_b200_fbd_config* cfg,
+                                         dspsr_b200_filterbank_during** fbd);
+int dspsr_b200_filterbank_during_destroy (dspsr_b200_filterbank_during* fbd);
+/* info[6] = {nsamp_fft, nsamp_step, nsamp_overlap, nkeep, n1, parts per batch} */
+int dspsr_b200_filterbank_during_info (dspsr_b200_filterbank_during* fbd, uint64_t* info);
+/* Engine::copy_response: host complex [input_nchan*nsub][freq_res] as
+   Response holds it after swap_as_needed, normaliser 1/sqrt(nsamp_fft *
+   freq_res) applied (Filterbank.C:171-186). */
+int dspsr_b200_filterbank_during_copy_response (dspsr_b200_filterbank_during* fbd,
+                                                const float* response);
+/* Builds that response on the GPU in FP64: Dedispersion prepared for the
+   output channels (Response::prepare(input, nchan), Filterbank.C:101-110;
+   Dedispersion.C:84-186), each channel in natural frequency order, then the
+   whole response swapped (Response::doswap, Response.C:998-1050) when the
+   input is one dual-sideband channel or a swapped multi-channel band
+   (Response::swap_as_needed, Response.C:325-400), and the normaliser. */
+int dspsr_b200_filterbank_during_set_dedispersion (dspsr_b200_filterbank_during* fbd,
+                                                   double centre_freq_mhz,
+                                                   double bandwidth_mhz, double dm,
+                                                   int swapped, int chirp_mode);
+/* copies the response back: [input_nchan*nsub][freq_res] complex, FFT order */
+int dspsr_b200_filterbank_during_get_response (dspsr_b200_filterbank_during* fbd,
+                                               float* response);
+/* Engine::perform (FilterbankEngineCPU.C:379-535): input as
+   dspsr_b200_filterbank takes it (int8 / int16 TFPD or complex-float FPT with
+   in_span); output complex-float FPT, (chan*npol + pol)*out_span with
+   npart * nkeep samples written per span. */
+int dspsr_b200_filterbank_during_perform (dspsr_b200_filterbank_during* fbd, int input_kind,
+                                          const void* d_in, uint64_t ndat, uint64_t in_span,
+                                          const float* lut256, int offset_binary, float* d_out,
+                                          uint64_t out_span, uint64_t* npart);
+
+/* ---------------------------------------------------------------------- */
 /* Detection::Engine (CUDA::DetectionEngine, Signal/General/DetectionCUDA.cu;*/
 /* callers Detection.C:237-242, 483-489)                                    */
 /* ---------------------------------------------------------------------- */

@@ -105,6 +105,27 @@ uint64_t orc_filterbank_f32 (const float* in, uint64_t ndat, uint64_t in_span, i
 uint64_t orc_filterbank_f64 (const double* in, uint64_t ndat, uint64_t in_span, int nchan_in,
                              int npol, unsigned nchan_sub, double* out, uint64_t out_span);
 
+/* ---- filterbank with a response ("During", -F nchan:D): Filterbank.C:98-198,
+        398-420 and FilterbankEngineCPU.C:379-535 ------------------------------ */
+/* response: [nchan_in*nsub][freq_res] complex as Response holds it; out:
+   (chan*npol + pol)*out_span, npart*(freq_res - nfilt) samples each.
+   Returns npart. */
+uint64_t orc_filterbank_during_f32 (const float* in, uint64_t ndat, uint64_t in_span,
+                                    int nchan_in, int npol, unsigned nsub, unsigned freq_res,
+                                    unsigned nfilt_pos, unsigned nfilt_neg, const float* response,
+                                    float* out, uint64_t out_span);
+uint64_t orc_filterbank_during_f64 (const double* in, uint64_t ndat, uint64_t in_span,
+                                    int nchan_in, int npol, unsigned nsub, unsigned freq_res,
+                                    unsigned nfilt_pos, unsigned nfilt_neg, const double* response,
+                                    double* out, uint64_t out_span);
+/* its dedispersion response: channels centred at chan_freq, natural frequency
+   order within each channel, scaled by 1/sqrt(norm), norm = nsamp_fft*freq_res */
+void orc_dedispersion_response_during (const double* chan_freq, unsigned nchan, double bw,
+                                       double dm, unsigned ndat, int mode, double norm,
+                                       float* out);
+void orc_dedispersion_response_during_f64 (const double* chan_freq, unsigned nchan, double bw,
+                                           double dm, unsigned ndat, double norm, double* out);
+
 /* ---- overlap-save convolution (Signal/General/Convolution.C:316-813) ----- */
 /* in/out FPT: (ichan*npol+ipol)*span complex values; response nchan*nfft complex
    (one filter for all polns).  Returns npart.  out holds npart*(nfft-nfilt) values. */

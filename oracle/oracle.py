@@ -77,6 +77,14 @@ _SIGS = {
                                                       c_uint, f64p]),
     "orc_filterbank_f32": (c_u64, [f32p, c_u64, c_u64, c_int, c_int, c_uint, f32p, c_u64]),
     "orc_filterbank_f64": (c_u64, [f64p, c_u64, c_u64, c_int, c_int, c_uint, f64p, c_u64]),
+    "orc_filterbank_during_f32": (c_u64, [f32p, c_u64, c_u64, c_int, c_int, c_uint, c_uint,
+                                          c_uint, c_uint, f32p, f32p, c_u64]),
+    "orc_filterbank_during_f64": (c_u64, [f64p, c_u64, c_u64, c_int, c_int, c_uint, c_uint,
+                                          c_uint, c_uint, f64p, f64p, c_u64]),
+    "orc_dedispersion_response_during": (None, [f64p, c_uint, c_dbl, c_dbl, c_uint, c_int, c_dbl,
+                                                f32p]),
+    "orc_dedispersion_response_during_f64": (None, [f64p, c_uint, c_dbl, c_dbl, c_uint, c_dbl,
+                                                    f64p]),
 }
 
 
@@ -200,6 +208,50 @@ def filterbank(x, nsub):
         lib().orc_filterbank_f64(np.ascontiguousarray(x, np.complex128).view(np.float64).ravel(),
                                  ndat, ndat, nchan, npol, nsub, out.view(np.float64).ravel(), nout)
     return out
+
+
+def dedispersion_response_during(cf, bw, dm, nchan, freq_res, nsamp_fft, swapped=True, mode=0,
+                                 fp64=False):
+    """The filterbank-with-response (During) dedispersion response,
+    [nchan][freq_res] as Response holds it after swap_as_needed: Dedispersion
+    prepared for the nchan output channels (Filterbank.C:101-110), each channel
+    in natural frequency order, the whole response swapped when the input is
+    one dual-sideband channel (Response.C:336-345, 998-1050) -- a rotation by
+    nchan/2 whole channels -- and the normaliser 1/sqrt(nsamp_fft*freq_res)
+    (Filterbank.C:171-186)."""
+    chan_freq = channel_centres(cf, bw, nchan, swap=swapped)
+    norm = float(nsamp_fft) * float(freq_res)
+    if fp64:
+        out = np.empty(nchan * freq_res, np.complex128)
+        lib().orc_dedispersion_response_during_f64(chan_freq, nchan, bw, dm, freq_res, norm,
+                                                   out.view(np.float64))
+    else:
+        out = np.empty(nchan * freq_res, np.complex64)
+        lib().orc_dedispersion_response_during(chan_freq, nchan, bw, dm, freq_res, mode, norm,
+                                               out.view(np.float32))
+    return out.reshape(nchan, freq_res)
+
+
+def filterbank_during(x, nsub, freq_res, nfilt, response):
+    """x: complex (nchan_in, npol, ndat); response [nchan_in*nsub][freq_res] ->
+    (nchan_in*nsub, npol, npart*(freq_res - nfilt_pos - nfilt_neg))."""
+    nchan, npol, ndat = x.shape
+    pos, neg = nfilt
+    nkeep = freq_res - pos - neg
+    overlap = (pos + neg) * nsub
+    npart = (ndat - overlap) // (nsub * nkeep) if ndat > overlap else 0
+    if x.dtype == np.complex64:
+        dt, rdt, f = np.complex64, np.float32, lib().orc_filterbank_during_f32
+    else:
+        dt, rdt, f = np.complex128, np.float64, lib().orc_filterbank_during_f64
+    xin = np.ascontiguousarray(x, dt)
+    r = np.ascontiguousarray(response, dt)
+    assert r.shape == (nchan * nsub, freq_res)
+    out = np.zeros((nchan * nsub, npol, max(npart * nkeep, 1)), dt)
+    n = f(xin.view(rdt).ravel(), ndat, ndat, nchan, npol, nsub, freq_res, pos, neg,
+          r.view(rdt).ravel(), out.view(rdt).ravel(), out.shape[2])
+    assert n == npart
+    return out[:, :, :npart * nkeep]
 
 
 def build():

@@ -582,14 +582,15 @@ namespace {
 template <typename T>
 void response_channels (const double* chan_freq, unsigned nchan, double bw, double dm,
                         unsigned ndat, int mode, unsigned norm_nfft, std::complex<T>* h,
-                        const double* frac_delay_us = nullptr)
+                        const double* frac_delay_us = nullptr, bool swap_halves = true,
+                        double norm = 0.0)
 {
   const double chanwidth = bw / double (nchan);
   const double binwidth = chanwidth / double (ndat);
   const double sign = bw / std::fabs (bw);
   const double dispersion_per_MHz = 1e6 * dm / dm_dispersion;
-  const T s = sizeof (T) == 4 ? T (float (1.0 / std::sqrt (double (norm_nfft))))
-                              : T (1.0 / std::sqrt (double (norm_nfft)));
+  const double nrm = norm > 0 ? norm : double (norm_nfft);
+  const T s = sizeof (T) == 4 ? T (float (1.0 / std::sqrt (nrm))) : T (1.0 / std::sqrt (nrm));
   for (unsigned c = 0; c < nchan; c++)
   {
     const double f0 = chan_freq[c];
@@ -599,8 +600,9 @@ void response_channels (const double* chan_freq, unsigned nchan, double bw, doub
     const double fd = frac_delay_us ? frac_delay_us[c] : 0.0;
     for (unsigned k = 0; k < ndat; k++)
     {
-      // FFT-order bin k holds natural bin (k + ndat/2) mod ndat
-      const unsigned ipt = (k + ndat / 2) % ndat;
+      // FFT-order bin k holds natural bin (k + ndat/2) mod ndat when each
+      // channel is swapped; the filterbank's response keeps natural order
+      const unsigned ipt = swap_halves ? (k + ndat / 2) % ndat : k;
       const double freq = double (ipt) * binwidth - 0.5 * chanwidth;
       const double phase = coeff * sqr (freq) / (f0 + freq) + (-2.0 * M_PI * freq * fd);
       std::complex<T>& o = h[uint64_t (c) * ndat + k];
@@ -647,6 +649,54 @@ uint64_t filterbank (const T* in, uint64_t ndat, uint64_t in_span, int nchan_in,
       }
   return npart;
 }
+// Filterbank with a response, the "During" form (-F nchan:D):
+// Filterbank::do_prepare (Filterbank.C:98-198) sizes nsamp_fft = nsub *
+// freq_res (complex input), nsamp_overlap = nfilt_tot * nsub and nsamp_step =
+// nsamp_fft - nsamp_overlap; Filterbank::resize_output (Filterbank.C:398-420)
+// npart = (ndat - nsamp_overlap) / nsamp_step; FilterbankEngineCPU::perform
+// (FilterbankEngineCPU.C:379-535): forward FFT of each part, Response::operate
+// over the nsub channels of the input channel (Response.C:662-726), then per
+// output channel a backward FFT of freq_res points and the nkeep samples from
+// nfilt_pos.  response: [nchan_in*nsub][freq_res] complex, normaliser applied.
+template <typename T>
+uint64_t filterbank_during (const T* in, uint64_t ndat, uint64_t in_span, int nchan_in, int npol,
+                            unsigned nsub, unsigned freq_res, unsigned nfilt_pos,
+                            unsigned nfilt_neg, const T* response, T* out, uint64_t out_span)
+{
+  typedef std::complex<T> C;
+  const uint64_t nsamp_fft = uint64_t (nsub) * freq_res;
+  const unsigned nfilt_tot = nfilt_pos + nfilt_neg;
+  const uint64_t overlap = uint64_t (nfilt_tot) * nsub;
+  const uint64_t step = nsamp_fft - overlap;
+  const uint64_t npart = ndat > overlap ? (ndat - overlap) / step : 0;
+  const unsigned nkeep = freq_res - nfilt_tot;
+  const C* resp = reinterpret_cast<const C*> (response);
+  std::vector<C> spec (nsamp_fft), tmp (freq_res);
+  for (int ic = 0; ic < nchan_in; ic++)
+    for (uint64_t ipart = 0; ipart < npart; ipart++)
+      for (int p = 0; p < npol; p++)
+      {
+        const C* x = reinterpret_cast<const C*> (in) + (uint64_t (ic) * npol + p) * in_span
+                     + ipart * step;
+        fft<T> (int (nsamp_fft), -1, x, spec.data ());
+        const C* h = resp + uint64_t (ic) * nsamp_fft;
+        for (uint64_t k = 0; k < nsamp_fft; k++)
+        {
+          const T d_r = spec[k].real (), d_i = spec[k].imag ();
+          const T f_r = h[k].real (), f_i = h[k].imag ();
+          spec[k] = C (f_r * d_r - f_i * d_i, f_i * d_r + f_r * d_i);
+        }
+        for (unsigned cs = 0; cs < nsub; cs++)
+        {
+          fft<T> (int (freq_res), +1, spec.data () + uint64_t (cs) * freq_res, tmp.data ());
+          C* o = reinterpret_cast<C*> (out) + ((uint64_t (ic) * nsub + cs) * npol + p) * out_span
+                 + ipart * nkeep;
+          for (unsigned i = 0; i < nkeep; i++) o[i] = tmp[nfilt_pos + i];
+        }
+      }
+  return npart;
+}
+
 } // namespace
 
 extern "C" {
@@ -666,6 +716,42 @@ void orc_dedispersion_response_channels_delay (const double* chan_freq, unsigned
 {
   response_channels<float> (chan_freq, nchan, bw, dm, ndat, mode, norm_nfft,
                             reinterpret_cast<std::complex<float>*> (out), frac_delay_us);
+}
+
+// The response of the filterbank with a response: channels centred at
+// chan_freq, each in natural frequency order (no per-channel swap), scaled by
+// 1/sqrt(norm) with norm = nsamp_fft * freq_res.
+void orc_dedispersion_response_during (const double* chan_freq, unsigned nchan, double bw,
+                                       double dm, unsigned ndat, int mode, double norm,
+                                       float* out)
+{
+  response_channels<float> (chan_freq, nchan, bw, dm, ndat, mode, 1,
+                            reinterpret_cast<std::complex<float>*> (out), nullptr, false, norm);
+}
+
+void orc_dedispersion_response_during_f64 (const double* chan_freq, unsigned nchan, double bw,
+                                           double dm, unsigned ndat, double norm, double* out)
+{
+  response_channels<double> (chan_freq, nchan, bw, dm, ndat, 1, 1,
+                             reinterpret_cast<std::complex<double>*> (out), nullptr, false, norm);
+}
+
+uint64_t orc_filterbank_during_f32 (const float* in, uint64_t ndat, uint64_t in_span,
+                                    int nchan_in, int npol, unsigned nsub, unsigned freq_res,
+                                    unsigned nfilt_pos, unsigned nfilt_neg, const float* response,
+                                    float* out, uint64_t out_span)
+{
+  return filterbank_during<float> (in, ndat, in_span, nchan_in, npol, nsub, freq_res, nfilt_pos,
+                                   nfilt_neg, response, out, out_span);
+}
+
+uint64_t orc_filterbank_during_f64 (const double* in, uint64_t ndat, uint64_t in_span,
+                                    int nchan_in, int npol, unsigned nsub, unsigned freq_res,
+                                    unsigned nfilt_pos, unsigned nfilt_neg, const double* response,
+                                    double* out, uint64_t out_span)
+{
+  return filterbank_during<double> (in, ndat, in_span, nchan_in, npol, nsub, freq_res, nfilt_pos,
+                                    nfilt_neg, response, out, out_span);
 }
 
 void orc_dedispersion_response_channels_f64 (const double* chan_freq, unsigned nchan, double bw,

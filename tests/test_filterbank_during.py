@@ -1,0 +1,210 @@
+"""Filterbank with a response (the "During" filterbank, -F nchan:D;
+Filterbank.C:98-198, 398-420; FilterbankEngineCPU.C:379-535): the oracle's
+restatement pinned on the CPU against an independent numpy evaluation of the
+same steps, its response against the dedispersion response of the
+convolution path, and the GPU engine against the oracle through the C ABI.
+
+Bars: oracle FP64 equal to numpy to 1e-12 relative RMS; GPU output within
+relative RMS DURING_RTOL of the FP32 oracle fed the GPU's own response and of
+the FP64 oracle fed the FP64 response; the GPU-built response within 1e-6
+relative RMS of the oracle's."""
+import numpy as np
+import pytest
+
+DURING_RTOL = 5e-6
+DURING_RTOL_FP64 = 5e-6
+
+
+def rel_rms(a, b):
+    a = np.asarray(a, np.complex128)
+    b = np.asarray(b, np.complex128)
+    return float(np.sqrt(np.mean(np.abs(a - b) ** 2) / np.mean(np.abs(b) ** 2)))
+
+
+def numpy_during(x, nsub, freq_res, nfilt, response):
+    """The same filterbank straight from its definition with numpy's FFT."""
+    nin, npol, ndat = x.shape
+    pos, neg = nfilt
+    nkeep = freq_res - pos - neg
+    n = nsub * freq_res
+    step = nsub * nkeep
+    npart = (ndat - (pos + neg) * nsub) // step
+    out = np.zeros((nin * nsub, npol, npart * nkeep), np.complex128)
+    for ic in range(nin):
+        h = response[ic * nsub:(ic + 1) * nsub].reshape(-1)
+        for ip in range(npart):
+            for p in range(npol):
+                spec = np.fft.fft(x[ic, p, ip * step:ip * step + n]) * h
+                for cs in range(nsub):
+                    y = np.fft.ifft(spec[cs * freq_res:(cs + 1) * freq_res]) * freq_res
+                    out[ic * nsub + cs, p, ip * nkeep:(ip + 1) * nkeep] = y[pos:pos + nkeep]
+    return out
+
+
+@pytest.mark.parametrize("nin,npol,nsub,freq_res,nfilt", [(1, 2, 8, 64, (5, 9)),
+                                                         (2, 1, 4, 128, (0, 0)),
+                                                         (1, 2, 16, 32, (7, 0))])
+def test_oracle_matches_numpy(orc, nin, npol, nsub, freq_res, nfilt):
+    rng = np.random.default_rng(nsub * freq_res + nin)
+    nkeep = freq_res - sum(nfilt)
+    ndat = 3 * nsub * nkeep + sum(nfilt) * nsub + 11
+    x = rng.standard_normal((nin, npol, ndat)) + 1j * rng.standard_normal((nin, npol, ndat))
+    h = rng.standard_normal((nin * nsub, freq_res)) + 1j * rng.standard_normal((nin * nsub, freq_res))
+    ref = numpy_during(x, nsub, freq_res, nfilt, h)
+    got64 = orc.filterbank_during(x, nsub, freq_res, nfilt, h)
+    assert got64.shape == ref.shape and ref.shape[2] == 3 * nkeep
+    assert rel_rms(got64, ref) < 1e-12
+    got32 = orc.filterbank_during(x.astype(np.complex64), nsub, freq_res, nfilt,
+                                  h.astype(np.complex64))
+    assert rel_rms(got32, ref) < 1e-5
+
+
+def test_oracle_response_is_the_unswapped_channel_response(orc):
+    """Each channel of the During response is the convolution path's channel
+    response (DC at bin 0) rotated back to natural order; the whole swap
+    rotates the channels by nchan/2; the normaliser is 1/sqrt(nsamp_fft *
+    freq_res)."""
+    cf, bw, dm, nchan, fr = 1400.0, -64.0, 30.0, 16, 512
+    nfft_big = nchan * fr
+    for swapped in (False, True):
+        r = orc.dedispersion_response_during(cf, bw, dm, nchan, fr, nfft_big, swapped=swapped,
+                                             fp64=True)
+        freq = orc.channel_centres(cf, bw, nchan, swap=swapped)
+        conv = orc.dedispersion_response_channels(freq, bw, dm, fr, norm_nfft=fr, fp64=True)
+        expect = np.roll(conv, fr // 2, axis=1) * np.sqrt(fr) / np.sqrt(float(nfft_big) * fr)
+        assert rel_rms(r, expect) < 1e-12
+    r0 = orc.dedispersion_response_during(cf, bw, dm, nchan, fr, nfft_big, swapped=False,
+                                          fp64=True)
+    r1 = orc.dedispersion_response_during(cf, bw, dm, nchan, fr, nfft_big, swapped=True,
+                                          fp64=True)
+    assert np.array_equal(np.roll(r0, -nchan // 2, axis=0), r1)
+
+
+def test_oracle_restores_a_dispersed_pulse(orc):
+    """Physics check of the restatement: a pulse dispersed by the exact FP64
+    inverse of the response over the whole band comes out of the filterbank
+    with its power at one time in every channel."""
+    cf, bw, dm, nsub, fr = 1400.0, 16.0, 8.0, 8, 1024
+    n = nsub * fr
+    r = orc.dedispersion_response_during(cf, bw, dm, nsub, fr, n, swapped=True, fp64=True)
+    # the response in FFT order of the big transform: its inverse disperses
+    big = r.reshape(-1) * np.sqrt(float(n) * fr)
+    x = np.zeros(3 * n, np.complex128)
+    x[n + n // 2] = 1.0
+    spec = np.fft.fft(x[n:2 * n])
+    disp = np.fft.ifft(spec * np.conj(big))
+    xin = np.zeros((1, 1, 3 * n), np.complex128)
+    xin[0, 0, n:2 * n] = disp
+    out = orc.filterbank_during(xin, nsub, fr, (0, 0), r)
+    power = np.abs(out[:, 0, :]) ** 2
+    peaks = np.argmax(power, axis=1)
+    assert np.ptp(peaks) <= 1, peaks
+
+
+# ---------------------------------------------------------------- GPU engine
+
+GPU_CASES = {
+    # 16 channels of 1024 points: n1 = 2, 512-point channel transforms
+    "dedisp_16x1024_float": dict(nin=1, npol=2, nsub=16, fr=1024, dm=2.0, kind="float",
+                                 npart=3),
+    # 64 channels of 4096 points (2^18 points, n1 = 32, 128-point segments), int8
+    "dedisp_64x4096_int8": dict(nin=1, npol=2, nsub=64, fr=4096, dm=60.0, kind="int8",
+                                npart=2),
+    # two input channels, one polarisation, a random response, int16
+    "random_2in_8x4096_int16": dict(nin=2, npol=1, nsub=8, fr=4096, nfilt=(300, 200),
+                                    kind="int16", npart=3),
+    # the smallest segments: 128 channels of 128 points
+    "random_128x128_float": dict(nin=1, npol=2, nsub=128, fr=128, nfilt=(16, 8), kind="float",
+                                 npart=4),
+    # two channels of 65536 points (n1 = 16, 4096-point segments)
+    "dedisp_2x65536_float": dict(nin=1, npol=1, nsub=2, fr=65536, dm=20.0, kind="float",
+                                 npart=2),
+}
+CF, BW = 1400.0, 64.0
+
+
+def _input(rng, nin, npol, ndat, kind, b2):
+    if kind == "int16":
+        raw = rng.integers(-3000, 3000, (ndat, nin, npol, 2)).astype(np.int16)
+        x = (raw.astype(np.float32) + 0.5).transpose(1, 2, 0, 3).copy().view(np.complex64)[..., 0]
+        return raw.reshape(-1), x, b2.INT16_TFPD, None
+    if kind == "int8":
+        raw = rng.integers(-128, 128, (ndat, nin, npol, 2)).astype(np.int8).view(np.uint8)
+        lut, _ = b2.bittable8()
+        x = lut[raw].transpose(1, 2, 0, 3).copy().view(np.complex64)[..., 0]
+        return raw.reshape(-1), x, b2.INT8_TFPD, lut
+    x = (rng.standard_normal((nin, npol, ndat)) +
+         1j * rng.standard_normal((nin, npol, ndat))).astype(np.complex64)
+    return x, x, b2.FLOAT_FPT, None
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(GPU_CASES))
+def test_during_gpu_matches_oracle(ctx, b2, orc, name):
+    torch = pytest.importorskip("torch")
+    case = GPU_CASES[name]
+    nin, npol, nsub, fr = case["nin"], case["npol"], case["nsub"], case["fr"]
+    nchan = nin * nsub
+    rng = np.random.default_rng(len(name))
+    if "dm" in case:
+        half = b2.smearing_samples(CF, BW, case["dm"], nchan, 1)
+        nfilt = (half, half)
+    else:
+        nfilt = case["nfilt"]
+    fbd = b2.FilterbankDuring(ctx, nin, npol, nsub, fr, nfilt)
+    info = fbd.info
+    nkeep = fr - sum(nfilt)
+    assert info["nkeep"] == nkeep and info["nsamp_step"] == nsub * nkeep
+    assert info["nsamp_fft"] == nsub * fr and info["nsamp_overlap"] == sum(nfilt) * nsub
+    if "dm" in case:
+        fbd.set_dedispersion(CF, BW, case["dm"], swapped=True)
+        resp = fbd.get_response()
+        ref_resp = orc.dedispersion_response_during(CF, BW, case["dm"], nchan, fr, nsub * fr,
+                                                    swapped=True)
+        assert rel_rms(resp, ref_resp) < 1e-6, rel_rms(resp, ref_resp)
+        resp64 = orc.dedispersion_response_during(CF, BW, case["dm"], nchan, fr, nsub * fr,
+                                                  swapped=True, fp64=True)
+    else:
+        ph = rng.uniform(0, 2 * np.pi, (nchan, fr))
+        resp = (np.exp(1j * ph) * rng.uniform(0.5, 1.5, (nchan, fr))
+                / np.sqrt(float(nsub) * fr * fr)).astype(np.complex64)
+        fbd.copy_response(resp)
+        assert np.array_equal(fbd.get_response(), resp)
+        resp64 = resp.astype(np.complex128)
+    ndat = case["npart"] * nsub * nkeep + sum(nfilt) * nsub + 7      # a ragged tail
+    raw, x, kind, lut = _input(rng, nin, npol, ndat, case["kind"], b2)
+    ref = orc.filterbank_during(x, nsub, fr, nfilt, resp)
+    ref64 = orc.filterbank_during(x.astype(np.complex128), nsub, fr, nfilt, resp64)
+    span = case["npart"] * nkeep + 3
+    d_out = torch.full((nchan, npol, span, 2), float("nan"), device="cuda")
+    if kind == b2.FLOAT_FPT:
+        d_in = torch.from_numpy(np.ascontiguousarray(x).view(np.float32)).cuda()
+        n = fbd.perform(d_in, ndat, d_out, span)
+    else:
+        d_in = torch.from_numpy(raw).cuda()
+        n = fbd.perform(d_in, ndat, d_out, span, input_kind=kind, lut=lut)
+    ctx.synchronize()
+    assert n == case["npart"] == fbd.npart(ndat)
+    out = d_out.cpu().numpy().view(np.complex64)[..., 0]
+    body = out[:, :, :n * nkeep]
+    assert np.isnan(out[:, :, n * nkeep:].view(np.float32)).all()
+    assert rel_rms(body, ref) < DURING_RTOL, rel_rms(body, ref)
+    assert rel_rms(body, ref64) < DURING_RTOL_FP64, rel_rms(body, ref64)
+    fbd.close()
+
+
+@pytest.mark.gpu
+def test_during_rejects_unsupported_shapes(ctx, b2):
+    for nsub, fr, nfilt in [(256, 1024, (0, 0)),     # segments below 64 points
+                            (3, 8192, (0, 0)),       # not a power of two
+                            (8, 1024, (0, 0)),       # 8192 points: below the four-step split
+                            (64, 8192, (0, 0)),      # 2^19 points
+                            (16, 1024, (600, 424))]:  # nothing kept
+        with pytest.raises(b2.B200Error):
+            b2.FilterbankDuring(ctx, 1, 2, nsub, fr, nfilt)
+    fbd = b2.FilterbankDuring(ctx, 1, 2, 16, 1024, (10, 10))
+    torch = pytest.importorskip("torch")
+    buf = torch.zeros(1 << 16, device="cuda")
+    with pytest.raises(b2.B200Error, match="no response"):
+        fbd.perform(buf, 1000, buf, 1000)
+    fbd.close()
