@@ -3,7 +3,7 @@
 dedispersion -> detection -> fold, in complex Msamples/s.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                  [--config c1|c2|c3|c4|c5|c5ifb]
+                  [--config c1|c2|c2d|c3|c4|c5|c5ifb]
 
 One step = one block of the workload processed end to end (unpack -> fold),
 the InputBuffering overlap carried from block to block.  Inputs are seeded
@@ -79,6 +79,14 @@ CONFIGS = {
         workload=("inverse filterbank stage of C5 alone: 256 PFB channels int16 dual-pol, "
                   "1024-point input FFTs, 196608-point output spectra, 1 s of 800 MHz"),
         nin=256, npol=2, lin=1024, disc=12288, ndat=4166784),
+    "c2d": dict(
+        kind="fbd",
+        workload=("filterbank with the dedispersion inside it (-F 64:D): 256 MHz complex "
+                  "baseband at 1400 MHz, 2 pol int8, one 2^18-point FFT per part, the "
+                  "response of 64 x 4 MHz channels at DM 25, 64 inverse FFTs of 4096 points, "
+                  "full Stokes, 2048-bin fold, P=5.757 ms, 2^26 samples/pol per block"),
+        cf=1400.0, bw=256.0, dm=25.0, npol=2, nsub=64, freq_res=4096, nbin=2048,
+        period=5.757e-3, state=3, ndat=1 << 26),
 }
 
 NBLOCKS = 4
@@ -961,6 +969,143 @@ def run_b200_ifb(args, cfg, world, rank, local):
 
 
 # ---------------------------------------------------------------------------
+# Filterbank with the dedispersion inside it ("During")
+# ---------------------------------------------------------------------------
+
+def fbd_sizes(cfg, b2):
+    half = b2.smearing_samples(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nsub"], 1)
+    return half, cfg["freq_res"] - 2 * half
+
+
+def run_reference_fbd(args, cfg, world, rank):
+    if rank != 0:
+        return
+    import dspsr_b200 as b2
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    half, nkeep = fbd_sizes(cfg, b2)
+    nsub, fr = cfg["nsub"], cfg["freq_res"]
+    resp = orc.dedispersion_response_during(cfg["cf"], cfg["bw"], cfg["dm"], nsub, fr, nsub * fr)
+    nparts = 2
+    ndat = nparts * nsub * nkeep + 2 * half * nsub
+    rng = np.random.default_rng(5)
+    lut, _ = b2.bittable8()
+    raw = rng.integers(0, 256, (cfg["npol"], ndat, 2), dtype=np.uint8)
+    nbin = cfg["nbin"]
+    pps = (nsub / (cfg["bw"] * 1e6)) / cfg["period"]
+
+    def step():
+        t0 = time.perf_counter()
+        x = lut[raw].view(np.complex64)[None, :, :, 0]
+        v = orc.filterbank_during(x, nsub, fr, (half, half), resp)
+        det = orc.detect(v, cfg["state"])
+        plan = orc.fold_binplan(0.1, pps, v.shape[2], nbin)
+        orc.fold_accumulate(det, plan, nbin)
+        return time.perf_counter() - t0
+    for _ in range(args.warmup):
+        step()
+    total = sum(step() for _ in range(args.steps))
+    msps = cfg["npol"] * nparts * nsub * nkeep * args.steps / total / 1e6
+    line = {
+        "impl": "reference", "metric": "complex Msamples/s filterbank-with-dedispersion -> fold",
+        "value": round(msps, 3), "unit": "complex Msamples/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * total / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded uniform int8 voltages)",
+        "config": {"workload": cfg["workload"], "sample_parts_per_step": nparts},
+        "cpu_baseline": {"value": round(msps, 3), "unit": "complex Msamples/s", "cores": 1,
+                         "kind": "port",
+                         "sample": (f"{nparts} parts of {nsub * fr} samples x {cfg['npol']} pol "
+                                    "through the oracle restatement of FilterbankEngineCPU with "
+                                    "a response, Detection and Fold (single thread, FP32)")},
+        "e2e": {"value": round(msps, 3), "unit": "complex Msamples/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_b200_fbd(args, cfg, world, rank, local):
+    import torch
+    import dspsr_b200 as b2
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    ctx = b2.Context(local)
+    half, nkeep = fbd_sizes(cfg, b2)
+    nsub, fr, npol = cfg["nsub"], cfg["freq_res"], cfg["npol"]
+    fbd = b2.FilterbankDuring(ctx, 1, npol, nsub, fr, (half, half))
+    fbd.set_dedispersion(cfg["cf"], cfg["bw"], cfg["dm"])
+    ndat = cfg["ndat"]
+    npart = fbd.npart(ndat)
+    span = npart * nkeep
+    nout = b2.NOUT[cfg["state"]]
+    fold = b2.Fold(ctx, cfg["nbin"], nsub, nout)
+    lut, _ = b2.bittable8()
+    gen = torch.Generator(device=device)
+    gen.manual_seed(17 + rank)
+    # two distinct int8 TFPD blocks, each larger than L2
+    raws = [torch.randint(0, 256, (ndat * npol * 2,), dtype=torch.uint8, device=device,
+                          generator=gen) for _ in range(2)]
+    rate = cfg["bw"] * 1e6 / nsub
+    pps = (1.0 / rate) / cfg["period"]
+    used = npol * npart * nsub * nkeep
+
+    def step(i):
+        fold.set_bins(0.1 + 1e-3 * i, pps, span)
+        fbd.perform_fold(raws[i % 2], ndat, fold, cfg["state"], input_kind=b2.INT8_TFPD, lut=lut)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(1.0)
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    launches0 = b2.kernel_launches()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    evs[0].record()
+    for i in range(args.steps):
+        step(i)
+        evs[i + 1].record()
+    torch.cuda.synchronize()
+    launches = b2.kernel_launches() - launches0
+    clk = clocks.stop()
+    barrier(world)
+    ms = evs[0].elapsed_time(evs[-1])
+    ms_max = max_over_ranks(ms, world)
+    value = used * args.steps * world / (ms_max / 1e3) / 1e6
+    hbm_peak, _, peak_src = measured_peaks()
+    alg = ndat * npol * 2
+    achieved = alg / (ms / args.steps / 1e3) / 1e9
+    line = {
+        "metric": "complex Msamples/s filterbank-with-dedispersion -> fold",
+        "value": round(value, 3), "unit": "complex Msamples/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded uniform int8 voltages)",
+        "config": {"workload": cfg["workload"], "npart": npart, "nkeep": nkeep,
+                   "nfilt": 2 * half, "fft_split": [fbd.info["n1"], 8192],
+                   "parts_per_batch": fbd.info["max_batch"],
+                   "l2": f"input {ndat * npol * 2 >> 20} MiB per step, larger than L2",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "clocks": clk,
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "filterbank with response (3 kernels)",
+                     "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
+                     "frac": round(achieved / hbm_peak, 4), "traffic": None,
+                     "peak_source": peak_src,
+                     "note": "algorithmic bytes: the int8 input once; FP32-ALU bound like c2"},
+        "e2e": None,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    fold.close()
+    fbd.close()
+    ctx.close()
+
+
+# ---------------------------------------------------------------------------
 # Multi-stream workload: many independent beams / DM trials at once
 # ---------------------------------------------------------------------------
 
@@ -1446,10 +1591,12 @@ def main():
         kind = cfg.get("kind", "path")
         if args.impl == "reference":
             {"sk": run_reference_sk, "ifb": run_reference_ifb, "c3": run_reference_c3,
-             "c5": run_reference_c5}.get(kind, run_reference)(args, cfg, world, rank)
+             "c5": run_reference_c5, "fbd": run_reference_fbd}.get(kind, run_reference)(
+                 args, cfg, world, rank)
         else:
             {"sk": run_b200_sk, "ifb": run_b200_ifb, "c3": run_b200_c3,
-             "c5": run_b200_c5}.get(kind, run_b200)(args, cfg, world, rank, local)
+             "c5": run_b200_c5, "fbd": run_b200_fbd}.get(kind, run_b200)(
+                 args, cfg, world, rank, local)
     finally:
         if world > 1:
             import torch.distributed as dist

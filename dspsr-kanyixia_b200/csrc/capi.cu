@@ -1681,6 +1681,61 @@ int dspsr_b200_filterbank_during_perform (dspsr_b200_filterbank_during* f, int i
   return DSPSR_B200_OK;
 }
 
+int dspsr_b200_filterbank_during_perform_fold (dspsr_b200_filterbank_during* f, int input_kind,
+                                               const void* d_in, uint64_t ndat, uint64_t in_span,
+                                               const float* lut256, int offset_binary,
+                                               dspsr_b200_fold* fold, int state,
+                                               uint64_t* npart_out)
+{
+  if (!f) return DSPSR_B200_EINVAL;
+  dspsr_b200_context* ctx = f->ctx;
+  if (npart_out) *npart_out = 0;
+  if (!f->have_response) return fail (ctx, DSPSR_B200_ESTATE, "filterbank during: no response set");
+  if (!d_in || !fold) return fail (ctx, DSPSR_B200_EINVAL, "filterbank during: null argument");
+  if (input_kind < 0 || input_kind > 2 || (input_kind == DSPSR_B200_INT8_TFPD && !lut256))
+    return fail (ctx, DSPSR_B200_EINVAL, "filterbank during: invalid input kind or missing table");
+  if (input_kind == DSPSR_B200_FLOAT_FPT && in_span < ndat)
+    return fail (ctx, DSPSR_B200_EINVAL, "filterbank during: in_span < ndat");
+  const DuringShape& s = f->shape;
+  if (state < 0 || state > 3 || (s.npol == 1 && state != DSPSR_B200_INTENSITY))
+    return fail (ctx, DSPSR_B200_EINVAL, "filterbank during: detection state %d with %u pol",
+                 state, s.npol);
+  const int nout = detect_nout (state);
+  const uint64_t overlap = uint64_t (s.nsub) * (s.nfilt_pos + s.nfilt_neg);
+  const uint64_t npart = ndat > overlap ? (ndat - overlap) / s.in_step : 0;
+  if (fold->ctx != ctx || fold->nchan != s.nchan_in * s.nsub || fold->npol != unsigned (nout))
+    return fail (ctx, DSPSR_B200_EINVAL,
+                 "filterbank during: fold engine of %u channels x %u products, expected %u x %d",
+                 fold->nchan, fold->npol, s.nchan_in * s.nsub, nout);
+  if (fold->ndat != npart * s.nkeep)
+    return fail (ctx, DSPSR_B200_ESTATE,
+                 "filterbank during: fold plan covers %llu samples, the parts give %llu",
+                 (unsigned long long) fold->ndat, (unsigned long long) (npart * s.nkeep));
+  if (input_kind == DSPSR_B200_INT8_TFPD)
+    B200_CHECK (ctx, cudaMemcpyAsync (ctx->d_lut, lut256, 256 * sizeof (float),
+                                      cudaMemcpyHostToDevice, ctx->stream), "upload lut");
+  InputView in {};
+  in.kind = input_kind;
+  in.main = d_in;
+  in.main_span = in_span;
+  in.nchan = s.nchan_in;
+  in.npol = s.npol;
+  in.offset_binary = offset_binary;
+  VoltView vv {nullptr, 0};
+  const FoldView fv = fold->view (state, nout, fold->nchan);
+  const DuringTables tb = f->tables ();
+  for (uint64_t p0 = 0; p0 < npart; p0 += f->max_batch)
+  {
+    const unsigned nb = unsigned (std::min<uint64_t> (f->max_batch, npart - p0));
+    B200_CHECK (ctx, launch_filterbank_during (s, tb, in, p0, nb, f->scratch.ptr, OUT_FOLD, fv, vv,
+                                               ctx->stream), "filterbank during kernels");
+  }
+  const int rc = fold->release_plan ();
+  if (rc) return rc;
+  if (npart_out) *npart_out = npart;
+  return DSPSR_B200_OK;
+}
+
 int dspsr_b200_apodization (int type, unsigned ndat, unsigned transition_start,
                             unsigned transition_end, int swap_halves, float* window)
 {

@@ -422,6 +422,18 @@ class FilterbankDuring:
             "filterbank_during_perform")
         return n.value
 
+    def perform_fold(self, d_in, ndat, fold, state, input_kind=FLOAT_FPT, in_span=None, lut=None,
+                     offset_binary=False):
+        """Filterbank, detection and fold in one pass; fold's plan (set_bins)
+        covers npart(ndat) * nkeep output samples."""
+        n = ctypes.c_uint64()
+        lp = _fptr(np.ascontiguousarray(lut, np.float32)) if lut is not None else None
+        self.ctx.check(self._lib.dspsr_b200_filterbank_during_perform_fold(
+            self.handle, input_kind, _ptr(d_in), ndat, ndat if in_span is None else in_span, lp,
+            int(offset_binary), fold.handle, state, ctypes.byref(n)),
+            "filterbank_during_perform_fold")
+        return n.value
+
     def close(self):
         if self.handle:
             self._lib.dspsr_b200_filterbank_during_destroy(self.handle)

@@ -373,6 +373,16 @@ int dspsr_b200_filterbank_during_perform (dspsr_b200_filterbank_during* fbd, int
                                           const void* d_in, uint64_t ndat, uint64_t in_span,
                                           const float* lut256, int offset_binary, float* d_out,
                                           uint64_t out_span, uint64_t* npart);
+/* The same filterbank with Detection::Engine and Fold::Engine fused into its
+   last pass (the filterbank's output never reaches memory): the channels are
+   detected to state (Detection.C:225-577) and folded by fold, whose plan
+   (dspsr_b200_fold_set_bins) must cover exactly npart * nkeep output samples
+   and whose nchan / npol must be input_nchan*nsub / the state's products. */
+int dspsr_b200_filterbank_during_perform_fold (dspsr_b200_filterbank_during* fbd,
+                                               int input_kind, const void* d_in, uint64_t ndat,
+                                               uint64_t in_span, const float* lut256,
+                                               int offset_binary, dspsr_b200_fold* fold,
+                                               int state, uint64_t* npart);
 
 /* ---------------------------------------------------------------------- */
 /* Detection::Engine (CUDA::DetectionEngine, Signal/General/DetectionCUDA.cu;*/

@@ -117,7 +117,7 @@ GPU_CASES = {
     "random_128x128_float": dict(nin=1, npol=2, nsub=128, fr=128, nfilt=(16, 8), kind="float",
                                  npart=4),
     # two channels of 65536 points (n1 = 16, 4096-point segments)
-    "dedisp_2x65536_float": dict(nin=1, npol=1, nsub=2, fr=65536, dm=20.0, kind="float",
+    "dedisp_2x65536_float": dict(nin=1, npol=1, nsub=2, fr=65536, dm=5.0, kind="float",
                                  npart=2),
 }
 CF, BW = 1400.0, 64.0
@@ -157,13 +157,20 @@ def test_during_gpu_matches_oracle(ctx, b2, orc, name):
     assert info["nkeep"] == nkeep and info["nsamp_step"] == nsub * nkeep
     assert info["nsamp_fft"] == nsub * fr and info["nsamp_overlap"] == sum(nfilt) * nsub
     if "dm" in case:
+        # the FP64-phase chirp against the FP64 response
+        fbd.set_dedispersion(CF, BW, case["dm"], swapped=True, chirp_mode=b2.CHIRP_FP64)
+        exact = orc.dedispersion_response_during(CF, BW, case["dm"], nchan, fr, nsub * fr,
+                                                 swapped=True, fp64=True)
+        assert rel_rms(fbd.get_response(), exact) < 1e-6
+        # the reference's chirp (phases rounded to float, Dedispersion.C:104-111)
+        # against the oracle's; the transforms are then checked with the
+        # response the GPU holds, so that the float phases do not hide their error
         fbd.set_dedispersion(CF, BW, case["dm"], swapped=True)
         resp = fbd.get_response()
         ref_resp = orc.dedispersion_response_during(CF, BW, case["dm"], nchan, fr, nsub * fr,
                                                     swapped=True)
         assert rel_rms(resp, ref_resp) < 1e-6, rel_rms(resp, ref_resp)
-        resp64 = orc.dedispersion_response_during(CF, BW, case["dm"], nchan, fr, nsub * fr,
-                                                  swapped=True, fp64=True)
+        resp64 = resp.astype(np.complex128)
     else:
         ph = rng.uniform(0, 2 * np.pi, (nchan, fr))
         resp = (np.exp(1j * ph) * rng.uniform(0.5, 1.5, (nchan, fr))
@@ -207,4 +214,47 @@ def test_during_rejects_unsupported_shapes(ctx, b2):
     buf = torch.zeros(1 << 16, device="cuda")
     with pytest.raises(b2.B200Error, match="no response"):
         fbd.perform(buf, 1000, buf, 1000)
+    fbd.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("state,npol", [(3, 2), (1, 2), (0, 1)])
+def test_during_fold_matches_its_voltages(ctx, b2, orc, state, npol):
+    """Detection and fold fused into the last pass give the profiles that the
+    oracle's Detection and Fold make of the engine's own voltages (checked
+    against the oracle above); hits bit-exact."""
+    torch = pytest.importorskip("torch")
+    nsub, fr, dm, npart = 32, 2048, 10.0, 3
+    half = b2.smearing_samples(CF, BW, dm, nsub, 1)
+    fbd = b2.FilterbankDuring(ctx, 1, npol, nsub, fr, (half, half))
+    fbd.set_dedispersion(CF, BW, dm)
+    nkeep = fbd.info["nkeep"]
+    ndat = npart * nsub * nkeep + 2 * half * nsub + 5
+    rng = np.random.default_rng(state + 10 * npol)
+    x = (rng.standard_normal((1, npol, ndat)) + 1j * rng.standard_normal((1, npol, ndat))
+         ).astype(np.complex64)
+    d_in = torch.from_numpy(x.view(np.float32)).cuda()
+    span = npart * nkeep
+    d_v = torch.zeros((nsub, npol, span, 2), device="cuda")
+    assert fbd.perform(d_in, ndat, d_v, span) == npart
+    ctx.synchronize()
+    v = d_v.cpu().numpy().view(np.complex64)[..., 0].astype(np.complex128)
+    if npol == 2:
+        det = orc.detect(v, state)
+    else:
+        det = np.abs(v) ** 2
+    nout = det.shape[1]
+    nbin, phi, pps = 256, 0.3, 1.0 / 1234.5
+    plan = orc.fold_binplan(phi, pps, span, nbin)
+    rprof, rhits = orc.fold_accumulate(det, plan, nbin)
+    f = b2.Fold(ctx, nbin, nsub, nout)
+    f.set_bins(phi, pps, span - 1)
+    with pytest.raises(b2.B200Error, match="fold plan"):
+        fbd.perform_fold(d_in, ndat, f, state)
+    f.set_bins(phi, pps, span)
+    assert fbd.perform_fold(d_in, ndat, f, state) == npart
+    prof, hits = f.get_profiles()
+    assert np.array_equal(hits, rhits)
+    assert rel_rms(prof, rprof) < 1e-5, rel_rms(prof, rprof)
+    f.close()
     fbd.close()
