@@ -2196,6 +2196,10 @@ int dspsr_b200_fold_create (dspsr_b200_context* ctx, unsigned nbin, unsigned nch
     delete f;
     return rc;
   }
+  // engines that fold many channels from one plan (the filterbank with a
+  // response) read each sample's column once per block instead of searching
+  // the plan in every channel
+  f->use_cols = nchan >= 4;
   *out = f;
   return DSPSR_B200_OK;
 }

@@ -733,8 +733,30 @@ k_rows_tma (float2* __restrict__ scratch, const float2* __restrict__ ptab,
 // K3: inverse column DFTs, overlap discard, voltage out or detect + fold
 // --------------------------------------------------------------------------
 
+// One column of an inverse four-step pass: N1 values stride apart, the
+// conjugate twiddles tw[k*tw_stride], then the N1-point inverse DFT.
+template <int N1>
+__device__ __forceinline__ void inv_column (const float2* __restrict__ src, uint64_t stride,
+                                            const float2* __restrict__ tw, unsigned tw_stride,
+                                            float2* v)
+{
+#pragma unroll
+  for (int k = 0; k < N1; k++)
+    v[k] = src[uint64_t (k) * stride];
+#pragma unroll
+  for (int k = 1; k < N1; k++)
+    v[k] = cmulc (v[k], __ldg (tw + uint64_t (k) * tw_stride));
+  RegDFT<N1, +1>::run (v);
+}
+
+// Two polarisations of 16 or 32 values each do not fit in registers beside
+// the DFT's temporaries: the first waits in shared memory (one slot per
+// thread, so no barrier) while the second is transformed.
+template <int N1, int NPOL>
+__host__ __device__ constexpr bool stage_first_pol () { return NPOL == 2 && N1 >= 16; }
+
 template <int N1, int NPOL, int MODE, int NOUT>
-__global__ void __launch_bounds__ (128, 4)
+__global__ void __launch_bounds__ (128, N1 >= 32 ? 3 : 4)
 k_inv_cols (const float2* __restrict__ scratch, const unsigned n2, const unsigned nchan,
             const uint64_t nkeep, const unsigned nfilt_pos, const uint64_t part0,
             const float2* __restrict__ tw4, const FoldView fv, const VoltView vv)
@@ -743,6 +765,39 @@ k_inv_cols (const float2* __restrict__ scratch, const unsigned n2, const unsigne
   const unsigned b = blockIdx.y;
   const unsigned c = blockIdx.z;
   const uint64_t N = uint64_t (N1) * n2;
+  const uint64_t tbase0 = (part0 + b) * nkeep;
+  if constexpr (stage_first_pol<N1, NPOL> ())
+  {
+    __shared__ float2 s0[N1 * 128];
+    const float2* src = scratch + (uint64_t (b) * nchan + c) * 2 * N + i2;
+    {
+      float2 v[N1];
+      inv_column<N1> (src, n2, tw4 + i2, n2, v);
+#pragma unroll
+      for (int k = 0; k < N1; k++) s0[k * 128 + threadIdx.x] = v[k];
+    }
+    float2 q[N1];
+    inv_column<N1> (src + N, n2, tw4 + i2, n2, q);
+#pragma unroll
+    for (int k = 0; k < N1; k++)
+    {
+      const uint64_t tl = uint64_t (k) * n2 + i2;
+      const bool ok = tl >= nfilt_pos && tl < nfilt_pos + nkeep;
+      const uint64_t t = tbase0 + (tl - nfilt_pos);
+      const float2 p = s0[k * 128 + threadIdx.x];
+      if constexpr (MODE == OUT_VOLTAGE)
+      {
+        if (ok)
+        {
+          vv.out[(uint64_t (c) * 2) * vv.span + t] = p;
+          vv.out[(uint64_t (c) * 2 + 1) * vv.span + t] = q[k];
+        }
+      }
+      else
+        emit_fold<NOUT> (fv, c, 2, ok, t, p, q[k]);
+    }
+    return;
+  }
   float2 w[N1];
 #pragma unroll
   for (int k = 1; k < N1; k++)
@@ -1195,7 +1250,7 @@ k_rows_during (float2* __restrict__ scratch, const float2* __restrict__ ptab,
 // (FilterbankEngineCPU.C:516-523) and voltages out, or detection + fold.
 // seg >= 64, so the 32 lanes of a warp share one output channel.
 template <int N1, int NPOL, int MODE, int NOUT>
-__global__ void __launch_bounds__ (128, 4)
+__global__ void __launch_bounds__ (128, N1 >= 32 ? 3 : 4)
 k_inv_cols_during (const float2* __restrict__ scratch, const DuringShape sh, const uint64_t part0,
                    const float2* __restrict__ twd, const FoldView fv, const VoltView vv)
 {
@@ -1205,6 +1260,39 @@ k_inv_cols_during (const float2* __restrict__ scratch, const DuringShape sh, con
   const uint64_t N = uint64_t (N1) * sh.n2;
   const unsigned cs = i2 / sh.seg, t2 = i2 % sh.seg;
   const unsigned c = cin * sh.nsub + cs;
+  if constexpr (stage_first_pol<N1, NPOL> ())
+  {
+    __shared__ float2 s0[N1 * 128];
+    const float2* src = scratch + (uint64_t (b) * sh.nchan_in + cin) * 2 * N + i2;
+    {
+      float2 v[N1];
+      inv_column<N1> (src, sh.n2, twd + t2, sh.seg, v);
+#pragma unroll
+      for (int k = 0; k < N1; k++) s0[k * 128 + threadIdx.x] = v[k];
+    }
+    float2 q[N1];
+    inv_column<N1> (src + N, sh.n2, twd + t2, sh.seg, q);
+    const uint64_t tb = (part0 + b) * sh.nkeep;
+#pragma unroll
+    for (int k = 0; k < N1; k++)
+    {
+      const uint64_t tl = uint64_t (k) * sh.seg + t2;
+      const bool ok = tl >= sh.nfilt_pos && tl < sh.nfilt_pos + sh.nkeep;
+      const uint64_t t = tb + (tl - sh.nfilt_pos);
+      const float2 p = s0[k * 128 + threadIdx.x];
+      if constexpr (MODE == OUT_VOLTAGE)
+      {
+        if (ok)
+        {
+          vv.out[(uint64_t (c) * 2) * vv.span + t] = p;
+          vv.out[(uint64_t (c) * 2 + 1) * vv.span + t] = q[k];
+        }
+      }
+      else
+        emit_fold<NOUT> (fv, c, 2, ok, t, p, q[k]);
+    }
+    return;
+  }
   float2 w[N1];
 #pragma unroll
   for (int k = 1; k < N1; k++)
