@@ -5,6 +5,8 @@ C ABI of libdspsr_b200.so (include/dspsr_b200.h):
 
   Unpacker           -> unpack8 / unpack16      (GenericEightBitUnpacker, SixteenBitUnpacker)
   Convolution engine -> Convolution             (CUDA::ConvolutionEngine)
+  Filterbank engine  -> FilterbankDuring        (Filterbank with a response, -F N:D)
+  InverseFilterbank  -> InverseFilterbank       (InverseFilterbank::Engine)
   Detection engine   -> detect                  (CUDA::DetectionEngine)
   Fold engine        -> Fold                    (CUDA::FoldEngine with use_set_bins)
   SingleThread loop  -> Pipeline                (unpack -> convolve -> detect -> fold)
