@@ -248,6 +248,9 @@ template <int NOUT>
 __device__ __forceinline__ void emit_fold (const FoldView& fv, unsigned c, unsigned npol, bool ok,
                                            uint64_t t, float2 p, float2 q)
 {
+  // a warp whose samples all fall in the overlap discard has nothing to add
+  // (all 32 lanes are here, so the vote and the return are warp-uniform)
+  if (!__any_sync (FULL, ok)) return;
   float v[4] = {0.f, 0.f, 0.f, 0.f};
   unsigned bin = fv.cols ? (ok ? __ldg (fv.cols + t) : NO_COLUMN)
                          : warp_fold_bin (fv.segs, fv.nseg, ok, t, fv.nbin);
