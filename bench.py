@@ -3,7 +3,7 @@
 dedispersion -> detection -> fold, in complex Msamples/s.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                  [--config c1|c2|c2d|c3|c4|c5|c5ifb]
+                  [--config c1|c2|c2d|c2d500|c3|c4|c5|c5ifb]
 
 One step = one block of the workload processed end to end (unpack -> fold),
 the InputBuffering overlap carried from block to block.  Inputs are seeded
@@ -86,6 +86,14 @@ CONFIGS = {
                   "response of 64 x 4 MHz channels at DM 25, 64 inverse FFTs of 4096 points, "
                   "full Stokes, 2048-bin fold, P=5.757 ms, 2^26 samples/pol per block"),
         cf=1400.0, bw=256.0, dm=25.0, npol=2, nsub=64, freq_res=4096, nbin=2048,
+        period=5.757e-3, state=3, ndat=1 << 26),
+    "c2d500": dict(
+        kind="fbd",
+        workload=("C2 with the dedispersion inside the filterbank (-F 64:D): 256 MHz complex "
+                  "baseband at 1400 MHz, 2 pol int8, DM 500, one 2^22-point FFT per part "
+                  "(512 x 8192), 64 x 4 MHz channels of 65536 points, full Stokes, 2048-bin "
+                  "fold, P=5.757 ms, 2^26 samples/pol per block"),
+        cf=1400.0, bw=256.0, dm=500.0, npol=2, nsub=64, freq_res=65536, nbin=2048,
         period=5.757e-3, state=3, ndat=1 << 26),
 }
 

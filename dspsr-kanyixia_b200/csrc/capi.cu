@@ -1430,7 +1430,7 @@ struct dspsr_b200_filterbank_during
 {
   dspsr_b200_context* ctx = nullptr;
   DuringShape shape {};
-  DevBuf<float2> tw4, ptab, ptab_seg, twd, H, tmp, scratch;
+  DevBuf<float2> tw4, ptab, ptab_seg, ptab_col, twd, H, tmp, scratch;
   DevBuf<double> chan_par;
   bool have_response = false;
   int nsm = 148;
@@ -1443,6 +1443,7 @@ struct dspsr_b200_filterbank_during
     t.ptab = ptab.ptr;
     t.ptab_seg = ptab_seg.ptr;
     t.twd = twd.ptr;
+    t.ptab_col = ptab_col.ptr;
     t.H = H.ptr;
     t.lut = ctx->d_lut;
     t.nsm = nsm;
@@ -1454,6 +1455,7 @@ struct dspsr_b200_filterbank_during
     tw4.release ();
     ptab.release ();
     ptab_seg.release ();
+    ptab_col.release ();
     twd.release ();
     H.release ();
     tmp.release ();
@@ -1471,7 +1473,7 @@ int dspsr_b200_filterbank_during::init (dspsr_b200_context* c, const dspsr_b200_
   if (!during_supported (cfg.nsub, cfg.freq_res))
     return fail (ctx, DSPSR_B200_EINVAL,
                  "filterbank during: nsub=%u freq_res=%u unsupported (nsub a power of two in "
-                 "[2, 128], freq_res a power of two, nsub*freq_res in [16384, 262144])",
+                 "[2, 128], freq_res a power of two, nsub*freq_res in [16384, 4194304])",
                  cfg.nsub, cfg.freq_res);
   // Filterbank::do_prepare (Filterbank.C:155-196): nkeep = freq_res - nfilt_tot
   if (uint64_t (cfg.nfilt_pos) + cfg.nfilt_neg >= cfg.freq_res)
@@ -1498,10 +1500,12 @@ int dspsr_b200_filterbank_during::init (dspsr_b200_context* c, const dspsr_b200_
   B200_CHECK (ctx, twd.reserve (td.size ()), "cudaMalloc channel twiddles");
   B200_CHECK (ctx, cudaMemcpy (twd.ptr, td.data (), td.size () * sizeof (float2),
                                cudaMemcpyHostToDevice), "copy channel twiddles");
-  for (int which = 0; which < 2; which++)
+  // pass tables of the row, segment and (n1 >= 64) column transforms
+  for (int which = 0; which < 3; which++)
   {
-    const unsigned n = which ? s.seg : s.n2;
-    DevBuf<float2>& dst = which ? ptab_seg : ptab;
+    if (which == 2 && s.n1 < 64) break;
+    const unsigned n = which == 2 ? s.n1 : which ? s.seg : s.n2;
+    DevBuf<float2>& dst = which == 2 ? ptab_col : which ? ptab_seg : ptab;
     const unsigned cnt = pass_tables_count (n);
     std::vector<float2> pt (std::max (cnt, 1u), make_float2 (0.f, 0.f));
     make_pass_tables (n, pt.data (), cnt);

@@ -1334,6 +1334,151 @@ k_inv_cols_during (const float2* __restrict__ scratch, const DuringShape sh, con
   }
 }
 
+// Column passes of N1 = 64 .. 512 points (big transforms of up to 2^22 =
+// 512 x 8192 points): a CTA of N1 threads takes COLW = 16 adjacent columns,
+// loads them row by row (16 consecutive samples per row) into shared memory,
+// one column per group of N1/16 threads, and runs the N1-point Stockham
+// transforms there (per-pass tables in shared memory).  Column stride
+// spad_size(N1) + 1 keeps the 16 columns of a row on different banks.
+constexpr int COLW = 16;
+
+template <int N1>
+B200_CE int colbig_stride () { return spad_size (N1) + 1; }
+
+template <int N1, int NPOL>
+constexpr size_t colbig_smem ()
+{
+  return size_t (NPOL * COLW * colbig_stride<N1> () + pass_tables_size (N1)) * sizeof (float2);
+}
+
+// the N1-point transform (direction D) of every column in col[]
+template <int N1, int D>
+__device__ __forceinline__ void colbig_fft (float2* col, const float2* tab)
+{
+  constexpr int TS = stockham_threads (N1);
+  const int g = threadIdx.x / TS, lane = threadIdx.x % TS;
+  float2* base = col + g * colbig_stride<N1> ();
+  float2 v[16];
+  gpass<N1, D, 0, true> (lane, base, base, v, tab);
+  gpass<N1, D, 1, true> (lane, base, base, v, tab);
+  gpass<N1, D, 2, true> (lane, base, base, v, tab);
+}
+
+// Forward: unpack (and window) on load, N1-point DFTs down the columns, the
+// four-step twiddle w_N^{k1 i2}, rows of the scratch out.
+template <int N1, int KIND>
+__global__ void __launch_bounds__ (N1)
+k_fwd_cols_big (const InputView in, const float* __restrict__ lut, const uint64_t step,
+                const uint64_t part0, const unsigned n2, const float2* __restrict__ tw4,
+                const float2* __restrict__ ptab_col, float2* __restrict__ scratch,
+                const float* __restrict__ apod)
+{
+  static_assert (stockham_npass (N1) <= 3, "column transforms of at most three passes");
+  constexpr int T = N1;
+  constexpr int SP = colbig_stride<N1> ();
+  constexpr int TAB = pass_tables_size (N1);
+  extern __shared__ __align__ (16) float2 s_cb[];
+  float2* col = s_cb;
+  float2* tab = s_cb + COLW * SP;
+  __shared__ float s_lut[256];
+  load_lut (in, lut, s_lut);
+  for (int i = threadIdx.x; i < TAB; i += T) tab[i] = __ldg (ptab_col + i);
+  const unsigned c0 = blockIdx.x * COLW;
+  const unsigned b = blockIdx.y;
+  const unsigned c = blockIdx.z;
+  const uint64_t N = uint64_t (N1) * n2;
+  const uint64_t t0 = (part0 + b) * step + c0;
+  for (unsigned p = 0; p < in.npol; p++)
+  {
+    __syncthreads ();
+    for (int e = threadIdx.x; e < COLW * N1; e += T)
+    {
+      const int j = e % COLW, k = e / COLW;
+      float2 x = fetch<KIND> (in, s_lut, c, p, t0 + uint64_t (k) * n2 + j);
+      if (apod)
+      {
+        const float w = __ldg (apod + uint64_t (k) * n2 + c0 + j);
+        x = make_float2 (__fmul_rn (x.x, w), __fmul_rn (x.y, w));
+      }
+      col[j * SP + spad (k)] = x;
+    }
+    __syncthreads ();
+    colbig_fft<N1, -1> (col, tab);
+    float2* dst = scratch + ((uint64_t (b) * in.nchan + c) * in.npol + p) * N + c0;
+    for (int e = threadIdx.x; e < COLW * N1; e += T)
+    {
+      const int j = e % COLW, k1 = e / COLW;
+      float2 y = col[j * SP + spad (k1)];
+      if (k1) y = cmul (y, __ldg (tw4 + uint64_t (k1) * n2 + c0 + j));
+      dst[uint64_t (k1) * n2 + j] = y;
+    }
+  }
+}
+
+// Inverse columns of the During filterbank for N1 = 64 .. 512: the 16
+// columns of a CTA lie in one output channel's segment (seg >= 64); both
+// polarisations are loaded with the conjugate twiddle exp(+2 pi i k1 t2 /
+// freq_res), transformed, and read back in time order (16 consecutive
+// samples per row) for the discard and the voltages or detection + fold.
+template <int N1, int NPOL, int MODE, int NOUT>
+__global__ void __launch_bounds__ (N1)
+k_inv_cols_during_big (const float2* __restrict__ scratch, const DuringShape sh,
+                       const uint64_t part0, const float2* __restrict__ twd,
+                       const float2* __restrict__ ptab_col, const FoldView fv, const VoltView vv)
+{
+  constexpr int T = N1;
+  constexpr int SP = colbig_stride<N1> ();
+  constexpr int TAB = pass_tables_size (N1);
+  extern __shared__ __align__ (16) float2 s_cb[];
+  float2* tab = s_cb + NPOL * COLW * SP;
+  for (int i = threadIdx.x; i < TAB; i += T) tab[i] = __ldg (ptab_col + i);
+  const unsigned c0 = blockIdx.x * COLW;
+  const unsigned b = blockIdx.y;
+  const unsigned cin = blockIdx.z;
+  const uint64_t N = uint64_t (N1) * sh.n2;
+  const unsigned cs = c0 / sh.seg, t20 = c0 % sh.seg;
+  const unsigned c = cin * sh.nsub + cs;
+#pragma unroll
+  for (int p = 0; p < NPOL; p++)
+  {
+    const float2* src = scratch + ((uint64_t (b) * sh.nchan_in + cin) * NPOL + p) * N + c0;
+    float2* col = s_cb + p * COLW * SP;
+    for (int e = threadIdx.x; e < COLW * N1; e += T)
+    {
+      const int j = e % COLW, k1 = e / COLW;
+      float2 x = src[uint64_t (k1) * sh.n2 + j];
+      if (k1) x = cmulc (x, __ldg (twd + uint64_t (k1) * sh.seg + t20 + j));
+      col[j * SP + spad (k1)] = x;
+    }
+  }
+  __syncthreads ();
+#pragma unroll
+  for (int p = 0; p < NPOL; p++)
+    colbig_fft<N1, +1> (s_cb + p * COLW * SP, tab);
+  const uint64_t tbase = (part0 + b) * sh.nkeep;
+  const float2* c0p = s_cb;
+  const float2* c1p = s_cb + (NPOL - 1) * COLW * SP;
+  for (int e = threadIdx.x; e < COLW * N1; e += T)
+  {
+    const int j = e % COLW, t1 = e / COLW;
+    const uint64_t tl = uint64_t (t1) * sh.seg + t20 + j;
+    const bool ok = tl >= sh.nfilt_pos && tl < sh.nfilt_pos + sh.nkeep;
+    const uint64_t t = tbase + (tl - sh.nfilt_pos);
+    const float2 pv = c0p[j * SP + spad (t1)];
+    const float2 qv = c1p[j * SP + spad (t1)];
+    if constexpr (MODE == OUT_VOLTAGE)
+    {
+      if (ok)
+      {
+        vv.out[(uint64_t (c) * NPOL) * vv.span + t] = pv;
+        if (NPOL == 2) vv.out[(uint64_t (c) * NPOL + 1) * vv.span + t] = qv;
+      }
+    }
+    else
+      emit_fold<NOUT> (fv, c, NPOL, ok, t, pv, qv);
+  }
+}
+
 // --------------------------------------------------------------------------
 // response construction
 // --------------------------------------------------------------------------
@@ -2189,13 +2334,91 @@ cudaError_t run_during_n1 (const DuringShape& sh, const DuringTables& tb, const 
   return cudaGetLastError ();
 }
 
+template <int N1, int NPOL>
+void launch_inv_during_big (const DuringShape& sh, dim3 grid, const float2* scratch,
+                            uint64_t part0, const DuringTables& tb, int mode, const FoldView& fv,
+                            const VoltView& vv, cudaStream_t st)
+{
+  constexpr size_t smem = colbig_smem<N1, NPOL> ();
+  if (mode == OUT_VOLTAGE)
+  {
+    auto k = k_inv_cols_during_big<N1, NPOL, OUT_VOLTAGE, 1>;
+    cudaFuncSetAttribute (k, cudaFuncAttributeMaxDynamicSharedMemorySize, int (smem));
+    k<<<grid, N1, smem, st>>> (scratch, sh, part0, tb.twd, tb.ptab_col, fv, vv);
+    return;
+  }
+  auto k = NPOL == 1 || fv.nout == 1 ? k_inv_cols_during_big<N1, NPOL, OUT_FOLD, 1>
+         : fv.nout == 2 ? k_inv_cols_during_big<N1, NPOL, OUT_FOLD, 2>
+                        : k_inv_cols_during_big<N1, NPOL, OUT_FOLD, 4>;
+  cudaFuncSetAttribute (k, cudaFuncAttributeMaxDynamicSharedMemorySize, int (smem));
+  k<<<grid, N1, smem, st>>> (scratch, sh, part0, tb.twd, tb.ptab_col, fv, vv);
+}
+
+template <int N1>
+cudaError_t run_during_big (const DuringShape& sh, const DuringTables& tb, const InputView& in,
+                            uint64_t part0, unsigned nbatch, float2* scratch, int mode,
+                            const FoldView& fv, const VoltView& vv, cudaStream_t st,
+                            const KernelClock* clk)
+{
+  static_assert (colbig_smem<N1, 2> () <= 227u * 1024u, "column kernel shared memory");
+  const dim3 gcol (sh.n2 / COLW, nbatch, sh.nchan_in);
+  {
+    ClockScope cs (clk, KK_FWD_COLS, st);
+    constexpr size_t smem = colbig_smem<N1, 1> ();
+    if (in.kind == IN_INT8)
+    {
+      cudaFuncSetAttribute (k_fwd_cols_big<N1, IN_INT8>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, int (smem));
+      k_fwd_cols_big<N1, IN_INT8><<<gcol, N1, smem, st>>> (in, tb.lut, sh.in_step, part0, sh.n2,
+                                                          tb.tw4, tb.ptab_col, scratch, tb.apod);
+    }
+    else if (in.kind == IN_INT16)
+    {
+      cudaFuncSetAttribute (k_fwd_cols_big<N1, IN_INT16>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, int (smem));
+      k_fwd_cols_big<N1, IN_INT16><<<gcol, N1, smem, st>>> (in, tb.lut, sh.in_step, part0, sh.n2,
+                                                           tb.tw4, tb.ptab_col, scratch, tb.apod);
+    }
+    else
+    {
+      cudaFuncSetAttribute (k_fwd_cols_big<N1, IN_FLOAT>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, int (smem));
+      k_fwd_cols_big<N1, IN_FLOAT><<<gcol, N1, smem, st>>> (in, tb.lut, sh.in_step, part0, sh.n2,
+                                                           tb.tw4, tb.ptab_col, scratch, tb.apod);
+    }
+  }
+  const unsigned nrows = N1 * nbatch * sh.nchan_in * sh.npol;
+  cudaError_t e = cudaSuccess;
+  {
+    ClockScope cs (clk, KK_ROWS, st);
+    switch (sh.seg)
+    {
+      case 64: e = launch_rows_during<64> (nrows, scratch, sh, tb, st); break;
+      case 128: e = launch_rows_during<128> (nrows, scratch, sh, tb, st); break;
+      case 256: e = launch_rows_during<256> (nrows, scratch, sh, tb, st); break;
+      case 512: e = launch_rows_during<512> (nrows, scratch, sh, tb, st); break;
+      case 1024: e = launch_rows_during<1024> (nrows, scratch, sh, tb, st); break;
+      case 2048: e = launch_rows_during<2048> (nrows, scratch, sh, tb, st); break;
+      case 4096: e = launch_rows_during<4096> (nrows, scratch, sh, tb, st); break;
+      default: return cudaErrorInvalidValue;
+    }
+  }
+  if (e != cudaSuccess) return e;
+  ClockScope cs (clk, KK_INV_COLS, st);
+  if (sh.npol == 2)
+    launch_inv_during_big<N1, 2> (sh, gcol, scratch, part0, tb, mode, fv, vv, st);
+  else
+    launch_inv_during_big<N1, 1> (sh, gcol, scratch, part0, tb, mode, fv, vv, st);
+  return cudaGetLastError ();
+}
+
 } // namespace
 
 bool during_supported (unsigned nsub, unsigned freq_res)
 {
   if (nsub < 2 || nsub > 128 || (nsub & (nsub - 1))) return false;
   const uint64_t n = uint64_t (nsub) * freq_res;
-  return freq_res && (freq_res & (freq_res - 1)) == 0 && n >= 2 * DUR_N2 && n <= 32 * DUR_N2;
+  return freq_res && (freq_res & (freq_res - 1)) == 0 && n >= 2 * DUR_N2 && n <= 512 * DUR_N2;
 }
 
 cudaError_t launch_filterbank_during (const DuringShape& sh, const DuringTables& tb,
@@ -2216,6 +2439,13 @@ cudaError_t launch_filterbank_during (const DuringShape& sh, const DuringTables&
     case 8: return run_during_n1<8> (sh, tb, in, part0, nbatch, scratch, mode, fv, vv, st, clk);
     case 16: return run_during_n1<16> (sh, tb, in, part0, nbatch, scratch, mode, fv, vv, st, clk);
     case 32: return run_during_n1<32> (sh, tb, in, part0, nbatch, scratch, mode, fv, vv, st, clk);
+    case 64: return run_during_big<64> (sh, tb, in, part0, nbatch, scratch, mode, fv, vv, st, clk);
+    case 128:
+      return run_during_big<128> (sh, tb, in, part0, nbatch, scratch, mode, fv, vv, st, clk);
+    case 256:
+      return run_during_big<256> (sh, tb, in, part0, nbatch, scratch, mode, fv, vv, st, clk);
+    case 512:
+      return run_during_big<512> (sh, tb, in, part0, nbatch, scratch, mode, fv, vv, st, clk);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -182,7 +182,7 @@ bool ifb_supported_lin (unsigned lin);
 struct DuringShape
 {
   unsigned nchan_in, npol, nsub;
-  unsigned n1, n2, seg;          // nsub * freq_res = n1 * n2, seg = n2 / nsub
+  unsigned n1, n2, seg;          // nsub * freq_res = n1 * n2 (n1 <= 512), seg = n2 / nsub
   unsigned freq_res, nfilt_pos, nfilt_neg;
   uint64_t nkeep;                // freq_res - nfilt_pos - nfilt_neg
   uint64_t in_step;              // nsub * nkeep input samples between parts
@@ -194,6 +194,7 @@ struct DuringTables
   const float2* ptab;      // per-pass tables of the n2-point FFT
   const float2* ptab_seg;  // per-pass tables of the seg-point FFT
   const float2* twd;       // [n1][seg] exp(-2 pi i k1 t2 / freq_res)
+  const float2* ptab_col;  // per-pass tables of the n1-point FFT (n1 >= 64)
   const float2* H;         // [nchan_in*nsub][n1][seg]: bin k1 + n1*f2 of each channel
   const float* lut;        // 8-bit table for int8 input
   int nsm;

@@ -328,7 +328,7 @@ int dspsr_b200_inverse_filterbank_status (dspsr_b200_inverse_filterbank* ifb);
    input samples apart; npart = (ndat - nsub*(nfilt_pos+nfilt_neg)) /
    nsamp_step (Filterbank::resize_output, Filterbank.C:398-420).  Supported:
    nsub a power of two in [2, 128], freq_res a power of two, nsub * freq_res
-   in [16384, 262144]. */
+   in [16384, 4194304]. */
 typedef struct dspsr_b200_filterbank_during dspsr_b200_filterbank_during;
 typedef struct dspsr_b200_fbd_config
 {

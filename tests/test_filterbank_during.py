@@ -119,6 +119,13 @@ GPU_CASES = {
     # two channels of 65536 points (n1 = 16, 4096-point segments)
     "dedisp_2x65536_float": dict(nin=1, npol=1, nsub=2, fr=65536, dm=5.0, kind="float",
                                  npart=2),
+    # 2^19 points: 64-point columns in shared memory
+    "random_8x65536_float": dict(nin=1, npol=2, nsub=8, fr=65536, nfilt=(900, 1100),
+                                 kind="float", npart=2),
+    # the reference's C2 shape with the dedispersion inside the filterbank
+    # (-F 64:D at DM 500 over 256 MHz): 2^22 points, 512-point columns
+    "dedisp_64x65536_int8_dm500": dict(nin=1, npol=2, nsub=64, fr=65536, dm=500.0, bw=256.0,
+                                       kind="int8", npart=2),
 }
 CF, BW = 1400.0, 64.0
 
@@ -146,8 +153,9 @@ def test_during_gpu_matches_oracle(ctx, b2, orc, name):
     nin, npol, nsub, fr = case["nin"], case["npol"], case["nsub"], case["fr"]
     nchan = nin * nsub
     rng = np.random.default_rng(len(name))
+    bw = case.get("bw", BW)
     if "dm" in case:
-        half = b2.smearing_samples(CF, BW, case["dm"], nchan, 1)
+        half = b2.smearing_samples(CF, bw, case["dm"], nchan, 1)
         nfilt = (half, half)
     else:
         nfilt = case["nfilt"]
@@ -158,16 +166,16 @@ def test_during_gpu_matches_oracle(ctx, b2, orc, name):
     assert info["nsamp_fft"] == nsub * fr and info["nsamp_overlap"] == sum(nfilt) * nsub
     if "dm" in case:
         # the FP64-phase chirp against the FP64 response
-        fbd.set_dedispersion(CF, BW, case["dm"], swapped=True, chirp_mode=b2.CHIRP_FP64)
-        exact = orc.dedispersion_response_during(CF, BW, case["dm"], nchan, fr, nsub * fr,
+        fbd.set_dedispersion(CF, bw, case["dm"], swapped=True, chirp_mode=b2.CHIRP_FP64)
+        exact = orc.dedispersion_response_during(CF, bw, case["dm"], nchan, fr, nsub * fr,
                                                  swapped=True, fp64=True)
         assert rel_rms(fbd.get_response(), exact) < 1e-6
         # the reference's chirp (phases rounded to float, Dedispersion.C:104-111)
         # against the oracle's; the transforms are then checked with the
         # response the GPU holds, so that the float phases do not hide their error
-        fbd.set_dedispersion(CF, BW, case["dm"], swapped=True)
+        fbd.set_dedispersion(CF, bw, case["dm"], swapped=True)
         resp = fbd.get_response()
-        ref_resp = orc.dedispersion_response_during(CF, BW, case["dm"], nchan, fr, nsub * fr,
+        ref_resp = orc.dedispersion_response_during(CF, bw, case["dm"], nchan, fr, nsub * fr,
                                                     swapped=True)
         assert rel_rms(resp, ref_resp) < 1e-6, rel_rms(resp, ref_resp)
         resp64 = resp.astype(np.complex128)
@@ -205,7 +213,7 @@ def test_during_rejects_unsupported_shapes(ctx, b2):
     for nsub, fr, nfilt in [(256, 1024, (0, 0)),     # segments below 64 points
                             (3, 8192, (0, 0)),       # not a power of two
                             (8, 1024, (0, 0)),       # 8192 points: below the four-step split
-                            (64, 8192, (0, 0)),      # 2^19 points
+                            (128, 65536, (0, 0)),    # 2^23 points
                             (16, 1024, (600, 424))]:  # nothing kept
         with pytest.raises(b2.B200Error):
             b2.FilterbankDuring(ctx, 1, 2, nsub, fr, nfilt)
@@ -218,13 +226,14 @@ def test_during_rejects_unsupported_shapes(ctx, b2):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("state,npol", [(3, 2), (1, 2), (0, 1)])
-def test_during_fold_matches_its_voltages(ctx, b2, orc, state, npol):
+@pytest.mark.parametrize("state,npol,nsub,fr", [(3, 2, 32, 2048), (1, 2, 32, 2048), (0, 1, 32, 2048),
+                                                (3, 2, 16, 65536)])
+def test_during_fold_matches_its_voltages(ctx, b2, orc, state, npol, nsub, fr):
     """Detection and fold fused into the last pass give the profiles that the
     oracle's Detection and Fold make of the engine's own voltages (checked
     against the oracle above); hits bit-exact."""
     torch = pytest.importorskip("torch")
-    nsub, fr, dm, npart = 32, 2048, 10.0, 3
+    dm, npart = 10.0, 3
     half = b2.smearing_samples(CF, BW, dm, nsub, 1)
     fbd = b2.FilterbankDuring(ctx, 1, npol, nsub, fr, (half, half))
     fbd.set_dedispersion(CF, BW, dm)
