@@ -96,6 +96,58 @@ uint64_t FilterbankEngine::perform (const TimeSeriesView& in, TimeSeriesView& ou
   return n;
 }
 
+// ---- filterbank with a response --------------------------------------------
+
+FilterbankDuringEngine::~FilterbankDuringEngine ()
+{
+  if (fbd) dspsr_b200_filterbank_during_destroy (fbd);
+}
+
+void FilterbankDuringEngine::setup (unsigned input_nchan, unsigned npol, unsigned nchan_subband,
+                                    unsigned freq_res, unsigned nfilt_pos, unsigned nfilt_neg)
+{
+  if (fbd) dspsr_b200_filterbank_during_destroy (fbd);
+  fbd = nullptr;
+  dspsr_b200_fbd_config cfg {};
+  cfg.input_nchan = input_nchan;
+  cfg.npol = npol;
+  cfg.nsub = nchan_subband;
+  cfg.freq_res = freq_res;
+  cfg.nfilt_pos = nfilt_pos;
+  cfg.nfilt_neg = nfilt_neg;
+  ctx.check (dspsr_b200_filterbank_during_create (ctx.handle (), &cfg, &fbd),
+             "FilterbankDuringEngine::setup");
+  nsub = nchan_subband;
+  keep = freq_res - nfilt_pos - nfilt_neg;
+}
+
+void FilterbankDuringEngine::copy_response (const float* response)
+{
+  ctx.check (dspsr_b200_filterbank_during_copy_response (fbd, response),
+             "FilterbankDuringEngine::copy_response");
+}
+
+void FilterbankDuringEngine::set_dedispersion (double cf, double bw, double dm, bool swapped,
+                                               int chirp_mode)
+{
+  ctx.check (dspsr_b200_filterbank_during_set_dedispersion (fbd, cf, bw, dm, swapped ? 1 : 0,
+                                                            chirp_mode),
+             "FilterbankDuringEngine::set_dedispersion");
+}
+
+uint64_t FilterbankDuringEngine::perform (const TimeSeriesView& in, TimeSeriesView& out)
+{
+  if (out.nchan != in.nchan * nsub)
+    throw Error (DSPSR_B200_ESTATE, "FilterbankDuringEngine::perform: output nchan mismatch");
+  uint64_t npart = 0;
+  ctx.check (dspsr_b200_filterbank_during_perform (fbd, DSPSR_B200_FLOAT_FPT, in.base, in.ndat,
+                                                   in.span_floats / 2, nullptr, 0, out.base,
+                                                   out.span_floats / 2, &npart),
+             "FilterbankDuringEngine::perform");
+  out.ndat = npart * keep;
+  return npart;
+}
+
 // ---- detection -------------------------------------------------------------
 
 void DetectionEngine::square_law (const TimeSeriesView& in, TimeSeriesView& out)

@@ -97,6 +97,31 @@ private:
   unsigned nsub;
 };
 
+// CUDA::FilterbankEngine with a response (the "During" filterbank, -F N:D):
+// one nsub*freq_res-point FFT per part, the response, freq_res-point inverse
+// FFTs per output channel (FilterbankEngineCPU.C:379-535)
+class FilterbankDuringEngine
+{
+public:
+  explicit FilterbankDuringEngine (Context& ctx) : ctx (ctx) {}
+  ~FilterbankDuringEngine ();
+  // Engine::setup(Filterbank*): the sizes Filterbank::do_prepare computed
+  void setup (unsigned input_nchan, unsigned npol, unsigned nchan_subband, unsigned freq_res,
+              unsigned nfilt_pos, unsigned nfilt_neg);
+  // Engine::copy_response: [input_nchan*nchan_subband][freq_res] complex floats
+  void copy_response (const float* response);
+  void set_dedispersion (double centre_freq, double bandwidth, double dm, bool swapped = true,
+                         int chirp_mode = DSPSR_B200_CHIRP_REFERENCE);
+  // Engine::perform(in, out, npart, in_step, out_step); returns npart
+  uint64_t perform (const TimeSeriesView& input, TimeSeriesView& output);
+  uint64_t nkeep () const { return keep; }
+private:
+  Context& ctx;
+  dspsr_b200_filterbank_during* fbd = nullptr;
+  unsigned nsub = 0;
+  uint64_t keep = 0;
+};
+
 // CUDA::DetectionEngine
 class DetectionEngine
 {

@@ -1,6 +1,6 @@
 // engines_main.cpp -- drives the C++ engine classes the way DSPSR's operations
-// call their engines (unpack -> convolve -> detect -> fold) and checks them
-// against closed forms: a unit response returns the kept input scaled by
+// call their engines (unpack -> convolve -> detect -> fold, and the filterbank
+// with a response) and checks them against closed forms: a unit response returns the kept input scaled by
 // sqrt(nfft) (the Convolution normaliser of Convolution.C:401-414 left out),
 // detection of constant data, and fold bins equal to the reference's
 // sequential recurrence (Fold.C:815-818) run here on the host.
@@ -134,6 +134,66 @@ int main ()
              "profile[%u] %g != %g", b, prof[b], rprof[b]);
     }
     CHECK (fold.get_bin_hits (3) == rhits[3], "get_bin_hits");
+
+    // Filterbank::Engine with a unit response (normaliser 1/sqrt(N F)): a
+    // complex exponential at big-FFT bin k0 = c0*F + f0 comes out of output
+    // channel c0 as sqrt(nsub) exp(2 pi i f0 t / F) and nowhere else
+    {
+      const unsigned fsub = 16, fres = 1024, nbig = fsub * fres, c0 = 5, f0 = 37;
+      const uint64_t nd = 3 * uint64_t (nbig);
+      std::vector<float> hxin (nd * 2);
+      for (uint64_t t = 0; t < nd; t++)
+      {
+        const double a = 2 * M_PI * double ((uint64_t (c0) * fres + f0) * t % nbig) / nbig;
+        hxin[2 * t] = float (std::cos (a));
+        hxin[2 * t + 1] = float (std::sin (a));
+      }
+      float *d_in = nullptr, *d_out = nullptr;
+      cudaMalloc (&d_in, nd * 2 * sizeof (float));
+      cudaMalloc (&d_out, uint64_t (fsub) * nd * 2 * sizeof (float));
+      cudaMemcpy (d_in, hxin.data (), nd * 2 * sizeof (float), cudaMemcpyHostToDevice);
+      b200::FilterbankDuringEngine fb (ctx);
+      fb.setup (1, 1, fsub, fres, 0, 0);
+      std::vector<float> resp (uint64_t (fsub) * fres * 2, 0.f);
+      const float norm = float (1.0 / std::sqrt (double (nbig) * fres));
+      for (uint64_t k = 0; k < uint64_t (fsub) * fres; k++) resp[2 * k] = norm;
+      fb.copy_response (resp.data ());
+      b200::TimeSeriesView in;
+      in.base = d_in;
+      in.span_floats = nd * 2;
+      in.ndat = nd;
+      in.nchan = 1;
+      in.npol = 1;
+      b200::TimeSeriesView out = in;
+      out.base = d_out;
+      out.nchan = fsub;
+      const uint64_t np = fb.perform (in, out);
+      CHECK (np == 3 && out.ndat == 3 * uint64_t (fres), "filterbank during npart=%llu",
+             (unsigned long long) np);
+      std::vector<float> ho (uint64_t (fsub) * nd * 2);
+      ctx.synchronize ();
+      cudaMemcpy (ho.data (), d_out, ho.size () * 4, cudaMemcpyDeviceToHost);
+      double e2 = 0, r2 = 0, leak = 0;
+      const double amp = std::sqrt (double (fsub));
+      for (unsigned c = 0; c < fsub; c++)
+        for (uint64_t t = 0; t < out.ndat; t++)
+        {
+          const double re = ho[(c * nd + t) * 2], im = ho[(c * nd + t) * 2 + 1];
+          if (c != c0)
+          {
+            leak += re * re + im * im;
+            continue;
+          }
+          const double a = 2 * M_PI * double ((f0 * (t % fres)) % fres) / fres;
+          e2 += (re - amp * std::cos (a)) * (re - amp * std::cos (a))
+                + (im - amp * std::sin (a)) * (im - amp * std::sin (a));
+          r2 += amp * amp;
+        }
+      CHECK (std::sqrt (e2 / r2) < 1e-5, "filterbank during tone rel err %g", std::sqrt (e2 / r2));
+      CHECK (std::sqrt (leak / r2) < 1e-5, "filterbank during leakage %g", std::sqrt (leak / r2));
+      cudaFree (d_in);
+      cudaFree (d_out);
+    }
 
     cudaFree (d_raw);
     cudaFree (d_x);
