@@ -1351,6 +1351,18 @@ constexpr size_t colbig_smem ()
   return size_t (NPOL * COLW * colbig_stride<N1> () + pass_tables_size (N1)) * sizeof (float2);
 }
 
+// columns per CTA of the inverse pass: 8 for 512-point columns, so that both
+// polarisations (72 KB) leave room for a second CTA on the SM
+template <int N1>
+B200_CE int inv_colw () { return N1 >= 512 ? 8 : COLW; }
+
+template <int N1, int NPOL>
+constexpr size_t colbig_inv_smem ()
+{
+  return size_t (NPOL * inv_colw<N1> () * colbig_stride<N1> () + pass_tables_size (N1))
+         * sizeof (float2);
+}
+
 // the N1-point transform (direction D) of every column in col[]
 template <int N1, int D>
 __device__ __forceinline__ void colbig_fft (float2* col, const float2* tab)
@@ -1367,7 +1379,7 @@ __device__ __forceinline__ void colbig_fft (float2* col, const float2* tab)
 // Forward: unpack (and window) on load, N1-point DFTs down the columns, the
 // four-step twiddle w_N^{k1 i2}, rows of the scratch out.
 template <int N1, int KIND>
-__global__ void __launch_bounds__ (N1)
+__global__ void __launch_bounds__ (N1, 1024 / N1)
 k_fwd_cols_big (const InputView in, const float* __restrict__ lut, const uint64_t step,
                 const uint64_t part0, const unsigned n2, const float2* __restrict__ tw4,
                 const float2* __restrict__ ptab_col, float2* __restrict__ scratch,
@@ -1421,18 +1433,19 @@ k_fwd_cols_big (const InputView in, const float* __restrict__ lut, const uint64_
 // freq_res), transformed, and read back in time order (16 consecutive
 // samples per row) for the discard and the voltages or detection + fold.
 template <int N1, int NPOL, int MODE, int NOUT>
-__global__ void __launch_bounds__ (N1)
+__global__ void __launch_bounds__ (inv_colw<N1> () * stockham_threads (N1), 1024 / N1)
 k_inv_cols_during_big (const float2* __restrict__ scratch, const DuringShape sh,
                        const uint64_t part0, const float2* __restrict__ twd,
                        const float2* __restrict__ ptab_col, const FoldView fv, const VoltView vv)
 {
-  constexpr int T = N1;
+  constexpr int CW = inv_colw<N1> ();
+  constexpr int T = CW * stockham_threads (N1);
   constexpr int SP = colbig_stride<N1> ();
   constexpr int TAB = pass_tables_size (N1);
   extern __shared__ __align__ (16) float2 s_cb[];
-  float2* tab = s_cb + NPOL * COLW * SP;
+  float2* tab = s_cb + NPOL * CW * SP;
   for (int i = threadIdx.x; i < TAB; i += T) tab[i] = __ldg (ptab_col + i);
-  const unsigned c0 = blockIdx.x * COLW;
+  const unsigned c0 = blockIdx.x * CW;
   const unsigned b = blockIdx.y;
   const unsigned cin = blockIdx.z;
   const uint64_t N = uint64_t (N1) * sh.n2;
@@ -1442,10 +1455,10 @@ k_inv_cols_during_big (const float2* __restrict__ scratch, const DuringShape sh,
   for (int p = 0; p < NPOL; p++)
   {
     const float2* src = scratch + ((uint64_t (b) * sh.nchan_in + cin) * NPOL + p) * N + c0;
-    float2* col = s_cb + p * COLW * SP;
-    for (int e = threadIdx.x; e < COLW * N1; e += T)
+    float2* col = s_cb + p * CW * SP;
+    for (int e = threadIdx.x; e < CW * N1; e += T)
     {
-      const int j = e % COLW, k1 = e / COLW;
+      const int j = e % CW, k1 = e / CW;
       float2 x = src[uint64_t (k1) * sh.n2 + j];
       if (k1) x = cmulc (x, __ldg (twd + uint64_t (k1) * sh.seg + t20 + j));
       col[j * SP + spad (k1)] = x;
@@ -1454,13 +1467,13 @@ k_inv_cols_during_big (const float2* __restrict__ scratch, const DuringShape sh,
   __syncthreads ();
 #pragma unroll
   for (int p = 0; p < NPOL; p++)
-    colbig_fft<N1, +1> (s_cb + p * COLW * SP, tab);
+    colbig_fft<N1, +1> (s_cb + p * CW * SP, tab);
   const uint64_t tbase = (part0 + b) * sh.nkeep;
   const float2* c0p = s_cb;
-  const float2* c1p = s_cb + (NPOL - 1) * COLW * SP;
-  for (int e = threadIdx.x; e < COLW * N1; e += T)
+  const float2* c1p = s_cb + (NPOL - 1) * CW * SP;
+  for (int e = threadIdx.x; e < CW * N1; e += T)
   {
-    const int j = e % COLW, t1 = e / COLW;
+    const int j = e % CW, t1 = e / CW;
     const uint64_t tl = uint64_t (t1) * sh.seg + t20 + j;
     const bool ok = tl >= sh.nfilt_pos && tl < sh.nfilt_pos + sh.nkeep;
     const uint64_t t = tbase + (tl - sh.nfilt_pos);
@@ -2339,19 +2352,21 @@ void launch_inv_during_big (const DuringShape& sh, dim3 grid, const float2* scra
                             uint64_t part0, const DuringTables& tb, int mode, const FoldView& fv,
                             const VoltView& vv, cudaStream_t st)
 {
-  constexpr size_t smem = colbig_smem<N1, NPOL> ();
+  constexpr size_t smem = colbig_inv_smem<N1, NPOL> ();
+  constexpr int T = inv_colw<N1> () * stockham_threads (N1);
+  grid.x = sh.n2 / inv_colw<N1> ();
   if (mode == OUT_VOLTAGE)
   {
     auto k = k_inv_cols_during_big<N1, NPOL, OUT_VOLTAGE, 1>;
     cudaFuncSetAttribute (k, cudaFuncAttributeMaxDynamicSharedMemorySize, int (smem));
-    k<<<grid, N1, smem, st>>> (scratch, sh, part0, tb.twd, tb.ptab_col, fv, vv);
+    k<<<grid, T, smem, st>>> (scratch, sh, part0, tb.twd, tb.ptab_col, fv, vv);
     return;
   }
   auto k = NPOL == 1 || fv.nout == 1 ? k_inv_cols_during_big<N1, NPOL, OUT_FOLD, 1>
          : fv.nout == 2 ? k_inv_cols_during_big<N1, NPOL, OUT_FOLD, 2>
                         : k_inv_cols_during_big<N1, NPOL, OUT_FOLD, 4>;
   cudaFuncSetAttribute (k, cudaFuncAttributeMaxDynamicSharedMemorySize, int (smem));
-  k<<<grid, N1, smem, st>>> (scratch, sh, part0, tb.twd, tb.ptab_col, fv, vv);
+  k<<<grid, T, smem, st>>> (scratch, sh, part0, tb.twd, tb.ptab_col, fv, vv);
 }
 
 template <int N1>
@@ -2360,7 +2375,7 @@ cudaError_t run_during_big (const DuringShape& sh, const DuringTables& tb, const
                             const FoldView& fv, const VoltView& vv, cudaStream_t st,
                             const KernelClock* clk)
 {
-  static_assert (colbig_smem<N1, 2> () <= 227u * 1024u, "column kernel shared memory");
+  static_assert (colbig_inv_smem<N1, 2> () <= 227u * 1024u, "column kernel shared memory");
   const dim3 gcol (sh.n2 / COLW, nbatch, sh.nchan_in);
   {
     ClockScope cs (clk, KK_FWD_COLS, st);
