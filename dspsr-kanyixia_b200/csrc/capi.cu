@@ -1740,6 +1740,16 @@ int dspsr_b200_filterbank_during_perform_fold (dspsr_b200_filterbank_during* f, 
   return DSPSR_B200_OK;
 }
 
+int dspsr_b200_archive_profiles (const float* sums, const uint32_t* hits, int zeroed_data,
+                                 unsigned nchan, unsigned npol, unsigned nbin, double scale,
+                                 uint64_t ndat_total, int unload_zero_hits, float* amps,
+                                 float* weights, unsigned* corrupted)
+{
+  const int rc = archive_profiles (sums, hits, zeroed_data != 0, nchan, npol, nbin, scale,
+                                   ndat_total, unload_zero_hits != 0, amps, weights, corrupted);
+  return rc == 0 ? DSPSR_B200_OK : rc == -2 ? DSPSR_B200_ESTATE : DSPSR_B200_EINVAL;
+}
+
 int dspsr_b200_apodization (int type, unsigned ndat, unsigned transition_start,
                             unsigned transition_end, int swap_halves, float* window)
 {

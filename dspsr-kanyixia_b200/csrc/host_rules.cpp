@@ -662,4 +662,73 @@ int64_t build_fold_plan (double phi, double p, uint64_t ndat, std::vector<FoldSe
   return int64_t (segs.size ());
 }
 
+// Archiver::set(Pulsar::Profile*) (Archiver.C:852-984): the amplitude of bin
+// ibin is the folded sum over (scale * hits) in double, stored as float;
+// unhit bins take the double mean of the hit bins (Archiver.C:944-971);
+// a non-finite sum zeroes the profile and marks the channel corrupted, which
+// sets the channel's weight to 0 (Archiver.C:776-783).
+int archive_profiles (const float* sums, const uint32_t* hits, bool zeroed,
+                      unsigned nchan, unsigned npol, unsigned nbin, double scale,
+                      uint64_t ndat_total, bool unload_zero_hits, float* amps, float* weights,
+                      unsigned* corrupted)
+{
+  if (!sums || !hits || !amps || !weights || nchan == 0 || npol == 0 || nbin == 0)
+    return -1;
+  if (scale == 0 || !std::isfinite (scale)) return -1;
+  if (zeroed && ndat_total == 0) return -1;
+  unsigned bad = 0;
+  for (unsigned ic = 0; ic < nchan; ic++)
+  {
+    const uint32_t* h = hits + (zeroed ? uint64_t (ic) * nbin : 0);
+    bool chan_corrupt = false;
+    float chan_weight = 1.0f;
+    for (unsigned ip = 0; ip < npol; ip++)
+    {
+      const float* from = sums + (uint64_t (ic) * npol + ip) * nbin;
+      float* into = amps + (uint64_t (ic) * npol + ip) * nbin;
+      unsigned zeroes = 0, not_finite = 0;
+      uint32_t hits_sum = 0;
+      for (unsigned ib = 0; ib < nbin; ib++)
+      {
+        hits_sum += h[ib];
+        if (h[ib] == 0)
+        {
+          zeroes++;
+          into[ib] = 0.0f;
+        }
+        else if (!std::isfinite (from[ib]))
+          not_finite++;
+        else
+          into[ib] = float (double (from[ib]) / (scale * double (h[ib])));
+      }
+      if (not_finite)
+      {
+        for (unsigned ib = 0; ib < nbin; ib++) into[ib] = 0.0f;
+        chan_corrupt = true;
+        bad++;
+      }
+      if (zeroes)
+      {
+        if (!unload_zero_hits) return -2;
+        double sum = 0.0;
+        unsigned count = 0;
+        for (unsigned ib = 0; ib < nbin; ib++)
+          if (h[ib] != 0)
+          {
+            sum += into[ib];
+            count++;
+          }
+        if (count == 0) count = 1;
+        const double mean = sum / count;
+        for (unsigned ib = 0; ib < nbin; ib++)
+          if (h[ib] == 0) into[ib] = float (mean);
+      }
+      if (zeroed) chan_weight = float (hits_sum) / float (ndat_total);
+    }
+    weights[ic] = chan_corrupt ? 0.0f : chan_weight;
+  }
+  if (corrupted) *corrupted = bad;
+  return 0;
+}
+
 } // namespace b200

@@ -64,6 +64,21 @@ struct InterchannelDelays
 void interchannel_delays (double centre_frequency, double dm, double rate, const double* freq,
                           unsigned nchan, InterchannelDelays* out);
 
+// Archiver::set(Pulsar::Profile*, ...) (Signal/Pulsar/Archiver.C:852-984) with
+// Archiver::set(Integration*, ...) (:740-792) for the profiles of one
+// sub-integration: sums [nchan][npol][nbin], hits [nbin], or [nchan][nbin]
+// when the data were zeroed per channel (PhaseSeries::get_zeroed_data).  amps
+// get sum / (scale * hits); bins without hits are 0, or with
+// unload_zero_hits the mean of the hit bins; a profile holding a non-finite
+// sum is zeroed and its channel's weight set to 0; the weights [nchan] are
+// otherwise 1, or hits_sum / ndat_total for zeroed data.  Returns 0, -1 for
+// invalid arguments (a scale of 0 or not finite), -2 for bins without hits
+// when unload_zero_hits is false; *corrupted counts zeroed profiles.
+int archive_profiles (const float* sums, const uint32_t* hits, bool zeroed_data,
+                      unsigned nchan, unsigned npol, unsigned nbin, double scale,
+                      uint64_t ndat_total, bool unload_zero_hits, float* amps, float* weights,
+                      unsigned* corrupted);
+
 // Returns the number of segments; fills *out when non-null.  *x_end, when
 // non-null, receives the recurrence's phase after the last sample: the phi
 // with which the sequence goes on for the samples that follow.

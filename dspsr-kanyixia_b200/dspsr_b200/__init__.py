@@ -29,7 +29,7 @@ __all__ = ["Context", "Convolution", "InverseFilterbank", "FilterbankDuring", "F
            "smearing_samples", "minimum_ndat", "optimal_fft_length", "bittable8", "fold_phi",
            "sk_limits", "DADAFile", "dada_parse", "dada_is_valid", "ascii_header_get",
            "ascii_header_set", "write_dada", "TimeDivide", "interchannel_delays",
-           "fold_plan_count", "INTENSITY", "PPQQ", "COHERENCE", "STOKES", "INT8_TFPD",
+           "fold_plan_count", "archive_profiles", "INTENSITY", "PPQQ", "COHERENCE", "STOKES", "INT8_TFPD",
            "INT16_TFPD", "FLOAT_FPT", "CHIRP_REFERENCE", "CHIRP_FP64", "NOUT"]
 
 NOUT = {INTENSITY: 1, PPQQ: 2, COHERENCE: 4, STOKES: 4}
@@ -95,6 +95,28 @@ def apodization(kind, ndat, transition_start=0, transition_end=0, swap_halves=Fa
     if rc != _capi.OK:
         raise B200Error(rc, f"apodization: invalid type {kind} or size {ndat}")
     return w
+
+
+def archive_profiles(sums, hits, scale=1.0, zeroed_data=False, ndat_total=0,
+                     unload_zero_hits=False):
+    """Archiver::set for one sub-integration's profiles: sums (nchan, npol,
+    nbin), hits (nbin,) or (nchan, nbin) when zeroed_data -> (amps, weights,
+    corrupted)."""
+    s = np.ascontiguousarray(sums, np.float32)
+    nchan, npol, nbin = s.shape
+    h = np.ascontiguousarray(hits, np.uint32)
+    assert h.size == (nchan * nbin if zeroed_data else nbin)
+    amps = np.empty_like(s)
+    weights = np.empty(nchan, np.float32)
+    bad = ctypes.c_uint()
+    rc = _capi.lib().dspsr_b200_archive_profiles(
+        _fptr(s), h.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), int(zeroed_data), nchan,
+        npol, nbin, scale, ndat_total, int(unload_zero_hits), _fptr(amps), _fptr(weights),
+        ctypes.byref(bad))
+    if rc:
+        raise B200Error(rc, "archive_profiles: " + ("bins without hits" if rc == _capi.ESTATE
+                                                    else "invalid argument"))
+    return amps, weights, bad.value
 
 
 def fold_phi(start_mjd, epoch_mjd, idat_start, rate, period, reference_phase=0.0):

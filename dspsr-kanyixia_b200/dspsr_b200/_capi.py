@@ -231,6 +231,9 @@ SIGNATURES = {
     "dspsr_b200_filterbank_during_perform_fold": (c_int, [c_vp, c_int, c_vp, c_u64, c_u64, c_fp,
                                                           c_int, c_vp, c_int, c_u64p]),
     "dspsr_b200_apodization": (c_int, [c_int, c_uint, c_uint, c_uint, c_int, c_fp]),
+    "dspsr_b200_archive_profiles": (c_int, [c_fp, ctypes.POINTER(ctypes.c_uint32), c_int, c_uint,
+                                            c_uint, c_uint, c_dbl, c_u64, c_int, c_fp, c_fp,
+                                            ctypes.POINTER(c_uint)]),
     "dspsr_b200_sk": (c_int, [c_vp, c_vp, c_u64, c_u64, c_uint, c_uint, c_uint, c_int, c_uint,
                               ctypes.c_float, ctypes.c_float, c_vp, c_u64, c_vp, c_vp, c_vp, c_vp,
                               c_u64p]),

@@ -129,6 +129,22 @@ int dspsr_b200_interchannel_delays (double centre_freq_mhz, double dm, double ra
                                     const double* freq_mhz, unsigned nchan, int64_t* delay,
                                     double* frac, int64_t* applied, int64_t* zero_delay,
                                     uint64_t* total_delay);
+/* The profile arithmetic of the PhaseSeries -> archive unloader:
+   Archiver::set(Pulsar::Profile*) (Signal/Pulsar/Archiver.C:852-984) and the
+   channel weights of Archiver::set(Integration*) (:740-792), for one
+   sub-integration.  sums [nchan][npol][nbin] as the fold left them; hits
+   [nbin], or [nchan][nbin] when zeroed_data (PhaseSeries::get_zeroed_data);
+   scale = PhaseSeries::get_scale; ndat_total = get_ndat_total (zeroed data
+   only).  amps [nchan][npol][nbin] = sum / (scale * hits); unhit bins: an
+   error (DSPSR_B200_ESTATE, the reference's InvalidParam throw) unless
+   unload_zero_hits, then the mean of the hit bins; a profile with a
+   non-finite sum is zeroed and its channel's weight set to 0.  weights
+   [nchan]: 1, or hits_sum / ndat_total for zeroed data.  *corrupted (may
+   be NULL) counts the zeroed profiles.  Host only. */
+int dspsr_b200_archive_profiles (const float* sums, const uint32_t* hits, int zeroed_data,
+                                 unsigned nchan, unsigned npol, unsigned nbin, double scale,
+                                 uint64_t ndat_total, int unload_zero_hits, float* amps,
+                                 float* weights, unsigned* corrupted);
 /* Number of arithmetic segments the exact fold-bin plan needs for a block
    (see dspsr_b200_fold_set_bins); lets a caller size buffers. */
 int64_t dspsr_b200_fold_plan_count (double phi, double phase_per_sample,

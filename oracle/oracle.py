@@ -603,3 +603,58 @@ def sample_delay_block(y, applied, total):
     for c in range(y.shape[0]):
         out[c] = y[c, :, applied[c]:applied[c] + n]
     return out
+
+
+def archive_profiles(sums, hits, scale=1.0, zeroed_data=False, ndat_total=0,
+                     unload_zero_hits=False):
+    """Archiver::set(Pulsar::Profile*) (Signal/Pulsar/Archiver.C:852-984) and the
+    channel weights of Archiver::set(Integration*) (:740-792), restated with
+    Python scalars: amp = float32(float64(sum) / (scale * float64(hits)));
+    unhit bins 0, or (unload_zero_hits) the float64 mean of the hit bins; a
+    non-finite sum zeroes its profile and the channel's weight; weights 1, or
+    float32(hits_sum) / float32(ndat_total) for zeroed data.  Raises
+    ValueError where the reference throws for unhit bins."""
+    sums = np.asarray(sums, np.float32)
+    nchan, npol, nbin = sums.shape
+    hits = np.asarray(hits, np.uint32).reshape(nchan if zeroed_data else 1, nbin)
+    amps = np.zeros_like(sums)
+    weights = np.ones(nchan, np.float32)
+    corrupted = 0
+    for ic in range(nchan):
+        h = hits[ic if zeroed_data else 0]
+        bad_chan = False
+        w = np.float32(1.0)
+        for ip in range(npol):
+            src = sums[ic, ip]
+            out = amps[ic, ip]
+            zeroes = not_finite = 0
+            hits_sum = 0
+            for ib in range(nbin):
+                hits_sum = (hits_sum + int(h[ib])) & 0xffffffff
+                if h[ib] == 0:
+                    zeroes += 1
+                    out[ib] = 0.0
+                elif not np.isfinite(src[ib]):
+                    not_finite += 1
+                else:
+                    out[ib] = np.float32(float(src[ib]) / (scale * float(h[ib])))
+            if not_finite:
+                out[:] = 0.0
+                bad_chan = True
+                corrupted += 1
+            if zeroes:
+                if not unload_zero_hits:
+                    raise ValueError("bins without hits")
+                tot, cnt = 0.0, 0
+                for ib in range(nbin):
+                    if h[ib] != 0:
+                        tot += float(out[ib])
+                        cnt += 1
+                mean = tot / max(cnt, 1)
+                for ib in range(nbin):
+                    if h[ib] == 0:
+                        out[ib] = np.float32(mean)
+            if zeroed_data:
+                w = np.float32(np.float32(hits_sum) / np.float32(ndat_total))
+        weights[ic] = 0.0 if bad_chan else w
+    return amps, weights, corrupted
