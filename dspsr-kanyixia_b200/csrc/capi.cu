@@ -1430,9 +1430,10 @@ struct dspsr_b200_filterbank_during
 {
   dspsr_b200_context* ctx = nullptr;
   DuringShape shape {};
-  DevBuf<float2> tw4, ptab, ptab_seg, ptab_col, twd, H, tmp, scratch;
+  DevBuf<float2> tw4, ptab, ptab_seg, ptab_col, twd, H, Hw, tmp, scratch;
   DevBuf<double> chan_par;
-  bool have_response = false;
+  DevBuf<float> temporal, spectral;
+  bool have_response = false, have_temporal = false, have_spectral = false;
   int nsm = 148;
   unsigned max_batch = 1;
 
@@ -1444,11 +1445,18 @@ struct dspsr_b200_filterbank_during
     t.ptab_seg = ptab_seg.ptr;
     t.twd = twd.ptr;
     t.ptab_col = ptab_col.ptr;
-    t.H = H.ptr;
+    t.H = have_spectral ? Hw.ptr : H.ptr;
     t.lut = ctx->d_lut;
     t.nsm = nsm;
-    t.apod = nullptr;
+    t.apod = have_temporal ? temporal.ptr : nullptr;
     return t;
+  }
+  // the response the kernels read: H, times the spectral window when one is set
+  cudaError_t window_response ()
+  {
+    if (!have_spectral || !have_response) return cudaSuccess;
+    return launch_window_response (Hw.ptr, H.ptr, spectral.ptr, shape.nchan_in * shape.nsub,
+                                   shape.n1, shape.seg, ctx->stream);
   }
   void release ()
   {
@@ -1458,6 +1466,9 @@ struct dspsr_b200_filterbank_during
     ptab_col.release ();
     twd.release ();
     H.release ();
+    Hw.release ();
+    temporal.release ();
+    spectral.release ();
     tmp.release ();
     scratch.release ();
     chan_par.release ();
@@ -1582,8 +1593,9 @@ int dspsr_b200_filterbank_during_copy_response (dspsr_b200_filterbank_during* f,
   // bin k1 + n1*f2 of each channel to [chan][k1][f2]
   B200_CHECK (ctx, launch_permute_response (f->H.ptr, f->tmp.ptr, nchan, s.n1, s.seg, ctx->stream),
               "permute response");
-  B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "copy_response sync");
   f->have_response = true;
+  B200_CHECK (ctx, f->window_response (), "spectral window");
+  B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "copy_response sync");
   return DSPSR_B200_OK;
 }
 
@@ -1620,8 +1632,40 @@ int dspsr_b200_filterbank_during_set_dedispersion (dspsr_b200_filterbank_during*
                                        nchan, s.freq_res, s.n1, s.seg, binwidth, 0.5 * chanwidth,
                                        0, chirp_mode, scale, ctx->stream),
               "build chirp");
-  B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "set_dedispersion sync");
   f->have_response = true;
+  B200_CHECK (ctx, f->window_response (), "spectral window");
+  B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "set_dedispersion sync");
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_filterbank_during_set_apodization (dspsr_b200_filterbank_during* f,
+                                                   const float* temporal, const float* spectral)
+{
+  if (!f) return DSPSR_B200_EINVAL;
+  dspsr_b200_context* ctx = f->ctx;
+  const DuringShape& s = f->shape;
+  const uint64_t nfft = uint64_t (s.nsub) * s.freq_res;
+  B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "set_apodization sync");
+  f->have_temporal = false;
+  if (temporal)
+  {
+    B200_CHECK (ctx, f->temporal.reserve (nfft), "cudaMalloc temporal window");
+    B200_CHECK (ctx, cudaMemcpy (f->temporal.ptr, temporal, nfft * sizeof (float),
+                                 cudaMemcpyHostToDevice), "upload temporal window");
+    f->have_temporal = true;
+  }
+  f->have_spectral = false;
+  if (spectral)
+  {
+    B200_CHECK (ctx, f->spectral.reserve (s.freq_res), "cudaMalloc spectral window");
+    B200_CHECK (ctx, cudaMemcpy (f->spectral.ptr, spectral, s.freq_res * sizeof (float),
+                                 cudaMemcpyHostToDevice), "upload spectral window");
+    B200_CHECK (ctx, f->Hw.reserve (uint64_t (s.nchan_in) * s.nsub * s.freq_res),
+                "cudaMalloc windowed response");
+    f->have_spectral = true;
+    B200_CHECK (ctx, f->window_response (), "spectral window");
+    B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "set_apodization sync");
+  }
   return DSPSR_B200_OK;
 }
 

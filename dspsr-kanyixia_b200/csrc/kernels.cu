@@ -2429,6 +2429,31 @@ cudaError_t run_during_big (const DuringShape& sh, const DuringTables& tb, const
 
 } // namespace
 
+namespace {
+__global__ void k_window_response (float2* __restrict__ out, const float2* __restrict__ in,
+                                   const float* __restrict__ w, const uint64_t n,
+                                   const unsigned n1, const unsigned seg)
+{
+  const uint64_t idx = uint64_t (blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  const uint64_t fr = uint64_t (n1) * seg;
+  const unsigned r = unsigned (idx % fr);
+  const unsigned f = r / seg + n1 * (r % seg);
+  const float2 h = in[idx];
+  const float x = __ldg (w + f);
+  out[idx] = make_float2 (__fmul_rn (h.x, x), __fmul_rn (h.y, x));
+}
+} // namespace
+
+cudaError_t launch_window_response (float2* out, const float2* in, const float* window,
+                                    unsigned nchan, unsigned n1, unsigned seg, cudaStream_t st)
+{
+  const uint64_t n = uint64_t (nchan) * n1 * seg;
+  g_launches++;
+  k_window_response<<<unsigned ((n + 255) / 256), 256, 0, st>>> (out, in, window, n, n1, seg);
+  return cudaGetLastError ();
+}
+
 bool during_supported (unsigned nsub, unsigned freq_res)
 {
   if (nsub < 2 || nsub > 128 || (nsub & (nsub - 1))) return false;

@@ -202,6 +202,12 @@ struct DuringTables
 };
 
 bool during_supported (unsigned nsub, unsigned freq_res);
+// out = in x window[f] for every bin f = k1 + n1*f2 of the [nchan][n1][seg]
+// response layout (Apodization::operate on each channel's spectrum,
+// FilterbankEngineCPU.C:507-509, folded into the response)
+cudaError_t launch_window_response (float2* out, const float2* in, const float* window,
+                                    unsigned nchan, unsigned n1, unsigned seg,
+                                    cudaStream_t stream);
 // Parts [part0, part0 + nbatch); scratch holds nbatch*nchan_in*npol*n1*n2
 // values.  mode OUT_VOLTAGE writes the output channels (chan*npol + pol)*span;
 // OUT_FOLD detects and folds them (fold.nout products).

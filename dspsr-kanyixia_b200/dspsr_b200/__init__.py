@@ -426,6 +426,15 @@ class FilterbankDuring:
         self.ctx.check(self._lib.dspsr_b200_filterbank_during_set_dedispersion(
             self.handle, centre_freq, bandwidth, dm, int(swapped), chirp_mode), "set_dedispersion")
 
+    def set_apodization(self, temporal=None, spectral=None):
+        t = None if temporal is None else np.ascontiguousarray(temporal, np.float32)
+        sp = None if spectral is None else np.ascontiguousarray(spectral, np.float32)
+        assert t is None or t.size == self.nsub * self.freq_res
+        assert sp is None or sp.size == self.freq_res
+        self.ctx.check(self._lib.dspsr_b200_filterbank_during_set_apodization(
+            self.handle, None if t is None else _fptr(t), None if sp is None else _fptr(sp)),
+            "set_apodization")
+
     def get_response(self):
         out = np.empty(self.nchan * self.freq_res, np.complex64)
         self.ctx.check(self._lib.dspsr_b200_filterbank_during_get_response(

@@ -226,6 +226,7 @@ SIGNATURES = {
     "dspsr_b200_filterbank_during_set_dedispersion": (c_int, [c_vp, c_dbl, c_dbl, c_dbl,
                                                               c_int, c_int]),
     "dspsr_b200_filterbank_during_get_response": (c_int, [c_vp, c_fp]),
+    "dspsr_b200_filterbank_during_set_apodization": (c_int, [c_vp, c_fp, c_fp]),
     "dspsr_b200_filterbank_during_perform": (c_int, [c_vp, c_int, c_vp, c_u64, c_u64, c_fp, c_int,
                                                      c_vp, c_u64, c_u64p]),
     "dspsr_b200_filterbank_during_perform_fold": (c_int, [c_vp, c_int, c_vp, c_u64, c_u64, c_fp,

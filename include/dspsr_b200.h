@@ -378,6 +378,14 @@ int dspsr_b200_filterbank_during_set_dedispersion (dspsr_b200_filterbank_during*
                                                    double centre_freq_mhz,
                                                    double bandwidth_mhz, double dm,
                                                    int swapped, int chirp_mode);
+/* Filterbank::set_temporal_apodization / set_spectral_apodization
+   (Filterbank.C:201-207, applied at FilterbankEngineCPU.C:447-449, 507-509):
+   a window of nsub*freq_res floats multiplied into each part before the
+   forward FFT, and one of freq_res floats multiplied into each output
+   channel's spectrum before its inverse FFT (held folded into the response);
+   NULL removes either. */
+int dspsr_b200_filterbank_during_set_apodization (dspsr_b200_filterbank_during* fbd,
+                                                  const float* temporal, const float* spectral);
 /* copies the response back: [input_nchan*nsub][freq_res] complex, FFT order */
 int dspsr_b200_filterbank_during_get_response (dspsr_b200_filterbank_during* fbd,
                                                float* response);

@@ -110,14 +110,17 @@ uint64_t orc_filterbank_f64 (const double* in, uint64_t ndat, uint64_t in_span, 
 /* response: [nchan_in*nsub][freq_res] complex as Response holds it; out:
    (chan*npol + pol)*out_span, npart*(freq_res - nfilt) samples each.
    Returns npart. */
+/* temporal (nsub*freq_res) and spectral (freq_res) windows may be NULL */
 uint64_t orc_filterbank_during_f32 (const float* in, uint64_t ndat, uint64_t in_span,
                                     int nchan_in, int npol, unsigned nsub, unsigned freq_res,
                                     unsigned nfilt_pos, unsigned nfilt_neg, const float* response,
-                                    float* out, uint64_t out_span);
+                                    float* out, uint64_t out_span, const float* temporal,
+                                    const float* spectral);
 uint64_t orc_filterbank_during_f64 (const double* in, uint64_t ndat, uint64_t in_span,
                                     int nchan_in, int npol, unsigned nsub, unsigned freq_res,
                                     unsigned nfilt_pos, unsigned nfilt_neg, const double* response,
-                                    double* out, uint64_t out_span);
+                                    double* out, uint64_t out_span, const float* temporal,
+                                    const float* spectral);
 /* its dedispersion response: channels centred at chan_freq, natural frequency
    order within each channel, scaled by 1/sqrt(norm), norm = nsamp_fft*freq_res */
 void orc_dedispersion_response_during (const double* chan_freq, unsigned nchan, double bw,

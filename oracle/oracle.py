@@ -78,9 +78,11 @@ _SIGS = {
     "orc_filterbank_f32": (c_u64, [f32p, c_u64, c_u64, c_int, c_int, c_uint, f32p, c_u64]),
     "orc_filterbank_f64": (c_u64, [f64p, c_u64, c_u64, c_int, c_int, c_uint, f64p, c_u64]),
     "orc_filterbank_during_f32": (c_u64, [f32p, c_u64, c_u64, c_int, c_int, c_uint, c_uint,
-                                          c_uint, c_uint, f32p, f32p, c_u64]),
+                                          c_uint, c_uint, f32p, f32p, c_u64, ctypes.c_void_p,
+                                          ctypes.c_void_p]),
     "orc_filterbank_during_f64": (c_u64, [f64p, c_u64, c_u64, c_int, c_int, c_uint, c_uint,
-                                          c_uint, c_uint, f64p, f64p, c_u64]),
+                                          c_uint, c_uint, f64p, f64p, c_u64, ctypes.c_void_p,
+                                          ctypes.c_void_p]),
     "orc_dedispersion_response_during": (None, [f64p, c_uint, c_dbl, c_dbl, c_uint, c_int, c_dbl,
                                                 f32p]),
     "orc_dedispersion_response_during_f64": (None, [f64p, c_uint, c_dbl, c_dbl, c_uint, c_dbl,
@@ -232,8 +234,9 @@ def dedispersion_response_during(cf, bw, dm, nchan, freq_res, nsamp_fft, swapped
     return out.reshape(nchan, freq_res)
 
 
-def filterbank_during(x, nsub, freq_res, nfilt, response):
-    """x: complex (nchan_in, npol, ndat); response [nchan_in*nsub][freq_res] ->
+def filterbank_during(x, nsub, freq_res, nfilt, response, temporal=None, spectral=None):
+    """x: complex (nchan_in, npol, ndat); response [nchan_in*nsub][freq_res];
+    optional float windows temporal (nsub*freq_res) and spectral (freq_res) ->
     (nchan_in*nsub, npol, npart*(freq_res - nfilt_pos - nfilt_neg))."""
     nchan, npol, ndat = x.shape
     pos, neg = nfilt
@@ -248,8 +251,13 @@ def filterbank_during(x, nsub, freq_res, nfilt, response):
     r = np.ascontiguousarray(response, dt)
     assert r.shape == (nchan * nsub, freq_res)
     out = np.zeros((nchan * nsub, npol, max(npart * nkeep, 1)), dt)
+    tw = None if temporal is None else np.ascontiguousarray(temporal, np.float32)
+    sw = None if spectral is None else np.ascontiguousarray(spectral, np.float32)
+    assert tw is None or tw.size == nsub * freq_res
+    assert sw is None or sw.size == freq_res
     n = f(xin.view(rdt).ravel(), ndat, ndat, nchan, npol, nsub, freq_res, pos, neg,
-          r.view(rdt).ravel(), out.view(rdt).ravel(), out.shape[2])
+          r.view(rdt).ravel(), out.view(rdt).ravel(), out.shape[2],
+          None if tw is None else tw.ctypes.data, None if sw is None else sw.ctypes.data)
     assert n == npart
     return out[:, :, :npart * nkeep]
 

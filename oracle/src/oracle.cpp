@@ -661,7 +661,8 @@ uint64_t filterbank (const T* in, uint64_t ndat, uint64_t in_span, int nchan_in,
 template <typename T>
 uint64_t filterbank_during (const T* in, uint64_t ndat, uint64_t in_span, int nchan_in, int npol,
                             unsigned nsub, unsigned freq_res, unsigned nfilt_pos,
-                            unsigned nfilt_neg, const T* response, T* out, uint64_t out_span)
+                            unsigned nfilt_neg, const T* response, T* out, uint64_t out_span,
+                            const float* temporal = nullptr, const float* spectral = nullptr)
 {
   typedef std::complex<T> C;
   const uint64_t nsamp_fft = uint64_t (nsub) * freq_res;
@@ -671,13 +672,21 @@ uint64_t filterbank_during (const T* in, uint64_t ndat, uint64_t in_span, int nc
   const uint64_t npart = ndat > overlap ? (ndat - overlap) / step : 0;
   const unsigned nkeep = freq_res - nfilt_tot;
   const C* resp = reinterpret_cast<const C*> (response);
-  std::vector<C> spec (nsamp_fft), tmp (freq_res);
+  std::vector<C> spec (nsamp_fft), tmp (freq_res), win;
   for (int ic = 0; ic < nchan_in; ic++)
     for (uint64_t ipart = 0; ipart < npart; ipart++)
       for (int p = 0; p < npol; p++)
       {
         const C* x = reinterpret_cast<const C*> (in) + (uint64_t (ic) * npol + p) * in_span
                      + ipart * step;
+        if (temporal)
+        {
+          // Apodization::operate before the forward FFT (FilterbankEngineCPU.C:447-449)
+          win.resize (nsamp_fft);
+          for (uint64_t k = 0; k < nsamp_fft; k++)
+            win[k] = C (x[k].real () * T (temporal[k]), x[k].imag () * T (temporal[k]));
+          x = win.data ();
+        }
         fft<T> (int (nsamp_fft), -1, x, spec.data ());
         const C* h = resp + uint64_t (ic) * nsamp_fft;
         for (uint64_t k = 0; k < nsamp_fft; k++)
@@ -688,7 +697,12 @@ uint64_t filterbank_during (const T* in, uint64_t ndat, uint64_t in_span, int nc
         }
         for (unsigned cs = 0; cs < nsub; cs++)
         {
-          fft<T> (int (freq_res), +1, spec.data () + uint64_t (cs) * freq_res, tmp.data ());
+          C* chan = spec.data () + uint64_t (cs) * freq_res;
+          if (spectral)
+            // Apodization::operate on the channel's spectrum (FilterbankEngineCPU.C:507-509)
+            for (unsigned f = 0; f < freq_res; f++)
+              chan[f] = C (chan[f].real () * T (spectral[f]), chan[f].imag () * T (spectral[f]));
+          fft<T> (int (freq_res), +1, chan, tmp.data ());
           C* o = reinterpret_cast<C*> (out) + ((uint64_t (ic) * nsub + cs) * npol + p) * out_span
                  + ipart * nkeep;
           for (unsigned i = 0; i < nkeep; i++) o[i] = tmp[nfilt_pos + i];
@@ -739,19 +753,21 @@ void orc_dedispersion_response_during_f64 (const double* chan_freq, unsigned nch
 uint64_t orc_filterbank_during_f32 (const float* in, uint64_t ndat, uint64_t in_span,
                                     int nchan_in, int npol, unsigned nsub, unsigned freq_res,
                                     unsigned nfilt_pos, unsigned nfilt_neg, const float* response,
-                                    float* out, uint64_t out_span)
+                                    float* out, uint64_t out_span, const float* temporal,
+                                    const float* spectral)
 {
   return filterbank_during<float> (in, ndat, in_span, nchan_in, npol, nsub, freq_res, nfilt_pos,
-                                   nfilt_neg, response, out, out_span);
+                                   nfilt_neg, response, out, out_span, temporal, spectral);
 }
 
 uint64_t orc_filterbank_during_f64 (const double* in, uint64_t ndat, uint64_t in_span,
                                     int nchan_in, int npol, unsigned nsub, unsigned freq_res,
                                     unsigned nfilt_pos, unsigned nfilt_neg, const double* response,
-                                    double* out, uint64_t out_span)
+                                    double* out, uint64_t out_span, const float* temporal,
+                                    const float* spectral)
 {
   return filterbank_during<double> (in, ndat, in_span, nchan_in, npol, nsub, freq_res, nfilt_pos,
-                                    nfilt_neg, response, out, out_span);
+                                    nfilt_neg, response, out, out_span, temporal, spectral);
 }
 
 void orc_dedispersion_response_channels_f64 (const double* chan_freq, unsigned nchan, double bw,

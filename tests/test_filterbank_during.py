@@ -21,7 +21,7 @@ def rel_rms(a, b):
     return float(np.sqrt(np.mean(np.abs(a - b) ** 2) / np.mean(np.abs(b) ** 2)))
 
 
-def numpy_during(x, nsub, freq_res, nfilt, response):
+def numpy_during(x, nsub, freq_res, nfilt, response, temporal=None, spectral=None):
     """The same filterbank straight from its definition with numpy's FFT."""
     nin, npol, ndat = x.shape
     pos, neg = nfilt
@@ -34,9 +34,15 @@ def numpy_during(x, nsub, freq_res, nfilt, response):
         h = response[ic * nsub:(ic + 1) * nsub].reshape(-1)
         for ip in range(npart):
             for p in range(npol):
-                spec = np.fft.fft(x[ic, p, ip * step:ip * step + n]) * h
+                seg = x[ic, p, ip * step:ip * step + n]
+                if temporal is not None:
+                    seg = seg * temporal
+                spec = np.fft.fft(seg) * h
                 for cs in range(nsub):
-                    y = np.fft.ifft(spec[cs * freq_res:(cs + 1) * freq_res]) * freq_res
+                    chan = spec[cs * freq_res:(cs + 1) * freq_res]
+                    if spectral is not None:
+                        chan = chan * spectral
+                    y = np.fft.ifft(chan) * freq_res
                     out[ic * nsub + cs, p, ip * nkeep:(ip + 1) * nkeep] = y[pos:pos + nkeep]
     return out
 
@@ -57,6 +63,23 @@ def test_oracle_matches_numpy(orc, nin, npol, nsub, freq_res, nfilt):
     got32 = orc.filterbank_during(x.astype(np.complex64), nsub, freq_res, nfilt,
                                   h.astype(np.complex64))
     assert rel_rms(got32, ref) < 1e-5
+
+
+def test_oracle_windows_match_numpy(orc, b2):
+    """Filterbank::set_temporal_apodization / set_spectral_apodization: the
+    windows multiply each part before the forward FFT and each channel's
+    spectrum before its inverse FFT (FilterbankEngineCPU.C:447-449, 507-509)."""
+    rng = np.random.default_rng(11)
+    nsub, fr, nfilt = 8, 64, (6, 4)
+    nkeep = fr - sum(nfilt)
+    ndat = 3 * nsub * nkeep + sum(nfilt) * nsub
+    x = rng.standard_normal((1, 2, ndat)) + 1j * rng.standard_normal((1, 2, ndat))
+    h = rng.standard_normal((nsub, fr)) + 1j * rng.standard_normal((nsub, fr))
+    tw = b2.apodization(b2.APOD_TUKEY, nsub * fr, nfilt[0] * nsub, nfilt[1] * nsub)
+    sw = b2.apodization(b2.APOD_HANNING, fr)
+    ref = numpy_during(x, nsub, fr, nfilt, h, tw.astype(np.float64), sw.astype(np.float64))
+    got = orc.filterbank_during(x, nsub, fr, nfilt, h, temporal=tw, spectral=sw)
+    assert rel_rms(got, ref) < 1e-12
 
 
 def test_oracle_response_is_the_unswapped_channel_response(orc):
@@ -122,6 +145,9 @@ GPU_CASES = {
     # 2^19 points: 64-point columns in shared memory
     "random_8x65536_float": dict(nin=1, npol=2, nsub=8, fr=65536, nfilt=(900, 1100),
                                  kind="float", npart=2),
+    # temporal Tukey and spectral Hanning windows, 2^20 points (128-point columns)
+    "windows_16x65536_int16": dict(nin=1, npol=2, nsub=16, fr=65536, nfilt=(2000, 1500),
+                                   kind="int16", npart=2, windows=True),
     # the reference's C2 shape with the dedispersion inside the filterbank
     # (-F 64:D at DM 500 over 256 MHz): 2^22 points, 512-point columns
     "dedisp_64x65536_int8_dm500": dict(nin=1, npol=2, nsub=64, fr=65536, dm=500.0, bw=256.0,
@@ -186,10 +212,18 @@ def test_during_gpu_matches_oracle(ctx, b2, orc, name):
         fbd.copy_response(resp)
         assert np.array_equal(fbd.get_response(), resp)
         resp64 = resp.astype(np.complex128)
+    tw = sw = None
+    if case.get("windows"):
+        tw = b2.apodization(b2.APOD_TUKEY, nsub * fr, nfilt[0] * nsub, nfilt[1] * nsub)
+        sw = b2.apodization(b2.APOD_HANNING, fr)
+        fbd.set_apodization(tw, sw)
+        # the response read back is the one set, without the spectral window
+        assert np.array_equal(fbd.get_response(), resp)
     ndat = case["npart"] * nsub * nkeep + sum(nfilt) * nsub + 7      # a ragged tail
     raw, x, kind, lut = _input(rng, nin, npol, ndat, case["kind"], b2)
-    ref = orc.filterbank_during(x, nsub, fr, nfilt, resp)
-    ref64 = orc.filterbank_during(x.astype(np.complex128), nsub, fr, nfilt, resp64)
+    ref = orc.filterbank_during(x, nsub, fr, nfilt, resp, temporal=tw, spectral=sw)
+    ref64 = orc.filterbank_during(x.astype(np.complex128), nsub, fr, nfilt, resp64, temporal=tw,
+                                  spectral=sw)
     span = case["npart"] * nkeep + 3
     d_out = torch.full((nchan, npol, span, 2), float("nan"), device="cuda")
     if kind == b2.FLOAT_FPT:
