@@ -207,9 +207,9 @@ __device__ __forceinline__ unsigned warp_fold_bin (const FoldSegment* __restrict
 // All 32 lanes call this together.  Lanes holding consecutive time samples
 // with equal bins form runs; each run is summed by a segmented shuffle
 // reduction and added to the profile by its first lane with one atomic.
-template <int NOUT>
-__device__ __forceinline__ void warp_fold (bool ok, unsigned bin, const float* v,
-                                           float* prof, unsigned nbin, unsigned* hits)
+template <int NOUT, bool HITS>
+__device__ __forceinline__ void warp_fold_t (bool ok, unsigned bin, const float* v,
+                                             float* prof, unsigned nbin, unsigned* hits)
 {
   const int lane = threadIdx.x & 31;
   const unsigned key = ok ? bin : 0xffffffffu;
@@ -232,16 +232,31 @@ __device__ __forceinline__ void warp_fold (bool ok, unsigned bin, const float* v
       const float o = __shfl_down_sync (FULL, acc[k], off);
       if (take) acc[k] += o;
     }
-    const int oc = __shfl_down_sync (FULL, cnt, off);
-    if (take) cnt += oc;
+    if constexpr (HITS)
+    {
+      const int oc = __shfl_down_sync (FULL, cnt, off);
+      if (take) cnt += oc;
+    }
   }
   if (head && ok)
   {
 #pragma unroll
     for (int k = 0; k < NOUT; k++)
       atomicAdd (prof + uint64_t (k) * nbin + bin, acc[k]);
-    if (hits) atomicAdd (hits + bin, unsigned (cnt));
+    if constexpr (HITS) atomicAdd (hits + bin, unsigned (cnt));
   }
+}
+
+// Only the warps that count hits (one channel's) reduce the counts; hits is
+// the same pointer in every lane, so the choice is warp-uniform.
+template <int NOUT>
+__device__ __forceinline__ void warp_fold (bool ok, unsigned bin, const float* v,
+                                           float* prof, unsigned nbin, unsigned* hits)
+{
+  if (hits)
+    warp_fold_t<NOUT, true> (ok, bin, v, prof, nbin, hits);
+  else
+    warp_fold_t<NOUT, false> (ok, bin, v, prof, nbin, hits);
 }
 
 template <int NOUT>
