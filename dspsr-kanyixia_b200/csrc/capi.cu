@@ -613,6 +613,8 @@ struct dspsr_b200_pipeline
   void* pinned[2] = {nullptr, nullptr};   // run_dada: file blocks in page-locked memory
   uint64_t pinned_bytes = 0;
   cudaEvent_t host_free[2] = {nullptr, nullptr};   // uploads of pinned[b] done
+  cudaEvent_t snap_ev = nullptr;    // the last asynchronous profile snapshot landed
+  int* snap_err = nullptr;          // pinned copy of the row kernel's wait flag at the snapshot
   bool host_free_pending[2] = {false, false};
 };
 
@@ -2506,6 +2508,8 @@ int dspsr_b200_pipeline_destroy (dspsr_b200_pipeline* pl)
     if (pl->pinned[i]) cudaFreeHost (pl->pinned[i]);
     if (pl->host_free[i]) cudaEventDestroy (pl->host_free[i]);
   }
+  if (pl->snap_ev) cudaEventDestroy (pl->snap_ev);
+  if (pl->snap_err) cudaFreeHost (pl->snap_err);
   for (auto& u : pl->sub_pending) pl->sub_spare.push_back (u);   // undelivered: dropped
   for (auto& u : pl->sub_spare)
   {
@@ -2700,6 +2704,50 @@ int dspsr_b200_pipeline_get_profiles (dspsr_b200_pipeline* pl, float* profiles, 
   int rc = dspsr_b200_fold_get_profiles (&pl->fold, profiles, hits);
   if (rc) return rc;
   return pl->conv.status ();
+}
+
+int dspsr_b200_pipeline_get_profiles_async (dspsr_b200_pipeline* pl, float* profiles,
+                                            uint32_t* hits)
+{
+  if (!pl) return DSPSR_B200_EINVAL;
+  dspsr_b200_context* ctx = pl->ctx;
+  if (pl->sub_on)
+    return fail (ctx, DSPSR_B200_ESTATE,
+                 "pipeline_get_profiles_async: the pipeline folds sub-integrations; take them "
+                 "with pop_subint or an unloader");
+  if (!profiles && !hits) return fail (ctx, DSPSR_B200_EINVAL, "get_profiles_async: no buffer");
+  dspsr_b200_fold& f = pl->fold;
+  if (!pl->snap_ev)
+    B200_CHECK (ctx, cudaEventCreateWithFlags (&pl->snap_ev, cudaEventDisableTiming),
+                "cudaEventCreate");
+  if (!pl->snap_err)
+  {
+    B200_CHECK (ctx, cudaHostAlloc (&pl->snap_err, sizeof (int), cudaHostAllocDefault),
+                "cudaHostAlloc status");
+    *pl->snap_err = 0;
+  }
+  if (pl->conv.err.ptr)
+    B200_CHECK (ctx, cudaMemcpyAsync (pl->snap_err, pl->conv.err.ptr, sizeof (int),
+                                      cudaMemcpyDeviceToHost, ctx->stream), "read device status");
+  if (profiles)
+    B200_CHECK (ctx, cudaMemcpyAsync (profiles, f.profiles.ptr,
+                                      uint64_t (f.nchan) * f.npol * f.nbin * sizeof (float),
+                                      cudaMemcpyDeviceToHost, ctx->stream), "download profiles");
+  if (hits)
+    B200_CHECK (ctx, cudaMemcpyAsync (hits, f.hits.ptr, f.nbin * sizeof (unsigned),
+                                      cudaMemcpyDeviceToHost, ctx->stream), "download hits");
+  B200_CHECK (ctx, cudaEventRecord (pl->snap_ev, ctx->stream), "record snapshot");
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_pipeline_wait_profiles (dspsr_b200_pipeline* pl)
+{
+  if (!pl) return DSPSR_B200_EINVAL;
+  if (pl->snap_ev)
+    B200_CHECK (pl->ctx, cudaEventSynchronize (pl->snap_ev), "wait snapshot");
+  if (pl->snap_err && *pl->snap_err)
+    return fail (pl->ctx, DSPSR_B200_ESTATE, "a device-side wait timed out");
+  return DSPSR_B200_OK;
 }
 
 int dspsr_b200_pipeline_set_unloader (dspsr_b200_pipeline* pl, dspsr_b200_unload_fn fn,

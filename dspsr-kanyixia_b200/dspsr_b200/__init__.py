@@ -611,6 +611,24 @@ class Pipeline:
             self.handle, _fptr(prof), hits.ctypes.data_as(_capi.c_u32p)), "get_profiles")
         return prof, hits
 
+    def profile_buffers(self):
+        """Page-locked host arrays (profiles, hits) for get_profiles_async."""
+        import torch
+        c = self.config
+        nchan = c.nchan * (c.filterbank_nchan if c.filterbank_nchan > 1 else 1)
+        prof = torch.empty((nchan, self.nout, c.nbin), dtype=torch.float32, pin_memory=True)
+        hits = torch.empty(c.nbin, dtype=torch.int32, pin_memory=True)
+        return prof.numpy(), hits.numpy().view(np.uint32)
+
+    def get_profiles_async(self, prof, hits):
+        """Queue the copy of the profiles and hits so far into prof / hits
+        (from profile_buffers) and return; wait_profiles() waits for it."""
+        self.ctx.check(self._lib.dspsr_b200_pipeline_get_profiles_async(
+            self.handle, _fptr(prof), hits.ctypes.data_as(_capi.c_u32p)), "get_profiles_async")
+
+    def wait_profiles(self):
+        self.ctx.check(self._lib.dspsr_b200_pipeline_wait_profiles(self.handle), "wait_profiles")
+
     def reset(self):
         self.ctx.check(self._lib.dspsr_b200_pipeline_reset(self.handle), "pipeline_reset")
 

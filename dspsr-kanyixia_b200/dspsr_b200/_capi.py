@@ -251,6 +251,8 @@ SIGNATURES = {
     "dspsr_b200_pipeline_run": (c_int, [c_vp, c_vp, c_u64, c_u64, c_u64p]),
     "dspsr_b200_pipeline_run_host": (c_int, [c_vp, c_vp, c_u64, c_u64p]),
     "dspsr_b200_pipeline_get_profiles": (c_int, [c_vp, c_fp, c_u32p]),
+    "dspsr_b200_pipeline_get_profiles_async": (c_int, [c_vp, c_fp, ctypes.POINTER(ctypes.c_uint32)]),
+    "dspsr_b200_pipeline_wait_profiles": (c_int, [c_vp]),
     "dspsr_b200_pipeline_reset": (c_int, [c_vp]),
     "dspsr_b200_pipeline_info": (c_int, [c_vp, c_u64p]),
     "dspsr_b200_pipeline_profile": (c_int, [c_vp, c_int]),

@@ -547,6 +547,15 @@ int dspsr_b200_pipeline_run_host (dspsr_b200_pipeline* pipe, const void* h_in,
 /* profiles [chan][nout][nbin] and hits[nbin] into host memory */
 int dspsr_b200_pipeline_get_profiles (dspsr_b200_pipeline* pipe, float* profiles,
                                       uint32_t* hits);
+/* The same without waiting (PhaseSeries read back while the next block is
+   already on its way): queues the copies behind the blocks run so far and
+   returns; dspsr_b200_pipeline_wait_profiles waits for the latest such copy
+   and reports a timed-out device wait up to that point.  Give pinned host
+   memory (cudaHostAlloc) for copies that overlap; keep the buffers untouched
+   until the wait returns. */
+int dspsr_b200_pipeline_get_profiles_async (dspsr_b200_pipeline* pipe, float* profiles,
+                                            uint32_t* hits);
+int dspsr_b200_pipeline_wait_profiles (dspsr_b200_pipeline* pipe);
 int dspsr_b200_pipeline_reset (dspsr_b200_pipeline* pipe);
 /* Per-kernel timing: when enabled, CUDA events are recorded on the context's
    stream around every kernel of the convolution path (column pass, row pass,

@@ -334,6 +334,46 @@ def test_pipeline_host_upload_in_pieces(ctx, b2, nfft_mult):
     check(a[0], a[1], a[2], b[0].astype(np.float64), b[1], b[2], cfg["state"], rtol=1e-6)
 
 
+def test_pipeline_async_profiles_follow_each_block(ctx, b2):
+    """get_profiles_async queued after each host block, and waited for once
+    the next block is already queued, gives the profiles a synchronous
+    get_profiles gives after the same blocks."""
+    cfg = base_cfg(b2, dm=20.0, nfft=1 << 15, nbin=512, period=0.08933)
+    rng = np.random.default_rng(5)
+    blocks = make_blocks(rng, cfg, [9 * cfg["nfft"] + 333, 5 * cfg["nfft"], 9 * cfg["nfft"],
+                                    2 * cfg["nfft"] + 1])
+
+    def pipe():
+        c = b2.make_config(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nchan"], cfg["npol"],
+                           cfg["nfft"], cfg["pos"], cfg["neg"], cfg["nbin"], cfg["period"],
+                           state=cfg["state"], input_kind=cfg["kind"], lut=cfg["lut"],
+                           start_mjd=START, epoch_mjd=EPOCH)
+        return b2.Pipeline(ctx, c)
+
+    nsamp = [r.size // (cfg["nchan"] * cfg["npol"] * 2) for r in blocks]
+    pl = pipe()
+    want = []
+    for r, n in zip(blocks, nsamp):
+        pl.run_host(r, n)
+        want.append(pl.get_profiles())
+    pl.close()
+    pl = pipe()
+    bufs = [pl.profile_buffers(), pl.profile_buffers()]
+    got = []
+    for i, (r, n) in enumerate(zip(blocks, nsamp)):
+        pl.run_host(r, n)
+        if i:
+            pl.wait_profiles()
+            got.append(tuple(x.copy() for x in bufs[(i - 1) % 2]))
+        pl.get_profiles_async(*bufs[i % 2])
+    pl.wait_profiles()
+    got.append(tuple(x.copy() for x in bufs[(len(blocks) - 1) % 2]))
+    pl.close()
+    for (gp, gh), (wp, wh) in zip(got, want):
+        assert np.array_equal(gh, wh)
+        assert np.allclose(gp, wp, rtol=1e-6, atol=1e-6 * np.abs(wp).max())
+
+
 def test_pipeline_short_blocks_only_carry(ctx, b2):
     """Blocks shorter than one FFT fold nothing and are carried forward."""
     cfg = base_cfg(b2, dm=5.0)
