@@ -1326,9 +1326,6 @@ def run_b200_c3(args, cfg, world, rank, local):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    # each step's results come back asynchronously and are waited for once
-    # the next step's blocks are queued
-    bufs = [[s["pipe"].profile_buffers() for s in streams] for _ in range(2)]
     e0.record(default)
     for i in range(args.steps):
         for s in streams:
@@ -1337,14 +1334,7 @@ def run_b200_c3(args, cfg, world, rank, local):
             s["pipe"].run_host(h, s["ndat"])
         for s in streams:
             default.wait_stream(s["tstream"])
-        if i:
-            for s in streams:
-                s["pipe"].wait_profiles()
-        for s, b in zip(streams, bufs[i % 2]):
-            s["pipe"].get_profiles_async(*b)
-    for s in streams:
-        s["pipe"].wait_profiles()
-    profs = bufs[(args.steps - 1) % 2]
+        profs = [s["pipe"].get_profiles() for s in streams]
     e1.record(default)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
