@@ -796,7 +796,7 @@ k_inv_cols (const float2* __restrict__ scratch, const unsigned n2, const unsigne
     }
     float2 q[N1];
     inv_column<N1> (src + N, n2, tw4 + i2, n2, q);
-#pragma unroll
+#pragma unroll (N1 >= 32 ? 2 : N1)
     for (int k = 0; k < N1; k++)
     {
       const uint64_t tl = uint64_t (k) * n2 + i2;
@@ -1291,7 +1291,7 @@ k_inv_cols_during (const float2* __restrict__ scratch, const DuringShape sh, con
     float2 q[N1];
     inv_column<N1> (src + N, sh.n2, twd + t2, sh.seg, q);
     const uint64_t tb = (part0 + b) * sh.nkeep;
-#pragma unroll
+#pragma unroll (N1 >= 32 ? 2 : N1)
     for (int k = 0; k < N1; k++)
     {
       const uint64_t tl = uint64_t (k) * sh.seg + t2;
