@@ -1105,7 +1105,9 @@ def run_b200_fbd(args, cfg, world, rank, local):
         "config": {"workload": cfg["workload"], "npart": npart, "nkeep": nkeep,
                    "nfilt": 2 * half, "fft_split": [fbd.info["n1"], 8192],
                    "parts_per_batch": fbd.info["max_batch"],
-                   "l2": f"input {ndat * npol * 2 >> 20} MiB per step, larger than L2",
+                   "l2": (f"two distinct {ndat * npol * 2 >> 20} MiB input blocks alternate"
+                          + (", each larger than L2" if ndat * npol * 2 > (126 << 20)
+                             else " (profiling size: they fit in L2)")),
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "clocks": clk,
         "gpu_launches": int(launches),
