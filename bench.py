@@ -224,6 +224,9 @@ def ncu_traffic(kernel):
 # synthetic blocks
 # ---------------------------------------------------------------------------
 
+FFT_FORMS = {"fp32": 0, "bf16x2": 2, "bf16x3": 3}
+
+
 def make_blocks(cfg, seed, device):
     """NBLOCKS consecutive int8 TFPD blocks generated on the GPU (torch is the
     synthesis tool here; the product path never uses it)."""
@@ -347,6 +350,56 @@ def cpu_baseline(cfg, target_s=15.0):
                        f"(self-written FP32 FFT, OpenMP over parts), {total:.1f} s")}
 
 
+def parity_block(cfg, b2, ctx, pcfg, raw_dev, ndat, pos, neg, nfft, lut):
+    """One full block of the timed workload (its first block, a fresh
+    pipeline) against the oracle chain on the same bytes: unpack -> (the
+    filterbank) -> overlap-save -> detection -> fold with the block's phase
+    (Convolution.C:724-803, Fold.C:790-837).  Returns the max relative error of
+    the folded profiles (per bin, against the bin's total power) and whether
+    the hits are bit-exact."""
+    orc = cpu_prepare(cfg)[0]
+    pl = b2.Pipeline(ctx, pcfg)
+    nout = pl.run(raw_dev, ndat)
+    prof, hits = pl.get_profiles()
+    pl.close()
+    raw = raw_dev.cpu().numpy()
+    nc = nchan_conv(cfg)
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    x = orc.unpack8(raw, ndat, cfg["nchan"], cfg["npol"], 2, np.asarray(lut, np.float32))
+    x = x.view(np.complex64).reshape(cfg["nchan"], cfg["npol"], ndat)
+    if cfg["fb"]:
+        x = orc.filterbank(x, cfg["fb"])
+        freqs = orc.channel_centres(cfg["cf"], cfg["bw"], nc, swap=True, dc_centred=True)
+        h = orc.dedispersion_response_channels(freqs, cfg["bw"], cfg["dm"], nfft, mode=0)
+    else:
+        h = orc.dedispersion_response(cfg["cf"], cfg["bw"], cfg["dm"], 1, nfft, mode=0)
+    y = orc.convolve(x, h, nfft, pos, neg, nthreads=threads)
+    del x
+    d = orc.detect(y, cfg["state"])
+    rate = abs(cfg["bw"]) / nc * 1e6
+    phi = orc.fold_phi(START_MJD, EPOCH_MJD, pos, rate, cfg["period"])
+    plan = orc.fold_binplan(phi, (1.0 / rate) / cfg["period"], y.shape[2], cfg["nbin"])
+    del y
+    rprof, rhits = orc.fold_accumulate(d, plan, cfg["nbin"])
+    rprof = rprof.astype(np.float64)
+    # scale: the bin itself for intensity-like products, else total power
+    if cfg["state"] in (0, 1):
+        scale = np.abs(rprof)
+    else:
+        scale = np.broadcast_to(rprof[:, 0:1] if cfg["state"] == 3
+                                else rprof[:, 0:1] + rprof[:, 1:2], rprof.shape)
+    hit = rhits > 0
+    err = float(np.max(np.abs(prof.astype(np.float64) - rprof)[..., hit] / scale[..., hit]))
+    ok = bool(np.array_equal(hits, rhits)) and err < 1e-5 and int(nout) == int(d.shape[2])
+    return {"block": f"first timed block, {ndat} input samples/pol, fresh pipeline",
+            "samples_folded": int(nout), "oracle_samples": int(d.shape[2]),
+            "hits_bit_exact": bool(np.array_equal(hits, rhits)),
+            "max_profile_rel_err": err, "rtol": 1e-5, "pass": ok,
+            "oracle_s": round(time.perf_counter() - t0, 2),
+            "oracle": "CPU restatement (FP32, reference-mode chirp)"}
+
+
 def run_reference(args, cfg, world, rank):
     if rank != 0:
         return
@@ -443,6 +496,52 @@ def run_b200(args, cfg, world, rank, local):
     info = pl.info()
     prof, hits = pl.get_profiles()
     pl.close()
+
+    # the mixed-precision arms: the same workload with the convolution's row
+    # FFTs on the tensor cores (split-BF16 DFT GEMMs), timed the same way
+    mixed = {}
+    forms = [f for f in args.fft.split(",") if f in FFT_FORMS and f != "fp32"]
+    if info["n1"] > 1 and forms:
+        for form in forms:
+            cm = b2.make_config(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nchan"], cfg["npol"], nfft,
+                                pos, neg, cfg["nbin"], cfg["period"], state=cfg["state"],
+                                lut=lut, start_mjd=START_MJD, epoch_mjd=EPOCH_MJD,
+                                filterbank_nchan=cfg["fb"], scratch_bytes=args.scratch_mib << 20,
+                                fft_precision=FFT_FORMS[form])
+            pm = b2.Pipeline(ctx, cm)
+            for i in range(args.warmup):
+                pm.run(blocks[i % NBLOCKS], ndat)
+            torch.cuda.synchronize()
+            barrier(world)
+            torch.cuda.synchronize()
+            m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            m0.record()
+            for i in range(args.steps):
+                pm.run(blocks[(args.warmup + i) % NBLOCKS], ndat)
+            m1.record()
+            torch.cuda.synchronize()
+            mms = max_over_ranks(m0.elapsed_time(m1), world)
+            pm.profile(True)
+            for i in range(args.steps):
+                pm.run(blocks[(args.warmup + i) % NBLOCKS], ndat)
+            mk = pm.kernel_times()
+            pm.profile(False)
+            mprof, mhits = pm.get_profiles()
+            pm.close()
+            mval = samples_per_step * args.steps * world / (mms / 1e3) / 1e6
+            scale = np.maximum(np.abs(prof[:, :1].astype(np.float64)), 1e-30)
+            hit = hits > 0
+            mixed[form] = {
+                "value": round(mval, 3), "ms_per_step": round(mms / args.steps, 4),
+                "ratio_to_fp32": round(mval / value, 4),
+                "kernel_ms": {k: round(v[0], 3) for k, v in mk.items() if v[1]},
+                "profile_max_rel_diff_vs_fp32": float(np.max(
+                    np.abs(mprof.astype(np.float64) - prof)[..., hit]
+                    / np.broadcast_to(scale, prof.shape)[..., hit])),
+                "hits_equal_fp32": bool(np.array_equal(mhits, hits)),
+                "note": ("rows on the tensor cores (tcgen05.mma kind::f16, DFT16/DFT32 "
+                         f"stages, {form[-1]} BF16 terms per operand), columns, filterbank, "
+                         "detection and fold as in the FP32 arm")}
 
     # ---- end to end through the public API from pinned host memory ----------
     host = [b.cpu().pin_memory() for b in blocks]
@@ -627,12 +726,14 @@ def run_b200(args, cfg, world, rank, local):
                 "h2d_bytes_per_step": int(bytes_per_block), "d2h_bytes_per_step": int(d2h),
                 "readback": "each step's profiles copied back asynchronously and waited for "
                             "once the next block is queued"},
+        "mixed": mixed or None,
         "check": {"samples_folded": int(folded), "hits_total": int(hits.sum()),
                   "profile_peak_over_median": float(np.max(prof) / max(np.median(prof), 1e-30))},
     }
     line.update(extra)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg)
+        line["parity"] = parity_block(cfg, b2, ctx, c, blocks[0], ndat, pos, neg, nfft, lut)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -1587,6 +1688,10 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fft", default="fp32,bf16x3,bf16x2",
+                    help="row-FFT arithmetic forms to time (comma list of fp32, bf16x3, "
+                         "bf16x2); the first is the line's value, the others go under "
+                         "'mixed' with their ratio to it (nfft >= 16384 only)")
     ap.add_argument("--subint-seconds", type=float, default=0.0,
                     help="also time the device-resident run folding sub-integrations of this "
                          "length (TimeDivide), unloaded through the callback (c1/c2)")

@@ -247,4 +247,133 @@ void unpack8 (Context& ctx, const void* d_bytes, const float lut256[256], TimeSe
              "unpack8");
 }
 
+// ---- spectral kurtosis ------------------------------------------------------
+
+uint64_t SpectralKurtosisEngine::compute (const TimeSeriesView& in, SKSums& sums, unsigned M,
+                                          bool zero_is_valid)
+{
+  if (in.ndim != 2)
+    throw Error (DSPSR_B200_ESTATE, "SpectralKurtosisEngine::compute: complex data required");
+  uint64_t npart = 0;
+  ctx.check (dspsr_b200_sk_compute (ctx.handle (), in.base, in.span_floats / 2, in.ndat, in.nchan,
+                                    in.npol, M, zero_is_valid ? 1 : 0, sums.sums, sums.counts,
+                                    &npart),
+             "SpectralKurtosisEngine::compute");
+  sums.npart = npart;
+  sums.nchan = in.nchan;
+  sums.npol = in.npol;
+  sums.M = M;
+  return npart;
+}
+
+void SpectralKurtosisEngine::detect_ft (const SKSums& s, uint8_t* mask, float upper, float lower)
+{
+  ctx.check (dspsr_b200_sk_detect_ft (ctx.handle (), s.sums, s.counts, s.npart, s.nchan, s.npol,
+                                      s.M, nd, lower, upper, mask, nullptr),
+             "SpectralKurtosisEngine::detect_ft");
+}
+
+unsigned SpectralKurtosisEngine::detect_tscr (const SKSums& s, uint8_t* mask, float std_devs)
+{
+  uint32_t n = 0;
+  ctx.check (dspsr_b200_sk_detect_tscr (ctx.handle (), s.sums, s.counts, s.npart, s.nchan, s.npol,
+                                        s.M, nd, std_devs, mask, &n),
+             "SpectralKurtosisEngine::detect_tscr");
+  return n;
+}
+
+void SpectralKurtosisEngine::reset_mask (uint8_t* mask, uint64_t npart, unsigned nchan)
+{
+  ctx.check (dspsr_b200_sk_reset_mask (ctx.handle (), mask, npart, nchan),
+             "SpectralKurtosisEngine::reset_mask");
+}
+
+uint64_t SpectralKurtosisEngine::count_mask (const uint8_t* mask, uint64_t npart, unsigned nchan)
+{
+  uint64_t n = 0;
+  ctx.check (dspsr_b200_sk_count_mask (ctx.handle (), mask, npart, nchan, &n),
+             "SpectralKurtosisEngine::count_mask");
+  return n;
+}
+
+void SpectralKurtosisEngine::mask (const uint8_t* mask, const TimeSeriesView& in,
+                                   TimeSeriesView& out, unsigned M)
+{
+  ctx.check (dspsr_b200_sk_mask (ctx.handle (), mask, in.base, in.span_floats / 2, out.base,
+                                 out.span_floats / 2, in.ndat, in.nchan, in.npol, M),
+             "SpectralKurtosisEngine::mask");
+  out.ndat = (in.ndat / M) * M;
+}
+
+// ---- inverse filterbank -----------------------------------------------------
+
+InverseFilterbankEngine::~InverseFilterbankEngine ()
+{
+  if (ifb) dspsr_b200_inverse_filterbank_destroy (ifb);
+}
+
+void InverseFilterbankEngine::setup (const dspsr_b200_ifb_config& cfg)
+{
+  if (ifb) dspsr_b200_inverse_filterbank_destroy (ifb);
+  ifb = nullptr;
+  ctx.check (dspsr_b200_inverse_filterbank_create (ctx.handle (), &cfg, &ifb),
+             "InverseFilterbankEngine::setup");
+}
+
+void InverseFilterbankEngine::set_response (const float* response)
+{
+  ctx.check (dspsr_b200_inverse_filterbank_copy_response (ifb, response),
+             "InverseFilterbankEngine::set_response");
+}
+
+void InverseFilterbankEngine::set_apodization (const float* temporal, const float* spectral)
+{
+  ctx.check (dspsr_b200_inverse_filterbank_set_apodization (ifb, temporal, spectral),
+             "InverseFilterbankEngine::set_apodization");
+}
+
+uint64_t InverseFilterbankEngine::perform (const TimeSeriesView& in, TimeSeriesView& out)
+{
+  if (in.ndim != 2 || out.ndim != 2)
+    throw Error (DSPSR_B200_ESTATE, "InverseFilterbankEngine::perform: complex data required");
+  uint64_t npart = 0;
+  ctx.check (dspsr_b200_inverse_filterbank_perform (ifb, DSPSR_B200_FLOAT_FPT, in.base, in.ndat,
+                                                    in.span_floats / 2, nullptr, 0, out.base,
+                                                    out.span_floats / 2, &npart),
+             "InverseFilterbankEngine::perform");
+  const std::vector<uint64_t> i = info ();
+  out.ndat = npart * i[3];
+  return npart;
+}
+
+std::vector<uint64_t> InverseFilterbankEngine::info ()
+{
+  std::vector<uint64_t> v (10, 0);
+  ctx.check (dspsr_b200_inverse_filterbank_info (ifb, v.data ()), "InverseFilterbankEngine::info");
+  return v;
+}
+
+// ---- unpackers --------------------------------------------------------------
+
+void Unpacker::set_table (const float lut256[256])
+{
+  for (int i = 0; i < 256; i++) lut[i] = lut256[i];
+  have_lut = true;
+}
+
+void Unpacker::unpack (const void* d_words, TimeSeriesView& out)
+{
+  if (kind == EightBit)
+  {
+    if (!have_lut) throw Error (DSPSR_B200_ESTATE, "Unpacker::unpack: no 8-bit table set");
+    ctx.check (dspsr_b200_unpack8 (ctx.handle (), d_words, out.ndat, out.nchan, out.npol,
+                                   out.ndim, lut, out.base, out.span_floats),
+               "Unpacker::unpack (8-bit)");
+  }
+  else
+    ctx.check (dspsr_b200_unpack16 (ctx.handle (), d_words, out.ndat, out.nchan, out.npol,
+                                    out.ndim, offset_binary ? 1 : 0, out.base, out.span_floats),
+               "Unpacker::unpack (16-bit)");
+}
+
 } // namespace b200

@@ -13,6 +13,10 @@
 //   Detection::Engine    square_law / polarimetry               Detection.C:237-242, 483-489
 //   Fold::Engine         set_nbin / set_ndat / set_bins / fold  Fold.C:760-887, 1011-1035
 //                        get_bin_hits / synch
+//   SpectralKurtosis::Engine  setup / compute / detect_ft /     SpectralKurtosisCUDA.cu:28-104
+//                        detect_tscr / reset_mask / count_mask / mask
+//   InverseFilterbank::Engine setup / perform                   InverseFilterbank.C:215-228, 441-449
+//   Unpacker             matches / unpack / set_device          Unpacker.h:57-103
 //
 // A TimeSeriesView carries what those call sites read from a dsp::TimeSeries
 // (get_datptr(0,0), get_nfloat_span(), get_ndat(), get_nchan(), get_npol()).
@@ -165,5 +169,83 @@ private:
 // GenericEightBitUnpacker::unpack_on_gpu: TFPD bytes on the device -> FPT
 void unpack8 (Context& ctx, const void* d_bytes, const float lut256[256],
               TimeSeriesView& output);
+
+// The block layout of the SK engine's sums and mask: S1, S2 per
+// (part, chan, pol) as floats, counts and mask per (part, chan)
+struct SKSums
+{
+  float* sums = nullptr;        // [npart][nchan][npol][2], device
+  uint32_t* counts = nullptr;   // [npart][nchan], device (may be null: M counted)
+  uint64_t npart = 0;
+  unsigned nchan = 0, npol = 0, M = 0;
+};
+
+// CUDA::SpectralKurtosisEngine: the engine steps SpectralKurtosis::
+// transformation drives one after another (compute, detect_ft or detect_tscr,
+// count_mask, mask), each on the device
+class SpectralKurtosisEngine
+{
+public:
+  explicit SpectralKurtosisEngine (Context& ctx) : ctx (ctx) {}
+  // Engine::setup: the integrated samples per value (SpectralKurtosis's Nd)
+  void setup (unsigned Nd = 1) { nd = Nd; }
+  // Engine::compute(input, sums, sums_tscr, M): returns npart = ndat / M
+  uint64_t compute (const TimeSeriesView& input, SKSums& sums, unsigned M,
+                    bool zero_is_valid = true);
+  // Engine::detect_ft(sums, mask, upper, lower)
+  void detect_ft (const SKSums& sums, uint8_t* mask, float upper, float lower);
+  // Engine::detect_tscr: each channel over all parts; returns channels zapped
+  unsigned detect_tscr (const SKSums& sums, uint8_t* mask, float std_devs);
+  void reset_mask (uint8_t* mask, uint64_t npart, unsigned nchan);
+  uint64_t count_mask (const uint8_t* mask, uint64_t npart, unsigned nchan);
+  // Engine::mask(mask, input, output, M)
+  void mask (const uint8_t* mask, const TimeSeriesView& input, TimeSeriesView& output,
+             unsigned M);
+private:
+  Context& ctx;
+  unsigned nd = 1;
+};
+
+// InverseFilterbank's engine (InverseFilterbankEngineCPU.C:46-792 on the
+// device): setup with the configuration InverseFilterbank::make_preparations
+// derives, the response and apodizations, perform
+class InverseFilterbankEngine
+{
+public:
+  explicit InverseFilterbankEngine (Context& ctx) : ctx (ctx) {}
+  ~InverseFilterbankEngine ();
+  void setup (const dspsr_b200_ifb_config& config);
+  void set_response (const float* response);      // host, [output_nchan][Lout] complex
+  void set_apodization (const float* temporal, const float* spectral);
+  // Engine::perform(in, out, npart): complex FPT in and out; returns npart
+  uint64_t perform (const TimeSeriesView& input, TimeSeriesView& output);
+  // {kept bins, Lout, input step, output step, ...} as dspsr_b200_inverse_filterbank_info
+  std::vector<uint64_t> info ();
+private:
+  Context& ctx;
+  dspsr_b200_inverse_filterbank* ifb = nullptr;
+};
+
+// dsp::Unpacker on the device: GenericEightBitUnpacker (BitTable lookup) and
+// SixteenBitUnpacker (float(x) + 0.5, optional offset binary)
+class Unpacker
+{
+public:
+  enum Kind { EightBit, SixteenBit };
+  Unpacker (Context& ctx, Kind kind) : ctx (ctx), kind (kind) {}
+  // Unpacker::matches(const Observation*): NBIT of the data
+  bool matches (unsigned nbit) const { return nbit == (kind == EightBit ? 8u : 16u); }
+  // Unpacker::get_device_supported / set_device: always the device here
+  bool get_device_supported () const { return true; }
+  void set_table (const float lut256[256]);        // 8-bit: the BitTable values
+  void set_offset_binary (bool on) { offset_binary = on; }
+  // Unpacker::unpack: TFPD words on the device -> FPT
+  void unpack (const void* d_words, TimeSeriesView& output);
+private:
+  Context& ctx;
+  Kind kind;
+  float lut[256] = {};
+  bool have_lut = false, offset_binary = false;
+};
 
 } // namespace b200

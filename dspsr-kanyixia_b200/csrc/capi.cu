@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <map>
 #include <cstdint>
 #include <algorithm>
 #include <cstdarg>
@@ -23,15 +24,7 @@
 
 using namespace b200;
 
-struct dspsr_b200_context
-{
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  std::string error;
-  float* d_lut = nullptr;     // scratch LUT for the standalone unpacker
-  float2* d_fb_tab = nullptr; // pass tables of the standalone filterbank's FFT
-  unsigned fb_tab_n = 0;      // ... for this transform length
-};
+#include "context.h"
 
 namespace {
 
@@ -141,9 +134,13 @@ struct dspsr_b200_convolution
   DevBuf<double> chan_par;
   DevBuf<float> lut, apod;
   DevBuf<int> err;
+  DevBuf<uint8_t> tc_dft;
+  int tc_splits = 0;
   int nsm = 148;
   bool have_response = false, have_apod = false;
   unsigned max_batch = 1;
+
+  int set_fft_precision (int mode);
 
   int init (dspsr_b200_context* c, unsigned nchan, unsigned npol, unsigned nfft,
             unsigned pos, unsigned neg, uint64_t scratch_bytes);
@@ -158,10 +155,13 @@ struct dspsr_b200_convolution
     t.err = err.ptr;
     t.nsm = nsm;
     t.apod = have_apod ? apod.ptr : nullptr;
+    t.tc_dft = tc_dft.ptr;
+    t.tc_splits = tc_splits;
     return t;
   }
   void release ()
   {
+    tc_dft.release ();
     apod.release ();
     tw2.release ();
     tw4.release ();
@@ -574,6 +574,21 @@ struct dspsr_b200_pipeline
   int sd_cur = 0;
   uint64_t sd_ncarry = 0;           // voltages carried per row
   uint64_t sd_out0 = 0;             // SampleDelay output samples before this block
+  // SpectralKurtosis between the convolution and detection (LoadToFold1.C:
+  // 310-351 with the zero-DM input): dedispersed voltages in sk_v[sk_cur],
+  // zero-DM voltages in sk_z[sk_cur] (rows [chan][pol], sk_span values), the
+  // last len % M of them carried into the next block
+  bool sk_on = false;
+  unsigned sk_M = 0;
+  float sk_lower = 0.f, sk_upper = 0.f;
+  DevBuf<float2> sk_v[2], sk_z[2];
+  DevBuf<uint8_t> sk_mask;
+  DevBuf<unsigned long long> sk_zapped;
+  uint64_t sk_span = 0;
+  int sk_cur = 0;
+  uint64_t sk_ncarry = 0;
+  uint64_t sk_out0 = 0;             // SpectralKurtosis output samples before this block
+  uint64_t sk_tested = 0;           // (block, channel) cells tested
   DevBuf<float2> fbbuf;             // filterbank output, FPT
   float2* fb_tab = nullptr;         // pass tables of the filterbank FFT (fb_nsub >= 128)
   size_t fb_tab_cap = 0;
@@ -896,6 +911,113 @@ int pipeline_sd_block (dspsr_b200_pipeline* pl, const InputView& in, uint64_t np
   return DSPSR_B200_OK;
 }
 
+// One block through SpectralKurtosis (SpectralKurtosis::transformation with
+// one resolution, noverlap 1, the zero-DM input: compute on the zero-DM
+// voltages, detect_skfb, mask of the dedispersed voltages; SpectralKurtosis.C
+// 542-671) and the fold of zeroed data (Fold.C:895-930).  The SK blocks of M
+// samples run from the start of the stream; the samples after the last whole
+// block are carried (the zero-DM InputBuffering of SpectralKurtosis.C:43).
+int pipeline_sk_block (dspsr_b200_pipeline* pl, const InputView& in, uint64_t npart,
+                       uint64_t nout, const KernelClock* clk, uint64_t* folded)
+{
+  dspsr_b200_context* ctx = pl->ctx;
+  const ConvShape& sh = pl->conv.shape;
+  const auto& cfg = pl->cfg;
+  const uint64_t rows = uint64_t (sh.nchan) * cfg.npol;
+  const uint64_t len = pl->sk_ncarry + nout;
+  const unsigned M = pl->sk_M;
+  if (len > pl->sk_span)
+  {
+    // rows of an even number of samples keep every row 16-byte aligned
+    const uint64_t span = (len + len / 4 + 1) & ~uint64_t (1);
+    DevBuf<float2> nv[2], nz[2];
+    for (int i = 0; i < 2; i++)
+    {
+      B200_CHECK (ctx, nv[i].reserve (rows * span), "cudaMalloc sk voltages");
+      B200_CHECK (ctx, nz[i].reserve (rows * span), "cudaMalloc sk zero-DM");
+    }
+    if (pl->sk_ncarry)
+    {
+      B200_CHECK (ctx, cudaMemcpy2DAsync (nv[0].ptr, span * sizeof (float2),
+                                          pl->sk_v[pl->sk_cur].ptr, pl->sk_span * sizeof (float2),
+                                          pl->sk_ncarry * sizeof (float2), rows,
+                                          cudaMemcpyDeviceToDevice, ctx->stream), "sk carry");
+      B200_CHECK (ctx, cudaMemcpy2DAsync (nz[0].ptr, span * sizeof (float2),
+                                          pl->sk_z[pl->sk_cur].ptr, pl->sk_span * sizeof (float2),
+                                          pl->sk_ncarry * sizeof (float2), rows,
+                                          cudaMemcpyDeviceToDevice, ctx->stream), "sk carry");
+    }
+    B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "sk resize");
+    for (int i = 0; i < 2; i++)
+    {
+      pl->sk_v[i].release ();
+      pl->sk_z[i].release ();
+      std::swap (pl->sk_v[i], nv[i]);
+      std::swap (pl->sk_z[i], nz[i]);
+    }
+    pl->sk_span = span;
+    pl->sk_cur = 0;
+  }
+  float2* v = pl->sk_v[pl->sk_cur].ptr;
+  float2* z = pl->sk_z[pl->sk_cur].ptr;
+  FoldView fv0 {};
+  VoltView vv {v + pl->sk_ncarry, pl->sk_span};
+  const ConvTables tb = pl->conv.tables ();
+  for (uint64_t p0 = 0; p0 < npart; p0 += pl->conv.max_batch)
+  {
+    const unsigned nb = unsigned (std::min<uint64_t> (pl->conv.max_batch, npart - p0));
+    B200_CHECK (ctx, launch_convolution (sh, tb, in, p0, nb, pl->conv.scratch.ptr, OUT_VOLTAGE,
+                                         fv0, vv, ctx->stream, clk), "convolution kernels");
+  }
+  // the zero-DM output: the input samples aligned with the output
+  // (Convolution.C:789-796), nfilt_pos after the start of the block
+  B200_CHECK (ctx, launch_zero_dm (in, tb.lut, sh.nfilt_pos, nout, z + pl->sk_ncarry,
+                                   pl->sk_span, ctx->stream), "zero-DM output");
+  const uint64_t nblk = len / M;
+  const uint64_t out_n = nblk * M;
+  if (nblk)
+  {
+    B200_CHECK (ctx, pl->sk_mask.reserve (nblk * sh.nchan), "cudaMalloc sk mask");
+    // statistics and test of the zero-DM blocks (the kernel masks them in
+    // place too, which nothing reads), then the mask of the dedispersed ones
+    B200_CHECK (ctx, launch_sk (z, pl->sk_span, z, pl->sk_span, nblk, sh.nchan, cfg.npol, M, 1, 1,
+                                pl->sk_lower, pl->sk_upper, nullptr, nullptr, pl->sk_mask.ptr,
+                                pl->sk_zapped.ptr, ctx->stream), "spectral kurtosis");
+    B200_CHECK (ctx, launch_sk_apply (pl->sk_mask.ptr, v, pl->sk_span, out_n, sh.nchan, cfg.npol,
+                                      M, ctx->stream), "sk mask");
+    pl->sk_tested += nblk * sh.nchan;
+    int rc = pipeline_fold_plan (pl, pl->sk_out0, pl->sk_out0 + sh.nfilt_pos, out_n);
+    if (rc) return rc;
+    const FoldView fv = pl->fold.view (cfg.state, pl->nout, cfg.nchan);
+    B200_CHECK (ctx, launch_zeroed_fold (v, pl->sk_span, out_n, sh.nchan, cfg.npol, fv,
+                                         ctx->stream, clk), "zeroed fold");
+    rc = pl->fold.release_plan ();
+    if (rc) return rc;
+    if (pl->sub_on)
+    {
+      rc = subint_drain (pl, false);
+      if (rc) return rc;
+    }
+  }
+  const uint64_t keep = len - out_n;
+  if (keep)
+  {
+    B200_CHECK (ctx, cudaMemcpy2DAsync (pl->sk_v[pl->sk_cur ^ 1].ptr, pl->sk_span * sizeof (float2),
+                                        v + out_n, pl->sk_span * sizeof (float2),
+                                        keep * sizeof (float2), rows, cudaMemcpyDeviceToDevice,
+                                        ctx->stream), "sk carry");
+    B200_CHECK (ctx, cudaMemcpy2DAsync (pl->sk_z[pl->sk_cur ^ 1].ptr, pl->sk_span * sizeof (float2),
+                                        z + out_n, pl->sk_span * sizeof (float2),
+                                        keep * sizeof (float2), rows, cudaMemcpyDeviceToDevice,
+                                        ctx->stream), "sk carry");
+  }
+  pl->sk_cur ^= 1;
+  pl->sk_ncarry = keep;
+  pl->sk_out0 += out_n;
+  *folded = out_n;
+  return DSPSR_B200_OK;
+}
+
 int pipeline_block (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat_new,
                     uint64_t in_span, uint64_t* ndat_folded)
 {
@@ -933,6 +1055,12 @@ int pipeline_block (dspsr_b200_pipeline* pl, const void* d_in, uint64_t ndat_new
   {
     KernelClock kc {&PipeClock::mark, &pl->clock};
     int rc = pipeline_sd_block (pl, in, npart, nout, pl->clock.on ? &kc : nullptr, &nfolded);
+    if (rc) return rc;
+  }
+  else if (npart > 0 && pl->sk_on)
+  {
+    KernelClock kc {&PipeClock::mark, &pl->clock};
+    int rc = pipeline_sk_block (pl, in, npart, nout, pl->clock.on ? &kc : nullptr, &nfolded);
     if (rc) return rc;
   }
   else if (npart > 0)
@@ -1962,7 +2090,157 @@ int dspsr_b200_sk (dspsr_b200_context* ctx, const float* d_in, uint64_t in_span,
   return DSPSR_B200_OK;
 }
 
-// ---- unpack ----------------------------------------------------------------
+// ---- SpectralKurtosis::Engine, step by step --------------------------------
+// (CUDA::SpectralKurtosisEngine::compute / detect_ft / detect_tscr /
+// reset_mask / count_mask / mask, Signal/General/SpectralKurtosisCUDA.cu:
+// 45-99, with the host loops of SpectralKurtosis.C:674-798, 1012-1222,
+// 1465-1566)
+
+int dspsr_b200_sk_compute (dspsr_b200_context* ctx, const float* d_in, uint64_t in_span,
+                           uint64_t ndat, unsigned nchan, unsigned npol, unsigned M,
+                           int zero_is_valid, float* d_sums, uint32_t* d_counts,
+                           uint64_t* npart_out)
+{
+  if (!ctx) return DSPSR_B200_EINVAL;
+  if (npart_out) *npart_out = 0;
+  if (!d_in || !d_sums || nchan == 0 || nchan > 65535 || (npol != 1 && npol != 2))
+    return fail (ctx, DSPSR_B200_EINVAL, "sk_compute: invalid argument");
+  if (M < 2 || (M & 1) || (in_span & 1) || (reinterpret_cast<uintptr_t> (d_in) & 15))
+    return fail (ctx, DSPSR_B200_EINVAL, "sk_compute: M and the span must be even, the input "
+                 "16-byte aligned");
+  if (M > (1u << 20) || sk_smem_bytes (npol, M, 1) > SK_SMEM_MAX)
+    return fail (ctx, DSPSR_B200_EINVAL, "sk_compute: npol*M = %u exceeds the kernel's block",
+                 npol * M);
+  const uint64_t npart = ndat / M;
+  if (in_span < npart * M || npart > 0x7fffffffull)
+    return fail (ctx, DSPSR_B200_EINVAL, "sk_compute: span smaller than the blocks");
+  B200_CHECK (ctx, launch_sk (reinterpret_cast<const float2*> (d_in), in_span, nullptr, in_span,
+                              npart, nchan, npol, M, zero_is_valid, 1, -3.4e38f, 3.4e38f, d_sums,
+                              d_counts, nullptr, nullptr, ctx->stream), "sk compute");
+  if (npart_out) *npart_out = npart;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_sk_detect_ft (dspsr_b200_context* ctx, const float* d_sums,
+                             const uint32_t* d_counts, uint64_t npart, unsigned nchan,
+                             unsigned npol, unsigned M, unsigned Nd, float lower, float upper,
+                             uint8_t* d_mask, uint64_t* d_zapped)
+{
+  if (!ctx) return DSPSR_B200_EINVAL;
+  if (!d_sums || !d_mask || nchan == 0 || (npol != 1 && npol != 2) || Nd == 0 || M < 2)
+    return fail (ctx, DSPSR_B200_EINVAL, "sk_detect_ft: invalid argument");
+  B200_CHECK (ctx, launch_sk_detect (d_sums, d_counts, npart, nchan, npol, M, Nd, lower, upper,
+                                     d_mask, reinterpret_cast<unsigned long long*> (d_zapped),
+                                     ctx->stream), "sk detect_ft");
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_sk_detect_tscr (dspsr_b200_context* ctx, const float* d_sums,
+                               const uint32_t* d_counts, uint64_t npart, unsigned nchan,
+                               unsigned npol, unsigned M, unsigned Nd, float std_devs,
+                               uint8_t* d_mask, uint32_t* nzapped_chan)
+{
+  if (!ctx) return DSPSR_B200_EINVAL;
+  if (nzapped_chan) *nzapped_chan = 0;
+  if (!d_sums || !d_mask || nchan == 0 || (npol != 1 && npol != 2) || Nd == 0 || M < 2)
+    return fail (ctx, DSPSR_B200_EINVAL, "sk_detect_tscr: invalid argument");
+  if (npart == 0) return DSPSR_B200_OK;
+  // the time-scrunched sums are small: they are formed on the host as the
+  // reference does, in double over the float sums, then tested with the
+  // limits for each channel's count (SpectralKurtosis::get_limits)
+  std::vector<float> sums (npart * nchan * npol * 2);
+  std::vector<uint32_t> counts (npart * nchan, M);
+  B200_CHECK (ctx, cudaMemcpyAsync (sums.data (), d_sums, sums.size () * sizeof (float),
+                                    cudaMemcpyDeviceToHost, ctx->stream), "sk tscr sums");
+  if (d_counts)
+    B200_CHECK (ctx, cudaMemcpyAsync (counts.data (), d_counts, counts.size () * sizeof (uint32_t),
+                                      cudaMemcpyDeviceToHost, ctx->stream), "sk tscr counts");
+  B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "sk tscr sync");
+  std::map<uint64_t, std::pair<float, float>> limits;
+  uint32_t nz = 0;
+  for (unsigned c = 0; c < nchan; c++)
+  {
+    uint64_t count = 0;
+    for (uint64_t ip = 0; ip < npart; ip++) count += counts[ip * nchan + c];
+    if (count == 0) continue;
+    auto it = limits.find (count);
+    if (it == limits.end ())
+    {
+      float lo = 0.f, hi = 0.f;
+      const unsigned mc = unsigned (std::min<uint64_t> (count, 0xffffffffull));
+      if (sk_limits (mc, Nd, std_devs, npol, &lo, &hi) != 0)
+        return fail (ctx, DSPSR_B200_ESTATE, "sk_detect_tscr: no limits for count=%llu",
+                     (unsigned long long) count);
+      it = limits.emplace (count, std::make_pair (lo, hi)).first;
+    }
+    const float M_t = float (count);
+    // Equation (8) of Nita & Gary (2010b), as detect_tscr evaluates it
+    const float M_fac = (M_t * float (Nd) + 1) / (M_t - 1);
+    bool zap = false;
+    for (unsigned p = 0; p < npol; p++)
+    {
+      double S1 = 0.0, S2 = 0.0;
+      for (uint64_t ip = 0; ip < npart; ip++)
+      {
+        const uint64_t idx = (ip * nchan + c) * npol + p;
+        S1 += sums[idx * 2];
+        S2 += sums[idx * 2 + 1];
+      }
+      const double SK = M_fac * (M_t * (S2 / (S1 * S1)) - 1);
+      if (SK > it->second.second || SK < it->second.first) zap = true;
+    }
+    if (zap)
+    {
+      nz++;
+      B200_CHECK (ctx, cudaMemset2DAsync (d_mask + c, nchan, 1, 1, npart, ctx->stream),
+                  "sk tscr mask");
+    }
+  }
+  if (nzapped_chan) *nzapped_chan = nz;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_sk_reset_mask (dspsr_b200_context* ctx, uint8_t* d_mask, uint64_t npart,
+                              unsigned nchan)
+{
+  if (!ctx || !d_mask) return DSPSR_B200_EINVAL;
+  B200_CHECK (ctx, cudaMemsetAsync (d_mask, 0, npart * nchan, ctx->stream), "sk reset mask");
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_sk_count_mask (dspsr_b200_context* ctx, const uint8_t* d_mask, uint64_t npart,
+                              unsigned nchan, uint64_t* nzapped)
+{
+  if (!ctx || !d_mask || !nzapped) return DSPSR_B200_EINVAL;
+  std::vector<uint8_t> h (npart * nchan);
+  B200_CHECK (ctx, cudaMemcpyAsync (h.data (), d_mask, h.size (), cudaMemcpyDeviceToHost,
+                                    ctx->stream), "sk count mask");
+  B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "sk count mask");
+  uint64_t n = 0;
+  for (uint8_t v : h) n += v != 0;
+  *nzapped = n;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_sk_mask (dspsr_b200_context* ctx, const uint8_t* d_mask, const float* d_in,
+                        uint64_t in_span, float* d_out, uint64_t out_span, uint64_t ndat,
+                        unsigned nchan, unsigned npol, unsigned M)
+{
+  if (!ctx) return DSPSR_B200_EINVAL;
+  if (!d_mask || !d_in || !d_out || nchan == 0 || (npol != 1 && npol != 2) || M == 0)
+    return fail (ctx, DSPSR_B200_EINVAL, "sk_mask: invalid argument");
+  const uint64_t n = (ndat / M) * M;
+  if (in_span < n || out_span < n)
+    return fail (ctx, DSPSR_B200_EINVAL, "sk_mask: span smaller than the blocks");
+  if (d_in == d_out && in_span != out_span)
+    return fail (ctx, DSPSR_B200_EINVAL, "sk_mask: in-place masking needs equal spans");
+  B200_CHECK (ctx, launch_sk_mask (d_mask, reinterpret_cast<const float2*> (d_in), in_span,
+                                   reinterpret_cast<float2*> (d_out), out_span, n, nchan, npol, M,
+                                   ctx->stream), "sk mask");
+  return DSPSR_B200_OK;
+}
+
+// ---- unpack ----------------------------------------------------------------// ---- unpack ----------------------------------------------------------------
 
 int dspsr_b200_unpack8 (dspsr_b200_context* ctx, const void* d_in, uint64_t ndat,
                         unsigned nchan, unsigned npol, unsigned ndim, const float* lut256,
@@ -2126,6 +2404,38 @@ int dspsr_b200_filterbank (dspsr_b200_context* ctx, int input_kind, const void* 
                                       nullptr, ctx->d_fb_tab), "filterbank");
   if (ndat_out) *ndat_out = nblk;
   return DSPSR_B200_OK;
+}
+
+// The row FFTs in FP32 on the CUDA cores, or on the tensor cores with the
+// data and DFT operands split into 2 or 3 BF16 terms.
+int dspsr_b200_convolution::set_fft_precision (int mode)
+{
+  if (mode != DSPSR_B200_FFT_FP32 && mode != DSPSR_B200_FFT_BF16X2
+      && mode != DSPSR_B200_FFT_BF16X3)
+    return fail (ctx, DSPSR_B200_EINVAL, "fft precision: unknown mode %d", mode);
+  if (mode == DSPSR_B200_FFT_FP32)
+  {
+    tc_splits = 0;
+    return DSPSR_B200_OK;
+  }
+  if (shape.n1 < 2 || shape.n2 != 8192)
+    return fail (ctx, DSPSR_B200_EINVAL,
+                 "fft precision: the tensor-core rows need nfft >= 16384 (nfft=%u)", shape.nfft);
+  const unsigned ns = mode == DSPSR_B200_FFT_BF16X2 ? 2 : 3;
+  std::vector<uint8_t> img;
+  make_tc_dft_image (ns, img);
+  B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "sync before DFT upload");
+  B200_CHECK (ctx, tc_dft.reserve (img.size ()), "cudaMalloc DFT operands");
+  B200_CHECK (ctx, cudaMemcpy (tc_dft.ptr, img.data (), img.size (), cudaMemcpyHostToDevice),
+              "copy DFT operands");
+  tc_splits = int (ns);
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_convolution_set_fft_precision (dspsr_b200_convolution* c, int mode)
+{
+  if (!c) return DSPSR_B200_EINVAL;
+  return c->set_fft_precision (mode);
 }
 
 int dspsr_b200_convolution_set_temporal_apodization (dspsr_b200_convolution* c,
@@ -2369,6 +2679,8 @@ int dspsr_b200_pipeline_create (dspsr_b200_context* ctx, const dspsr_b200_pipeli
   pl->rate = std::fabs (cfg->bandwidth_mhz) / double (nchan) * 1e6;
   int rc = pl->conv.init (ctx, nchan, cfg->npol, cfg->nfft, cfg->nfilt_pos, cfg->nfilt_neg,
                           cfg->scratch_bytes);
+  if (!rc && cfg->fft_precision != DSPSR_B200_FFT_FP32)
+    rc = pl->conv.set_fft_precision (cfg->fft_precision);
   if (!rc && cfg->interchannel)
   {
     // DedispersionPipe::construct_interchan (DedispersionPipe.C:435-470): the
@@ -2465,7 +2777,32 @@ int dspsr_b200_pipeline_create (dspsr_b200_context* ctx, const dspsr_b200_pipeli
   // inside the forward column pass: its output never goes through memory
   pl->fb_fused = !rc && fb == 64 && cfg->nchan == 1 && cfg->npol == 2
                  && cfg->input_kind != DSPSR_B200_FLOAT_FPT && pl->conv.shape.n1 == 8
-                 && cfg->fused_filterbank >= 0;
+                 && cfg->fused_filterbank >= 0 && cfg->sk_M == 0;
+  // SpectralKurtosis between the convolution and detection: its zero-DM
+  // input needs the filterbank's channels in memory
+  if (!rc && cfg->sk_M)
+  {
+    if (cfg->sk_M < 4 || (cfg->sk_M & 1) || sk_smem_bytes (cfg->npol, cfg->sk_M, 1) > SK_SMEM_MAX)
+      rc = fail (ctx, DSPSR_B200_EINVAL, "pipeline: sk_M=%u must be even, >= 4 and fit the "
+                 "SK kernel's block", cfg->sk_M);
+    else if (cfg->interchannel)
+      rc = fail (ctx, DSPSR_B200_EINVAL, "pipeline: SpectralKurtosis with inter-channel "
+                 "dedispersion is not supported");
+    else
+    {
+      const float sd = cfg->sk_std_devs > 0.f ? cfg->sk_std_devs : 3.f;
+      if (sk_limits (cfg->sk_M, 1, sd, cfg->npol, &pl->sk_lower, &pl->sk_upper) != 0)
+        rc = fail (ctx, DSPSR_B200_EINVAL, "pipeline: no SK limits for M=%u", cfg->sk_M);
+      else if (pl->sk_zapped.reserve (1) != cudaSuccess
+               || cudaMemset (pl->sk_zapped.ptr, 0, sizeof (unsigned long long)) != cudaSuccess)
+        rc = fail (ctx, DSPSR_B200_ECUDA, "pipeline: sk counter");
+      else
+      {
+        pl->sk_on = true;
+        pl->sk_M = cfg->sk_M;
+      }
+    }
+  }
   // the carry never exceeds nfft samples: size both carry buffers once
   for (int i = 0; i < 2 && !rc; i++)
   {
@@ -2521,6 +2858,13 @@ int dspsr_b200_pipeline_destroy (dspsr_b200_pipeline* pl)
   pl->sd_applied.release ();
   pl->sd_buf[0].release ();
   pl->sd_buf[1].release ();
+  for (int i = 0; i < 2; i++)
+  {
+    pl->sk_v[i].release ();
+    pl->sk_z[i].release ();
+  }
+  pl->sk_mask.release ();
+  pl->sk_zapped.release ();
   delete pl;
   return DSPSR_B200_OK;
 }
@@ -2799,6 +3143,8 @@ int dspsr_b200_pipeline_reset (dspsr_b200_pipeline* pl)
   pl->in0 = 0;
   pl->sd_ncarry = 0;
   pl->sd_out0 = 0;
+  pl->sk_ncarry = 0;
+  pl->sk_out0 = 0;
   if (pl->sub_on)
   {
     const int rc = subint_drain (pl, true);      // unloads already started complete
@@ -2843,6 +3189,20 @@ int dspsr_b200_pipeline_kernel_times (dspsr_b200_pipeline* pl, double* ms, uint6
 }
 
 uint64_t dspsr_b200_kernel_launches (void) { return kernel_launches (); }
+
+int dspsr_b200_pipeline_sk_counts (dspsr_b200_pipeline* pl, uint64_t* zapped, uint64_t* tested)
+{
+  if (!pl || !zapped || !tested) return DSPSR_B200_EINVAL;
+  *zapped = *tested = 0;
+  if (!pl->sk_on) return DSPSR_B200_OK;
+  unsigned long long h = 0;
+  B200_CHECK (pl->ctx, cudaMemcpyAsync (&h, pl->sk_zapped.ptr, sizeof (h), cudaMemcpyDeviceToHost,
+                                        pl->ctx->stream), "sk count");
+  B200_CHECK (pl->ctx, cudaStreamSynchronize (pl->ctx->stream), "sk count");
+  *zapped = h;
+  *tested = pl->sk_tested;
+  return DSPSR_B200_OK;
+}
 
 int dspsr_b200_pipeline_info (dspsr_b200_pipeline* pl, uint64_t* info)
 {

@@ -660,12 +660,9 @@ k_rows_tma (float2* __restrict__ scratch, const float2* __restrict__ ptab,
   float2 v[16];
   for (; row < nrows; row += gridDim.x)
   {
-    if (!mbar_wait_bounded (&bar, parity))
-    {
-      if (tid == 0) atomicExch (err, 1);
-      mbar_wait_bounded (&bar, parity);   // let the copy in flight land
-      return;
-    }
+    // every thread polls the barrier (bounded); whether to give up is decided
+    // for the whole block at the barrier below, before anyone returns
+    const bool landed = mbar_wait_bounded (&bar, parity);
     parity ^= 1;
     const unsigned k1 = row % n1;
     const unsigned c = (row / n1 / npol) % nchan;
@@ -676,8 +673,18 @@ k_rows_tma (float2* __restrict__ scratch, const float2* __restrict__ ptab,
     {
       constexpr int R0 = stockham_radix (N2, 0);
       constexpr int D0 = CONV ? -1 : +1;
+      // (a thread whose wait gave up reads stale shared memory here; its
+      // values are dropped with the block's return below)
       StockhamPassT<N2, R0, T, D0, false, true>::load (tid, stage, v);
-      __syncthreads ();
+      if (__syncthreads_or (!landed))
+      {
+        if (tid == 0)
+        {
+          atomicExch (err, 1);
+          mbar_wait_bounded (&bar, parity ^ 1);   // let the copy in flight land
+        }
+        return;
+      }
       const unsigned next = row + gridDim.x;
       if (tid == 0 && next < nrows)
       {
@@ -1764,7 +1771,8 @@ k_sk (const float2* __restrict__ in, const uint64_t in_span, float2* out, const 
   const unsigned nu = unsigned (min (uint64_t (U), npart - part0));
   const unsigned Ms = sk_column (M);
   const unsigned n4 = M / 2;                      // float4 (two samples) per (block, pol)
-  const bool through = !(out == in && out_span == in_span);
+  // out == nullptr: statistics only (SpectralKurtosis::compute), nothing written back
+  const bool through = out && !(out == in && out_span == in_span);
   const bool two = npol == 2;
   if (threadIdx.x < U) s_zero[threadIdx.x] = 0;
   // both pols of the CTA's blocks are contiguous runs of nu*M samples
@@ -1885,6 +1893,7 @@ k_sk (const float2* __restrict__ in, const uint64_t in_span, float2* out, const 
   }
   __syncthreads ();
   // zero the zapped blocks; each thread overwrites exactly the float4s it wrote through
+  if (!out) return;
   const float4 zero = make_float4 (0.f, 0.f, 0.f, 0.f);
   for (unsigned f = threadIdx.x; f < total; f += SK_THREADS)
     if (s_zap[f / n4])
@@ -1984,6 +1993,122 @@ __global__ void k_delay_fold (const float2* __restrict__ v, const uint64_t span,
   emit_fold<NOUT> (fv, c, npol, ok, t, p, q);
 }
 
+// SpectralKurtosis::detect_skfb (SpectralKurtosis.C:1105-1222) from sums
+// already formed: per (part, chan), Mprime = counts (M when counts is null);
+// none counted leaves the mask as it is, one or two zap, otherwise the
+// estimator of each polarisation is tested in float as the reference does.
+// Zapped cells are set to 1 (others are left alone, as the reference leaves
+// them to reset_mask).
+__global__ void k_sk_detect (const float* __restrict__ sums, const unsigned* __restrict__ counts,
+                             const uint64_t ncell, const unsigned npol, const unsigned M,
+                             const unsigned Nd, const float lower, const float upper,
+                             uint8_t* __restrict__ mask, unsigned long long* __restrict__ nzap)
+{
+  const uint64_t unit = uint64_t (blockIdx.x) * blockDim.x + threadIdx.x;
+  if (unit >= ncell) return;
+  const unsigned Mprime = counts ? counts[unit] : M;
+  if (Mprime == 0) return;
+  bool zap = true;
+  if (Mprime > 2)
+  {
+    const float M_fac = __fdiv_rn (float (Mprime * Nd + 1), float (Mprime - 1));
+    zap = false;
+    for (unsigned p = 0; p < npol; p++)
+    {
+      const float S1 = sums[2 * (unit * npol + p)];
+      const float S2 = sums[2 * (unit * npol + p) + 1];
+      const float r = __fdiv_rn (S2, __fmul_rn (S1, S1));
+      const float V = __fmul_rn (M_fac, __fsub_rn (__fmul_rn (float (Mprime), r), 1.0f));
+      if (V > upper || V < lower) zap = true;
+    }
+  }
+  if (zap)
+  {
+    mask[unit] = 1;
+    if (nzap) atomicAdd (nzap, 1ull);
+  }
+}
+
+// SpectralKurtosis::mask (SpectralKurtosis.C:1465-1566): out = in, with the
+// blocks whose mask is set zeroed (in place when out == in: only those are
+// written).
+__global__ void k_sk_mask (const uint8_t* __restrict__ mask, const float2* in, const uint64_t in_span,
+                           float2* out, const uint64_t out_span, const uint64_t ndat,
+                           const unsigned nchan, const unsigned npol, const unsigned M)
+{
+  const uint64_t t = uint64_t (blockIdx.x) * blockDim.x + threadIdx.x;
+  const unsigned c = blockIdx.y;
+  if (t >= ndat) return;
+  const bool zap = __ldg (mask + (t / M) * nchan + c) != 0;
+  const bool inplace = in == out && in_span == out_span;
+  for (unsigned p = 0; p < npol; p++)
+  {
+    const uint64_t r = uint64_t (c) * npol + p;
+    if (zap) out[r * out_span + t] = make_float2 (0.f, 0.f);
+    else if (!inplace) out[r * out_span + t] = in[r * in_span + t];
+  }
+}
+
+// Convolution's zero-DM output (Convolution.C:175-193, 789-796) for the
+// pipeline: input sample first + t of every (chan, pol), unpacked, into
+// out[(c*npol + p)*span + t]
+template <int KIND>
+__global__ void k_zero_dm (const InputView in, const float* __restrict__ lut, const uint64_t first,
+                           const uint64_t n, float2* __restrict__ out, const uint64_t span)
+{
+  __shared__ float s_lut[256];
+  if constexpr (KIND == IN_INT8) load_lut (in, lut, s_lut);
+  __syncthreads ();
+  const uint64_t t = uint64_t (blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const unsigned row = blockIdx.y, c = row / in.npol, p = row % in.npol;
+  out[uint64_t (row) * span + t] = fetch<KIND> (in, s_lut, c, p, first + t);
+}
+
+// SpectralKurtosis::mask (SpectralKurtosis.C:1465-1566) applied to other
+// voltages than the statistics came from (the dedispersed ones, when the
+// statistics are of the zero-DM input): block t / M of channel c is zeroed
+// in every polarisation where mask[(t / M) * nchan + c] is set.
+__global__ void k_sk_apply (const uint8_t* __restrict__ mask, float2* __restrict__ v,
+                            const uint64_t span, const uint64_t ndat, const unsigned nchan,
+                            const unsigned npol, const unsigned M)
+{
+  const uint64_t t = uint64_t (blockIdx.x) * blockDim.x + threadIdx.x;
+  const unsigned c = blockIdx.y;
+  if (t >= ndat || !__ldg (mask + (t / M) * nchan + c)) return;
+  for (unsigned p = 0; p < npol; p++) v[(uint64_t (c) * npol + p) * span + t] = make_float2 (0.f, 0.f);
+}
+
+// Detection and Fold::fold of data with zeroed samples (Fold.C:895-930,
+// zeroed_samples): every sample is added to its bin, and a hit is counted
+// for each channel whose first detected value of the first polarisation is
+// non-zero -- into the one hits array shared by all channels.
+template <int NOUT>
+__global__ void k_zeroed_fold (const float2* __restrict__ v, const uint64_t span,
+                               const uint64_t ndat, const unsigned npol, const FoldView fv)
+{
+  const uint64_t t = uint64_t (blockIdx.x) * blockDim.x + threadIdx.x;
+  const unsigned c = blockIdx.y;
+  bool ok = t < ndat;
+  if (!__any_sync (FULL, ok)) return;
+  float2 p = make_float2 (0.f, 0.f), q = make_float2 (0.f, 0.f);
+  if (ok)
+  {
+    p = v[(uint64_t (c) * npol) * span + t];
+    if (npol == 2) q = v[(uint64_t (c) * npol + 1) * span + t];
+  }
+  float d[4] = {0.f, 0.f, 0.f, 0.f};
+  const unsigned bin = fv.cols ? (ok ? __ldg (fv.cols + t) : NO_COLUMN)
+                               : warp_fold_bin (fv.segs, fv.nseg, ok, t, fv.nbin);
+  if (ok)
+  {
+    detect_values (fv.state, npol, p, q, d);
+    // a zeroed sample adds nothing to the profile and counts no hit
+    ok = bin < fv.stride && d[0] != 0.f;
+  }
+  warp_fold<NOUT> (ok, bin, d, fv.profiles + uint64_t (c) * NOUT * fv.stride, fv.stride, fv.hits);
+}
+
 // one thread per sample: the column warp_fold_bin would give it
 __global__ void k_colplan (const FoldSegment* __restrict__ segs, const int nseg,
                            const uint64_t ndat, const unsigned nbin, unsigned* __restrict__ cols)
@@ -2023,6 +2148,11 @@ void launch_rows (unsigned nrows, float2* scratch, const ConvTables& tb, unsigne
   // n2 = 8192 and 2 at n2 = 4096)
   const unsigned per_sm = N2 >= 8192 ? 1 : 2;
   const unsigned grid = std::min<unsigned> (nrows, per_sm * unsigned (tb.nsm));
+  if (N2 == 8192 && tb.tc_splits)
+  {
+    launch_rows_mma (nrows, scratch, tb, n1, sh, st);
+    return;
+  }
   k_rows_tma<N2, true><<<grid, T, rows_smem_bytes<N2> (), st>>> (scratch, tb.ptab, tb.H, n1,
                                                                  sh.nchan, sh.npol, nrows, tb.err);
 }
@@ -2231,6 +2361,31 @@ void make_pass_tables (unsigned n, float2* out, unsigned capacity)
   }
 }
 
+// The four-step kernels' shared-memory opt-in, once per device (the current
+// one); later calls only test a bit.
+cudaError_t convolution_kernel_setup ()
+{
+  static std::atomic<unsigned> attr_done {0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice (&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned bit = dev < 32 ? 1u << dev : 0u;    // devices past 32: set every time
+  if (bit && (attr_done.load () & bit)) return cudaSuccess;
+  e = set_rows_smem<8192> ();
+  if (e == cudaSuccess) e = set_rows_smem<4096> ();
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute (k_fwd_cols_fb64<IN_INT8, false>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, int (FBC_SMEM));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute (k_fwd_cols_fb64<IN_INT8, true>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, int (FBC_SMEM));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute (k_fwd_cols_fb64<IN_INT16, false>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, int (FBC_SMEM));
+  if (e == cudaSuccess) attr_done.fetch_or (bit);
+  return e;
+}
+
 cudaError_t launch_convolution (const ConvShape& sh, const ConvTables& tb, const InputView& in,
                                 uint64_t part0, unsigned nbatch, float2* scratch, int mode,
                                 const FoldView& fv, const VoltView& vv, cudaStream_t st,
@@ -2246,25 +2401,9 @@ cudaError_t launch_convolution (const ConvShape& sh, const ConvTables& tb, const
       default: return cudaErrorInvalidValue;
     }
   }
-  // the shared-memory opt-in is per device
-  static unsigned attr_done = 0;
-  int dev = 0;
-  cudaGetDevice (&dev);
-  if (dev < 32 && !(attr_done & (1u << dev)))
   {
-    cudaError_t e = set_rows_smem<8192> ();
-    if (e == cudaSuccess) e = set_rows_smem<4096> ();
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute (k_fwd_cols_fb64<IN_INT8, false>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, int (FBC_SMEM));
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute (k_fwd_cols_fb64<IN_INT8, true>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, int (FBC_SMEM));
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute (k_fwd_cols_fb64<IN_INT16, false>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, int (FBC_SMEM));
+    const cudaError_t e = convolution_kernel_setup ();
     if (e != cudaSuccess) return e;
-    attr_done |= 1u << dev;
   }
   switch (sh.n1)
   {
@@ -2777,6 +2916,70 @@ cudaError_t launch_delay_fold (const float2* v, uint64_t span, const int* applie
     k_delay_fold<2><<<grid, 256, 0, st>>> (v, span, applied, ndat, npol, fv);
   else
     k_delay_fold<4><<<grid, 256, 0, st>>> (v, span, applied, ndat, npol, fv);
+  return cudaGetLastError ();
+}
+
+cudaError_t launch_sk_detect (const float* sums, const unsigned* counts, uint64_t npart,
+                              unsigned nchan, unsigned npol, unsigned M, unsigned Nd, float lower,
+                              float upper, uint8_t* mask, unsigned long long* nzap, cudaStream_t st)
+{
+  const uint64_t ncell = npart * nchan;
+  if (ncell == 0) return cudaSuccess;
+  g_launches++;
+  k_sk_detect<<<unsigned ((ncell + 255) / 256), 256, 0, st>>> (sums, counts, ncell, npol, M, Nd,
+                                                              lower, upper, mask, nzap);
+  return cudaGetLastError ();
+}
+
+cudaError_t launch_sk_mask (const uint8_t* mask, const float2* in, uint64_t in_span, float2* out,
+                            uint64_t out_span, uint64_t ndat, unsigned nchan, unsigned npol,
+                            unsigned M, cudaStream_t st)
+{
+  if (ndat == 0) return cudaSuccess;
+  g_launches++;
+  k_sk_mask<<<dim3 (unsigned ((ndat + 255) / 256), nchan), 256, 0, st>>> (
+      mask, in, in_span, out, out_span, ndat, nchan, npol, M);
+  return cudaGetLastError ();
+}
+
+cudaError_t launch_zero_dm (const InputView& in, const float* lut, uint64_t first, uint64_t n,
+                            float2* out, uint64_t span, cudaStream_t st)
+{
+  if (n == 0) return cudaSuccess;
+  g_launches++;
+  const dim3 grid (unsigned ((n + 255) / 256), in.nchan * in.npol);
+  if (in.kind == IN_INT8)
+    k_zero_dm<IN_INT8><<<grid, 256, 0, st>>> (in, lut, first, n, out, span);
+  else if (in.kind == IN_INT16)
+    k_zero_dm<IN_INT16><<<grid, 256, 0, st>>> (in, lut, first, n, out, span);
+  else
+    k_zero_dm<IN_FLOAT><<<grid, 256, 0, st>>> (in, lut, first, n, out, span);
+  return cudaGetLastError ();
+}
+
+cudaError_t launch_sk_apply (const uint8_t* mask, float2* v, uint64_t span, uint64_t ndat,
+                             unsigned nchan, unsigned npol, unsigned M, cudaStream_t st)
+{
+  if (ndat == 0) return cudaSuccess;
+  g_launches++;
+  k_sk_apply<<<dim3 (unsigned ((ndat + 255) / 256), nchan), 256, 0, st>>> (mask, v, span, ndat,
+                                                                            nchan, npol, M);
+  return cudaGetLastError ();
+}
+
+cudaError_t launch_zeroed_fold (const float2* v, uint64_t span, uint64_t ndat, unsigned nchan,
+                                unsigned npol, const FoldView& fv, cudaStream_t st,
+                                const KernelClock* clk)
+{
+  if (ndat == 0) return cudaSuccess;
+  const dim3 grid (unsigned ((ndat + 255) / 256), nchan);
+  ClockScope cs (clk, KK_INV_COLS, st);
+  if (fv.nout == 1)
+    k_zeroed_fold<1><<<grid, 256, 0, st>>> (v, span, ndat, npol, fv);
+  else if (fv.nout == 2)
+    k_zeroed_fold<2><<<grid, 256, 0, st>>> (v, span, ndat, npol, fv);
+  else
+    k_zeroed_fold<4><<<grid, 256, 0, st>>> (v, span, ndat, npol, fv);
   return cudaGetLastError ();
 }
 

@@ -2,6 +2,9 @@
 #pragma once
 
 #include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
 #include <stdint.h>
 
 #include "host_rules.h"
@@ -69,15 +72,27 @@ struct ConvShape
 
 struct ConvTables
 {
-  const float2* tw2;         // n2-point table exp(-2 pi i m / n2)
-  const float2* tw4;         // [n1][n2] exp(-2 pi i k1 n2 / nfft), null when n1 == 1
-  const float2* ptab;        // per-pass Stockham twiddle tables of the n2-point FFT
-  const float2* H;           // [nchan][n1][n2] response in four-step order
-  const float* lut;          // 8-bit lookup table (device), 256 floats
-  int* err;                  // device flag: set when a bounded wait gave up
-  int nsm;                   // multiprocessors of the device
-  const float* apod;         // temporal window [nfft] applied to each part, or null
+  const float2* tw2 = nullptr;   // n2-point table exp(-2 pi i m / n2)
+  const float2* tw4 = nullptr;   // [n1][n2] exp(-2 pi i k1 n2 / nfft), null when n1 == 1
+  const float2* ptab = nullptr;  // per-pass Stockham twiddle tables of the n2-point FFT
+  const float2* H = nullptr;     // [nchan][n1][n2] response in four-step order
+  const float* lut = nullptr;    // 8-bit lookup table (device), 256 floats
+  int* err = nullptr;            // device flag: set when a bounded wait gave up
+  int nsm = 0;                   // multiprocessors of the device
+  const float* apod = nullptr;   // temporal window [nfft] applied to each part, or null
+  // tensor-core row FFT: the DFT16/DFT32 operand image (make_tc_dft_image)
+  // and its number of BF16 terms (2 or 3); 0 = the FP32 row kernel
+  const void* tc_dft = nullptr;
+  int tc_splits = 0;
 };
+
+// The DFT16 and DFT32 blocks of the tensor-core row kernel in its shared
+// memory operand layout, split into ns BF16 terms (bytes for a device copy).
+void make_tc_dft_image (unsigned ns, std::vector<uint8_t>& img);
+
+// The convolution rows (n2 = 8192) on the tensor cores: k_rows_mma.
+cudaError_t launch_rows_mma (unsigned nrows, float2* scratch, const ConvTables& tables,
+                             unsigned n1, const ConvShape& shape, cudaStream_t stream);
 
 // Per-pass Stockham twiddle tables of an n-point transform, as the row
 // kernel reads them (fft_core.cuh pass_table_offset layout).
@@ -100,6 +115,32 @@ struct KernelClock
 
 // Number of kernels this library has launched since it was loaded.
 uint64_t kernel_launches ();
+
+// SpectralKurtosis engine steps on their own: the test of sums already formed
+// (detect_skfb) and the mask applied to voltages (out == in: in place).
+cudaError_t launch_sk_detect (const float* sums, const unsigned* counts, uint64_t npart,
+                              unsigned nchan, unsigned npol, unsigned M, unsigned Nd, float lower,
+                              float upper, uint8_t* mask, unsigned long long* nzap,
+                              cudaStream_t stream);
+cudaError_t launch_sk_mask (const uint8_t* mask, const float2* in, uint64_t in_span, float2* out,
+                            uint64_t out_span, uint64_t ndat, unsigned nchan, unsigned npol,
+                            unsigned M, cudaStream_t stream);
+
+// SpectralKurtosis as a stage of the pipeline: the zero-DM input of n
+// output samples starting at input sample `first` (unpacked, FPT rows of
+// span), the mask of its blocks applied to other voltages, and detection +
+// fold of zeroed data (hits counted per non-zeroed channel sample).
+cudaError_t launch_zero_dm (const InputView& in, const float* lut, uint64_t first, uint64_t n,
+                            float2* out, uint64_t span, cudaStream_t stream);
+cudaError_t launch_sk_apply (const uint8_t* mask, float2* v, uint64_t span, uint64_t ndat,
+                             unsigned nchan, unsigned npol, unsigned M, cudaStream_t stream);
+cudaError_t launch_zeroed_fold (const float2* v, uint64_t span, uint64_t ndat, unsigned nchan,
+                                unsigned npol, const FoldView& fold, cudaStream_t stream,
+                                const KernelClock* clock = nullptr);
+
+// Per-device set-up of the four-step convolution kernels (their shared-memory
+// opt-in) on the current device; launch_convolution calls it itself.
+cudaError_t convolution_kernel_setup ();
 
 // Runs parts [part0, part0 + nbatch) of one block.  scratch holds
 // nbatch*nchan*npol*nfft complex values (unused when n1 == 1).
@@ -218,7 +259,8 @@ cudaError_t launch_filterbank_during (const DuringShape& shape, const DuringTabl
                                       const KernelClock* clock = nullptr);
 
 // SpectralKurtosis (one resolution, noverlap 1): statistics, test and masked
-// copy (out may equal in: then only zapped blocks are written).  sums
+// copy (out may equal in: then only zapped blocks are written; out null:
+// statistics, counts and mask only, nothing written back).  sums
 // [npart][nchan][npol][2], counts and mask [npart][nchan] are optional.
 // in/out spans are complex samples; M and the spans must be even, npol 1 or 2,
 // and sk_smem_bytes(npol, M, 1) at most SK_SMEM_MAX.

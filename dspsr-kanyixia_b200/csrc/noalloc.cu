@@ -1,24 +1,24 @@
 // noalloc.cu -- an overlap-save convolution entry point that allocates no
 // memory at all.
 //
-// Who needs it: callers that must not call cudaMalloc while they run -- code
-// running inside a CUDA stream capture that other code will replay, real-time
-// processes that fix every allocation at start-up to keep their latency flat,
-// and hosts whose device memory belongs to another allocator (a framework's
-// caching pool, an embedding application) that does not let this library
-// allocate behind its back.  dspsr_b200_convolution_perform needs an engine
-// object whose creation allocates its tables and scratch; this entry point
-// instead keeps everything it needs in one fixed array in device memory that
-// the library owns from load time.
+// Who needs it: callers that must not call cudaMalloc while they run --
+// real-time processes that fix every allocation at start-up to keep their
+// latency flat, and hosts whose device memory belongs to another allocator (a
+// framework's caching pool, an embedding application) that does not let this
+// library allocate behind its back.  dspsr_b200_convolution_perform needs an
+// engine object whose creation allocates its tables and scratch; this entry
+// point instead keeps everything it needs in one fixed array in device memory
+// that the library owns from load time.
 //
 // The array: g_noalloc_scratch below, DSPSR_B200_NOALLOC_SCRATCH_BYTES
 // (32 MiB) of static device memory.  Every GPU that loads the library holds it
 // until the process exits.  Its device address is taken with
-// cudaGetSymbolAddress once per device, on the first call made with that
-// device current (so that first call should come before any stream capture).
-// Every call on a device reuses the same array and leaves its contents
-// behind, so calls whose work overlaps on the GPU (two streams, two threads)
-// race with each other; serialise them.
+// cudaGetSymbolAddress once per device, together with the kernels' shared-
+// memory opt-in, by the first call made with that device current (whatever
+// its shape, even one with no whole part), so that first call should come
+// before any stream capture.  Every call on a device reuses the same array and
+// leaves its contents behind, so calls whose work overlaps on the GPU (two
+// streams, two threads) race with each other; serialise them.
 
 #include "dspsr_b200.h"
 #include "kernels.cuh"
@@ -116,7 +116,8 @@ cudaError_t scratch_for_device (void** ptr, int* nsm)
 extern "C" int dspsr_b200_convolution_perform_noalloc (
     void* stream, const float* d_in, uint64_t in_span, uint64_t ndat, unsigned nchan,
     unsigned npol, unsigned nfft, unsigned nfilt_pos, unsigned nfilt_neg,
-    const float* d_response, float* d_out, uint64_t out_span, uint64_t* npart_out)
+    const float* d_response, float* d_out, uint64_t out_span, uint64_t* npart_out,
+    int* d_status)
 {
   if (npart_out) *npart_out = 0;
   if (!d_in || !d_out || !d_response || nchan == 0 || npol == 0 || npol > 2)
@@ -124,6 +125,13 @@ extern "C" int dspsr_b200_convolution_perform_noalloc (
   if (nfft < 4096 || nfft > 262144 || (nfft & (nfft - 1)))
     return DSPSR_B200_EINVAL;
   if (uint64_t (nfilt_pos) + nfilt_neg >= nfft || in_span < ndat) return DSPSR_B200_EINVAL;
+
+  // per-device set-up first, whatever the shape: the array's address, the
+  // multiprocessor count and the kernels' shared-memory opt-in
+  void* base = nullptr;
+  int nsm = 0;
+  if (scratch_for_device (&base, &nsm) != cudaSuccess) return DSPSR_B200_ECUDA;
+  if (convolution_kernel_setup () != cudaSuccess) return DSPSR_B200_ECUDA;
 
   ConvShape sh {};
   sh.nchan = nchan;
@@ -153,24 +161,34 @@ extern "C" int dspsr_b200_convolution_perform_noalloc (
     off_scratch = off_H + align256 (uint64_t (nchan) * nfft * sizeof (float2));
     const uint64_t per_part = uint64_t (nchan) * npol * nfft * sizeof (float2);
     if (off_scratch + per_part > SCRATCH_BYTES) return DSPSR_B200_ETOOBIG;
-    nbatch = std::min<uint64_t> (65535, (SCRATCH_BYTES - off_scratch) / per_part);
+    // as many parts as fit, reduced (down to half) to a batch whose rows
+    // spread evenly over the persistent row kernel's one CTA per SM
+    const uint64_t bmax = std::min<uint64_t> (65535, (SCRATCH_BYTES - off_scratch) / per_part);
+    const uint64_t rows_per_part = uint64_t (sh.n1) * nchan * npol;
+    nbatch = bmax;
+    for (uint64_t b = bmax; b >= std::max<uint64_t> (1, bmax / 2); b--)
+      if ((b * rows_per_part) % uint64_t (nsm) == 0)
+      {
+        nbatch = b;
+        break;
+      }
   }
-  if (npart == 0) return DSPSR_B200_OK;
 
   cudaStream_t st = static_cast<cudaStream_t> (stream);
-  void* base = nullptr;
-  int nsm = 0;
-  if (scratch_for_device (&base, &nsm) != cudaSuccess) return DSPSR_B200_ECUDA;
   unsigned char* b = static_cast<unsigned char*> (base);
-  int* err = reinterpret_cast<int*> (b);
+  // the row kernel's give-up flag: the caller's int when given, else a word
+  // of the array; either way it starts every call at zero
+  int* err = d_status ? d_status : reinterpret_cast<int*> (b);
+  if (cudaMemsetAsync (err, 0, sizeof (int), st) != cudaSuccess) return DSPSR_B200_ECUDA;
+  if (npart == 0) return DSPSR_B200_OK;
+
   float2* tw2 = reinterpret_cast<float2*> (b + off_tw2);
   float2* ptab = reinterpret_cast<float2*> (b + off_ptab);
   float2* tw4 = reinterpret_cast<float2*> (b + off_tw4);
   float2* H = reinterpret_cast<float2*> (b + off_H);
   float2* scratch = reinterpret_cast<float2*> (b + off_scratch);
 
-  // the flag must start at zero; the tables are rewritten for this shape
-  if (cudaMemsetAsync (err, 0, sizeof (int), st) != cudaSuccess) return DSPSR_B200_ECUDA;
+  // the tables are rewritten for this shape
   k_tw2<<<(sh.n2 + 255) / 256, 256, 0, st>>> (tw2, sh.n2);
   ConvTables tb {};
   tb.tw2 = tw2;

@@ -23,14 +23,16 @@ import numpy as np
 
 from . import _capi
 from ._capi import (B200Error, PipelineConfig, INTENSITY, PPQQ, COHERENCE, STOKES, INT8_TFPD,
-                    INT16_TFPD, FLOAT_FPT, CHIRP_REFERENCE, CHIRP_FP64)
+                    INT16_TFPD, FLOAT_FPT, CHIRP_REFERENCE, CHIRP_FP64, FFT_FP32, FFT_BF16X2,
+                    FFT_BF16X3)
 
-__all__ = ["Context", "Convolution", "InverseFilterbank", "FilterbankDuring", "Fold", "apodization", "Pipeline", "PipelineConfig", "B200Error",
+__all__ = ["Context", "Convolution", "RfiProposer", "InverseFilterbank", "FilterbankDuring", "Fold", "apodization", "Pipeline", "PipelineConfig", "B200Error",
            "smearing_samples", "minimum_ndat", "optimal_fft_length", "bittable8", "fold_phi",
            "sk_limits", "DADAFile", "dada_parse", "dada_is_valid", "ascii_header_get",
            "ascii_header_set", "write_dada", "TimeDivide", "interchannel_delays",
            "fold_plan_count", "archive_profiles", "INTENSITY", "PPQQ", "COHERENCE", "STOKES", "INT8_TFPD",
-           "INT16_TFPD", "FLOAT_FPT", "CHIRP_REFERENCE", "CHIRP_FP64", "NOUT"]
+           "INT16_TFPD", "FLOAT_FPT", "CHIRP_REFERENCE", "CHIRP_FP64", "NOUT",
+           "FFT_FP32", "FFT_BF16X2", "FFT_BF16X3"]
 
 NOUT = {INTENSITY: 1, PPQQ: 2, COHERENCE: 4, STOKES: 4}
 # Jenet & Anderson (1998) optimal uniform-quantiser input spacing for 8 bits
@@ -225,6 +227,46 @@ class Context:
         self.check(self._lib.dspsr_b200_detect(self.handle, _ptr(d_in), in_span, ndat, nchan,
                                                state, _ptr(d_out), out_span), "detect")
 
+    # ---- SpectralKurtosis engine, step by step --------------------------------------
+    def sk_compute(self, d_in, in_span, ndat, nchan, npol, M, d_sums, d_counts=None,
+                   zero_is_valid=True):
+        n = ctypes.c_uint64()
+        self.check(self._lib.dspsr_b200_sk_compute(self.handle, _ptr(d_in), in_span, ndat, nchan,
+                                                   npol, M, int(zero_is_valid), _ptr(d_sums),
+                                                   _ptr(d_counts), ctypes.byref(n)),
+                   "sk_compute")
+        return n.value
+
+    def sk_detect_ft(self, d_sums, d_counts, npart, nchan, npol, M, lower, upper, d_mask,
+                     Nd=1, d_zapped=None):
+        self.check(self._lib.dspsr_b200_sk_detect_ft(self.handle, _ptr(d_sums), _ptr(d_counts),
+                                                     npart, nchan, npol, M, Nd, lower, upper,
+                                                     _ptr(d_mask), _ptr(d_zapped)),
+                   "sk_detect_ft")
+
+    def sk_detect_tscr(self, d_sums, d_counts, npart, nchan, npol, M, std_devs, d_mask, Nd=1):
+        n = ctypes.c_uint32()
+        self.check(self._lib.dspsr_b200_sk_detect_tscr(self.handle, _ptr(d_sums), _ptr(d_counts),
+                                                       npart, nchan, npol, M, Nd, std_devs,
+                                                       _ptr(d_mask), ctypes.byref(n)),
+                   "sk_detect_tscr")
+        return n.value
+
+    def sk_reset_mask(self, d_mask, npart, nchan):
+        self.check(self._lib.dspsr_b200_sk_reset_mask(self.handle, _ptr(d_mask), npart, nchan),
+                   "sk_reset_mask")
+
+    def sk_count_mask(self, d_mask, npart, nchan):
+        n = ctypes.c_uint64()
+        self.check(self._lib.dspsr_b200_sk_count_mask(self.handle, _ptr(d_mask), npart, nchan,
+                                                      ctypes.byref(n)), "sk_count_mask")
+        return n.value
+
+    def sk_mask(self, d_mask, d_in, in_span, d_out, out_span, ndat, nchan, npol, M):
+        self.check(self._lib.dspsr_b200_sk_mask(self.handle, _ptr(d_mask), _ptr(d_in), in_span,
+                                                _ptr(d_out), out_span, ndat, nchan, npol, M),
+                   "sk_mask")
+
     # ---- SpectralKurtosis engine (one resolution, noverlap 1) -----------------------
     def sk(self, d_in, in_span, ndat, nchan, npol, M, lower, upper, d_out, out_span,
            d_sums=None, d_counts=None, d_mask=None, d_zapped=None, Nd=1, zero_is_valid=True):
@@ -235,6 +277,77 @@ class Context:
                                            out_span, _ptr(d_sums), _ptr(d_counts), _ptr(d_mask),
                                            _ptr(d_zapped), ctypes.byref(n)), "sk")
         return n.value
+
+
+class RfiProposer:
+    """The learned RFI-mask proposer in front of SpectralKurtosis: features
+    from the SK sums, training on SK masks, tensor-core inference with the SK
+    mask as the fallback where it is not confident."""
+
+    NFEAT = 8
+
+    def __init__(self, ctx, nchan, M, Nd=1, max_npart=1024, max_batch_blocks=32, seed=1):
+        self.ctx = ctx
+        self._lib = ctx._lib
+        h = ctypes.c_void_p()
+        ctx.check(self._lib.dspsr_b200_rfi_proposer_create(ctx.handle, nchan, M, Nd, max_npart,
+                                                           max_batch_blocks, seed,
+                                                           ctypes.byref(h)), "rfi_proposer_create")
+        self.handle = h
+        ctx._adopt(self)
+        self.nchan, self.M = nchan, M
+        self.npart = 0
+
+    def features(self, d_sums, npart, npol, d_counts=None):
+        self.ctx.check(self._lib.dspsr_b200_rfi_proposer_features(
+            self.handle, _ptr(d_sums), _ptr(d_counts), npart, npol), "rfi_proposer_features")
+        self.npart = npart
+
+    def train(self, d_labels, steps, batch_blocks=16, lr=3e-3, pos_weight=4.0):
+        loss = ctypes.c_float()
+        self.ctx.check(self._lib.dspsr_b200_rfi_proposer_train(
+            self.handle, _ptr(d_labels), steps, batch_blocks, lr, pos_weight,
+            ctypes.byref(loss)), "rfi_proposer_train")
+        return loss.value
+
+    def infer(self, d_mask, d_prob=None, d_sk_mask=None, confidence=0.9):
+        """Returns the number of (block, channel) cells that fell back to SK."""
+        n = ctypes.c_uint64()
+        self.ctx.check(self._lib.dspsr_b200_rfi_proposer_infer(
+            self.handle, _ptr(d_sk_mask), confidence, _ptr(d_mask), _ptr(d_prob),
+            ctypes.byref(n)), "rfi_proposer_infer")
+        return n.value
+
+    def params(self):
+        n = ctypes.c_uint()
+        self.ctx.check(self._lib.dspsr_b200_rfi_proposer_get_params(self.handle, None,
+                                                                    ctypes.byref(n)), "params")
+        out = np.empty(n.value, np.float32)
+        self.ctx.check(self._lib.dspsr_b200_rfi_proposer_get_params(self.handle, _fptr(out),
+                                                                    ctypes.byref(n)), "params")
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        self.ctx.check(self._lib.dspsr_b200_rfi_proposer_set_params(self.handle, _fptr(p),
+                                                                    p.size), "set_params")
+
+    def get_features(self):
+        out = np.empty((self.npart, self.nchan, self.NFEAT), np.float32)
+        self.ctx.check(self._lib.dspsr_b200_rfi_proposer_get_features(self.handle, _fptr(out)),
+                       "get_features")
+        return out
+
+    def close(self):
+        if self.handle:
+            self._lib.dspsr_b200_rfi_proposer_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Convolution:
@@ -279,6 +392,12 @@ class Convolution:
         assert w is None or w.size == self.nfft
         self.ctx.check(self._lib.dspsr_b200_convolution_set_temporal_apodization(
             self.handle, None if w is None else _fptr(w)), "set_temporal_apodization")
+
+    def set_fft_precision(self, mode):
+        """FFT_FP32 (default), FFT_BF16X3 or FFT_BF16X2: the row FFTs on the
+        CUDA cores or as split-BF16 tensor-core GEMMs (nfft >= 16384)."""
+        self.ctx.check(self._lib.dspsr_b200_convolution_set_fft_precision(self.handle, mode),
+                       "set_fft_precision")
 
     def status(self):
         self.ctx.check(self._lib.dspsr_b200_convolution_status(self.handle), "status")
@@ -646,6 +765,13 @@ class Pipeline:
                        "kernel_times")
         return {k: (ms[i], n[i]) for i, k in enumerate(self.KERNELS)}
 
+    def sk_counts(self):
+        """(zapped, tested) (block, channel) cells of the SpectralKurtosis stage."""
+        z, t = ctypes.c_uint64(), ctypes.c_uint64()
+        self.ctx.check(self._lib.dspsr_b200_pipeline_sk_counts(self.handle, ctypes.byref(z),
+                                                               ctypes.byref(t)), "sk_counts")
+        return z.value, t.value
+
     def info(self):
         a = (ctypes.c_uint64 * 8)()
         self.ctx.check(self._lib.dspsr_b200_pipeline_info(self.handle, a), "pipeline_info")
@@ -841,7 +967,8 @@ def make_config(centre_freq, bandwidth, dm, nchan, npol, nfft, nfilt_pos, nfilt_
                 start_mjd=(60000, 0, 0.0), epoch_mjd=(60000, 0, 0.0), reference_phase=0.0,
                 dual_sideband=1, offset_binary=0, scratch_bytes=0, filterbank_nchan=0,
                 subint_seconds=0.0, subint_turns=0.0, subint_slots=0,
-                subint_epoch=(0, 0, 0.0), fused_filterbank=0, interchannel=0):
+                subint_epoch=(0, 0, 0.0), fused_filterbank=0, interchannel=0,
+                fft_precision=FFT_FP32, sk_M=0, sk_std_devs=3.0):
     """Fill a PipelineConfig (the fields DedispersionPipe / LoadToFold set up).
     With filterbank_nchan > 1, nchan counts input channels, and nfft and the
     smearing (nfilt_pos, nfilt_neg) refer to the filterbank's output channels."""
@@ -877,6 +1004,9 @@ def make_config(centre_freq, bandwidth, dm, nchan, npol, nfft, nfilt_pos, nfilt_
     cfg.subint_epoch_day, cfg.subint_epoch_sec, cfg.subint_epoch_frac = subint_epoch
     cfg.fused_filterbank = fused_filterbank
     cfg.interchannel = interchannel
+    cfg.fft_precision = fft_precision
+    cfg.sk_M = sk_M
+    cfg.sk_std_devs = sk_std_devs
     return cfg
 
 

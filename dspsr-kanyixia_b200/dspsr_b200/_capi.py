@@ -17,6 +17,7 @@ NOALLOC_SCRATCH_BYTES = 32 << 20
 INTENSITY, PPQQ, COHERENCE, STOKES = 0, 1, 2, 3
 INT8_TFPD, INT16_TFPD, FLOAT_FPT = 0, 1, 2
 CHIRP_REFERENCE, CHIRP_FP64 = 0, 1
+FFT_FP32, FFT_BF16X2, FFT_BF16X3 = 0, 2, 3
 
 c_vp = ctypes.c_void_p
 c_u64 = ctypes.c_uint64
@@ -66,6 +67,9 @@ class PipelineConfig(ctypes.Structure):
         ("subint_slots", c_uint),
         ("fused_filterbank", c_int),
         ("interchannel", c_int),
+        ("fft_precision", c_int),
+        ("sk_M", c_uint),
+        ("sk_std_devs", ctypes.c_float),
     ]
 
 
@@ -198,9 +202,10 @@ SIGNATURES = {
     "dspsr_b200_convolution_get_response": (c_int, [c_vp, c_fp]),
     "dspsr_b200_convolution_status": (c_int, [c_vp]),
     "dspsr_b200_convolution_set_temporal_apodization": (c_int, [c_vp, c_fp]),
+    "dspsr_b200_convolution_set_fft_precision": (c_int, [c_vp, c_int]),
     "dspsr_b200_convolution_perform_noalloc": (c_int, [c_vp, c_vp, c_u64, c_u64, c_uint, c_uint,
                                                        c_uint, c_uint, c_uint, c_vp, c_vp, c_u64,
-                                                       c_u64p]),
+                                                       c_u64p, c_vp]),
     "dspsr_b200_convolution_set_dedispersion_channels": (c_int, [c_vp, ctypes.POINTER(c_dbl),
                                                                  c_dbl, c_dbl, c_int, c_uint]),
     "dspsr_b200_filterbank": (c_int, [c_vp, c_int, c_vp, c_u64, c_u64, c_uint, c_uint, c_uint,
@@ -238,6 +243,27 @@ SIGNATURES = {
     "dspsr_b200_sk": (c_int, [c_vp, c_vp, c_u64, c_u64, c_uint, c_uint, c_uint, c_int, c_uint,
                               ctypes.c_float, ctypes.c_float, c_vp, c_u64, c_vp, c_vp, c_vp, c_vp,
                               c_u64p]),
+    "dspsr_b200_rfi_proposer_create": (c_int, [c_vp, c_uint, c_uint, c_uint, c_u64, c_uint, c_u64,
+                                               ctypes.POINTER(c_vp)]),
+    "dspsr_b200_rfi_proposer_destroy": (c_int, [c_vp]),
+    "dspsr_b200_sk_compute": (c_int, [c_vp, c_vp, c_u64, c_u64, c_uint, c_uint, c_uint, c_int,
+                                      c_vp, c_vp, c_u64p]),
+    "dspsr_b200_sk_detect_ft": (c_int, [c_vp, c_vp, c_vp, c_u64, c_uint, c_uint, c_uint, c_uint,
+                                        ctypes.c_float, ctypes.c_float, c_vp, c_vp]),
+    "dspsr_b200_sk_detect_tscr": (c_int, [c_vp, c_vp, c_vp, c_u64, c_uint, c_uint, c_uint, c_uint,
+                                          ctypes.c_float, c_vp, ctypes.POINTER(ctypes.c_uint32)]),
+    "dspsr_b200_sk_reset_mask": (c_int, [c_vp, c_vp, c_u64, c_uint]),
+    "dspsr_b200_sk_count_mask": (c_int, [c_vp, c_vp, c_u64, c_uint, c_u64p]),
+    "dspsr_b200_sk_mask": (c_int, [c_vp, c_vp, c_vp, c_u64, c_vp, c_u64, c_u64, c_uint, c_uint,
+                                   c_uint]),
+    "dspsr_b200_pipeline_sk_counts": (c_int, [c_vp, c_u64p, c_u64p]),
+    "dspsr_b200_rfi_proposer_features": (c_int, [c_vp, c_vp, c_vp, c_u64, c_uint]),
+    "dspsr_b200_rfi_proposer_train": (c_int, [c_vp, c_vp, c_uint, c_uint, ctypes.c_float,
+                                              ctypes.c_float, c_fp]),
+    "dspsr_b200_rfi_proposer_infer": (c_int, [c_vp, c_vp, ctypes.c_float, c_vp, c_vp, c_u64p]),
+    "dspsr_b200_rfi_proposer_get_params": (c_int, [c_vp, c_fp, ctypes.POINTER(c_uint)]),
+    "dspsr_b200_rfi_proposer_set_params": (c_int, [c_vp, c_fp, c_uint]),
+    "dspsr_b200_rfi_proposer_get_features": (c_int, [c_vp, c_fp]),
     "dspsr_b200_fold_create": (c_int, [c_vp, c_uint, c_uint, c_uint, ctypes.POINTER(c_vp)]),
     "dspsr_b200_fold_destroy": (c_int, [c_vp]),
     "dspsr_b200_fold_set_bins": (c_int, [c_vp, c_dbl, c_dbl, c_u64, c_u64, c_u64p]),

@@ -46,6 +46,15 @@ extern "C" {
 #define DSPSR_B200_INT16_TFPD  1 /* 16-bit, float(x)+0.5 (SixteenBitUnpacker.C:54-79) */
 #define DSPSR_B200_FLOAT_FPT   2 /* complex float, one span per (chan, pol) */
 
+/* arithmetic of the convolution's row FFTs (the n2 = 8192 half of the
+   four-step split, nfft >= 16384) */
+#define DSPSR_B200_FFT_FP32   0  /* FP32 Stockham passes on the CUDA cores */
+#define DSPSR_B200_FFT_BF16X3 3  /* DFT16/DFT32 stages as tensor-core GEMMs, operands
+                                    split into three BF16 terms (six products,
+                                    FP32 accumulation: FP32-level accuracy) */
+#define DSPSR_B200_FFT_BF16X2 2  /* the same with two BF16 terms (three products,
+                                    about 16 significant bits per stage) */
+
 /* dispersion response evaluation */
 #define DSPSR_B200_CHIRP_REFERENCE 0 /* phase rounded to float before sin/cos,
                                         as Dedispersion.C:104-111 does */
@@ -202,27 +211,33 @@ int dspsr_b200_convolution_set_dedispersion_channels (dspsr_b200_convolution* co
                                                       int chirp_mode, unsigned norm_nfft);
 /* The same overlap-save convolution without allocating anything.  This entry
    point has no counterpart in the reference: it exists for callers that
-   cannot call cudaMalloc while they run -- code inside a CUDA stream capture
-   that others replay, real-time processes that fix all memory at start-up,
-   hosts whose device memory is owned by another allocator.  It takes no
-   context or engine object: stream (a cudaStream_t, NULL for the legacy
-   default stream), the complex FPT input (in_span complex samples per
-   (chan, pol)), the response (nchan*nfft complex floats in FFT order, in
-   device memory, normaliser applied), and the output; sizes as for
-   dspsr_b200_convolution_create.  Its tables and FFT scratch live in one
-   static device array of DSPSR_B200_NOALLOC_SCRATCH_BYTES that every GPU
-   loading the library keeps until exit; shapes needing more (roughly
-   nchan*(npol+1)*nfft*8 bytes plus nfft*8 for FFTs above 8192 points) return
-   DSPSR_B200_ETOOBIG.  The array's address is set up on the first call made
-   on each device (make that call before any stream capture).  All calls
-   share the one array: calls whose work overlaps on the GPU race.  Returns
-   the status; *npart as for dspsr_b200_convolution_perform. */
+   cannot call cudaMalloc while they run -- real-time processes that fix all
+   memory at start-up so that no allocation stalls a block, and hosts whose
+   device memory is owned by another allocator that does not let a library
+   allocate behind its back.  It takes no context or engine object: stream (a
+   cudaStream_t, NULL for the legacy default stream), the complex FPT input
+   (in_span complex samples per (chan, pol)), the response (nchan*nfft complex
+   floats in FFT order, in device memory, normaliser applied), and the output;
+   sizes as for dspsr_b200_convolution_create.  Its tables and FFT scratch
+   live in one static device array of DSPSR_B200_NOALLOC_SCRATCH_BYTES that
+   every GPU loading the library keeps until exit; shapes needing more
+   (roughly nchan*(npol+1)*nfft*8 bytes plus nfft*8 for FFTs above 8192
+   points) return DSPSR_B200_ETOOBIG.  The array's address and the kernels'
+   shared-memory opt-in are set up by the first call made on each device,
+   whatever its shape (make that call before any stream capture).  All calls
+   share the one array and leave their contents in it: calls whose work
+   overlaps on the GPU race.  d_status (device memory, may be NULL) is set to
+   0 in stream order at the start of the call and to 1 if one of the row
+   kernel's bounded device-side waits gave up, in which case the output is
+   not valid; read it once the stream has passed the call.  Returns the
+   launch status; *npart as for dspsr_b200_convolution_perform. */
 #define DSPSR_B200_NOALLOC_SCRATCH_BYTES (32ull << 20)
 int dspsr_b200_convolution_perform_noalloc (void* stream, const float* d_in, uint64_t in_span,
                                             uint64_t ndat, unsigned nchan, unsigned npol,
                                             unsigned nfft, unsigned nfilt_pos,
                                             unsigned nfilt_neg, const float* d_response,
-                                            float* d_out, uint64_t out_span, uint64_t* npart);
+                                            float* d_out, uint64_t out_span, uint64_t* npart,
+                                            int* d_status);
 /* Blocks until the engine's queued work is done and returns DSPSR_B200_ESTATE
    if one of its device-side waits gave up (each wait is bounded to about a
    second; see the row kernel), DSPSR_B200_OK otherwise. */
@@ -235,6 +250,11 @@ int dspsr_b200_convolution_get_response (dspsr_b200_convolution* conv, float* re
    before its forward FFT; NULL removes it. */
 int dspsr_b200_convolution_set_temporal_apodization (dspsr_b200_convolution* conv,
                                                      const float* window);
+/* The row FFTs' arithmetic, DSPSR_B200_FFT_FP32 (default), _BF16X3 or
+   _BF16X2.  The tensor-core forms replace the cuFFT C2C plans of the
+   reference's engine (ConvolutionCUDA.cu:370-413) for the rows of the
+   four-step split; they need nfft >= 16384 (EINVAL otherwise). */
+int dspsr_b200_convolution_set_fft_precision (dspsr_b200_convolution* conv, int mode);
 /* Engine::perform(input, output, npart): complex FPT in (span in complex
    samples per (chan, pol)), complex FPT out; returns npart
    = (ndat - nfilt_pos - nfilt_neg)/(nfft - nfilt_pos - nfilt_neg). */
@@ -445,6 +465,88 @@ int dspsr_b200_sk (dspsr_b200_context* ctx, const float* d_in, uint64_t in_span,
                    float* d_sums, uint32_t* d_counts, uint8_t* d_mask, uint64_t* d_zapped,
                    uint64_t* npart_out);
 
+/* The same engine step by step, as SpectralKurtosis::transformation drives
+   it (SpectralKurtosis.C:542-671; CUDA::SpectralKurtosisEngine,
+   SpectralKurtosisCUDA.cu:45-99).  Layouts as for dspsr_b200_sk. */
+/* Engine::compute (SpectralKurtosis.C:674-798): S1, S2 (d_sums, float) and
+   the counted samples (d_counts, optional) of every (part, chan, pol); the
+   input is not written. */
+int dspsr_b200_sk_compute (dspsr_b200_context* ctx, const float* d_in, uint64_t in_span,
+                           uint64_t ndat, unsigned nchan, unsigned npol, unsigned M,
+                           int zero_is_valid, float* d_sums, uint32_t* d_counts,
+                           uint64_t* npart);
+/* Engine::detect_ft (detect_skfb, SpectralKurtosis.C:1105-1222) with the
+   thresholds given: d_mask[part][chan] set to 1 where zapped (others left as
+   they are); d_counts NULL means M counted everywhere; *d_zapped (device,
+   optional) += zapped cells. */
+int dspsr_b200_sk_detect_ft (dspsr_b200_context* ctx, const float* d_sums,
+                             const uint32_t* d_counts, uint64_t npart, unsigned nchan,
+                             unsigned npol, unsigned M, unsigned Nd, float lower, float upper,
+                             uint8_t* d_mask, uint64_t* d_zapped);
+/* Engine::detect_tscr (SpectralKurtosis.C:1012-1098): each channel's sums
+   over all parts tested against the limits for its total count (SKLimits of
+   that count, std_devs, npol tests); every part of a zapped channel is set in
+   d_mask.  Synchronises; *nzapped_chan = channels zapped. */
+int dspsr_b200_sk_detect_tscr (dspsr_b200_context* ctx, const float* d_sums,
+                               const uint32_t* d_counts, uint64_t npart, unsigned nchan,
+                               unsigned npol, unsigned M, unsigned Nd, float std_devs,
+                               uint8_t* d_mask, uint32_t* nzapped_chan);
+/* Engine::reset_mask and count_mask (synchronises) */
+int dspsr_b200_sk_reset_mask (dspsr_b200_context* ctx, uint8_t* d_mask, uint64_t npart,
+                              unsigned nchan);
+int dspsr_b200_sk_count_mask (dspsr_b200_context* ctx, const uint8_t* d_mask, uint64_t npart,
+                              unsigned nchan, uint64_t* nzapped);
+/* Engine::mask (SpectralKurtosis.C:1465-1566): the ndat/M whole blocks of
+   d_in copied to d_out with the masked blocks zeroed (d_out == d_in: in
+   place, only those blocks written). */
+int dspsr_b200_sk_mask (dspsr_b200_context* ctx, const uint8_t* d_mask, const float* d_in,
+                        uint64_t in_span, float* d_out, uint64_t out_span, uint64_t ndat,
+                        unsigned nchan, unsigned npol, unsigned M);
+
+/* ---------------------------------------------------------------------- */
+/* Learned RFI-mask proposer in front of SpectralKurtosis.  It has no       */
+/* counterpart in the reference; it proposes the mask that                  */
+/* SpectralKurtosis::detect_skfb (SpectralKurtosis.C:1105-1222) would set,  */
+/* from features of the SK sums (SpectralKurtosis::compute, :674-798), and   */
+/* defers to the SK mask where it is not confident.                         */
+/* ---------------------------------------------------------------------- */
+
+typedef struct dspsr_b200_rfi_proposer dspsr_b200_rfi_proposer;
+/* nchan in [1, 512] channels per block of M samples (Nd integrated
+   samples each), features for up to max_npart blocks, training batches of
+   up to max_batch_blocks blocks; weights initialised from seed. */
+int dspsr_b200_rfi_proposer_create (dspsr_b200_context* ctx, unsigned nchan, unsigned M,
+                                    unsigned Nd, uint64_t max_npart, unsigned max_batch_blocks,
+                                    uint64_t seed, dspsr_b200_rfi_proposer** proposer);
+int dspsr_b200_rfi_proposer_destroy (dspsr_b200_rfi_proposer* proposer);
+/* Features of npart blocks from the SK sums of dspsr_b200_sk (d_sums laid
+   out [part][chan][pol][S1, S2], d_counts [part][chan] or NULL for M each). */
+int dspsr_b200_rfi_proposer_features (dspsr_b200_rfi_proposer* proposer, const float* d_sums,
+                                      const uint32_t* d_counts, uint64_t npart, unsigned npol);
+/* steps of Adam (learning rate lr) on random runs of batch_blocks blocks of
+   the current features, labels d_labels[part][chan] (1 = zapped, e.g. the
+   mask of dspsr_b200_sk); zapped examples weigh pos_weight in the binary
+   cross-entropy.  *mean_loss (optional) = mean loss per example. */
+int dspsr_b200_rfi_proposer_train (dspsr_b200_rfi_proposer* proposer, const uint8_t* d_labels,
+                                   unsigned steps, unsigned batch_blocks, float lr,
+                                   float pos_weight, float* mean_loss);
+/* The proposal for the current features on the tensor cores: probability
+   p of "zap" per (part, chan) into d_prob (optional); d_mask[part][chan] =
+   1 where p >= confidence, 0 where p <= 1 - confidence, else d_sk_mask's
+   value (the SK fallback; p >= 0.5 when d_sk_mask is NULL).  *n_fallback
+   (optional, synchronises) = the number of fallbacks.  confidence in
+   [0.5, 1]. */
+int dspsr_b200_rfi_proposer_infer (dspsr_b200_rfi_proposer* proposer, const uint8_t* d_sk_mask,
+                                   float confidence, uint8_t* d_mask, float* d_prob,
+                                   uint64_t* n_fallback);
+/* the FP32 weights (host memory): *n = their count (params may be NULL) */
+int dspsr_b200_rfi_proposer_get_params (dspsr_b200_rfi_proposer* proposer, float* params,
+                                        unsigned* n);
+int dspsr_b200_rfi_proposer_set_params (dspsr_b200_rfi_proposer* proposer, const float* params,
+                                        unsigned n);
+/* the current features, [part][chan][8] floats, into host memory */
+int dspsr_b200_rfi_proposer_get_features (dspsr_b200_rfi_proposer* proposer, float* features);
+
 /* ---------------------------------------------------------------------- */
 /* Fold::Engine (CUDA::FoldEngine, Signal/Pulsar/FoldCUDA.cu:78-704;        */
 /* callers Fold.C:760-887, 1011-1035)                                       */
@@ -528,12 +630,29 @@ typedef struct
      (SampleDelay.C:65-304) shifts the channels by whole samples before
      detection, so the channels' profiles line up; 0 = off */
   int interchannel;
+  /* the convolution's row FFTs: DSPSR_B200_FFT_FP32 (0), _BF16X3 or _BF16X2
+     (dspsr_b200_convolution_set_fft_precision) */
+  int fft_precision;
+  /* SpectralKurtosis between the convolution and detection, as LoadToFold
+     sets it up with coherent dedispersion (LoadToFold1.C:310-351): sk_M > 0
+     = blocks of sk_M samples (even, one resolution, noverlap 1), statistics
+     of the convolution's zero-DM output, the mask applied to the dedispersed
+     voltages, thresholds SKLimits(sk_M, 1, sk_std_devs (0 = 3), npol); the
+     fold then counts a hit for every channel's non-zeroed sample (Fold.C:
+     895-930, zeroed data).  Not with interchannel; a filterbank stage runs
+     on its own (fused_filterbank is ignored). */
+  unsigned sk_M;
+  float sk_std_devs;
 } dspsr_b200_pipeline_config;
 
 int dspsr_b200_pipeline_create (dspsr_b200_context* ctx,
                                 const dspsr_b200_pipeline_config* config,
                                 dspsr_b200_pipeline** pipe);
 int dspsr_b200_pipeline_destroy (dspsr_b200_pipeline* pipe);
+/* SpectralKurtosis of the pipeline so far: (block, channel) cells zapped
+   and tested (SpectralKurtosis::Count); synchronises */
+int dspsr_b200_pipeline_sk_counts (dspsr_b200_pipeline* pipe, uint64_t* zapped,
+                                   uint64_t* tested);
 /* Processes one block of ndat new input samples (device memory, layout given
    by input_kind; for FLOAT_FPT in_span is the complex-sample span per
    (chan, pol), otherwise ignored).  Samples that do not complete an FFT part

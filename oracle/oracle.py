@@ -113,6 +113,37 @@ def sk(x, M, lower, upper, Nd=1, zero_is_valid=True, ndat=None):
     return sums, counts, mask, out
 
 
+def sk_detect_tscr(sums, counts, Nd, std_devs):
+    """SpectralKurtosis::detect_tscr (Signal/General/SpectralKurtosis.C:
+    1012-1098) with noverlap 1: per channel, the count and the double sums of
+    the float S1, S2 over all parts; the SK estimator against the limits of
+    SKLimits(count, std_devs) with Nd and ntest = npol; a zapped channel is
+    flagged in every part.  sums (npart, nchan, npol, 2) float32, counts
+    (npart, nchan).  Returns the mask (npart, nchan) uint8 of these flags."""
+    npart, nchan, npol, _ = sums.shape
+    mask = np.zeros((npart, nchan), np.uint8)
+    for c in range(nchan):
+        count = int(np.sum(counts[:, c], dtype=np.uint64))
+        if count == 0:
+            continue
+        lo, hi = sk_limits(count, Nd, std_devs, npol)
+        M_t = np.float32(count)
+        M_fac = np.float32((M_t * np.float32(Nd) + np.float32(1)) / (M_t - np.float32(1)))
+        zap = False
+        for p in range(npol):
+            S1 = 0.0
+            S2 = 0.0
+            for ip in range(npart):                 # sequential double sums
+                S1 += float(sums[ip, c, p, 0])
+                S2 += float(sums[ip, c, p, 1])
+            SK = float(M_fac) * (float(M_t) * (S2 / (S1 * S1)) - 1)
+            if SK > float(hi) or SK < float(lo):
+                zap = True
+        if zap:
+            mask[:, c] = 1
+    return mask
+
+
 def sk_limits(M, Nd=1, std_devs=3.0, ntest=1):
     """(lower, upper) float32 thresholds of SKLimits::calc_limits."""
     lo, hi = ctypes.c_float(), ctypes.c_float()
@@ -441,6 +472,21 @@ def fold_accumulate(data, binplan, nbin, profiles=None, hits=None):
     fn = lib().orc_fold_accumulate_f64 if f64 else lib().orc_fold_accumulate
     fn(np.ascontiguousarray(data).ravel(), ndat, ndat, nchan, npol, 1,
        np.ascontiguousarray(binplan, np.uint32), nbin, profiles.reshape(-1), hits)
+    return profiles, hits
+
+
+def fold_accumulate_zeroed(data, binplan, nbin, profiles, hits):
+    """Fold::fold of data with zeroed samples (Signal/Pulsar/Fold.C:895-930,
+    zeroed_samples true, one hits array for all channels): every sample is
+    added to its bin in sequence (zeroed ones add nothing); a hit is counted
+    for each channel sample whose first polarisation's value is non-zero.
+    data: float (nchan, npol, ndat); profiles (nchan, npol, nbin) and hits
+    (nbin) are updated in place."""
+    scratch = np.zeros_like(hits)
+    fold_accumulate(data, binplan, nbin, profiles, scratch)
+    plan = np.asarray(binplan, np.int64)
+    for c in range(data.shape[0]):
+        np.add.at(hits, plan[data[c, 0] != 0], 1)
     return profiles, hits
 
 

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -193,6 +194,188 @@ int main ()
       CHECK (std::sqrt (leak / r2) < 1e-5, "filterbank during leakage %g", std::sqrt (leak / r2));
       cudaFree (d_in);
       cudaFree (d_out);
+    }
+
+    // dsp::Unpacker: the 8-bit class equals unpack8; the 16-bit class gives
+    // float(x) + 0.5 with offset binary undone (SixteenBitUnpacker.C:54-79)
+    {
+      b200::Unpacker u8 (ctx, b200::Unpacker::EightBit), u16 (ctx, b200::Unpacker::SixteenBit);
+      CHECK (u8.matches (8) && !u8.matches (16) && u16.matches (16), "Unpacker::matches");
+      u8.set_table (lut);
+      b200::TimeSeriesView y8 = x;
+      y8.base = d_y;
+      u8.unpack (d_raw, y8);
+      std::vector<float> a (ndat * npol * 2), b (ndat * npol * 2);
+      ctx.synchronize ();
+      cudaMemcpy (a.data (), d_x, a.size () * 4, cudaMemcpyDeviceToHost);
+      cudaMemcpy (b.data (), d_y, b.size () * 4, cudaMemcpyDeviceToHost);
+      CHECK (a == b, "8-bit Unpacker differs from unpack8");
+      const uint64_t n16 = 1000;
+      std::vector<uint16_t> w (n16 * 2 * 2);
+      for (size_t i = 0; i < w.size (); i++) w[i] = uint16_t (i * 2654435761u);
+      void* d_w = nullptr;
+      float* d_f = nullptr;
+      cudaMalloc (&d_w, w.size () * 2);
+      cudaMalloc (&d_f, n16 * 2 * 2 * 4);
+      cudaMemcpy (d_w, w.data (), w.size () * 2, cudaMemcpyHostToDevice);
+      b200::TimeSeriesView f;
+      f.base = d_f;
+      f.span_floats = n16 * 2;
+      f.ndat = n16;
+      f.nchan = 1;
+      f.npol = 2;
+      u16.set_offset_binary (true);
+      u16.unpack (d_w, f);
+      std::vector<float> hf (n16 * 2 * 2);
+      ctx.synchronize ();
+      cudaMemcpy (hf.data (), d_f, hf.size () * 4, cudaMemcpyDeviceToHost);
+      for (uint64_t t = 0; t < n16; t++)
+        for (unsigned p = 0; p < 2; p++)
+          for (unsigned d = 0; d < 2; d++)
+          {
+            const int16_t v = int16_t (w[(t * 2 + p) * 2 + d] ^ 0x8000);
+            CHECK (hf[p * n16 * 2 + t * 2 + d] == float (v) + 0.5f, "16-bit value at %llu",
+                   (unsigned long long) t);
+          }
+      cudaFree (d_w);
+      cudaFree (d_f);
+    }
+
+    // SpectralKurtosis engine steps: an outlying block is zapped by
+    // detect_ft and zeroed by mask; the rest passes unchanged
+    {
+      const unsigned sc = 4, sp = 2, M = 256;
+      const uint64_t sn = 16 * M;
+      std::vector<float> v (uint64_t (sc) * sp * sn * 2);
+      uint64_t state = 12345;
+      auto gauss = [&state] () {
+        double u = 0;
+        for (int k = 0; k < 12; k++)
+        {
+          state = state * 6364136223846793005ull + 1442695040888963407ull;
+          u += double (state >> 11) / double (1ull << 53);
+        }
+        return float (u - 6.0);
+      };
+      for (auto& e : v) e = gauss ();
+      // channel 2, block 5: a few huge samples (impulsive RFI)
+      for (unsigned p = 0; p < sp; p++)
+        for (uint64_t t = 5 * M; t < 5 * M + 8; t++) v[((2 * sp + p) * sn + t) * 2] = 300.f;
+      float *d_v = nullptr, *d_o = nullptr, *d_s = nullptr;
+      uint32_t* d_c = nullptr;
+      uint8_t* d_m = nullptr;
+      const uint64_t npart = sn / M;
+      cudaMalloc (&d_v, v.size () * 4);
+      cudaMalloc (&d_o, v.size () * 4);
+      cudaMalloc (&d_s, npart * sc * sp * 2 * 4);
+      cudaMalloc (&d_c, npart * sc * 4);
+      cudaMalloc (&d_m, npart * sc);
+      cudaMemcpy (d_v, v.data (), v.size () * 4, cudaMemcpyHostToDevice);
+      b200::TimeSeriesView in;
+      in.base = d_v;
+      in.span_floats = sn * 2;
+      in.ndat = sn;
+      in.nchan = sc;
+      in.npol = sp;
+      b200::TimeSeriesView out = in;
+      out.base = d_o;
+      b200::SpectralKurtosisEngine sk (ctx);
+      sk.setup (1);
+      b200::SKSums sums;
+      sums.sums = d_s;
+      sums.counts = d_c;
+      CHECK (sk.compute (in, sums, M) == npart, "SK compute npart");
+      float lo = 0, hi = 0;
+      ctx.check (dspsr_b200_sk_limits (M, 1, 3.f, sp, &lo, &hi), "sk limits");
+      sk.reset_mask (d_m, npart, sc);
+      sk.detect_ft (sums, d_m, hi, lo);
+      const uint64_t nz = sk.count_mask (d_m, npart, sc);
+      std::vector<uint8_t> hm (npart * sc);
+      cudaMemcpy (hm.data (), d_m, hm.size (), cudaMemcpyDeviceToHost);
+      CHECK (hm[5 * sc + 2] == 1, "SK missed the outlying block");
+      CHECK (nz >= 1 && nz <= 4, "SK zapped %llu cells", (unsigned long long) nz);
+      sk.mask (d_m, in, out, M);
+      std::vector<float> ho (v.size ());
+      ctx.synchronize ();
+      cudaMemcpy (ho.data (), d_o, ho.size () * 4, cudaMemcpyDeviceToHost);
+      for (unsigned c = 0; c < sc; c++)
+        for (unsigned p = 0; p < sp; p++)
+          for (uint64_t t = 0; t < sn; t++)
+          {
+            const uint64_t i = ((c * sp + p) * sn + t) * 2;
+            const bool z = hm[(t / M) * sc + c] != 0;
+            CHECK (z ? (ho[i] == 0.f && ho[i + 1] == 0.f) : (ho[i] == v[i] && ho[i + 1] == v[i + 1]),
+                   "SK mask at chan %u sample %llu", c, (unsigned long long) t);
+          }
+      cudaFree (d_v);
+      cudaFree (d_o);
+      cudaFree (d_s);
+      cudaFree (d_c);
+      cudaFree (d_m);
+    }
+
+    // InverseFilterbank engine: a tone channelised exactly (fine channel c
+    // holds wideband bins c*keep + s, s signed, channel 0 on DC) comes back
+    // as L times the tone (256 channels of 64 points, 4/3 oversampled:
+    // 48 kept bins, L = 12288)
+    {
+      const unsigned inch = 256, lin = 64, keep = 48, L = inch * keep, f0 = 1000;
+      std::vector<float> xin (uint64_t (inch) * lin * 2, 0.f);
+      for (unsigned c = 0; c < inch; c++)
+        for (int s = -int (lin) / 2; s < int (lin) / 2; s++)
+          if ((int64_t (c) * keep + s + L) % L == f0)
+            for (unsigned m = 0; m < lin; m++)
+            {
+              const double a = 2 * M_PI * double (s) * m / lin;
+              xin[(uint64_t (c) * lin + m) * 2] += float (double (L) / lin * std::cos (a));
+              xin[(uint64_t (c) * lin + m) * 2 + 1] += float (double (L) / lin * std::sin (a));
+            }
+      dspsr_b200_ifb_config cfg {};
+      cfg.input_nchan = inch;
+      cfg.output_nchan = 1;
+      cfg.pfb_nchan = inch;
+      cfg.npol = 1;
+      cfg.input_fft_length = lin;
+      cfg.os_num = 4;
+      cfg.os_den = 3;
+      cfg.pfb_dc_chan = 1;
+      cfg.pfb_all_chan = 1;
+      cfg.dual_sideband = 1;
+      b200::InverseFilterbankEngine ifb (ctx);
+      ifb.setup (cfg);
+      const std::vector<uint64_t> info = ifb.info ();
+      CHECK (info[0] == keep && info[1] == L, "IFB kept %llu Lout %llu",
+             (unsigned long long) info[0], (unsigned long long) info[1]);
+      float *d_i = nullptr, *d_o = nullptr;
+      cudaMalloc (&d_i, xin.size () * 4);
+      cudaMalloc (&d_o, uint64_t (L) * 2 * 4);
+      cudaMemcpy (d_i, xin.data (), xin.size () * 4, cudaMemcpyHostToDevice);
+      b200::TimeSeriesView in;
+      in.base = d_i;
+      in.span_floats = lin * 2;
+      in.ndat = lin;
+      in.nchan = inch;
+      in.npol = 1;
+      b200::TimeSeriesView out;
+      out.base = d_o;
+      out.span_floats = uint64_t (L) * 2;
+      out.nchan = 1;
+      out.npol = 1;
+      CHECK (ifb.perform (in, out) == 1 && out.ndat == L, "IFB npart / ndat");
+      std::vector<float> ho (uint64_t (L) * 2);
+      ctx.synchronize ();
+      cudaMemcpy (ho.data (), d_o, ho.size () * 4, cudaMemcpyDeviceToHost);
+      double e2 = 0, r2 = 0;
+      for (unsigned n = 0; n < L; n++)
+      {
+        const double a = 2 * M_PI * double ((uint64_t (f0) * n) % L) / L;
+        const double re = double (L) * std::cos (a), im = double (L) * std::sin (a);
+        e2 += (ho[2 * n] - re) * (ho[2 * n] - re) + (ho[2 * n + 1] - im) * (ho[2 * n + 1] - im);
+        r2 += re * re + im * im;
+      }
+      CHECK (std::sqrt (e2 / r2) < 1e-5, "IFB tone rel err %g", std::sqrt (e2 / r2));
+      cudaFree (d_i);
+      cudaFree (d_o);
     }
 
     cudaFree (d_raw);

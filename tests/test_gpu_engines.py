@@ -374,3 +374,50 @@ def test_convolution_zero_dm_output_is_input(ctx, b2, orc, nfft, pos, neg):
     assert np.isnan(z[:, :, 3 * nk:].view(np.float32)).all()
     assert out.cpu().numpy().tobytes() == out2.cpu().numpy().tobytes()
     conv.close()
+
+
+def test_c2_shape_voltages_within_2e6_of_fp64(ctx, b2, orc):
+    """The C2 shape (256 MHz dual-pol int8 at 1400 MHz, a 64-channel FFT
+    filterbank, each 4 MHz channel dedispersed at DM 500 with 2^16-point
+    FFTs, FP64-phase chirp): the dedispersed voltages of every channel against
+    the all-FP64 oracle chain (FP64 unpack values, filterbank, response and
+    FFTs; Filterbank.C:549-565, Convolution.C:724-803): relative RMS error
+    <= 2e-6 over all channels and polarisations."""
+    cf, bw, dm, nsub, nfft = 1400.0, 256.0, 500.0, 64, 1 << 16
+    pos = orc.smearing_samples(cf, bw, dm, nsub, 1)
+    neg = orc.smearing_samples(cf, bw, dm, nsub, -1)
+    nk = nfft - pos - neg
+    npart = 3
+    nch = nfft + (npart - 1) * nk + 77            # samples per channel
+    ndat = nch * nsub                              # input samples per pol
+    rng = np.random.default_rng(500)
+    raw = np.clip(np.round(rng.standard_normal(ndat * 4) * 12), -128, 127).astype(np.int8)
+    raw = raw.view(np.uint8)
+    lut, _ = b2.bittable8()
+    lut = np.asarray(lut, np.float32)
+
+    # GPU: filterbank engine, then the convolution engine on its channels
+    fbo = torch.zeros((nsub, 2, nch), dtype=torch.complex64, device="cuda")
+    n = ctx.filterbank(b2.INT8_TFPD, dev(raw), ndat, 1, 2, nsub, fbo, nch, lut=lut)
+    assert n == nch
+    freqs = orc.channel_centres(cf, bw, nsub, swap=True, dc_centred=True)
+    c = b2.Convolution(ctx, nsub, 2, nfft, pos, neg)
+    c.set_dedispersion_channels(freqs, bw, dm, chirp_mode=b2.CHIRP_FP64)
+    out = torch.zeros((nsub, 2, npart * nk), dtype=torch.complex64, device="cuda")
+    assert c.perform(fbo, nch, nch, out, npart * nk) == npart
+    ctx.synchronize()
+    c.status()
+    got = out.cpu().numpy()
+    c.close()
+
+    # FP64 oracle chain on the same bytes
+    x = orc.unpack8(raw, ndat, 1, 2, 2, lut).view(np.complex64).reshape(1, 2, ndat)
+    y = orc.filterbank(x.astype(np.complex128), nsub)
+    h = orc.dedispersion_response_channels(freqs, bw, dm, nfft, fp64=True)
+    ref = orc.convolve(y, h, nfft, pos, neg)
+    assert ref.shape == got.shape
+    err = rel_rms(got, ref)
+    assert err < VOLTAGE_RTOL_FP64, err
+    # and channel by channel (no channel may hide behind the average)
+    per = [rel_rms(got[k], ref[k]) for k in range(nsub)]
+    assert max(per) < 2 * VOLTAGE_RTOL_FP64, max(per)

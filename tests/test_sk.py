@@ -197,3 +197,55 @@ def test_sk_rejects_bad_arguments(ctx, b2):
             ctx.sk(a["d_in"], a["in_span"], a["ndat"], a["nchan"], a["npol"], a["M"], 0.5, 1.5,
                    a["d_out"], a["out_span"])
         assert e.value.code == b2._capi.EINVAL, b
+
+
+# ---------------------------------------------------------------- engine steps (GPU)
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nchan,npol,M,ndat,zero_is_valid", [(8, 2, 128, 5157, True),
+                                                             (4, 1, 1024, 12288, False),
+                                                             (16, 2, 64, 1925, True)])
+def test_sk_engine_steps_match_oracle(ctx, b2, orc, nchan, npol, M, ndat, zero_is_valid):
+    """compute / detect_ft / detect_tscr / reset_mask / count_mask / mask,
+    each through the C ABI, against the oracle's restatement of the same step
+    and against the fused single-pass engine."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(nchan * M + npol)
+    span = ndat + (ndat & 1)
+    x = (rng.standard_normal((nchan, npol, span)) + 1j * rng.standard_normal((nchan, npol, span))
+         ).astype(np.complex64)
+    x[0, :, :M] *= 8.0                                   # an outlying block
+    x[nchan - 1, :, 2 * M:3 * M] = 0.0                   # a silent block
+    if nchan > 2:
+        x[1] += 0.8 * np.exp(2j * np.pi * 0.1 * np.arange(span))   # a tone all along channel 1
+    lo, hi = b2.sk_limits(M, 1, 3.0, npol)
+    rs, rc, rm, rout = orc.sk(x, M, lo, hi, zero_is_valid=zero_is_valid, ndat=ndat)
+    npart = ndat // M
+    d = torch.from_numpy(x).cuda()
+    sums = torch.zeros((npart, nchan, npol, 2), dtype=torch.float32, device="cuda")
+    counts = torch.zeros((npart, nchan), dtype=torch.int32, device="cuda")
+    assert ctx.sk_compute(d, span, ndat, nchan, npol, M, sums, counts, zero_is_valid) == npart
+    ctx.synchronize()
+    assert np.array_equal(sums.cpu().numpy(), rs)
+    assert np.array_equal(counts.cpu().numpy().astype(np.uint32), rc)
+    assert np.array_equal(d.cpu().numpy(), x), "compute must not write its input"
+    mask = torch.full((npart, nchan), 7, dtype=torch.uint8, device="cuda")
+    ctx.sk_reset_mask(mask, npart, nchan)
+    ctx.sk_detect_ft(sums, counts, npart, nchan, npol, M, lo, hi, mask)
+    assert np.array_equal(mask.cpu().numpy(), rm)
+    assert ctx.sk_count_mask(mask, npart, nchan) == int(rm.sum())
+    # mask out of place and in place: the oracle's masked copy
+    out = torch.full_like(d, complex(np.nan, np.nan))
+    ctx.sk_mask(mask, d, span, out, span, ndat, nchan, npol, M)
+    ctx.sk_mask(mask, d, span, d, span, ndat, nchan, npol, M)
+    ctx.synchronize()
+    n = npart * M
+    assert np.array_equal(out.cpu().numpy()[..., :n], rout[..., :n])
+    assert np.array_equal(d.cpu().numpy()[..., :n], rout[..., :n])
+    # detect_tscr ORs each zapped channel into every part
+    ref_t = orc.sk_detect_tscr(rs, rc, 1, 3.0)
+    nz = ctx.sk_detect_tscr(sums, counts, npart, nchan, npol, M, 3.0, mask)
+    assert nz == int(ref_t[0].sum())
+    assert np.array_equal(mask.cpu().numpy(), rm | ref_t)
+    if nchan > 2:
+        assert ref_t[0, 1] == 1, "the tone channel is zapped by the time-scrunched test"

@@ -1,14 +1,14 @@
 """dspsr_b200_convolution_perform_noalloc: the overlap-save convolution for
-callers that cannot allocate device memory while they run (inside a stream
-capture someone else replays, in a real-time loop with all memory fixed at
-start-up, or under another allocator that owns the device memory).  It keeps
-its tables and FFT scratch in one static device array instead of an engine
-object.
+callers that cannot allocate device memory while they run (a real-time loop
+with all memory fixed at start-up, or a host whose device memory belongs to
+another allocator).  It keeps its tables and FFT scratch in one static device
+array instead of an engine object.
 
 The test calls it through the C ABI and checks its output against the
 engine-object entry point (dspsr_b200_convolution_perform) on the same input,
-twice in a row, and that the second call leaves the device's free memory
-unchanged.  This file is named to be collected last."""
+twice in a row, that its status word reads 0 after each call, and that the
+second call leaves the device's free memory unchanged.  This file is named to
+be collected last."""
 import ctypes
 
 import numpy as np
@@ -29,12 +29,13 @@ def rel_rms(a, b):
     return float(np.sqrt(np.mean(np.abs(a - b) ** 2) / np.mean(np.abs(b) ** 2)))
 
 
-def call_noalloc(b2, x, ndat, nchan, npol, nfft, pos, neg, h_dev, out):
+def call_noalloc(b2, x, ndat, nchan, npol, nfft, pos, neg, h_dev, out, status=None):
     lib = b2._capi.lib()
     n = ctypes.c_uint64()
     rc = lib.dspsr_b200_convolution_perform_noalloc(
         None, x.data_ptr(), ndat, ndat, nchan, npol, nfft, pos, neg, h_dev.data_ptr(),
-        out.data_ptr(), out.shape[-1], ctypes.byref(n))
+        out.data_ptr(), out.shape[-1], ctypes.byref(n),
+        None if status is None else status.data_ptr())
     return rc, n.value
 
 
@@ -63,15 +64,24 @@ def test_noalloc_matches_engine_entry_point(ctx, b2, nchan, nfft, pos, neg):
     ref = ref.cpu().numpy()
     c.close()
 
+    # a first call with less than one part still sets the device up
+    status = torch.full((1,), 7, dtype=torch.int32, device="cuda")
+    rc, n = call_noalloc(b2, xd, nfft - 1, nchan, npol, nfft, pos, neg, hd, xd, status)
+    torch.cuda.synchronize()
+    assert rc == 0 and n == 0
+    assert int(status.item()) == 0
+
     free_after = None
     for call in range(2):
         out = torch.full((nchan, npol, npart * nk), np.nan, dtype=torch.complex64, device="cuda")
+        status.fill_(7)
         torch.cuda.synchronize()
         free_before = torch.cuda.mem_get_info()[0]
-        rc, n = call_noalloc(b2, xd, ndat, nchan, npol, nfft, pos, neg, hd, out)
+        rc, n = call_noalloc(b2, xd, ndat, nchan, npol, nfft, pos, neg, hd, out, status)
         torch.cuda.synchronize()
         assert rc == 0, rc
         assert n == npart
+        assert int(status.item()) == 0, "a device-side wait gave up"
         got = out.cpu().numpy()
         assert np.all(np.isfinite(got))
         assert rel_rms(got, ref) < NOALLOC_RTOL, (call, rel_rms(got, ref))
