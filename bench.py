@@ -946,11 +946,83 @@ def run_b200_sk(args, cfg, world, rank, local):
                 "h2d_bytes_per_step": int(hx.numel() * 4),
                 "d2h_bytes_per_step": int(hout.numel() * 4 + hmask.numel())},
     }
+    if not args.no_proposer:
+        line["proposer"] = sk_proposer(args, cfg, b2, ctx, device, lo, hi, rank, world)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sk(cfg)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
+
+
+def sk_proposer(args, cfg, b2, ctx, device, lo, hi, rank, world):
+    """The learned RFI-mask proposer in front of SpectralKurtosis: trained on
+    the SK masks of one RFI-injected block, judged by SK on another (miss =
+    SK zaps, proposer keeps; false zap = SK keeps, proposer zaps), alone and
+    with the SK fallback below the confidence threshold; its throughput is
+    that of the feature + tensor-core inference kernels on the SK sums."""
+    import torch
+    nchan, npol, ndat, M = cfg["nchan"], cfg["npol"], cfg["ndat"], cfg["M"]
+    npart = ndat // M
+    conf = 0.9
+
+    def sk_of(seed):
+        x = make_sk_block(cfg, seed, device)
+        sums = torch.empty(npart * nchan * npol * 2, dtype=torch.float32, device=device)
+        counts = torch.empty(npart * nchan, dtype=torch.int32, device=device)
+        mask = torch.empty(npart * nchan, dtype=torch.uint8, device=device)
+        ctx.sk(x, ndat, ndat, nchan, npol, M, lo, hi, x, ndat, sums, counts, mask)
+        torch.cuda.synchronize()
+        del x
+        torch.cuda.empty_cache()
+        return sums, counts, mask
+
+    pr = b2.RfiProposer(ctx, nchan, M, max_npart=npart, max_batch_blocks=32, seed=7)
+    sums, counts, mask = sk_of(9001 + rank)
+    pr.features(sums, npart, npol, counts)
+    t0 = time.perf_counter()
+    loss0 = pr.train(mask, 20, batch_blocks=32, lr=3e-3)
+    loss1 = pr.train(mask, args.proposer_steps, batch_blocks=32, lr=3e-3)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    sums2, counts2, mask2 = sk_of(9101 + rank)
+    alone = torch.empty(npart * nchan, dtype=torch.uint8, device=device)
+    fb = torch.empty_like(alone)
+    prob = torch.empty(npart * nchan, dtype=torch.float32, device=device)
+    # timed: features from the sums + inference with the fallback
+    for _ in range(3):
+        pr.features(sums2, npart, npol, counts2)
+        pr.infer(fb, prob, mask2, confidence=conf)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        pr.features(sums2, npart, npol, counts2)
+        pr.infer(fb, prob, mask2, confidence=conf, count=False)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), world) / args.steps
+    nfall = pr.infer(fb, prob, mask2, confidence=conf)
+    pr.infer(alone, None, None, confidence=0.5)
+    sk = mask2.bool()
+    a, f = alone.bool(), fb.bool()
+    nsk, nkeep = int(sk.sum()), int((~sk).sum())
+
+    def rates(m):
+        return {"miss_rate": round(int((sk & ~m).sum()) / max(nsk, 1), 5),
+                "false_zap_rate": round(int((~sk & m).sum()) / max(nkeep, 1), 6)}
+
+    pr.close()
+    return {"train": {"steps": 20 + args.proposer_steps, "batch_blocks": 32,
+                      "loss_first": round(loss0, 5), "loss_last": round(loss1, 5),
+                      "seconds": round(train_s, 2)},
+            "sk_zapped_cells": nsk, "cells": int(sk.numel()),
+            "alone": rates(a), "with_sk_fallback": dict(rates(f), confidence=conf,
+                                                          fallback_cells=int(nfall)),
+            "ms_per_block": round(ms, 4),
+            "value": round(nchan * npol * ndat / (ms / 1e3) / 1e6, 1),
+            "unit": "complex Msamples/s (features + inference on the SK sums)",
+            "params": 3937, "weights": "BF16 on the tensor cores, FP32 master copy"}
 
 
 # ---------------------------------------------------------------------------
@@ -1019,15 +1091,9 @@ def run_b200_ifb(args, cfg, world, rank, local):
     ndat = cfg["ndat"]
     npart = ifb.npart(ndat)
     # int16 TFPD voltages (seeded Gaussian, sigma 100), generated on the GPU
-    gen = torch.Generator(device=device)
-    gen.manual_seed(99 + rank)
-    raw = torch.empty((ndat, cfg["nin"], cfg["npol"], 2), dtype=torch.int16, device=device)
-    chunk = 1 << 18
-    for t0 in range(0, ndat, chunk):
-        n = min(chunk, ndat - t0)
-        raw[t0:t0 + n] = (torch.randn((n, cfg["nin"], cfg["npol"], 2), generator=gen,
-                                      device=device) * 100).round().to(torch.int16)
-    raw = raw.reshape(-1)
+    t_gen = time.perf_counter()
+    raw = make_pfb_block(cfg, 99 + rank, device)
+    t_gen = time.perf_counter() - t_gen
     out = torch.empty((1, cfg["npol"], npart * out_step, 2), dtype=torch.float32, device=device)
     samples_per_step = cfg["nin"] * cfg["npol"] * npart * in_step
 
@@ -1066,7 +1132,10 @@ def run_b200_ifb(args, cfg, world, rank, local):
         "unit": "complex Msamples/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded Gaussian int16 PFB-channel voltages)",
+        "data": ("synthetic: one periodic second of 800 MHz complex baseband (seeded Gaussian "
+                 "noise + a 1.6 ms pulsar, 3 % duty, at DM 1000 by an FP64 inverse chirp) "
+                 "channelised by a 12-tap-per-channel Kaiser-windowed 4/3-oversampled PFB "
+                 f"into 256 int16 channels (generated on the GPU in {t_gen:.1f} s)"),
         "config": {"workload": cfg["workload"], "npart": npart, "input_fft_length": cfg["lin"],
                    "output_fft_length": info["lout"], "fft_split": [info["n1"], info["n2"]],
                    "parts_per_batch": info["max_batch"],
@@ -1339,23 +1408,44 @@ def run_b200_c3(args, cfg, world, rank, local):
         s["tstream"] = torch.cuda.Stream(device=device)
         s["ctx"] = b2.Context(local, s["tstream"].cuda_stream)
 
-    def make_pipe(s, scratch):
+    def make_pipe(s, plan):
+        scratch, row, fft = plan
         c = b2.make_config(cfg["cf"], s["bw"], s["dm"], s["nchan"], 2, s["nfft"], s["pos"],
                            s["neg"], s["nbin"], s["period"], state=b2.INTENSITY, lut=lut,
-                           start_mjd=START_MJD, epoch_mjd=EPOCH_MJD, scratch_bytes=scratch)
+                           start_mjd=START_MJD, epoch_mjd=EPOCH_MJD, scratch_bytes=scratch,
+                           row_length=row, fft_precision=fft)
         return b2.Pipeline(s["ctx"], c)
 
-    # autotuner: per shape class (FFT length, channels) the FFT-batch scratch
-    # that runs one block fastest, timed alone on the stream
+    def plans(nfft):
+        """The autotuner's candidates for one FFT length: the four-step split
+        (8192- or 4096-point rows, i.e. nfft/8192 or nfft/4096 columns), the
+        rows' arithmetic (FP32 CUDA cores, or the three-term split-BF16
+        tensor-core DFT stages, which hold the FP32 error bar) and the
+        scratch budget of the FFT batches."""
+        out = []
+        for sc in (64 << 20, 256 << 20, 1024 << 20):
+            if nfft <= 8192:
+                out.append((sc, 0, b2.FFT_FP32))
+                if nfft == 8192:
+                    out.append((sc, 4096, b2.FFT_FP32))
+                continue
+            out.append((sc, 8192, b2.FFT_FP32))
+            if args.c3_tensor:
+                out.append((sc, 8192, b2.FFT_BF16X3))
+            if nfft <= 131072:
+                out.append((sc, 4096, b2.FFT_FP32))
+        return out
+
+    # autotuner: per shape class (FFT length, channels) the plan that runs one
+    # block fastest, timed alone on the stream
     tuned = {}
-    candidates = [64 << 20, 256 << 20, 1024 << 20]
     t_tune = time.perf_counter()
     for s in streams:
         key = (s["nfft"], s["nchan"])
         if key not in tuned:
             best = None
-            for sc in candidates:
-                pl = make_pipe(s, sc)
+            for plan in plans(s["nfft"]):
+                pl = make_pipe(s, plan)
                 for w in range(2):
                     pl.run(s["blocks"][w % nblk], s["ndat"])
                 st = s["tstream"]
@@ -1367,10 +1457,11 @@ def run_b200_c3(args, cfg, world, rank, local):
                 ms = e0.elapsed_time(e1)
                 pl.close()
                 if best is None or ms < best[0]:
-                    best = (ms, sc)
+                    best = (ms, plan)
             tuned[key] = best[1]
-        s["scratch"] = tuned[key]
-        s["pipe"] = make_pipe(s, s["scratch"])
+        s["plan"] = tuned[key]
+        s["scratch"] = tuned[key][0]
+        s["pipe"] = make_pipe(s, s["plan"])
     t_tune = time.perf_counter() - t_tune
     torch.cuda.synchronize()
     samples_per_step = sum(s["ndat"] * s["nchan"] * 2 for s in streams)
@@ -1463,7 +1554,10 @@ def run_b200_c3(args, cfg, world, rank, local):
         "data": "synthetic (seeded Gaussian noise, int8)",
         "config": {"workload": cfg["workload"], "streams": len(streams),
                    "shape_classes": [list(x) for x in shapes],
-                   "tuned_scratch_mib": {f"{k[0]}x{k[1]}": v >> 20 for k, v in tuned.items()},
+                   "tuned": {f"{k[0]}x{k[1]}": {"scratch_mib": v[0] >> 20,
+                                                  "row_length": v[1] or min(k[0], 8192),
+                                                  "rows": "bf16x3 tensor" if v[2] == 3 else "fp32"}
+                             for k, v in tuned.items()},
                    "autotune_s": round(t_tune, 2),
                    "schedule": "pipelines one after another on the device",
                    "concurrent_streams_value": round(conc_value, 3),
@@ -1573,6 +1667,94 @@ def run_reference_c5(args, cfg, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def make_pfb_block(cfg, seed, device, taps=12, beta=8.0, duty=0.03, snr=10.0):
+    """nin channels of a 4/3-oversampled polyphase filterbank of one second
+    of complex baseband at |bw| MHz: seeded Gaussian noise plus a pulsar of
+    cfg's period (noise switched on for `duty` of each turn) dispersed at
+    cfg's DM by an FP64 inverse chirp over the whole second (the second holds
+    a whole number of turns, so the circular chirp is exact).  The prototype
+    filter is a Kaiser-windowed sinc of taps * nin points with its cut-off at
+    half the channel spacing (pfb_channelise).  Returns int16 TFPD
+    [ndat][nin][npol][2], scaled to a noise sigma of about 300.  torch is the
+    synthesis tool here (it is not on the product path)."""
+    import torch
+    from dspsr_b200 import synth
+    nin, npol, ndat = cfg["nin"], cfg["npol"], cfg["ndat"]
+    L = taps * nin
+    nw = int(round(abs(cfg["bw"]) * 1e6))          # one second of wideband samples
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    k = torch.arange(L, device=device, dtype=torch.float64) - (L - 1) / 2
+    h = torch.sinc(k / nin) * torch.kaiser_window(L, periodic=False, beta=beta,
+                                                   dtype=torch.float64, device=device)
+    h = (h / h.sum()).to(torch.float32)
+    out = torch.empty((ndat, nin, npol, 2), dtype=torch.int16, device=device)
+    rate = abs(cfg["bw"]) * 1e6
+    d = cfg["dm"] / synth.DM_DISPERSION * 1e6
+    cf, bw = cfg["cf"], cfg["bw"]
+    for p in range(npol):
+        t = (torch.arange(nw, device=device, dtype=torch.float64) + 0.5) / rate
+        on = (torch.remainder(t / cfg["period"] - 0.3, 1.0) < duty).to(torch.float32)
+        del t
+        x = torch.complex(torch.randn(nw, generator=gen, device=device),
+                          torch.randn(nw, generator=gen, device=device)) * (np.sqrt(snr / 2) * on)
+        del on
+        X = torch.fft.fft(x)
+        del x
+        chunk = 1 << 26
+        for a in range(0, nw, chunk):
+            kk = torch.arange(a, min(a + chunk, nw), device=device, dtype=torch.float64)
+            kk = torch.where(kk >= (nw + 1) // 2, kk - nw, kk)      # FFT order
+            f = kk * (bw / nw)
+            ph = torch.remainder(2 * np.pi * d * f * f / (cf * cf * (cf + f)) * np.sign(bw),
+                                 2 * np.pi)
+            X[a:a + kk.numel()] *= torch.polar(torch.ones_like(ph), ph).to(torch.complex64)
+            del kk, f, ph
+        x = torch.fft.ifft(X)
+        del X
+        x += torch.complex(torch.randn(nw, generator=gen, device=device),
+                           torch.randn(nw, generator=gen, device=device)) * np.sqrt(0.5)
+        for m0, y in pfb_channelise(x, h, nin, taps, ndat):
+            n = y.shape[0]
+            out[m0:m0 + n, :, p, 0] = torch.clamp(torch.round(y.real * 300 * np.sqrt(nin)),
+                                                  -32768, 32767).to(torch.int16)
+            out[m0:m0 + n, :, p, 1] = torch.clamp(torch.round(y.imag * 300 * np.sqrt(nin)),
+                                                  -32768, 32767).to(torch.int16)
+        del x
+        torch.cuda.empty_cache()
+    torch.cuda.synchronize()
+    return out.reshape(-1)
+
+
+def pfb_channelise(x, h, nin, taps, ndat, mch=1 << 15):
+    """The oversampled PFB of a periodic signal x (complex64, one period):
+    yields (m0, y[m, c]) chunks, y[m, c] = sum_k h[k] x[(mD - k) mod len(x)]
+    exp(-2 pi i c (mD - k) / nin), D = 3 nin / 4: the band around c fs / nin
+    shifted to DC, sampled every D samples (channel 0 on DC)."""
+    import torch
+    nw, D, L = x.numel(), nin * 3 // 4, taps * nin
+    device = x.device
+    hr = torch.flip(h, [0]).to(torch.complex64)
+    c = torch.arange(nin, device=device, dtype=torch.float64)
+    # xs[i] = x[(i - (L - 1)) mod nw]; frame m reads xs[mD + j], k = L - 1 - j
+    need = (ndat - 1) * D + L
+    reps = (need + nw - 1) // nw + 1
+    xs = torch.cat([x[nw - (L - 1):]] + [x] * reps)[:need]
+    for m0 in range(0, ndat, mch):
+        m1 = min(ndat, m0 + mch)
+        frames = xs.as_strided((m1 - m0, L), (D, 1), m0 * D)
+        # z[r] = sum over k = r (mod nin) of h[k] x[mD - k]; then
+        # sum_k h[k] x[mD - k] exp(2 pi i c k / nin) = nin * ifft(z)[c]
+        z = (frames * hr).reshape(m1 - m0, taps, nin)
+        z = torch.flip(z, [1, 2]).sum(1)
+        z = torch.roll(z, shifts=-(nin - 1 - (L - 1) % nin) % nin, dims=1)
+        y = torch.fft.ifft(z, dim=1) * nin
+        m = torch.arange(m0, m1, device=device, dtype=torch.float64)
+        rot = torch.remainder(torch.outer(m * D, c), nin) * (-2 * np.pi / nin)
+        yield m0, y * torch.polar(torch.ones_like(rot), rot).to(torch.complex64)
+    del xs
+
+
 def run_b200_c5(args, cfg, world, rank, local):
     import math
     import torch
@@ -1671,7 +1853,9 @@ def run_b200_c5(args, cfg, world, rank, local):
                      "traffic": None, "peak_source": peak_src,
                      "note": "algorithmic bytes: the int16 input once; FFT-bound chain"},
         "e2e": None,
-        "check": {"hits_total": int(hits.sum())},
+        "check": {"hits_total": int(hits.sum()),
+                  "profile_peak_over_median": float(np.max(prof[:, 0].sum(0))
+                                                    / max(np.median(prof[:, 0].sum(0)), 1e-30))},
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -1688,6 +1872,12 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--c3-tensor", type=int, default=1,
+                    help="c3: let the autotuner also try the tensor-core rows (1) or not (0)")
+    ap.add_argument("--no-proposer", action="store_true",
+                    help="c4: skip the learned RFI-mask proposer")
+    ap.add_argument("--proposer-steps", type=int, default=600,
+                    help="c4: Adam steps of the proposer's training")
     ap.add_argument("--fft", default="fp32,bf16x3,bf16x2",
                     help="row-FFT arithmetic forms to time (comma list of fp32, bf16x3, "
                          "bf16x2); the first is the line's value, the others go under "

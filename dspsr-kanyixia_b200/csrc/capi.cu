@@ -142,8 +142,10 @@ struct dspsr_b200_convolution
 
   int set_fft_precision (int mode);
 
+  // row_len: the four-step row length, 8192 (0 = default) or 4096 (nfft
+  // from 8192 to 131072: then n1 = nfft / 4096 columns)
   int init (dspsr_b200_context* c, unsigned nchan, unsigned npol, unsigned nfft,
-            unsigned pos, unsigned neg, uint64_t scratch_bytes);
+            unsigned pos, unsigned neg, uint64_t scratch_bytes, unsigned row_len = 0);
   ConvTables tables () const
   {
     ConvTables t;
@@ -188,7 +190,7 @@ struct dspsr_b200_convolution
 
 int dspsr_b200_convolution::init (dspsr_b200_context* c, unsigned nchan, unsigned npol,
                                   unsigned nfft, unsigned pos, unsigned neg,
-                                  uint64_t scratch_bytes)
+                                  uint64_t scratch_bytes, unsigned row_len)
 {
   ctx = c;
   if (nchan == 0 || npol == 0 || npol > 2)
@@ -205,7 +207,18 @@ int dspsr_b200_convolution::init (dspsr_b200_context* c, unsigned nchan, unsigne
   shape.nfilt_pos = pos;
   shape.nfilt_neg = neg;
   shape.nkeep = nfft - pos - neg;
-  if (nfft <= 8192)
+  if (row_len != 0 && row_len != 4096 && row_len != 8192)
+    return fail (ctx, DSPSR_B200_EINVAL, "convolution: row length %u is not 4096 or 8192",
+                 row_len);
+  if (row_len == 4096 && nfft >= 8192)
+  {
+    if (nfft > 131072)
+      return fail (ctx, DSPSR_B200_EINVAL,
+                   "convolution: 4096-point rows need nfft <= 131072 (nfft=%u)", nfft);
+    shape.n2 = 4096;
+    shape.n1 = nfft / 4096;
+  }
+  else if (nfft <= 8192)
   {
     shape.n1 = 1;
     shape.n2 = nfft;
@@ -2678,7 +2691,7 @@ int dspsr_b200_pipeline_create (dspsr_b200_context* ctx, const dspsr_b200_pipeli
   const unsigned nchan = fb ? cfg->nchan * fb : cfg->nchan;
   pl->rate = std::fabs (cfg->bandwidth_mhz) / double (nchan) * 1e6;
   int rc = pl->conv.init (ctx, nchan, cfg->npol, cfg->nfft, cfg->nfilt_pos, cfg->nfilt_neg,
-                          cfg->scratch_bytes);
+                          cfg->scratch_bytes, cfg->row_length);
   if (!rc && cfg->fft_precision != DSPSR_B200_FFT_FP32)
     rc = pl->conv.set_fft_precision (cfg->fft_precision);
   if (!rc && cfg->interchannel)

@@ -310,13 +310,14 @@ class RfiProposer:
             ctypes.byref(loss)), "rfi_proposer_train")
         return loss.value
 
-    def infer(self, d_mask, d_prob=None, d_sk_mask=None, confidence=0.9):
-        """Returns the number of (block, channel) cells that fell back to SK."""
+    def infer(self, d_mask, d_prob=None, d_sk_mask=None, confidence=0.9, count=True):
+        """Returns the number of (block, channel) cells that fell back to SK
+        (count=False: queued without waiting, returns None)."""
         n = ctypes.c_uint64()
         self.ctx.check(self._lib.dspsr_b200_rfi_proposer_infer(
             self.handle, _ptr(d_sk_mask), confidence, _ptr(d_mask), _ptr(d_prob),
-            ctypes.byref(n)), "rfi_proposer_infer")
-        return n.value
+            ctypes.byref(n) if count else None), "rfi_proposer_infer")
+        return n.value if count else None
 
     def params(self):
         n = ctypes.c_uint()
@@ -968,7 +969,7 @@ def make_config(centre_freq, bandwidth, dm, nchan, npol, nfft, nfilt_pos, nfilt_
                 dual_sideband=1, offset_binary=0, scratch_bytes=0, filterbank_nchan=0,
                 subint_seconds=0.0, subint_turns=0.0, subint_slots=0,
                 subint_epoch=(0, 0, 0.0), fused_filterbank=0, interchannel=0,
-                fft_precision=FFT_FP32, sk_M=0, sk_std_devs=3.0):
+                fft_precision=FFT_FP32, sk_M=0, sk_std_devs=3.0, row_length=0):
     """Fill a PipelineConfig (the fields DedispersionPipe / LoadToFold set up).
     With filterbank_nchan > 1, nchan counts input channels, and nfft and the
     smearing (nfilt_pos, nfilt_neg) refer to the filterbank's output channels."""
@@ -1007,6 +1008,7 @@ def make_config(centre_freq, bandwidth, dm, nchan, npol, nfft, nfilt_pos, nfilt_
     cfg.fft_precision = fft_precision
     cfg.sk_M = sk_M
     cfg.sk_std_devs = sk_std_devs
+    cfg.row_length = row_length
     return cfg
 
 

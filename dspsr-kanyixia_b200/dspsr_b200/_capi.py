@@ -70,6 +70,7 @@ class PipelineConfig(ctypes.Structure):
         ("fft_precision", c_int),
         ("sk_M", c_uint),
         ("sk_std_devs", ctypes.c_float),
+        ("row_length", c_uint),
     ]
 
 

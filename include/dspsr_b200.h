@@ -643,6 +643,10 @@ typedef struct
      on its own (fused_filterbank is ignored). */
   unsigned sk_M;
   float sk_std_devs;
+  /* tuning: the four-step split's row length, 8192 (0 = default) or 4096
+     (nfft from 8192 to 131072, n1 = nfft / 4096 columns; the tensor-core rows
+     need 8192) */
+  unsigned row_length;
 } dspsr_b200_pipeline_config;
 
 int dspsr_b200_pipeline_create (dspsr_b200_context* ctx,

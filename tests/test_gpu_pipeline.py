@@ -202,7 +202,8 @@ def run_pipeline(ctx, b2, blocks, cfg, host=False):
                        input_kind=cfg["kind"], lut=cfg["lut"], start_mjd=START, epoch_mjd=EPOCH,
                        scratch_bytes=cfg.get("scratch", 0),
                        chirp_mode=cfg.get("chirp", b2.CHIRP_REFERENCE),
-                       filterbank_nchan=cfg.get("fb", 0))
+                       filterbank_nchan=cfg.get("fb", 0), row_length=cfg.get("row", 0),
+                       fft_precision=cfg.get("fft", 0))
     pl = b2.Pipeline(ctx, c)
     total = 0
     for r in blocks:
@@ -278,6 +279,12 @@ CASES = {
     "c2_fb64k_table": dict(dm=500.0, bw=256.0, fb=64, nfft=1 << 16, state=3, nbin=2048,
                            period=5.757e-3, lut=(np.asarray(__import__("dspsr_b200").bittable8()[0])
                                                  * (1 + 1e-3 * np.cos(np.arange(256)))).astype(np.float32)),
+    # the four-step split with 4096-point rows (n1 = 8 and 32 columns)
+    "rows4096_2p15": dict(dm=30.0, bw=64.0, nchan=2, nfft=1 << 15, state=2, nbin=256,
+                          row=4096),
+    "rows4096_2p17": dict(dm=67.99, nfft=1 << 17, nbin=1024, period=0.08933, row=4096),
+    # the rows on the tensor cores (three BF16 terms), four channels
+    "tensor_rows_4ch": dict(dm=8.0, bw=32.0, nchan=4, nfft=1 << 15, state=3, nbin=256, fft=3),
     "fused8k_table": dict(dm=5.0, lut=(np.asarray(__import__("dspsr_b200").bittable8()[0])
                                        * (1 + 1e-3 * np.sin(np.arange(256)))).astype(np.float32)),
 }
