@@ -26,9 +26,11 @@
 // (x = x0 + x1 [+ x2], each term the BF16 rounding of what the previous ones
 // left), and the MMAs form the products whose order is below the last term
 // kept: NS = 2 -> x0 w0 + x0 w1 + x1 w0 (about 16 significant bits), NS = 3 ->
-// also x0 w2 + x2 w0 + x1 w1 (about 24 bits, i.e. FP32 accuracy).  The sums
-// accumulate in FP32 in tensor memory (tcgen05.mma kind::f16, M = 128,
-// N = 32 or 64, one elected thread issues; tcgen05.commit arrives on an
+// also x0 w2 + x2 w0 + x1 w1 (about 24 bits, i.e. FP32 accuracy).  The DFT
+// terms are stacked along N, so each data term is one MMA against all the
+// DFT terms it pairs with (read once per stage, not once per product).  The
+// sums accumulate in FP32 in tensor memory (tcgen05.mma kind::f16, M = 128,
+// N = 32 ... 192, one elected thread issues; tcgen05.commit arrives on an
 // mbarrier the block waits on, bounded).  Each thread then reads its row of
 // the accumulator (tcgen05.ld 32x32b), applies the twiddles in FP32, splits
 // again and writes the next stage's operand rows in shared memory.  Twiddles
@@ -64,21 +66,25 @@ constexpr unsigned LBO32 = 256 * 16 + 16;    // R = 32 stages: 256 rows, K = 64
 constexpr unsigned A_SPLIT_BYTES = 4 * LBO16;          // = 8 * LBO32 = 32896
 static_assert (4 * LBO16 == 8 * LBO32, "both stage layouts fill one operand buffer");
 static_assert (A_SPLIT_BYTES % 128 == 0, "operand buffers stay 128-byte aligned");
-constexpr unsigned B16_LBO = 32 * 16, B16_BYTES = 4 * B16_LBO;   // 32 x 32
-constexpr unsigned B32_LBO = 64 * 16, B32_BYTES = 8 * B32_LBO;   // 64 x 64
-constexpr unsigned TMEM_COLS = 128;
+// The B operand of an R-point stage stacks the NS terms of the DFT block
+// along N: rows [s 2R, (s + 1) 2R) hold term s (N = NS 2R rows, K = 2R).  A
+// product of data term s with terms 0 .. NS-1-s is then one MMA of N = (NS -
+// s) 2R that reads its A operand once; it accumulates into column groups s ..
+// NS-1 of the tile's NS 2R accumulator columns, and group g ends up holding
+// the sum of all products x_s w_j with s + j = g.  The epilogue adds the
+// groups.
+constexpr unsigned B16_BYTES = 4 * 32 * 16, B32_BYTES = 8 * 64 * 16;   // per term
+template <int NS> __host__ __device__ constexpr unsigned b_lbo (int R) { return NS * 2 * R * 16; }
+template <int NS> __host__ __device__ constexpr unsigned tmem_cols () { return NS == 2 ? 256 : 512; }
 
+// two operand buffers (a stage reads one while its epilogue writes the
+// other), the DFT terms, four mbarriers (one per row tile) and the tensor-
+// memory address
 template <int NS>
 constexpr unsigned tc_smem_bytes ()
 {
-  return NS * (A_SPLIT_BYTES + B16_BYTES + B32_BYTES) + 16;
+  return NS * (2 * A_SPLIT_BYTES + B16_BYTES + B32_BYTES) + 64;
 }
-
-// products x_i w_j kept for NS terms (i + j < NS, in order of size)
-template <int NS>
-__host__ __device__ constexpr int npairs () { return NS == 2 ? 3 : 6; }
-__host__ __device__ constexpr int pair_a (int p) { return p == 2 ? 1 : p == 4 ? 2 : p == 5 ? 1 : 0; }
-__host__ __device__ constexpr int pair_b (int p) { return p == 1 ? 1 : p == 3 ? 2 : p == 5 ? 1 : 0; }
 
 __device__ __forceinline__ float2 cmulf (float2 a, float2 b)
 {
@@ -133,30 +139,50 @@ __device__ __forceinline__ void put_c4 (unsigned char* A, unsigned r, unsigned j
         make_uint4 (s[0][i], s[1][i], s[2][i], s[3][i]);
 }
 
-// One stage's MMAs, issued by one thread: R = 16 -> 4 row tiles x N = 32,
-// R = 32 -> 2 row tiles x N = 64; K = 2R in steps of 16.
+// One stage's MMAs, issued by one thread: R = 16 -> 4 row tiles, R = 32 -> 2
+// row tiles; K = 2R in steps of 16; per tile and step one MMA per data term
+// (N = (NS - s) 2R, see b_lbo).  Each tile's MMAs are committed to that
+// tile's mbarrier, so its epilogue can start while later tiles compute.
 template <int NS, int R>
-__device__ __forceinline__ void issue_stage (uint32_t tmem, uint32_t a_base, uint32_t b_base)
+__device__ __forceinline__ void issue_stage (uint32_t tmem, uint32_t a_base, uint32_t b_base,
+                                             uint64_t* bars)
 {
   constexpr unsigned NT = R == 16 ? 4 : 2;
-  constexpr unsigned N = 2 * R;
+  constexpr unsigned G = 2 * R;                 // one column group
   constexpr unsigned KS = 2 * R / 16;
   constexpr unsigned LBO = R == 16 ? LBO16 : LBO32;
-  constexpr unsigned BLBO = R == 16 ? B16_LBO : B32_LBO;
-  constexpr unsigned BBYTES = R == 16 ? B16_BYTES : B32_BYTES;
-  constexpr uint32_t ID = idesc_bf16 (128, N);
+  constexpr unsigned BLBO = b_lbo<NS> (R);
 #pragma unroll
   for (unsigned t = 0; t < NT; t++)
+  {
 #pragma unroll
     for (unsigned ks = 0; ks < KS; ks++)
 #pragma unroll
-      for (int p = 0; p < npairs<NS> (); p++)
+      for (int sp = 0; sp < NS; sp++)
       {
-        const uint32_t a = a_base + pair_a (p) * A_SPLIT_BYTES + t * 2048 + ks * 2 * LBO;
-        const uint32_t b = b_base + pair_b (p) * BBYTES + ks * 2 * BLBO;
-        mma_bf16 (tmem + t * N, sdesc (a, LBO, 128), sdesc (b, BLBO, 128), ID,
-                  (ks | p) ? 1u : 0u);
+        const uint32_t a = a_base + sp * A_SPLIT_BYTES + t * 2048 + ks * 2 * LBO;
+        const uint32_t b = b_base + ks * 2 * BLBO;
+        mma_bf16 (tmem + t * NS * G + sp * G, sdesc (a, LBO, 128), sdesc (b, BLBO, 128),
+                  idesc_bf16 (128, (NS - sp) * G), (ks | sp) ? 1u : 0u);
       }
+    mma_commit (bars + t);
+  }
+}
+
+// this thread's 32 accumulator columns of the stage: the NS column groups
+// (stride apart) added
+template <int NS>
+__device__ __forceinline__ void tmem_sum (uint32_t taddr, uint32_t stride, float* v)
+{
+  tmem_ld32 (taddr, v);
+#pragma unroll
+  for (int g = 1; g < NS; g++)
+  {
+    float u[32];
+    tmem_ld32 (taddr + g * stride, u);
+#pragma unroll
+    for (int i = 0; i < 32; i++) v[i] += u[i];
+  }
 }
 
 } // namespace
@@ -170,11 +196,11 @@ k_rows_mma (float2* __restrict__ scratch, const float2* __restrict__ tw,
             int* __restrict__ err)
 {
   extern __shared__ __align__ (1024) unsigned char sm[];
-  unsigned char* A = sm;                                   // NS operand splits
-  unsigned char* B16 = sm + NS * A_SPLIT_BYTES;            // NS splits of the DFT16 block
-  unsigned char* B32 = B16 + NS * B16_BYTES;               // NS splits of the DFT32 block
-  uint64_t* bar = reinterpret_cast<uint64_t*> (B32 + NS * B32_BYTES);
-  uint32_t* tslot = reinterpret_cast<uint32_t*> (bar + 1);
+  unsigned char* Abuf[2] = {sm, sm + NS * A_SPLIT_BYTES};   // NS operand terms each
+  unsigned char* B16 = sm + 2 * NS * A_SPLIT_BYTES;         // NS terms of the DFT16 block
+  unsigned char* B32 = B16 + NS * B16_BYTES;                // NS terms of the DFT32 block
+  uint64_t* bars = reinterpret_cast<uint64_t*> (B32 + NS * B32_BYTES);
+  uint32_t* tslot = reinterpret_cast<uint32_t*> (bars + 4);
   const unsigned tid = threadIdx.x, w = tid >> 5, l = tid & 31;
 
   // the DFT blocks (already in the operand layout) into shared memory
@@ -183,34 +209,41 @@ k_rows_mma (float2* __restrict__ scratch, const float2* __restrict__ tw,
     uint4* dst = reinterpret_cast<uint4*> (B16);
     for (unsigned i = tid; i < NV; i += TC_THREADS) dst[i] = __ldg (dft + i);
   }
-  if (tid == 0) bar_init (bar, 1);
-  if (w == 0) tmem_alloc (tslot, TMEM_COLS);
+  if (tid < 4) bar_init (bars + tid, 1);
+  if (w == 0) tmem_alloc (tslot, tmem_cols<NS> ());
   fence_async_smem ();
   fence_before ();
   __syncthreads ();
   fence_after ();
   const uint32_t tmem = *tslot;
-  const uint32_t a_base = saddr (A), b16 = saddr (B16), b32 = saddr (B32);
+  const uint32_t b16 = saddr (B16), b32 = saddr (B32);
   // this thread's accumulator lanes: warp w reads lanes 32 (w % 4) ... + 31
   const uint32_t tlane = tmem + ((32u * (w & 3)) << 16);
-  unsigned parity = 0;
-  bool failed = false;
+  unsigned phase = 0;          // bit t: the parity the next wait on bars[t] expects
+  bool lost = false;           // this thread's wait gave up
+  bool failed = false;         // some thread's did (block-uniform)
+  int last_bar = -1;           // thread 0: the barrier of the last commit, and its parity
+  unsigned last_parity = 0;
 
-  // one stage: operands are in place; issue, wait (bounded, block-uniform)
-  auto run_stage = [&] (auto rtag) -> bool {
+  // one stage on operand buffer `cur`: all operands are in place (barrier,
+  // with the block-uniform check of the last waits), thread 0 issues tile by
+  // tile, each thread waits (bounded) for its own tile only
+  auto run_stage = [&] (auto rtag, int cur) -> bool {
     constexpr int R = decltype (rtag)::value;
+    constexpr unsigned NT = R == 16 ? 4 : 2;
     fence_async_smem ();
     fence_before ();
-    __syncthreads ();
+    if (__syncthreads_or (lost)) return false;
     if (tid == 0)
     {
       fence_after ();
-      issue_stage<NS, R> (tmem, a_base, R == 16 ? b16 : b32);
-      mma_commit (bar);
+      issue_stage<NS, R> (tmem, saddr (Abuf[cur]), R == 16 ? b16 : b32, bars);
+      last_bar = int (NT - 1);
+      last_parity = (phase >> (NT - 1)) & 1;
     }
-    const bool ok = bar_wait (bar, parity);
-    parity ^= 1;
-    if (__syncthreads_or (!ok)) return false;
+    const unsigned t = R == 16 ? (w >> 2) : ((w >> 2) & 1);
+    lost = !bar_wait (bars + t, (phase >> t) & 1);
+    phase ^= (1u << NT) - 1;
     fence_after ();
     return true;
   };
@@ -225,30 +258,29 @@ k_rows_mma (float2* __restrict__ scratch, const float2* __restrict__ tw,
     const float2* h = H + (uint64_t (c) * n1 + k1) * TC_N;
     float v[32];
 
-    // F1 operand: row n_a = tid holds x[n_a + 512 n_b], n_b = 0..15
+    // F1 operand (buffer 0): row n_a = tid holds x[n_a + 512 n_b], n_b = 0..15
     {
       float2 z[16];
 #pragma unroll
       for (int nb = 0; nb < 16; nb++) z[nb] = g[tid + 512 * nb];
 #pragma unroll
-      for (int j = 0; j < 4; j++) put_c4<NS> (A, tid, j, LBO16, z + 4 * j);
+      for (int j = 0; j < 4; j++) put_c4<NS> (Abuf[0], tid, j, LBO16, z + 4 * j);
     }
-    if (!run_stage (R16 {})) { failed = true; break; }
+    if (!run_stage (R16 {}, 0)) { failed = true; break; }
     // F1 epilogue: Y1[n_a][k_b] x w8192^(n_a k_b) -> F2 rows 32 k_b + n_d, K = n_c
-    tmem_ld32 (tlane + (w >> 2) * 32, v);
+    tmem_sum<NS> (tlane + (w >> 2) * NS * 32, 32, v);
     {
       const unsigned na = tid, nd = l, nc = w;
 #pragma unroll
       for (int kb = 0; kb < 16; kb++)
       {
         const float2 y = cmulf (make_float2 (v[2 * kb], v[2 * kb + 1]), __ldg (tw + ((na * kb) & 8191)));
-        put_c<NS> (A, aoff (32 * kb + nd, nc, LBO16), y);
+        put_c<NS> (Abuf[1], aoff (32 * kb + nd, nc, LBO16), y);
       }
     }
-    fence_before ();
-    if (!run_stage (R16 {})) { failed = true; break; }
+    if (!run_stage (R16 {}, 1)) { failed = true; break; }
     // F2 epilogue: row (k_b = w, n_d = l), Y2[k_c] x w512^(n_d k_c) -> F3 rows k_b + 16 k_c, K = n_d
-    tmem_ld32 (tlane + (w >> 2) * 32, v);
+    tmem_sum<NS> (tlane + (w >> 2) * NS * 32, 32, v);
     {
       const unsigned kb = w, nd = l;
 #pragma unroll
@@ -256,16 +288,15 @@ k_rows_mma (float2* __restrict__ scratch, const float2* __restrict__ tw,
       {
         const float2 y = cmulf (make_float2 (v[2 * kc], v[2 * kc + 1]),
                                 __ldg (tw + ((16 * nd * kc) & 8191)));
-        put_c<NS> (A, aoff (kb + 16 * kc, nd, LBO32), y);
+        put_c<NS> (Abuf[0], aoff (kb + 16 * kc, nd, LBO32), y);
       }
     }
-    fence_before ();
-    if (!run_stage (R32 {})) { failed = true; break; }
+    if (!run_stage (R32 {}, 0)) { failed = true; break; }
     // F3 epilogue: row r3 = k_b + 16 k_c (tile m, quarter q), half hh of k_d:
     // X[r3 + 256 k_d] x H, conjugated -> I1 operand, own row, K = k_d
     const unsigned m = (w >> 2) & 1, hh = w >> 3;
     const unsigned r3 = 128 * m + 32 * (w & 3) + l;
-    tmem_ld32 (tlane + m * 64 + hh * 32, v);
+    tmem_sum<NS> (tlane + m * NS * 64 + hh * 32, 64, v);
     {
       float2 z[16];
 #pragma unroll
@@ -278,13 +309,12 @@ k_rows_mma (float2* __restrict__ scratch, const float2* __restrict__ tw,
         z[j] = make_float2 (x.x * f.x - x.y * f.y, -(x.x * f.y + x.y * f.x));
       }
 #pragma unroll
-      for (int j = 0; j < 4; j++) put_c4<NS> (A, r3, 4 * hh + j, LBO32, z + 4 * j);
+      for (int j = 0; j < 4; j++) put_c4<NS> (Abuf[1], r3, 4 * hh + j, LBO32, z + 4 * j);
     }
-    fence_before ();
-    if (!run_stage (R32 {})) { failed = true; break; }
+    if (!run_stage (R32 {}, 1)) { failed = true; break; }
     // I1 epilogue: row r3, U1[n_d] (n_d in this half) x w512^(n_d k_c)
     // -> I2 rows k_b + 16 n_d, K = k_c
-    tmem_ld32 (tlane + m * 64 + hh * 32, v);
+    tmem_sum<NS> (tlane + m * NS * 64 + hh * 32, 64, v);
     {
       const unsigned kb = r3 & 15, kc = r3 >> 4;
 #pragma unroll
@@ -293,14 +323,13 @@ k_rows_mma (float2* __restrict__ scratch, const float2* __restrict__ tw,
         const unsigned nd = 16 * hh + j;
         const float2 y = cmulf (make_float2 (v[2 * j], v[2 * j + 1]),
                                 __ldg (tw + ((16 * nd * kc) & 8191)));
-        put_c<NS> (A, aoff (kb + 16 * nd, kc, LBO16), y);
+        put_c<NS> (Abuf[0], aoff (kb + 16 * nd, kc, LBO16), y);
       }
     }
-    fence_before ();
-    if (!run_stage (R16 {})) { failed = true; break; }
+    if (!run_stage (R16 {}, 0)) { failed = true; break; }
     // I2 epilogue: row r5 = tid = k_b + 16 n_d, U2[n_c] x w8192^(n_a k_b),
     // n_a = n_d + 32 n_c -> I3 rows n_a, K = k_b
-    tmem_ld32 (tlane + (w >> 2) * 32, v);
+    tmem_sum<NS> (tlane + (w >> 2) * NS * 32, 32, v);
     {
       const unsigned kb = tid & 15, nd = tid >> 4;
 #pragma unroll
@@ -309,30 +338,28 @@ k_rows_mma (float2* __restrict__ scratch, const float2* __restrict__ tw,
         const unsigned na = nd + 32 * nc;
         const float2 y = cmulf (make_float2 (v[2 * nc], v[2 * nc + 1]),
                                 __ldg (tw + ((na * kb) & 8191)));
-        put_c<NS> (A, aoff (na, kb, LBO16), y);
+        put_c<NS> (Abuf[1], aoff (na, kb, LBO16), y);
       }
     }
-    fence_before ();
-    if (!run_stage (R16 {})) { failed = true; break; }
-    // I3 epilogue: row n_a = tid, y[n_a + 512 n_b] = conjugate
-    tmem_ld32 (tlane + (w >> 2) * 32, v);
+    if (!run_stage (R16 {}, 1)) { failed = true; break; }
+    // I3 epilogue: row n_a = tid, y[n_a + 512 n_b] = conjugate.  The next
+    // row's F1 operand goes to buffer 0, which no MMA reads any more: every
+    // thread passed its I2 wait before the I3 stage began.
+    tmem_sum<NS> (tlane + (w >> 2) * NS * 32, 32, v);
 #pragma unroll
     for (int nb = 0; nb < 16; nb++) g[tid + 512 * nb] = make_float2 (v[2 * nb], -v[2 * nb + 1]);
-    fence_before ();
-  }
-
-  if (failed)
-  {
-    if (tid == 0)
-    {
-      atomicExch (err, 1);
-      bar_wait (bar, parity ^ 1);   // let the MMAs in flight finish
-    }
   }
   fence_before ();
+  if (__syncthreads_or (lost)) failed = true;
+  if (failed && tid == 0)
+  {
+    atomicExch (err, 1);
+    // the last commit covers every MMA issued before it: let them finish
+    if (last_bar >= 0) bar_wait (bars + last_bar, last_parity);
+  }
   __syncthreads ();
   fence_after ();
-  if (w == 0) tmem_free (tmem, TMEM_COLS);
+  if (w == 0) tmem_free (tmem, tmem_cols<NS> ());
 }
 
 // ---------------------------------------------------------------------------
@@ -361,8 +388,9 @@ double bf16_value (uint16_t b)
 
 // Real block B[K][N] of the R-point DFT (W[n][k] = exp(-2 pi i n k / R)),
 // stored K-major (row N, column K) in the operand layout, split into ns terms.
-void put_dft_block (unsigned R, unsigned ns, unsigned lbo, unsigned bytes, uint8_t* out)
+void put_dft_block (unsigned R, unsigned ns, uint8_t* out)
 {
+  const unsigned lbo = ns * 2 * R * 16;
   const unsigned K = 2 * R;
   for (unsigned kn = 0; kn < K; kn++)      // B row index (input real index)
     for (unsigned nn = 0; nn < K; nn++)    // B column index (output real index)
@@ -378,9 +406,9 @@ void put_dft_block (unsigned R, unsigned ns, unsigned lbo, unsigned bytes, uint8
       {
         const uint16_t b = bf16_bits (rem);
         rem -= bf16_value (b);
-        // element (row nn, column kn) of the K-major N x K matrix
-        const unsigned off = (kn / 8) * lbo + nn * 16 + (kn % 8) * 2;
-        std::memcpy (out + s * bytes + off, &b, 2);
+        // element (row s 2R + nn, column kn) of the K-major (ns 2R) x K matrix
+        const unsigned off = (kn / 8) * lbo + (s * 2 * R + nn) * 16 + (kn % 8) * 2;
+        std::memcpy (out + off, &b, 2);
       }
     }
 }
@@ -390,8 +418,8 @@ void put_dft_block (unsigned R, unsigned ns, unsigned lbo, unsigned bytes, uint8
 void make_tc_dft_image (unsigned ns, std::vector<uint8_t>& img)
 {
   img.assign (ns * (B16_BYTES + B32_BYTES), 0);
-  put_dft_block (16, ns, B16_LBO, B16_BYTES, img.data ());
-  put_dft_block (32, ns, B32_LBO, B32_BYTES, img.data () + ns * B16_BYTES);
+  put_dft_block (16, ns, img.data ());
+  put_dft_block (32, ns, img.data () + ns * B16_BYTES);
 }
 
 template <int NS>

@@ -197,11 +197,14 @@ def test_fold_accumulate(ctx, b2, orc):
 
 # ---------------------------------------------------------------- convolution
 
-@pytest.mark.parametrize("nfft", [4096, 8192, 16384, 1 << 16, 1 << 17, 1 << 18])
-def test_convolution_tukey_known_answer(ctx, b2, orc, nfft):
+@pytest.mark.parametrize("nfft,fft", [(4096, 0), (8192, 0), (16384, 0), (1 << 16, 0),
+                                      (1 << 17, 0), (1 << 18, 0), (16384, 3), (1 << 16, 3),
+                                      (1 << 17, 3), (1 << 18, 3)])
+def test_convolution_tukey_known_answer(ctx, b2, orc, nfft, fft):
     """ConvolutionTest.test_operate_tukey (ConvolutionTest.cpp:148-308) on the
     GPU engine, at the reference's FFT length and at the lengths the BASELINE
-    configurations use."""
+    configurations use; fft = 3: the rows on the tensor cores (three BF16
+    terms), held to the same thresholds."""
     from test_oracle import _tukey_case
 
     def gpu_convolve(x, r, n, pos, neg):
@@ -213,6 +216,8 @@ def test_convolution_tukey_known_answer(ctx, b2, orc, nfft):
         nchan, npol, ndat = x.shape
         c = b2.Convolution(ctx, nchan, npol, nfft, pos, neg)
         c.copy_response(r)
+        if fft:
+            c.set_fft_precision(fft)
         npart = c.npart(ndat)
         out = torch.zeros((nchan, npol, npart * c.nkeep), dtype=torch.complex64, device="cuda")
         c.perform(dev(x), ndat, ndat, out, npart * c.nkeep)

@@ -126,9 +126,10 @@ def test_proposer_inference_matches_torch(ctx, b2, rfi_case):
     z = torch_forward(p, X, emulate_bf16=True).numpy()
     ref = 1 / (1 + np.exp(-z))
     assert np.max(np.abs(got - ref)) < 2e-4, float(np.max(np.abs(got - ref)))
-    # and against the plain FP32 network: BF16 operands move it only a little
+    # and against the plain FP32 network: BF16 operands (8 significant bits)
+    # move logits near 0 by up to a few tenths
     z32 = torch_forward(p, X, emulate_bf16=False).numpy()
-    assert np.max(np.abs(got - 1 / (1 + np.exp(-z32)))) < 0.05
+    assert np.max(np.abs(got - 1 / (1 + np.exp(-z32)))) < 0.1
     assert np.array_equal(out.cpu().numpy(), (got >= 0.5).astype(np.uint8))
     pr.close()
 

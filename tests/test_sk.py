@@ -217,7 +217,7 @@ def test_sk_engine_steps_match_oracle(ctx, b2, orc, nchan, npol, M, ndat, zero_i
     x[0, :, :M] *= 8.0                                   # an outlying block
     x[nchan - 1, :, 2 * M:3 * M] = 0.0                   # a silent block
     if nchan > 2:
-        x[1] += 0.8 * np.exp(2j * np.pi * 0.1 * np.arange(span))   # a tone all along channel 1
+        x[1] += 2.0 * np.exp(2j * np.pi * 0.1 * np.arange(span))   # a tone all along channel 1
     lo, hi = b2.sk_limits(M, 1, 3.0, npol)
     rs, rc, rm, rout = orc.sk(x, M, lo, hi, zero_is_valid=zero_is_valid, ndat=ndat)
     npart = ndat // M

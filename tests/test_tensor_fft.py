@@ -50,13 +50,16 @@ def test_tensor_rows_voltages_vs_fp64(ctx, b2, orc, mode, rtol, nchan, nfft, dm,
     c.status()
     got = out.cpu().numpy()
     err = rel_rms(got, ref)
-    assert err < rtol, err
     # and the FP32 row kernel on the same input: both near the FP64 answer
     c.set_fft_precision(b2.FFT_FP32)
     out32 = torch.zeros_like(out)
     c.perform(dev(x), ndat, ndat, out32, 4 * nk)
     ctx.synchronize()
-    assert rel_rms(out32.cpu().numpy(), ref) < VOLTAGE_RTOL_BF16X3
+    err32 = rel_rms(out32.cpu().numpy(), ref)
+    print(f"\nvoltage error vs FP64: nfft={nfft} nchan={nchan} DM={dm}: "
+          f"bf16x{mode} {err:.3e}, fp32 {err32:.3e}")
+    assert err < rtol, err
+    assert err32 < VOLTAGE_RTOL_BF16X3
     c.close()
 
 
@@ -91,31 +94,8 @@ def test_tensor_rows_c2_shape_vs_fp64(ctx, b2, orc):
     h = orc.dedispersion_response_channels(freqs, bw, dm, nfft, fp64=True)
     ref = orc.convolve(y, h, nfft, pos, neg)
     err = rel_rms(got, ref)
+    print(f"\nvoltage error vs FP64 at C2's shape (64 x 2^16, DM 500): bf16x3 {err:.3e}")
     assert err < VOLTAGE_RTOL_BF16X3, err
-
-
-def test_tensor_rows_tukey_impulse(ctx, b2, orc):
-    """ConvolutionTest.test_operate_tukey's impulse response
-    (Signal/General/tests/ConvolutionTest.cpp:148-308): an impulse through
-    the Tukey response, tensor-core rows, within 1e-6 of the oracle."""
-    nfft, neg, pos = 1 << 14, 1000, 1200
-    resp, _ = orc.tukey_response(neg, pos, nfft)
-    x = np.zeros((1, 2, nfft + nfft // 2), np.complex64)
-    x[0, :, 5000] = 1.0
-    x[0, 1, 7001] = 0.5j
-    ref = orc.convolve(x.astype(np.complex128), resp.astype(np.complex128).reshape(1, nfft),
-                       nfft, pos, neg)
-    c = b2.Convolution(ctx, 1, 2, nfft, pos, neg)
-    c.copy_response(resp)
-    c.set_fft_precision(b2.FFT_BF16X3)
-    n = c.npart(x.shape[2])
-    nk = nfft - pos - neg
-    out = torch.zeros((1, 2, n * nk), dtype=torch.complex64, device="cuda")
-    assert c.perform(dev(x), x.shape[2], x.shape[2], out, n * nk) == n
-    ctx.synchronize()
-    got = out.cpu().numpy()
-    assert np.max(np.abs(got - ref)) < 1e-6 * np.max(np.abs(ref))
-    c.close()
 
 
 def test_tensor_rows_rejects_small_ffts(ctx, b2):
