@@ -1449,12 +1449,16 @@ def run_b200_c3(args, cfg, world, rank, local):
                 for w in range(2):
                     pl.run(s["blocks"][w % nblk], s["ndat"])
                 st = s["tstream"]
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(st)
-                pl.run(s["blocks"][0], s["ndat"])
-                e1.record(st)
-                e1.synchronize()
-                ms = e0.elapsed_time(e1)
+                times = []
+                for rep in range(3):
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(st)
+                    pl.run(s["blocks"][rep % nblk], s["ndat"])
+                    e1.record(st)
+                    e1.synchronize()
+                    times.append(e0.elapsed_time(e1))
+                ms = statistics.median(times)
                 pl.close()
                 if best is None or ms < best[0]:
                     best = (ms, plan)
@@ -1854,8 +1858,13 @@ def run_b200_c5(args, cfg, world, rank, local):
                      "note": "algorithmic bytes: the int16 input once; FFT-bound chain"},
         "e2e": None,
         "check": {"hits_total": int(hits.sum()),
-                  "profile_peak_over_median": float(np.max(prof[:, 0].sum(0))
-                                                    / max(np.median(prof[:, 0].sum(0)), 1e-30))},
+                  # a 1.6 ms turn is 1250 samples of the re-channelised data,
+                  # so most of the 4096 bins get no hits: judge the hit ones
+                  "bins_hit": int((hits > 0).sum()),
+                  "profile_peak_over_median_of_hit_bins": float(
+                      np.max((prof[:, 0].sum(0) / np.maximum(hits, 1))[hits > 0])
+                      / max(np.median((prof[:, 0].sum(0) / np.maximum(hits, 1))[hits > 0]),
+                            1e-30))},
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

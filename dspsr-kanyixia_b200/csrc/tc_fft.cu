@@ -34,7 +34,8 @@
 // mbarrier the block waits on, bounded).  Each thread then reads its row of
 // the accumulator (tcgen05.ld 32x32b), applies the twiddles in FP32, splits
 // again and writes the next stage's operand rows in shared memory.  Twiddles
-// and the response are FP32; the DFT blocks are split from FP64 values.
+// (two FP64-rounded tables in shared memory, w^e = T_hi[e/64] T_lo[e%64]) and
+// the response are FP32; the DFT blocks are split from FP64 values.
 //
 // Operand layout in shared memory: K-major without swizzle; element (r, k) of
 // a rows x K BF16 matrix at (k/8)*LBO + r*16 + (k%8)*2 (8-row core matrices
@@ -77,13 +78,17 @@ constexpr unsigned B16_BYTES = 4 * 32 * 16, B32_BYTES = 8 * 64 * 16;   // per te
 template <int NS> __host__ __device__ constexpr unsigned b_lbo (int R) { return NS * 2 * R * 16; }
 template <int NS> __host__ __device__ constexpr unsigned tmem_cols () { return NS == 2 ? 256 : 512; }
 
+// twiddles w8192^e = T_hi[e >> 6] T_lo[e & 63] from two small tables
+constexpr unsigned TW_HI = 128, TW_LO = 64;
+constexpr unsigned TW_BYTES = (TW_HI + TW_LO) * 8;
+
 // two operand buffers (a stage reads one while its epilogue writes the
 // other), the DFT terms, four mbarriers (one per row tile) and the tensor-
 // memory address
 template <int NS>
 constexpr unsigned tc_smem_bytes ()
 {
-  return NS * (2 * A_SPLIT_BYTES + B16_BYTES + B32_BYTES) + 64;
+  return NS * (2 * A_SPLIT_BYTES + B16_BYTES + B32_BYTES) + 64 + TW_BYTES;
 }
 
 __device__ __forceinline__ float2 cmulf (float2 a, float2 b)
@@ -201,14 +206,24 @@ k_rows_mma (float2* __restrict__ scratch, const float2* __restrict__ tw,
   unsigned char* B32 = B16 + NS * B16_BYTES;                // NS terms of the DFT32 block
   uint64_t* bars = reinterpret_cast<uint64_t*> (B32 + NS * B32_BYTES);
   uint32_t* tslot = reinterpret_cast<uint32_t*> (bars + 4);
+  float2* tw_hi = reinterpret_cast<float2*> (reinterpret_cast<unsigned char*> (bars) + 64);
+  float2* tw_lo = tw_hi + TW_HI;
   const unsigned tid = threadIdx.x, w = tid >> 5, l = tid & 31;
 
-  // the DFT blocks (already in the operand layout) into shared memory
+  // the DFT blocks (already in the operand layout) and the twiddle tables
+  // into shared memory
   {
     constexpr unsigned NV = NS * (B16_BYTES + B32_BYTES) / 16;
     uint4* dst = reinterpret_cast<uint4*> (B16);
     for (unsigned i = tid; i < NV; i += TC_THREADS) dst[i] = __ldg (dft + i);
+    if (tid < TW_HI) tw_hi[tid] = __ldg (tw + 64 * tid);
+    else if (tid < TW_HI + TW_LO) tw_lo[tid - TW_HI] = __ldg (tw + (tid - TW_HI));
   }
+  // y w8192^e
+  auto twiddle = [&] (float2 y, unsigned e) {
+    e &= 8191;
+    return cmulf (cmulf (y, tw_hi[e >> 6]), tw_lo[e & 63]);
+  };
   if (tid < 4) bar_init (bars + tid, 1);
   if (w == 0) tmem_alloc (tslot, tmem_cols<NS> ());
   fence_async_smem ();
@@ -274,7 +289,7 @@ k_rows_mma (float2* __restrict__ scratch, const float2* __restrict__ tw,
 #pragma unroll
       for (int kb = 0; kb < 16; kb++)
       {
-        const float2 y = cmulf (make_float2 (v[2 * kb], v[2 * kb + 1]), __ldg (tw + ((na * kb) & 8191)));
+        const float2 y = twiddle (make_float2 (v[2 * kb], v[2 * kb + 1]), na * kb);
         put_c<NS> (Abuf[1], aoff (32 * kb + nd, nc, LBO16), y);
       }
     }
@@ -286,8 +301,7 @@ k_rows_mma (float2* __restrict__ scratch, const float2* __restrict__ tw,
 #pragma unroll
       for (int kc = 0; kc < 16; kc++)
       {
-        const float2 y = cmulf (make_float2 (v[2 * kc], v[2 * kc + 1]),
-                                __ldg (tw + ((16 * nd * kc) & 8191)));
+        const float2 y = twiddle (make_float2 (v[2 * kc], v[2 * kc + 1]), 16 * nd * kc);
         put_c<NS> (Abuf[0], aoff (kb + 16 * kc, nd, LBO32), y);
       }
     }
@@ -321,8 +335,7 @@ k_rows_mma (float2* __restrict__ scratch, const float2* __restrict__ tw,
       for (int j = 0; j < 16; j++)
       {
         const unsigned nd = 16 * hh + j;
-        const float2 y = cmulf (make_float2 (v[2 * j], v[2 * j + 1]),
-                                __ldg (tw + ((16 * nd * kc) & 8191)));
+        const float2 y = twiddle (make_float2 (v[2 * j], v[2 * j + 1]), 16 * nd * kc);
         put_c<NS> (Abuf[0], aoff (kb + 16 * nd, kc, LBO16), y);
       }
     }
@@ -336,8 +349,7 @@ k_rows_mma (float2* __restrict__ scratch, const float2* __restrict__ tw,
       for (int nc = 0; nc < 16; nc++)
       {
         const unsigned na = nd + 32 * nc;
-        const float2 y = cmulf (make_float2 (v[2 * nc], v[2 * nc + 1]),
-                                __ldg (tw + ((na * kb) & 8191)));
+        const float2 y = twiddle (make_float2 (v[2 * nc], v[2 * nc + 1]), na * kb);
         put_c<NS> (Abuf[1], aoff (na, kb, LBO16), y);
       }
     }
