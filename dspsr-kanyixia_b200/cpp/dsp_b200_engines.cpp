@@ -256,7 +256,7 @@ uint64_t SpectralKurtosisEngine::compute (const TimeSeriesView& in, SKSums& sums
     throw Error (DSPSR_B200_ESTATE, "SpectralKurtosisEngine::compute: complex data required");
   uint64_t npart = 0;
   ctx.check (dspsr_b200_sk_compute (ctx.handle (), in.base, in.span_floats / 2, in.ndat, in.nchan,
-                                    in.npol, M, zero_is_valid ? 1 : 0, sums.sums, sums.counts,
+                                    in.npol, M, 1, zero_is_valid ? 1 : 0, sums.sums, sums.counts,
                                     &npart),
              "SpectralKurtosisEngine::compute");
   sums.npart = npart;

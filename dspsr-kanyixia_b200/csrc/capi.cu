@@ -2111,13 +2111,31 @@ int dspsr_b200_sk (dspsr_b200_context* ctx, const float* d_in, uint64_t in_span,
 
 int dspsr_b200_sk_compute (dspsr_b200_context* ctx, const float* d_in, uint64_t in_span,
                            uint64_t ndat, unsigned nchan, unsigned npol, unsigned M,
-                           int zero_is_valid, float* d_sums, uint32_t* d_counts,
-                           uint64_t* npart_out)
+                           unsigned noverlap, int zero_is_valid, float* d_sums,
+                           uint32_t* d_counts, uint64_t* npart_out)
 {
   if (!ctx) return DSPSR_B200_EINVAL;
   if (npart_out) *npart_out = 0;
   if (!d_in || !d_sums || nchan == 0 || nchan > 65535 || (npol != 1 && npol != 2))
     return fail (ctx, DSPSR_B200_EINVAL, "sk_compute: invalid argument");
+  if (noverlap == 0 || M < 2 || M % noverlap)
+    return fail (ctx, DSPSR_B200_EINVAL, "sk_compute: noverlap=%u does not divide M=%u",
+                 noverlap, M);
+  if (noverlap > 1)
+  {
+    // Resolution::prepare (SpectralKurtosis.C:251-281): blocks of M every
+    // M / noverlap samples, the first idat_start = M - M / noverlap
+    // samples of the input only completing the first block
+    const uint64_t stride = M / noverlap, idat_start = M - stride;
+    const uint64_t npart = ndat >= idat_start ? (ndat - idat_start) / stride : 0;
+    if (in_span < ndat)
+      return fail (ctx, DSPSR_B200_EINVAL, "sk_compute: span smaller than ndat");
+    B200_CHECK (ctx, launch_sk_sums_strided (reinterpret_cast<const float2*> (d_in), in_span,
+                                             npart, stride, nchan, npol, M, zero_is_valid,
+                                             d_sums, d_counts, ctx->stream), "sk compute");
+    if (npart_out) *npart_out = npart;
+    return DSPSR_B200_OK;
+  }
   if (M < 2 || (M & 1) || (in_span & 1) || (reinterpret_cast<uintptr_t> (d_in) & 15))
     return fail (ctx, DSPSR_B200_EINVAL, "sk_compute: M and the span must be even, the input "
                  "16-byte aligned");
@@ -2210,6 +2228,100 @@ int dspsr_b200_sk_detect_tscr (dspsr_b200_context* ctx, const float* d_sums,
     }
   }
   if (nzapped_chan) *nzapped_chan = nz;
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_sk_tscrunch (dspsr_b200_context* ctx, const float* d_sums,
+                            const uint32_t* d_counts, uint64_t npart_from, uint64_t npart_to,
+                            unsigned nchan, unsigned npol, unsigned nsum, unsigned offset,
+                            float* d_sums_out, uint32_t* d_counts_out)
+{
+  if (!ctx) return DSPSR_B200_EINVAL;
+  if (!d_sums || !d_counts || !d_sums_out || !d_counts_out || nchan == 0 || nsum == 0
+      || offset == 0 || (npol != 1 && npol != 2))
+    return fail (ctx, DSPSR_B200_EINVAL, "sk_tscrunch: invalid argument");
+  if (npart_to && (npart_to - 1) * offset + uint64_t (nsum - 1) * offset >= npart_from)
+    return fail (ctx, DSPSR_B200_EINVAL, "sk_tscrunch: the coarse parts reach past the fine ones");
+  B200_CHECK (ctx, launch_sk_tscrunch (d_sums, d_counts, npart_to, nchan, npol, nsum, offset,
+                                       d_sums_out, d_counts_out, ctx->stream), "sk tscrunch");
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_sk_detect_skfb (dspsr_b200_context* ctx, const float* d_sums,
+                               const uint32_t* d_counts, uint64_t npart, unsigned nchan,
+                               unsigned npol, unsigned Nd, float std_devs, unsigned nflag,
+                               unsigned flag_step, unsigned flag_offset, uint8_t* d_mask,
+                               uint64_t mask_npart, uint64_t* d_zapped)
+{
+  if (!ctx) return DSPSR_B200_EINVAL;
+  if (!d_sums || !d_counts || !d_mask || nchan == 0 || Nd == 0 || nflag == 0
+      || flag_step == 0 || (npol != 1 && npol != 2))
+    return fail (ctx, DSPSR_B200_EINVAL, "sk_detect_skfb: invalid argument");
+  if (npart == 0) return DSPSR_B200_OK;
+  if ((npart - 1) * flag_offset + uint64_t (nflag - 1) * flag_step >= mask_npart)
+    return fail (ctx, DSPSR_B200_EINVAL, "sk_detect_skfb: flags reach past the mask");
+  // get_limits (SpectralKurtosis.C:988-1008) for every count present
+  std::vector<uint32_t> counts (npart * nchan);
+  B200_CHECK (ctx, cudaMemcpyAsync (counts.data (), d_counts, counts.size () * sizeof (uint32_t),
+                                    cudaMemcpyDeviceToHost, ctx->stream), "sk counts");
+  B200_CHECK (ctx, cudaStreamSynchronize (ctx->stream), "sk counts");
+  std::vector<uint32_t> uniq (counts);
+  std::sort (uniq.begin (), uniq.end ());
+  uniq.erase (std::unique (uniq.begin (), uniq.end ()), uniq.end ());
+  std::vector<uint32_t> lc;
+  std::vector<float2> lim;
+  for (uint32_t m : uniq)
+  {
+    if (m <= 2) continue;
+    float lo = 0.f, hi = 0.f;
+    if (sk_limits (m, Nd, std_devs, npol, &lo, &hi) != 0)
+      return fail (ctx, DSPSR_B200_ESTATE, "sk_detect_skfb: no limits for count %u", m);
+    lc.push_back (m);
+    lim.push_back (make_float2 (lo, hi));
+  }
+  if (lc.empty ())
+  {
+    lc.push_back (0);
+    lim.push_back (make_float2 (0.f, 0.f));
+  }
+  DevBuf<uint32_t> d_lc;
+  DevBuf<float2> d_lim;
+  B200_CHECK (ctx, d_lc.reserve (lc.size ()), "cudaMalloc sk limits");
+  B200_CHECK (ctx, d_lim.reserve (lim.size ()), "cudaMalloc sk limits");
+  B200_CHECK (ctx, cudaMemcpy (d_lc.ptr, lc.data (), lc.size () * 4, cudaMemcpyHostToDevice),
+              "sk limits");
+  B200_CHECK (ctx, cudaMemcpy (d_lim.ptr, lim.data (), lim.size () * 8, cudaMemcpyHostToDevice),
+              "sk limits");
+  const cudaError_t e = launch_sk_detect_skfb (
+      d_sums, d_counts, npart, nchan, npol, Nd, d_lc.ptr, d_lim.ptr, unsigned (lc.size ()), nflag,
+      flag_step, flag_offset, d_mask, reinterpret_cast<unsigned long long*> (d_zapped),
+      ctx->stream);
+  const cudaError_t e2 = cudaStreamSynchronize (ctx->stream);
+  d_lc.release ();
+  d_lim.release ();
+  if (e != cudaSuccess) return cuda_fail (ctx, e, "sk detect_skfb");
+  if (e2 != cudaSuccess) return cuda_fail (ctx, e2, "sk detect_skfb");
+  return DSPSR_B200_OK;
+}
+
+int dspsr_b200_sk_mask_overlap (dspsr_b200_context* ctx, const uint8_t* d_mask,
+                                const float* d_in, uint64_t in_span, float* d_out,
+                                uint64_t out_span, unsigned nchan, unsigned npol, unsigned M,
+                                unsigned offset, uint64_t npart, uint64_t nskip,
+                                uint64_t idat_start)
+{
+  if (!ctx) return DSPSR_B200_EINVAL;
+  if (!d_mask || !d_in || !d_out || d_in == d_out || nchan == 0 || offset == 0 || M == 0
+      || (npol != 1 && npol != 2))
+    return fail (ctx, DSPSR_B200_EINVAL, "sk_mask_overlap: invalid argument");
+  if (npart == 0) return DSPSR_B200_OK;
+  const uint64_t nout = (npart - 1) * offset + M;
+  if (out_span < nout || in_span < idat_start + nout)
+    return fail (ctx, DSPSR_B200_EINVAL, "sk_mask_overlap: spans smaller than the blocks");
+  B200_CHECK (ctx, launch_sk_mask_overlap (d_mask, reinterpret_cast<const float2*> (d_in), in_span,
+                                           reinterpret_cast<float2*> (d_out), out_span, nout,
+                                           nchan, npol, offset, npart, nskip, idat_start,
+                                           ctx->stream), "sk mask overlap");
   return DSPSR_B200_OK;
 }
 

@@ -2029,6 +2029,141 @@ __global__ void k_sk_detect (const float* __restrict__ sums, const unsigned* __r
   }
 }
 
+// SpectralKurtosis::compute (SpectralKurtosis.C:674-798) for blocks of M
+// samples every `stride` samples (Resolution::prepare with noverlap =
+// M / stride, :251-281): one thread per (block, chan, pol, S1 or S2) adds the
+// block's values in order in double, as the reference does; S2 adds the
+// float square of each sqld.  counts (pol 0's S1 thread) as the reference's
+// sum weights.  Blocks overlap, so each sample is read noverlap times; the
+// non-overlapping case has its own faster kernel (k_sk).
+__global__ void k_sk_sums_strided (const float2* __restrict__ in, const uint64_t span,
+                                   const uint64_t nblk, const uint64_t stride,
+                                   const unsigned nchan, const unsigned npol, const unsigned M,
+                                   const int zero_is_valid, float* __restrict__ sums,
+                                   unsigned* __restrict__ counts)
+{
+  const uint64_t idx = uint64_t (blockIdx.x) * blockDim.x + threadIdx.x;
+  const uint64_t total = nblk * nchan * npol * 2;
+  if (idx >= total) return;
+  const unsigned sq = unsigned (idx & 1);
+  const unsigned p = unsigned ((idx >> 1) % npol);
+  const uint64_t bc = (idx >> 1) / npol;
+  const unsigned c = unsigned (bc % nchan);
+  const uint64_t b = bc / nchan;
+  const float2* x = in + (uint64_t (c) * npol + p) * span + b * stride;
+  double acc = 0.0;
+  unsigned n = 0;
+  for (unsigned i = 0; i < M; i++)
+  {
+    const float2 v = x[i];
+    const float d = __fadd_rn (__fmul_rn (v.x, v.x), __fmul_rn (v.y, v.y));
+    if (zero_is_valid || d != 0.0f)
+    {
+      acc = __dadd_rn (acc, double (sq ? __fmul_rn (d, d) : d));
+      n++;
+    }
+  }
+  const uint64_t unit = b * nchan + c;
+  sums[2 * (unit * npol + p) + sq] = __double2float_rn (acc);
+  if (counts && p == 0 && sq == 0) counts[unit] = n;
+}
+
+// SpectralKurtosis::tscrunch_sums (SpectralKurtosis.C:917-986): coarse part q
+// takes the fine parts q*offset + isum*offset, isum < nsum, adding the float
+// sums and the counts in that order (the reference's indexing, kept as it is)
+__global__ void k_sk_tscrunch (const float* __restrict__ sums, const unsigned* __restrict__ counts,
+                               const uint64_t npart, const unsigned nchan, const unsigned npol,
+                               const unsigned nsum, const unsigned offset,
+                               float* __restrict__ osums, unsigned* __restrict__ ocounts)
+{
+  const uint64_t idx = uint64_t (blockIdx.x) * blockDim.x + threadIdx.x;
+  const uint64_t per = uint64_t (nchan) * npol * 2;
+  if (idx >= npart * per) return;
+  const uint64_t q = idx / per, e = idx % per;
+  float acc = sums[(q * offset) * per + e];
+  for (unsigned isum = 1; isum < nsum; isum++)
+    acc = __fadd_rn (acc, sums[(q * offset + uint64_t (isum) * offset) * per + e]);
+  osums[idx] = acc;
+  // the counts: one per (part, chan), from the threads of pol 0's S1
+  if (e % (npol * 2) == 0)
+  {
+    const unsigned c = unsigned (e / (npol * 2));
+    unsigned n = counts ? counts[(q * offset) * nchan + c] : 0;
+    for (unsigned isum = 1; isum < nsum && counts; isum++)
+      n += counts[(q * offset + uint64_t (isum) * offset) * nchan + c];
+    if (ocounts) ocounts[q * nchan + c] = n;
+  }
+}
+
+// SpectralKurtosis::detect_skfb (SpectralKurtosis.C:1105-1222) at one
+// resolution: thresholds from a table of (count, lower, upper) sorted by
+// count (get_limits of each count present); a zapped coarse cell flags nflag
+// fine cells, flag_step fine parts apart, starting at q * flag_offset.
+__global__ void k_sk_detect_skfb (const float* __restrict__ sums, const unsigned* __restrict__ counts,
+                                  const uint64_t npart, const unsigned nchan, const unsigned npol,
+                                  const unsigned Nd, const unsigned* __restrict__ lim_count,
+                                  const float2* __restrict__ lim, const unsigned nlim,
+                                  const unsigned nflag, const unsigned flag_step,
+                                  const unsigned flag_offset, uint8_t* __restrict__ mask,
+                                  unsigned long long* __restrict__ nzap)
+{
+  const uint64_t unit = uint64_t (blockIdx.x) * blockDim.x + threadIdx.x;
+  if (unit >= npart * nchan) return;
+  const unsigned Mprime = counts[unit];
+  if (Mprime == 0) return;
+  bool zap = true;
+  if (Mprime > 2)
+  {
+    unsigned lo = 0, hi = nlim;
+    while (lo + 1 < hi)
+    {
+      const unsigned mid = (lo + hi) / 2;
+      if (lim_count[mid] <= Mprime) lo = mid; else hi = mid;
+    }
+    const float2 L = lim[lo];       // (lower, upper); the table holds every count present
+    const float M_fac = __fdiv_rn (float (Mprime * Nd + 1), float (Mprime - 1));
+    zap = false;
+    for (unsigned p = 0; p < npol; p++)
+    {
+      const float S1 = sums[2 * (unit * npol + p)];
+      const float S2 = sums[2 * (unit * npol + p) + 1];
+      const float r = __fdiv_rn (S2, __fmul_rn (S1, S1));
+      const float V = __fmul_rn (M_fac, __fsub_rn (__fmul_rn (float (Mprime), r), 1.0f));
+      if (V > L.y || V < L.x) zap = true;
+    }
+  }
+  if (!zap) return;
+  if (nzap) atomicAdd (nzap, 1ull);
+  const uint64_t q = unit / nchan;
+  const unsigned c = unsigned (unit % nchan);
+  for (unsigned f = 0; f < nflag; f++)
+    mask[(q * flag_offset + uint64_t (f) * flag_step) * nchan + c] = 1;
+}
+
+// SpectralKurtosis::mask with overlapping blocks (SpectralKurtosis.C:1465-
+// 1566): the reference copies (or zeroes) part after part, M samples each,
+// parts `offset` apart, so a sample keeps the decision of the last part that
+// covers it: part min(t / offset, npart - 1), mask row part + nskip; the
+// input is read from idat_start on.
+__global__ void k_sk_mask_overlap (const uint8_t* __restrict__ mask, const float2* __restrict__ in,
+                                   const uint64_t in_span, float2* __restrict__ out,
+                                   const uint64_t out_span, const uint64_t ndat_out,
+                                   const unsigned nchan, const unsigned npol,
+                                   const unsigned offset, const uint64_t npart,
+                                   const uint64_t nskip, const uint64_t idat_start)
+{
+  const uint64_t t = uint64_t (blockIdx.x) * blockDim.x + threadIdx.x;
+  const unsigned c = blockIdx.y;
+  if (t >= ndat_out) return;
+  const uint64_t part = min (t / offset, npart - 1);
+  const bool zap = __ldg (mask + (part + nskip) * nchan + c) != 0;
+  for (unsigned p = 0; p < npol; p++)
+  {
+    const uint64_t r = uint64_t (c) * npol + p;
+    out[r * out_span + t] = zap ? make_float2 (0.f, 0.f) : in[r * in_span + idat_start + t];
+  }
+}
+
 // SpectralKurtosis::mask (SpectralKurtosis.C:1465-1566): out = in, with the
 // blocks whose mask is set zeroed (in place when out == in: only those are
 // written).
@@ -2916,6 +3051,59 @@ cudaError_t launch_delay_fold (const float2* v, uint64_t span, const int* applie
     k_delay_fold<2><<<grid, 256, 0, st>>> (v, span, applied, ndat, npol, fv);
   else
     k_delay_fold<4><<<grid, 256, 0, st>>> (v, span, applied, ndat, npol, fv);
+  return cudaGetLastError ();
+}
+
+cudaError_t launch_sk_sums_strided (const float2* in, uint64_t span, uint64_t nblk,
+                                   uint64_t stride, unsigned nchan, unsigned npol, unsigned M,
+                                   int zero_is_valid, float* sums, unsigned* counts,
+                                   cudaStream_t st)
+{
+  const uint64_t total = nblk * nchan * npol * 2;
+  if (total == 0) return cudaSuccess;
+  g_launches++;
+  k_sk_sums_strided<<<unsigned ((total + 127) / 128), 128, 0, st>>> (
+      in, span, nblk, stride, nchan, npol, M, zero_is_valid, sums, counts);
+  return cudaGetLastError ();
+}
+
+cudaError_t launch_sk_tscrunch (const float* sums, const unsigned* counts, uint64_t npart,
+                                unsigned nchan, unsigned npol, unsigned nsum, unsigned offset,
+                                float* osums, unsigned* ocounts, cudaStream_t st)
+{
+  const uint64_t total = npart * nchan * npol * 2;
+  if (total == 0) return cudaSuccess;
+  g_launches++;
+  k_sk_tscrunch<<<unsigned ((total + 255) / 256), 256, 0, st>>> (sums, counts, npart, nchan, npol,
+                                                                 nsum, offset, osums, ocounts);
+  return cudaGetLastError ();
+}
+
+cudaError_t launch_sk_detect_skfb (const float* sums, const unsigned* counts, uint64_t npart,
+                                   unsigned nchan, unsigned npol, unsigned Nd,
+                                   const unsigned* lim_count, const float2* lim, unsigned nlim,
+                                   unsigned nflag, unsigned flag_step, unsigned flag_offset,
+                                   uint8_t* mask, unsigned long long* nzap, cudaStream_t st)
+{
+  const uint64_t total = npart * nchan;
+  if (total == 0) return cudaSuccess;
+  g_launches++;
+  k_sk_detect_skfb<<<unsigned ((total + 255) / 256), 256, 0, st>>> (
+      sums, counts, npart, nchan, npol, Nd, lim_count, lim, nlim, nflag, flag_step, flag_offset,
+      mask, nzap);
+  return cudaGetLastError ();
+}
+
+cudaError_t launch_sk_mask_overlap (const uint8_t* mask, const float2* in, uint64_t in_span,
+                                    float2* out, uint64_t out_span, uint64_t ndat_out,
+                                    unsigned nchan, unsigned npol, unsigned offset,
+                                    uint64_t npart, uint64_t nskip, uint64_t idat_start,
+                                    cudaStream_t st)
+{
+  if (ndat_out == 0 || npart == 0) return cudaSuccess;
+  g_launches++;
+  k_sk_mask_overlap<<<dim3 (unsigned ((ndat_out + 255) / 256), nchan), 256, 0, st>>> (
+      mask, in, in_span, out, out_span, ndat_out, nchan, npol, offset, npart, nskip, idat_start);
   return cudaGetLastError ();
 }
 

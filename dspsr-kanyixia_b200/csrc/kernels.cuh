@@ -126,6 +126,28 @@ cudaError_t launch_sk_mask (const uint8_t* mask, const float2* in, uint64_t in_s
                             uint64_t out_span, uint64_t ndat, unsigned nchan, unsigned npol,
                             unsigned M, cudaStream_t stream);
 
+// SpectralKurtosis with overlapping blocks and several resolutions (engine
+// steps): sums of blocks of M every `stride` samples, the reference's
+// tscrunch of sums, detect_skfb with per-count limits flagging fine cells,
+// and the mask of overlapping blocks.
+cudaError_t launch_sk_sums_strided (const float2* in, uint64_t span, uint64_t nblk,
+                                   uint64_t stride, unsigned nchan, unsigned npol, unsigned M,
+                                   int zero_is_valid, float* sums, unsigned* counts,
+                                   cudaStream_t stream);
+cudaError_t launch_sk_tscrunch (const float* sums, const unsigned* counts, uint64_t npart,
+                                unsigned nchan, unsigned npol, unsigned nsum, unsigned offset,
+                                float* osums, unsigned* ocounts, cudaStream_t stream);
+cudaError_t launch_sk_detect_skfb (const float* sums, const unsigned* counts, uint64_t npart,
+                                   unsigned nchan, unsigned npol, unsigned Nd,
+                                   const unsigned* lim_count, const float2* lim, unsigned nlim,
+                                   unsigned nflag, unsigned flag_step, unsigned flag_offset,
+                                   uint8_t* mask, unsigned long long* nzap, cudaStream_t stream);
+cudaError_t launch_sk_mask_overlap (const uint8_t* mask, const float2* in, uint64_t in_span,
+                                    float2* out, uint64_t out_span, uint64_t ndat_out,
+                                    unsigned nchan, unsigned npol, unsigned offset,
+                                    uint64_t npart, uint64_t nskip, uint64_t idat_start,
+                                    cudaStream_t stream);
+
 // SpectralKurtosis as a stage of the pipeline: the zero-DM input of n
 // output samples starting at input sample `first` (unpacked, FPT rows of
 // span), the mask of its blocks applied to other voltages, and detection +

@@ -229,13 +229,35 @@ class Context:
 
     # ---- SpectralKurtosis engine, step by step --------------------------------------
     def sk_compute(self, d_in, in_span, ndat, nchan, npol, M, d_sums, d_counts=None,
-                   zero_is_valid=True):
+                   zero_is_valid=True, noverlap=1):
         n = ctypes.c_uint64()
         self.check(self._lib.dspsr_b200_sk_compute(self.handle, _ptr(d_in), in_span, ndat, nchan,
-                                                   npol, M, int(zero_is_valid), _ptr(d_sums),
-                                                   _ptr(d_counts), ctypes.byref(n)),
-                   "sk_compute")
+                                                   npol, M, noverlap, int(zero_is_valid),
+                                                   _ptr(d_sums), _ptr(d_counts),
+                                                   ctypes.byref(n)), "sk_compute")
         return n.value
+
+    def sk_tscrunch(self, d_sums, d_counts, npart_from, npart_to, nchan, npol, nsum, offset,
+                    d_sums_out, d_counts_out):
+        self.check(self._lib.dspsr_b200_sk_tscrunch(self.handle, _ptr(d_sums), _ptr(d_counts),
+                                                    npart_from, npart_to, nchan, npol, nsum,
+                                                    offset, _ptr(d_sums_out), _ptr(d_counts_out)),
+                   "sk_tscrunch")
+
+    def sk_detect_skfb(self, d_sums, d_counts, npart, nchan, npol, std_devs, d_mask, mask_npart,
+                       nflag=1, flag_step=1, flag_offset=1, Nd=1, d_zapped=None):
+        self.check(self._lib.dspsr_b200_sk_detect_skfb(self.handle, _ptr(d_sums), _ptr(d_counts),
+                                                       npart, nchan, npol, Nd, std_devs, nflag,
+                                                       flag_step, flag_offset, _ptr(d_mask),
+                                                       mask_npart, _ptr(d_zapped)),
+                   "sk_detect_skfb")
+
+    def sk_mask_overlap(self, d_mask, d_in, in_span, d_out, out_span, nchan, npol, M, offset,
+                        npart, nskip, idat_start):
+        self.check(self._lib.dspsr_b200_sk_mask_overlap(self.handle, _ptr(d_mask), _ptr(d_in),
+                                                        in_span, _ptr(d_out), out_span, nchan,
+                                                        npol, M, offset, npart, nskip,
+                                                        idat_start), "sk_mask_overlap")
 
     def sk_detect_ft(self, d_sums, d_counts, npart, nchan, npol, M, lower, upper, d_mask,
                      Nd=1, d_zapped=None):

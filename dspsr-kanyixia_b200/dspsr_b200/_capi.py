@@ -247,8 +247,15 @@ SIGNATURES = {
     "dspsr_b200_rfi_proposer_create": (c_int, [c_vp, c_uint, c_uint, c_uint, c_u64, c_uint, c_u64,
                                                ctypes.POINTER(c_vp)]),
     "dspsr_b200_rfi_proposer_destroy": (c_int, [c_vp]),
-    "dspsr_b200_sk_compute": (c_int, [c_vp, c_vp, c_u64, c_u64, c_uint, c_uint, c_uint, c_int,
-                                      c_vp, c_vp, c_u64p]),
+    "dspsr_b200_sk_compute": (c_int, [c_vp, c_vp, c_u64, c_u64, c_uint, c_uint, c_uint, c_uint,
+                                      c_int, c_vp, c_vp, c_u64p]),
+    "dspsr_b200_sk_tscrunch": (c_int, [c_vp, c_vp, c_vp, c_u64, c_u64, c_uint, c_uint, c_uint,
+                                       c_uint, c_vp, c_vp]),
+    "dspsr_b200_sk_detect_skfb": (c_int, [c_vp, c_vp, c_vp, c_u64, c_uint, c_uint, c_uint,
+                                          ctypes.c_float, c_uint, c_uint, c_uint, c_vp, c_u64,
+                                          c_vp]),
+    "dspsr_b200_sk_mask_overlap": (c_int, [c_vp, c_vp, c_vp, c_u64, c_vp, c_u64, c_uint, c_uint,
+                                           c_uint, c_uint, c_u64, c_u64, c_u64]),
     "dspsr_b200_sk_detect_ft": (c_int, [c_vp, c_vp, c_vp, c_u64, c_uint, c_uint, c_uint, c_uint,
                                         ctypes.c_float, ctypes.c_float, c_vp, c_vp]),
     "dspsr_b200_sk_detect_tscr": (c_int, [c_vp, c_vp, c_vp, c_u64, c_uint, c_uint, c_uint, c_uint,

@@ -470,11 +470,13 @@ int dspsr_b200_sk (dspsr_b200_context* ctx, const float* d_in, uint64_t in_span,
    SpectralKurtosisCUDA.cu:45-99).  Layouts as for dspsr_b200_sk. */
 /* Engine::compute (SpectralKurtosis.C:674-798): S1, S2 (d_sums, float) and
    the counted samples (d_counts, optional) of every (part, chan, pol); the
-   input is not written. */
+   input is not written.  noverlap > 1 (Resolution::prepare, :251-281): blocks
+   of M samples every M / noverlap samples, npart = (ndat - (M - M/noverlap))
+   / (M / noverlap). */
 int dspsr_b200_sk_compute (dspsr_b200_context* ctx, const float* d_in, uint64_t in_span,
                            uint64_t ndat, unsigned nchan, unsigned npol, unsigned M,
-                           int zero_is_valid, float* d_sums, uint32_t* d_counts,
-                           uint64_t* npart);
+                           unsigned noverlap, int zero_is_valid, float* d_sums,
+                           uint32_t* d_counts, uint64_t* npart);
 /* Engine::detect_ft (detect_skfb, SpectralKurtosis.C:1105-1222) with the
    thresholds given: d_mask[part][chan] set to 1 where zapped (others left as
    they are); d_counts NULL means M counted everywhere; *d_zapped (device,
@@ -491,6 +493,36 @@ int dspsr_b200_sk_detect_tscr (dspsr_b200_context* ctx, const float* d_sums,
                                const uint32_t* d_counts, uint64_t npart, unsigned nchan,
                                unsigned npol, unsigned M, unsigned Nd, float std_devs,
                                uint8_t* d_mask, uint32_t* nzapped_chan);
+/* Several resolutions (SpectralKurtosis::detect, SpectralKurtosis.C:830-
+   915).  tscrunch_sums (:917-986): coarse part q of npart_to sums the fine
+   parts q*offset + i*offset, i < nsum (nsum = M_coarse / M_fine, offset =
+   the ratio of the two resolutions' block strides -- the reference's own
+   indexing), sums and counts; the fine sums hold npart_from parts. */
+int dspsr_b200_sk_tscrunch (dspsr_b200_context* ctx, const float* d_sums,
+                            const uint32_t* d_counts, uint64_t npart_from, uint64_t npart_to,
+                            unsigned nchan, unsigned npol, unsigned nsum, unsigned offset,
+                            float* d_sums_out, uint32_t* d_counts_out);
+/* detect_skfb at one resolution (:1105-1222): each (part, chan) is tested
+   against SKLimits(count, std_devs) with Nd and npol tests (get_limits,
+   :988-1008); a zapped cell sets nflag cells of the finest mask, flag_step
+   fine parts apart, from fine part q * flag_offset (nflag = M / M_finest,
+   flag_step = the finest noverlap, flag_offset = nflag * flag_step /
+   noverlap; all 1 at the finest resolution).  Synchronises. */
+int dspsr_b200_sk_detect_skfb (dspsr_b200_context* ctx, const float* d_sums,
+                               const uint32_t* d_counts, uint64_t npart, unsigned nchan,
+                               unsigned npol, unsigned Nd, float std_devs, unsigned nflag,
+                               unsigned flag_step, unsigned flag_offset, uint8_t* d_mask,
+                               uint64_t mask_npart, uint64_t* d_zapped);
+/* mask (:1465-1566) with overlapping blocks: npart parts of M samples,
+   offset apart, from input sample idat_start, mask rows from part nskip; a
+   sample takes the decision of the last part that covers it, as the
+   reference's part-after-part copy leaves it.  Out of place; writes
+   (npart - 1) * offset + M samples per span. */
+int dspsr_b200_sk_mask_overlap (dspsr_b200_context* ctx, const uint8_t* d_mask,
+                                const float* d_in, uint64_t in_span, float* d_out,
+                                uint64_t out_span, unsigned nchan, unsigned npol, unsigned M,
+                                unsigned offset, uint64_t npart, uint64_t nskip,
+                                uint64_t idat_start);
 /* Engine::reset_mask and count_mask (synchronises) */
 int dspsr_b200_sk_reset_mask (dspsr_b200_context* ctx, uint8_t* d_mask, uint64_t npart,
                               unsigned nchan);

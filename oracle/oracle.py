@@ -144,6 +144,110 @@ def sk_detect_tscr(sums, counts, Nd, std_devs):
     return mask
 
 
+def sk_resolution(M, noverlap, ndat):
+    """Resolution::prepare (Signal/General/SpectralKurtosis.C:251-281):
+    (overlap_offset, npart, output_ndat, idat_start)."""
+    off = M // noverlap
+    start = M - off
+    if ndat < start:
+        return off, 0, 0, start
+    nblock = (ndat - start) // off
+    end = nblock * off
+    if end < start:
+        return off, 0, 0, start
+    return off, nblock, end - start, start
+
+
+def sk_compute_overlap(x, M, noverlap, zero_is_valid=True, ndat=None):
+    """SpectralKurtosis::compute (SpectralKurtosis.C:674-798) for the blocks
+    Resolution::prepare gives: block b holds samples b*off ... b*off + M - 1;
+    S1 and S2 of each (block, chan, pol) summed in order in double from the
+    float sqld (S2 of its float square), the pol-0 count as the weight.
+    Returns sums (npart, nchan, npol, 2) float32 and counts (npart, nchan)."""
+    nchan, npol, span = x.shape
+    ndat = span if ndat is None else ndat
+    off, npart, _, _ = sk_resolution(M, noverlap, ndat)
+    xr = np.ascontiguousarray(x.real, np.float32)
+    xi = np.ascontiguousarray(x.imag, np.float32)
+    sqld = xr * xr + xi * xi                              # float32, no contraction
+    sums = np.zeros((npart, nchan, npol, 2), np.float32)
+    counts = np.zeros((npart, nchan), np.uint32)
+    for b in range(npart):
+        blk = sqld[:, :, b * off:b * off + M]
+        keep = np.ones_like(blk, bool) if zero_is_valid else blk != 0
+        v1 = np.where(keep, blk, np.float32(0)).astype(np.float64)
+        v2 = np.where(keep, blk * blk, np.float32(0)).astype(np.float64)
+        # sequential double sums (adding +0.0 for skipped values changes nothing)
+        sums[b, :, :, 0] = np.cumsum(v1, axis=2)[:, :, -1].astype(np.float32)
+        sums[b, :, :, 1] = np.cumsum(v2, axis=2)[:, :, -1].astype(np.float32)
+        counts[b] = keep[:, 0].sum(axis=1)
+    return sums, counts
+
+
+def sk_tscrunch(sums, counts, npart_to, nsum, offset):
+    """SpectralKurtosis::tscrunch_sums (SpectralKurtosis.C:917-986): coarse
+    part q adds the fine parts q*offset + i*offset, i < nsum, in that order
+    (float sums, integer counts) -- the reference's indexing."""
+    out = np.zeros((npart_to,) + sums.shape[1:], np.float32)
+    oc = np.zeros((npart_to, counts.shape[1]), np.uint32)
+    for q in range(npart_to):
+        acc = sums[q * offset].copy()
+        cc = counts[q * offset].astype(np.uint64)
+        for i in range(1, nsum):
+            acc = (acc + sums[q * offset + i * offset]).astype(np.float32)
+            cc = cc + counts[q * offset + i * offset]
+        out[q] = acc
+        oc[q] = cc.astype(np.uint32)
+    return out, oc
+
+
+def sk_detect_skfb(sums, counts, Nd, std_devs, mask, nflag=1, flag_step=1, flag_offset=1):
+    """SpectralKurtosis::detect_skfb (SpectralKurtosis.C:1105-1222) at one
+    resolution, limits of SKLimits(count, std_devs) per count (get_limits,
+    :988-1008) with npol tests; a zapped cell sets nflag fine mask cells from
+    fine part q*flag_offset, flag_step apart.  Updates mask in place."""
+    npart, nchan, npol, _ = sums.shape
+    cache = {}
+    for q in range(npart):
+        for c in range(nchan):
+            mp = int(counts[q, c])
+            if mp == 0:
+                continue
+            zap = True
+            if mp > 2:
+                if mp not in cache:
+                    cache[mp] = sk_limits(mp, Nd, std_devs, npol)
+                lo, hi = cache[mp]
+                m_fac = np.float32(mp * Nd + 1) / np.float32(mp - 1)
+                zap = False
+                for p in range(npol):
+                    s1, s2 = sums[q, c, p, 0], sums[q, c, p, 1]
+                    v = m_fac * (np.float32(mp) * (s2 / (s1 * s1)) - np.float32(1))
+                    if v > hi or v < lo:
+                        zap = True
+            if zap:
+                for f in range(nflag):
+                    mask[q * flag_offset + f * flag_step, c] = 1
+    return mask
+
+
+def sk_mask_overlap(mask, x, M, offset, npart, nskip, idat_start):
+    """SpectralKurtosis::mask (SpectralKurtosis.C:1465-1566): part after part,
+    M samples from the input at idat_start + ipart*offset copied (or zeroed
+    where mask[ipart + nskip] is set) to the output at ipart*offset."""
+    nchan, npol, _ = x.shape
+    out = np.zeros((nchan, npol, (npart - 1) * offset + M), x.dtype)
+    for c in range(nchan):
+        for p in range(npol):
+            for ip in range(npart):
+                a = ip * offset
+                if mask[ip + nskip, c]:
+                    out[c, p, a:a + M] = 0
+                else:
+                    out[c, p, a:a + M] = x[c, p, idat_start + a:idat_start + a + M]
+    return out
+
+
 def sk_limits(M, Nd=1, std_devs=3.0, ntest=1):
     """(lower, upper) float32 thresholds of SKLimits::calc_limits."""
     lo, hi = ctypes.c_float(), ctypes.c_float()

@@ -249,3 +249,74 @@ def test_sk_engine_steps_match_oracle(ctx, b2, orc, nchan, npol, M, ndat, zero_i
     assert np.array_equal(mask.cpu().numpy(), rm | ref_t)
     if nchan > 2:
         assert ref_t[0, 1] == 1, "the tone channel is zapped by the time-scrunched test"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("res,zero_is_valid", [([(64, 1), (128, 2), (256, 4)], True),
+                                               ([(128, 1), (256, 2)], False),
+                                               ([(64, 2)], True)])
+def test_sk_resolutions_match_oracle(ctx, b2, orc, res, zero_is_valid):
+    """SpectralKurtosis::detect over several resolutions with overlapping
+    blocks (SpectralKurtosis.C:251-281, 830-986, 1105-1222, 1465-1566): sums
+    of every resolution, the finest mask and the masked voltages through the
+    C ABI's engine steps, bit-exact against the oracle's restatement."""
+    torch = pytest.importorskip("torch")
+    nchan, npol, ndat = 6, 2, 5000
+    rng = np.random.default_rng(len(res) * 7 + int(zero_is_valid))
+    x = (rng.standard_normal((nchan, npol, ndat)) + 1j * rng.standard_normal((nchan, npol, ndat))
+         ).astype(np.complex64)
+    x[1, :, 700:760] *= 12.0                        # a burst
+    x[3] += 3.0 * np.exp(2j * np.pi * 0.21 * np.arange(ndat))     # a tone
+    if not zero_is_valid:
+        x[4, :, 1000:1100] = 0                      # dropped samples
+    d = torch.from_numpy(x).cuda()
+    std_devs = 3.0
+    # the reference's order: compute at the finest, then per resolution
+    # tscrunch (from the previous one) and detect_skfb into the finest mask
+    M0, nov0 = res[0]
+    off0, npart0, _, _ = orc.sk_resolution(M0, nov0, ndat)
+    rs, rc = orc.sk_compute_overlap(x, M0, nov0, zero_is_valid)
+    assert rs.shape[0] == npart0
+    gs = torch.zeros((npart0, nchan, npol, 2), dtype=torch.float32, device="cuda")
+    gc = torch.zeros((npart0, nchan), dtype=torch.int32, device="cuda")
+    assert ctx.sk_compute(d, ndat, ndat, nchan, npol, M0, gs, gc, zero_is_valid, nov0) == npart0
+    ctx.synchronize()
+    assert np.array_equal(gs.cpu().numpy(), rs)
+    assert np.array_equal(gc.cpu().numpy().astype(np.uint32), rc)
+    rmask = np.zeros((npart0, nchan), np.uint8)
+    gmask = torch.zeros((npart0, nchan), dtype=torch.uint8, device="cuda")
+    prev = (M0, nov0, off0, npart0)
+    for ires, (M, nov) in enumerate(res):
+        off, npart, _, _ = orc.sk_resolution(M, nov, ndat)
+        if ires > 0:
+            nsum, offset = M // prev[0], off // prev[2]
+            rs, rc = orc.sk_tscrunch(rs, rc, npart, nsum, offset)
+            gs2 = torch.zeros((npart, nchan, npol, 2), dtype=torch.float32, device="cuda")
+            gc2 = torch.zeros((npart, nchan), dtype=torch.int32, device="cuda")
+            ctx.sk_tscrunch(gs, gc, prev[3], npart, nchan, npol, nsum, offset, gs2, gc2)
+            gs, gc = gs2, gc2
+            ctx.synchronize()
+            assert np.array_equal(gs.cpu().numpy(), rs), ires
+            assert np.array_equal(gc.cpu().numpy().astype(np.uint32), rc), ires
+        nflag = M // M0 if ires else 1
+        flag_step = nov0 if ires else 1
+        flag_offset = nflag * flag_step // nov if ires else 1
+        orc.sk_detect_skfb(rs, rc, 1, std_devs, rmask, nflag, flag_step, flag_offset)
+        ctx.sk_detect_skfb(gs, gc, npart, nchan, npol, std_devs, gmask, npart0, nflag, flag_step,
+                           flag_offset)
+        assert np.array_equal(gmask.cpu().numpy(), rmask), ires
+        prev = (M, nov, off, npart)
+    assert rmask.sum() > 0
+    # mask (SpectralKurtosis.C:1465-1566)
+    max_M, max_off = res[-1][0], orc.sk_resolution(res[-1][0], res[-1][1], ndat)[0]
+    idat_start = max_M - max_off
+    nskip = idat_start // off0
+    back_out = orc.sk_resolution(res[-1][0], res[-1][1], ndat)[2]
+    npart_m = (back_out - M0) // off0 + 1
+    ref = orc.sk_mask_overlap(rmask, x, M0, off0, npart_m, nskip, idat_start)
+    out = torch.full((nchan, npol, ref.shape[2]), complex(np.nan, np.nan), dtype=torch.complex64,
+                     device="cuda")
+    ctx.sk_mask_overlap(gmask, d, ndat, out, ref.shape[2], nchan, npol, M0, off0, npart_m, nskip,
+                        idat_start)
+    ctx.synchronize()
+    assert np.array_equal(out.cpu().numpy(), ref)
