@@ -1597,11 +1597,49 @@ def run_b200_c3(args, cfg, world, rank, local):
                                 "cores": threads, "kind": "port",
                                 "sample": (f"two FFT parts of each of the first {ns} streams x "
                                            f"{reps} through the oracle chain, {total:.1f} s")}
+        # parity: the first stream, and the first four-step stream of several
+        # channels, one block each through a fresh pipeline with the tuned
+        # plan, against the oracle chain
+        picks = [0] + [i for i, st in enumerate(streams)
+                       if st["nfft"] > 8192 and st["nchan"] > 1][:1]
+        line["parity"] = [c3_parity(cfg, b2, orc, streams[i], make_pipe, lut) for i in picks]
     if rank == 0:
         print(json.dumps(line), flush=True)
     for s in streams:
         s["pipe"].close()
         s["ctx"].close()
+
+
+def c3_parity(cfg, b2, orc, s, make_pipe, lut):
+    """One block of stream s through a fresh pipeline (its tuned plan) and
+    through the oracle chain unpack -> overlap-save -> intensity -> fold
+    (Convolution.C:724-803, Fold.C:790-837): hits bit-exact, profiles within
+    1e-5 of each bin."""
+    pl = make_pipe(s, s["plan"])
+    nout = pl.run(s["blocks"][0], s["ndat"])
+    prof, hits = pl.get_profiles()
+    pl.close()
+    raw = s["blocks"][0].cpu().numpy()
+    x = orc.unpack8(raw, s["ndat"], s["nchan"], 2, 2, np.asarray(lut, np.float32))
+    x = x.view(np.complex64).reshape(s["nchan"], 2, s["ndat"])
+    h = orc.dedispersion_response(cfg["cf"], s["bw"], s["dm"], s["nchan"], s["nfft"],
+                                  input_nchan=s["nchan"], mode=0)
+    y = orc.convolve(x, h, s["nfft"], s["pos"], s["neg"], nthreads=os.cpu_count() or 1)
+    d = orc.detect(y, 0)
+    rate = abs(s["bw"]) / s["nchan"] * 1e6
+    phi = orc.fold_phi(START_MJD, EPOCH_MJD, s["pos"], rate, s["period"])
+    plan = orc.fold_binplan(phi, (1.0 / rate) / s["period"], y.shape[2], s["nbin"])
+    rprof, rhits = orc.fold_accumulate(d, plan, s["nbin"])
+    hit = rhits > 0
+    err = float(np.max(np.abs(prof.astype(np.float64) - rprof)[..., hit]
+                       / np.abs(rprof.astype(np.float64))[..., hit]))
+    return {"stream": {k: s[k] for k in ("nchan", "nfft", "bw", "dm", "nbin")},
+            "plan": {"row_length": s["plan"][1] or min(s["nfft"], 8192),
+                     "rows": "bf16x3 tensor" if s["plan"][2] == 3 else "fp32"},
+            "samples_folded": int(nout), "oracle_samples": int(y.shape[2]),
+            "hits_bit_exact": bool(np.array_equal(hits, rhits)),
+            "max_profile_rel_err": err,
+            "pass": bool(np.array_equal(hits, rhits)) and err < 1e-5 and nout == y.shape[2]}
 
 
 def c5_plan(cfg, b2):
@@ -1669,6 +1707,65 @@ def run_reference_c5(args, cfg, world, rank):
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def c5_parity(cfg, b2, raw, pos, neg, nfft):
+    """A bounded sample of C5's input (the first inverse-filterbank parts,
+    enough for one FFT part of every re-channelised output channel) through
+    fresh GPU objects and through the oracle chain: InverseFilterbank
+    (InverseFilterbankEngineCPU.C:46-792) -> 1024-channel filterbank ->
+    overlap-save -> Stokes -> fold.  Hits bit-exact, profiles within 5e-5 of
+    Stokes I per bin."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    orc.lib()
+    c = ifb_cfg_dict(cfg)
+    keep, lout, ipos, ineg, in_step, out_step = orc.ifb_sizes(c)
+    nc = cfg["fb"]
+    nparts = -(-((nfft + 16) * nc) // out_step)
+    ndat = nparts * in_step + ipos + ineg
+    nin, npol = cfg["nin"], cfg["npol"]
+    sample = raw[:ndat * nin * npol * 2].clone()
+    ctx = b2.Context(torch.cuda.current_device())
+    ifb = b2.InverseFilterbank(ctx, nin, 1, nin, npol, cfg["lin"], os=(4, 3),
+                               output_discard=(cfg["disc"], cfg["disc"]))
+    np_ = ifb.npart(ndat)
+    nwide = np_ * ifb.info["out_step"]
+    wide = torch.empty((1, npol, nwide, 2), dtype=torch.float32, device=sample.device)
+    ifb.perform(sample, ndat, wide, nwide, input_kind=b2.INT16_TFPD)
+    pcfg = b2.make_config(cfg["cf"], cfg["bw"], cfg["dm"], 1, npol, nfft, pos, neg, cfg["nbin"],
+                          cfg["period"], state=b2.STOKES, input_kind=b2.FLOAT_FPT,
+                          start_mjd=START_MJD, epoch_mjd=EPOCH_MJD, filterbank_nchan=nc)
+    pipe = b2.Pipeline(ctx, pcfg)
+    nout = pipe.run(wide, nwide, nwide)
+    prof, hits = pipe.get_profiles()
+    pipe.close()
+    ifb.close()
+    ctx.close()
+    t0 = time.perf_counter()
+    h16 = sample.cpu().numpy()
+    x = orc.unpack16(h16, ndat, nin, npol, 2, False).view(np.complex64).reshape(nin, npol, ndat)
+    w = orc.inverse_filterbank(x, c)
+    n = (w.shape[2] // nc) * nc
+    y = orc.filterbank(w[:, :, :n], nc)
+    freqs = orc.channel_centres(cfg["cf"], cfg["bw"], nc, swap=True, dc_centred=True)
+    hresp = orc.dedispersion_response_channels(freqs, cfg["bw"], cfg["dm"], nfft, mode=0)
+    z = orc.convolve(y, hresp, nfft, pos, neg, nthreads=os.cpu_count() or 1)
+    d = orc.detect(z, 3)
+    rate = abs(cfg["bw"]) / nc * 1e6
+    phi = orc.fold_phi(START_MJD, EPOCH_MJD, pos, rate, cfg["period"])
+    plan = orc.fold_binplan(phi, (1.0 / rate) / cfg["period"], z.shape[2], cfg["nbin"])
+    rprof, rhits = orc.fold_accumulate(d, plan, cfg["nbin"])
+    rprof = rprof.astype(np.float64)
+    scale = np.broadcast_to(rprof[:, 0:1], rprof.shape)
+    hit = rhits > 0
+    err = float(np.max(np.abs(prof.astype(np.float64) - rprof)[..., hit] / scale[..., hit]))
+    ok = bool(np.array_equal(hits, rhits)) and err < 5e-5 and nout == z.shape[2]
+    return {"sample": f"{np_} inverse-filterbank parts ({ndat} samples per PFB channel)",
+            "samples_folded": int(nout), "oracle_samples": int(z.shape[2]),
+            "hits_bit_exact": bool(np.array_equal(hits, rhits)), "max_profile_rel_err": err,
+            "rtol": 5e-5, "pass": ok, "oracle_s": round(time.perf_counter() - t0, 1)}
 
 
 def make_pfb_block(cfg, seed, device, taps=12, beta=8.0, duty=0.03, snr=10.0):
@@ -1857,6 +1954,7 @@ def run_b200_c5(args, cfg, world, rank, local):
                      "traffic": None, "peak_source": peak_src,
                      "note": "algorithmic bytes: the int16 input once; FFT-bound chain"},
         "e2e": None,
+        "parity": c5_parity(cfg, b2, raw, pos, neg, nfft) if rank == 0 and world == 1 else None,
         "check": {"hits_total": int(hits.sum()),
                   # a 1.6 ms turn is 1250 samples of the re-channelised data,
                   # so most of the 4096 bins get no hits: judge the hit ones
