@@ -449,6 +449,10 @@ def run_b200(args, cfg, world, rank, local):
     pos, neg, nfft = b2.dispersion_plan(cfg["cf"], cfg["bw"], cfg["dm"], nc, cfg["nfft"])
     nk = nfft - pos - neg
     lut, _ = b2.bittable8()
+    if args.lut_perturb:
+        # a table that is not (x + 0.5) * scale: the kernels look it up
+        lut = (np.asarray(lut, np.float32)
+               * (1 + 1e-3 * np.sin(np.arange(256)))).astype(np.float32)
     c = b2.make_config(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nchan"], cfg["npol"], nfft, pos,
                        neg, cfg["nbin"], cfg["period"], state=cfg["state"], lut=lut,
                        start_mjd=START_MJD, epoch_mjd=EPOCH_MJD, filterbank_nchan=cfg["fb"],
@@ -1979,6 +1983,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--lut-perturb", action="store_true",
+                    help="c1/c2: an 8-bit table that is not affine, so the kernels look it up")
     ap.add_argument("--c3-tensor", type=int, default=1,
                     help="c3: let the autotuner also try the tensor-core rows (1) or not (0)")
     ap.add_argument("--no-proposer", action="store_true",

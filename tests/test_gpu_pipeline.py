@@ -602,14 +602,18 @@ def test_pipeline_subint_slots_exhausted(ctx, b2):
                                         subint_turns=1.0))
 
 
-@pytest.mark.parametrize("kind", [0, 1])
-def test_pipeline_fused_filterbank_matches_stage(ctx, b2, orc, kind):
+@pytest.mark.parametrize("kind,perturb", [(0, False), (1, False), (0, True)])
+def test_pipeline_fused_filterbank_matches_stage(ctx, b2, orc, kind, perturb):
     """The 64-channel filterbank computed inside the column pass (C2's shape)
     against the filterbank as a stage of its own and against the oracle
     chain, over blocks whose carry crosses parts, from device and host
-    memory."""
+    memory; perturb: an 8-bit table that is not affine, looked up from the
+    pass's replicated shared-memory copies."""
     cfg = base_cfg(b2, dm=500.0, bw=256.0, fb=64, nfft=1 << 16, state=3, nbin=512,
                    period=5.757e-3, kind=kind)
+    if perturb:
+        cfg["lut"] = (np.asarray(cfg["lut"], np.float32)
+                      * (1 + 1e-3 * np.cos(np.arange(256)))).astype(np.float32)
     rng = np.random.default_rng(77 + kind)
     nk = cfg["nfft"] - cfg["pos"] - cfg["neg"]
     blocks = make_blocks(rng, cfg, [(cfg["nfft"] + 2 * nk + 321) * 64, (nk - 17) * 64,
