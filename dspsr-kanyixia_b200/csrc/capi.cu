@@ -602,6 +602,13 @@ struct dspsr_b200_pipeline
   uint64_t sk_ncarry = 0;
   uint64_t sk_out0 = 0;             // SpectralKurtosis output samples before this block
   uint64_t sk_tested = 0;           // (block, channel) cells tested
+  // an RFI-mask proposer in front of the SK stage: its mask replaces SK's
+  // where it is confident, SK's own decision is the fallback
+  dspsr_b200_rfi_proposer* sk_proposer = nullptr;
+  float sk_confidence = 0.9f;
+  DevBuf<float> sk_sums;
+  DevBuf<uint32_t> sk_counts;
+  DevBuf<uint8_t> sk_pmask;
   DevBuf<float2> fbbuf;             // filterbank output, FPT
   float2* fb_tab = nullptr;         // pass tables of the filterbank FFT (fb_nsub >= 128)
   size_t fb_tab_cap = 0;
@@ -993,11 +1000,32 @@ int pipeline_sk_block (dspsr_b200_pipeline* pl, const InputView& in, uint64_t np
     B200_CHECK (ctx, pl->sk_mask.reserve (nblk * sh.nchan), "cudaMalloc sk mask");
     // statistics and test of the zero-DM blocks (the kernel masks them in
     // place too, which nothing reads), then the mask of the dedispersed ones
-    B200_CHECK (ctx, launch_sk (z, pl->sk_span, z, pl->sk_span, nblk, sh.nchan, cfg.npol, M, 1, 1,
-                                pl->sk_lower, pl->sk_upper, nullptr, nullptr, pl->sk_mask.ptr,
-                                pl->sk_zapped.ptr, ctx->stream), "spectral kurtosis");
-    B200_CHECK (ctx, launch_sk_apply (pl->sk_mask.ptr, v, pl->sk_span, out_n, sh.nchan, cfg.npol,
-                                      M, ctx->stream), "sk mask");
+    const uint8_t* mask = pl->sk_mask.ptr;
+    if (pl->sk_proposer)
+    {
+      // the SK sums feed the proposer; SK's mask is its fallback
+      B200_CHECK (ctx, pl->sk_sums.reserve (nblk * sh.nchan * cfg.npol * 2), "cudaMalloc sk sums");
+      B200_CHECK (ctx, pl->sk_counts.reserve (nblk * sh.nchan), "cudaMalloc sk counts");
+      B200_CHECK (ctx, pl->sk_pmask.reserve (nblk * sh.nchan), "cudaMalloc proposer mask");
+      B200_CHECK (ctx, launch_sk (z, pl->sk_span, z, pl->sk_span, nblk, sh.nchan, cfg.npol, M, 1,
+                                  1, pl->sk_lower, pl->sk_upper, pl->sk_sums.ptr,
+                                  pl->sk_counts.ptr, pl->sk_mask.ptr, pl->sk_zapped.ptr,
+                                  ctx->stream), "spectral kurtosis");
+      int rc = dspsr_b200_rfi_proposer_features (pl->sk_proposer, pl->sk_sums.ptr,
+                                                 pl->sk_counts.ptr, nblk, cfg.npol);
+      if (!rc)
+        rc = dspsr_b200_rfi_proposer_infer (pl->sk_proposer, pl->sk_mask.ptr, pl->sk_confidence,
+                                            pl->sk_pmask.ptr, nullptr, nullptr);
+      if (rc) return fail (ctx, rc, "pipeline: rfi proposer: %s", ctx->error.c_str ());
+      mask = pl->sk_pmask.ptr;
+    }
+    else
+      B200_CHECK (ctx, launch_sk (z, pl->sk_span, z, pl->sk_span, nblk, sh.nchan, cfg.npol, M, 1,
+                                  1, pl->sk_lower, pl->sk_upper, nullptr, nullptr,
+                                  pl->sk_mask.ptr, pl->sk_zapped.ptr, ctx->stream),
+                  "spectral kurtosis");
+    B200_CHECK (ctx, launch_sk_apply (mask, v, pl->sk_span, out_n, sh.nchan, cfg.npol, M,
+                                      ctx->stream), "sk mask");
     pl->sk_tested += nblk * sh.nchan;
     int rc = pipeline_fold_plan (pl, pl->sk_out0, pl->sk_out0 + sh.nfilt_pos, out_n);
     if (rc) return rc;
@@ -2990,6 +3018,9 @@ int dspsr_b200_pipeline_destroy (dspsr_b200_pipeline* pl)
   }
   pl->sk_mask.release ();
   pl->sk_zapped.release ();
+  pl->sk_sums.release ();
+  pl->sk_counts.release ();
+  pl->sk_pmask.release ();
   delete pl;
   return DSPSR_B200_OK;
 }
@@ -3314,6 +3345,33 @@ int dspsr_b200_pipeline_kernel_times (dspsr_b200_pipeline* pl, double* ms, uint6
 }
 
 uint64_t dspsr_b200_kernel_launches (void) { return kernel_launches (); }
+
+int dspsr_b200_pipeline_set_rfi_proposer (dspsr_b200_pipeline* pl,
+                                          dspsr_b200_rfi_proposer* proposer, float confidence)
+{
+  if (!pl) return DSPSR_B200_EINVAL;
+  if (!proposer)
+  {
+    pl->sk_proposer = nullptr;
+    return DSPSR_B200_OK;
+  }
+  if (!pl->sk_on)
+    return fail (pl->ctx, DSPSR_B200_ESTATE, "pipeline: the proposer needs the SK stage (sk_M)");
+  if (confidence < 0.5f || confidence > 1.f)
+    return fail (pl->ctx, DSPSR_B200_EINVAL, "pipeline: confidence %g outside [0.5, 1]",
+                 double (confidence));
+  dspsr_b200_context* pctx = nullptr;
+  unsigned pnchan = 0, pM = 0;
+  rfi_proposer_shape (proposer, &pctx, &pnchan, &pM);
+  if (pctx != pl->ctx || pnchan != pl->conv.shape.nchan || pM != pl->sk_M)
+    return fail (pl->ctx, DSPSR_B200_EINVAL,
+                 "pipeline: the proposer is for %u channels of %u samples on another or the "
+                 "same context; the pipeline needs %u channels of %u on its own", pnchan, pM,
+                 pl->conv.shape.nchan, pl->sk_M);
+  pl->sk_proposer = proposer;
+  pl->sk_confidence = confidence;
+  return DSPSR_B200_OK;
+}
 
 int dspsr_b200_pipeline_sk_counts (dspsr_b200_pipeline* pl, uint64_t* zapped, uint64_t* tested)
 {

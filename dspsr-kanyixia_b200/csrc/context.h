@@ -15,3 +15,11 @@ struct dspsr_b200_context
   float2* d_fb_tab = nullptr; // pass tables of the standalone filterbank's FFT
   unsigned fb_tab_n = 0;      // ... for this transform length
 };
+
+struct dspsr_b200_rfi_proposer;
+
+namespace b200 {
+// the context, channels per block and block length a proposer was made for
+void rfi_proposer_shape (const dspsr_b200_rfi_proposer* proposer, dspsr_b200_context** ctx,
+                         unsigned* nchan, unsigned* M);
+} // namespace b200

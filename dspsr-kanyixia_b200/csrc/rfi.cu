@@ -543,6 +543,14 @@ struct dspsr_b200_rfi_proposer
   }
 };
 
+void b200::rfi_proposer_shape (const dspsr_b200_rfi_proposer* r, dspsr_b200_context** ctx,
+                               unsigned* nchan, unsigned* M)
+{
+  *ctx = r->ctx;
+  *nchan = r->nchan;
+  *M = r->M;
+}
+
 namespace {
 
 int rfail (dspsr_b200_context* ctx, int code, const char* fmt, ...)

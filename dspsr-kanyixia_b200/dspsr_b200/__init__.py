@@ -788,6 +788,13 @@ class Pipeline:
                        "kernel_times")
         return {k: (ms[i], n[i]) for i, k in enumerate(self.KERNELS)}
 
+    def set_rfi_proposer(self, proposer, confidence=0.9):
+        """Put an RfiProposer in front of the SK stage (None detaches it)."""
+        self.ctx.check(self._lib.dspsr_b200_pipeline_set_rfi_proposer(
+            self.handle, proposer.handle if proposer is not None else None, confidence),
+            "set_rfi_proposer")
+        self._proposer = proposer
+
     def sk_counts(self):
         """(zapped, tested) (block, channel) cells of the SpectralKurtosis stage."""
         z, t = ctypes.c_uint64(), ctypes.c_uint64()

@@ -265,6 +265,7 @@ SIGNATURES = {
     "dspsr_b200_sk_mask": (c_int, [c_vp, c_vp, c_vp, c_u64, c_vp, c_u64, c_u64, c_uint, c_uint,
                                    c_uint]),
     "dspsr_b200_pipeline_sk_counts": (c_int, [c_vp, c_u64p, c_u64p]),
+    "dspsr_b200_pipeline_set_rfi_proposer": (c_int, [c_vp, c_vp, ctypes.c_float]),
     "dspsr_b200_rfi_proposer_features": (c_int, [c_vp, c_vp, c_vp, c_u64, c_uint]),
     "dspsr_b200_rfi_proposer_train": (c_int, [c_vp, c_vp, c_uint, c_uint, ctypes.c_float,
                                               ctypes.c_float, c_fp]),

@@ -685,8 +685,15 @@ int dspsr_b200_pipeline_create (dspsr_b200_context* ctx,
                                 const dspsr_b200_pipeline_config* config,
                                 dspsr_b200_pipeline** pipe);
 int dspsr_b200_pipeline_destroy (dspsr_b200_pipeline* pipe);
+/* The RFI-mask proposer (dspsr_b200_rfi_proposer_*, created on the same
+   context, for the pipeline's channels and sk_M, with max_npart at least the
+   SK blocks of one call) in front of the SK stage: each block's SK sums feed
+   it, and its mask -- SK's own decision where it is less confident than
+   `confidence` -- zeroes the dedispersed voltages.  NULL detaches it. */
+int dspsr_b200_pipeline_set_rfi_proposer (dspsr_b200_pipeline* pipe,
+                                          dspsr_b200_rfi_proposer* proposer, float confidence);
 /* SpectralKurtosis of the pipeline so far: (block, channel) cells zapped
-   and tested (SpectralKurtosis::Count); synchronises */
+   and tested (SpectralKurtosis::Count; SK's own decisions); synchronises */
 int dspsr_b200_pipeline_sk_counts (dspsr_b200_pipeline* pipe, uint64_t* zapped,
                                    uint64_t* tested);
 /* Processes one block of ndat new input samples (device memory, layout given

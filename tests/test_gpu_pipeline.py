@@ -891,3 +891,49 @@ def test_pipeline_sk_stage_matches_oracle(ctx, b2, orc, name, kw, M):
     assert tested == rtested and zapped == rzap, (zapped, rzap, tested, rtested)
     assert rzap > 0
     check(prof, hits, tot, rprof, rhits, rtotal, cfg["state"])
+
+
+def test_pipeline_sk_stage_with_rfi_proposer(ctx, b2):
+    """The RFI-mask proposer in front of the pipeline's SK stage: a proposer
+    that is never confident (p = 0.5 everywhere) defers every cell to SK, so
+    profiles and hits equal the SK-only pipeline's bit for bit; one that is
+    sure of RFI everywhere (p ~ 1) zaps every block, so nothing is folded."""
+    cfg = base_cfg(b2, dm=5.0, bw=64.0, nchan=4, nfft=1 << 14, state=3, nbin=128)
+    rng = np.random.default_rng(31)
+    nk = cfg["nfft"] - cfg["pos"] - cfg["neg"]
+    blocks = make_blocks(rng, cfg, [cfg["nfft"] + 3 * nk + 17, 2 * nk - 5])
+    for r in blocks:
+        v = r.view(np.int8).reshape(-1)
+        v[1000:5000] = 90                                   # a burst SK flags
+    M = 256
+
+    def run(bias=None):
+        c = b2.make_config(cfg["cf"], cfg["bw"], cfg["dm"], cfg["nchan"], cfg["npol"],
+                           cfg["nfft"], cfg["pos"], cfg["neg"], cfg["nbin"], cfg["period"],
+                           state=cfg["state"], lut=cfg["lut"], start_mjd=START, epoch_mjd=EPOCH,
+                           sk_M=M)
+        pl = b2.Pipeline(ctx, c)
+        pr = None
+        if bias is not None:
+            pr = b2.RfiProposer(ctx, cfg["nchan"], M, max_npart=4096)
+            p = np.zeros_like(pr.params())
+            p[-1] = bias                                     # the head's bias alone
+            pr.set_params(p)
+            pl.set_rfi_proposer(pr, confidence=0.9)
+        tot = 0
+        for r in blocks:
+            tot += pl.run(torch.from_numpy(r).cuda(), r.size // (cfg["nchan"] * 4))
+        prof, hits = pl.get_profiles()
+        zap, tested = pl.sk_counts()
+        pl.close()
+        if pr is not None:
+            pr.close()
+        return prof, hits, tot, zap
+
+    p0, h0, t0, z0 = run()
+    assert z0 > 0
+    p1, h1, t1, z1 = run(bias=0.0)
+    assert t1 == t0 and z1 == z0
+    assert np.array_equal(h1, h0) and np.array_equal(p1, p0)
+    p2, h2, t2, _ = run(bias=20.0)
+    assert t2 == t0 and h2.sum() == 0 and np.all(p2 == 0)
