@@ -3365,9 +3365,9 @@ int dspsr_b200_pipeline_set_rfi_proposer (dspsr_b200_pipeline* pl,
   rfi_proposer_shape (proposer, &pctx, &pnchan, &pM);
   if (pctx != pl->ctx || pnchan != pl->conv.shape.nchan || pM != pl->sk_M)
     return fail (pl->ctx, DSPSR_B200_EINVAL,
-                 "pipeline: the proposer is for %u channels of %u samples on another or the "
-                 "same context; the pipeline needs %u channels of %u on its own", pnchan, pM,
-                 pl->conv.shape.nchan, pl->sk_M);
+                 "pipeline: the proposer (%u channels, blocks of %u%s) does not match the "
+                 "pipeline (%u channels, sk_M %u, its own context)", pnchan, pM,
+                 pctx != pl->ctx ? ", another context" : "", pl->conv.shape.nchan, pl->sk_M);
   pl->sk_proposer = proposer;
   pl->sk_confidence = confidence;
   return DSPSR_B200_OK;
