@@ -1604,8 +1604,12 @@ def run_b200_c3(args, cfg, world, rank, local):
         # parity: the first stream, and the first four-step stream of several
         # channels, one block each through a fresh pipeline with the tuned
         # plan, against the oracle chain
-        picks = [0] + [i for i, st in enumerate(streams)
-                       if st["nfft"] > 8192 and st["nchan"] > 1][:1]
+        # the first stream and the first of another shape class (the
+        # single-kernel path when there is one)
+        first = (streams[0]["nfft"], streams[0]["nchan"])
+        others = [i for i, st in enumerate(streams) if (st["nfft"], st["nchan"]) != first]
+        fused = [i for i in others if streams[i]["nfft"] <= 8192]
+        picks = [0] + (fused or others)[:1]
         line["parity"] = [c3_parity(cfg, b2, orc, streams[i], make_pipe, lut) for i in picks]
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -896,7 +896,8 @@ def test_pipeline_sk_stage_matches_oracle(ctx, b2, orc, name, kw, M):
 def test_pipeline_sk_stage_with_rfi_proposer(ctx, b2):
     """The RFI-mask proposer in front of the pipeline's SK stage: a proposer
     that is never confident (p = 0.5 everywhere) defers every cell to SK, so
-    profiles and hits equal the SK-only pipeline's bit for bit; one that is
+    hits equal the SK-only pipeline's exactly and profiles to the rounding of
+    the fold's atomic sums (their order differs from run to run); one that is
     sure of RFI everywhere (p ~ 1) zaps every block, so nothing is folded."""
     cfg = base_cfg(b2, dm=5.0, bw=64.0, nchan=4, nfft=1 << 14, state=3, nbin=128)
     rng = np.random.default_rng(31)
@@ -934,6 +935,7 @@ def test_pipeline_sk_stage_with_rfi_proposer(ctx, b2):
     assert z0 > 0
     p1, h1, t1, z1 = run(bias=0.0)
     assert t1 == t0 and z1 == z0
-    assert np.array_equal(h1, h0) and np.array_equal(p1, p0)
+    assert np.array_equal(h1, h0)
+    assert np.allclose(p1, p0, rtol=1e-6, atol=0)
     p2, h2, t2, _ = run(bias=20.0)
     assert t2 == t0 and h2.sum() == 0 and np.all(p2 == 0)
