@@ -391,11 +391,10 @@ __device__ __forceinline__ float unpack_affine (unsigned byte, float scale)
   return __fmul_rn (__fsub_rn (big, 4194431.5f), scale);
 }
 
-// The 8-bit table of the fused filterbank pass is held eight times,
-// interleaved (entry v of copy k at 8 v + k), and lane l reads copy l % 8:
-// the bank of a lookup is then 8 (v % 4) + l % 8, so the 32 random lookups
-// of a warp spread over all 32 banks instead of the 32 entries' own.
-constexpr int FBC_LUT_COPIES = 8;
+// The 8-bit table of the fused filterbank pass is one 1 KB copy in shared
+// memory.  Eight interleaved copies (lane l reading copy l % 8, so a warp's
+// random lookups spread over all banks) measured 10 % slower on the C2 pass:
+// the 8 KB table costs more in occupancy than the bank conflicts it removes.
 
 template <int KIND, bool AFFINE>
 __device__ __forceinline__ void fetch_raw2 (const InputView& in, const float* s_lut, uint64_t r,
@@ -418,11 +417,8 @@ __device__ __forceinline__ void fetch_raw2 (const InputView& in, const float* s_
     }
     else
     {
-      // s_lut points at this lane's copy (see FBC_LUT_COPIES)
-      p0 = make_float2 (s_lut[(w & 0xff) * FBC_LUT_COPIES],
-                        s_lut[((w >> 8) & 0xff) * FBC_LUT_COPIES]);
-      p1 = make_float2 (s_lut[((w >> 16) & 0xff) * FBC_LUT_COPIES],
-                        s_lut[(w >> 24) * FBC_LUT_COPIES]);
+      p0 = make_float2 (s_lut[w & 0xff], s_lut[(w >> 8) & 0xff]);
+      p1 = make_float2 (s_lut[(w >> 16) & 0xff], s_lut[w >> 24]);
     }
   }
   else
@@ -449,17 +445,16 @@ k_fwd_cols_fb64 (const InputView in, const float* __restrict__ lut, const uint64
                  float2* __restrict__ scratch)
 {
   extern __shared__ float2 s_fbc[];
-  __shared__ float s_lut[AFFINE ? 1 : 256 * FBC_LUT_COPIES];
+  __shared__ float s_lut[AFFINE ? 1 : 256];
   __shared__ float2 s_tw64[64];
   if (!AFFINE && in.kind == IN_INT8)
-    for (int i = threadIdx.x; i < 256 * FBC_LUT_COPIES; i += blockDim.x)
-      s_lut[i] = lut[i / FBC_LUT_COPIES];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x)
+      s_lut[i] = lut[i];
   if (threadIdx.x < 64)
     s_tw64[threadIdx.x] = make_float2 (cos64 (int (threadIdx.x)), -sin64 (int (threadIdx.x)));
   __syncthreads ();
   const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const unsigned j = lane >> 2, q = lane & 3;
-  const float* my_lut = s_lut + (AFFINE ? 0 : lane % FBC_LUT_COPIES);
   const unsigned i0 = blockIdx.x * FBC_COLS;
   const unsigned i2 = i0 + warp;
   const unsigned b = blockIdx.y;
@@ -471,7 +466,7 @@ k_fwd_cols_fb64 (const InputView in, const float* __restrict__ lut, const uint64
   float2 x0[16], x1[16];
 #pragma unroll
   for (int m = 0; m < 16; m++)
-    fetch_raw2<KIND, AFFINE> (in, my_lut, t * 64 + q + 4 * m, x0[m], x1[m]);
+    fetch_raw2<KIND, AFFINE> (in, s_lut, t * 64 + q + 4 * m, x0[m], x1[m]);
   RegDFT<16, -1>::run (x0);
   RegDFT<16, -1>::run (x1);
   // twiddle w64^(q ka), then the quad exchange: column q ^ (ka >> 2)

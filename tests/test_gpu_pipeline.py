@@ -934,8 +934,9 @@ def test_pipeline_sk_stage_with_rfi_proposer(ctx, b2):
     p0, h0, t0, z0 = run()
     assert z0 > 0
     p1, h1, t1, z1 = run(bias=0.0)
-    assert t1 == t0 and z1 == z0
-    assert np.array_equal(h1, h0)
-    assert np.allclose(p1, p0, rtol=1e-6, atol=0)
+    assert z1 == z0
+    # Stokes Q, U, V bins are sums with cancellation: their rounding is
+    # measured against the bin's Stokes I
+    check(p1, h1, t1, p0, h0, t0, state=cfg["state"], rtol=1e-6)
     p2, h2, t2, _ = run(bias=20.0)
     assert t2 == t0 and h2.sum() == 0 and np.all(p2 == 0)
