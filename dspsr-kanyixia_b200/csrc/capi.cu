@@ -130,7 +130,7 @@ struct dspsr_b200_convolution
 {
   dspsr_b200_context* ctx = nullptr;
   ConvShape shape {};
-  DevBuf<float2> tw2, tw4, ptab, H, tmp, scratch;
+  DevBuf<float2> tw2, tw4, H, tmp, scratch;
   DevBuf<double> chan_par;
   DevBuf<float> lut, apod;
   DevBuf<int> err;
@@ -151,7 +151,6 @@ struct dspsr_b200_convolution
     ConvTables t;
     t.tw2 = tw2.ptr;
     t.tw4 = tw4.ptr;
-    t.ptab = ptab.ptr;
     t.H = H.ptr;
     t.lut = lut.ptr;
     t.err = err.ptr;
@@ -167,7 +166,6 @@ struct dspsr_b200_convolution
     apod.release ();
     tw2.release ();
     tw4.release ();
-    ptab.release ();
     H.release ();
     tmp.release ();
     scratch.release ();
@@ -238,12 +236,6 @@ int dspsr_b200_convolution::init (dspsr_b200_context* c, unsigned nchan, unsigne
     std::vector<float2> t4 = make_tw4 (shape.n1, shape.n2);
     B200_CHECK (ctx, cudaMemcpy (tw4.ptr, t4.data (), t4.size () * sizeof (float2),
                                  cudaMemcpyHostToDevice), "copy tw4");
-    const unsigned ntab = pass_tables_count (shape.n2);
-    std::vector<float2> pt (ntab);
-    make_pass_tables (shape.n2, pt.data (), ntab);
-    B200_CHECK (ctx, ptab.reserve (ntab), "cudaMalloc pass tables");
-    B200_CHECK (ctx, cudaMemcpy (ptab.ptr, pt.data (), ntab * sizeof (float2),
-                                 cudaMemcpyHostToDevice), "copy pass tables");
     B200_CHECK (ctx, err.reserve (1), "cudaMalloc status flag");
     B200_CHECK (ctx, cudaMemset (err.ptr, 0, sizeof (int)), "clear status flag");
     int dev = 0;
@@ -257,7 +249,9 @@ int dspsr_b200_convolution::init (dspsr_b200_context* c, unsigned nchan, unsigne
     const uint64_t budget = scratch_bytes ? scratch_bytes : (uint64_t (512) << 20);
     const uint64_t bmax = std::max<uint64_t> (1, std::min<uint64_t> (65535, budget / per_part));
     const uint64_t rows_per_part = uint64_t (shape.n1) * nchan * npol;
-    const uint64_t ctas = uint64_t (nsm) * (shape.n2 >= 8192 ? 1 : 2);
+    // (a multiple of the SM count, so also even for the tensor-core rows'
+    // one CTA per SM)
+    const uint64_t ctas = uint64_t (nsm) * b200::rows_ctas_per_sm (shape.n2);
     max_batch = unsigned (bmax);
     for (uint64_t b = bmax; b >= std::max<uint64_t> (1, bmax / 2); b--)
       if ((b * rows_per_part) % ctas == 0)
@@ -1240,7 +1234,7 @@ struct dspsr_b200_inverse_filterbank
   IfbShape shape {};
   unsigned in_discard_pos = 0, in_discard_neg = 0;
   DevBuf<int4> map;
-  DevBuf<float2> tw_lin, tw4, ptab, response, scratch;
+  DevBuf<float2> tw_lin, tw4, response, scratch;
   DevBuf<float> temporal, spectral;
   DevBuf<int> err;
   bool have_response = false, have_temporal = false, have_spectral = false;
@@ -1254,7 +1248,6 @@ struct dspsr_b200_inverse_filterbank
     t.map = map.ptr;
     t.ptab_lin = tw_lin.ptr;
     t.tw4 = tw4.ptr;
-    t.ptab = ptab.ptr;
     t.response = have_response ? response.ptr : nullptr;
     t.temporal = have_temporal ? temporal.ptr : nullptr;
     t.spectral = have_spectral ? spectral.ptr : nullptr;
@@ -1268,7 +1261,6 @@ struct dspsr_b200_inverse_filterbank
     map.release ();
     tw_lin.release ();
     tw4.release ();
-    ptab.release ();
     response.release ();
     scratch.release ();
     temporal.release ();
@@ -1439,12 +1431,6 @@ int dspsr_b200_inverse_filterbank::init (dspsr_b200_context* c, const dspsr_b200
   B200_CHECK (ctx, tw4.reserve (lout), "cudaMalloc four-step twiddles");
   B200_CHECK (ctx, cudaMemcpy (tw4.ptr, t.data (), lout * sizeof (float2),
                                cudaMemcpyHostToDevice), "copy four-step twiddles");
-  const unsigned ntab = pass_tables_count (n2);
-  t.assign (ntab, make_float2 (0.f, 0.f));
-  make_pass_tables (n2, t.data (), ntab);
-  B200_CHECK (ctx, ptab.reserve (ntab), "cudaMalloc pass tables");
-  B200_CHECK (ctx, cudaMemcpy (ptab.ptr, t.data (), ntab * sizeof (float2),
-                               cudaMemcpyHostToDevice), "copy pass tables");
   B200_CHECK (ctx, err.reserve (1), "cudaMalloc status flag");
   B200_CHECK (ctx, cudaMemset (err.ptr, 0, sizeof (int)), "clear status flag");
   int dev = 0;

@@ -11,6 +11,7 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <math.h>
 
 #define B200_HD __host__ __device__ __forceinline__
 #define B200_CE __host__ __device__ constexpr
@@ -381,6 +382,156 @@ struct StockhamPassT
       for (int r = 0; r < R; r++)
         s[PADO ? spad (idxD + r * Ns) : idxD + r * Ns] = x[r];
     }
+  }
+};
+
+// Rows of N2 = 4096 or 8192 points run by T = N2 / 32 threads holding 32
+// values each, in three passes: radix 16 (Ns 1), radix N2 / 256 (Ns 16),
+// radix 16 (Ns N2 / 16).  The last pass leaves in thread tid the values
+// X[j + r N2/16] (j = tid + b T, b < 2, r < 16), exactly what the first pass
+// of a following transform needs in that thread, so a response multiply and
+// the next transform's first pass follow in registers.  Pass 0 reads its
+// input in natural order from anywhere (global memory); passes 1 and 2 go
+// through one padded shared-memory row.  Twiddles: pass 1 from a table
+// w_{16 R1}^{a r} [r-1][a]; pass 2 (a < N2/16) as the product of
+// w_N2^{32 ah r} [r-1][ah] and w_N2^{al r} [r-1][al], a = 32 ah + al.
+template <int N2>
+struct Row32
+{
+  static_assert (N2 == 4096 || N2 == 8192, "Row32 covers 4096- and 8192-point rows");
+  static constexpr int T = N2 / 32;        // threads
+  static constexpr int R1 = N2 / 256;      // radix of pass 1
+  static constexpr int B1 = 256 / T;       // butterflies per thread in pass 1
+  static constexpr int NS2 = N2 / 16;      // Ns of pass 2 (and the stride of pass 0's inputs)
+  static constexpr int AH = NS2 / 32;      // high digits of a pass-2 twiddle index
+  static constexpr int TAB1 = (R1 - 1) * 16;
+  static constexpr int TABH = 15 * AH;
+  static constexpr int TABL = 15 * 32;
+  static constexpr int TABN = TAB1 + TABH + TABL;
+
+  // entry i of the concatenated tables (pass 1, pass-2 high, pass-2 low), as
+  // w^m = exp(-2 pi i m / n) rounded from double
+  B200_HD static float2 table_entry (int i)
+  {
+    int m, n;
+    if (i < TAB1)
+    {
+      m = (i % 16) * (i / 16 + 1);
+      n = 16 * R1;
+    }
+    else if (i < TAB1 + TABH)
+    {
+      i -= TAB1;
+      m = 32 * (i % AH) * (i / AH + 1);
+      n = N2;
+    }
+    else
+    {
+      i -= TAB1 + TABH;
+      m = (i % 32) * (i / 32 + 1);
+      n = N2;
+    }
+    m %= n;
+    double sn, cs;
+#ifdef __CUDA_ARCH__
+    sincospi (2.0 * double (m) / double (n), &sn, &cs);
+#else
+    const double ang = 2.0 * 3.14159265358979323846 * double (m) / double (n);
+    sn = sin (ang);
+    cs = cos (ang);
+#endif
+    return make_float2 (float (cs), float (-sn));
+  }
+
+  // pass 0 input: v[16 b + r] = x[j + r NS2]
+  B200_HD static void p0_load (int tid, const float2* x, float2* v)
+  {
+#pragma unroll
+    for (int b = 0; b < 2; b++)
+#pragma unroll
+      for (int r = 0; r < 16; r++) v[16 * b + r] = x[tid + b * T + r * NS2];
+  }
+
+  // pass 0 (or the first pass of a transform whose input the previous pass 2
+  // left in registers): 16-point DFTs, outputs to s[j 16 + r]
+  template <int D>
+  B200_HD static void p0_compute_store (int tid, float2* v, float2* s)
+  {
+#pragma unroll
+    for (int b = 0; b < 2; b++)
+    {
+      const int j = tid + b * T;
+      RegDFT<16, D>::run (v + 16 * b);
+#pragma unroll
+      for (int r = 0; r < 16; r++) s[spad (j * 16 + r)] = v[16 * b + r];
+    }
+  }
+
+  B200_HD static void p1_load (int tid, const float2* s, float2* v)
+  {
+#pragma unroll
+    for (int b = 0; b < B1; b++)
+#pragma unroll
+      for (int r = 0; r < R1; r++) v[b * R1 + r] = s[spad (tid + b * T + r * 256)];
+  }
+
+  template <int D>
+  B200_HD static void p1_compute_store (int tid, float2* v, float2* s, const float2* tab1)
+  {
+#pragma unroll
+    for (int b = 0; b < B1; b++)
+    {
+      const int j = tid + b * T;
+      const int a = j & 15;
+      float2* x = v + b * R1;
+#pragma unroll
+      for (int r = 1; r < R1; r++)
+      {
+        const float2 w = tab1[(r - 1) * 16 + a];
+        x[r] = D < 0 ? cmul (x[r], w) : cmulc (x[r], w);
+      }
+      RegDFT<R1, D>::run (x);
+      const int o = (j - a) * R1 + a;
+#pragma unroll
+      for (int r = 0; r < R1; r++) s[spad (o + r * 16)] = x[r];
+    }
+  }
+
+  B200_HD static void p2_load (int tid, const float2* s, float2* v)
+  {
+#pragma unroll
+    for (int b = 0; b < 2; b++)
+#pragma unroll
+      for (int r = 0; r < 16; r++) v[16 * b + r] = s[spad (tid + b * T + r * NS2)];
+  }
+
+  // pass 2 in registers: afterwards v[16 b + r] = X[j + r NS2]
+  template <int D>
+  B200_HD static void p2_compute (int tid, float2* v, const float2* th, const float2* tl)
+  {
+#pragma unroll
+    for (int b = 0; b < 2; b++)
+    {
+      const int a = tid + b * T;            // < NS2: j itself
+      const int ah = a >> 5, al = a & 31;
+      float2* x = v + 16 * b;
+#pragma unroll
+      for (int r = 1; r < 16; r++)
+      {
+        const float2 w = cmul (th[(r - 1) * AH + ah], tl[(r - 1) * 32 + al]);
+        x[r] = D < 0 ? cmul (x[r], w) : cmulc (x[r], w);
+      }
+      RegDFT<16, D>::run (x);
+    }
+  }
+
+  // natural-order output of pass 2
+  B200_HD static void p2_store (int tid, const float2* v, float2* x)
+  {
+#pragma unroll
+    for (int b = 0; b < 2; b++)
+#pragma unroll
+      for (int r = 0; r < 16; r++) x[tid + b * T + r * NS2] = v[16 * b + r];
   }
 };
 

@@ -548,70 +548,9 @@ k_fwd_cols_fb64 (const InputView in, const float* __restrict__ lut, const uint64
 }
 
 // --------------------------------------------------------------------------
-// K2 (persistent): one CTA per SM walks the rows.  The next row is fetched
-// into a staging buffer by the bulk-copy engine (cp.async.bulk, completion on
-// an mbarrier) while the current row is transformed; the per-pass twiddle
-// tables stay resident in shared memory.  Row r holds n2 contiguous values,
+// K2 (persistent): the rows.  Row r holds n2 contiguous values,
 // r = ((b*nchan + c)*npol + p)*n1 + k1.
 // --------------------------------------------------------------------------
-
-__device__ __forceinline__ uint32_t smem_u32 (const void* p)
-{
-  return static_cast<uint32_t> (__cvta_generic_to_shared (p));
-}
-
-__device__ __forceinline__ void mbar_init (uint64_t* bar, unsigned count)
-{
-  asm volatile ("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32 (bar)), "r"(count)
-                : "memory");
-  asm volatile ("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx (uint64_t* bar, unsigned bytes)
-{
-  asm volatile ("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32 (bar)),
-                "r"(bytes)
-                : "memory");
-}
-
-// global -> shared bulk copy (16-byte aligned, multiple of 16 bytes),
-// completing `bytes` transactions on the mbarrier; no multicast
-__device__ __forceinline__ void bulk_g2s (void* dst, const void* src, unsigned bytes,
-                                          uint64_t* bar)
-{
-  asm volatile (
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-          "r"(smem_u32 (dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32 (bar))
-      : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait (uint64_t* bar, unsigned parity)
-{
-  uint32_t ok;
-  asm volatile (
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_u32 (bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait: gives up after ~2^21 polls (about a second) and reports it.
-__device__ __forceinline__ bool mbar_wait_bounded (uint64_t* bar, unsigned parity)
-{
-  for (int it = 0; it < (1 << 21); it++)
-    if (mbar_try_wait (bar, parity)) return true;
-  return false;
-}
-
-template <int N>
-constexpr size_t rows_smem_bytes ()
-{
-  return size_t (N + spad_size (N) + pass_tables_size (N)) * sizeof (float2);
-}
 
 template <int N, int D, int P, bool PI, bool PO>
 __device__ __forceinline__ void tpass (const float2* src, float2* dst, float2* v,
@@ -630,134 +569,102 @@ __device__ __forceinline__ void tpass (const float2* src, float2* dst, float2* v
   }
 }
 
-// CONV: the convolution row (forward FFT, x H, inverse FFT).  Otherwise the
-// inverse FFT of the row alone (the inverse filterbank's stitched spectra).
-template <int N2, bool CONV>
-__global__ void __launch_bounds__ (stockham_threads (N2), 1)
-k_rows_tma (float2* __restrict__ scratch, const float2* __restrict__ ptab,
-            const float2* __restrict__ H, const unsigned n1, const unsigned nchan,
-            const unsigned npol, const unsigned nrows, int* __restrict__ err)
+// L2 prefetch of a global range (16-byte aligned, multiple of 16 bytes)
+__device__ __forceinline__ void prefetch_l2 (const void* p, unsigned bytes)
 {
-  constexpr int T = stockham_threads (N2);
-  constexpr int NP = stockham_npass (N2);
-  constexpr int TABN = pass_tables_size (N2);
+  asm volatile ("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+template <int N2>
+constexpr size_t rows32_smem_bytes ()
+{
+  return size_t (spad_size (N2) + Row32<N2>::TABN) * sizeof (float2);
+}
+
+// CTAs of k_rows32 resident per SM: at 8192 shared memory (one padded row +
+// 10 KB of twiddles) and 128 registers per thread allow two; at 4096 three
+// (four would cap the registers at 128, where the 4096-point schedule spills)
+template <int N2>
+constexpr unsigned rows32_ctas_per_sm ()
+{
+  return N2 == 8192 ? 2u : 3u;
+}
+
+// The convolution row (CONV: forward FFT, x H, inverse FFT; otherwise the
+// inverse FFT alone, for the inverse filterbank's stitched spectra) with 32
+// points per thread in three radix passes each way (Row32): pass 0 reads the
+// row straight from the scratch in natural order, the forward pass 2, the
+// response multiply and the inverse pass 0 run in registers, the last pass
+// writes the row back in natural order.  One padded row of shared memory per
+// CTA, used in place; several CTAs per SM overlap one another's
+// barrier-separated phases.  The next row (and its response) is prefetched
+// into L2 while this one is transformed.
+template <int N2, bool CONV>
+__global__ void __launch_bounds__ (Row32<N2>::T, rows32_ctas_per_sm<N2> ())
+k_rows32 (float2* scratch, const float2* __restrict__ H, const unsigned n1,
+          const unsigned nchan, const unsigned npol, const unsigned nrows)
+{
+  using RS = Row32<N2>;
   constexpr unsigned ROW_BYTES = N2 * sizeof (float2);
   constexpr unsigned CHUNK = 16384;
-  static_assert (NP == 3 || NP == 4, "row kernel supports 3 or 4 Stockham passes");
-  extern __shared__ __align__ (128) unsigned char smraw[];
-  float2* stage = reinterpret_cast<float2*> (smraw);
-  float2* work = stage + N2;
-  float2* tab = work + spad_size (N2);
-  __shared__ __align__ (8) uint64_t bar;
+  extern __shared__ __align__ (16) float2 s_row32[];
+  float2* work = s_row32;
+  float2* tab1 = work + spad_size (N2);
+  float2* th = tab1 + RS::TAB1;
+  float2* tl = th + RS::TABH;
   const int tid = threadIdx.x;
+  for (int i = tid; i < RS::TABN; i += RS::T) tab1[i] = RS::table_entry (i);
 
-  for (int i = tid; i < TABN; i += T) tab[i] = __ldg (ptab + i);
-  if (tid == 0) mbar_init (&bar, 1);
-  __syncthreads ();
-
-  unsigned row = blockIdx.x;
-  if (tid == 0 && row < nrows)
+  float2 v[32];
+  for (unsigned row = blockIdx.x; row < nrows; row += gridDim.x)
   {
-    mbar_expect_tx (&bar, ROW_BYTES);
-    const char* src = reinterpret_cast<const char*> (scratch + uint64_t (row) * N2);
-    for (unsigned o = 0; o < ROW_BYTES; o += CHUNK)
-      bulk_g2s (reinterpret_cast<char*> (stage) + o, src + o, CHUNK, &bar);
-  }
-  unsigned parity = 0;
-  float2 v[16];
-  for (; row < nrows; row += gridDim.x)
-  {
-    // every thread polls the barrier (bounded); whether to give up is decided
-    // for the whole block at the barrier below, before anyone returns
-    const bool landed = mbar_wait_bounded (&bar, parity);
-    parity ^= 1;
-    const unsigned k1 = row % n1;
-    const unsigned c = (row / n1 / npol) % nchan;
     float2* grow = scratch + uint64_t (row) * N2;
-
-    // pass 0 reads the staged row; once every thread has its values the
-    // staging buffer is refilled with the next row in the background
+    const unsigned next = row + gridDim.x;
+    if (tid == 0 && next < nrows)
     {
-      constexpr int R0 = stockham_radix (N2, 0);
-      constexpr int D0 = CONV ? -1 : +1;
-      // (a thread whose wait gave up reads stale shared memory here; its
-      // values are dropped with the block's return below)
-      StockhamPassT<N2, R0, T, D0, false, true>::load (tid, stage, v);
-      if (__syncthreads_or (!landed))
+      const char* nr = reinterpret_cast<const char*> (scratch + uint64_t (next) * N2);
+      for (unsigned o = 0; o < ROW_BYTES; o += CHUNK) prefetch_l2 (nr + o, CHUNK);
+      if constexpr (CONV)
       {
-        if (tid == 0)
-        {
-          atomicExch (err, 1);
-          mbar_wait_bounded (&bar, parity ^ 1);   // let the copy in flight land
-        }
-        return;
+        const char* nh = reinterpret_cast<const char*> (
+            H + (uint64_t ((next / n1 / npol) % nchan) * n1 + next % n1) * N2);
+        for (unsigned o = 0; o < ROW_BYTES; o += CHUNK) prefetch_l2 (nh + o, CHUNK);
       }
-      const unsigned next = row + gridDim.x;
-      if (tid == 0 && next < nrows)
-      {
-        mbar_expect_tx (&bar, ROW_BYTES);
-        const char* src = reinterpret_cast<const char*> (scratch + uint64_t (next) * N2);
-        for (unsigned o = 0; o < ROW_BYTES; o += CHUNK)
-          bulk_g2s (reinterpret_cast<char*> (stage) + o, src + o, CHUNK, &bar);
-      }
-      StockhamPassT<N2, R0, T, D0, false, true>::compute_store (tid, 1, v, work, nullptr);
-      __syncthreads ();
     }
+    RS::p0_load (tid, grow, v);
+    __syncthreads ();     // the previous row's last shared-memory reads are done
     if constexpr (CONV)
     {
-      // forward passes but the last
-      tpass<N2, -1, 1, true, true> (work, work, v, tab);
-      if constexpr (NP == 4) tpass<N2, -1, 2, true, true> (work, work, v, tab);
-      // The last forward pass leaves in thread tid exactly the 16 values that
-      // the first inverse pass needs in that thread (x[tid + m T], m < 16), so
-      // the response multiply and the inverse pass-0 butterfly follow in
-      // registers, with no shared-memory round trip between them.
-      constexpr int PL = NP - 1;
-      constexpr int RL = stockham_radix (N2, PL);
-      constexpr int NsL = stockham_ns (N2, PL);
-      constexpr int BPT = (N2 / RL) / T;
-      StockhamPassT<N2, RL, T, -1, true, true>::load (tid, work, v);
+      RS::template p0_compute_store<-1> (tid, v, work);
       __syncthreads ();
-      const float2* twp = tab + pass_table_offset (N2, PL);
-#pragma unroll
-      for (int bb = 0; bb < BPT; bb++)
-      {
-        const int j = tid + bb * T;
-        const int a = j & (NsL - 1);
-        float2* x = v + bb * RL;
-#pragma unroll
-        for (int r = 1; r < RL; r++) x[r] = cmul (x[r], twp[(r - 1) * NsL + a]);
-        RegDFT<RL, -1>::run (x);
-      }
+      RS::p1_load (tid, work, v);
+      __syncthreads ();
+      RS::template p1_compute_store<-1> (tid, v, work, tab1);
+      __syncthreads ();
+      RS::p2_load (tid, work, v);
+      __syncthreads ();
+      RS::template p2_compute<-1> (tid, v, th, tl);
       // Response::operate (Response.C:662-726): (f_r d_r - f_i d_i, f_i d_r + f_r d_i)
-      const float2* h = H + (uint64_t (c) * n1 + k1) * N2;
-      float2 u[16];
+      const float2* h = H + (uint64_t ((row / n1 / npol) % nchan) * n1 + row % n1) * N2;
 #pragma unroll
-      for (int bb = 0; bb < BPT; bb++)
+      for (int b = 0; b < 2; b++)
 #pragma unroll
-        for (int r = 0; r < RL; r++)
+        for (int r = 0; r < 16; r++)
         {
-          const int m = bb + r * (16 / RL);
-          const float2 d = v[bb * RL + r];
-          const float2 f = __ldg (h + tid + m * T);
-          u[m] = make_float2 (d.x * f.x - d.y * f.y, d.x * f.y + d.y * f.x);
+          const float2 d = v[16 * b + r];
+          const float2 f = __ldg (h + tid + b * RS::T + r * RS::NS2);
+          v[16 * b + r] = make_float2 (d.x * f.x - d.y * f.y, d.x * f.y + d.y * f.x);
         }
-      static_assert (stockham_radix (N2, 0) == 16, "inverse pass 0 must be radix 16");
-      RegDFT<16, +1>::run (u);
-#pragma unroll
-      for (int r = 0; r < 16; r++) work[spad (tid * 16 + r)] = u[r];
-      __syncthreads ();
     }
-
-    // inverse: all but the last pass in shared memory, the last straight to HBM
-    tpass<N2, +1, 1, true, true> (work, work, v, tab);
-    if constexpr (NP == 3)
-      tpass<N2, +1, 2, true, false> (work, grow, v, tab);
-    else
-    {
-      tpass<N2, +1, 2, true, true> (work, work, v, tab);
-      tpass<N2, +1, 3, true, false> (work, grow, v, tab);
-    }
+    RS::template p0_compute_store<+1> (tid, v, work);
+    __syncthreads ();
+    RS::p1_load (tid, work, v);
+    __syncthreads ();
+    RS::template p1_compute_store<+1> (tid, v, work, tab1);
+    __syncthreads ();
+    RS::p2_load (tid, work, v);
+    RS::template p2_compute<+1> (tid, v, th, tl);
+    RS::p2_store (tid, v, grow);
   }
 }
 
@@ -2285,18 +2192,15 @@ template <int N2>
 void launch_rows (unsigned nrows, float2* scratch, const ConvTables& tb, unsigned n1,
                   const ConvShape& sh, cudaStream_t st)
 {
-  constexpr int T = stockham_threads (N2);
-  // persistent: as many CTAs as fit at once (shared memory allows 1 per SM at
-  // n2 = 8192 and 2 at n2 = 4096)
-  const unsigned per_sm = N2 >= 8192 ? 1 : 2;
-  const unsigned grid = std::min<unsigned> (nrows, per_sm * unsigned (tb.nsm));
   if (N2 == 8192 && tb.tc_splits)
   {
     launch_rows_mma (nrows, scratch, tb, n1, sh, st);
     return;
   }
-  k_rows_tma<N2, true><<<grid, T, rows_smem_bytes<N2> (), st>>> (scratch, tb.ptab, tb.H, n1,
-                                                                 sh.nchan, sh.npol, nrows, tb.err);
+  // persistent: as many CTAs as are resident at once
+  const unsigned grid = std::min<unsigned> (nrows, rows_ctas_per_sm (N2) * unsigned (tb.nsm));
+  k_rows32<N2, true><<<grid, Row32<N2>::T, rows32_smem_bytes<N2> (), st>>> (
+      scratch, tb.H, n1, sh.nchan, sh.npol, nrows);
 }
 
 template <int N1>
@@ -2450,23 +2354,26 @@ template <int N2>
 void launch_rows_inv (unsigned nrows, float2* scratch, const IfbTables& tb, unsigned n1,
                       unsigned npol, cudaStream_t st)
 {
-  constexpr int T = stockham_threads (N2);
-  const unsigned per_sm = N2 >= 8192 ? 1 : 2;
-  const unsigned grid = std::min<unsigned> (nrows, per_sm * unsigned (tb.nsm));
-  k_rows_tma<N2, false><<<grid, T, rows_smem_bytes<N2> (), st>>> (scratch, tb.ptab, nullptr, n1,
-                                                                  1, npol, nrows, tb.err);
+  const unsigned grid = std::min<unsigned> (nrows, rows_ctas_per_sm (N2) * unsigned (tb.nsm));
+  k_rows32<N2, false><<<grid, Row32<N2>::T, rows32_smem_bytes<N2> (), st>>> (
+      scratch, nullptr, n1, 1, npol, nrows);
 }
 
-template <int N2, bool CONV = true>
+template <int N2, bool CONV>
 cudaError_t set_rows_smem ()
 {
-  return cudaFuncSetAttribute (k_rows_tma<N2, CONV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               int (rows_smem_bytes<N2> ()));
+  return cudaFuncSetAttribute (k_rows32<N2, CONV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int (rows32_smem_bytes<N2> ()));
 }
 
 } // namespace
 
 uint64_t kernel_launches () { return g_launches.load (); }
+
+unsigned rows_ctas_per_sm (unsigned n2)
+{
+  return n2 == 8192 ? rows32_ctas_per_sm<8192> () : rows32_ctas_per_sm<4096> ();
+}
 
 unsigned pass_tables_count (unsigned n)
 {
@@ -2513,8 +2420,8 @@ cudaError_t convolution_kernel_setup ()
   if (e != cudaSuccess) return e;
   const unsigned bit = dev < 32 ? 1u << dev : 0u;    // devices past 32: set every time
   if (bit && (attr_done.load () & bit)) return cudaSuccess;
-  e = set_rows_smem<8192> ();
-  if (e == cudaSuccess) e = set_rows_smem<4096> ();
+  e = set_rows_smem<8192, true> ();
+  if (e == cudaSuccess) e = set_rows_smem<4096, true> ();
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute (k_fwd_cols_fb64<IN_INT8, false>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize, int (FBC_SMEM));

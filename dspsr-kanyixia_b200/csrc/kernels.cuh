@@ -74,10 +74,9 @@ struct ConvTables
 {
   const float2* tw2 = nullptr;   // n2-point table exp(-2 pi i m / n2)
   const float2* tw4 = nullptr;   // [n1][n2] exp(-2 pi i k1 n2 / nfft), null when n1 == 1
-  const float2* ptab = nullptr;  // per-pass Stockham twiddle tables of the n2-point FFT
   const float2* H = nullptr;     // [nchan][n1][n2] response in four-step order
   const float* lut = nullptr;    // 8-bit lookup table (device), 256 floats
-  int* err = nullptr;            // device flag: set when a bounded wait gave up
+  int* err = nullptr;            // device flag: set when a bounded wait (tensor-core rows) gave up
   int nsm = 0;                   // multiprocessors of the device
   const float* apod = nullptr;   // temporal window [nfft] applied to each part, or null
   // tensor-core row FFT: the DFT16/DFT32 operand image (make_tc_dft_image)
@@ -115,6 +114,10 @@ struct KernelClock
 
 // Number of kernels this library has launched since it was loaded.
 uint64_t kernel_launches ();
+
+// CTAs of the FP32 convolution row kernel resident per SM for n2-point rows
+// (the persistent grid is this times the SM count)
+unsigned rows_ctas_per_sm (unsigned n2);
 
 // SpectralKurtosis engine steps on their own: the test of sums already formed
 // (detect_skfb) and the mask applied to voltages (out == in: in place).
@@ -215,7 +218,6 @@ struct IfbTables
   const int4* map;
   const float2* ptab_lin;    // per-pass Stockham tables of the lin-point transform
   const float2* tw4;         // [n1][n2] four-step table of the lout-point transform
-  const float2* ptab;        // per-pass tables of the n2-point row transform
   const float2* response;    // [nout][lout] or null
   const float* temporal;     // [lin] or null
   const float* spectral;     // [lout] or null

@@ -69,23 +69,6 @@ __global__ void k_tw4 (float2* tw4, unsigned n1, unsigned n2)
   tw4[idx] = make_float2 (float (c), float (s));
 }
 
-// per-pass Stockham tables of the n2-point transform (fft_core.cuh layout)
-template <int N>
-__global__ void k_ptab (float2* tab)
-{
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= pass_tables_size (N)) return;
-  int p = 1;
-  while (p + 1 < stockham_npass (N) && idx >= pass_table_offset (N, p + 1)) p++;
-  const int Ns = stockham_ns (N, p);
-  const int off = idx - pass_table_offset (N, p);
-  const int r = off / Ns + 1, a = off % Ns;
-  const int R = stockham_radix (N, p);
-  double s, c;
-  sincospi (-2.0 * double (a) * r / (double (Ns) * R), &s, &c);
-  tab[idx] = make_float2 (float (c), float (s));
-}
-
 // Device address of the static array for the current device (set-up once per
 // device: cudaGetSymbolAddress, checked), plus its multiprocessor count.
 cudaError_t scratch_for_device (void** ptr, int* nsm)
@@ -147,12 +130,11 @@ extern "C" int dspsr_b200_convolution_perform_noalloc (
   if (ndat >= nfft) npart = (ndat - nfilt_pos - nfilt_neg) / sh.nkeep;
   if (out_span < npart * sh.nkeep) return DSPSR_B200_EINVAL;
 
-  // layout of the static array: status flag, n2-point table, pass tables,
-  // then (four-step only) the [n1][n2] twiddles, the response in four-step
-  // order and the FFT scratch of as many parts as fit
+  // layout of the static array: status flag, n2-point table, then (four-step
+  // only) the [n1][n2] twiddles, the response in four-step order and the FFT
+  // scratch of as many parts as fit
   const uint64_t off_tw2 = 256;
-  const uint64_t off_ptab = off_tw2 + align256 (uint64_t (sh.n2) * sizeof (float2));
-  const uint64_t off_tw4 = off_ptab + align256 (uint64_t (pass_tables_count (8192)) * sizeof (float2));
+  const uint64_t off_tw4 = off_tw2 + align256 (uint64_t (sh.n2) * sizeof (float2));
   uint64_t off_H = off_tw4, off_scratch = off_tw4;
   uint64_t nbatch = 65535;
   if (sh.n1 > 1)
@@ -162,12 +144,12 @@ extern "C" int dspsr_b200_convolution_perform_noalloc (
     const uint64_t per_part = uint64_t (nchan) * npol * nfft * sizeof (float2);
     if (off_scratch + per_part > SCRATCH_BYTES) return DSPSR_B200_ETOOBIG;
     // as many parts as fit, reduced (down to half) to a batch whose rows
-    // spread evenly over the persistent row kernel's one CTA per SM
+    // spread evenly over the persistent row kernel's CTAs
     const uint64_t bmax = std::min<uint64_t> (65535, (SCRATCH_BYTES - off_scratch) / per_part);
     const uint64_t rows_per_part = uint64_t (sh.n1) * nchan * npol;
     nbatch = bmax;
     for (uint64_t b = bmax; b >= std::max<uint64_t> (1, bmax / 2); b--)
-      if ((b * rows_per_part) % uint64_t (nsm) == 0)
+      if ((b * rows_per_part) % (uint64_t (nsm) * rows_ctas_per_sm (sh.n2)) == 0)
       {
         nbatch = b;
         break;
@@ -176,14 +158,14 @@ extern "C" int dspsr_b200_convolution_perform_noalloc (
 
   cudaStream_t st = static_cast<cudaStream_t> (stream);
   unsigned char* b = static_cast<unsigned char*> (base);
-  // the row kernel's give-up flag: the caller's int when given, else a word
-  // of the array; either way it starts every call at zero
+  // the status word: the caller's int when given, else a word of the array;
+  // either way it starts every call at zero, and the FP32 kernels this call
+  // runs have no device-side waits that could set it
   int* err = d_status ? d_status : reinterpret_cast<int*> (b);
   if (cudaMemsetAsync (err, 0, sizeof (int), st) != cudaSuccess) return DSPSR_B200_ECUDA;
   if (npart == 0) return DSPSR_B200_OK;
 
   float2* tw2 = reinterpret_cast<float2*> (b + off_tw2);
-  float2* ptab = reinterpret_cast<float2*> (b + off_ptab);
   float2* tw4 = reinterpret_cast<float2*> (b + off_tw4);
   float2* H = reinterpret_cast<float2*> (b + off_H);
   float2* scratch = reinterpret_cast<float2*> (b + off_scratch);
@@ -197,13 +179,11 @@ extern "C" int dspsr_b200_convolution_perform_noalloc (
   tb.lut = nullptr;
   if (sh.n1 > 1)
   {
-    k_ptab<8192><<<(pass_tables_size (8192) + 255) / 256, 256, 0, st>>> (ptab);
     k_tw4<<<unsigned ((uint64_t (nfft) + 255) / 256), 256, 0, st>>> (tw4, sh.n1, sh.n2);
     if (launch_permute_response (H, reinterpret_cast<const float2*> (d_response), nchan, sh.n1,
                                  sh.n2, st) != cudaSuccess)
       return DSPSR_B200_ECUDA;
     tb.tw4 = tw4;
-    tb.ptab = ptab;
     tb.H = H;
   }
   else

@@ -4,7 +4,7 @@
 // It replaces the cuFFT C2C plans of the reference's convolution engine
 // (Signal/General/ConvolutionCUDA.cu:370-413, the batched forward and
 // backward plans around the response multiply) for the row half of the
-// four-step split, as a drop-in for k_rows_tma<8192, true>: the same row of
+// four-step split, as a drop-in for k_rows32<8192, true>: the same row of
 // the scratch in (natural order), the same row out, the response row of
 // (channel, k1) in between.
 //

@@ -227,9 +227,10 @@ int dspsr_b200_convolution_set_dedispersion_channels (dspsr_b200_convolution* co
    whatever its shape (make that call before any stream capture).  All calls
    share the one array and leave their contents in it: calls whose work
    overlaps on the GPU race.  d_status (device memory, may be NULL) is set to
-   0 in stream order at the start of the call and to 1 if one of the row
-   kernel's bounded device-side waits gave up, in which case the output is
-   not valid; read it once the stream has passed the call.  Returns the
+   0 in stream order at the start of the call; a kernel with a bounded
+   device-side wait would set it to 1 when the wait gave up (the output then
+   not valid), but the FP32 kernels this call runs have none, so it reads 0
+   once the stream has passed the call.  Returns the
    launch status; *npart as for dspsr_b200_convolution_perform. */
 #define DSPSR_B200_NOALLOC_SCRATCH_BYTES (32ull << 20)
 int dspsr_b200_convolution_perform_noalloc (void* stream, const float* d_in, uint64_t in_span,
@@ -239,8 +240,9 @@ int dspsr_b200_convolution_perform_noalloc (void* stream, const float* d_in, uin
                                             float* d_out, uint64_t out_span, uint64_t* npart,
                                             int* d_status);
 /* Blocks until the engine's queued work is done and returns DSPSR_B200_ESTATE
-   if one of its device-side waits gave up (each wait is bounded to about a
-   second; see the row kernel), DSPSR_B200_OK otherwise. */
+   if one of its device-side waits gave up (the tensor-core rows' mbarrier
+   waits, each bounded to about a second; the FP32 kernels have none),
+   DSPSR_B200_OK otherwise. */
 int dspsr_b200_convolution_status (dspsr_b200_convolution* conv);
 /* copies the response (FFT order) back to host memory, nchan*nfft complex */
 int dspsr_b200_convolution_get_response (dspsr_b200_convolution* conv, float* response);
@@ -345,7 +347,10 @@ int dspsr_b200_inverse_filterbank_perform (dspsr_b200_inverse_filterbank* ifb, i
                                            const void* d_in, uint64_t ndat, uint64_t in_span,
                                            const float* lut256, int offset_binary, float* d_out,
                                            uint64_t out_span, uint64_t* npart);
-/* DSPSR_B200_ESTATE when a bounded device wait of the row kernel gave up */
+/* Blocks until the engine's queued work is done; DSPSR_B200_ESTATE would
+   report a device-side wait that gave up, but the inverse filterbank's
+   kernels have none, so it returns DSPSR_B200_OK (kept for callers that
+   check every engine the same way). */
 int dspsr_b200_inverse_filterbank_status (dspsr_b200_inverse_filterbank* ifb);
 
 /* ---------------------------------------------------------------------- */
