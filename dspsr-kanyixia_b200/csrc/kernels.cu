@@ -370,17 +370,26 @@ k_fwd_cols (const InputView in, const float* __restrict__ lut, const uint64_t nk
 // columns) stage their outputs in shared memory and write each scratch row
 // in runs of one 32-byte sector (blocks of two or eight warps measured
 // slower).  Both exchanges swizzle their shared-memory columns against bank
-// conflicts.
+// conflicts.  The staging is column-major with the even and odd rows in two
+// halves (row -> row/2 + (row odd) FBC_SODD, column stride FBC_SP = 2 mod 16):
+// the 16 rows a half-warp stores (two apart) and the 4 x 4 (row, column)
+// pairs it loads for the write-out then fall in 16 distinct bank pairs.
 // --------------------------------------------------------------------------
 
 constexpr int FBC_THREADS = 128;
 constexpr int FBC_COLS = FBC_THREADS / 32;      // columns per block, one per warp
 constexpr int FBC_XSTRIDE = 1056;               // float2 per warp exchange buffer
-constexpr int FBC_SROW = FBC_COLS + 1;          // staging row stride (float2)
+constexpr int FBC_SODD = 520;                   // staging offset of the odd rows (8 mod 16)
+constexpr int FBC_SP = 1042;                    // staging column stride (2 mod 16)
 constexpr size_t FBC_SMEM =
-    (size_t (FBC_SROW) * 1024 > size_t (FBC_COLS) * FBC_XSTRIDE ? size_t (FBC_SROW) * 1024
-                                                                : size_t (FBC_COLS) * FBC_XSTRIDE)
+    (size_t (FBC_SP) * FBC_COLS > size_t (FBC_COLS) * FBC_XSTRIDE ? size_t (FBC_SP) * FBC_COLS
+                                                                  : size_t (FBC_COLS) * FBC_XSTRIDE)
     * sizeof (float2);
+
+__host__ __device__ constexpr int fbc_stage (int row, int col)
+{
+  return col * FBC_SP + (row >> 1) + (row & 1) * FBC_SODD;
+}
 
 // (float(x) + 0.5f) * scale for the two's-complement byte x, bit for bit:
 // 2^22 + (x + 128) has its last mantissa bit worth 0.5, so subtracting
@@ -439,7 +448,7 @@ __device__ __forceinline__ void fetch_raw2 (const InputView& in, const float* s_
 }
 
 template <int KIND, bool AFFINE>
-__global__ void __launch_bounds__ (FBC_THREADS, 512 / FBC_THREADS)
+__global__ void __launch_bounds__ (FBC_THREADS, 640 / FBC_THREADS)
 k_fwd_cols_fb64 (const InputView in, const float* __restrict__ lut, const uint64_t nkeep,
                  const uint64_t part0, const unsigned n2, const float2* __restrict__ tw4,
                  float2* __restrict__ scratch)
@@ -532,7 +541,7 @@ k_fwd_cols_fb64 (const InputView in, const float* __restrict__ lut, const uint64
     {
       float2 o = k1 ? cmul (z[f][k1], tw[k1]) : z[f][k1];
       o = make_float2 (__fmul_rn (o.x, 0.125f), __fmul_rn (o.y, 0.125f));
-      s_fbc[(k1 * 128 + c * 2 + pol) * FBC_SROW + warp] = o;
+      s_fbc[fbc_stage (k1 * 128 + c * 2 + pol, warp)] = o;
     }
   }
   __syncthreads ();
@@ -543,7 +552,7 @@ k_fwd_cols_fb64 (const InputView in, const float* __restrict__ lut, const uint64
     const unsigned row = idx / FBC_COLS, w = idx % FBC_COLS;
     const unsigned k1 = row >> 7, c = (row & 127) >> 1, pol = row & 1;
     scratch[((uint64_t (b) * 64 + c) * 2 + pol) * N + uint64_t (k1) * n2 + i0 + w] =
-        s_fbc[row * FBC_SROW + w];
+        s_fbc[fbc_stage (row, w)];
   }
 }
 
@@ -615,20 +624,32 @@ k_rows32 (float2* scratch, const float2* __restrict__ H, const unsigned n1,
   const int tid = threadIdx.x;
   for (int i = tid; i < RS::TABN; i += RS::T) tab1[i] = RS::table_entry (i);
 
+  // Rows are walked with their response row (channel, k1) outermost and the
+  // parts and polarisations innermost, so that the CTAs working at one time
+  // share few response rows and find them in L2.
+  const unsigned inner = nrows / (n1 * nchan);      // parts x polarisations
+  const auto row_of = [=] (unsigned idx, unsigned& hrow) {
+    hrow = idx / inner;                             // c * n1 + k1
+    const unsigned bp = idx % inner;
+    return ((bp / npol) * nchan * n1 + hrow / n1 * n1) * npol + (bp % npol) * n1 + hrow % n1;
+  };
   float2 v[32];
-  for (unsigned row = blockIdx.x; row < nrows; row += gridDim.x)
+  for (unsigned idx = blockIdx.x; idx < nrows; idx += gridDim.x)
   {
+    unsigned hrow = 0;
+    const unsigned row = CONV ? row_of (idx, hrow) : idx;
     float2* grow = scratch + uint64_t (row) * N2;
-    const unsigned next = row + gridDim.x;
+    const unsigned next = idx + gridDim.x;
     if (tid == 0 && next < nrows)
     {
-      const char* nr = reinterpret_cast<const char*> (scratch + uint64_t (next) * N2);
+      unsigned nh = 0;
+      const unsigned nrow = CONV ? row_of (next, nh) : next;
+      const char* nr = reinterpret_cast<const char*> (scratch + uint64_t (nrow) * N2);
       for (unsigned o = 0; o < ROW_BYTES; o += CHUNK) prefetch_l2 (nr + o, CHUNK);
-      if constexpr (CONV)
+      if (CONV && nh != hrow)
       {
-        const char* nh = reinterpret_cast<const char*> (
-            H + (uint64_t ((next / n1 / npol) % nchan) * n1 + next % n1) * N2);
-        for (unsigned o = 0; o < ROW_BYTES; o += CHUNK) prefetch_l2 (nh + o, CHUNK);
+        const char* hp = reinterpret_cast<const char*> (H + uint64_t (nh) * N2);
+        for (unsigned o = 0; o < ROW_BYTES; o += CHUNK) prefetch_l2 (hp + o, CHUNK);
       }
     }
     RS::p0_load (tid, grow, v);
@@ -645,7 +666,7 @@ k_rows32 (float2* scratch, const float2* __restrict__ H, const unsigned n1,
       __syncthreads ();
       RS::template p2_compute<-1> (tid, v, th, tl);
       // Response::operate (Response.C:662-726): (f_r d_r - f_i d_i, f_i d_r + f_r d_i)
-      const float2* h = H + (uint64_t ((row / n1 / npol) % nchan) * n1 + row % n1) * N2;
+      const float2* h = H + uint64_t (hrow) * N2;
 #pragma unroll
       for (int b = 0; b < 2; b++)
 #pragma unroll
