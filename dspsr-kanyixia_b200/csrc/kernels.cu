@@ -362,15 +362,17 @@ k_fwd_cols (const InputView in, const float* __restrict__ lut, const uint64_t nk
 // polarisations, then each channel's 8-point column DFT.
 //
 // Lane (j, q), j = lane/4, q = lane%4, reads raw samples s = q + 4m (m < 16)
-// of filterbank sample j: a 16-point DFT over m, the twiddle w64^(q k),
-// then, after an exchange inside the quad, 4-point DFTs over q give channel
-// c = 4q + e + 16 kb for e, kb < 4.  A second exchange inside each group of
-// lanes with equal q gathers the eight j of four (channel, pol) pairs per
-// lane for the 8-point DFTs.  The block's four warps (four consecutive
+// of filterbank sample j: a 16-point DFT over m and the twiddle w64^(q ka)
+// give Y[q][ka] (ka < 16).  One transpose through the warp's shared buffer
+// hands lane 2 ka + pol the 32 values Y[q][ka] of every (q, j): 4-point DFTs
+// over q give channels c = ka + 16 kb (kb < 4) of each filterbank sample,
+// and 8-point DFTs over j the four channels' column DFTs, all in registers
+// (64-point DFT as 16 x 4, X[ka + 16 kb] = sum_q w4^(q kb) w64^(q ka)
+// Y[q][ka]).  The block's four warps (four consecutive
 // columns) stage their outputs in shared memory and write each scratch row
 // in runs of one 32-byte sector (blocks of two or eight warps measured
-// slower).  Both exchanges swizzle their shared-memory columns against bank
-// conflicts.  The staging is column-major with the even and odd rows in two
+// slower).  The transpose's rows are 34 float2 apart, so its stores (one row,
+// 32 lanes) and 16-byte loads (32 rows) are free of bank conflicts.  The staging is column-major with the even and odd rows in two
 // halves (row -> row/2 + (row odd) FBC_SODD, column stride FBC_SP = 2 mod 16):
 // the 16 rows a half-warp stores (two apart) and the 4 x 4 (row, column)
 // pairs it loads for the write-out then fall in 16 distinct bank pairs.
@@ -378,7 +380,8 @@ k_fwd_cols (const InputView in, const float* __restrict__ lut, const uint64_t nk
 
 constexpr int FBC_THREADS = 128;
 constexpr int FBC_COLS = FBC_THREADS / 32;      // columns per block, one per warp
-constexpr int FBC_XSTRIDE = 1056;               // float2 per warp exchange buffer
+constexpr int FBC_XROW = 34;                    // exchange row stride (float2; 16-byte reads)
+constexpr int FBC_XSTRIDE = 32 * FBC_XROW;      // float2 per warp exchange buffer
 constexpr int FBC_SODD = 520;                   // staging offset of the odd rows (8 mod 16)
 constexpr int FBC_SP = 1042;                    // staging column stride (2 mod 16)
 constexpr size_t FBC_SMEM =
@@ -453,7 +456,7 @@ k_fwd_cols_fb64 (const InputView in, const float* __restrict__ lut, const uint64
                  const uint64_t part0, const unsigned n2, const float2* __restrict__ tw4,
                  float2* __restrict__ scratch)
 {
-  extern __shared__ float2 s_fbc[];
+  extern __shared__ __align__ (16) float2 s_fbc[];
   __shared__ float s_lut[AFFINE ? 1 : 256];
   __shared__ float2 s_tw64[64];
   if (!AFFINE && in.kind == IN_INT8)
@@ -478,50 +481,40 @@ k_fwd_cols_fb64 (const InputView in, const float* __restrict__ lut, const uint64
     fetch_raw2<KIND, AFFINE> (in, s_lut, t * 64 + q + 4 * m, x0[m], x1[m]);
   RegDFT<16, -1>::run (x0);
   RegDFT<16, -1>::run (x1);
-  // twiddle w64^(q ka), then the quad exchange: column q ^ (ka >> 2)
+  // twiddle w64^(q ka); lane (j, q) then hands Y[q][ka] of both
+  // polarisations to lane 2 ka + pol through the warp's buffer (row 2 ka + pol,
+  // column 4 j + q, rows FBC_XROW float2 apart)
 #pragma unroll
   for (int ka = 0; ka < 16; ka++)
   {
     const float2 w = s_tw64[(q * ka) & 63];
-    const unsigned col = q ^ unsigned (ka >> 2);
-    xb[j * 132 + (0 * 16 + ka) * 4 + col] = cmul (x0[ka], w);
-    xb[j * 132 + (1 * 16 + ka) * 4 + col] = cmul (x1[ka], w);
+    xb[(2 * ka) * FBC_XROW + lane] = cmul (x0[ka], w);
+    xb[(2 * ka + 1) * FBC_XROW + lane] = cmul (x1[ka], w);
   }
   __syncwarp ();
-  // 4-point DFTs over the quad: channel 4q + e + 16 kb
-  float2 y[2][4][4];
+  // lane 2 ka + pol reads its row in 16-byte pairs: z[jj][qq] = Y[qq][ka] of
+  // filterbank sample jj
+  float2 z[8][4];
 #pragma unroll
-  for (int pol = 0; pol < 2; pol++)
+  for (int jj = 0; jj < 8; jj++)
 #pragma unroll
-    for (int e = 0; e < 4; e++)
+    for (int qq = 0; qq < 4; qq += 2)
     {
-#pragma unroll
-      for (int qq = 0; qq < 4; qq++)
-        y[pol][e][qq] = xb[j * 132 + (pol * 16 + 4 * q + e) * 4 + (unsigned (qq) ^ q)];
-      RegDFT<4, -1>::run (y[pol][e]);
+      const float4 t = *reinterpret_cast<const float4*> (xb + lane * FBC_XROW + 4 * jj + qq);
+      z[jj][qq] = make_float2 (t.x, t.y);
+      z[jj][qq + 1] = make_float2 (t.z, t.w);
     }
-  __syncwarp ();
-  // gather the eight j of (channel, pol) pairs v = 4j + f of this quad group:
-  // pair v = pol*16 + e*4 + kb is stored at column j ^ (v >> 2)
+  // 4-point DFTs over q: z[jj][kb] = channel ka + 16 kb of filterbank sample jj
 #pragma unroll
-  for (int pol = 0; pol < 2; pol++)
+  for (int jj = 0; jj < 8; jj++) RegDFT<4, -1>::run (z[jj]);
+  // the column DFTs over the eight filterbank samples, per channel
+  float2 col[4][8];
 #pragma unroll
-    for (int e = 0; e < 4; e++)
-#pragma unroll
-      for (int kb = 0; kb < 4; kb++)
-      {
-        const unsigned v = pol * 16 + e * 4 + kb;
-        xb[q * 260 + v * 8 + (j ^ (v >> 2))] = y[pol][e][kb];
-      }
-  __syncwarp ();
-  float2 z[4][8];
-#pragma unroll
-  for (int f = 0; f < 4; f++)
+  for (int kb = 0; kb < 4; kb++)
   {
 #pragma unroll
-    for (int jj = 0; jj < 8; jj++)
-      z[f][jj] = xb[q * 260 + (4 * j + f) * 8 + (unsigned (jj) ^ j)];
-    RegDFT<8, -1>::run (z[f]);
+    for (int jj = 0; jj < 8; jj++) col[kb][jj] = z[jj][kb];
+    RegDFT<8, -1>::run (col[kb]);
   }
   // four-step twiddle w_N^(k1 n2) of column i2, and the filterbank
   // normaliser 1/sqrt(64) (exact)
@@ -530,18 +523,21 @@ k_fwd_cols_fb64 (const InputView in, const float* __restrict__ lut, const uint64
 #pragma unroll
   for (int k1 = 1; k1 < 8; k1++) tw[k1] = __ldg (tw4 + uint64_t (k1) * n2 + i2);
   __syncthreads ();                    // every warp is done with its exchange buffer
-  // pair f of lane (j, q): channel c = 4q + (j & 3) + 16 f, pol = j >> 2;
-  // staging row k1*128 + c*2 + pol, column = warp
-#pragma unroll
-  for (int f = 0; f < 4; f++)
+  // channel c = ka + 16 kb, pol of lane 2 ka + pol; staging row
+  // k1*128 + c*2 + pol, column = warp
   {
-    const unsigned c = 4 * q + (j & 3) + 16 * f, pol = j >> 2;
+    const unsigned ka = lane >> 1, pol = lane & 1;
 #pragma unroll
-    for (int k1 = 0; k1 < 8; k1++)
+    for (int kb = 0; kb < 4; kb++)
     {
-      float2 o = k1 ? cmul (z[f][k1], tw[k1]) : z[f][k1];
-      o = make_float2 (__fmul_rn (o.x, 0.125f), __fmul_rn (o.y, 0.125f));
-      s_fbc[fbc_stage (k1 * 128 + c * 2 + pol, warp)] = o;
+      const unsigned c = ka + 16 * kb;
+#pragma unroll
+      for (int k1 = 0; k1 < 8; k1++)
+      {
+        float2 o = k1 ? cmul (col[kb][k1], tw[k1]) : col[kb][k1];
+        o = make_float2 (__fmul_rn (o.x, 0.125f), __fmul_rn (o.y, 0.125f));
+        s_fbc[fbc_stage (k1 * 128 + c * 2 + pol, warp)] = o;
+      }
     }
   }
   __syncthreads ();
