@@ -451,7 +451,7 @@ __device__ __forceinline__ void fetch_raw2 (const InputView& in, const float* s_
 }
 
 template <int KIND, bool AFFINE>
-__global__ void __launch_bounds__ (FBC_THREADS, 640 / FBC_THREADS)
+__global__ void __launch_bounds__ (FBC_THREADS, 768 / FBC_THREADS)
 k_fwd_cols_fb64 (const InputView in, const float* __restrict__ lut, const uint64_t nkeep,
                  const uint64_t part0, const unsigned n2, const float2* __restrict__ tw4,
                  float2* __restrict__ scratch)
@@ -588,7 +588,10 @@ constexpr size_t rows32_smem_bytes ()
 
 // CTAs of k_rows32 resident per SM: at 8192 shared memory (one padded row +
 // 10 KB of twiddles) and 128 registers per thread allow two; at 4096 three
-// (four would cap the registers at 128, where the 4096-point schedule spills)
+// (four would cap the registers at 128, where the 4096-point schedule spills).
+// A 30 KB pass-2 table shared by a thread's two butterflies (fewer
+// instructions) measured slower: 208 KB of shared memory per SM leaves too
+// little L1 for the rows' global loads.
 template <int N2>
 constexpr unsigned rows32_ctas_per_sm ()
 {
@@ -607,7 +610,7 @@ constexpr unsigned rows32_ctas_per_sm ()
 template <int N2, bool CONV>
 __global__ void __launch_bounds__ (Row32<N2>::T, rows32_ctas_per_sm<N2> ())
 k_rows32 (float2* scratch, const float2* __restrict__ H, const unsigned n1,
-          const unsigned nchan, const unsigned npol, const unsigned nrows)
+          const unsigned nchan, const unsigned npol, const unsigned nrows, const unsigned inner)
 {
   using RS = Row32<N2>;
   constexpr unsigned ROW_BYTES = N2 * sizeof (float2);
@@ -621,9 +624,9 @@ k_rows32 (float2* scratch, const float2* __restrict__ H, const unsigned n1,
   for (int i = tid; i < RS::TABN; i += RS::T) tab1[i] = RS::table_entry (i);
 
   // Rows are walked with their response row (channel, k1) outermost and the
-  // parts and polarisations innermost, so that the CTAs working at one time
-  // share few response rows and find them in L2.
-  const unsigned inner = nrows / (n1 * nchan);      // parts x polarisations
+  // parts and polarisations innermost (inner = parts x polarisations), so
+  // that the CTAs working at one time share few response rows and find them
+  // in L2.
   const auto row_of = [=] (unsigned idx, unsigned& hrow) {
     hrow = idx / inner;                             // c * n1 + k1
     const unsigned bp = idx % inner;
@@ -2217,7 +2220,7 @@ void launch_rows (unsigned nrows, float2* scratch, const ConvTables& tb, unsigne
   // persistent: as many CTAs as are resident at once
   const unsigned grid = std::min<unsigned> (nrows, rows_ctas_per_sm (N2) * unsigned (tb.nsm));
   k_rows32<N2, true><<<grid, Row32<N2>::T, rows32_smem_bytes<N2> (), st>>> (
-      scratch, tb.H, n1, sh.nchan, sh.npol, nrows);
+      scratch, tb.H, n1, sh.nchan, sh.npol, nrows, nrows / (n1 * sh.nchan));
 }
 
 template <int N1>
@@ -2373,7 +2376,7 @@ void launch_rows_inv (unsigned nrows, float2* scratch, const IfbTables& tb, unsi
 {
   const unsigned grid = std::min<unsigned> (nrows, rows_ctas_per_sm (N2) * unsigned (tb.nsm));
   k_rows32<N2, false><<<grid, Row32<N2>::T, rows32_smem_bytes<N2> (), st>>> (
-      scratch, nullptr, n1, 1, npol, nrows);
+      scratch, nullptr, n1, 1, npol, nrows, nrows / n1);
 }
 
 template <int N2, bool CONV>
