@@ -1101,10 +1101,25 @@ k_ifb_cols (const float2* __restrict__ scratch, const IfbShape sh, const float2*
 // Filterbank with a response ("During")
 // --------------------------------------------------------------------------
 
+// Barrier of a group of TS consecutive threads that exchange data only among
+// themselves: a warp barrier when the group lies inside one warp (TS divides
+// 32), else the block's.
+template <int TS>
+__device__ __forceinline__ void group_sync ()
+{
+  static_assert (TS <= 32 ? 32 % TS == 0 : TS % 32 == 0, "groups must tile the warps");
+  if constexpr (TS <= 32)
+    __syncwarp ();
+  else
+    __syncthreads ();
+}
+
 // One radix pass of an N-point transform run by the stockham_threads(N)
 // threads of one group (lane = index in the group), both sides in the padded
 // layout relative to the group's base, or the output unpadded (PO false).
-// Every thread of the block calls it: the barriers are block-wide.
+// Every thread of the block calls it.  Its barriers cover the group only, so
+// a caller that reads or writes the groups' buffers across groups puts a
+// block barrier between that and the passes.
 template <int N, int D, int P, bool PO>
 __device__ __forceinline__ void gpass (int lane, const float2* src, float2* dst, float2* v,
                                        const float2* tab)
@@ -1115,10 +1130,10 @@ __device__ __forceinline__ void gpass (int lane, const float2* src, float2* dst,
     constexpr int R = stockham_radix (N, P);
     constexpr int Ns = stockham_ns (N, P);
     StockhamPassT<N, R, T, D, true, PO>::load (lane, src, v);
-    __syncthreads ();
+    group_sync<T> ();
     StockhamPassT<N, R, T, D, true, PO>::compute_store (
         lane, Ns, v, dst, P ? tab + pass_table_offset (N, P) : nullptr);
-    __syncthreads ();
+    group_sync<T> ();
   }
 }
 
@@ -1127,77 +1142,101 @@ constexpr int DUR_N2 = 8192;
 template <int SEG>
 constexpr size_t during_rows_smem ()
 {
-  return size_t (spad_size (DUR_N2) + pass_tables_size (DUR_N2) + pass_tables_size (SEG))
+  return size_t (spad_size (DUR_N2) + Row32<DUR_N2>::TABN + pass_tables_size (SEG))
          * sizeof (float2);
 }
 
-// Rows of the big transform (persistent CTAs, one row at a time): the
-// forward n2-point FFT, the response of each output channel on its segment
-// (Response::operate over nchan_subband channels from input_ichan*nchan_subband,
-// FilterbankEngineCPU.C:480-484), then the seg-point inverse FFT of every
-// segment, written back in place.  Row r of the scratch is row k1 = r mod n1
-// of (part, input channel, pol).
+// Rows of the big transform (persistent CTAs, one row at a time, two per SM):
+// the forward n2-point FFT with 32 points per thread in three passes
+// (Row32), the response of each output channel on its segment multiplied in
+// registers (Response::operate over nchan_subband channels from
+// input_ichan*nchan_subband, FilterbankEngineCPU.C:480-484), then the
+// seg-point inverse FFT of every segment, written back in place: each group
+// of seg/16 threads takes two segments.  Row r of the scratch is row
+// k1 = r mod n1 of (part, input channel, pol).
 template <int SEG>
-__global__ void __launch_bounds__ (stockham_threads (DUR_N2), 1)
-k_rows_during (float2* __restrict__ scratch, const float2* __restrict__ ptab,
-               const float2* __restrict__ ptab_seg, const float2* __restrict__ H,
-               const unsigned n1, const unsigned nsub, const unsigned npol,
-               const unsigned nchan_in, const unsigned nrows)
+__global__ void __launch_bounds__ (Row32<DUR_N2>::T, 2)
+k_rows_during (float2* __restrict__ scratch, const float2* __restrict__ ptab_seg,
+               const float2* __restrict__ H, const unsigned n1, const unsigned nsub,
+               const unsigned npol, const unsigned nchan_in, const unsigned nrows)
 {
   constexpr int N2 = DUR_N2;
-  constexpr int T = stockham_threads (N2);
-  constexpr int TABN = pass_tables_size (N2);
+  using RS = Row32<N2>;
+  constexpr int T = RS::T;
   constexpr int TABS = pass_tables_size (SEG);
   constexpr int TS = stockham_threads (SEG);
   constexpr int NPS = stockham_npass (SEG);
-  static_assert (stockham_npass (N2) == 4, "row schedule of 8192 points has four passes");
+  constexpr int NG = T / TS;                      // segment groups
+  constexpr unsigned ROW_BYTES = N2 * sizeof (float2);
+  constexpr unsigned CHUNK = 16384;
   static_assert (NPS == 2 || NPS == 3, "segment transforms of 64 .. 4096 points");
-  static_assert (T % TS == 0, "segments tile the block");
+  static_assert (T % TS == 0 && (N2 / SEG) == 2 * NG, "each group takes two segments");
   extern __shared__ __align__ (16) float2 s_dur[];
   float2* work = s_dur;
-  float2* tab = work + spad_size (N2);
-  float2* tabs = tab + TABN;
+  float2* tab1 = work + spad_size (N2);
+  float2* th = tab1 + RS::TAB1;
+  float2* tl = th + RS::TABH;
+  float2* tabs = tab1 + RS::TABN;
   const int tid = threadIdx.x;
-  for (int i = tid; i < TABN; i += T) tab[i] = __ldg (ptab + i);
+  for (int i = tid; i < RS::TABN; i += T) tab1[i] = RS::table_entry (i);
   for (int i = tid; i < TABS; i += T) tabs[i] = __ldg (ptab_seg + i);
-  __syncthreads ();
-  // group g transforms segment g; spad(g*SEG + i) = spad(g*SEG) + spad(i)
-  // because SEG is a multiple of 16
   const int g = tid / TS, lane = tid % TS;
-  float2* wseg = work + spad (g * SEG);
-  float2 v[16];
+  float2 v[32];
   for (unsigned row = blockIdx.x; row < nrows; row += gridDim.x)
   {
     const unsigned k1 = row % n1;
     const unsigned cin = (row / n1 / npol) % nchan_in;
     float2* grow = scratch + uint64_t (row) * N2;
-    tpass<N2, -1, 0, false, true> (grow, work, v, tab);
-    tpass<N2, -1, 1, true, true> (work, work, v, tab);
-    tpass<N2, -1, 2, true, true> (work, work, v, tab);
-    tpass<N2, -1, 3, true, true> (work, work, v, tab);
+    const unsigned next = row + gridDim.x;
+    if (tid == 0 && next < nrows)
+    {
+      const char* nr = reinterpret_cast<const char*> (scratch + uint64_t (next) * N2);
+      for (unsigned o = 0; o < ROW_BYTES; o += CHUNK) prefetch_l2 (nr + o, CHUNK);
+    }
+    RS::p0_load (tid, grow, v);
+    __syncthreads ();     // the previous row's segment passes are done
+    RS::template p0_compute_store<-1> (tid, v, work);
+    __syncthreads ();
+    RS::p1_load (tid, work, v);
+    __syncthreads ();
+    RS::template p1_compute_store<-1> (tid, v, work, tab1);
+    __syncthreads ();
+    RS::p2_load (tid, work, v);
+    __syncthreads ();
+    RS::template p2_compute<-1> (tid, v, th, tl);
     // position i = cs*SEG + f2 of row k1 is bin k1 + n1*f2 of output channel
     // cin*nsub + cs: (f_r d_r - f_i d_i, f_i d_r + f_r d_i), Response.C:662-726
+    const float2* hc = H + (uint64_t (cin) * nsub * n1 + k1) * SEG;
 #pragma unroll
-    for (int m = 0; m < 16; m++)
-    {
-      const int i = tid + m * T;
-      const unsigned cs = unsigned (i) / SEG, f2 = unsigned (i) % SEG;
-      const float2 f = __ldg (H + ((uint64_t (cin) * nsub + cs) * n1 + k1) * SEG + f2);
-      const float2 d = work[spad (i)];
-      work[spad (i)] = make_float2 (d.x * f.x - d.y * f.y, d.x * f.y + d.y * f.x);
-    }
+    for (int b = 0; b < 2; b++)
+#pragma unroll
+      for (int r = 0; r < 16; r++)
+      {
+        const int i = tid + b * T + r * RS::NS2;
+        const unsigned cs = unsigned (i) / SEG, f2 = unsigned (i) % SEG;
+        const float2 f = __ldg (hc + uint64_t (cs) * n1 * SEG + f2);
+        const float2 d = v[16 * b + r];
+        work[spad (i)] = make_float2 (d.x * f.x - d.y * f.y, d.x * f.y + d.y * f.x);
+      }
     __syncthreads ();
-    float2* gseg = grow + g * SEG;
-    if constexpr (NPS == 2)
+    // spad(s*SEG + i) = spad(s*SEG) + spad(i) because SEG is a multiple of 16
+#pragma unroll
+    for (int s2 = 0; s2 < 2; s2++)
     {
-      gpass<SEG, +1, 0, true> (lane, wseg, wseg, v, tabs);
-      gpass<SEG, +1, 1, false> (lane, wseg, gseg, v, tabs);
-    }
-    else
-    {
-      gpass<SEG, +1, 0, true> (lane, wseg, wseg, v, tabs);
-      gpass<SEG, +1, 1, true> (lane, wseg, wseg, v, tabs);
-      gpass<SEG, +1, 2, false> (lane, wseg, gseg, v, tabs);
+      const int sg = g + s2 * NG;
+      float2* wseg = work + spad (sg * SEG);
+      float2* gseg = grow + sg * SEG;
+      if constexpr (NPS == 2)
+      {
+        gpass<SEG, +1, 0, true> (lane, wseg, wseg, v, tabs);
+        gpass<SEG, +1, 1, false> (lane, wseg, gseg, v, tabs);
+      }
+      else
+      {
+        gpass<SEG, +1, 0, true> (lane, wseg, wseg, v, tabs);
+        gpass<SEG, +1, 1, true> (lane, wseg, wseg, v, tabs);
+        gpass<SEG, +1, 2, false> (lane, wseg, gseg, v, tabs);
+      }
     }
   }
 }
@@ -1356,29 +1395,81 @@ k_fwd_cols_big (const InputView in, const float* __restrict__ lut, const uint64_
   const unsigned c = blockIdx.z;
   const uint64_t N = uint64_t (N1) * n2;
   const uint64_t t0 = (part0 + b) * step + c0;
+  // thread (kk, j) takes rows k = kk + m KSTEP of column c0 + j
+  constexpr int KSTEP = T / COLW;
+  const int j = threadIdx.x % COLW, kk = threadIdx.x / COLW;
+  // The block's window t0 + k n2 + j lies in one segment of the input (the
+  // carried prefix or the main block) except in the parts that straddle the
+  // prefix's end; there each sample takes the general fetch.
+  const bool one_seg = t0 >= in.npre || t0 + uint64_t (N1 - 1) * n2 + (COLW - 1) < in.npre;
+  const bool in_pre = t0 < in.npre;
+  const uint64_t ts = in_pre ? t0 : t0 - in.npre;
+  const float* ap = apod ? apod + uint64_t (kk) * n2 + c0 + j : nullptr;
+  const uint64_t rstep = uint64_t (KSTEP) * n2;
   for (unsigned p = 0; p < in.npol; p++)
   {
     __syncthreads ();
-    for (int e = threadIdx.x; e < COLW * N1; e += T)
-    {
-      const int j = e % COLW, k = e / COLW;
-      float2 x = fetch<KIND> (in, s_lut, c, p, t0 + uint64_t (k) * n2 + j);
-      if (apod)
+    const auto put = [&] (int k, float2 x) {
+      if (ap)
       {
-        const float w = __ldg (apod + uint64_t (k) * n2 + c0 + j);
+        const float w = __ldg (ap + uint64_t (k - kk) * n2);
         x = make_float2 (__fmul_rn (x.x, w), __fmul_rn (x.y, w));
       }
       col[j * SP + spad (k)] = x;
+    };
+    if (one_seg && KIND == IN_FLOAT)
+    {
+      const float2* f = static_cast<const float2*> (in_pre ? in.pre : in.main)
+                        + (uint64_t (c) * in.npol + p) * (in_pre ? in.pre_span : in.main_span)
+                        + ts + uint64_t (kk) * n2 + j;
+      for (int k = kk; k < N1; k += KSTEP, f += rstep) put (k, __ldg (f));
     }
+    else if (one_seg)
+    {
+      // one complex sample per (t, c, p): 2 bytes (int8) or 4 (int16)
+      const uint64_t cs = uint64_t (in.nchan) * in.npol;
+      const uint64_t i0 = (ts + uint64_t (kk) * n2 + j) * cs + c * in.npol + p;
+      const uint64_t istep = rstep * cs;
+      if constexpr (KIND == IN_INT8)
+      {
+        const unsigned short* q = static_cast<const unsigned short*> (in_pre ? in.pre : in.main) + i0;
+        for (int k = kk; k < N1; k += KSTEP, q += istep)
+        {
+          const unsigned short w = __ldg (q);
+          put (k, make_float2 (s_lut[w & 0xff], s_lut[w >> 8]));
+        }
+      }
+      else
+      {
+        const unsigned* q = static_cast<const unsigned*> (in_pre ? in.pre : in.main) + i0;
+        for (int k = kk; k < N1; k += KSTEP, q += istep)
+        {
+          const unsigned w = __ldg (q);
+          short re = short (w & 0xffff), im = short (w >> 16);
+          if (in.offset_binary)
+          {
+            re = short (re ^ 0x8000);
+            im = short (im ^ 0x8000);
+          }
+          // SixteenBitUnpacker.C:69: float(x) + 0.5
+          put (k, make_float2 (__fadd_rn (float (re), 0.5f), __fadd_rn (float (im), 0.5f)));
+        }
+      }
+    }
+    else
+      for (int k = kk; k < N1; k += KSTEP)
+        put (k, fetch<KIND> (in, s_lut, c, p, t0 + uint64_t (k) * n2 + j));
     __syncthreads ();
     colbig_fft<N1, -1> (col, tab);
-    float2* dst = scratch + ((uint64_t (b) * in.nchan + c) * in.npol + p) * N + c0;
-    for (int e = threadIdx.x; e < COLW * N1; e += T)
+    __syncthreads ();                  // the output below reads across columns' groups
+    float2* dst = scratch + ((uint64_t (b) * in.nchan + c) * in.npol + p) * N + c0 + j
+                  + uint64_t (kk) * n2;
+    const float2* tw = tw4 + uint64_t (kk) * n2 + c0 + j;
+    for (int k1 = kk; k1 < N1; k1 += KSTEP, dst += rstep, tw += rstep)
     {
-      const int j = e % COLW, k1 = e / COLW;
       float2 y = col[j * SP + spad (k1)];
-      if (k1) y = cmul (y, __ldg (tw4 + uint64_t (k1) * n2 + c0 + j));
-      dst[uint64_t (k1) * n2 + j] = y;
+      if (k1) y = cmul (y, __ldg (tw));
+      *dst = y;
     }
   }
 }
@@ -1407,23 +1498,29 @@ k_inv_cols_during_big (const float2* __restrict__ scratch, const DuringShape sh,
   const uint64_t N = uint64_t (N1) * sh.n2;
   const unsigned cs = c0 / sh.seg, t20 = c0 % sh.seg;
   const unsigned c = cin * sh.nsub + cs;
+  // thread (kk, j) takes rows k1 = kk + m KSTEP of column c0 + j
+  constexpr int KSTEP = T / CW;
+  const int j = threadIdx.x % CW, kk = threadIdx.x / CW;
 #pragma unroll
   for (int p = 0; p < NPOL; p++)
   {
-    const float2* src = scratch + ((uint64_t (b) * sh.nchan_in + cin) * NPOL + p) * N + c0;
-    float2* col = s_cb + p * CW * SP;
-    for (int e = threadIdx.x; e < CW * N1; e += T)
+    const float2* src = scratch + ((uint64_t (b) * sh.nchan_in + cin) * NPOL + p) * N + c0 + j
+                        + uint64_t (kk) * sh.n2;
+    const float2* tw = twd + uint64_t (kk) * sh.seg + t20 + j;
+    float2* col = s_cb + p * CW * SP + j * SP;
+    const uint64_t sstep = uint64_t (KSTEP) * sh.n2, tstep = uint64_t (KSTEP) * sh.seg;
+    for (int k1 = kk; k1 < N1; k1 += KSTEP, src += sstep, tw += tstep)
     {
-      const int j = e % CW, k1 = e / CW;
-      float2 x = src[uint64_t (k1) * sh.n2 + j];
-      if (k1) x = cmulc (x, __ldg (twd + uint64_t (k1) * sh.seg + t20 + j));
-      col[j * SP + spad (k1)] = x;
+      float2 x = *src;
+      if (k1) x = cmulc (x, __ldg (tw));
+      col[spad (k1)] = x;
     }
   }
   __syncthreads ();
 #pragma unroll
   for (int p = 0; p < NPOL; p++)
     colbig_fft<N1, +1> (s_cb + p * CW * SP, tab);
+  __syncthreads ();                    // the fold below reads across columns' groups
   const uint64_t tbase = (part0 + b) * sh.nkeep;
   const float2* c0p = s_cb;
   const float2* c1p = s_cb + (NPOL - 1) * CW * SP;
@@ -2496,9 +2593,10 @@ cudaError_t launch_rows_during (unsigned nrows, float2* scratch, const DuringSha
   cudaError_t e = cudaFuncSetAttribute (k_rows_during<SEG>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int (smem));
   if (e != cudaSuccess) return e;
-  const unsigned grid = std::min<unsigned> (nrows, unsigned (tb.nsm));
-  k_rows_during<SEG><<<grid, stockham_threads (DUR_N2), smem, st>>> (
-      scratch, tb.ptab, tb.ptab_seg, tb.H, sh.n1, sh.nsub, sh.npol, sh.nchan_in, nrows);
+  // persistent: two CTAs per SM
+  const unsigned grid = std::min<unsigned> (nrows, 2 * unsigned (tb.nsm));
+  k_rows_during<SEG><<<grid, Row32<DUR_N2>::T, smem, st>>> (
+      scratch, tb.ptab_seg, tb.H, sh.n1, sh.nsub, sh.npol, sh.nchan_in, nrows);
   return cudaSuccess;
 }
 
