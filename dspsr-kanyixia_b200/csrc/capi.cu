@@ -1587,7 +1587,7 @@ struct dspsr_b200_filterbank_during
 {
   dspsr_b200_context* ctx = nullptr;
   DuringShape shape {};
-  DevBuf<float2> tw4, ptab, ptab_seg, ptab_col, twd, H, Hw, tmp, scratch;
+  DevBuf<float2> tw4, ptab_seg, ptab_col, twd, H, Hw, tmp, scratch;
   DevBuf<double> chan_par;
   DevBuf<float> temporal, spectral;
   bool have_response = false, have_temporal = false, have_spectral = false;
@@ -1598,7 +1598,6 @@ struct dspsr_b200_filterbank_during
   {
     DuringTables t;
     t.tw4 = tw4.ptr;
-    t.ptab = ptab.ptr;
     t.ptab_seg = ptab_seg.ptr;
     t.twd = twd.ptr;
     t.ptab_col = ptab_col.ptr;
@@ -1618,7 +1617,6 @@ struct dspsr_b200_filterbank_during
   void release ()
   {
     tw4.release ();
-    ptab.release ();
     ptab_seg.release ();
     ptab_col.release ();
     twd.release ();
@@ -1668,12 +1666,13 @@ int dspsr_b200_filterbank_during::init (dspsr_b200_context* c, const dspsr_b200_
   B200_CHECK (ctx, twd.reserve (td.size ()), "cudaMalloc channel twiddles");
   B200_CHECK (ctx, cudaMemcpy (twd.ptr, td.data (), td.size () * sizeof (float2),
                                cudaMemcpyHostToDevice), "copy channel twiddles");
-  // pass tables of the row, segment and (n1 >= 64) column transforms
-  for (int which = 0; which < 3; which++)
+  // pass tables of the segment and (n1 >= 64) column transforms (the row
+  // kernel builds its own)
+  for (int which = 1; which < 3; which++)
   {
     if (which == 2 && s.n1 < 64) break;
-    const unsigned n = which == 2 ? s.n1 : which ? s.seg : s.n2;
-    DevBuf<float2>& dst = which == 2 ? ptab_col : which ? ptab_seg : ptab;
+    const unsigned n = which == 2 ? s.n1 : s.seg;
+    DevBuf<float2>& dst = which == 2 ? ptab_col : ptab_seg;
     const unsigned cnt = pass_tables_count (n);
     std::vector<float2> pt (std::max (cnt, 1u), make_float2 (0.f, 0.f));
     make_pass_tables (n, pt.data (), cnt);

@@ -1337,8 +1337,11 @@ k_inv_cols_during (const float2* __restrict__ scratch, const DuringShape sh, con
 // spad_size(N1) + 1 keeps the 16 columns of a row on different banks.
 constexpr int COLW = 16;
 
-template <int N1>
-B200_CE int colbig_stride () { return spad_size (N1) + 1; }
+// Buffer stride: with 16 columns per CTA (a half-warp touches one row) 1 mod
+// 16 float2 keeps the columns on distinct bank pairs; with 8 (a half-warp
+// touches two adjacent rows, k even and k + 1) 2 mod 16 does.
+template <int N1, int CW = COLW>
+B200_CE int colbig_stride () { return spad_size (N1) + (CW >= 16 ? 1 : 2); }
 
 template <int N1, int NPOL>
 constexpr size_t colbig_smem ()
@@ -1354,17 +1357,18 @@ B200_CE int inv_colw () { return N1 >= 512 ? 8 : COLW; }
 template <int N1, int NPOL>
 constexpr size_t colbig_inv_smem ()
 {
-  return size_t (NPOL * inv_colw<N1> () * colbig_stride<N1> () + pass_tables_size (N1))
+  return size_t (NPOL * inv_colw<N1> () * colbig_stride<N1, inv_colw<N1> ()> ()
+                 + pass_tables_size (N1))
          * sizeof (float2);
 }
 
 // the N1-point transform (direction D) of every column in col[]
-template <int N1, int D>
+template <int N1, int D, int SP = colbig_stride<N1> ()>
 __device__ __forceinline__ void colbig_fft (float2* col, const float2* tab)
 {
   constexpr int TS = stockham_threads (N1);
   const int g = threadIdx.x / TS, lane = threadIdx.x % TS;
-  float2* base = col + g * colbig_stride<N1> ();
+  float2* base = col + g * SP;
   float2 v[16];
   gpass<N1, D, 0, true> (lane, base, base, v, tab);
   gpass<N1, D, 1, true> (lane, base, base, v, tab);
@@ -1487,7 +1491,7 @@ k_inv_cols_during_big (const float2* __restrict__ scratch, const DuringShape sh,
 {
   constexpr int CW = inv_colw<N1> ();
   constexpr int T = CW * stockham_threads (N1);
-  constexpr int SP = colbig_stride<N1> ();
+  constexpr int SP = colbig_stride<N1, CW> ();
   constexpr int TAB = pass_tables_size (N1);
   extern __shared__ __align__ (16) float2 s_cb[];
   float2* tab = s_cb + NPOL * CW * SP;
@@ -1519,7 +1523,7 @@ k_inv_cols_during_big (const float2* __restrict__ scratch, const DuringShape sh,
   __syncthreads ();
 #pragma unroll
   for (int p = 0; p < NPOL; p++)
-    colbig_fft<N1, +1> (s_cb + p * CW * SP, tab);
+    colbig_fft<N1, +1, SP> (s_cb + p * CW * SP, tab);
   __syncthreads ();                    // the fold below reads across columns' groups
   const uint64_t tbase = (part0 + b) * sh.nkeep;
   const float2* c0p = s_cb;

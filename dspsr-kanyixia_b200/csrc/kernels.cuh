@@ -256,7 +256,6 @@ struct DuringShape
 struct DuringTables
 {
   const float2* tw4;       // [n1][n2] exp(-2 pi i k1 m / (n1 n2))
-  const float2* ptab;      // per-pass tables of the n2-point FFT
   const float2* ptab_seg;  // per-pass tables of the seg-point FFT
   const float2* twd;       // [n1][seg] exp(-2 pi i k1 t2 / freq_res)
   const float2* ptab_col;  // per-pass tables of the n1-point FFT (n1 >= 64)
