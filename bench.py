@@ -1443,6 +1443,7 @@ def run_b200_c3(args, cfg, world, rank, local):
     # autotuner: per shape class (FFT length, channels) the plan that runs one
     # block fastest, timed alone on the stream
     tuned = {}
+    tuned_ms = {}
     t_tune = time.perf_counter()
     for s in streams:
         key = (s["nfft"], s["nchan"])
@@ -1467,6 +1468,7 @@ def run_b200_c3(args, cfg, world, rank, local):
                 if best is None or ms < best[0]:
                     best = (ms, plan)
             tuned[key] = best[1]
+            tuned_ms[key] = best[0]
         s["plan"] = tuned[key]
         s["scratch"] = tuned[key][0]
         s["pipe"] = make_pipe(s, s["plan"])
@@ -1564,7 +1566,10 @@ def run_b200_c3(args, cfg, world, rank, local):
                    "shape_classes": [list(x) for x in shapes],
                    "tuned": {f"{k[0]}x{k[1]}": {"scratch_mib": v[0] >> 20,
                                                   "row_length": v[1] or min(k[0], 8192),
-                                                  "rows": "bf16x3 tensor" if v[2] == 3 else "fp32"}
+                                                  "rows": "bf16x3 tensor" if v[2] == 3 else "fp32",
+                                                  "block_ms": round(tuned_ms[k], 3),
+                                                  "streams": sum(1 for s in streams
+                                                                 if (s["nfft"], s["nchan"]) == k)}
                              for k, v in tuned.items()},
                    "autotune_s": round(t_tune, 2),
                    "schedule": "pipelines one after another on the device",

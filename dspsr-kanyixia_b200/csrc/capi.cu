@@ -325,8 +325,10 @@ struct dspsr_b200_fold
   static constexpr int NRING = 8;
   static constexpr size_t INITIAL_SEGMENTS = 16384;
   DevBuf<FoldSegment> d_segs[NRING];
-  // with many channels the column of each sample is computed once per block
-  // (k_colplan) instead of from the segments in every channel
+  // the column of each sample is computed once per block (k_colplan: one
+  // segment search per 1024 samples) instead of by a search per warp in every
+  // channel's epilogue; with one channel it still pays (C1: 0.867 -> 0.827 ms
+  // per block)
   bool use_cols = false;
   DevBuf<unsigned> d_cols[NRING];
   uint64_t cols_cap = 0;
@@ -2707,7 +2709,7 @@ int dspsr_b200_fold_create (dspsr_b200_context* ctx, unsigned nbin, unsigned nch
   // engines that fold many channels from one plan (the filterbank with a
   // response) read each sample's column once per block instead of searching
   // the plan in every channel
-  f->use_cols = nchan >= 4;
+  f->use_cols = true;
   *out = f;
   return DSPSR_B200_OK;
 }
@@ -2909,7 +2911,7 @@ int dspsr_b200_pipeline_create (dspsr_b200_context* ctx, const dspsr_b200_pipeli
   }
   if (!rc) rc = pl->fold.init (ctx, cfg->nbin, nchan, pl->nout,
                                pl->sub_on ? unsigned (pl->sub_slots.size ()) : 1);
-  pl->fold.use_cols = nchan >= 4;
+  pl->fold.use_cols = true;
   // C2's shape -- a 64-channel filterbank of one dual-polarisation int8 or
   // int16 channel with four-step parts of 8 x n2 -- runs the filterbank
   // inside the forward column pass: its output never goes through memory

@@ -2280,13 +2280,34 @@ __global__ void k_zeroed_fold (const float2* __restrict__ v, const uint64_t span
 }
 
 // one thread per sample: the column warp_fold_bin would give it
+// A warp takes COLPLAN_GROUPS consecutive groups of 32 samples: one binary
+// search for the first sample, then each lane steps forward over the
+// segment boundaries from where the previous group's last lane ended.
+constexpr int COLPLAN_GROUPS = 32;
+
 __global__ void k_colplan (const FoldSegment* __restrict__ segs, const int nseg,
                            const uint64_t ndat, const unsigned nbin, unsigned* __restrict__ cols)
 {
-  const uint64_t t = uint64_t (blockIdx.x) * blockDim.x + threadIdx.x;
-  const bool ok = t < ndat;
-  const unsigned col = warp_fold_bin (segs, nseg, ok, t, nbin);
-  if (ok) cols[t] = col;
+  const int lane = threadIdx.x & 31;
+  const uint64_t w0 = (uint64_t (blockIdx.x) * (blockDim.x / 32) + threadIdx.x / 32) * 32
+                      * COLPLAN_GROUPS;
+  if (w0 >= ndat) return;             // whole warps
+  int s = 0;
+  if (lane == 0) s = seg_search (segs, nseg, w0);
+  s = __shfl_sync (FULL, s, 0);
+  for (int g = 0; g < COLPLAN_GROUPS; g++)
+  {
+    const uint64_t t = w0 + uint64_t (g) * 32 + lane;
+    int sl = s;
+    while (sl + 1 < nseg && __ldg (&segs[sl + 1].start) <= t) sl++;
+    if (t < ndat)
+    {
+      const unsigned base = __ldg (&segs[sl].base);
+      const unsigned bin = seg_bin (segs, sl, t, nbin);
+      cols[t] = (base == FOLD_SKIP || bin >= nbin) ? NO_COLUMN : base + bin;
+    }
+    s = __shfl_sync (FULL, sl, 31);
+  }
 }
 
 __global__ void k_binplan (const FoldSegment* __restrict__ segs, const int nseg,
@@ -3070,7 +3091,9 @@ cudaError_t launch_colplan (const FoldSegment* segs, int nseg, uint64_t ndat, un
 {
   if (ndat == 0) return cudaSuccess;
   g_launches++;
-  k_colplan<<<unsigned ((ndat + 255) / 256), 256, 0, st>>> (segs, nseg, ndat, nbin, cols);
+  const uint64_t per_block = uint64_t (256) * COLPLAN_GROUPS;
+  k_colplan<<<unsigned ((ndat + per_block - 1) / per_block), 256, 0, st>>> (segs, nseg, ndat,
+                                                                           nbin, cols);
   return cudaGetLastError ();
 }
 
