@@ -574,6 +574,16 @@ __device__ __forceinline__ void tpass (const float2* src, float2* dst, float2* v
   }
 }
 
+// read-only load kept in L1 ahead of other lines (reused by later rows)
+__device__ __forceinline__ float2 ldg_evict_last (const float2* p)
+{
+  float2 v;
+  asm volatile ("ld.global.nc.L1::evict_last.v2.f32 {%0, %1}, [%2];"
+                : "=f"(v.x), "=f"(v.y)
+                : "l"(p));
+  return v;
+}
+
 // L2 prefetch of a global range (16-byte aligned, multiple of 16 bytes)
 __device__ __forceinline__ void prefetch_l2 (const void* p, unsigned bytes)
 {
@@ -624,22 +634,25 @@ k_rows32 (float2* scratch, const float2* __restrict__ H, const unsigned n1,
   for (int i = tid; i < RS::TABN; i += RS::T) tab1[i] = RS::table_entry (i);
 
   // Rows are walked with their response row (channel, k1) outermost and the
-  // parts and polarisations innermost (inner = parts x polarisations), so
-  // that the CTAs working at one time share few response rows and find them
-  // in L2.
+  // parts and polarisations innermost (inner = parts x polarisations), and
+  // each CTA takes a contiguous run of that order: the rows of one response
+  // row follow each other on one SM, which keeps the response in its L1
+  // (loaded evict-last, the streamed rows evict-first).
   const auto row_of = [=] (unsigned idx, unsigned& hrow) {
     hrow = idx / inner;                             // c * n1 + k1
     const unsigned bp = idx % inner;
     return ((bp / npol) * nchan * n1 + hrow / n1 * n1) * npol + (bp % npol) * n1 + hrow % n1;
   };
   float2 v[32];
-  for (unsigned idx = blockIdx.x; idx < nrows; idx += gridDim.x)
+  const unsigned run = (nrows + gridDim.x - 1) / gridDim.x;
+  const unsigned idx_end = min (nrows, (blockIdx.x + 1) * run);
+  for (unsigned idx = blockIdx.x * run; idx < idx_end; idx++)
   {
     unsigned hrow = 0;
     const unsigned row = CONV ? row_of (idx, hrow) : idx;
     float2* grow = scratch + uint64_t (row) * N2;
-    const unsigned next = idx + gridDim.x;
-    if (tid == 0 && next < nrows)
+    const unsigned next = idx + 1;
+    if (tid == 0 && next < idx_end)
     {
       unsigned nh = 0;
       const unsigned nrow = CONV ? row_of (next, nh) : next;
@@ -651,7 +664,10 @@ k_rows32 (float2* scratch, const float2* __restrict__ H, const unsigned n1,
         for (unsigned o = 0; o < ROW_BYTES; o += CHUNK) prefetch_l2 (hp + o, CHUNK);
       }
     }
-    RS::p0_load (tid, grow, v);
+#pragma unroll
+    for (int b = 0; b < 2; b++)
+#pragma unroll
+      for (int r = 0; r < 16; r++) v[16 * b + r] = __ldcs (grow + tid + b * RS::T + r * RS::NS2);
     __syncthreads ();     // the previous row's last shared-memory reads are done
     if constexpr (CONV)
     {
@@ -672,7 +688,7 @@ k_rows32 (float2* scratch, const float2* __restrict__ H, const unsigned n1,
         for (int r = 0; r < 16; r++)
         {
           const float2 d = v[16 * b + r];
-          const float2 f = __ldg (h + tid + b * RS::T + r * RS::NS2);
+          const float2 f = ldg_evict_last (h + tid + b * RS::T + r * RS::NS2);
           v[16 * b + r] = make_float2 (d.x * f.x - d.y * f.y, d.x * f.y + d.y * f.x);
         }
     }
