@@ -1174,7 +1174,8 @@ template <int SEG>
 __global__ void __launch_bounds__ (Row32<DUR_N2>::T, 2)
 k_rows_during (float2* __restrict__ scratch, const float2* __restrict__ ptab_seg,
                const float2* __restrict__ H, const unsigned n1, const unsigned nsub,
-               const unsigned npol, const unsigned nchan_in, const unsigned nrows)
+               const unsigned npol, const unsigned nchan_in, const unsigned nrows,
+               const unsigned inner)
 {
   constexpr int N2 = DUR_N2;
   using RS = Row32<N2>;
@@ -1197,19 +1198,35 @@ k_rows_during (float2* __restrict__ scratch, const float2* __restrict__ ptab_seg
   for (int i = tid; i < RS::TABN; i += T) tab1[i] = RS::table_entry (i);
   for (int i = tid; i < TABS; i += T) tabs[i] = __ldg (ptab_seg + i);
   const int g = tid / TS, lane = tid % TS;
+  // As in k_rows32: rows walked with their response rows (input channel,
+  // k1) outermost, parts and polarisations innermost (inner of them), each
+  // CTA a contiguous run, the response kept in L1 (evict-last loads) and the
+  // scratch rows streamed (evict-first).
+  const auto row_of = [=] (unsigned idx, unsigned& hrow) {
+    hrow = idx / inner;                             // cin * n1 + k1
+    const unsigned bp = idx % inner;
+    return ((bp / npol) * nchan_in * n1 + hrow / n1 * n1) * npol + (bp % npol) * n1 + hrow % n1;
+  };
   float2 v[32];
-  for (unsigned row = blockIdx.x; row < nrows; row += gridDim.x)
+  const unsigned run = (nrows + gridDim.x - 1) / gridDim.x;
+  const unsigned idx_end = min (nrows, (blockIdx.x + 1) * run);
+  for (unsigned idx = blockIdx.x * run; idx < idx_end; idx++)
   {
-    const unsigned k1 = row % n1;
-    const unsigned cin = (row / n1 / npol) % nchan_in;
+    unsigned hrow = 0;
+    const unsigned row = row_of (idx, hrow);
+    const unsigned k1 = hrow % n1;
+    const unsigned cin = hrow / n1;
     float2* grow = scratch + uint64_t (row) * N2;
-    const unsigned next = row + gridDim.x;
-    if (tid == 0 && next < nrows)
+    if (tid == 0 && idx + 1 < idx_end)
     {
-      const char* nr = reinterpret_cast<const char*> (scratch + uint64_t (next) * N2);
+      unsigned nh = 0;
+      const char* nr = reinterpret_cast<const char*> (scratch + uint64_t (row_of (idx + 1, nh)) * N2);
       for (unsigned o = 0; o < ROW_BYTES; o += CHUNK) prefetch_l2 (nr + o, CHUNK);
     }
-    RS::p0_load (tid, grow, v);
+#pragma unroll
+    for (int b = 0; b < 2; b++)
+#pragma unroll
+      for (int r = 0; r < 16; r++) v[16 * b + r] = __ldcs (grow + tid + b * T + r * RS::NS2);
     __syncthreads ();     // the previous row's segment passes are done
     RS::template p0_compute_store<-1> (tid, v, work);
     __syncthreads ();
@@ -1230,7 +1247,7 @@ k_rows_during (float2* __restrict__ scratch, const float2* __restrict__ ptab_seg
       {
         const int i = tid + b * T + r * RS::NS2;
         const unsigned cs = unsigned (i) / SEG, f2 = unsigned (i) % SEG;
-        const float2 f = __ldg (hc + uint64_t (cs) * n1 * SEG + f2);
+        const float2 f = ldg_evict_last (hc + uint64_t (cs) * n1 * SEG + f2);
         const float2 d = v[16 * b + r];
         work[spad (i)] = make_float2 (d.x * f.x - d.y * f.y, d.x * f.y + d.y * f.x);
       }
@@ -2637,7 +2654,8 @@ cudaError_t launch_rows_during (unsigned nrows, float2* scratch, const DuringSha
   // persistent: two CTAs per SM
   const unsigned grid = std::min<unsigned> (nrows, 2 * unsigned (tb.nsm));
   k_rows_during<SEG><<<grid, Row32<DUR_N2>::T, smem, st>>> (
-      scratch, tb.ptab_seg, tb.H, sh.n1, sh.nsub, sh.npol, sh.nchan_in, nrows);
+      scratch, tb.ptab_seg, tb.H, sh.n1, sh.nsub, sh.npol, sh.nchan_in, nrows,
+      nrows / (sh.n1 * sh.nchan_in));
   return cudaSuccess;
 }
 
