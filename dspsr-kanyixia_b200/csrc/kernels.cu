@@ -601,7 +601,9 @@ constexpr size_t rows32_smem_bytes ()
 // (four would cap the registers at 128, where the 4096-point schedule spills).
 // A 30 KB pass-2 table shared by a thread's two butterflies (fewer
 // instructions) measured slower: 208 KB of shared memory per SM leaves too
-// little L1 for the rows' global loads.
+// little L1 for the rows' global loads.  So did one CTA per SM running two
+// row groups with named barriers on alternate rows of one run (sharing one
+// response row in L1): 1.91 against 1.78 ms per C2 step.
 template <int N2>
 constexpr unsigned rows32_ctas_per_sm ()
 {
@@ -2449,6 +2451,25 @@ cudaError_t run_fourstep_n1 (const ConvShape& sh, const ConvTables& tb, const In
   return cudaGetLastError ();
 }
 
+// The fused kernel's shared-memory opt-in (sized for two polarisations), once
+// per device and instantiation; later calls only test a bit, so that calls
+// made inside a stream capture set nothing up.
+template <int N, int KIND, int MODE, int NOUT>
+cudaError_t fused_setup ()
+{
+  static std::atomic<unsigned> done {0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice (&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned bit = dev < 32 ? 1u << dev : 0u;    // devices past 32: set every time
+  if (bit && (done.load () & bit)) return cudaSuccess;
+  e = cudaFuncSetAttribute (k_fused<N, stockham_threads (N), KIND, MODE, NOUT>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            int (2 * spad_size (N) * sizeof (float2)));
+  if (e == cudaSuccess) done.fetch_or (bit);
+  return e;
+}
+
 template <int N, int KIND, int MODE, int NOUT>
 cudaError_t run_fused_t (const ConvShape& sh, const ConvTables& tb, const InputView& in,
                          uint64_t part0, unsigned nbatch, const FoldView& fv,
@@ -2457,8 +2478,7 @@ cudaError_t run_fused_t (const ConvShape& sh, const ConvTables& tb, const InputV
   constexpr int T = stockham_threads (N);
   const size_t smem = size_t (in.npol) * spad_size (N) * sizeof (float2);
   auto kern = k_fused<N, T, KIND, MODE, NOUT>;
-  cudaError_t err = cudaFuncSetAttribute (kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          int (smem));
+  cudaError_t err = fused_setup<N, KIND, MODE, NOUT> ();
   if (err != cudaSuccess) return err;
   ClockScope cs (clk, KK_FUSED, st);
   kern<<<dim3 (nbatch, sh.nchan), T, smem, st>>> (in, tb.lut, tb.tw2, tb.H, sh.nkeep,
@@ -2597,6 +2617,10 @@ cudaError_t convolution_kernel_setup ()
   if (bit && (attr_done.load () & bit)) return cudaSuccess;
   e = set_rows_smem<8192, true> ();
   if (e == cudaSuccess) e = set_rows_smem<4096, true> ();
+  // the single-kernel transforms of the float voltage path (the no-alloc
+  // entry point's)
+  if (e == cudaSuccess) e = fused_setup<4096, IN_FLOAT, OUT_VOLTAGE, 1> ();
+  if (e == cudaSuccess) e = fused_setup<8192, IN_FLOAT, OUT_VOLTAGE, 1> ();
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute (k_fwd_cols_fb64<IN_INT8, false>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize, int (FBC_SMEM));
