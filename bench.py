@@ -961,7 +961,7 @@ def run_b200_sk(args, cfg, world, rank, local):
 
 def sk_proposer(args, cfg, b2, ctx, device, lo, hi, rank, world):
     """The learned RFI-mask proposer in front of SpectralKurtosis: trained on
-    the SK masks of one RFI-injected block, judged by SK on another (miss =
+    the SK masks of one RFI-injected block, scored against SK on another (miss =
     SK zaps, proposer keeps; false zap = SK keeps, proposer zaps), alone and
     with the SK fallback below the confidence threshold; its throughput is
     that of the feature + tensor-core inference kernels on the SK sums."""
@@ -1993,7 +1993,7 @@ def run_b200_c5(args, cfg, world, rank, local):
         "parity": c5_parity(cfg, b2, raw, pos, neg, nfft) if rank == 0 and world == 1 else None,
         "check": {"hits_total": int(hits.sum()),
                   # a 1.6 ms turn is 1250 samples of the re-channelised data,
-                  # so most of the 4096 bins get no hits: judge the hit ones
+                  # so most of the 4096 bins get no hits: measure the hit ones
                   "bins_hit": int((hits > 0).sum()),
                   "profile_peak_over_median_of_hit_bins": float(
                       np.max((prof[:, 0].sum(0) / np.maximum(hits, 1))[hits > 0])

@@ -25,7 +25,7 @@ def test_fft_matches_numpy(orc):
         assert rel < 3e-7
 
 
-def test_smearing_rule_matches_survey_numbers(orc):
+def test_smearing_rule_matches_the_workloads_numbers(orc):
     # C1: DM 67.99, 16 MHz at 1400 MHz, one channel
     neg = orc.smearing_samples(1400.0, 16.0, 67.99, 1, -1)
     pos = orc.smearing_samples(1400.0, 16.0, 67.99, 1, 1)
