@@ -350,6 +350,67 @@ def cpu_baseline(cfg, target_s=15.0):
                        f"(self-written FP32 FFT, OpenMP over parts), {total:.1f} s")}
 
 
+def noalloc_compare(b2, ctx):
+    """dspsr_b200_convolution_perform_noalloc beside the engine entry point
+    (dspsr_b200_convolution_perform) on one shape that fits the no-alloc
+    entry's static 32 MiB array: one channel, two polarisations, C1's FFT
+    length and smearing, 2^21 complex float samples per polarisation on the
+    device; CUDA events around 10 calls of each after 3 warm-up calls (outside
+    the timed region of the line)."""
+    import ctypes
+    import torch
+    nchan, npol, nfft, pos, neg = 1, 2, 1 << 17, 28462, 29455
+    nk = nfft - pos - neg
+    ndat = 1 << 21
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(5)
+    x = torch.complex(torch.randn((nchan, npol, ndat), generator=gen, device="cuda"),
+                      torch.randn((nchan, npol, ndat), generator=gen, device="cuda"))
+    rng = np.random.default_rng(5)
+    h = ((rng.standard_normal((nchan, nfft)) + 1j * rng.standard_normal((nchan, nfft)))
+         / np.sqrt(nfft)).astype(np.complex64)
+    hd = torch.from_numpy(h).cuda()
+    conv = b2.Convolution(ctx, nchan, npol, nfft, pos, neg)
+    conv.copy_response(h)
+    npart = conv.npart(ndat)
+    out_e = torch.empty((nchan, npol, npart * nk), dtype=torch.complex64, device="cuda")
+    out_n = torch.empty_like(out_e)
+    lib = b2._capi.lib()
+    nret = ctypes.c_uint64()
+
+    def engine():
+        conv.perform(x, ndat, ndat, out_e, npart * nk)
+
+    def noalloc():
+        rc = lib.dspsr_b200_convolution_perform_noalloc(
+            None, x.data_ptr(), ndat, ndat, nchan, npol, nfft, pos, neg, hd.data_ptr(),
+            out_n.data_ptr(), npart * nk, ctypes.byref(nret), None)
+        if rc != 0:
+            raise RuntimeError(f"noalloc call failed: {rc}")
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(10):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 10
+
+    ms_e, ms_n = timed(engine), timed(noalloc)
+    a = out_n.cpu().numpy().astype(np.complex128)
+    b = out_e.cpu().numpy().astype(np.complex128)
+    conv.close()
+    return {"shape": f"{nchan} ch x {npol} pol x {ndat} complex float, nfft {nfft}, "
+                     f"{npart} parts", "engine_ms_per_call": round(ms_e, 4),
+            "noalloc_ms_per_call": round(ms_n, 4),
+            "rel_rms_difference": float(np.sqrt(np.mean(np.abs(a - b) ** 2)
+                                                / np.mean(np.abs(b) ** 2)))}
+
+
 def parity_block(cfg, b2, ctx, pcfg, raw_dev, ndat, pos, neg, nfft, lut):
     """One full block of the timed workload (its first block, a fresh
     pipeline) against the oracle chain on the same bytes: unpack -> (the
@@ -735,6 +796,8 @@ def run_b200(args, cfg, world, rank, local):
                   "profile_peak_over_median": float(np.max(prof) / max(np.median(prof), 1e-30))},
     }
     line.update(extra)
+    if rank == 0 and world == 1 and args.config == "c1":
+        line["noalloc"] = noalloc_compare(b2, ctx)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg)
         line["parity"] = parity_block(cfg, b2, ctx, c, blocks[0], ndat, pos, neg, nfft, lut)
