@@ -310,6 +310,13 @@ __device__ __forceinline__ void smem_fft (float2* s, const float2* tw)
 // K1: forward column DFTs with the unpack fused into the load
 // --------------------------------------------------------------------------
 
+// columns per 128-thread block: one thread per column, two at n1 = 32
+template <int N1>
+constexpr unsigned fwd_cols_per_block ()
+{
+  return N1 == 32 ? 64u : 128u;
+}
+
 template <int N1, int KIND>
 __global__ void __launch_bounds__ (128, 2)
 k_fwd_cols (const InputView in, const float* __restrict__ lut, const uint64_t nkeep,
@@ -319,10 +326,60 @@ k_fwd_cols (const InputView in, const float* __restrict__ lut, const uint64_t nk
   __shared__ float s_lut[256];
   load_lut (in, lut, s_lut);
   __syncthreads ();
-  const unsigned i2 = blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned b = blockIdx.y;
   const unsigned c = blockIdx.z;
   const uint64_t N = uint64_t (N1) * n2;
+  if constexpr (N1 == 32)
+  {
+    // Two threads per column (a 32-point DFT in one thread's registers
+    // spills): thread h of the pair takes rows 2m + h, a 16-point DFT of
+    // them gives E (h = 0) or O (h = 1), thread 1 applies w32^j, and one
+    // exchange gives X[j] = E[j] + w32^j O[j] to thread 0 and
+    // X[j + 16] = E[j] - w32^j O[j] to thread 1.
+    const unsigned h = threadIdx.x & 1;
+    const unsigned i2 = blockIdx.x * 64 + (threadIdx.x >> 1);
+    const uint64_t t0 = (part0 + b) * nkeep + i2;
+    for (unsigned p = 0; p < in.npol; p++)
+    {
+      float2 v[16];
+#pragma unroll
+      for (int m = 0; m < 16; m++)
+        v[m] = fetch<KIND> (in, s_lut, c, p, t0 + uint64_t (2 * m + h) * n2);
+      if (apod)
+      {
+        // Apodization::operate on the part before the forward FFT (Convolution.C:739-743)
+#pragma unroll
+        for (int m = 0; m < 16; m++)
+        {
+          const float w = __ldg (apod + uint64_t (2 * m + h) * n2 + i2);
+          v[m] = make_float2 (__fmul_rn (v[m].x, w), __fmul_rn (v[m].y, w));
+        }
+      }
+      RegDFT<16, -1>::run (v);
+#pragma unroll
+      for (int j = 0; j < 16; j++)
+      {
+        const float2 mine = h ? tw_mul<32, -1> (j, v[j]) : v[j];
+        const float2 other = make_float2 (__shfl_xor_sync (0xffffffffu, mine.x, 1),
+                                          __shfl_xor_sync (0xffffffffu, mine.y, 1));
+        // thread 0: E + O'; thread 1: E - O' (E is the partner's value)
+        v[j] = h ? csub (other, mine) : cadd (mine, other);
+      }
+      const unsigned k0 = 16 * h;
+      float2* dst = scratch + ((uint64_t (b) * in.nchan + c) * in.npol + p) * N + i2;
+#pragma unroll
+      for (int j = 0; j < 16; j++)
+      {
+        const unsigned k1 = k0 + j;
+        float2 y = v[j];
+        // four-step twiddle w_N^{k1 n2} (row k1 of the [n1][n2] table)
+        if (k1) y = cmul (y, __ldg (tw4 + uint64_t (k1) * n2 + i2));
+        dst[uint64_t (k1) * n2] = y;
+      }
+    }
+    return;
+  }
+  const unsigned i2 = blockIdx.x * blockDim.x + threadIdx.x;
   const uint64_t t0 = (part0 + b) * nkeep + i2;
   for (unsigned p = 0; p < in.npol; p++)
   {
@@ -2387,6 +2444,7 @@ cudaError_t run_fourstep_n1 (const ConvShape& sh, const ConvTables& tb, const In
                              const KernelClock* clk)
 {
   const dim3 gcol (sh.n2 / 128, nbatch, sh.nchan);
+  const dim3 gfwd (sh.n2 / fwd_cols_per_block<N1> (), nbatch, sh.nchan);
   if (in.fb_nsub)
   {
     // the 64-channel filterbank inside the column pass
@@ -2410,13 +2468,13 @@ cudaError_t run_fourstep_n1 (const ConvShape& sh, const ConvTables& tb, const In
   {
   ClockScope cs (clk, KK_FWD_COLS, st);
   if (in.kind == IN_INT8)
-    k_fwd_cols<N1, IN_INT8><<<gcol, 128, 0, st>>> (in, tb.lut, sh.nkeep, part0, sh.n2, tb.tw4,
+    k_fwd_cols<N1, IN_INT8><<<gfwd, 128, 0, st>>> (in, tb.lut, sh.nkeep, part0, sh.n2, tb.tw4,
                                                    scratch, tb.apod);
   else if (in.kind == IN_INT16)
-    k_fwd_cols<N1, IN_INT16><<<gcol, 128, 0, st>>> (in, tb.lut, sh.nkeep, part0, sh.n2, tb.tw4,
+    k_fwd_cols<N1, IN_INT16><<<gfwd, 128, 0, st>>> (in, tb.lut, sh.nkeep, part0, sh.n2, tb.tw4,
                                                     scratch, tb.apod);
   else
-    k_fwd_cols<N1, IN_FLOAT><<<gcol, 128, 0, st>>> (in, tb.lut, sh.nkeep, part0, sh.n2, tb.tw4,
+    k_fwd_cols<N1, IN_FLOAT><<<gfwd, 128, 0, st>>> (in, tb.lut, sh.nkeep, part0, sh.n2, tb.tw4,
                                                     scratch, tb.apod);
   }
   const unsigned nrows = N1 * nbatch * sh.nchan * sh.npol;
@@ -2714,16 +2772,17 @@ cudaError_t run_during_n1 (const DuringShape& sh, const DuringTables& tb, const 
                            const KernelClock* clk)
 {
   const dim3 gcol (sh.n2 / 128, nbatch, sh.nchan_in);
+  const dim3 gfwd (sh.n2 / fwd_cols_per_block<N1> (), nbatch, sh.nchan_in);
   {
     ClockScope cs (clk, KK_FWD_COLS, st);
     if (in.kind == IN_INT8)
-      k_fwd_cols<N1, IN_INT8><<<gcol, 128, 0, st>>> (in, tb.lut, sh.in_step, part0, sh.n2, tb.tw4,
+      k_fwd_cols<N1, IN_INT8><<<gfwd, 128, 0, st>>> (in, tb.lut, sh.in_step, part0, sh.n2, tb.tw4,
                                                      scratch, tb.apod);
     else if (in.kind == IN_INT16)
-      k_fwd_cols<N1, IN_INT16><<<gcol, 128, 0, st>>> (in, tb.lut, sh.in_step, part0, sh.n2,
+      k_fwd_cols<N1, IN_INT16><<<gfwd, 128, 0, st>>> (in, tb.lut, sh.in_step, part0, sh.n2,
                                                       tb.tw4, scratch, tb.apod);
     else
-      k_fwd_cols<N1, IN_FLOAT><<<gcol, 128, 0, st>>> (in, tb.lut, sh.in_step, part0, sh.n2,
+      k_fwd_cols<N1, IN_FLOAT><<<gfwd, 128, 0, st>>> (in, tb.lut, sh.in_step, part0, sh.n2,
                                                       tb.tw4, scratch, tb.apod);
   }
   const unsigned nrows = N1 * nbatch * sh.nchan_in * sh.npol;
