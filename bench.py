@@ -19,6 +19,7 @@ independent replicas (weak scaling); rank 0 reports the max-over-ranks time.
 the block per step.
 """
 import argparse
+import contextlib
 import json
 import os
 import statistics
@@ -98,6 +99,49 @@ CONFIGS = {
 }
 
 NBLOCKS = 4
+
+
+def _cpulist(text):
+    out = set()
+    for part in text.strip().split(","):
+        if "-" in part:
+            lo, hi = part.split("-")
+            out.update(range(int(lo), int(hi) + 1))
+        elif part:
+            out.add(int(part))
+    return out
+
+
+@contextlib.contextmanager
+def near_gpu_memory(local, info=None):
+    """Host allocations made inside land in the memory of the NUMA node that
+    the GPU is attached to: the thread runs on that node's cores while the
+    pages are first touched, so the host-to-device copies of the end-to-end
+    figures cross no socket link.  The thread's cores are restored after.
+    Without NUMA information (no node, no sysfs) it changes nothing.  `info`
+    (a dict) receives the node."""
+    old = None
+    try:
+        import torch
+        p = torch.cuda.get_device_properties(local)
+        dev = (f"/sys/bus/pci/devices/{p.pci_domain_id:04x}:{p.pci_bus_id:02x}:"
+               f"{p.pci_device_id:02x}.0")
+        with open(dev + "/numa_node") as f:
+            node = int(f.read())
+        if node >= 0:
+            with open(f"/sys/devices/system/node/node{node}/cpulist") as f:
+                cpus = _cpulist(f.read())
+            old = os.sched_getaffinity(0)
+            os.sched_setaffinity(0, cpus)
+            if info is not None:
+                info["host_numa_node"] = node
+    except Exception:
+        pass
+    try:
+        yield
+    finally:
+        if old is not None:
+            os.sched_setaffinity(0, old)
 
 
 def log(*a):
@@ -609,7 +653,9 @@ def run_b200(args, cfg, world, rank, local):
                          "detection and fold as in the FP32 arm")}
 
     # ---- end to end through the public API from pinned host memory ----------
-    host = [b.cpu().pin_memory() for b in blocks]
+    numa = {}
+    with near_gpu_memory(local, numa):
+        host = [b.cpu().pin_memory() for b in blocks]
     pl = b2.Pipeline(ctx, c)
     for i in range(args.warmup):
         pl.run_host(host[i % NBLOCKS], ndat)
@@ -790,7 +836,7 @@ def run_b200(args, cfg, world, rank, local):
         "e2e": {"value": round(e2e, 3), "unit": "complex Msamples/s",
                 "h2d_bytes_per_step": int(bytes_per_block), "d2h_bytes_per_step": int(d2h),
                 "readback": "each step's profiles copied back asynchronously and waited for "
-                            "once the next block is queued"},
+                            "once the next block is queued", **numa},
         "mixed": mixed or None,
         "check": {"samples_folded": int(folded), "hits_total": int(hits.sum()),
                   "profile_peak_over_median": float(np.max(prof) / max(np.median(prof), 1e-30))},
@@ -963,10 +1009,14 @@ def run_b200_sk(args, cfg, world, rank, local):
     zap_frac = float(mask.float().mean().item())
 
     # ---- end to end: pinned host voltages in, masked voltages and mask out --
-    hx = torch.empty(x.shape, dtype=x.dtype, pin_memory=True)
-    hx.copy_(x)
-    hout = torch.empty(x.shape, dtype=x.dtype, pin_memory=True)
-    hmask = torch.empty(mask.shape, dtype=mask.dtype, pin_memory=True)
+    numa = {}
+    with near_gpu_memory(local, numa):
+        hx = torch.empty(x.shape, dtype=x.dtype, pin_memory=True)
+        hx.copy_(x)
+        hout = torch.empty(x.shape, dtype=x.dtype, pin_memory=True)
+        hout.zero_()
+        hmask = torch.empty(mask.shape, dtype=mask.dtype, pin_memory=True)
+        hmask.zero_()
     for _ in range(max(1, args.warmup)):
         x.copy_(hx, non_blocking=True)
         step(x, x if inplace else out)
@@ -1608,7 +1658,9 @@ def run_b200_c3(args, cfg, world, rank, local):
     other_value = samples_per_step * args.steps / (ms_other / 1e3) / 1e6
 
     # end to end: pinned host blocks uploaded by each stream's pipeline
-    host = [s["blocks"][0].cpu().pin_memory() for s in streams]
+    numa = {}
+    with near_gpu_memory(local, numa):
+        host = [s["blocks"][0].cpu().pin_memory() for s in streams]
     for s, h in zip(streams, host):
         s["pipe"].run_host(h, s["ndat"])
     torch.cuda.synchronize()
@@ -1674,7 +1726,7 @@ def run_b200_c3(args, cfg, world, rank, local):
                           "peak": round(fp32_peak, 1), "frac": round(fp32_tflops / fp32_peak, 4)},
         "e2e": {"value": round(e2e, 3), "unit": "complex Msamples/s",
                 "h2d_bytes_per_step": int(sum(h.numel() for h in host)),
-                "d2h_bytes_per_step": int(d2h)},
+                "d2h_bytes_per_step": int(d2h), **numa},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
