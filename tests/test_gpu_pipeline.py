@@ -286,6 +286,9 @@ CASES = {
     "rows4096_2p15": dict(dm=5.0, bw=64.0, nchan=2, nfft=1 << 15, state=2, nbin=256,
                           row=4096),
     "rows4096_2p17": dict(dm=67.99, nfft=1 << 17, nbin=1024, period=0.08933, row=4096),
+    # the largest FFT of the multi-stream workload: 2^18 = 32 x 8192 (the
+    # 32-row column passes), full Stokes
+    "c3_2p18_stokes": dict(dm=100.0, bw=16.0, nfft=1 << 18, state=3, nbin=512, period=0.05),
     # the rows on the tensor cores (three BF16 terms), four channels
     "tensor_rows_4ch": dict(dm=8.0, bw=32.0, nchan=4, nfft=1 << 15, state=3, nbin=256, fft=3),
     "fused8k_table": dict(dm=5.0, lut=(np.asarray(__import__("dspsr_b200").bittable8()[0])
