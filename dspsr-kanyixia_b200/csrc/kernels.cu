@@ -795,12 +795,75 @@ k_inv_cols (const float2* __restrict__ scratch, const unsigned n2, const unsigne
             const uint64_t nkeep, const unsigned nfilt_pos, const uint64_t part0,
             const float2* __restrict__ tw4, const FoldView fv, const VoltView vv)
 {
-  const unsigned i2 = blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned b = blockIdx.y;
   const unsigned c = blockIdx.z;
   const uint64_t N = uint64_t (N1) * n2;
   const uint64_t tbase0 = (part0 + b) * nkeep;
+  if constexpr (N1 == 32)
+  {
+    // Two threads per column (16 columns per warp): thread h = lane & 1 of a
+    // pair takes rows 2m + h, a 16-point inverse DFT of them gives E (h = 0)
+    // or O (h = 1), thread 1 applies w32^j, one exchange leaves
+    // X[j] = E[j] + w32^j O[j] with thread 0 and X[j + 16] = E[j] - w32^j O[j]
+    // with thread 1; a second shuffle moves them so that lanes 0..15 hold
+    // X[j] of the warp's 16 columns and lanes 16..31 X[j + 16] (runs of
+    // consecutive samples for the fold).
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned h = lane & 1;
+    const unsigned colw = blockIdx.x * 64 + (threadIdx.x >> 5) * 16;
+    const unsigned i2 = colw + (lane >> 1);
+    float2 v[NPOL][16];
+#pragma unroll
+    for (int m = 0; m < 16; m++)
+    {
+      const unsigned k = 2 * m + h;
+      const float2 w = __ldg (tw4 + uint64_t (k) * n2 + i2);
+#pragma unroll
+      for (int p = 0; p < NPOL; p++)
+      {
+        const float2 x = scratch[((uint64_t (b) * nchan + c) * NPOL + p) * N + uint64_t (k) * n2 + i2];
+        v[p][m] = k ? cmulc (x, w) : x;
+      }
+    }
+    const int srcl = lane < 16 ? 2 * int (lane) : 2 * (int (lane) - 16) + 1;
+#pragma unroll
+    for (int p = 0; p < NPOL; p++)
+    {
+      RegDFT<16, +1>::run (v[p]);
+#pragma unroll
+      for (int j = 0; j < 16; j++)
+      {
+        const float2 mine = h ? tw_mul<32, +1> (j, v[p][j]) : v[p][j];
+        const float2 other = make_float2 (__shfl_xor_sync (FULL, mine.x, 1),
+                                          __shfl_xor_sync (FULL, mine.y, 1));
+        const float2 x = h ? csub (other, mine) : cadd (mine, other);
+        v[p][j] = make_float2 (__shfl_sync (FULL, x.x, srcl), __shfl_sync (FULL, x.y, srcl));
+      }
+    }
+    const unsigned ocol = colw + (lane & 15), koff = 16 * (lane >> 4);
+#pragma unroll
+    for (int j = 0; j < 16; j++)
+    {
+      const uint64_t tl = uint64_t (koff + j) * n2 + ocol;
+      const bool ok = tl >= nfilt_pos && tl < nfilt_pos + nkeep;
+      const uint64_t t = tbase0 + (tl - nfilt_pos);
+      if constexpr (MODE == OUT_VOLTAGE)
+      {
+        if (ok)
+        {
+#pragma unroll
+          for (int p = 0; p < NPOL; p++)
+            vv.out[(uint64_t (c) * NPOL + p) * vv.span + t] = v[p][j];
+        }
+      }
+      else
+        emit_fold<NOUT> (fv, c, NPOL, ok, t, v[0][j], v[NPOL - 1][j]);
+    }
+    return;
+  }
+  const unsigned i2 = blockIdx.x * blockDim.x + threadIdx.x;
   if constexpr (stage_first_pol<N1, NPOL> ())
+
   {
     __shared__ float2 s0[N1 * 128];
     const float2* src = scratch + (uint64_t (b) * nchan + c) * 2 * N + i2;
@@ -2418,6 +2481,7 @@ template <int N1, int NPOL, int MODE, int NOUT>
 void launch_inv (const ConvShape& sh, dim3 grid, float2* scratch, uint64_t part0,
                  const ConvTables& tb, const FoldView& fv, const VoltView& vv, cudaStream_t st)
 {
+  if (N1 == 32) grid.x = sh.n2 / 64;        // two threads per column
   k_inv_cols<N1, NPOL, MODE, NOUT><<<grid, 128, 0, st>>> (scratch, sh.n2, sh.nchan, sh.nkeep,
                                                           sh.nfilt_pos, part0, tb.tw4, fv, vv);
 }
